@@ -1,0 +1,306 @@
+"""Benchmark: LDL^T factor + solve at backward error <= 1e-14 on a B200.
+
+Workload (one step): the complex-symmetric 3D 7-point Helmholtz matrix
+A = -Delta_h - k^2 (1 + 0.05 i) I on a side^3 grid (default 64^3, n = 262,144),
+k^2 = 0.2 lambda_max, 16 right-hand sides with U[-1, 1) real and imaginary
+parts (seed 1).  Analysis (ordering + symbolic) is done once, outside the
+timed region, as in the reference's methodology.
+  * headline (`value`): the mixed-precision path — c32 numeric factor on the
+    GPU + FP64 refinement against the original A (IR -> GMRES-IR) until every
+    right-hand side's normwise backward error is <= 1e-14; GFLOP/s counts the
+    model flops of the FP64-equivalent factor (sum_s sum_m (m^2 - 1), x4 for
+    complex) per step time;
+  * `fp64_gpu`: the plain FP64 GPU factor + solve (+ FP64 IR to 1e-14) on the
+    same matrix, for the mixed/FP64 ratio;
+  * `e2e`: the mixed path through the public Python API with host buffers
+    (values + RHS copied in, solution copied out, every step).
+Multi-GPU (--gpus N under torchrun): replicas — each rank factors and solves
+its own copy (the path does not shard), value = N x per-rank work / max time.
+`--impl reference` times the CPU oracle (C++ restatement of the reference's
+CPU path) on a bounded sample on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+EPS = 2.220446049250313e-16
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--side", type=int, default=64)
+    p.add_argument("--nrhs", type=int, default=16)
+    p.add_argument("--target", type=float, default=1e-14)
+    p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--cpu-sample-side", type=int, default=24)
+    return p.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev: int):
+        self.dev = dev
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def allmax(v: float, ws: int) -> float:
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference(args, ws, rank):
+    """CPU oracle on a bounded sample (rank 0 only)."""
+    if rank != 0:
+        return
+    from oracle.oracle import OracleSolver, backward_error, mixed_solve
+    from rslab_b200 import LdltSymbolic, matgen
+    side = args.cpu_sample_side
+    a = matgen.c2_matrix(side)
+    sym = LdltSymbolic.analyze(a)
+    flops = 4.0 * sym.info().flops_model
+    b = matgen.uniform_rhs(a.n, args.nrhs, 1, complex_=True)
+    cores = os.cpu_count()
+    times = []
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        o = OracleSolver(a, sym.export())
+        x = o.solve_many(b, args.nrhs)
+        dt = time.perf_counter() - t0
+        if it >= args.warmup:
+            times.append(dt)
+    be = backward_error(a, x, b)
+    t = float(np.mean(times))
+    gf = flops / t / 1e9
+    line = {
+        "impl": "reference", "metric": "LDLT factor+solve GFLOP/s at bwd err <= 1e-14 (mixed/batched vs FP64 GPU)",
+        "value": gf, "unit": "GFLOP/s", "higher_is_better": True, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3, "dtype": "c64", "data": "synthetic",
+        "config": {"workload": f"helmholtz3d_{side}^3_c64_nrhs{args.nrhs}_cpu_sample", "n": a.n, "nrhs": args.nrhs},
+        "cpu_baseline": {"value": gf, "unit": "GFLOP/s", "cores": cores, "kind": "port",
+                         "sample": f"FP64 factor+solve of the {side}^3 Helmholtz sample (n={a.n}), "
+                                   f"model flops {flops:.3g}; backward error {be:.2e}"},
+        "e2e": {"value": gf, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "vs_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init(args)
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        return
+    import torch
+
+    from rslab_b200 import LdltSymbolic, MixedLdltSolver, SolverSettings, matgen
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    a = matgen.c2_matrix(args.side)
+    n, nrhs = a.n, args.nrhs
+    sym = LdltSymbolic.analyze(a)
+    info = sym.info()
+    flops = 4.0 * info.flops_model  # complex: 4 real flops per complex multiply-add pair
+    b = matgen.uniform_rhs(n, nrhs, 1, complex_=True)
+    vals_d = torch.from_numpy(np.ascontiguousarray(a.values)).to(dev)
+    b_d = torch.from_numpy(np.ascontiguousarray(b)).to(dev)
+    x_d = torch.empty_like(b_d)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    st = SolverSettings()
+    mixed = MixedLdltSolver.factor_with(a, st, sym=sym)
+    stream = torch.cuda.ExternalStream(mixed.stream())
+    import ctypes as C
+
+    from rslab_b200 import _native as N
+
+    def mixed_step():
+        rc = N.lib.rslab_refactor(mixed._h, C.c_void_p(vals_d.data_ptr()), 1)
+        assert rc == 0, N.last_error()
+        inf = N.MixedInfoC()
+        rc = N.lib.rslab_mixed_solve(mixed._h, C.c_void_p(b_d.data_ptr()), nrhs, args.target,
+                                     C.c_void_p(x_d.data_ptr()), 1, C.byref(inf))
+        assert rc == 0, N.last_error()
+        return inf
+
+    def timed(fn, steps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        barrier(ws)
+        tot = 0.0
+        last = None
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            last = fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        barrier(ws)
+        return tot / steps, last
+
+    clk = ClockSampler(local)
+    clk.start()
+    ms_mixed, minfo = timed(mixed_step, args.steps, args.warmup)
+    clocks = clk.stop()
+    ms_mixed = allmax(ms_mixed, ws)
+
+    out_fp64 = None
+    if not args.no_fp64:
+        f64 = sym.factor(a, st)
+        s64 = f64.stream()
+        stream64 = torch.cuda.ExternalStream(s64)
+
+        def fp64_step():
+            rc = N.lib.rslab_refactor(f64._h, C.c_void_p(vals_d.data_ptr()), 1)
+            assert rc == 0, N.last_error()
+            rc = N.lib.rslab_solve(f64._h, C.c_void_p(b_d.data_ptr()), nrhs, C.c_void_p(x_d.data_ptr()), 1)
+            assert rc == 0, N.last_error()
+
+        stream_save = stream
+        stream = stream64
+        ms64, _ = timed(fp64_step, max(1, args.steps // 2), 1)
+        stream = stream_save
+        ms64 = allmax(ms64, ws)
+        x64 = x_d.cpu().numpy()
+        from oracle.oracle import backward_error
+        be64 = backward_error(a, x64, b)
+        fi = N.FactorInfo()
+        N.lib.rslab_factor_info(f64._h, C.byref(fi))
+        out_fp64 = {"ms_per_step": ms64, "factor_ms": fi.factor_ms, "solve_ms": fi.solve_ms,
+                    "gflops": flops / (ms64 * 1e-3) / 1e9, "backward_error_no_ir": be64}
+
+    # End-to-end through the public API with host buffers.
+    t_e2e = []
+    for it in range(1 + args.steps):
+        t0 = time.perf_counter()
+        mixed.refactor(a)
+        x_h, inf_h = mixed.solve_to(a, b, args.target)
+        dt = time.perf_counter() - t0
+        if it > 0:
+            t_e2e.append(dt)
+    e2e_s = allmax(float(np.mean(t_e2e)), ws)
+    fi = N.FactorInfo()
+    N.lib.rslab_factor_info(mixed._h, C.byref(fi))
+    gflops = flops / (ms_mixed * 1e-3) / 1e9 * ws
+    if rank == 0:
+        line = {
+            "metric": "LDLT factor+solve GFLOP/s at bwd err <= 1e-14 (mixed/batched vs FP64 GPU)",
+            "value": gflops, "unit": "GFLOP/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c32 factor / f64 refinement", "data": "synthetic",
+            "config": {"workload": f"helmholtz3d_{args.side}^3_c64_nrhs{nrhs}", "n": n, "nnz_lower": a.nnz,
+                       "nrhs": nrhs, "ordering": "AMD", "target_backward_error": args.target,
+                       "model_flops": flops, "factor_nnz_panels": info.panel_elems,
+                       "parallelism": f"replicas{ws}", "l2": "flushed between steps (256 MB write)"},
+            "mixed": {"certified": bool(minfo.certified), "backward_error": minfo.backward_error,
+                      "ir_iters": minfo.ir_iters, "gmres_iters": minfo.gmres_iters,
+                      "last_factor_ms": fi.factor_ms},
+            "fp64_gpu": out_fp64,
+            "e2e": {"value": flops / e2e_s / 1e9 * ws, "unit": "GFLOP/s", "seconds_per_step": e2e_s,
+                    "h2d_bytes_per_step": int(a.values.nbytes + b.nbytes),
+                    "d2h_bytes_per_step": int(b.nbytes), "certified": bool(inf_h.certified)},
+            "clocks": clocks,
+            "roofline": None,
+            "cpu_baseline": None,
+            "gpu_launches": int(info.n_factor_launches),
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,169 @@
+/*
+ * rslab_b200 — C ABI of the B200-native supernodal LDL^T factor + solve.
+ *
+ * The drop-in boundary for RSLAB's symmetric direct-solver path.  Every entry
+ * point takes plain pointers and sizes, returns an int status (0 = ok) and
+ * never throws; rslab_last_error() gives the message of the calling thread's
+ * last failure.  Status codes mirror RslabError (src/error.rs:15-55).
+ *
+ * Reference interfaces replaced (paths in the RSLAB source tree):
+ *   rslab_analyze        LdltSymbolic::analyze / analyze_with
+ *                        (src/numeric/sparse_solver.rs:493,506) ->
+ *                        multifrontal_ldlt::analyze_with (src/numeric/multifrontal_ldlt.rs:1667)
+ *   rslab_factor         LdltSymbolic::factor (src/numeric/sparse_solver.rs:677) ->
+ *                        factor_numeric (src/numeric/multifrontal_ldlt.rs:1851)
+ *   rslab_refactor       LdltSymbolic::factor on a new value set of the same
+ *                        pattern (frequency sweeps, src/numeric/sparse_solver.rs:457-478)
+ *   rslab_solve          LdltSolver::solve / solve_many (src/numeric/sparse_solver.rs:274,302)
+ *   rslab_mixed_factor   MixedLdltSolver::factor / factor_with (src/numeric/mixed.rs:234,245)
+ *   rslab_mixed_solve    MixedLdltSolver::solve / solve_to (src/numeric/mixed.rs:258,267)
+ *   rslab_factor_info    LdltSolver::inertia / n_perturbed / diagnostics
+ *                        (src/numeric/sparse_solver.rs:81,72,57)
+ *   rslab_export_factors LdltFactors (src/dense/ldlt_generic.rs:31-66), the
+ *                        factor_numeric return value
+ *   rslab_amd_order      rslab_amd::amd_order (crates/rslab-amd/src/lib.rs:66)
+ */
+#ifndef RSLAB_B200_H
+#define RSLAB_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RSLAB_ABI_VERSION 1
+
+/* Status codes (RslabError). */
+#define RSLAB_OK 0
+#define RSLAB_NUMERICALLY_RANK_DEFICIENT 1
+#define RSLAB_INVALID_INPUT 2
+#define RSLAB_DIMENSION_MISMATCH 3
+#define RSLAB_CUDA_ERROR 4
+
+/* Scalar fields: the reference's f64 / Complex<f64> / f32 / Complex<f32>.
+ * Complex values are interleaved (re, im) pairs; complex matrices are
+ * complex-SYMMETRIC (A = A^T), never Hermitian. */
+#define RSLAB_F64 0
+#define RSLAB_C64 1
+#define RSLAB_F32 2
+#define RSLAB_C32 3
+
+/* Orderings (OrderingMethod, src/symbolic/mod.rs:28). */
+#define RSLAB_ORDER_AMD 0
+#define RSLAB_ORDER_METIS_ND 1
+#define RSLAB_ORDER_NATURAL 2
+#define RSLAB_ORDER_GIVEN 3
+
+/* Zero-pivot policy (ZeroPivotAction, src/numeric/multifrontal_ldlt.rs:165). */
+#define RSLAB_PIVOT_FAIL 0
+#define RSLAB_PIVOT_PERTURB 1
+
+/* Equilibration (ScalingStrategy): one-pass inf-norm (default) or identity. */
+#define RSLAB_SCALING_ONEPASS 0
+#define RSLAB_SCALING_IDENTITY 1
+
+typedef struct rslab_sym_handle rslab_sym_handle;
+typedef struct rslab_fac_handle rslab_fac_handle;
+
+/* Analyze-time half of SolverSettings (defaults :583-614). */
+typedef struct {
+  int32_t ordering;            /* RSLAB_ORDER_* (default AMD) */
+  int64_t nemin;               /* 16 */
+  int32_t relax;               /* relaxed amalgamation on (1) */
+  int64_t relax_max_width;     /* 256 */
+  int64_t relax_max_extra_rows;/* 64 */
+  int32_t hybrid_liu;          /* child reordering (scheduling only) */
+  int64_t panel_nb;            /* BK panel width, 64 (128 when ncol >= 512) */
+  const int64_t* given_perm;   /* RSLAB_ORDER_GIVEN: new-to-old permutation */
+} rslab_analyze_settings;
+
+/* Numeric half of SolverSettings. */
+typedef struct {
+  int32_t on_zero_pivot;       /* RSLAB_PIVOT_FAIL | RSLAB_PIVOT_PERTURB */
+  double abs_floor;            /* PerturbToEps floor */
+  int32_t scaling;             /* RSLAB_SCALING_* */
+  int32_t use_graph;           /* capture factor / solve as CUDA graphs (1) */
+  void* stream;                /* cudaStream_t to run on, or NULL for a private one */
+} rslab_factor_settings;
+
+typedef struct {
+  int64_t n, nnz, nsuper, nlevels;
+  int64_t factor_nnz_sym;      /* sum of symbolic column counts */
+  int64_t panel_elems;         /* device panel pool size in scalars */
+  double flops_model;          /* sum_s sum_{m=r-c+1}^{r} (m^2 - 1) */
+  double flops_proxy;          /* sum_s r^2 c (factor_flops of the reference) */
+  int32_t renumbered;
+  int64_t amd_ncmpa, amd_ndense;
+  double amd_ndiv, amd_nms_ldl, amd_nms_lu;
+  int64_t n_factor_launches, n_solve_launches;
+} rslab_symbolic_info_t;
+
+typedef struct {
+  int32_t status;              /* last factor status */
+  int64_t failing_supernode;
+  int64_t inertia_pos, inertia_neg, inertia_zero;
+  int64_t n_perturbed;
+  double factor_ms, solve_ms;  /* device time of the last factor / solve */
+  int32_t dtype, dtype_hi;
+} rslab_factor_info_t;
+
+typedef struct {
+  int64_t ir_iters;
+  int64_t gmres_iters;
+  double backward_error;       /* max over right-hand sides */
+  int32_t certified;           /* backward_error <= target for every rhs */
+} rslab_mixed_info;
+
+int rslab_version(void);
+const char* rslab_last_error(void);
+int rslab_device_count(int* count);
+
+void rslab_default_analyze_settings(rslab_analyze_settings* s);
+void rslab_default_factor_settings(rslab_factor_settings* s);
+
+/* Phase 1: analyze a lower-triangle CSC pattern (n, col_ptr[n+1], row_idx). */
+int rslab_analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx,
+                  const rslab_analyze_settings* settings, rslab_sym_handle** out);
+int rslab_symbolic_info(const rslab_sym_handle* sym, rslab_symbolic_info_t* info);
+int rslab_symbolic_export(const rslab_sym_handle* sym, int64_t* perm, int64_t* sn_first, int64_t* sn_ncol,
+                          int64_t* sn_nrow, int64_t* sn_level, int64_t* child_ptr, int64_t* child_idx,
+                          int64_t* col_counts, int64_t* parent);
+void rslab_free_symbolic(rslab_sym_handle* sym);
+
+/* Phases 2-3: equilibrate + numeric factor on the GPU.  `values` follow the
+ * analysed pattern's row_idx order; host memory unless values_on_device.  On a
+ * singular pivot returns RSLAB_NUMERICALLY_RANK_DEFICIENT and still hands
+ * back the handle (for rslab_factor_info); it must be freed. */
+int rslab_factor(rslab_sym_handle* sym, int dtype, const void* values, int values_on_device,
+                 const rslab_factor_settings* settings, rslab_fac_handle** out);
+int rslab_refactor(rslab_fac_handle* fac, const void* values, int values_on_device);
+/* x = A^-1 b, b and x row-major n x nrhs. */
+int rslab_solve(rslab_fac_handle* fac, const void* b, int64_t nrhs, void* x, int on_device);
+int rslab_factor_info(const rslab_fac_handle* fac, rslab_factor_info_t* info);
+void* rslab_factor_stream(const rslab_fac_handle* fac);
+/* Reference LdltFactors layout; pass NULL arrays to query *nnz_out first. */
+int rslab_export_factors(const rslab_fac_handle* fac, int64_t* l_col_ptr, int64_t* l_row_idx, void* l_values,
+                         void* d_diag, void* d_subdiag, uint8_t* two_by_two, int64_t* perm, double* scale,
+                         int64_t* nnz_out);
+void rslab_free_factor(rslab_fac_handle* fac);
+
+/* Mixed precision: factor cast(A) in f32/c32, refine against the f64/c64 A. */
+int rslab_mixed_factor(rslab_sym_handle* sym, int dtype_hi, const void* values_hi, int values_on_device,
+                       const rslab_factor_settings* settings, rslab_fac_handle** out);
+int rslab_mixed_solve(rslab_fac_handle* fac, const void* b, int64_t nrhs, double target, void* x, int on_device,
+                      rslab_mixed_info* info);
+
+/* Synthetic-workload generator: m unit draws of the xorshift64* state
+ * `state`; returns the advanced state. */
+uint64_t rslab_rng_units(uint64_t state, int64_t m, double* out);
+
+/* AMD on a full symmetric pattern; stats7 = ncmpa, ndense, ndiv, nms_ldl,
+ * nms_lu, mass eliminations, supervariable merges. */
+int rslab_amd_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, int64_t* perm, double* stats7);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RSLAB_B200_H */

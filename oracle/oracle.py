@@ -1,0 +1,164 @@
+"""ORACLE — test infrastructure only (see oracle.cpp).
+
+ctypes wrapper of oracle/_build/liboracle.so, the C++ restatement of the
+reference CPU LDL^T path.  Only tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg may import this module; the rslab_b200 product never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+
+_DT = {np.dtype(np.float64): 0, np.dtype(np.complex128): 1, np.dtype(np.float32): 2, np.dtype(np.complex64): 3}
+i64p = C.POINTER(C.c_int64)
+vp = C.c_void_p
+
+
+def build() -> Path:
+    src = HERE / "oracle.cpp"
+    if not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+        subprocess.run(["bash", str(HERE / "build_oracle.sh")], check=True, stdout=subprocess.DEVNULL)
+    return LIB
+
+
+def _load():
+    build()
+    lib = C.CDLL(str(LIB))
+    lib.oracle_factor.restype = vp
+    lib.oracle_factor.argtypes = [C.c_int, C.c_int64, i64p, i64p, vp, i64p, C.c_int64, i64p, i64p, i64p, i64p,
+                                  C.c_int, C.c_double, C.c_double, C.c_int64, C.POINTER(C.c_int)]
+    lib.oracle_factor_nnz.restype = C.c_int64
+    lib.oracle_factor_nnz.argtypes = [vp]
+    lib.oracle_export.restype = None
+    lib.oracle_export.argtypes = [vp, i64p, i64p, vp, vp, vp, C.POINTER(C.c_uint8), i64p, C.POINTER(C.c_double),
+                                  i64p]
+    lib.oracle_solve.restype = C.c_int
+    lib.oracle_solve.argtypes = [vp, vp, C.c_int64, vp]
+    lib.oracle_mixed_solve.restype = C.c_int
+    lib.oracle_mixed_solve.argtypes = [vp, C.c_int, C.c_int64, i64p, i64p, vp, vp, C.c_double, vp, i64p,
+                                       C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    lib.oracle_symv.restype = None
+    lib.oracle_symv.argtypes = [C.c_int, C.c_int64, i64p, i64p, vp, vp, vp]
+    lib.oracle_free.restype = None
+    lib.oracle_free.argtypes = [vp]
+    return lib
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = _load()
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(i64p)
+
+
+@dataclass
+class OracleFactors:
+    n: int
+    l_col_ptr: np.ndarray
+    l_row_idx: np.ndarray
+    l_values: np.ndarray
+    d_diag: np.ndarray
+    d_subdiag: np.ndarray
+    two_by_two: np.ndarray
+    perm: np.ndarray
+    scale: np.ndarray
+    inertia: tuple
+    n_perturbed: int
+    status: int
+
+
+class OracleSolver:
+    """LdltSymbolic::factor + LdltSolver::solve_many restated on the CPU."""
+
+    def __init__(self, a, sym_export: dict, dtype=None, perturb_floor: float = -1.0, panel_nb: int = 64,
+                 scaling: bool = True):
+        self.a = a
+        vals = np.ascontiguousarray(a.values if dtype is None else a.values.astype(dtype))
+        self.dtype = vals.dtype
+        self.vals = vals
+        st = C.c_int(0)
+        s = sym_export
+        self.sn_first = np.ascontiguousarray(s["sn_first"], np.int64)
+        self.sn_ncol = np.ascontiguousarray(s["sn_ncol"], np.int64)
+        self.cp = np.ascontiguousarray(s["child_ptr"], np.int64)
+        self.ci = np.ascontiguousarray(s["child_idx"] if len(s["child_idx"]) else np.zeros(1, np.int64), np.int64)
+        self.perm = np.ascontiguousarray(s["perm"], np.int64)
+        self.h = lib().oracle_factor(_DT[self.dtype], a.n, _p(a.col_ptr), _p(a.row_idx),
+                                     vals.ctypes.data_as(vp), _p(self.perm), len(self.sn_first), _p(self.sn_first),
+                                     _p(self.sn_ncol), _p(self.cp), _p(self.ci), int(scaling), perturb_floor, -1.0,
+                                     panel_nb, C.byref(st))
+        self.status = st.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_free(self.h)
+            self.h = None
+
+    def factors(self) -> OracleFactors:
+        n = self.a.n
+        nnz = lib().oracle_factor_nnz(self.h)
+        lcp = np.zeros(n + 1, np.int64)
+        lri = np.zeros(max(nnz, 1), np.int64)
+        lv = np.zeros(max(nnz, 1), self.dtype)
+        d = np.zeros(n, self.dtype)
+        ds = np.zeros(n, self.dtype)
+        two = np.zeros(n, np.uint8)
+        perm = np.zeros(n, np.int64)
+        scale = np.zeros(n, np.float64)
+        info = np.zeros(5, np.int64)
+        lib().oracle_export(self.h, _p(lcp), _p(lri), lv.ctypes.data_as(vp), d.ctypes.data_as(vp),
+                            ds.ctypes.data_as(vp), two.ctypes.data_as(C.POINTER(C.c_uint8)), _p(perm),
+                            scale.ctypes.data_as(C.POINTER(C.c_double)), _p(info))
+        return OracleFactors(n, lcp, lri[:nnz], lv[:nnz], d, ds, two.astype(bool), perm, scale,
+                             (int(info[0]), int(info[1]), int(info[2])), int(info[3]), int(info[4]))
+
+    def solve_many(self, b: np.ndarray, nrhs: int) -> np.ndarray:
+        b = np.ascontiguousarray(b, self.dtype).reshape(-1)
+        x = np.zeros_like(b)
+        rc = lib().oracle_solve(self.h, b.ctypes.data_as(vp), nrhs, x.ctypes.data_as(vp))
+        if rc != 0:
+            raise RuntimeError(f"oracle solve status {rc}")
+        return x.reshape(self.a.n, nrhs) if nrhs > 1 else x
+
+
+def mixed_solve(lo: OracleSolver, a, b: np.ndarray, target: float):
+    """MixedLdltSolver::solve_to with `lo` the f32/c32 oracle factor of cast(A)."""
+    hi = np.ascontiguousarray(a.values)
+    dt_hi = _DT[hi.dtype]
+    b = np.ascontiguousarray(b, hi.dtype)
+    x = np.zeros_like(b)
+    it = np.zeros(2, np.int64)
+    be = C.c_double(0)
+    cert = C.c_int(0)
+    rc = lib().oracle_mixed_solve(lo.h, dt_hi, a.n, _p(a.col_ptr), _p(a.row_idx), hi.ctypes.data_as(vp),
+                                  b.ctypes.data_as(vp), target, x.ctypes.data_as(vp), _p(it), C.byref(be),
+                                  C.byref(cert))
+    if rc != 0:
+        raise RuntimeError(f"oracle mixed solve status {rc}")
+    return x, {"ir_iters": int(it[0]), "gmres_iters": int(it[1]), "backward_error": be.value,
+               "certified": bool(cert.value)}
+
+
+def backward_error(a, x: np.ndarray, b: np.ndarray) -> float:
+    """Normwise ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) per column (max)."""
+    A = a.to_scipy_full()
+    r = b - A @ x
+    anorm = float(abs(A).sum(axis=1).max())
+    if x.ndim == 1:
+        x, r, b = x[:, None], r[:, None], b[:, None]
+    be = np.abs(r).max(axis=0) / np.maximum(anorm * np.abs(x).max(axis=0) + np.abs(b).max(axis=0), 1e-300)
+    return float(be.max())

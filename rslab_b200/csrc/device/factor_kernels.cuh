@@ -1,0 +1,737 @@
+// sm_100a kernels of the supernodal left-looking Bunch-Kaufman LDL^T factor.
+//
+// Data layout in HBM (one pool per factor handle, offsets fixed at analysis):
+//   panel[s]  : nrow_s x ncol_s column-major (stride nrow_s) at poff[s]; after
+//               the factor rows/cols are in the panel's pivot order, the
+//               strictly-lower part holds L (2x2 coupling entry = d21, never
+//               read as L), the diagonal holds D.
+//   e-indexed : d[n], dsub[n], kind[n] (0 = 1x1, 1/2 = first/second column of
+//               a 2x2 block), lperm[n] (pivot position -> pre-pivot local
+//               column) — e = first_col(s) + pivot position.
+// Kernels (one level of the assembly tree per launch group):
+//   k_assemble      scatter-add of the equilibrated A (precomputed targets)
+//   k_cmod          tile-owner gather of every descendant update (deterministic
+//                   updater order, no atomics) — ll_factor_node cmod
+//   k_getf2         panel-bounded BK on one nb-wide block — ll_cdiv_emit getf2
+//   k_deep          deep-row replay of a block's swaps/transforms —
+//                   apply_bk_panel_trailing
+//   k_schur         deferred in-panel Schur update of the remaining columns
+// Reference: src/numeric/multifrontal_ldlt.rs:2400-3256, 1347-1408.
+#pragma once
+
+#include "scalar.cuh"
+
+namespace rsd {
+
+constexpr int TILE = 64;      // output tile edge of the GEMM-class kernels
+constexpr int TPB = 256;      // threads per CTA of the GEMM-class kernels
+constexpr int FUSE_DEEP_ROWS = 192;  // getf2 replays this many deep rows itself
+
+struct FactorArgs {
+  // structure (device)
+  const int* sn_first;
+  const int* sn_ncol;
+  const int* sn_nrow;
+  const long long* sn_poff;
+  const long long* sn_rsoff;
+  const int* rs;
+  const int* upd_ptr;
+  const int* upd_k;
+  const int* upd_p0;
+  const int* upd_p1;
+  // numeric state
+  void* panel;
+  void* d;
+  void* dsub;
+  unsigned char* kind;
+  int* lperm;
+  void* scratch;        // per getf2 slot: snap[nb*nb] T + swaps[nb] int
+  long long scratch_stride;  // bytes per slot
+  int* status;          // [0] = error code, [1] = first failing supernode, [2] = n_perturbed
+  double perturb_floor; // < 0: exact mode
+};
+
+// ---------------------------------------------------------------------------
+// Equilibration + assembly.
+// ---------------------------------------------------------------------------
+
+// Row maxima of |A| over the stored lower triangle, both triangles counted
+// (onepass_scale, src/numeric/sparse_solver.rs:399-421).  Non-negative
+// doubles order like their bit patterns, so atomicMax on the bits is exact
+// and order independent.
+template <typename T>
+__global__ void k_rowmax(long long nnz, const int* __restrict__ row, const int* __restrict__ col,
+                         const T* __restrict__ val, unsigned long long* __restrict__ rmax) {
+  long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= nnz) return;
+  double m = Field<T>::mag(val[k]);
+  unsigned long long b = __double_as_longlong(m);
+  int i = row[k], j = col[k];
+  atomicMax(&rmax[i], b);
+  if (i != j) atomicMax(&rmax[j], b);
+}
+
+// s_i = 1/sqrt(rowmax_i), guarded (src/scaling/mod.rs:85-96).
+__global__ void k_scale_from_rowmax(int n, const unsigned long long* __restrict__ rmax, double* __restrict__ s) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double m = __longlong_as_double(rmax[i]);
+  double r = 1.0;
+  if (m > 0.0) {
+    double c = 1.0 / sqrt(m);
+    if (isfinite(c) && c > 0.0) r = c;
+  }
+  s[i] = r;
+}
+
+// panel[dst[k]] = A_k * s_i * s_j.  Every stored entry has its own target
+// (the permutation is a bijection), so this is a plain scatter.
+template <typename T>
+__global__ void k_assemble(long long nnz, const int* __restrict__ row, const int* __restrict__ col,
+                           const T* __restrict__ val, const double* __restrict__ s,
+                           const long long* __restrict__ dst, T* __restrict__ panel) {
+  long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= nnz) return;
+  int i = row[k], j = col[k];
+  panel[dst[k]] = Field<T>::scale(val[k], s[i] * s[j]);
+}
+
+// Demote a high-precision value array to the low-precision field.
+template <typename Hi, typename Lo>
+__global__ void k_demote(long long nnz, const Hi* __restrict__ a, Lo* __restrict__ b);
+
+template <>
+__global__ void k_demote<double, float>(long long nnz, const double* __restrict__ a, float* __restrict__ b) {
+  long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k < nnz) b[k] = (float)a[k];
+}
+template <>
+__global__ void k_demote<c64, c32>(long long nnz, const c64* __restrict__ a, c32* __restrict__ b) {
+  long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k < nnz) b[k] = c32{(float)a[k].re, (float)a[k].im};
+}
+
+// ---------------------------------------------------------------------------
+// Shared GEMM-class tile engine: acc[i][j] = sum_t A(i,t) * G(j,t), G = L*D,
+// i, j < 64, computed by 256 threads as 4x4 register micro-tiles
+// (rows ty + 16*ii, cols tx + 16*jj).
+// ---------------------------------------------------------------------------
+
+template <typename T> struct KChunk { static constexpr int v = 16; };
+template <> struct KChunk<c64> { static constexpr int v = 8; };
+
+// G(j, t) for column t of a factored panel with block-diagonal D.
+template <typename T>
+__device__ __forceinline__ T ld_G(const T* __restrict__ L, long long ld, int j, int t, const T* __restrict__ d,
+                                  const T* __restrict__ dsub, const unsigned char* __restrict__ kind) {
+  using F = Field<T>;
+  unsigned char kd = kind[t];
+  T a = L[j + (long long)t * ld];
+  if (kd == 0) return F::mul(a, d[t]);
+  if (kd == 1) {
+    T b = L[j + (long long)(t + 1) * ld];
+    return F::add(F::mul(d[t], a), F::mul(dsub[t], b));
+  }
+  T p = L[j + (long long)(t - 1) * ld];
+  return F::add(F::mul(dsub[t - 1], p), F::mul(d[t], a));
+}
+
+// A rows  : L_A + i (i < arows), column t at stride lda
+// G rows  : L_B + j (j < brows), column t at stride ldb; D indexed by t
+template <typename T>
+__device__ void tile_product(T (&acc)[4][4], const T* __restrict__ LA, long long lda, int arows,
+                             const T* __restrict__ LB, long long ldb, int brows, int kdim,
+                             const T* __restrict__ d, const T* __restrict__ dsub,
+                             const unsigned char* __restrict__ kind, T* As, T* Bs) {
+  using F = Field<T>;
+  constexpr int KT = KChunk<T>::v;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = F::zero();
+  for (int t0 = 0; t0 < kdim; t0 += KT) {
+    const int kt = min(KT, kdim - t0);
+    // Cooperative chunk loads: element e -> (t = e / 64, r = e % 64).
+    for (int e = tid; e < KT * TILE; e += TPB) {
+      int t = e / TILE, r = e % TILE;
+      T av = F::zero(), gv = F::zero();
+      if (t < kt) {
+        if (r < arows) av = LA[r + (long long)(t0 + t) * lda];
+        if (r < brows) gv = ld_G(LB, ldb, r, t0 + t, d, dsub, kind);
+      }
+      As[t * TILE + r] = av;
+      Bs[t * TILE + r] = gv;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int t = 0; t < kt; ++t) {
+      T a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[t * TILE + ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[t * TILE + tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = F::fma_(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ int lower_bound_i(const int* __restrict__ a, int lo, int hi, int key) {
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (a[mid] < key)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// ---------------------------------------------------------------------------
+// cmod: task = (s, r0, c0); tile rows [r0, r0+64) x cols [c0, c0+64) of s's
+// panel, pulling every descendant update in update-list order.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_cmod(FactorArgs fa, const int4* __restrict__ tasks) {
+  using F = Field<T>;
+  if (fa.status[0] != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* acc_s = reinterpret_cast<T*>(smem_raw);          // [64 cols][64 rows]
+  T* As = acc_s + TILE * TILE;
+  T* Bs = As + KChunk<T>::v * TILE;
+  int* rs_tile = reinterpret_cast<int*>(Bs + KChunk<T>::v * TILE);  // 64
+  int* rowmap = rs_tile + TILE;                                       // 64
+  int* colmap = rowmap + TILE;                                        // 64
+  int* meta = colmap + TILE;                                          // 8
+
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, r0 = tk.y, c0 = tk.z;
+  const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
+  const int rows_here = min(TILE, nrow - r0), cols_here = min(TILE, ncol - c0);
+  T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
+  const int* rss = fa.rs + fa.sn_rsoff[s];
+  const int tid = threadIdx.x;
+  // Load the tile (column-major in smem).
+  for (int e = tid; e < TILE * TILE; e += TPB) {
+    int c = e / TILE, r = e % TILE;
+    T v = F::zero();
+    if (r < rows_here && c < cols_here) v = panel[(r0 + r) + (long long)(c0 + c) * nrow];
+    acc_s[e] = v;
+  }
+  if (tid < TILE) rs_tile[tid] = tid < rows_here ? rss[r0 + tid] : INT_MAX;
+  __syncthreads();
+  const int g_row_lo = rs_tile[0], g_row_hi = rs_tile[rows_here - 1];
+  const int g_col_lo = first + c0, g_col_hi = first + c0 + cols_here;  // [lo, hi)
+  const T* dall = reinterpret_cast<const T*>(fa.d);
+  const T* dsall = reinterpret_cast<const T*>(fa.dsub);
+  const T* pall = reinterpret_cast<const T*>(fa.panel);
+  for (int u = fa.upd_ptr[s]; u < fa.upd_ptr[s + 1]; ++u) {
+    const int k = fa.upd_k[u];
+    const int nck = fa.sn_ncol[k], nrk = fa.sn_nrow[k], fk = fa.sn_first[k];
+    const int nok = nrk - nck;
+    const int* ok = fa.rs + fa.sn_rsoff[k] + nck;
+    if (tid == 0) {
+      int p0 = fa.upd_p0[u], p1 = fa.upd_p1[u];
+      int q0 = lower_bound_i(ok, p0, p1, g_col_lo);
+      int q1 = lower_bound_i(ok, q0, p1, g_col_hi);
+      int a = lower_bound_i(ok, q0, nok, g_row_lo);
+      int b = lower_bound_i(ok, a, nok, g_row_hi + 1);
+      meta[0] = q0;
+      meta[1] = q1;
+      meta[2] = a;
+      meta[3] = b;
+    }
+    __syncthreads();
+    const int q0 = meta[0], q1 = meta[1], a = meta[2], b = meta[3];
+    if (q1 <= q0 || b <= a) {
+      __syncthreads();
+      continue;
+    }
+    // Row map: position of ok[a + i] inside this tile's row slice.
+    if (tid < TILE) {
+      if (tid < b - a) {
+        int g = ok[a + tid];
+        rowmap[tid] = lower_bound_i(rs_tile, 0, rows_here, g);
+      }
+      if (tid < q1 - q0) colmap[tid] = ok[q0 + tid] - first - c0;
+    }
+    const T* Lk = pall + fa.sn_poff[k];
+    T acc[4][4];
+    tile_product<T>(acc, Lk + nck + a, nrk, b - a, Lk + nck + q0, nrk, q1 - q0, nck, dall + fk, dsall + fk,
+                    fa.kind + fk, As, Bs);
+    // Scatter-subtract (rows r >= column c in k's ordering only).
+    const int tx = tid & 15, ty = tid >> 4;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      int ri = ty + 16 * i;
+      if (ri >= b - a) continue;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        int cj = tx + 16 * j;
+        if (cj >= q1 - q0) continue;
+        if (a + ri < q0 + cj) continue;
+        int e = colmap[cj] * TILE + rowmap[ri];
+        acc_s[e] = F::sub(acc_s[e], acc[i][j]);
+      }
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < TILE * TILE; e += TPB) {
+    int c = e / TILE, r = e % TILE;
+    if (r < rows_here && c < cols_here && r0 + r >= c0 + c) panel[(r0 + r) + (long long)(c0 + c) * nrow] = acc_s[e];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Deferred in-panel Schur: task = (s, kb, r0, c0) with tile rows [ke+r0, ...)
+// and cols [ke+c0, ...): panel -= L21 D L21^T on rows >= cols.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_schur(FactorArgs fa, const int4* __restrict__ tasks, int nb_small,
+                                               int nb_big) {
+  using F = Field<T>;
+  if (fa.status[0] != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* As = reinterpret_cast<T*>(smem_raw);
+  T* Bs = As + KChunk<T>::v * TILE;
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, kb = tk.y, r0 = tk.z, c0 = tk.w;
+  const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
+  const int nb = ncol >= 512 ? nb_big : nb_small;
+  const int ke = min(kb + nb, ncol);
+  const int pw = ke - kb, mt = nrow - ke, cw = ncol - ke;
+  T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
+  const int rows_here = min(TILE, mt - r0), cols_here = min(TILE, cw - c0);
+  const T* L21 = panel + ke + (long long)kb * nrow;
+  T acc[4][4];
+  tile_product<T>(acc, L21 + r0, nrow, rows_here, L21 + c0, nrow, cols_here, pw,
+                  reinterpret_cast<const T*>(fa.d) + first + kb, reinterpret_cast<const T*>(fa.dsub) + first + kb,
+                  fa.kind + first + kb, As, Bs);
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    int rr = r0 + ty + 16 * i;
+    if (ty + 16 * i >= rows_here) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int cc = c0 + tx + 16 * j;
+      if (tx + 16 * j >= cols_here || rr < cc) continue;
+      T* p = panel + (ke + rr) + (long long)(ke + cc) * nrow;
+      *p = F::sub(*p, acc[i][j]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Block reductions for the pivot search: max of a non-negative double with
+// the lowest index on ties (the reference's strict `>` scan).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void argmax_combine(double& v, int& i, double v2, int i2) {
+  if (v2 > v || (v2 == v && i2 < i)) {
+    v = v2;
+    i = i2;
+  }
+}
+
+template <int NT>
+__device__ void block_argmax(double& v, int& idx, double* red_v, int* red_i) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    double v2 = __shfl_down_sync(0xffffffffu, v, o);
+    int i2 = __shfl_down_sync(0xffffffffu, idx, o);
+    argmax_combine(v, idx, v2, i2);
+  }
+  if (lane == 0) {
+    red_v[wid] = v;
+    red_i[wid] = idx;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    v = lane < NT / 32 ? red_v[lane] : -1.0;
+    idx = lane < NT / 32 ? red_i[lane] : INT_MAX;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double v2 = __shfl_down_sync(0xffffffffu, v, o);
+      int i2 = __shfl_down_sync(0xffffffffu, idx, o);
+      argmax_combine(v, idx, v2, i2);
+    }
+    if (lane == 0) {
+      red_v[0] = v;
+      red_i[0] = idx;
+    }
+  }
+  __syncthreads();
+  v = red_v[0];
+  idx = red_i[0];
+  __syncthreads();
+}
+
+// Packed lower-triangle index of (i, j), i >= j, in a pw x pw block.
+__device__ __forceinline__ int pk(int i, int j, int pw) { return j * pw - (j * (j - 1)) / 2 + (i - j); }
+
+// Apply one recorded pivot step of a block to R deep rows held in smem
+// (column-major, stride R): the exact per-row op sequence of
+// apply_bk_panel_trailing.
+template <typename T, int NT>
+__device__ void replay_rows(T* X, int R, int rows, int kb, int ke, int nb, const T* __restrict__ snap,
+                            const int* __restrict__ swaps, const T* __restrict__ d, const T* __restrict__ dsub,
+                            const unsigned char* __restrict__ kind) {
+  using F = Field<T>;
+  const int pw = ke - kb;
+  int k = 0;
+  while (k < pw) {
+    int kp = swaps[k];
+    bool two = kind[k] == 1;
+    if (kp >= 0) {
+      int src = two ? k + 1 : k;
+      for (int r = threadIdx.x; r < rows; r += NT) {
+        T t = X[src * R + r];
+        X[src * R + r] = X[(kp - kb) * R + r];
+        X[(kp - kb) * R + r] = t;
+      }
+      __syncthreads();
+    }
+    if (two) {
+      T d11 = d[k], d21 = dsub[k], d22 = d[k + 1];
+      T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
+      T detinv = F::recip(det);
+      int ncols = pw - (k + 2);
+      for (int e = threadIdx.x; e < ncols * rows; e += NT) {
+        int j = k + 2 + e / rows, r = e % rows;
+        T l1 = snap[k * nb + j], l2 = snap[(k + 1) * nb + j];
+        T x = X[j * R + r];
+        x = F::sub(x, F::mul(X[k * R + r], l1));
+        x = F::sub(x, F::mul(X[(k + 1) * R + r], l2));
+        X[j * R + r] = x;
+      }
+      __syncthreads();
+      for (int r = threadIdx.x; r < rows; r += NT) {
+        T wik = X[k * R + r], wik1 = X[(k + 1) * R + r];
+        X[k * R + r] = F::mul(F::sub(F::mul(d22, wik), F::mul(d21, wik1)), detinv);
+        X[(k + 1) * R + r] = F::mul(F::sub(F::mul(d11, wik1), F::mul(d21, wik)), detinv);
+      }
+      __syncthreads();
+      k += 2;
+    } else {
+      T dinv = F::recip(d[k]);
+      int ncols = pw - (k + 1);
+      for (int e = threadIdx.x; e < ncols * rows; e += NT) {
+        int j = k + 1 + e / rows, r = e % rows;
+        T w = snap[k * nb + j];
+        if (!F::is_zero(w)) X[j * R + r] = F::sub(X[j * R + r], F::mul(X[k * R + r], w));
+      }
+      __syncthreads();
+      for (int r = threadIdx.x; r < rows; r += NT) X[k * R + r] = F::mul(X[k * R + r], dinv);
+      __syncthreads();
+      k += 1;
+    }
+  }
+}
+
+constexpr int DEEP_R = 32;  // deep rows per replay chunk
+
+// ---------------------------------------------------------------------------
+// getf2: task = (s, kb, slot, fuse) — unblocked BK over panel columns [kb, ke)
+// with every pivot candidate, update and interchange bounded to rows < ke.
+// ---------------------------------------------------------------------------
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restrict__ tasks, int nb_small,
+                                              int nb_big) {
+  using F = Field<T>;
+  if (fa.status[0] != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, kb = tk.y, slot = tk.z, fuse = tk.w;
+  const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
+  const int nb = ncol >= 512 ? nb_big : nb_small;
+  const int ke = min(kb + nb, ncol), pw = ke - kb;
+  T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
+  T* dG = reinterpret_cast<T*>(fa.d) + first + kb;
+  T* dsG = reinterpret_cast<T*>(fa.dsub) + first + kb;
+  unsigned char* kindG = fa.kind + first + kb;
+  int* lpermG = fa.lperm + first;
+  unsigned char* sc = reinterpret_cast<unsigned char*>(fa.scratch) + (long long)slot * fa.scratch_stride;
+  T* snap = reinterpret_cast<T*>(sc);                      // nb x nb
+  int* swaps = reinterpret_cast<int*>(snap + (long long)nb * nb);  // nb
+  int* swp_p = swaps + nb;                                  // nb (row pairs for left swaps)
+  int* swp_q = swp_p + nb;
+
+  T* A = reinterpret_cast<T*>(smem_raw);              // packed lower pw x pw
+  const int npk = pw * (pw + 1) / 2;
+  T* l1 = A + npk;
+  T* l2 = l1 + pw;
+  double* red_v = reinterpret_cast<double*>(l2 + pw);
+  int* red_i = reinterpret_cast<int*>(red_v + 32);
+  int* ctl = red_i + 32;  // [0] kstep [1] kp [2] nswaps [3] error
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  constexpr int NW = NT / 32;
+  for (int j = warp; j < pw; j += NW)
+    for (int i = j + lane; i < pw; i += 32) A[pk(i, j, pw)] = panel[(kb + i) + (long long)(kb + j) * nrow];
+  if (kb == 0)
+    for (int p = tid; p < ncol; p += NT) lpermG[p] = p;
+  for (int e = tid; e < pw; e += NT) {
+    dG[e] = F::zero();
+    dsG[e] = F::zero();
+    kindG[e] = 0;
+    swaps[e] = -1;
+  }
+  for (int e = tid; e < pw * nb; e += NT) snap[(e / nb) * nb + (e % nb)] = F::zero();
+  if (tid == 0) {
+    ctl[2] = 0;
+    ctl[3] = 0;
+  }
+  __syncthreads();
+  const double alpha = (1.0 + sqrt(17.0)) / 8.0;
+  int nperturbed = 0;
+  int k = 0;
+  while (k < pw) {
+    // colmax over in-panel rows (k+1)..pw.
+    double v = -1.0;
+    int idx = INT_MAX;
+    for (int i = k + 1 + tid; i < pw; i += NT) argmax_combine(v, idx, F::mag2(A[pk(i, k, pw)]), i);
+    block_argmax<NT>(v, idx, red_v, red_i);
+    if (tid == 0) {
+      double absakk = F::mag(A[pk(k, k, pw)]);
+      double colmax_sq = v > 0.0 ? v : 0.0;
+      int imax = v > 0.0 ? idx : k;
+      double colmax = sqrt(colmax_sq);
+      int kstep = 1, kp = k;
+      if (fmax(absakk, colmax) == 0.0) {
+        if (fa.perturb_floor < 0.0) ctl[3] = 1;
+      } else if (absakk >= alpha * colmax) {
+      } else {
+        double rmx = 0.0;
+        for (int j = k; j < imax; ++j) rmx = fmax(rmx, F::mag2(A[pk(imax, j, pw)]));
+        for (int i = imax + 1; i < pw; ++i) rmx = fmax(rmx, F::mag2(A[pk(i, imax, pw)]));
+        double rowmax = sqrt(rmx);
+        if (absakk >= alpha * colmax * (colmax / rowmax)) {
+        } else if (F::mag(A[pk(imax, imax, pw)]) >= alpha * rowmax) {
+          kp = imax;
+        } else {
+          kstep = 2;
+          kp = imax;
+        }
+      }
+      ctl[0] = kstep;
+      ctl[1] = kp;
+    }
+    __syncthreads();
+    if (ctl[3]) break;
+    const int kstep = ctl[0], kp = ctl[1];
+    const int p = kstep == 1 ? k : k + 1;
+    if (kp != p) {
+      // swap_sym_lower_bounded(p, kp) restricted to the block + left segments.
+      const int q = kp;
+      for (int i = q + 1 + tid; i < pw; i += NT) {
+        T t = A[pk(i, p, pw)];
+        A[pk(i, p, pw)] = A[pk(i, q, pw)];
+        A[pk(i, q, pw)] = t;
+      }
+      for (int i = p + 1 + tid; i < q; i += NT) {
+        T t = A[pk(i, p, pw)];
+        A[pk(i, p, pw)] = A[pk(q, i, pw)];
+        A[pk(q, i, pw)] = t;
+      }
+      for (int j = tid; j < p; j += NT) {
+        T t = A[pk(p, j, pw)];
+        A[pk(p, j, pw)] = A[pk(q, j, pw)];
+        A[pk(q, j, pw)] = t;
+      }
+      if (tid == 0) {
+        T t = A[pk(p, p, pw)];
+        A[pk(p, p, pw)] = A[pk(q, q, pw)];
+        A[pk(q, q, pw)] = t;
+        int lp = lpermG[kb + p];
+        lpermG[kb + p] = lpermG[kb + q];
+        lpermG[kb + q] = lp;
+        swaps[k] = kb + q;
+        int ns = ctl[2];
+        swp_p[ns] = kb + p;
+        swp_q[ns] = kb + q;
+        ctl[2] = ns + 1;
+      }
+      __syncthreads();
+    }
+    if (kstep == 1) {
+      T dk = A[pk(k, k, pw)];
+      if (fa.perturb_floor >= 0.0) {
+        double m = F::mag(dk);
+        if (m < fa.perturb_floor) {
+          dk = m == 0.0 ? F::from_real(fa.perturb_floor) : F::scale(dk, fa.perturb_floor / m);
+          if (tid == 0) {
+            A[pk(k, k, pw)] = dk;
+            ++nperturbed;
+          }
+        }
+      } else if (F::is_zero(dk)) {
+        if (tid == 0) ctl[3] = 1;
+        __syncthreads();
+        break;
+      }
+      const T dinv = F::recip(dk);
+      if (tid == 0) dG[k] = dk;
+      // multipliers w_j = A(j,k) / d_k for j > k (snapshot), stored in l1.
+      for (int j = k + 1 + tid; j < pw; j += NT) {
+        T w = F::mul(A[pk(j, k, pw)], dinv);
+        l1[j] = w;
+        snap[k * nb + j] = w;
+      }
+      __syncthreads();
+      // rank-1 trailing update of the block: A(i,j) -= A(i,k) w_j, i >= j > k.
+      for (int j = k + 1 + warp; j < pw; j += NW) {
+        T w = l1[j];
+        if (F::is_zero(w)) continue;
+        for (int i = j + lane; i < pw; i += 32) A[pk(i, j, pw)] = F::sub(A[pk(i, j, pw)], F::mul(A[pk(i, k, pw)], w));
+      }
+      __syncthreads();
+      for (int i = k + 1 + tid; i < pw; i += NT) A[pk(i, k, pw)] = F::mul(A[pk(i, k, pw)], dinv);
+      __syncthreads();
+      k += 1;
+    } else {
+      T d11 = A[pk(k, k, pw)], d21 = A[pk(k + 1, k, pw)], d22 = A[pk(k + 1, k + 1, pw)];
+      T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
+      double scale = fmax(fmax(F::mag(d11), F::mag(d22)), F::mag(d21));
+      double growth_floor = 1e-14 * scale * scale;
+      if (fa.perturb_floor >= 0.0) {
+        double fl = fmax(fa.perturb_floor * fa.perturb_floor, growth_floor);
+        if (F::mag(det) < fl) {
+          double lift = fmax(fa.perturb_floor, scale * sqrt(1e-14));
+          d11 = F::add(d11, F::from_real(lift));
+          d22 = F::add(d22, F::from_real(lift));
+          det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
+          if (F::mag(det) < fl) det = F::add(det, F::from_real(fl));
+          if (tid == 0) ++nperturbed;
+        }
+      } else if (F::mag(det) <= growth_floor) {
+        if (tid == 0) ctl[3] = 1;
+        __syncthreads();
+        break;
+      }
+      const T detinv = F::recip(det);
+      if (tid == 0) {
+        dG[k] = d11;
+        dsG[k] = d21;
+        dG[k + 1] = d22;
+        kindG[k] = 1;
+        kindG[k + 1] = 2;
+      }
+      for (int i = k + 2 + tid; i < pw; i += NT) {
+        T wik = A[pk(i, k, pw)], wik1 = A[pk(i, k + 1, pw)];
+        T a1 = F::mul(F::sub(F::mul(d22, wik), F::mul(d21, wik1)), detinv);
+        T a2 = F::mul(F::sub(F::mul(d11, wik1), F::mul(d21, wik)), detinv);
+        l1[i] = a1;
+        l2[i] = a2;
+        snap[k * nb + i] = a1;
+        snap[(k + 1) * nb + i] = a2;
+      }
+      __syncthreads();
+      for (int j = k + 2 + warp; j < pw; j += NW) {
+        T a1 = l1[j], a2 = l2[j];
+        for (int i = j + lane; i < pw; i += 32) {
+          T x = A[pk(i, j, pw)];
+          x = F::sub(x, F::mul(A[pk(i, k, pw)], a1));
+          x = F::sub(x, F::mul(A[pk(i, k + 1, pw)], a2));
+          A[pk(i, j, pw)] = x;
+        }
+      }
+      __syncthreads();
+      for (int i = k + 2 + tid; i < pw; i += NT) {
+        A[pk(i, k, pw)] = l1[i];
+        A[pk(i, k + 1, pw)] = l2[i];
+      }
+      __syncthreads();
+      k += 2;
+    }
+  }
+  if (ctl[3]) {
+    if (tid == 0) {
+      if (atomicCAS(&fa.status[0], 0, 1) == 0) fa.status[1] = s;
+    }
+    return;
+  }
+  if (tid == 0 && nperturbed) atomicAdd(&fa.status[2], nperturbed);
+  // Write the block back; the 2x2 coupling entry (i = j + 1 of a 2x2) lives
+  // in dsub only, so its panel slot is stored as an exact zero (it is never
+  // an L multiplier).
+  __syncthreads();
+  for (int j = warp; j < pw; j += NW) {
+    const bool two = kindG[j] == 1;
+    for (int i = j + lane; i < pw; i += 32)
+      panel[(kb + i) + (long long)(kb + j) * nrow] = (two && i == j + 1) ? F::zero() : A[pk(i, j, pw)];
+  }
+  // Left row segments of each interchange: columns [0, kb) at rows p, q.
+  const int nsw = ctl[2];
+  if (nsw > 0 && kb > 0) {
+    for (int j = tid; j < kb; j += NT) {
+      T* col = panel + (long long)j * nrow;
+      for (int t = 0; t < nsw; ++t) {
+        int p = swp_p[t], q = swp_q[t];
+        T x = col[p];
+        col[p] = col[q];
+        col[q] = x;
+      }
+    }
+  }
+  // kind/d written by tid 0 are read by the replay below.
+  __syncthreads();
+  if (fuse && nrow > ke) {
+    // Replay this block's pivot steps on the deep rows [ke, nrow) in chunks.
+    T* X = A;  // reuse shared memory: DEEP_R x pw
+    for (int rs0 = ke; rs0 < nrow; rs0 += DEEP_R) {
+      const int rows = min(DEEP_R, nrow - rs0);
+      for (int e = tid; e < rows * pw; e += NT) {
+        int c = e / rows, r = e % rows;
+        X[c * DEEP_R + r] = panel[(rs0 + r) + (long long)(kb + c) * nrow];
+      }
+      __syncthreads();
+      replay_rows<T, NT>(X, DEEP_R, rows, kb, ke, nb, snap, swaps, dG, dsG, kindG);
+      for (int e = tid; e < rows * pw; e += NT) {
+        int c = e / rows, r = e % rows;
+        panel[(rs0 + r) + (long long)(kb + c) * nrow] = X[c * DEEP_R + r];
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Deep-row replay for tall panels: task = (s, kb, slot, row0); DEEP_R rows.
+// ---------------------------------------------------------------------------
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_deep(FactorArgs fa, const int4* __restrict__ tasks, int nb_small,
+                                             int nb_big) {
+  if (fa.status[0] != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, kb = tk.y, slot = tk.z, rs0 = tk.w;
+  const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
+  const int nb = ncol >= 512 ? nb_big : nb_small;
+  const int ke = min(kb + nb, ncol), pw = ke - kb;
+  T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
+  const unsigned char* sc = reinterpret_cast<const unsigned char*>(fa.scratch) + (long long)slot * fa.scratch_stride;
+  const T* snap = reinterpret_cast<const T*>(sc);
+  const int* swaps = reinterpret_cast<const int*>(snap + (long long)nb * nb);
+  T* X = reinterpret_cast<T*>(smem_raw);
+  const int rows = min(DEEP_R, nrow - rs0);
+  const int tid = threadIdx.x;
+  for (int e = tid; e < rows * pw; e += NT) {
+    int c = e / rows, r = e % rows;
+    X[c * DEEP_R + r] = panel[(rs0 + r) + (long long)(kb + c) * nrow];
+  }
+  __syncthreads();
+  replay_rows<T, NT>(X, DEEP_R, rows, kb, ke, nb, snap, swaps, reinterpret_cast<const T*>(fa.d) + first + kb,
+                     reinterpret_cast<const T*>(fa.dsub) + first + kb, fa.kind + first + kb);
+  for (int e = tid; e < rows * pw; e += NT) {
+    int c = e / rows, r = e % rows;
+    panel[(rs0 + r) + (long long)(kb + c) * nrow] = X[c * DEEP_R + r];
+  }
+}
+
+}  // namespace rsd

@@ -1,0 +1,467 @@
+// sm_100a kernels of the supernodal multi-RHS solve x = s . P L^-T D^-1 L^-1 P^T (s . b)
+// straight from the device-resident panels, plus the FP64 residual / norm /
+// Krylov vector kernels of the refinement driver.
+//
+// Vectors are row-major n x nrhs (the reference RHS layout,
+// src/dense/ldlt_generic.rs:556-714).  Two index spaces are used:
+//   g : the analysed (fill-reducing) order — panel row structures live here;
+//   e : pivot order, e = first_col(s) + pivot position inside s.
+// Forward:  per level, k_fwd_gather pulls every descendant's L_k * z_k into
+//           the columns of s (update-list order, no atomics), then
+//           k_fwd_diag solves the unit-lower diagonal block in pivot order and
+//           applies D^-1.
+// Backward: per level (root first), k_bwd dots each column of s against the
+//           already-solved rows (own pivots in e order, ancestors in g order)
+//           and back-substitutes the diagonal block.
+// Reference: solve_ldlt_block (src/dense/ldlt_generic.rs:618-714).
+#pragma once
+
+#include "scalar.cuh"
+
+namespace rsd {
+
+constexpr int SOLVE_NT = 256;
+constexpr int RHS_MAX = 16;  // right-hand sides per pass (larger counts loop)
+constexpr int SB = 32;       // diagonal-block edge of the blocked solves
+
+struct SolveArgs {
+  const int* sn_first;
+  const int* sn_ncol;
+  const int* sn_nrow;
+  const long long* sn_poff;
+  const long long* sn_rsoff;
+  const int* rs;
+  const int* upd_ptr;
+  const int* upd_k;
+  const int* upd_p0;
+  const int* upd_p1;
+  const void* panel;
+  const void* d;
+  const void* dsub;
+  const unsigned char* kind;
+  const int* lperm;
+  void* Yg;   // n x ld, g order
+  void* Ze;   // n x ld, e order
+  void* Xg;   // n x ld, g order
+  int ld;     // row stride (total rhs count)
+  int c0;     // first rhs column of this pass
+  int nrhs;   // rhs columns in this pass (<= RHS_MAX)
+};
+
+// Yg[g] = s[perm[g]] * b[perm[g]] (scaled, permuted in).
+template <typename T>
+__global__ void k_perm_in(int n, int nrhs, const int* __restrict__ perm, const double* __restrict__ s,
+                          const T* __restrict__ b, T* __restrict__ Yg) {
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * nrhs) return;
+  int g = (int)(idx / nrhs), c = (int)(idx % nrhs);
+  int i = perm[g];
+  Yg[idx] = Field<T>::scale(b[(long long)i * nrhs + c], s[i]);
+}
+
+// x[perm[g]] = s[perm[g]] * Xg[g] (permuted out, scaled back).
+template <typename T>
+__global__ void k_perm_out(int n, int nrhs, const int* __restrict__ perm, const double* __restrict__ s,
+                           const T* __restrict__ Xg, T* __restrict__ x) {
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * nrhs) return;
+  int g = (int)(idx / nrhs), c = (int)(idx % nrhs);
+  int i = perm[g];
+  x[(long long)i * nrhs + c] = Field<T>::scale(Xg[idx], s[i]);
+}
+
+// acc[c] += sum_{q in [q_begin, q_end)} L[r, q] * V[q][c]: one lane per row r,
+// warps split q; result reduced through smem `red` (NW x 32 x RHS_MAX).
+template <typename T>
+__device__ __forceinline__ void lane_row_dot(T (&acc)[RHS_MAX], const T* __restrict__ Lrow, long long ld,
+                                             int q_begin, int q_end, const T* __restrict__ V, int vld, int nrhs,
+                                             bool row_ok) {
+  using F = Field<T>;
+  const int warp = threadIdx.x >> 5;
+  constexpr int NW = SOLVE_NT / 32;
+  for (int q = q_begin + warp; q < q_end; q += NW) {
+    T l = row_ok ? Lrow[(long long)q * ld] : F::zero();
+    const T* v = V + (long long)q * vld;
+#pragma unroll
+    for (int c = 0; c < RHS_MAX; ++c)
+      if (c < nrhs) acc[c] = F::fma_(l, v[c], acc[c]);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void reduce_warps(T (&acc)[RHS_MAX], T* red, int nrhs) {
+  using F = Field<T>;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int NW = SOLVE_NT / 32;
+#pragma unroll
+  for (int c = 0; c < RHS_MAX; ++c)
+    if (c < nrhs) red[(warp * 32 + lane) * RHS_MAX + c] = acc[c];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int c = 0; c < RHS_MAX; ++c) {
+      if (c >= nrhs) continue;
+      T s = F::zero();
+      for (int w = 0; w < NW; ++w) s = F::add(s, red[(w * 32 + lane) * RHS_MAX + c]);
+      acc[c] = s;
+    }
+  }
+  __syncthreads();
+}
+
+// Forward gather: task = (s, c0) — columns [c0, c0+32) of s receive
+// sum_k L_k(rows landing there) * z_k, in update-list order.
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_NT) k_fwd_gather(SolveArgs a, const int2* __restrict__ tasks) {
+  using F = Field<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* red = reinterpret_cast<T*>(smem_raw);                         // NW*32*RHS_MAX
+  T* tsum = red + (SOLVE_NT / 32) * 32 * RHS_MAX;                   // 32 x RHS_MAX
+  int* meta = reinterpret_cast<int*>(tsum + 32 * RHS_MAX);
+  const int2 tk = tasks[blockIdx.x];
+  const int s = tk.x, cb = tk.y;
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s];
+  const int cols_here = min(SB, ncol - cb);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const T* P = reinterpret_cast<const T*>(a.panel);
+  const T* Z = reinterpret_cast<const T*>(a.Ze) + a.c0;
+  T* Y = reinterpret_cast<T*>(a.Yg) + a.c0;
+  for (int e = threadIdx.x; e < 32 * RHS_MAX; e += SOLVE_NT) tsum[e] = F::zero();
+  __syncthreads();
+  const int g_lo = first + cb, g_hi = first + cb + cols_here;
+  for (int u = a.upd_ptr[s]; u < a.upd_ptr[s + 1]; ++u) {
+    const int k = a.upd_k[u];
+    const int nck = a.sn_ncol[k], nrk = a.sn_nrow[k], fk = a.sn_first[k];
+    const int* ok = a.rs + a.sn_rsoff[k] + nck;
+    if (threadIdx.x == 0) {
+      int p0 = a.upd_p0[u], p1 = a.upd_p1[u];
+      int lo = p0, hi = p1;
+      while (lo < hi) {
+        int m = (lo + hi) >> 1;
+        if (ok[m] < g_lo) lo = m + 1; else hi = m;
+      }
+      int q0 = lo;
+      hi = p1;
+      while (lo < hi) {
+        int m = (lo + hi) >> 1;
+        if (ok[m] < g_hi) lo = m + 1; else hi = m;
+      }
+      meta[0] = q0;
+      meta[1] = lo;
+    }
+    __syncthreads();
+    const int q0 = meta[0], q1 = meta[1];
+    if (q1 > q0) {
+      const int nr = q1 - q0;  // <= 32
+      T acc[RHS_MAX];
+#pragma unroll
+      for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
+      const T* Lk = P + a.sn_poff[k] + nck + q0 + lane;
+      lane_row_dot<T>(acc, Lk, nrk, 0, nck, Z + (long long)fk * a.ld, a.ld, a.nrhs, lane < nr);
+      reduce_warps<T>(acc, red, a.nrhs);
+      if (warp == 0 && lane < nr) {
+        int tc = ok[q0 + lane] - g_lo;
+#pragma unroll
+        for (int c = 0; c < RHS_MAX; ++c)
+          if (c < a.nrhs) tsum[tc * RHS_MAX + c] = F::add(tsum[tc * RHS_MAX + c], acc[c]);
+      }
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < cols_here * a.nrhs; e += SOLVE_NT) {
+    int c = e / a.nrhs, r = e % a.nrhs;
+    T* y = Y + (long long)(g_lo + c) * a.ld + r;
+    *y = F::sub(*y, tsum[c * RHS_MAX + r]);
+  }
+}
+
+// Forward diagonal solve of supernode s (one CTA): pivot-order unit-lower
+// substitution in 32-column blocks (left-looking inside the panel), then D^-1.
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_NT) k_fwd_diag(SolveArgs a, const int* __restrict__ tasks) {
+  using F = Field<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* red = reinterpret_cast<T*>(smem_raw);
+  T* zb = red + (SOLVE_NT / 32) * 32 * RHS_MAX;  // 32 x RHS_MAX
+  const int s = tasks[blockIdx.x];
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
+  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
+  const T* d = reinterpret_cast<const T*>(a.d) + first;
+  const T* ds = reinterpret_cast<const T*>(a.dsub) + first;
+  const unsigned char* kind = a.kind + first;
+  const int* lp = a.lperm + first;
+  const T* Y = reinterpret_cast<const T*>(a.Yg) + a.c0;
+  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int j0 = 0; j0 < ncol; j0 += SB) {
+    const int nb = min(SB, ncol - j0);
+    T acc[RHS_MAX];
+#pragma unroll
+    for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
+    lane_row_dot<T>(acc, L + j0 + lane, nrow, 0, j0, Z, a.ld, a.nrhs, lane < nb);
+    reduce_warps<T>(acc, red, a.nrhs);
+    if (warp == 0) {
+      // y in pivot order minus the contribution of the solved columns.
+      T z[RHS_MAX];
+      const int p = j0 + lane;
+      const bool ok = lane < nb;
+      const T* yrow = Y + (long long)(first + (ok ? lp[p] : 0)) * a.ld;
+#pragma unroll
+      for (int c = 0; c < RHS_MAX; ++c) z[c] = (ok && c < a.nrhs) ? F::sub(yrow[c], acc[c]) : F::zero();
+      // In-block substitution: z[p] -= L[p, q] z[q], q < p (skip the 2x2 coupling).
+      for (int q = 0; q < nb; ++q) {
+        const int qq = j0 + q;
+        T l = F::zero();
+        if (ok && lane > q) l = L[p + (long long)qq * nrow];
+#pragma unroll
+        for (int c = 0; c < RHS_MAX; ++c) {
+          if (c >= a.nrhs) continue;
+          T zq;
+          if constexpr (Field<T>::complex) {
+            zq.re = __shfl_sync(0xffffffffu, z[c].re, q);
+            zq.im = __shfl_sync(0xffffffffu, z[c].im, q);
+          } else {
+            zq = __shfl_sync(0xffffffffu, z[c], q);
+          }
+          z[c] = F::fnma(l, zq, z[c]);
+        }
+      }
+      if (ok)
+#pragma unroll
+        for (int c = 0; c < RHS_MAX; ++c)
+          if (c < a.nrhs) Z[(long long)p * a.ld + c] = z[c];
+    }
+    __syncthreads();
+  }
+  // D^-1 (1x1 and 2x2 blocks).
+  for (int e = threadIdx.x; e < ncol * a.nrhs; e += SOLVE_NT) {
+    int p = e / a.nrhs, c = e % a.nrhs;
+    unsigned char kd = kind[p];
+    if (kd == 0) {
+      T* z = Z + (long long)p * a.ld + c;
+      *z = F::mul(*z, F::recip(d[p]));
+    } else if (kd == 1) {
+      T d11 = d[p], d21 = ds[p], d22 = d[p + 1];
+      T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
+      T di = F::recip(det);
+      T* z0 = Z + (long long)p * a.ld + c;
+      T* z1 = Z + (long long)(p + 1) * a.ld + c;
+      T a0 = *z0, a1 = *z1;
+      *z0 = F::mul(F::sub(F::mul(d22, a0), F::mul(d21, a1)), di);
+      *z1 = F::mul(F::sub(F::mul(d11, a1), F::mul(d21, a0)), di);
+    }
+  }
+}
+
+// Backward solve of supernode s (one CTA): blocks of 32 pivots from the
+// last; each column dotted against the solved rows below it.
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_NT) k_bwd(SolveArgs a, const int* __restrict__ tasks) {
+  using F = Field<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* red = reinterpret_cast<T*>(smem_raw);
+  T* vb = red + (SOLVE_NT / 32) * 32 * RHS_MAX;  // [32 rows of the block] x RHS_MAX
+  int* rsx = reinterpret_cast<int*>(vb + 32 * RHS_MAX);
+  const int s = tasks[blockIdx.x];
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
+  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
+  const int* lp = a.lperm + first;
+  const int* rss = a.rs + a.sn_rsoff[s];
+  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
+  const T* Xall = reinterpret_cast<const T*>(a.Xg) + a.c0;
+  T* Xw = reinterpret_cast<T*>(a.Xg) + a.c0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = SOLVE_NT / 32;
+  (void)rsx;
+  const int nblk = (ncol + SB - 1) / SB;
+  for (int b = nblk - 1; b >= 0; --b) {
+    const int j0 = b * SB, nb = min(SB, ncol - j0), j1 = j0 + nb;
+    // acc[p][c] = sum_{r >= j1} L[r, p] * v(r): warp per column p, lanes over r.
+    for (int pc = warp; pc < nb; pc += NW) {
+      const int p = j0 + pc;
+      T acc[RHS_MAX];
+#pragma unroll
+      for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
+      const T* Lc = L + (long long)p * nrow;
+      for (int r = j1 + lane; r < nrow; r += 32) {
+        T l = Lc[r];
+        const T* v = r < ncol ? Z + (long long)r * a.ld : Xall + (long long)rss[r] * a.ld;
+#pragma unroll
+        for (int c = 0; c < RHS_MAX; ++c)
+          if (c < a.nrhs) acc[c] = F::fma_(l, v[c], acc[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < RHS_MAX; ++c) {
+        if (c >= a.nrhs) continue;
+        T x = acc[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          if constexpr (Field<T>::complex) {
+            x.re += __shfl_down_sync(0xffffffffu, x.re, o);
+            x.im += __shfl_down_sync(0xffffffffu, x.im, o);
+          } else {
+            x += __shfl_down_sync(0xffffffffu, x, o);
+          }
+        }
+        if (lane == 0) vb[pc * RHS_MAX + c] = x;
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {
+      const int p = j0 + lane;
+      const bool ok = lane < nb;
+      T v[RHS_MAX];
+#pragma unroll
+      for (int c = 0; c < RHS_MAX; ++c)
+        v[c] = (ok && c < a.nrhs) ? F::sub(Z[(long long)p * a.ld + c], vb[lane * RHS_MAX + c]) : F::zero();
+      // Backward inside the block: v[p] -= L[q, p] v[q] for q > p.
+      for (int q = nb - 1; q >= 1; --q) {
+        const int qq = j0 + q;
+        T l = F::zero();
+        if (ok && lane < q) l = L[qq + (long long)p * nrow];
+#pragma unroll
+        for (int c = 0; c < RHS_MAX; ++c) {
+          if (c >= a.nrhs) continue;
+          T vq;
+          if constexpr (Field<T>::complex) {
+            vq.re = __shfl_sync(0xffffffffu, v[c].re, q);
+            vq.im = __shfl_sync(0xffffffffu, v[c].im, q);
+          } else {
+            vq = __shfl_sync(0xffffffffu, v[c], q);
+          }
+          v[c] = F::fnma(l, vq, v[c]);
+        }
+      }
+      if (ok) {
+        T* xo = Xw + (long long)(first + lp[p]) * a.ld;
+#pragma unroll
+        for (int c = 0; c < RHS_MAX; ++c)
+          if (c < a.nrhs) {
+            Z[(long long)p * a.ld + c] = v[c];
+            xo[c] = v[c];
+          }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 refinement kernels.
+// ---------------------------------------------------------------------------
+
+// r = b - A x (row-major n x nrhs) with the full symmetric CSR of A whose
+// values are gathered from the stored lower triangle through `vmap`.
+template <typename T>
+__global__ void k_residual(int n, int nrhs, const long long* __restrict__ rp, const int* __restrict__ ci,
+                           const long long* __restrict__ vmap, const T* __restrict__ val, const T* __restrict__ x,
+                           const T* __restrict__ b, T* __restrict__ r) {
+  using F = Field<T>;
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * nrhs) return;
+  int i = (int)(idx / nrhs), c = (int)(idx % nrhs);
+  T acc = F::zero();
+  for (long long p = rp[i]; p < rp[i + 1]; ++p) acc = F::fma_(val[vmap[p]], x[(long long)ci[p] * nrhs + c], acc);
+  r[idx] = F::sub(b[idx], acc);
+}
+
+// y = A x (same layout).
+template <typename T>
+__global__ void k_spmv(int n, int nrhs, const long long* __restrict__ rp, const int* __restrict__ ci,
+                       const long long* __restrict__ vmap, const T* __restrict__ val, const T* __restrict__ x,
+                       T* __restrict__ y) {
+  using F = Field<T>;
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * nrhs) return;
+  int i = (int)(idx / nrhs), c = (int)(idx % nrhs);
+  T acc = F::zero();
+  for (long long p = rp[i]; p < rp[i + 1]; ++p) acc = F::fma_(val[vmap[p]], x[(long long)ci[p] * nrhs + c], acc);
+  y[idx] = acc;
+}
+
+// Per-column max |v| (column c of a row-major n x nrhs) into out[c] as bits.
+template <typename T>
+__global__ void k_colmax(long long n, int nrhs, const T* __restrict__ v, unsigned long long* __restrict__ out) {
+  __shared__ double sm[256];
+  const int c = blockIdx.y;
+  double m = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    m = fmax(m, Field<T>::mag(v[i * nrhs + c]));
+  sm[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicMax(&out[c], __double_as_longlong(sm[0]));
+}
+
+// x += dx (elementwise).
+template <typename T>
+__global__ void k_axpy1(long long m, const T* __restrict__ dx, T* __restrict__ x) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < m) x[i] = Field<T>::add(x[i], dx[i]);
+}
+
+// Low <-> high precision vector casts.
+template <typename Hi, typename Lo>
+__global__ void k_cast_down(long long m, const Hi* __restrict__ a, Lo* __restrict__ b);
+template <>
+__global__ void k_cast_down<double, float>(long long m, const double* __restrict__ a, float* __restrict__ b) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < m) b[i] = (float)a[i];
+}
+template <>
+__global__ void k_cast_down<c64, c32>(long long m, const c64* __restrict__ a, c32* __restrict__ b) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < m) b[i] = c32{(float)a[i].re, (float)a[i].im};
+}
+template <typename Lo, typename Hi>
+__global__ void k_cast_up(long long m, const Lo* __restrict__ a, Hi* __restrict__ b);
+template <>
+__global__ void k_cast_up<float, double>(long long m, const float* __restrict__ a, double* __restrict__ b) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < m) b[i] = (double)a[i];
+}
+template <>
+__global__ void k_cast_up<c32, c64>(long long m, const c32* __restrict__ a, c64* __restrict__ b) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < m) b[i] = c64{(double)a[i].re, (double)a[i].im};
+}
+
+// Inertia of the factored D (per-pivot rules, multifrontal_ldlt.rs:3220-3249).
+template <typename T>
+__global__ void k_inertia(int n, const T* __restrict__ d, const T* __restrict__ dsub,
+                          const unsigned char* __restrict__ kind, unsigned long long* __restrict__ cnt) {
+  using F = Field<T>;
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long pos = 0, neg = 0, zer = 0;
+  if (e < n) {
+    unsigned char kd = kind[e];
+    if (kd == 0) {
+      double r = F::real(d[e]);
+      if (r > 0) pos = 1;
+      else if (r < 0) neg = 1;
+      else zer = 1;
+    } else if (kd == 1) {
+      double det_r = F::real(F::sub(F::mul(d[e], d[e + 1]), F::mul(dsub[e], dsub[e])));
+      double tr_r = F::real(F::add(d[e], d[e + 1]));
+      if (det_r < 0) {
+        pos = 1;
+        neg = 1;
+      } else if (det_r > 0) {
+        if (tr_r >= 0) pos = 2;
+        else neg = 2;
+      } else {
+        zer = 1;
+        if (tr_r >= 0) pos = 1;
+        else neg = 1;
+      }
+    }
+  }
+  if (pos) atomicAdd(&cnt[0], pos);
+  if (neg) atomicAdd(&cnt[1], neg);
+  if (zer) atomicAdd(&cnt[2], zer);
+}
+
+}  // namespace rsd

@@ -1,0 +1,1166 @@
+// Host runtime of the B200 LDL^T path: structure upload, the value-independent
+// launch plan (one launch group per assembly-tree level), numeric factor and
+// multi-RHS solve orchestration on one CUDA stream per handle with CUDA-graph
+// capture of the frozen-pattern refactor and of the solve, the device-side
+// mixed-precision refinement ladder, and the extern "C" entry points declared
+// in include/rslab_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/rslab_b200.h"
+#include "device/factor_kernels.cuh"
+#include "device/solve_kernels.cuh"
+#include "host/host.hpp"
+
+using namespace rsd;
+using rslab::RslabError;
+using rslab::Status;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+#define CK(call)                                                                                   \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      throw RslabError(Status::CudaError, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+template <typename T>
+T* dalloc(size_t n) {
+  void* p = nullptr;
+  if (n == 0) n = 1;
+  CK(cudaMalloc(&p, n * sizeof(T)));
+  return reinterpret_cast<T*>(p);
+}
+template <typename T>
+T* dupload(const std::vector<T>& v, cudaStream_t st) {
+  T* p = dalloc<T>(v.size());
+  if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  return p;
+}
+struct DFree {
+  void operator()(void* p) const {
+    if (p) cudaFree(p);
+  }
+};
+
+size_t elem_size(int dtype) {
+  switch (dtype) {
+    case RSLAB_F64: return 8;
+    case RSLAB_C64: return 16;
+    case RSLAB_F32: return 4;
+    case RSLAB_C32: return 8;
+  }
+  throw RslabError(Status::InvalidInput, "unknown dtype");
+}
+
+enum LaunchKind { L_CMOD, L_GETF2, L_DEEP, L_SCHUR, L_FWD_GATHER, L_FWD_DIAG, L_BWD };
+struct Launch {
+  int kind;
+  long long task_off;  // into the int4 / int2 / int task arrays
+  int ntasks;
+  int nb_slot;         // getf2/deep: scratch stride nb
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Analysis handle: host symbolic + device structure + launch plan.
+// ---------------------------------------------------------------------------
+struct rslab_sym_handle {
+  rslab::Symbolic S;
+  int panel_nb = 64;
+  int n = 0, ns = 0;
+  long long nnz = 0;
+  long long panel_elems = 0;
+  std::vector<long long> poff;
+  std::vector<int> nrow;
+  // assembly targets (user lower-CSC order)
+  std::vector<int> a_row, a_col;
+  std::vector<long long> a_dst;
+  // full symmetric CSR of A for SpMV
+  std::vector<long long> sp_rp, sp_vmap;
+  std::vector<int> sp_ci;
+  // plan
+  std::vector<int4> t4;
+  std::vector<int2> t2;
+  std::vector<int> t1;
+  std::vector<Launch> fplan, fwdplan, bwdplan;
+  int max_getf2_tasks = 0;
+  int max_nb = 64;
+  double flops_model = 0, flops_proxy = 0;
+  // device mirrors (uploaded lazily on first factor)
+  int device = -1;
+  std::vector<std::unique_ptr<void, DFree>> bufs;
+  int *d_sn_first = nullptr, *d_sn_ncol = nullptr, *d_sn_nrow = nullptr, *d_rs = nullptr;
+  long long *d_poff = nullptr, *d_rsoff = nullptr;
+  int *d_upd_ptr = nullptr, *d_upd_k = nullptr, *d_upd_p0 = nullptr, *d_upd_p1 = nullptr;
+  int *d_a_row = nullptr, *d_a_col = nullptr, *d_perm = nullptr;
+  long long* d_a_dst = nullptr;
+  long long *d_sp_rp = nullptr, *d_sp_vmap = nullptr;
+  int* d_sp_ci = nullptr;
+  int4* d_t4 = nullptr;
+  int2* d_t2 = nullptr;
+  int* d_t1 = nullptr;
+  std::mutex mu;
+  rslab_analyze_settings settings{};
+
+  template <typename T>
+  T* up(const std::vector<T>& v, cudaStream_t st) {
+    T* p = dupload(v, st);
+    bufs.emplace_back(p);
+    return p;
+  }
+
+  void ensure_device(cudaStream_t st) {
+    std::lock_guard<std::mutex> g(mu);
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (device == dev) return;
+    if (device >= 0) throw RslabError(Status::InvalidInput, "analysis already bound to another device");
+    const auto& s = S;
+    std::vector<int> f(ns), c(ns), rs(s.rs.size());
+    std::vector<long long> rso(ns);
+    for (int i = 0; i < ns; ++i) {
+      f[i] = (int)s.sn[i].first_col;
+      c[i] = (int)s.sn[i].ncol;
+      rso[i] = s.rs_ptr[i];
+    }
+    for (size_t i = 0; i < s.rs.size(); ++i) rs[i] = (int)s.rs[i];
+    std::vector<int> up_(s.upd_ptr.begin(), s.upd_ptr.end()), uk(s.upd.begin(), s.upd.end()),
+        u0(s.upd_p0.begin(), s.upd_p0.end()), u1(s.upd_p1.begin(), s.upd_p1.end());
+    std::vector<int> perm(s.perm.begin(), s.perm.end());
+    d_sn_first = up(f, st);
+    d_sn_ncol = up(c, st);
+    d_sn_nrow = up(nrow, st);
+    d_poff = up(poff, st);
+    d_rsoff = up(rso, st);
+    d_rs = up(rs, st);
+    d_upd_ptr = up(up_, st);
+    d_upd_k = up(uk, st);
+    d_upd_p0 = up(u0, st);
+    d_upd_p1 = up(u1, st);
+    d_a_row = up(a_row, st);
+    d_a_col = up(a_col, st);
+    d_a_dst = up(a_dst, st);
+    d_perm = up(perm, st);
+    d_sp_rp = up(sp_rp, st);
+    d_sp_ci = up(sp_ci, st);
+    d_sp_vmap = up(sp_vmap, st);
+    d_t4 = up(t4, st);
+    d_t2 = up(t2, st);
+    d_t1 = up(t1, st);
+    CK(cudaStreamSynchronize(st));
+    device = dev;
+  }
+};
+
+namespace {
+
+// Build panel offsets, assembly targets, SpMV structure and the launch plan.
+void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_idx) {
+  const auto& S = H.S;
+  H.n = (int)S.n;
+  H.ns = (int)S.sn.size();
+  H.nnz = S.nnz;
+  const int ns = H.ns, n = H.n;
+  H.poff.assign(ns, 0);
+  H.nrow.assign(ns, 0);
+  long long acc = 0;
+  for (int s = 0; s < ns; ++s) {
+    long long nr = S.rs_ptr[s + 1] - S.rs_ptr[s];
+    H.nrow[s] = (int)nr;
+    H.poff[s] = acc;
+    acc += nr * S.sn[s].ncol;
+    H.flops_model += rslab::supernode_flops(nr, S.sn[s].ncol);
+    H.flops_proxy += (double)nr * nr * S.sn[s].ncol;
+  }
+  H.panel_elems = acc;
+  // Assembly targets: user (i, j) -> permuted lower (r, c) -> panel slot.
+  std::vector<int> col2sn(n);
+  for (int s = 0; s < ns; ++s)
+    for (int c = 0; c < S.sn[s].ncol; ++c) col2sn[S.sn[s].first_col + c] = s;
+  H.a_row.resize(H.nnz);
+  H.a_col.resize(H.nnz);
+  H.a_dst.resize(H.nnz);
+  for (int j = 0; j < n; ++j)
+    for (int64_t k = col_ptr[j]; k < col_ptr[j + 1]; ++k) {
+      int i = (int)row_idx[k];
+      int gi = (int)S.perm_inv[i], gj = (int)S.perm_inv[j];
+      int r = std::max(gi, gj), c = std::min(gi, gj);
+      int s = col2sn[c];
+      const int64_t* rs = S.rs.data() + S.rs_ptr[s];
+      int nr = H.nrow[s];
+      int li = (int)(std::lower_bound(rs, rs + nr, (int64_t)r) - rs);
+      if (li >= nr || rs[li] != r) throw RslabError(Status::InvalidInput, "assembly target outside row structure");
+      H.a_row[k] = i;
+      H.a_col[k] = j;
+      H.a_dst[k] = H.poff[s] + li + (long long)(c - S.sn[s].first_col) * nr;
+    }
+  // Full symmetric CSR (rows = user order) with value map into the lower CSC.
+  std::vector<long long> cnt(n, 0);
+  for (int j = 0; j < n; ++j)
+    for (int64_t k = col_ptr[j]; k < col_ptr[j + 1]; ++k) {
+      cnt[row_idx[k]]++;
+      if (row_idx[k] != j) cnt[j]++;
+    }
+  H.sp_rp.assign(n + 1, 0);
+  for (int i = 0; i < n; ++i) H.sp_rp[i + 1] = H.sp_rp[i] + cnt[i];
+  H.sp_ci.assign(H.sp_rp[n], 0);
+  H.sp_vmap.assign(H.sp_rp[n], 0);
+  std::vector<long long> off(H.sp_rp.begin(), H.sp_rp.end() - 1);
+  for (int j = 0; j < n; ++j)
+    for (int64_t k = col_ptr[j]; k < col_ptr[j + 1]; ++k) {
+      int i = (int)row_idx[k];
+      H.sp_ci[off[i]] = j;
+      H.sp_vmap[off[i]++] = k;
+      if (i != j) {
+        H.sp_ci[off[j]] = i;
+        H.sp_vmap[off[j]++] = k;
+      }
+    }
+
+  // Launch plan.
+  const int nb_small = H.panel_nb, nb_big = std::max(H.panel_nb, 128);
+  H.max_nb = nb_big;
+  auto nb_of = [&](int s) { return S.sn[s].ncol >= 512 ? nb_big : nb_small; };
+  for (const auto& lvl : S.by_level) {
+    // cmod tiles (lower part of every panel that has updaters).
+    {
+      Launch L{L_CMOD, (long long)H.t4.size(), 0, 0};
+      for (int64_t s : lvl) {
+        if (S.upd_ptr[s + 1] == S.upd_ptr[s]) continue;
+        int nc = (int)S.sn[s].ncol, nr = H.nrow[s];
+        for (int c0 = 0; c0 < nc; c0 += TILE)
+          for (int r0 = c0; r0 < nr; r0 += TILE) H.t4.push_back(make_int4((int)s, r0, c0, 0));
+      }
+      L.ntasks = (int)(H.t4.size() - L.task_off);
+      if (L.ntasks) H.fplan.push_back(L);
+    }
+    int maxblocks = 0;
+    for (int64_t s : lvl) maxblocks = std::max(maxblocks, (int)((S.sn[s].ncol + nb_of(s) - 1) / nb_of(s)));
+    for (int b = 0; b < maxblocks; ++b) {
+      Launch G{L_GETF2, (long long)H.t4.size(), 0, 0};
+      std::vector<int4> deep, schur;
+      int slot = 0, launch_nb = 0;
+      for (int64_t s : lvl) {
+        int nb = nb_of(s), nc = (int)S.sn[s].ncol, nr = H.nrow[s];
+        int kb = b * nb;
+        if (kb >= nc) continue;
+        int ke = std::min(kb + nb, nc);
+        bool fuse = (nr - ke) <= FUSE_DEEP_ROWS;
+        H.t4.push_back(make_int4((int)s, kb, slot, fuse ? 1 : 0));
+        launch_nb = std::max(launch_nb, nb);
+        if (!fuse)
+          for (int r0 = ke; r0 < nr; r0 += DEEP_R) deep.push_back(make_int4((int)s, kb, slot, r0));
+        int mt = nr - ke, cw = nc - ke;
+        for (int c0 = 0; c0 < cw; c0 += TILE)
+          for (int r0 = c0; r0 < mt; r0 += TILE) schur.push_back(make_int4((int)s, kb, r0, c0));
+        ++slot;
+      }
+      G.ntasks = slot;
+      G.nb_slot = launch_nb;
+      if (!slot) continue;
+      H.fplan.push_back(G);
+      H.max_getf2_tasks = std::max(H.max_getf2_tasks, slot);
+      if (!deep.empty()) {
+        Launch D{L_DEEP, (long long)H.t4.size(), (int)deep.size(), launch_nb};
+        H.t4.insert(H.t4.end(), deep.begin(), deep.end());
+        H.fplan.push_back(D);
+      }
+      if (!schur.empty()) {
+        Launch C{L_SCHUR, (long long)H.t4.size(), (int)schur.size(), 0};
+        H.t4.insert(H.t4.end(), schur.begin(), schur.end());
+        H.fplan.push_back(C);
+      }
+    }
+    // Forward solve launches for this level.
+    {
+      Launch L{L_FWD_GATHER, (long long)H.t2.size(), 0, 0};
+      for (int64_t s : lvl) {
+        if (S.upd_ptr[s + 1] == S.upd_ptr[s]) continue;
+        for (int c0 = 0; c0 < S.sn[s].ncol; c0 += SB) H.t2.push_back(make_int2((int)s, c0));
+      }
+      L.ntasks = (int)(H.t2.size() - L.task_off);
+      if (L.ntasks) H.fwdplan.push_back(L);
+      Launch Dg{L_FWD_DIAG, (long long)H.t1.size(), (int)lvl.size(), 0};
+      for (int64_t s : lvl) H.t1.push_back((int)s);
+      H.fwdplan.push_back(Dg);
+    }
+  }
+  // Backward: levels root first; the task list reuses the level lists.
+  std::vector<std::pair<long long, int>> lvl_ranges;
+  for (const auto& L : H.fwdplan)
+    if (L.kind == L_FWD_DIAG) lvl_ranges.push_back({L.task_off, L.ntasks});
+  for (auto it = lvl_ranges.rbegin(); it != lvl_ranges.rend(); ++it) H.bwdplan.push_back({L_BWD, it->first, it->second, 0});
+}
+
+size_t smem_cmod(size_t es) { return (size_t)TILE * TILE * es + 2 * 16 * TILE * es + 3 * TILE * 4 + 64; }
+size_t smem_schur(size_t es) { return 2 * 16 * TILE * es; }
+size_t smem_getf2(size_t es, int nb) {
+  size_t a = (size_t)nb * (nb + 1) / 2 * es + 2 * nb * es + 32 * 8 + 32 * 4 + 16 * 4;
+  size_t b = (size_t)DEEP_R * nb * es;
+  return std::max(a, b) + 64;
+}
+size_t smem_deep(size_t es, int nb) { return (size_t)DEEP_R * nb * es + 64; }
+size_t smem_solve(size_t es) { return (size_t)(SOLVE_NT / 32) * 32 * RHS_MAX * es + 32 * RHS_MAX * es + 64 * 4; }
+
+template <typename T>
+struct KernelSetup {
+  static void configure() {
+    static bool done = false;
+    if (done) return;
+    const size_t es = sizeof(T);
+    CK(cudaFuncSetAttribute(k_cmod<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod(es)));
+    CK(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
+    CK(cudaFuncSetAttribute(k_getf2<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_getf2(es, 128)));
+    CK(cudaFuncSetAttribute(k_deep<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep(es, 128)));
+    CK(cudaFuncSetAttribute(k_fwd_gather<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
+    CK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
+    CK(cudaFuncSetAttribute(k_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
+    done = true;
+  }
+};
+
+inline unsigned grid1(long long m, int tpb = 256) { return (unsigned)((m + tpb - 1) / tpb); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Factor handle.
+// ---------------------------------------------------------------------------
+struct rslab_fac_handle {
+  rslab_sym_handle* sym = nullptr;
+  int dtype = RSLAB_F64;     // field the factor computes in
+  int dtype_hi = -1;         // mixed mode: field of the original A (else -1)
+  rslab_factor_settings set{};
+  cudaStream_t st = nullptr;
+  bool own_stream = false;
+  std::vector<std::unique_ptr<void, DFree>> bufs;
+  void* panel = nullptr;
+  void* d = nullptr;
+  void* dsub = nullptr;
+  unsigned char* kind = nullptr;
+  int* lperm = nullptr;
+  double* scale = nullptr;
+  unsigned long long* rowmax = nullptr;
+  void* aval = nullptr;     // A values in the factor field (device)
+  void* aval_hi = nullptr;  // mixed mode: original A (device, high precision)
+  int* status = nullptr;
+  int* h_status = nullptr;  // pinned
+  unsigned long long* cnt3 = nullptr;
+  void* scratch = nullptr;
+  long long scratch_stride = 0;
+  // graph of the numeric factor (values read from `aval`)
+  cudaGraphExec_t fgraph = nullptr;
+  // solve workspace
+  int ws_nrhs = 0;
+  void *Yg = nullptr, *Ze = nullptr, *Xg = nullptr, *bdev = nullptr, *xdev = nullptr;
+  std::vector<std::unique_ptr<void, DFree>> ws;
+  cudaGraphExec_t sgraph = nullptr;
+  int sgraph_nrhs = -1;
+  // results
+  long long ipos = 0, ineg = 0, izero = 0, nperturbed = 0;
+  int last_status = 0, failing_sn = -1;
+  double factor_ms = 0, solve_ms = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  ~rslab_fac_handle() {
+    if (fgraph) cudaGraphExecDestroy(fgraph);
+    if (sgraph) cudaGraphExecDestroy(sgraph);
+    if (h_status) cudaFreeHost(h_status);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (own_stream && st) cudaStreamDestroy(st);
+  }
+  template <typename T>
+  T* al(size_t n) {
+    T* p = dalloc<T>(n);
+    bufs.emplace_back(p);
+    return p;
+  }
+};
+
+namespace {
+
+template <typename T>
+FactorArgs make_fargs(rslab_fac_handle& F) {
+  auto& H = *F.sym;
+  FactorArgs a;
+  a.sn_first = H.d_sn_first;
+  a.sn_ncol = H.d_sn_ncol;
+  a.sn_nrow = H.d_sn_nrow;
+  a.sn_poff = H.d_poff;
+  a.sn_rsoff = H.d_rsoff;
+  a.rs = H.d_rs;
+  a.upd_ptr = H.d_upd_ptr;
+  a.upd_k = H.d_upd_k;
+  a.upd_p0 = H.d_upd_p0;
+  a.upd_p1 = H.d_upd_p1;
+  a.panel = F.panel;
+  a.d = F.d;
+  a.dsub = F.dsub;
+  a.kind = F.kind;
+  a.lperm = F.lperm;
+  a.scratch = F.scratch;
+  a.scratch_stride = F.scratch_stride;
+  a.status = F.status;
+  a.perturb_floor = F.set.on_zero_pivot == RSLAB_PIVOT_PERTURB ? F.set.abs_floor : -1.0;
+  return a;
+}
+
+// Enqueue the whole numeric factor of the values in F.aval on F.st.
+template <typename T>
+void enqueue_factor(rslab_fac_handle& F) {
+  auto& H = *F.sym;
+  const int n = H.n;
+  const size_t es = sizeof(T);
+  cudaStream_t st = F.st;
+  CK(cudaMemsetAsync(F.status, 0, 4 * sizeof(int), st));
+  CK(cudaMemsetAsync(F.panel, 0, H.panel_elems * es, st));
+  CK(cudaMemsetAsync(F.kind, 0, n, st));
+  CK(cudaMemsetAsync(F.d, 0, n * es, st));
+  CK(cudaMemsetAsync(F.dsub, 0, n * es, st));
+  if (F.set.scaling == RSLAB_SCALING_ONEPASS) {
+    CK(cudaMemsetAsync(F.rowmax, 0, n * sizeof(unsigned long long), st));
+    if (H.nnz) k_rowmax<T><<<grid1(H.nnz), 256, 0, st>>>(H.nnz, H.d_a_row, H.d_a_col, (const T*)F.aval, F.rowmax);
+    k_scale_from_rowmax<<<grid1(n), 256, 0, st>>>(n, F.rowmax, F.scale);
+  }
+  if (H.nnz)
+    k_assemble<T><<<grid1(H.nnz), 256, 0, st>>>(H.nnz, H.d_a_row, H.d_a_col, (const T*)F.aval, F.scale, H.d_a_dst,
+                                                (T*)F.panel);
+  FactorArgs fa = make_fargs<T>(F);
+  const int nb_small = H.panel_nb, nb_big = std::max(H.panel_nb, 128);
+  for (const Launch& L : H.fplan) {
+    switch (L.kind) {
+      case L_CMOD:
+        k_cmod<T><<<L.ntasks, TPB, smem_cmod(es), st>>>(fa, H.d_t4 + L.task_off);
+        break;
+      case L_GETF2: {
+        FactorArgs f2 = fa;
+        f2.scratch_stride = ((long long)L.nb_slot * L.nb_slot * es + 3 * L.nb_slot * 4 + 255) / 256 * 256;
+        k_getf2<T, 256><<<L.ntasks, 256, smem_getf2(es, L.nb_slot), st>>>(f2, H.d_t4 + L.task_off, nb_small, nb_big);
+        break;
+      }
+      case L_DEEP: {
+        FactorArgs f2 = fa;
+        f2.scratch_stride = ((long long)L.nb_slot * L.nb_slot * es + 3 * L.nb_slot * 4 + 255) / 256 * 256;
+        k_deep<T, 256><<<L.ntasks, 256, smem_deep(es, L.nb_slot), st>>>(f2, H.d_t4 + L.task_off, nb_small, nb_big);
+        break;
+      }
+      case L_SCHUR:
+        k_schur<T><<<L.ntasks, TPB, smem_schur(es), st>>>(fa, H.d_t4 + L.task_off, nb_small, nb_big);
+        break;
+    }
+  }
+  CK(cudaMemsetAsync(F.cnt3, 0, 3 * sizeof(unsigned long long), st));
+  k_inertia<T><<<grid1(n), 256, 0, st>>>(n, (const T*)F.d, (const T*)F.dsub, F.kind, F.cnt3);
+  CK(cudaGetLastError());
+}
+
+template <typename T>
+void run_factor(rslab_fac_handle& F) {
+  auto& H = *F.sym;
+  KernelSetup<T>::configure();
+  CK(cudaEventRecord(F.ev0, F.st));
+  if (F.set.use_graph) {
+    if (!F.fgraph) {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(F.st, cudaStreamCaptureModeThreadLocal));
+      try {
+        enqueue_factor<T>(F);
+      } catch (...) {
+        cudaStreamEndCapture(F.st, &g);
+        throw;
+      }
+      CK(cudaStreamEndCapture(F.st, &g));
+      CK(cudaGraphInstantiate(&F.fgraph, g, 0));
+      cudaGraphDestroy(g);
+    }
+    CK(cudaGraphLaunch(F.fgraph, F.st));
+  } else {
+    enqueue_factor<T>(F);
+  }
+  CK(cudaEventRecord(F.ev1, F.st));
+  // status + inertia back to the host
+  CK(cudaMemcpyAsync(F.h_status, F.status, 4 * sizeof(int), cudaMemcpyDeviceToHost, F.st));
+  unsigned long long c3[3];
+  CK(cudaMemcpyAsync(c3, F.cnt3, sizeof(c3), cudaMemcpyDeviceToHost, F.st));
+  CK(cudaStreamSynchronize(F.st));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, F.ev0, F.ev1));
+  F.factor_ms = ms;
+  F.last_status = F.h_status[0];
+  F.failing_sn = F.h_status[0] ? F.h_status[1] : -1;
+  F.nperturbed = F.h_status[2];
+  F.ipos = (long long)c3[0];
+  F.ineg = (long long)c3[1];
+  F.izero = (long long)c3[2];
+  (void)H;
+  if (F.last_status) throw RslabError(Status::NumericallyRankDeficient,
+                                      "numerically rank deficient pivot in supernode " + std::to_string(F.failing_sn));
+}
+
+template <typename T>
+void ensure_ws(rslab_fac_handle& F, int nrhs) {
+  if (F.ws_nrhs >= nrhs) return;
+  const size_t es = sizeof(T);
+  const long long m = (long long)F.sym->n * nrhs;
+  F.ws.clear();
+  auto a = [&](size_t bytes) {
+    void* p = nullptr;
+    CK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+    F.ws.emplace_back(p);
+    return p;
+  };
+  F.Yg = a(m * es);
+  F.Ze = a(m * es);
+  F.Xg = a(m * es);
+  F.bdev = a(m * es);
+  F.xdev = a(m * es);
+  F.ws_nrhs = nrhs;
+  if (F.sgraph) {
+    cudaGraphExecDestroy(F.sgraph);
+    F.sgraph = nullptr;
+    F.sgraph_nrhs = -1;
+  }
+}
+
+template <typename T>
+SolveArgs make_sargs(rslab_fac_handle& F, int ld, int c0, int nr) {
+  auto& H = *F.sym;
+  SolveArgs a;
+  a.sn_first = H.d_sn_first;
+  a.sn_ncol = H.d_sn_ncol;
+  a.sn_nrow = H.d_sn_nrow;
+  a.sn_poff = H.d_poff;
+  a.sn_rsoff = H.d_rsoff;
+  a.rs = H.d_rs;
+  a.upd_ptr = H.d_upd_ptr;
+  a.upd_k = H.d_upd_k;
+  a.upd_p0 = H.d_upd_p0;
+  a.upd_p1 = H.d_upd_p1;
+  a.panel = F.panel;
+  a.d = F.d;
+  a.dsub = F.dsub;
+  a.kind = F.kind;
+  a.lperm = F.lperm;
+  a.Yg = F.Yg;
+  a.Ze = F.Ze;
+  a.Xg = F.Xg;
+  a.ld = ld;
+  a.c0 = c0;
+  a.nrhs = nr;
+  return a;
+}
+
+// x = A^-1 b on device buffers (row-major n x nrhs) in the factor's field.
+template <typename T>
+void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs) {
+  auto& H = *F.sym;
+  const int n = H.n;
+  const size_t es = sizeof(T);
+  cudaStream_t st = F.st;
+  k_perm_in<T><<<grid1((long long)n * nrhs), 256, 0, st>>>(n, nrhs, H.d_perm, F.scale, b, (T*)F.Yg);
+  for (int c0 = 0; c0 < nrhs; c0 += RHS_MAX) {
+    const int nr = std::min(RHS_MAX, nrhs - c0);
+    SolveArgs sa = make_sargs<T>(F, nrhs, c0, nr);
+    for (const Launch& L : H.fwdplan) {
+      if (L.kind == L_FWD_GATHER)
+        k_fwd_gather<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t2 + L.task_off);
+      else
+        k_fwd_diag<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
+    }
+    for (const Launch& L : H.bwdplan) k_bwd<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
+  }
+  k_perm_out<T><<<grid1((long long)n * nrhs), 256, 0, st>>>(n, nrhs, H.d_perm, F.scale, (const T*)F.Xg, x);
+  CK(cudaGetLastError());
+}
+
+// Solve with graph capture keyed on nrhs; b, x are the workspace bdev/xdev.
+template <typename T>
+void solve_ws(rslab_fac_handle& F, int nrhs) {
+  KernelSetup<T>::configure();
+  if (F.set.use_graph) {
+    if (!F.sgraph || F.sgraph_nrhs != nrhs) {
+      if (F.sgraph) cudaGraphExecDestroy(F.sgraph);
+      F.sgraph = nullptr;
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(F.st, cudaStreamCaptureModeThreadLocal));
+      try {
+        enqueue_solve<T>(F, (const T*)F.bdev, (T*)F.xdev, nrhs);
+      } catch (...) {
+        cudaStreamEndCapture(F.st, &g);
+        throw;
+      }
+      CK(cudaStreamEndCapture(F.st, &g));
+      CK(cudaGraphInstantiate(&F.sgraph, g, 0));
+      cudaGraphDestroy(g);
+      F.sgraph_nrhs = nrhs;
+    }
+    CK(cudaGraphLaunch(F.sgraph, F.st));
+  } else {
+    enqueue_solve<T>(F, (const T*)F.bdev, (T*)F.xdev, nrhs);
+  }
+}
+
+template <typename T>
+void do_solve(rslab_fac_handle& F, const void* b, void* x, int nrhs, bool on_device) {
+  if (F.last_status) throw RslabError(Status::NumericallyRankDeficient, "factor is not valid");
+  const size_t es = sizeof(T);
+  const long long m = (long long)F.sym->n * nrhs;
+  ensure_ws<T>(F, nrhs);
+  CK(cudaMemcpyAsync(F.bdev, b, m * es, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, F.st));
+  CK(cudaEventRecord(F.ev0, F.st));
+  solve_ws<T>(F, nrhs);
+  CK(cudaEventRecord(F.ev1, F.st));
+  CK(cudaMemcpyAsync(x, F.xdev, m * es, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, F.st));
+  CK(cudaStreamSynchronize(F.st));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, F.ev0, F.ev1));
+  F.solve_ms = ms;
+}
+
+template <typename T>
+void dispatch_field(int dtype, T&& fn) {
+  switch (dtype) {
+    case RSLAB_F64: fn(double{}); break;
+    case RSLAB_C64: fn(c64{}); break;
+    case RSLAB_F32: fn(float{}); break;
+    case RSLAB_C32: fn(c32{}); break;
+    default: throw RslabError(Status::InvalidInput, "unknown dtype");
+  }
+}
+
+int fail(const RslabError& e) {
+  g_last_error = e.what();
+  return (int)e.status;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Mixed-precision refinement ladder (MixedLdltSolver::solve_to,
+// src/numeric/mixed.rs:140-221): x0 = promote(F_lo^-1 demote(b)); plain IR
+// with the FP64 residual against the original A while the normwise backward
+// error exceeds the target (<= 8 steps, contraction 0.5), then FGMRES(30)
+// (max 120) right-preconditioned by the low-precision factor, warm-started at
+// the best iterate.  Column-wise for several right-hand sides.
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename Hi>
+struct MixedCtx {
+  using Lo = typename Field<Hi>::Lo;
+  rslab_fac_handle& F;
+  int n, nrhs;
+  cudaStream_t st;
+  std::vector<std::unique_ptr<void, DFree>> bufs;
+  Hi *r = nullptr, *dx = nullptr, *ax = nullptr;
+  unsigned long long* nb = nullptr;
+  MixedCtx(rslab_fac_handle& f, int nr) : F(f), n(f.sym->n), nrhs(nr), st(f.st) {
+    const long long m = (long long)n * nrhs;
+    auto a = [&](size_t bytes) {
+      void* p = nullptr;
+      CK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+      bufs.emplace_back(p);
+      return p;
+    };
+    r = (Hi*)a(m * sizeof(Hi));
+    dx = (Hi*)a(m * sizeof(Hi));
+    ax = (Hi*)a(m * sizeof(Hi));
+    nb = (unsigned long long*)a(3 * 64 * sizeof(unsigned long long));
+  }
+  // dx = promote(F_lo^-1 demote(r)) for an n x k block (k <= nrhs, ld = k).
+  void precond(const Hi* rr, Hi* out, int k) {
+    const long long m = (long long)n * k;
+    ensure_ws<Lo>(F, k);
+    k_cast_down<Hi, Lo><<<grid1(m), 256, 0, st>>>(m, rr, (Lo*)F.bdev);
+    solve_ws<Lo>(F, k);
+    k_cast_up<Lo, Hi><<<grid1(m), 256, 0, st>>>(m, (const Lo*)F.xdev, out);
+  }
+  void residual(const Hi* x, const Hi* b, Hi* rr, int k) {
+    auto& H = *F.sym;
+    k_residual<Hi><<<grid1((long long)n * k), 256, 0, st>>>(n, k, H.d_sp_rp, H.d_sp_ci, H.d_sp_vmap,
+                                                          (const Hi*)F.aval_hi, x, b, rr);
+  }
+  void spmv(const Hi* x, Hi* y, int k) {
+    auto& H = *F.sym;
+    k_spmv<Hi><<<grid1((long long)n * k), 256, 0, st>>>(n, k, H.d_sp_rp, H.d_sp_ci, H.d_sp_vmap,
+                                                      (const Hi*)F.aval_hi, x, y);
+  }
+  // per-column inf norms of up to 3 vectors -> host
+  void colmax(const Hi* v, int k, double* out) {
+    CK(cudaMemsetAsync(nb, 0, k * sizeof(unsigned long long), st));
+    dim3 g(std::min<unsigned>(grid1(n), 1024u), k);
+    k_colmax<Hi><<<g, 256, 0, st>>>(n, k, v, nb);
+    std::vector<unsigned long long> h(k);
+    CK(cudaMemcpyAsync(h.data(), nb, k * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int c = 0; c < k; ++c) {
+      double dv;
+      std::memcpy(&dv, &h[c], 8);
+      out[c] = dv;
+    }
+  }
+};
+
+}  // namespace
+
+// FGMRES for one right-hand side column, all vectors on the device; the
+// Hessenberg least-squares and Givens rotations run on the host
+// (iterative.rs:822-1037).
+template <typename Hi>
+static int gmres_column(MixedCtx<Hi>& M, const Hi* b, Hi* x, double tol, int max_iter, int restart);
+
+#include "engine_gmres.inc"
+
+extern "C" {
+
+const char* rslab_last_error(void) { return g_last_error.c_str(); }
+
+int rslab_version(void) { return RSLAB_ABI_VERSION; }
+
+void rslab_default_analyze_settings(rslab_analyze_settings* s) {
+  s->ordering = RSLAB_ORDER_AMD;
+  s->nemin = 16;
+  s->relax = 1;
+  s->relax_max_width = 256;
+  s->relax_max_extra_rows = 64;
+  s->hybrid_liu = 1;
+  s->panel_nb = 64;
+  s->given_perm = nullptr;
+}
+
+void rslab_default_factor_settings(rslab_factor_settings* s) {
+  s->on_zero_pivot = RSLAB_PIVOT_FAIL;
+  s->abs_floor = 0.0;
+  s->scaling = RSLAB_SCALING_ONEPASS;
+  s->use_graph = 1;
+  s->stream = nullptr;
+}
+
+int rslab_analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, const rslab_analyze_settings* settings,
+                  rslab_sym_handle** out) {
+  try {
+    if (!out) throw RslabError(Status::InvalidInput, "null output handle");
+    *out = nullptr;
+    if (n < 0 || !col_ptr || (n > 0 && !row_idx && col_ptr[n] > 0)) throw RslabError(Status::InvalidInput, "bad CSC");
+    if (n >= (int64_t)1 << 31) throw RslabError(Status::InvalidInput, "n too large");
+    rslab::validate_lower_csc(n, col_ptr, row_idx, col_ptr[n]);
+    rslab_analyze_settings st;
+    if (settings)
+      st = *settings;
+    else
+      rslab_default_analyze_settings(&st);
+    rslab::AnalyzeOptions o;
+    o.ordering = (rslab::Ordering)st.ordering;
+    o.nemin = st.nemin;
+    o.relax = st.relax != 0;
+    o.relax_max_width = st.relax_max_width;
+    o.relax_max_extra_rows = st.relax_max_extra_rows;
+    o.hybrid_liu = st.hybrid_liu != 0;
+    o.given_perm = st.given_perm;
+    auto H = std::make_unique<rslab_sym_handle>();
+    H->settings = st;
+    H->panel_nb = (int)std::max<int64_t>(st.panel_nb, 8);
+    H->S = rslab::analyze(n, col_ptr, row_idx, o);
+    build_plan(*H, col_ptr, row_idx);
+    *out = H.release();
+    return 0;
+  } catch (const RslabError& e) {
+    return fail(e);
+  } catch (const std::exception& e) {
+    return fail(RslabError(Status::InvalidInput, e.what()));
+  }
+}
+
+void rslab_free_symbolic(rslab_sym_handle* h) { delete h; }
+
+int rslab_symbolic_info(const rslab_sym_handle* h, rslab_symbolic_info_t* info) {
+  if (!h || !info) return (int)Status::InvalidInput;
+  info->n = h->n;
+  info->nnz = h->nnz;
+  info->nsuper = h->ns;
+  info->nlevels = (int64_t)h->S.by_level.size();
+  info->factor_nnz_sym = h->S.factor_nnz_sym;
+  info->panel_elems = h->panel_elems;
+  info->flops_model = h->flops_model;
+  info->flops_proxy = h->flops_proxy;
+  info->renumbered = h->S.renumbered;
+  info->amd_ncmpa = h->S.amd.ncmpa;
+  info->amd_ndense = h->S.amd.n_dense;
+  info->amd_ndiv = h->S.amd.ndiv;
+  info->amd_nms_ldl = h->S.amd.nms_ldl;
+  info->amd_nms_lu = h->S.amd.nms_lu;
+  info->n_factor_launches = (int64_t)h->fplan.size();
+  info->n_solve_launches = (int64_t)(h->fwdplan.size() + h->bwdplan.size());
+  return 0;
+}
+
+// perm[n], sn_first/sn_ncol/sn_nrow/sn_level[nsuper], child_ptr[nsuper+1],
+// child_idx[nsuper], col_counts[n], parent[n]; any pointer may be null.
+int rslab_symbolic_export(const rslab_sym_handle* h, int64_t* perm, int64_t* sn_first, int64_t* sn_ncol,
+                          int64_t* sn_nrow, int64_t* sn_level, int64_t* child_ptr, int64_t* child_idx,
+                          int64_t* col_counts, int64_t* parent) {
+  if (!h) return (int)Status::InvalidInput;
+  const auto& S = h->S;
+  if (perm) std::copy(S.perm.begin(), S.perm.end(), perm);
+  if (col_counts) std::copy(S.col_counts.begin(), S.col_counts.end(), col_counts);
+  if (parent) std::copy(S.parent.begin(), S.parent.end(), parent);
+  int64_t cp = 0;
+  for (int s = 0; s < h->ns; ++s) {
+    if (sn_first) sn_first[s] = S.sn[s].first_col;
+    if (sn_ncol) sn_ncol[s] = S.sn[s].ncol;
+    if (sn_nrow) sn_nrow[s] = h->nrow[s];
+    if (sn_level) sn_level[s] = S.level[s];
+    if (child_ptr) child_ptr[s] = cp;
+    for (int64_t c : S.sn[s].children) {
+      if (child_idx) child_idx[cp] = c;
+      ++cp;
+    }
+  }
+  if (child_ptr) child_ptr[h->ns] = cp;
+  return 0;
+}
+
+static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const void* values, int on_device,
+                       const rslab_factor_settings* settings, rslab_fac_handle** out) {
+  try {
+    if (!sym || !out) throw RslabError(Status::InvalidInput, "null handle");
+    *out = nullptr;
+    auto F = std::make_unique<rslab_fac_handle>();
+    F->sym = sym;
+    F->dtype = dtype;
+    F->dtype_hi = dtype_hi;
+    if (settings)
+      F->set = *settings;
+    else
+      rslab_default_factor_settings(&F->set);
+    if (F->set.stream) {
+      F->st = (cudaStream_t)F->set.stream;
+    } else {
+      CK(cudaStreamCreateWithFlags(&F->st, cudaStreamNonBlocking));
+      F->own_stream = true;
+    }
+    CK(cudaEventCreate(&F->ev0));
+    CK(cudaEventCreate(&F->ev1));
+    sym->ensure_device(F->st);
+    const size_t es = elem_size(dtype);
+    const int n = sym->n;
+    F->panel = F->al<unsigned char>(sym->panel_elems * es);
+    F->d = F->al<unsigned char>(n * es);
+    F->dsub = F->al<unsigned char>(n * es);
+    F->kind = F->al<unsigned char>(n);
+    F->lperm = F->al<int>(n);
+    F->scale = F->al<double>(n);
+    F->rowmax = F->al<unsigned long long>(n);
+    F->status = F->al<int>(4);
+    F->cnt3 = F->al<unsigned long long>(3);
+    F->aval = F->al<unsigned char>(sym->nnz * es);
+    CK(cudaMallocHost(&F->h_status, 4 * sizeof(int)));
+    const long long nbm = sym->max_nb;
+    F->scratch_stride = (nbm * nbm * (long long)es + 3 * nbm * 4 + 255) / 256 * 256;
+    F->scratch = F->al<unsigned char>((size_t)std::max(1, sym->max_getf2_tasks) * F->scratch_stride);
+    if (F->set.scaling != RSLAB_SCALING_ONEPASS) {
+      std::vector<double> ones(n, 1.0);
+      CK(cudaMemcpyAsync(F->scale, ones.data(), n * 8, cudaMemcpyHostToDevice, F->st));
+      CK(cudaStreamSynchronize(F->st));
+    }
+    const cudaMemcpyKind kd = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (dtype_hi >= 0) {
+      const size_t eh = elem_size(dtype_hi);
+      F->aval_hi = F->al<unsigned char>(sym->nnz * eh);
+      CK(cudaMemcpyAsync(F->aval_hi, values, sym->nnz * eh, kd, F->st));
+      if (dtype_hi == RSLAB_F64)
+        k_demote<double, float><<<grid1(sym->nnz), 256, 0, F->st>>>(sym->nnz, (const double*)F->aval_hi,
+                                                                    (float*)F->aval);
+      else
+        k_demote<c64, c32><<<grid1(sym->nnz), 256, 0, F->st>>>(sym->nnz, (const c64*)F->aval_hi, (c32*)F->aval);
+    } else {
+      CK(cudaMemcpyAsync(F->aval, values, sym->nnz * es, kd, F->st));
+    }
+    rslab_fac_handle* raw = F.get();
+    int rc = 0;
+    try {
+      dispatch_field(dtype, [&](auto z) { run_factor<decltype(z)>(*raw); });
+    } catch (const RslabError& e) {
+      if (e.status != Status::NumericallyRankDeficient) throw;
+      rc = fail(e);
+    }
+    *out = F.release();
+    return rc;
+  } catch (const RslabError& e) {
+    return fail(e);
+  } catch (const std::exception& e) {
+    return fail(RslabError(Status::InvalidInput, e.what()));
+  }
+}
+
+int rslab_factor(rslab_sym_handle* sym, int dtype, const void* values, int values_on_device,
+                 const rslab_factor_settings* settings, rslab_fac_handle** out) {
+  return factor_impl(sym, dtype, -1, values, values_on_device, settings, out);
+}
+
+int rslab_mixed_factor(rslab_sym_handle* sym, int dtype_hi, const void* values_hi, int values_on_device,
+                       const rslab_factor_settings* settings, rslab_fac_handle** out) {
+  int lo = dtype_hi == RSLAB_F64 ? RSLAB_F32 : dtype_hi == RSLAB_C64 ? RSLAB_C32 : -1;
+  if (lo < 0) {
+    g_last_error = "mixed factor needs an f64 or c64 matrix";
+    return (int)Status::InvalidInput;
+  }
+  return factor_impl(sym, lo, dtype_hi, values_hi, values_on_device, settings, out);
+}
+
+int rslab_refactor(rslab_fac_handle* F, const void* values, int values_on_device) {
+  try {
+    if (!F) throw RslabError(Status::InvalidInput, "null handle");
+    auto& H = *F->sym;
+    const cudaMemcpyKind kd = values_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (F->dtype_hi >= 0) {
+      const size_t eh = elem_size(F->dtype_hi);
+      CK(cudaMemcpyAsync(F->aval_hi, values, H.nnz * eh, kd, F->st));
+      if (F->dtype_hi == RSLAB_F64)
+        k_demote<double, float><<<grid1(H.nnz), 256, 0, F->st>>>(H.nnz, (const double*)F->aval_hi, (float*)F->aval);
+      else
+        k_demote<c64, c32><<<grid1(H.nnz), 256, 0, F->st>>>(H.nnz, (const c64*)F->aval_hi, (c32*)F->aval);
+    } else {
+      CK(cudaMemcpyAsync(F->aval, values, H.nnz * elem_size(F->dtype), kd, F->st));
+    }
+    dispatch_field(F->dtype, [&](auto z) { run_factor<decltype(z)>(*F); });
+    return 0;
+  } catch (const RslabError& e) {
+    return fail(e);
+  } catch (const std::exception& e) {
+    return fail(RslabError(Status::InvalidInput, e.what()));
+  }
+}
+
+int rslab_solve(rslab_fac_handle* F, const void* b, int64_t nrhs, void* x, int on_device) {
+  try {
+    if (!F || nrhs <= 0) throw RslabError(Status::DimensionMismatch, "nrhs must be positive");
+    dispatch_field(F->dtype, [&](auto z) { do_solve<decltype(z)>(*F, b, x, (int)nrhs, on_device != 0); });
+    return 0;
+  } catch (const RslabError& e) {
+    return fail(e);
+  } catch (const std::exception& e) {
+    return fail(RslabError(Status::InvalidInput, e.what()));
+  }
+}
+
+int rslab_mixed_solve(rslab_fac_handle* F, const void* b, int64_t nrhs, double target, void* x, int on_device,
+                      rslab_mixed_info* info) {
+  try {
+    if (!F || F->dtype_hi < 0) throw RslabError(Status::InvalidInput, "not a mixed-precision factor");
+    if (nrhs <= 0) throw RslabError(Status::DimensionMismatch, "nrhs must be positive");
+    if (F->last_status) throw RslabError(Status::NumericallyRankDeficient, "factor is not valid");
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = 0;
+    if (F->dtype_hi == RSLAB_F64)
+      rc = mixed_solve_impl<double>(*F, b, (int)nrhs, target, x, on_device != 0, info);
+    else
+      rc = mixed_solve_impl<c64>(*F, b, (int)nrhs, target, x, on_device != 0, info);
+    F->solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+  } catch (const RslabError& e) {
+    return fail(e);
+  } catch (const std::exception& e) {
+    return fail(RslabError(Status::InvalidInput, e.what()));
+  }
+}
+
+int rslab_factor_info(const rslab_fac_handle* F, rslab_factor_info_t* info) {
+  if (!F || !info) return (int)Status::InvalidInput;
+  info->status = F->last_status;
+  info->failing_supernode = F->failing_sn;
+  info->inertia_pos = F->ipos;
+  info->inertia_neg = F->ineg;
+  info->inertia_zero = F->izero;
+  info->n_perturbed = F->nperturbed;
+  info->factor_ms = F->factor_ms;
+  info->solve_ms = F->solve_ms;
+  info->dtype = F->dtype;
+  info->dtype_hi = F->dtype_hi;
+  return 0;
+}
+
+void* rslab_factor_stream(const rslab_fac_handle* F) { return F ? (void*)F->st : nullptr; }
+
+// Export in the reference LdltFactors layout (src/dense/ldlt_generic.rs:31-66):
+// unit diagonal first, rows sorted, exact zeros dropped, the 2x2 coupling row
+// skipped.  l_col_ptr[n+1]; call with null value arrays to get nnz first via
+// rslab_factor_nnz.
+static void export_counts(const rslab_fac_handle* F, std::vector<unsigned char>& panel, std::vector<int>& lperm,
+                          std::vector<unsigned char>& kind) {
+  auto& H = *F->sym;
+  const size_t es = elem_size(F->dtype);
+  panel.resize(H.panel_elems * es);
+  lperm.resize(H.n);
+  kind.resize(H.n);
+  CK(cudaMemcpy(panel.data(), F->panel, panel.size(), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(lperm.data(), F->lperm, H.n * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(kind.data(), F->kind, H.n, cudaMemcpyDeviceToHost));
+}
+
+static bool is_zero_bytes(const unsigned char* p, size_t es) {
+  // exact zero of the field (both +0 and -0)
+  if (es == 8) {
+    double v;
+    std::memcpy(&v, p, 8);
+    return v == 0.0;
+  }
+  if (es == 16) {
+    double v[2];
+    std::memcpy(v, p, 16);
+    return v[0] == 0.0 && v[1] == 0.0;
+  }
+  if (es == 4) {
+    float v;
+    std::memcpy(&v, p, 4);
+    return v == 0.0f;
+  }
+  float v[2];
+  std::memcpy(v, p, 8);
+  return v[0] == 0.0f && v[1] == 0.0f;
+}
+
+int rslab_export_factors(const rslab_fac_handle* F, int64_t* l_col_ptr, int64_t* l_row_idx, void* l_values, void* d_diag,
+                         void* d_subdiag, uint8_t* two_by_two, int64_t* perm, double* scale, int64_t* nnz_out) {
+  try {
+    if (!F) throw RslabError(Status::InvalidInput, "null handle");
+    auto& H = *F->sym;
+    const auto& S = H.S;
+    const size_t es = elem_size(F->dtype);
+    std::vector<unsigned char> panel, kind;
+    std::vector<int> lperm;
+    export_counts(F, panel, lperm, kind);
+    const int n = H.n;
+    std::vector<int64_t> e_of_g(n);
+    for (int s = 0; s < H.ns; ++s) {
+      const int64_t f0 = S.sn[s].first_col;
+      for (int64_t p = 0; p < S.sn[s].ncol; ++p) e_of_g[S.rs[S.rs_ptr[s] + lperm[f0 + p]]] = f0 + p;
+    }
+    int64_t nnz = 0;
+    if (l_col_ptr) l_col_ptr[0] = 0;
+    std::vector<std::pair<int64_t, int64_t>> col;  // (row e, panel element index)
+    for (int s = 0; s < H.ns; ++s) {
+      const int64_t f0 = S.sn[s].first_col, nc = S.sn[s].ncol, nr = H.nrow[s];
+      const int64_t* rs = S.rs.data() + S.rs_ptr[s];
+      for (int64_t p = 0; p < nc; ++p) {
+        col.clear();
+        col.push_back({f0 + p, -1});
+        int64_t i0 = kind[f0 + p] == 1 ? p + 2 : p + 1;
+        for (int64_t i = i0; i < nr; ++i) {
+          int64_t idx = H.poff[s] + i + p * nr;
+          if (is_zero_bytes(&panel[idx * es], es)) continue;
+          int64_t g = i < nc ? rs[lperm[f0 + i]] : rs[i];
+          col.push_back({e_of_g[g], idx});
+        }
+        std::sort(col.begin(), col.end());
+        for (auto& x : col) {
+          if (l_row_idx) l_row_idx[nnz] = x.first;
+          if (l_values) {
+            unsigned char* dst = (unsigned char*)l_values + nnz * es;
+            if (x.second < 0) {
+              std::memset(dst, 0, es);
+              if (es == 8) {
+                double one = 1.0;
+                std::memcpy(dst, &one, 8);
+              } else if (es == 16) {
+                double one = 1.0;
+                std::memcpy(dst, &one, 8);
+              } else {
+                float one = 1.0f;
+                std::memcpy(dst, &one, 4);
+              }
+            } else {
+              std::memcpy(dst, &panel[x.second * es], es);
+            }
+          }
+          ++nnz;
+        }
+        if (l_col_ptr) l_col_ptr[f0 + p + 1] = nnz;
+      }
+    }
+    if (nnz_out) *nnz_out = nnz;
+    if (d_diag) CK(cudaMemcpy(d_diag, F->d, n * es, cudaMemcpyDeviceToHost));
+    if (d_subdiag) CK(cudaMemcpy(d_subdiag, F->dsub, n * es, cudaMemcpyDeviceToHost));
+    if (two_by_two)
+      for (int e = 0; e < n; ++e) two_by_two[e] = kind[e] == 1;
+    if (perm)
+      for (int s = 0; s < H.ns; ++s) {
+        const int64_t f0 = S.sn[s].first_col;
+        for (int64_t p = 0; p < S.sn[s].ncol; ++p) perm[f0 + p] = S.perm[S.rs[S.rs_ptr[s] + lperm[f0 + p]]];
+      }
+    if (scale) CK(cudaMemcpy(scale, F->scale, n * 8, cudaMemcpyDeviceToHost));
+    return 0;
+  } catch (const RslabError& e) {
+    return fail(e);
+  } catch (const std::exception& e) {
+    return fail(RslabError(Status::InvalidInput, e.what()));
+  }
+}
+
+void rslab_free_factor(rslab_fac_handle* F) { delete F; }
+
+int rslab_device_count(int* count) {
+  cudaError_t e = cudaGetDeviceCount(count);
+  if (e != cudaSuccess) {
+    *count = 0;
+    g_last_error = cudaGetErrorString(e);
+    return (int)Status::CudaError;
+  }
+  return 0;
+}
+
+// m successive unit draws of the xorshift64* generator of the synthetic
+// workloads from internal state `state` (Rng::unit, src/matgen/mod.rs:62-81);
+// returns the advanced state.
+uint64_t rslab_rng_units(uint64_t state, int64_t m, double* out) {
+  uint64_t x = state;
+  for (int64_t i = 0; i < m; ++i) {
+    x ^= x >> 12;
+    x ^= x << 25;
+    x ^= x >> 27;
+    out[i] = (double)((x * 0x2545F4914F6CDD1Dull) >> 11) / 9007199254740992.0;
+  }
+  return x;
+}
+
+// AMD ordering of a full symmetric pattern, for golden-vector checks.
+int rslab_amd_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, int64_t* perm, double* stats7) {
+  try {
+    rslab::CscPattern p;
+    p.n = n;
+    p.col_ptr.assign(col_ptr, col_ptr + n + 1);
+    p.row_idx.assign(row_idx, row_idx + col_ptr[n]);
+    rslab::AmdStats st;
+    std::vector<int64_t> pr = rslab::amd_order(p, &st);
+    std::copy(pr.begin(), pr.end(), perm);
+    if (stats7) {
+      stats7[0] = st.ncmpa;
+      stats7[1] = st.n_dense;
+      stats7[2] = st.ndiv;
+      stats7[3] = st.nms_ldl;
+      stats7[4] = st.nms_lu;
+      stats7[5] = st.n_mass_elim;
+      stats7[6] = st.n_supervar_merge;
+    }
+    return 0;
+  } catch (const RslabError& e) {
+    return fail(e);
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,110 @@
+// Host-side data structures of the B200 LDL^T path: the lower-triangle CSC
+// input, the full symmetric pattern, the symbolic analysis (ordering,
+// elimination tree, supernodes, row structures, update lists, level sets) and
+// the error type that the C ABI turns into a status code.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace rslab {
+
+// Mirrors the reference error enum (src/error.rs:15-55).
+enum class Status : int {
+  Ok = 0,
+  NumericallyRankDeficient = 1,
+  InvalidInput = 2,
+  DimensionMismatch = 3,
+  CudaError = 4,
+  NotCertified = 5,
+};
+
+struct RslabError : std::runtime_error {
+  Status status;
+  RslabError(Status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+// Full symmetric sparsity pattern (both triangles, sorted rows), the input of
+// the ordering and the elimination tree (src/sparse/csc.rs:24-29).
+struct CscPattern {
+  int64_t n = 0;
+  std::vector<int64_t> col_ptr;
+  std::vector<int64_t> row_idx;
+};
+
+// Validation of a lower-triangle CSC (src/sparse/csc.rs:157-237).
+void validate_lower_csc(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, int64_t nnz);
+// Lower triangle -> full symmetric pattern (src/sparse/csc.rs:240-291).
+CscPattern symmetric_pattern(int64_t n, const int64_t* col_ptr, const int64_t* row_idx);
+// Relabel a full symmetric pattern by a new-to-old permutation
+// (src/ordering/amd.rs:21-81).
+CscPattern permute_pattern(const CscPattern& pat, const std::vector<int64_t>& perm);
+
+struct AmdStats {
+  uint32_t ncmpa = 0, n_dense = 0, n_mass_elim = 0, n_supervar_merge = 0;
+  double ndiv = 0, nms_lu = 0, nms_ldl = 0;
+};
+std::vector<int64_t> amd_order(const CscPattern& pat, AmdStats* stats = nullptr,
+                               double dense_alpha = 10.0, bool aggressive = true);
+
+// Elimination tree: parent[j] > j or -1 (src/ordering/elimination_tree.rs:28-64).
+std::vector<int64_t> etree_from_pattern(const CscPattern& pat);
+// Children-by-ascending-subtree-size postorder, optionally merge-biased
+// (src/ordering/postorder.rs:22-143).
+void etree_postorder(const std::vector<int64_t>& parent, const std::vector<uint8_t>* bias,
+                     std::vector<int64_t>& post, std::vector<int64_t>& post_inv);
+// Exact column counts of L (src/symbolic/column_counts.rs:97-183).
+std::vector<int64_t> column_counts(const CscPattern& pat, const std::vector<int64_t>& parent);
+
+enum class Ordering : int { Amd = 0, MetisND = 1, Natural = 2, Given = 3 };
+
+// Analysis knobs (the analyze-time half of SolverSettings,
+// src/numeric/multifrontal_ldlt.rs:302-420, defaults :583-614).
+struct AnalyzeOptions {
+  Ordering ordering = Ordering::Amd;
+  int64_t nemin = 16;
+  bool relax = true;
+  int64_t relax_max_width = 256;
+  int64_t relax_max_extra_rows = 64;
+  bool hybrid_liu = true;
+  const int64_t* given_perm = nullptr;  // used with Ordering::Given
+};
+
+struct Supernode {
+  int64_t first_col = 0;
+  int64_t ncol = 0;
+  int64_t nrow_est = 0;  // col_counts-based frontal height
+  std::vector<int64_t> children;
+};
+
+struct Symbolic {
+  int64_t n = 0;
+  int64_t nnz = 0;  // stored lower-triangle entries of the analysed pattern
+  std::vector<int64_t> perm, perm_inv;  // new-to-old / old-to-new
+  CscPattern permuted;                  // full symmetric pattern of P A P^T
+  std::vector<int64_t> parent;          // etree of P A P^T
+  std::vector<int64_t> col_counts;
+  std::vector<Supernode> sn;
+  int resolved_ordering = 0;
+  int renumbered = 0;  // merge-biased postorder applied
+  AmdStats amd;
+  // Left-looking structure (src/numeric/multifrontal_ldlt.rs:2121-2152,
+  // 3380-3401): per supernode its row structure, and for each supernode the
+  // ordered list of descendants whose off-diagonal rows land in its columns.
+  std::vector<int64_t> rs_ptr, rs;          // rs[rs_ptr[s]..rs_ptr[s+1])
+  std::vector<int64_t> upd_ptr, upd;        // updater k of s
+  std::vector<int64_t> upd_p0, upd_p1;      // landing range in k's off-diag rows
+  std::vector<int64_t> level;               // assembly-tree level (leaves = 0)
+  std::vector<std::vector<int64_t>> by_level;
+  int64_t factor_nnz_sym = 0;  // sum of column counts
+};
+
+Symbolic analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx,
+                 const AnalyzeOptions& opt);
+
+// Dense partial BK flop model per supernode: F(r,c) = sum_{m=r-c+1}^{r}(m^2-1).
+double supernode_flops(int64_t r, int64_t c);
+
+}  // namespace rslab

@@ -1,0 +1,165 @@
+"""Seeded synthetic matrices with the shapes of the LDL^T benchmark workloads.
+
+Mirrors the reference generators (src/matgen/mod.rs:62-95 `Rng`, xorshift64*;
+src/matgen/stencil.rs:47-134 `laplacian_weights` / `laplacian` / `helmholtz`)
+so the same seed gives the same matrix, and adds the workloads that the
+reference does not ship: the shifted 2D/3D Laplacians, the 3D Helmholtz shift
+and the 27-point stencil.  All matrices are returned as lower-triangle
+CscMatrix objects.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .solver import CscMatrix
+
+MASK = (1 << 64) - 1
+
+
+class Rng:
+    """xorshift64* (src/matgen/mod.rs:62-95)."""
+
+    def __init__(self, seed: int):
+        self.s = ((seed ^ 0x9E3779B97F4A7C15) | 1) & MASK
+
+    def next_u64(self) -> int:
+        x = self.s
+        x ^= x >> 12
+        x ^= (x << 25) & MASK
+        x ^= x >> 27
+        self.s = x
+        return (x * 0x2545F4914F6CDD1D) & MASK
+
+    def unit(self) -> float:
+        return (self.next_u64() >> 11) / float(1 << 53)
+
+    def range(self, lo: float, hi: float) -> float:
+        return lo + (hi - lo) * self.unit()
+
+    def units(self, m: int) -> np.ndarray:
+        """m successive unit() draws (same sequence), generated natively."""
+        import ctypes as C
+        from . import _native as N
+        out = np.empty(m, dtype=np.float64)
+        self.s = int(N.lib.rslab_rng_units(C.c_uint64(self.s), m, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+
+def _lower_csc(n, diag, rows, cols, w) -> CscMatrix:
+    r = np.concatenate([np.arange(n), rows])
+    c = np.concatenate([np.arange(n), cols])
+    v = np.concatenate([diag, w])
+    return CscMatrix.from_triplets(n, r, c, v)
+
+
+def laplacian_weights(dims):
+    """(diag, rows, cols, w) of the Dirichlet grid Laplacian (unit weights)."""
+    dims = list(dims)
+    nd = len(dims)
+    n = int(np.prod(dims))
+    stride = [1] * nd
+    for d in range(1, nd):
+        stride[d] = stride[d - 1] * dims[d - 1]
+    idx = np.arange(n)
+    diag = np.zeros(n)
+    rows, cols = [], []
+    for d in range(min(nd, 3)):
+        c = (idx // stride[d]) % dims[d]
+        inner = c + 1 < dims[d]
+        i = idx[inner]
+        j = i + stride[d]
+        diag[i] += 1.0
+        diag[j] += 1.0
+        rows.append(j)
+        cols.append(i)
+        diag[~inner] += 1.0          # + boundary ghost
+        diag[c == 0] += 1.0          # - boundary ghost
+    rows = np.concatenate(rows) if rows else np.zeros(0, np.int64)
+    cols = np.concatenate(cols) if cols else np.zeros(0, np.int64)
+    return diag, rows, cols, -np.ones(len(rows))
+
+
+def lambda_max(dims) -> float:
+    """Largest eigenvalue of -Delta_h with Dirichlet ends: sum_d 2 + 2 cos(pi/(N_d+1))."""
+    return float(sum(2.0 + 2.0 * math.cos(math.pi / (m + 1)) for m in dims))
+
+
+def shifted_laplacian(dims, sigma: float) -> CscMatrix:
+    """A = -Delta_h - sigma I (real symmetric, indefinite once sigma > lambda_min)."""
+    diag, rows, cols, w = laplacian_weights(dims)
+    n = int(np.prod(dims))
+    return _lower_csc(n, diag - sigma, rows, cols, w)
+
+
+def helmholtz(dims, k2: complex) -> CscMatrix:
+    """Complex-symmetric A = -Delta_h - k2 I (src/matgen/stencil.rs:114-134)."""
+    diag, rows, cols, w = laplacian_weights(dims)
+    n = int(np.prod(dims))
+    return _lower_csc(n, diag.astype(np.complex128) - k2, rows, cols, w.astype(np.complex128))
+
+
+def stencil27(side: int, rng: Rng):
+    """3D 27-point stencil K (off-diagonal -1, diagonal 26 + U[0, 0.1]) as
+    (diag, rows, cols, w) lower-triangle arrays."""
+    n = side ** 3
+    idx = np.arange(n)
+    x, y, z = idx % side, (idx // side) % side, idx // (side * side)
+    rows, cols = [], []
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                off = dx + dy * side + dz * side * side
+                if off <= 0:
+                    continue
+                ok = (x + dx >= 0) & (x + dx < side) & (y + dy >= 0) & (y + dy < side) & (z + dz >= 0) & (z + dz < side)
+                i = idx[ok]
+                rows.append(i + off)
+                cols.append(i)
+    rows = np.concatenate(rows)
+    cols = np.concatenate(cols)
+    diag = 26.0 + 0.1 * rng.units(n)
+    return diag, rows, cols, -np.ones(len(rows))
+
+
+def uniform_rhs(n: int, nrhs: int, seed: int, complex_: bool = False) -> np.ndarray:
+    """Row-major n x nrhs right-hand sides, entries U[-1, 1) from Rng(seed)
+    (real then imaginary draw per entry for complex)."""
+    rng = Rng(seed)
+    m = n * nrhs * (2 if complex_ else 1)
+    u = 2.0 * rng.units(m) - 1.0
+    if complex_:
+        u = u[0::2] + 1j * u[1::2]
+    b = u.reshape(n, nrhs)
+    return b[:, 0].copy() if nrhs == 1 else b
+
+
+# Workloads -------------------------------------------------------------------
+
+def c1_matrix(side: int = 128) -> CscMatrix:
+    """2D 5-point Dirichlet Laplacian minus 0.3 lambda_max (real, indefinite)."""
+    dims = (side, side)
+    return shifted_laplacian(dims, 0.3 * lambda_max(dims))
+
+
+def c2_matrix(side: int = 64) -> CscMatrix:
+    """3D 7-point Helmholtz -Delta_h - k2 (1 + 0.05 i) I, k2 = 0.2 lambda_max."""
+    dims = (side, side, side)
+    k2 = 0.2 * lambda_max(dims)
+    return helmholtz(dims, k2 * (1.0 + 0.05j))
+
+
+def c3_matrix(side: int) -> CscMatrix:
+    """3D 7-point Laplacian shifted by 0.1 lambda_max."""
+    dims = (side, side, side)
+    return shifted_laplacian(dims, 0.1 * lambda_max(dims))
+
+
+def negative_eigs_shifted_laplacian(dims, sigma: float) -> int:
+    """Exact count of eigenvalues of -Delta_h - sigma I below zero (separable spectrum)."""
+    ev = None
+    for m in dims:
+        e = 2.0 - 2.0 * np.cos(np.arange(1, m + 1) * np.pi / (m + 1))
+        ev = e if ev is None else (ev[:, None] + e[None, :]).ravel()
+    return int(np.sum(ev < sigma))

@@ -1,0 +1,592 @@
+"""Host-side mirror of RSLAB's symmetric direct-solver API over the C ABI.
+
+Same names, argument meaning and error behaviour as the reference:
+  CscMatrix            src/sparse/csc.rs:15 (lower triangle, sorted, duplicates summed)
+  SolverSettings       src/numeric/multifrontal_ldlt.rs:302 (defaults :583-614)
+  LdltSymbolic         src/numeric/sparse_solver.rs:457-711 (analyze once, factor many)
+  LdltSolver           src/numeric/sparse_solver.rs:40-375
+  MixedLdltSolver      src/numeric/mixed.rs:225-291, MixedInfo :81
+  Inertia              src/inertia.rs:11
+  RslabError family    src/error.rs:15-55
+All numeric work runs in librslab_b200.so on the GPU; this module only moves
+arrays across the boundary.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import NamedTuple, Optional
+
+import numpy as np
+
+from . import _native as N
+
+# ---------------------------------------------------------------------------
+# Errors (src/error.rs).
+# ---------------------------------------------------------------------------
+
+
+class RslabError(Exception):
+    """Base of the reference error enum."""
+
+
+class NumericallyRankDeficient(RslabError):
+    pass
+
+
+class InvalidInput(RslabError):
+    pass
+
+
+class DimensionMismatch(RslabError):
+    def __init__(self, expected: int, got: int):
+        super().__init__(f"dimension mismatch: expected {expected}, got {got}")
+        self.expected = expected
+        self.got = got
+
+
+class CudaError(RslabError):
+    pass
+
+
+def _check(rc: int) -> None:
+    if rc == 0:
+        return
+    msg = N.last_error()
+    if rc == 1:
+        raise NumericallyRankDeficient(msg)
+    if rc == 2:
+        raise InvalidInput(msg)
+    if rc == 3:
+        raise DimensionMismatch(-1, -1) from RslabError(msg)
+    if rc == 4:
+        raise CudaError(msg)
+    raise RslabError(f"status {rc}: {msg}")
+
+
+_DT = {np.dtype(np.float64): N.F64, np.dtype(np.complex128): N.C64,
+       np.dtype(np.float32): N.F32, np.dtype(np.complex64): N.C32}
+_NP = {v: k for k, v in _DT.items()}
+
+
+def _i64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+def _p64(a: np.ndarray):
+    return a.ctypes.data_as(N.i64p)
+
+
+# ---------------------------------------------------------------------------
+# CSC container.
+# ---------------------------------------------------------------------------
+
+
+class CscMatrix:
+    """Lower-triangle CSC, rows sorted within each column (csc.rs:15)."""
+
+    def __init__(self, n: int, col_ptr, row_idx, values):
+        self.n = int(n)
+        self.col_ptr = _i64(col_ptr)
+        self.row_idx = _i64(row_idx)
+        self.values = np.ascontiguousarray(values)
+        if self.values.dtype not in _DT:
+            self.values = self.values.astype(np.float64)
+
+    @classmethod
+    def from_triplets(cls, n: int, rows, cols, vals) -> "CscMatrix":
+        """Entries must be lower (row >= col); duplicates are summed (csc.rs:41-105)."""
+        rows = _i64(rows)
+        cols = _i64(cols)
+        vals = np.asarray(vals)
+        if not (len(rows) == len(cols) == len(vals)):
+            raise InvalidInput("triplet arrays must have equal length")
+        if len(cols) and (cols.min() < 0 or cols.max() >= n):
+            raise InvalidInput(f"column index out of bounds for n={n}")
+        if len(rows) and (rows.min() < 0 or rows.max() >= n):
+            raise InvalidInput(f"row index out of bounds for n={n}")
+        if np.any(rows < cols):
+            k = int(np.nonzero(rows < cols)[0][0])
+            raise InvalidInput(f"triplet {k} ({rows[k]}, {cols[k]}) is upper-triangle; "
+                               "CscMatrix stores only the lower triangle (row >= col)")
+        key = cols * max(n, 1) + rows
+        order = np.argsort(key, kind="stable")
+        key_s = key[order]
+        uniq, start = np.unique(key_s, return_index=True)
+        summed = np.add.reduceat(vals[order], start) if len(vals) else vals
+        ucols = uniq // max(n, 1)
+        urows = uniq % max(n, 1)
+        col_ptr = np.zeros(n + 1, dtype=np.int64)
+        np.add.at(col_ptr, ucols + 1, 1)
+        col_ptr = np.cumsum(col_ptr)
+        return cls(n, col_ptr, urows, summed)
+
+    @property
+    def nnz(self) -> int:
+        return int(self.row_idx.shape[0])
+
+    def validate(self) -> None:
+        n = self.n
+        if self.col_ptr.shape[0] != n + 1:
+            raise InvalidInput(f"col_ptr length {self.col_ptr.shape[0]} != n+1={n + 1}")
+        if self.row_idx.shape[0] != self.values.shape[0]:
+            raise InvalidInput("row_idx and values length mismatch")
+        if self.col_ptr[0] != 0:
+            raise InvalidInput(f"col_ptr[0] must be 0, got {self.col_ptr[0]}")
+        if self.col_ptr[n] != self.row_idx.shape[0]:
+            raise InvalidInput("col_ptr[n] != nnz")
+        if np.any(np.diff(self.col_ptr) < 0):
+            raise InvalidInput("col_ptr not monotonically non-decreasing")
+        cols = np.repeat(np.arange(n), np.diff(self.col_ptr))
+        r = self.row_idx
+        if len(r) and (r.min() < 0 or r.max() >= n):
+            raise InvalidInput("row index out of bounds")
+        if np.any(r < cols):
+            raise InvalidInput("row index in upper triangle; CscMatrix stores only the lower triangle")
+        same = cols[1:] == cols[:-1]
+        if np.any(r[1:][same] <= r[:-1][same]):
+            raise InvalidInput("row indices not sorted in column")
+
+    def astype(self, dtype) -> "CscMatrix":
+        return CscMatrix(self.n, self.col_ptr, self.row_idx, self.values.astype(dtype))
+
+    def to_scipy_full(self):
+        import scipy.sparse as sp
+        L = sp.csc_matrix((self.values, self.row_idx, self.col_ptr), shape=(self.n, self.n))
+        D = sp.diags(L.diagonal())
+        return (L + L.T - D).tocsr()
+
+    def symv(self, x: np.ndarray) -> np.ndarray:
+        """y = A x from the stored lower triangle (csc.rs:294-308), on the host."""
+        return self.to_scipy_full() @ x
+
+
+# ---------------------------------------------------------------------------
+# Settings / results.
+# ---------------------------------------------------------------------------
+
+
+class Ordering:
+    AMD = N.ORDER_AMD
+    METIS_ND = N.ORDER_METIS_ND
+    NATURAL = N.ORDER_NATURAL
+    GIVEN = N.ORDER_GIVEN
+
+
+@dataclass
+class ZeroPivotAction:
+    """`Fail` (exact) or `PerturbToEps(abs_floor)` (static pivoting)."""
+    kind: str = "fail"
+    abs_floor: float = 0.0
+
+    @staticmethod
+    def fail() -> "ZeroPivotAction":
+        return ZeroPivotAction("fail")
+
+    @staticmethod
+    def perturb_to_eps(abs_floor: float) -> "ZeroPivotAction":
+        return ZeroPivotAction("perturb", float(abs_floor))
+
+
+@dataclass
+class SolverSettings:
+    on_zero_pivot: ZeroPivotAction = field(default_factory=ZeroPivotAction.fail)
+    ordering: int = Ordering.AMD
+    nemin: int = 16
+    relax: Optional[tuple] = (256, 64)
+    reorder_hybrid_liu: bool = True
+    panel_nb: int = 64
+    scaling: str = "onepass"  # or "identity"
+    use_graph: bool = True
+    given_perm: Optional[np.ndarray] = None
+
+    @staticmethod
+    def exact() -> "SolverSettings":
+        return SolverSettings()
+
+    @staticmethod
+    def preconditioner(abs_floor: float) -> "SolverSettings":
+        return SolverSettings(on_zero_pivot=ZeroPivotAction.perturb_to_eps(abs_floor))
+
+    def with_pivot(self, p: ZeroPivotAction) -> "SolverSettings":
+        self.on_zero_pivot = p
+        return self
+
+    def with_ordering(self, o: int) -> "SolverSettings":
+        self.ordering = o
+        return self
+
+    def with_nemin(self, nemin: int) -> "SolverSettings":
+        self.nemin = nemin
+        return self
+
+    def with_relax(self, relax) -> "SolverSettings":
+        self.relax = relax
+        return self
+
+    def with_panel_nb(self, nb: int) -> "SolverSettings":
+        self.panel_nb = nb
+        return self
+
+    def with_scaling(self, s: str) -> "SolverSettings":
+        self.scaling = s
+        return self
+
+    def _analyze_c(self):
+        s = N.AnalyzeSettings()
+        N.lib.rslab_default_analyze_settings(C.byref(s))
+        s.ordering = self.ordering
+        s.nemin = self.nemin
+        if self.relax is None:
+            s.relax = 0
+        else:
+            s.relax = 1
+            s.relax_max_width, s.relax_max_extra_rows = self.relax
+        s.hybrid_liu = int(self.reorder_hybrid_liu)
+        s.panel_nb = self.panel_nb
+        keep = None
+        if self.ordering == Ordering.GIVEN:
+            keep = _i64(self.given_perm)
+            s.given_perm = _p64(keep)
+        return s, keep
+
+    def _factor_c(self, stream=None):
+        s = N.FactorSettings()
+        N.lib.rslab_default_factor_settings(C.byref(s))
+        if self.on_zero_pivot.kind == "perturb":
+            s.on_zero_pivot = N.PIVOT_PERTURB
+            s.abs_floor = self.on_zero_pivot.abs_floor
+        s.scaling = N.SCALING_ONEPASS if self.scaling == "onepass" else N.SCALING_IDENTITY
+        s.use_graph = int(self.use_graph)
+        s.stream = stream
+        return s
+
+
+class Inertia(NamedTuple):
+    positive: int
+    negative: int
+    zero: int
+
+
+@dataclass
+class MixedInfo:
+    ir_iters: int
+    gmres_iters: int
+    backward_error: float
+    certified: bool
+
+
+@dataclass
+class Diagnostics:
+    factor_ms: float
+    solve_ms: float
+    factor_nnz: int
+    flops: float
+    flops_proxy: float
+    n_supernodes: int
+    n_levels: int
+
+
+@dataclass
+class LdltFactors:
+    """The reference factor container (src/dense/ldlt_generic.rs:31-66)."""
+    n: int
+    l_col_ptr: np.ndarray
+    l_row_idx: np.ndarray
+    l_values: np.ndarray
+    d_diag: np.ndarray
+    d_subdiag: np.ndarray
+    two_by_two: np.ndarray
+    perm: np.ndarray
+    n_perturbed: int
+    inertia: Inertia
+    scale: np.ndarray
+
+
+# ---------------------------------------------------------------------------
+# Analysis / factor handles.
+# ---------------------------------------------------------------------------
+
+
+class LdltSymbolic:
+    """Phase-1 analysis of a pattern, reusable across value sets."""
+
+    def __init__(self, handle, n: int, nnz: int, settings: SolverSettings):
+        self._h = handle
+        self.n = n
+        self.nnz = nnz
+        self.settings = settings
+
+    @classmethod
+    def analyze(cls, a: CscMatrix) -> "LdltSymbolic":
+        return cls.analyze_with(a, SolverSettings())
+
+    @classmethod
+    def analyze_with(cls, a: CscMatrix, opts: SolverSettings) -> "LdltSymbolic":
+        a.validate()
+        s, keep = opts._analyze_c()
+        h = C.c_void_p()
+        _check(N.lib.rslab_analyze(a.n, _p64(a.col_ptr), _p64(a.row_idx), C.byref(s), C.byref(h)))
+        del keep
+        return cls(h, a.n, a.nnz, opts)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            N.lib.rslab_free_symbolic(h)
+            self._h = None
+
+    def info(self) -> N.SymbolicInfo:
+        inf = N.SymbolicInfo()
+        _check(N.lib.rslab_symbolic_info(self._h, C.byref(inf)))
+        return inf
+
+    def n_levels(self) -> int:
+        return int(self.info().nlevels)
+
+    def export(self) -> dict:
+        inf = self.info()
+        n, ns = int(inf.n), int(inf.nsuper)
+        out = {k: np.zeros(n, np.int64) for k in ("perm", "col_counts", "parent")}
+        for k in ("sn_first", "sn_ncol", "sn_nrow", "sn_level", "child_idx"):
+            out[k] = np.zeros(max(ns, 1), np.int64)
+        out["child_ptr"] = np.zeros(ns + 1, np.int64)
+        _check(N.lib.rslab_symbolic_export(
+            self._h, _p64(out["perm"]), _p64(out["sn_first"]), _p64(out["sn_ncol"]), _p64(out["sn_nrow"]),
+            _p64(out["sn_level"]), _p64(out["child_ptr"]), _p64(out["child_idx"]), _p64(out["col_counts"]),
+            _p64(out["parent"])))
+        for k in ("sn_first", "sn_ncol", "sn_nrow", "sn_level"):
+            out[k] = out[k][:ns]
+        out["child_idx"] = out["child_idx"][: int(out["child_ptr"][-1])]
+        return out
+
+    def _check_pattern(self, a: CscMatrix) -> None:
+        a.validate()
+        if a.n != self.n or a.nnz != self.nnz:
+            raise InvalidInput("factor_numeric: matrix does not match the analyzed pattern")
+
+    def factor(self, a: CscMatrix, opts: Optional[SolverSettings] = None, stream=None) -> "LdltSolver":
+        self._check_pattern(a)
+        opts = opts or self.settings
+        vals = np.ascontiguousarray(a.values)
+        if vals.dtype not in _DT:
+            raise InvalidInput(f"unsupported dtype {vals.dtype}")
+        fs = opts._factor_c(stream)
+        h = C.c_void_p()
+        rc = N.lib.rslab_factor(self._h, _DT[vals.dtype], vals.ctypes.data_as(C.c_void_p), 0, C.byref(fs),
+                                C.byref(h))
+        solver = LdltSolver(h, self, vals.dtype) if h else None
+        _check(rc)
+        return solver
+
+    def factor_device(self, dtype, values_ptr: int, opts: Optional[SolverSettings] = None, stream=None):
+        """Factor values already resident in device memory (a raw pointer)."""
+        opts = opts or self.settings
+        fs = opts._factor_c(stream)
+        h = C.c_void_p()
+        rc = N.lib.rslab_factor(self._h, _DT[np.dtype(dtype)], C.c_void_p(values_ptr), 1, C.byref(fs), C.byref(h))
+        solver = LdltSolver(h, self, np.dtype(dtype)) if h else None
+        _check(rc)
+        return solver
+
+
+class LdltSolver:
+    """A factored matrix; solves against many right-hand sides."""
+
+    def __init__(self, handle, sym: LdltSymbolic, dtype):
+        self._h = handle
+        self._sym = sym
+        self.dtype = np.dtype(dtype)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            N.lib.rslab_free_factor(h)
+            self._h = None
+
+    @classmethod
+    def factor(cls, a: CscMatrix) -> "LdltSolver":
+        return LdltSymbolic.analyze(a).factor(a, SolverSettings())
+
+    @classmethod
+    def factor_with(cls, a: CscMatrix, opts: SolverSettings) -> "LdltSolver":
+        return LdltSymbolic.analyze_with(a, opts).factor(a, opts)
+
+    @property
+    def n(self) -> int:
+        return self._sym.n
+
+    def refactor(self, a: CscMatrix) -> None:
+        self._sym._check_pattern(a)
+        vals = np.ascontiguousarray(a.values, dtype=self.dtype)
+        _check(N.lib.rslab_refactor(self._h, vals.ctypes.data_as(C.c_void_p), 0))
+
+    def _info(self) -> N.FactorInfo:
+        inf = N.FactorInfo()
+        _check(N.lib.rslab_factor_info(self._h, C.byref(inf)))
+        return inf
+
+    def inertia(self) -> Inertia:
+        i = self._info()
+        return Inertia(int(i.inertia_pos), int(i.inertia_neg), int(i.inertia_zero))
+
+    def n_perturbed(self) -> int:
+        return int(self._info().n_perturbed)
+
+    def factor_nnz(self) -> int:
+        nnz = C.c_int64()
+        _check(N.lib.rslab_export_factors(self._h, None, None, None, None, None, None, None, None, C.byref(nnz)))
+        return int(nnz.value)
+
+    def diagnostics(self) -> Diagnostics:
+        i = self._info()
+        si = self._sym.info()
+        return Diagnostics(i.factor_ms, i.solve_ms, -1, si.flops_model, si.flops_proxy, int(si.nsuper),
+                           int(si.nlevels))
+
+    def stream(self) -> int:
+        return int(N.lib.rslab_factor_stream(self._h) or 0)
+
+    def solve(self, rhs) -> np.ndarray:
+        b = np.ascontiguousarray(rhs, dtype=self.dtype)
+        if b.shape[0] != self.n:
+            raise DimensionMismatch(self.n, b.shape[0])
+        return self.solve_many(b, 1).reshape(self.n)
+
+    def solve_many(self, b, nrhs: int) -> np.ndarray:
+        b = np.ascontiguousarray(b, dtype=self.dtype).reshape(-1)
+        if nrhs <= 0 or b.shape[0] != self.n * nrhs:
+            raise DimensionMismatch(self.n * nrhs, b.shape[0])
+        x = np.empty_like(b)
+        _check(N.lib.rslab_solve(self._h, b.ctypes.data_as(C.c_void_p), nrhs, x.ctypes.data_as(C.c_void_p), 0))
+        return x.reshape(self.n, nrhs) if nrhs > 1 else x
+
+    def solve_device(self, b_ptr: int, nrhs: int, x_ptr: int) -> None:
+        _check(N.lib.rslab_solve(self._h, C.c_void_p(b_ptr), nrhs, C.c_void_p(x_ptr), 1))
+
+    def solve_refined(self, a: CscMatrix, rhs, max_iter: int) -> np.ndarray:
+        """Iterative refinement against the original A (sparse_solver.rs:335-375)."""
+        if a.n != self.n:
+            raise DimensionMismatch(self.n, a.n)
+        rhs = np.ascontiguousarray(rhs, dtype=self.dtype)
+        A = a.to_scipy_full()
+        x = self.solve(rhs)
+        best_x, best_res = x.copy(), np.inf
+        for it in range(max_iter + 1):
+            r = rhs - A @ x
+            res = float(np.max(np.abs(r))) if len(r) else 0.0
+            if res < best_res:
+                best_res, best_x = res, x.copy()
+            if res == 0.0 or it == max_iter:
+                break
+            x = x + self.solve(r)
+        return best_x
+
+    def export_factors(self) -> LdltFactors:
+        n = self.n
+        nnz = self.factor_nnz()
+        lcp = np.zeros(n + 1, np.int64)
+        lri = np.zeros(max(nnz, 1), np.int64)
+        lv = np.zeros(max(nnz, 1), self.dtype)
+        d = np.zeros(n, self.dtype)
+        ds = np.zeros(n, self.dtype)
+        two = np.zeros(n, np.uint8)
+        perm = np.zeros(n, np.int64)
+        scale = np.zeros(n, np.float64)
+        _check(N.lib.rslab_export_factors(
+            self._h, _p64(lcp), _p64(lri), lv.ctypes.data_as(C.c_void_p), d.ctypes.data_as(C.c_void_p),
+            ds.ctypes.data_as(C.c_void_p), two.ctypes.data_as(C.POINTER(C.c_uint8)), _p64(perm),
+            scale.ctypes.data_as(C.POINTER(C.c_double)), None))
+        return LdltFactors(n, lcp, lri[:nnz], lv[:nnz], d, ds, two.astype(bool), perm, self.n_perturbed(),
+                           self.inertia(), scale)
+
+
+CERT_FACTOR = 64.0
+EPS_F64 = 2.220446049250313e-16
+
+
+class MixedLdltSolver:
+    """Low-precision factor of cast(A), refined to double precision (mixed.rs:225)."""
+
+    def __init__(self, handle, sym: LdltSymbolic, dtype_hi):
+        self._h = handle
+        self._sym = sym
+        self.dtype = np.dtype(dtype_hi)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            N.lib.rslab_free_factor(h)
+            self._h = None
+
+    @classmethod
+    def factor(cls, a: CscMatrix) -> "MixedLdltSolver":
+        return cls.factor_with(a, SolverSettings())
+
+    @classmethod
+    def factor_with(cls, a: CscMatrix, opts: SolverSettings, sym: Optional[LdltSymbolic] = None,
+                    stream=None) -> "MixedLdltSolver":
+        sym = sym or LdltSymbolic.analyze_with(a, opts)
+        sym._check_pattern(a)
+        vals = np.ascontiguousarray(a.values)
+        if vals.dtype not in (np.dtype(np.float64), np.dtype(np.complex128)):
+            raise InvalidInput("mixed factor needs an f64 or c64 matrix")
+        fs = opts._factor_c(stream)
+        h = C.c_void_p()
+        rc = N.lib.rslab_mixed_factor(sym._h, _DT[vals.dtype], vals.ctypes.data_as(C.c_void_p), 0, C.byref(fs),
+                                      C.byref(h))
+        out = cls(h, sym, vals.dtype) if h else None
+        _check(rc)
+        return out
+
+    def refactor(self, a: CscMatrix) -> None:
+        self._sym._check_pattern(a)
+        vals = np.ascontiguousarray(a.values, dtype=self.dtype)
+        _check(N.lib.rslab_refactor(self._h, vals.ctypes.data_as(C.c_void_p), 0))
+
+    def solve(self, a: CscMatrix, b) -> tuple:
+        return self.solve_to(a, b, CERT_FACTOR * EPS_F64)
+
+    def solve_to(self, a: CscMatrix, b, target_backward_error: float) -> tuple:
+        if a.n != self._sym.n:
+            raise DimensionMismatch(self._sym.n, a.n)
+        b = np.ascontiguousarray(b, dtype=self.dtype)
+        nrhs = 1 if b.ndim == 1 else b.shape[1]
+        if b.shape[0] != self._sym.n:
+            raise DimensionMismatch(self._sym.n, b.shape[0])
+        x = np.empty_like(b)
+        info = N.MixedInfoC()
+        _check(N.lib.rslab_mixed_solve(self._h, b.ctypes.data_as(C.c_void_p), nrhs, float(target_backward_error),
+                                       x.ctypes.data_as(C.c_void_p), 0, C.byref(info)))
+        return x, MixedInfo(int(info.ir_iters), int(info.gmres_iters), float(info.backward_error),
+                            bool(info.certified))
+
+    def inertia(self) -> Inertia:
+        inf = N.FactorInfo()
+        _check(N.lib.rslab_factor_info(self._h, C.byref(inf)))
+        return Inertia(int(inf.inertia_pos), int(inf.inertia_neg), int(inf.inertia_zero))
+
+    def diagnostics(self) -> N.FactorInfo:
+        inf = N.FactorInfo()
+        _check(N.lib.rslab_factor_info(self._h, C.byref(inf)))
+        return inf
+
+    def stream(self) -> int:
+        return int(N.lib.rslab_factor_stream(self._h) or 0)
+
+
+def amd_order(n: int, col_ptr, row_idx) -> tuple:
+    """AMD on a full symmetric pattern; returns (perm, stats dict)."""
+    cp = _i64(col_ptr)
+    ri = _i64(row_idx)
+    perm = np.zeros(n, np.int64)
+    st = (C.c_double * 7)()
+    _check(N.lib.rslab_amd_order(n, _p64(cp), _p64(ri), _p64(perm), st))
+    keys = ("ncmpa", "n_dense", "ndiv", "nms_ldl", "nms_lu", "n_mass_elim", "n_supervar_merge")
+    return perm, {k: st[i] for i, k in enumerate(keys)}
+
+
+def device_count() -> int:
+    c = C.c_int(0)
+    N.lib.rslab_device_count(C.byref(c))
+    return int(c.value)
