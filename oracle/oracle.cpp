@@ -88,7 +88,15 @@ template <typename R> struct SC {
   static T zero() { return T(0, 0); }
   static T one() { return T(1, 0); }
   static T from_real(double r) { return T((R)r, 0); }
-  static double mag(T x) { return std::hypot((double)x.re, (double)x.im); }
+  // |z| = m sqrt(1 + (s/m)^2) with m = max(|re|,|im|), s = min: the scaled
+  // modulus (the reference's hypot, up to its last-ulp rounding).
+  static double mag(T x) {
+    double a = std::fabs((double)x.re), b = std::fabs((double)x.im);
+    double m = std::max(a, b), s = std::min(a, b);
+    if (m == 0.0) return 0.0;
+    double r = s / m;
+    return m * std::sqrt(1.0 + r * r);
+  }
   static double mag2(T x) { return (double)x.re * (double)x.re + (double)x.im * (double)x.im; }
   static double real(T x) { return x.re; }
   static T conj(T x) { return T(x.re, -x.im); }
@@ -464,13 +472,15 @@ int cdiv(Panel<T>& P, int64_t nrow, int64_t ncol, const FactorOpts& o, int64_t& 
           cc += 1;
         }
       }
+      // tmp = G L21^T (FMA accumulation in ascending q), then the lower part
+      // of tmp is subtracted from the panel.
 #pragma omp parallel for schedule(dynamic, 16) if (mt * cw * pw > 4000000)
       for (int64_t c2 = 0; c2 < cw; ++c2) {
         T* col = panel.data() + (ke + c2) * nrow + ke;
-        for (int64_t q = 0; q < pw; ++q) {
-          T rb = l21[c2 + q * mt];
-          const T* gq = g.data() + q * mt;
-          for (int64_t rr = c2; rr < mt; ++rr) col[rr] = col[rr] - gq[rr] * rb;
+        for (int64_t rr = c2; rr < mt; ++rr) {
+          T acc = S<T>::zero();
+          for (int64_t q = 0; q < pw; ++q) acc = S<T>::fmadd(g[rr + q * mt], l21[c2 + q * mt], acc);
+          col[rr] = col[rr] - acc;
         }
       }
     }
@@ -602,14 +612,15 @@ int factor_left_looking(const SymIn& sym, const Csc<T>& a, const FactorOpts& o, 
           ck += 1;
         }
       }
-      // U[r, c] = sum_q L_k[p0 + r, q] * G[c, q]; rows r >= c only.
+      // U[r, c] = sum_q L_k[p0 + r, q] * G[c, q] (FMA accumulation in
+      // ascending q, as the gemm crate's FMA kernels); rows r >= c only.
 #pragma omp parallel for schedule(dynamic, 8) if ((nok - p0) * npk * nck > 4000000)
       for (int64_t c = 0; c < npk; ++c) {
         int64_t tcol = ok[p0 + c] - first;
         T* dst = P.p.data() + tcol * nrow;
         for (int64_t r = p0 + c; r < nok; ++r) {
           T acc = S<T>::zero();
-          for (int64_t q = 0; q < nck; ++q) acc = acc + K.p[(nck + r) + q * nrk] * vd[c + q * npk];
+          for (int64_t q = 0; q < nck; ++q) acc = S<T>::fmadd(K.p[(nck + r) + q * nrk], vd[c + q * npk], acc);
           int64_t tr = gloc[ok[r]];
           dst[tr] = dst[tr] - acc;
         }

@@ -137,8 +137,12 @@ __device__ __forceinline__ T ld_G(const T* __restrict__ L, long long ld, int j, 
 }
 
 // A rows  : L_A + i (i < arows), column t at stride lda
-// G rows  : L_B + j (j < brows), column t at stride ldb; D indexed by t
-template <typename T>
+// B rows  : L_B + j (j < brows), column t at stride ldb
+// D (indexed by t) multiplies the B operand (D_ON_A = false: the cmod form
+// U = L_k G^T, G = L_k D) or the A operand (D_ON_A = true: the deferred
+// panel Schur tmp = (L21 D) L21^T).  Accumulation is one explicit FMA per t in
+// ascending t, the same order as the oracle.
+template <typename T, bool D_ON_A = false>
 __device__ void tile_product(T (&acc)[4][4], const T* __restrict__ LA, long long lda, int arows,
                              const T* __restrict__ LB, long long ldb, int brows, int kdim,
                              const T* __restrict__ d, const T* __restrict__ dsub,
@@ -157,8 +161,13 @@ __device__ void tile_product(T (&acc)[4][4], const T* __restrict__ LA, long long
       int t = e / TILE, r = e % TILE;
       T av = F::zero(), gv = F::zero();
       if (t < kt) {
-        if (r < arows) av = LA[r + (long long)(t0 + t) * lda];
-        if (r < brows) gv = ld_G(LB, ldb, r, t0 + t, d, dsub, kind);
+        if constexpr (D_ON_A) {
+          if (r < arows) av = ld_G(LA, lda, r, t0 + t, d, dsub, kind);
+          if (r < brows) gv = LB[r + (long long)(t0 + t) * ldb];
+        } else {
+          if (r < arows) av = LA[r + (long long)(t0 + t) * lda];
+          if (r < brows) gv = ld_G(LB, ldb, r, t0 + t, d, dsub, kind);
+        }
       }
       As[t * TILE + r] = av;
       Bs[t * TILE + r] = gv;
@@ -308,7 +317,7 @@ __global__ void __launch_bounds__(TPB) k_schur(FactorArgs fa, const int4* __rest
   const int rows_here = min(TILE, mt - r0), cols_here = min(TILE, cw - c0);
   const T* L21 = panel + ke + (long long)kb * nrow;
   T acc[4][4];
-  tile_product<T>(acc, L21 + r0, nrow, rows_here, L21 + c0, nrow, cols_here, pw,
+  tile_product<T, true>(acc, L21 + r0, nrow, rows_here, L21 + c0, nrow, cols_here, pw,
                   reinterpret_cast<const T*>(fa.d) + first + kb, reinterpret_cast<const T*>(fa.dsub) + first + kb,
                   fa.kind + first + kb, As, Bs);
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
@@ -465,7 +474,8 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
   const int npk = pw * (pw + 1) / 2;
   T* l1 = A + npk;
   T* l2 = l1 + pw;
-  double* red_v = reinterpret_cast<double*>(l2 + pw);
+  // 16-byte aligned reduction scratch after the (possibly 4-byte) field arrays.
+  double* red_v = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(l2 + pw) + 15) & ~uintptr_t(15));
   int* red_i = reinterpret_cast<int*>(red_v + 32);
   int* ctl = red_i + 32;  // [0] kstep [1] kp [2] nswaps [3] error
 

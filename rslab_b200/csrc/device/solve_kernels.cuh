@@ -176,19 +176,15 @@ __global__ void __launch_bounds__(SOLVE_NT) k_fwd_gather(SolveArgs a, const int2
 }
 
 // Forward diagonal solve of supernode s (one CTA): pivot-order unit-lower
-// substitution in 32-column blocks (left-looking inside the panel), then D^-1.
+// substitution in 32-column blocks (left-looking inside the panel).
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_fwd_diag(SolveArgs a, const int* __restrict__ tasks) {
   using F = Field<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* red = reinterpret_cast<T*>(smem_raw);
-  T* zb = red + (SOLVE_NT / 32) * 32 * RHS_MAX;  // 32 x RHS_MAX
   const int s = tasks[blockIdx.x];
   const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
   const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
-  const T* d = reinterpret_cast<const T*>(a.d) + first;
-  const T* ds = reinterpret_cast<const T*>(a.dsub) + first;
-  const unsigned char* kind = a.kind + first;
   const int* lp = a.lperm + first;
   const T* Y = reinterpret_cast<const T*>(a.Yg) + a.c0;
   T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
@@ -233,23 +229,32 @@ __global__ void __launch_bounds__(SOLVE_NT) k_fwd_diag(SolveArgs a, const int* _
     }
     __syncthreads();
   }
-  // D^-1 (1x1 and 2x2 blocks).
-  for (int e = threadIdx.x; e < ncol * a.nrhs; e += SOLVE_NT) {
-    int p = e / a.nrhs, c = e % a.nrhs;
-    unsigned char kd = kind[p];
-    if (kd == 0) {
-      T* z = Z + (long long)p * a.ld + c;
-      *z = F::mul(*z, F::recip(d[p]));
-    } else if (kd == 1) {
-      T d11 = d[p], d21 = ds[p], d22 = d[p + 1];
-      T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
-      T di = F::recip(det);
-      T* z0 = Z + (long long)p * a.ld + c;
-      T* z1 = Z + (long long)(p + 1) * a.ld + c;
-      T a0 = *z0, a1 = *z1;
-      *z0 = F::mul(F::sub(F::mul(d22, a0), F::mul(d21, a1)), di);
-      *z1 = F::mul(F::sub(F::mul(d11, a1), F::mul(d21, a0)), di);
-    }
+}
+
+// D^-1 on the e-indexed forward solution, after the whole forward sweep
+// (ancestors' gathers need z, not D^-1 z).  1x1 and 2x2 blocks.
+template <typename T>
+__global__ void k_dsolve(int n, SolveArgs a) {
+  using F = Field<T>;
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * a.nrhs) return;
+  const int e = (int)(idx / a.nrhs), c = (int)(idx % a.nrhs);
+  const T* d = reinterpret_cast<const T*>(a.d);
+  const T* ds = reinterpret_cast<const T*>(a.dsub);
+  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0;
+  const unsigned char kd = a.kind[e];
+  if (kd == 0) {
+    T* z = Z + (long long)e * a.ld + c;
+    *z = F::mul(*z, F::recip(d[e]));
+  } else if (kd == 1) {
+    T d11 = d[e], d21 = ds[e], d22 = d[e + 1];
+    T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
+    T di = F::recip(det);
+    T* z0 = Z + (long long)e * a.ld + c;
+    T* z1 = Z + (long long)(e + 1) * a.ld + c;
+    T a0 = *z0, a1 = *z1;
+    *z0 = F::mul(F::sub(F::mul(d22, a0), F::mul(d21, a1)), di);
+    *z1 = F::mul(F::sub(F::mul(d11, a1), F::mul(d21, a0)), di);
   }
 }
 
@@ -261,7 +266,6 @@ __global__ void __launch_bounds__(SOLVE_NT) k_bwd(SolveArgs a, const int* __rest
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* red = reinterpret_cast<T*>(smem_raw);
   T* vb = red + (SOLVE_NT / 32) * 32 * RHS_MAX;  // [32 rows of the block] x RHS_MAX
-  int* rsx = reinterpret_cast<int*>(vb + 32 * RHS_MAX);
   const int s = tasks[blockIdx.x];
   const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
   const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
@@ -272,7 +276,6 @@ __global__ void __launch_bounds__(SOLVE_NT) k_bwd(SolveArgs a, const int* __rest
   T* Xw = reinterpret_cast<T*>(a.Xg) + a.c0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NW = SOLVE_NT / 32;
-  (void)rsx;
   const int nblk = (ncol + SB - 1) / SB;
   for (int b = nblk - 1; b >= 0; --b) {
     const int j0 = b * SB, nb = min(SB, ncol - j0), j1 = j0 + nb;

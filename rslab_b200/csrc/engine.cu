@@ -309,7 +309,7 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
 size_t smem_cmod(size_t es) { return (size_t)TILE * TILE * es + 2 * 16 * TILE * es + 3 * TILE * 4 + 64; }
 size_t smem_schur(size_t es) { return 2 * 16 * TILE * es; }
 size_t smem_getf2(size_t es, int nb) {
-  size_t a = (size_t)nb * (nb + 1) / 2 * es + 2 * nb * es + 32 * 8 + 32 * 4 + 16 * 4;
+  size_t a = (size_t)nb * (nb + 1) / 2 * es + 2 * nb * es + 16 + 32 * 8 + 32 * 4 + 16 * 4;
   size_t b = (size_t)DEEP_R * nb * es;
   return std::max(a, b) + 64;
 }
@@ -582,6 +582,7 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs) {
       else
         k_fwd_diag<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
     }
+    k_dsolve<T><<<grid1((long long)n * nr), 256, 0, st>>>(n, sa);
     for (const Launch& L : H.bwdplan) k_bwd<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
   }
   k_perm_out<T><<<grid1((long long)n * nrhs), 256, 0, st>>>(n, nrhs, H.d_perm, F.scale, (const T*)F.Xg, x);
