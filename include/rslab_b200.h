@@ -142,6 +142,11 @@ int rslab_refactor(rslab_fac_handle* fac, const void* values, int values_on_devi
 int rslab_solve(rslab_fac_handle* fac, const void* b, int64_t nrhs, void* x, int on_device);
 int rslab_factor_info(const rslab_fac_handle* fac, rslab_factor_info_t* info);
 void* rslab_factor_stream(const rslab_fac_handle* fac);
+/* Eager refactor with per-launch CUDA events: device ms, launches and
+ * algorithmic flops per kernel class ([0] equilibration + assembly, [1] cmod,
+ * [2] BK panel getf2, [3] deep-row replay, [4] in-panel Schur, [5] total).
+ * A measurement aid with no reference counterpart. */
+int rslab_factor_profile(rslab_fac_handle* fac, double* kind_ms, int64_t* kind_launches, double* kind_flops);
 /* Reference LdltFactors layout; pass NULL arrays to query *nnz_out first. */
 int rslab_export_factors(const rslab_fac_handle* fac, int64_t* l_col_ptr, int64_t* l_row_idx, void* l_values,
                          void* d_diag, void* d_subdiag, uint8_t* two_by_two, int64_t* perm, double* scale,

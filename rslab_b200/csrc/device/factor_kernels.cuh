@@ -201,11 +201,15 @@ __device__ __forceinline__ int lower_bound_i(const int* __restrict__ a, int lo, 
 }
 
 // ---------------------------------------------------------------------------
-// cmod: task = (s, r0, c0); tile rows [r0, r0+64) x cols [c0, c0+64) of s's
-// panel, pulling every descendant update in update-list order.
+// cmod: task = (s, (r0/64) << 16 | (c0/64), pair_begin, pair_end): tile rows
+// [r0, r0+64) x cols [c0, c0+64) of s's panel.  The pairs, precomputed at
+// analysis, list in update-list order every descendant k whose update lands
+// in the tile: (k, a, q0, nr << 16 | nc) = k's off-diagonal rows [a, a+nr)
+// times its rows [q0, q0+nc) (the tile's columns).  No searches at run time.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(TPB) k_cmod(FactorArgs fa, const int4* __restrict__ tasks) {
+__global__ void __launch_bounds__(TPB) k_cmod(FactorArgs fa, const int4* __restrict__ tasks,
+                                              const int4* __restrict__ pairs) {
   using F = Field<T>;
   if (fa.status[0] != 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -215,16 +219,14 @@ __global__ void __launch_bounds__(TPB) k_cmod(FactorArgs fa, const int4* __restr
   int* rs_tile = reinterpret_cast<int*>(Bs + KChunk<T>::v * TILE);  // 64
   int* rowmap = rs_tile + TILE;                                       // 64
   int* colmap = rowmap + TILE;                                        // 64
-  int* meta = colmap + TILE;                                          // 8
 
   const int4 tk = tasks[blockIdx.x];
-  const int s = tk.x, r0 = tk.y, c0 = tk.z;
+  const int s = tk.x, r0 = (tk.y >> 16) * TILE, c0 = (tk.y & 0xffff) * TILE;
   const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
   const int rows_here = min(TILE, nrow - r0), cols_here = min(TILE, ncol - c0);
   T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
   const int* rss = fa.rs + fa.sn_rsoff[s];
   const int tid = threadIdx.x;
-  // Load the tile (column-major in smem).
   for (int e = tid; e < TILE * TILE; e += TPB) {
     int c = e / TILE, r = e % TILE;
     T v = F::zero();
@@ -233,55 +235,33 @@ __global__ void __launch_bounds__(TPB) k_cmod(FactorArgs fa, const int4* __restr
   }
   if (tid < TILE) rs_tile[tid] = tid < rows_here ? rss[r0 + tid] : INT_MAX;
   __syncthreads();
-  const int g_row_lo = rs_tile[0], g_row_hi = rs_tile[rows_here - 1];
-  const int g_col_lo = first + c0, g_col_hi = first + c0 + cols_here;  // [lo, hi)
   const T* dall = reinterpret_cast<const T*>(fa.d);
   const T* dsall = reinterpret_cast<const T*>(fa.dsub);
   const T* pall = reinterpret_cast<const T*>(fa.panel);
-  for (int u = fa.upd_ptr[s]; u < fa.upd_ptr[s + 1]; ++u) {
-    const int k = fa.upd_k[u];
+  for (int u = tk.z; u < tk.w; ++u) {
+    const int4 pr = pairs[u];
+    const int k = pr.x, a = pr.y, q0 = pr.z, nr = pr.w >> 16, nc = pr.w & 0xffff;
     const int nck = fa.sn_ncol[k], nrk = fa.sn_nrow[k], fk = fa.sn_first[k];
-    const int nok = nrk - nck;
     const int* ok = fa.rs + fa.sn_rsoff[k] + nck;
-    if (tid == 0) {
-      int p0 = fa.upd_p0[u], p1 = fa.upd_p1[u];
-      int q0 = lower_bound_i(ok, p0, p1, g_col_lo);
-      int q1 = lower_bound_i(ok, q0, p1, g_col_hi);
-      int a = lower_bound_i(ok, q0, nok, g_row_lo);
-      int b = lower_bound_i(ok, a, nok, g_row_hi + 1);
-      meta[0] = q0;
-      meta[1] = q1;
-      meta[2] = a;
-      meta[3] = b;
-    }
-    __syncthreads();
-    const int q0 = meta[0], q1 = meta[1], a = meta[2], b = meta[3];
-    if (q1 <= q0 || b <= a) {
-      __syncthreads();
-      continue;
-    }
-    // Row map: position of ok[a + i] inside this tile's row slice.
+    // Row map: position of ok[a + i] inside this tile's row slice (smem search).
     if (tid < TILE) {
-      if (tid < b - a) {
-        int g = ok[a + tid];
-        rowmap[tid] = lower_bound_i(rs_tile, 0, rows_here, g);
-      }
-      if (tid < q1 - q0) colmap[tid] = ok[q0 + tid] - first - c0;
+      if (tid < nr) rowmap[tid] = lower_bound_i(rs_tile, 0, rows_here, ok[a + tid]);
+      if (tid < nc) colmap[tid] = ok[q0 + tid] - first - c0;
     }
     const T* Lk = pall + fa.sn_poff[k];
     T acc[4][4];
-    tile_product<T>(acc, Lk + nck + a, nrk, b - a, Lk + nck + q0, nrk, q1 - q0, nck, dall + fk, dsall + fk,
-                    fa.kind + fk, As, Bs);
+    tile_product<T>(acc, Lk + nck + a, nrk, nr, Lk + nck + q0, nrk, nc, nck, dall + fk, dsall + fk, fa.kind + fk,
+                    As, Bs);
     // Scatter-subtract (rows r >= column c in k's ordering only).
     const int tx = tid & 15, ty = tid >> 4;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       int ri = ty + 16 * i;
-      if (ri >= b - a) continue;
+      if (ri >= nr) continue;
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         int cj = tx + 16 * j;
-        if (cj >= q1 - q0) continue;
+        if (cj >= nc) continue;
         if (a + ri < q0 + cj) continue;
         int e = colmap[cj] * TILE + rowmap[ri];
         acc_s[e] = F::sub(acc_s[e], acc[i][j]);

@@ -43,6 +43,8 @@ struct SolveArgs {
   void* Yg;   // n x ld, g order
   void* Ze;   // n x ld, e order
   void* Xg;   // n x ld, g order
+  void* U;    // sum_s (nrow_s - ncol_s) x ld: U_s = L21_s z_s
+  const long long* uoff;  // row offset of U_s
   int ld;     // row stride (total rhs count)
   int c0;     // first rhs column of this pass
   int nrhs;   // rhs columns in this pass (<= RHS_MAX)
@@ -109,74 +111,13 @@ __device__ __forceinline__ void reduce_warps(T (&acc)[RHS_MAX], T* red, int nrhs
   __syncthreads();
 }
 
-// Forward gather: task = (s, c0) — columns [c0, c0+32) of s receive
-// sum_k L_k(rows landing there) * z_k, in update-list order.
-template <typename T>
-__global__ void __launch_bounds__(SOLVE_NT) k_fwd_gather(SolveArgs a, const int2* __restrict__ tasks) {
-  using F = Field<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* red = reinterpret_cast<T*>(smem_raw);                         // NW*32*RHS_MAX
-  T* tsum = red + (SOLVE_NT / 32) * 32 * RHS_MAX;                   // 32 x RHS_MAX
-  int* meta = reinterpret_cast<int*>(tsum + 32 * RHS_MAX);
-  const int2 tk = tasks[blockIdx.x];
-  const int s = tk.x, cb = tk.y;
-  const int first = a.sn_first[s], ncol = a.sn_ncol[s];
-  const int cols_here = min(SB, ncol - cb);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const T* P = reinterpret_cast<const T*>(a.panel);
-  const T* Z = reinterpret_cast<const T*>(a.Ze) + a.c0;
-  T* Y = reinterpret_cast<T*>(a.Yg) + a.c0;
-  for (int e = threadIdx.x; e < 32 * RHS_MAX; e += SOLVE_NT) tsum[e] = F::zero();
-  __syncthreads();
-  const int g_lo = first + cb, g_hi = first + cb + cols_here;
-  for (int u = a.upd_ptr[s]; u < a.upd_ptr[s + 1]; ++u) {
-    const int k = a.upd_k[u];
-    const int nck = a.sn_ncol[k], nrk = a.sn_nrow[k], fk = a.sn_first[k];
-    const int* ok = a.rs + a.sn_rsoff[k] + nck;
-    if (threadIdx.x == 0) {
-      int p0 = a.upd_p0[u], p1 = a.upd_p1[u];
-      int lo = p0, hi = p1;
-      while (lo < hi) {
-        int m = (lo + hi) >> 1;
-        if (ok[m] < g_lo) lo = m + 1; else hi = m;
-      }
-      int q0 = lo;
-      hi = p1;
-      while (lo < hi) {
-        int m = (lo + hi) >> 1;
-        if (ok[m] < g_hi) lo = m + 1; else hi = m;
-      }
-      meta[0] = q0;
-      meta[1] = lo;
-    }
-    __syncthreads();
-    const int q0 = meta[0], q1 = meta[1];
-    if (q1 > q0) {
-      const int nr = q1 - q0;  // <= 32
-      T acc[RHS_MAX];
-#pragma unroll
-      for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
-      const T* Lk = P + a.sn_poff[k] + nck + q0 + lane;
-      lane_row_dot<T>(acc, Lk, nrk, 0, nck, Z + (long long)fk * a.ld, a.ld, a.nrhs, lane < nr);
-      reduce_warps<T>(acc, red, a.nrhs);
-      if (warp == 0 && lane < nr) {
-        int tc = ok[q0 + lane] - g_lo;
-#pragma unroll
-        for (int c = 0; c < RHS_MAX; ++c)
-          if (c < a.nrhs) tsum[tc * RHS_MAX + c] = F::add(tsum[tc * RHS_MAX + c], acc[c]);
-      }
-    }
-    __syncthreads();
-  }
-  for (int e = threadIdx.x; e < cols_here * a.nrhs; e += SOLVE_NT) {
-    int c = e / a.nrhs, r = e % a.nrhs;
-    T* y = Y + (long long)(g_lo + c) * a.ld + r;
-    *y = F::sub(*y, tsum[c * RHS_MAX + r]);
-  }
-}
-
-// Forward diagonal solve of supernode s (one CTA): pivot-order unit-lower
-// substitution in 32-column blocks (left-looking inside the panel).
+// Forward step of supernode s (one CTA):
+//  1. pull the descendants' pushes: y[g] -= U_k[r] for every updater k (in
+//     update-list order) and its off-diagonal rows r landing in s's columns;
+//  2. pivot-order unit-lower substitution of the diagonal block in 32-column
+//     blocks (left-looking inside the panel) -> z_s (e order);
+//  3. push: U_s = L21_s z_s for the off-diagonal rows (lanes over rows,
+//     coalesced panel reads), consumed by the ancestors' step 1.
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_fwd_diag(SolveArgs a, const int* __restrict__ tasks) {
   using F = Field<T>;
@@ -186,9 +127,24 @@ __global__ void __launch_bounds__(SOLVE_NT) k_fwd_diag(SolveArgs a, const int* _
   const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
   const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
   const int* lp = a.lperm + first;
-  const T* Y = reinterpret_cast<const T*>(a.Yg) + a.c0;
+  T* Y = reinterpret_cast<T*>(a.Yg) + a.c0;
   T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
+  T* Uall = reinterpret_cast<T*>(a.U) + a.c0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // 1. gather the pushes of the updaters (distinct rows within one updater).
+  for (int u = a.upd_ptr[s]; u < a.upd_ptr[s + 1]; ++u) {
+    const int k = a.upd_k[u], p0 = a.upd_p0[u], p1 = a.upd_p1[u];
+    const int* ok = a.rs + a.sn_rsoff[k] + a.sn_ncol[k];
+    const T* Uk = Uall + a.uoff[k] * a.ld;
+    const int cnt = (p1 - p0) * a.nrhs;
+    for (int e = threadIdx.x; e < cnt; e += SOLVE_NT) {
+      const int r = p0 + e / a.nrhs, c = e % a.nrhs;
+      T* y = Y + (long long)ok[r] * a.ld + c;
+      *y = F::sub(*y, Uk[(long long)r * a.ld + c]);
+    }
+    __syncthreads();
+  }
+  // 2. diagonal block.
   for (int j0 = 0; j0 < ncol; j0 += SB) {
     const int nb = min(SB, ncol - j0);
     T acc[RHS_MAX];
@@ -197,14 +153,12 @@ __global__ void __launch_bounds__(SOLVE_NT) k_fwd_diag(SolveArgs a, const int* _
     lane_row_dot<T>(acc, L + j0 + lane, nrow, 0, j0, Z, a.ld, a.nrhs, lane < nb);
     reduce_warps<T>(acc, red, a.nrhs);
     if (warp == 0) {
-      // y in pivot order minus the contribution of the solved columns.
       T z[RHS_MAX];
       const int p = j0 + lane;
       const bool ok = lane < nb;
       const T* yrow = Y + (long long)(first + (ok ? lp[p] : 0)) * a.ld;
 #pragma unroll
       for (int c = 0; c < RHS_MAX; ++c) z[c] = (ok && c < a.nrhs) ? F::sub(yrow[c], acc[c]) : F::zero();
-      // In-block substitution: z[p] -= L[p, q] z[q], q < p (skip the 2x2 coupling).
       for (int q = 0; q < nb; ++q) {
         const int qq = j0 + q;
         T l = F::zero();
@@ -228,6 +182,27 @@ __global__ void __launch_bounds__(SOLVE_NT) k_fwd_diag(SolveArgs a, const int* _
           if (c < a.nrhs) Z[(long long)p * a.ld + c] = z[c];
     }
     __syncthreads();
+  }
+  // 3. push U_s = L21 z_s: warps take 32-row groups, lanes the rows.
+  T* Us = Uall + a.uoff[s] * a.ld;
+  constexpr int NW = SOLVE_NT / 32;
+  for (int r0 = ncol + warp * 32; r0 < nrow; r0 += NW * 32) {
+    const int r = r0 + lane;
+    const bool ok = r < nrow;
+    T acc[RHS_MAX];
+#pragma unroll
+    for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
+    for (int q = 0; q < ncol; ++q) {
+      T l = ok ? L[r + (long long)q * nrow] : F::zero();
+      const T* zq = Z + (long long)q * a.ld;
+#pragma unroll
+      for (int c = 0; c < RHS_MAX; ++c)
+        if (c < a.nrhs) acc[c] = F::fma_(l, zq[c], acc[c]);
+    }
+    if (ok)
+#pragma unroll
+      for (int c = 0; c < RHS_MAX; ++c)
+        if (c < a.nrhs) Us[(long long)(r - ncol) * a.ld + c] = acc[c];
   }
 }
 

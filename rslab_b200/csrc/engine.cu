@@ -65,7 +65,7 @@ size_t elem_size(int dtype) {
   throw RslabError(Status::InvalidInput, "unknown dtype");
 }
 
-enum LaunchKind { L_CMOD, L_GETF2, L_DEEP, L_SCHUR, L_FWD_GATHER, L_FWD_DIAG, L_BWD };
+enum LaunchKind { L_CMOD, L_GETF2, L_DEEP, L_SCHUR, L_FWD_DIAG, L_BWD };
 struct Launch {
   int kind;
   long long task_off;  // into the int4 / int2 / int task arrays
@@ -94,12 +94,17 @@ struct rslab_sym_handle {
   std::vector<int> sp_ci;
   // plan
   std::vector<int4> t4;
-  std::vector<int2> t2;
+  std::vector<int4> cpairs;   // cmod (k, a, q0, nr << 16 | nc) per tile, in update order
   std::vector<int> t1;
+  std::vector<long long> uoff;  // forward-push row offsets (nrow - ncol per supernode)
+  long long urows = 0;
   std::vector<Launch> fplan, fwdplan, bwdplan;
   int max_getf2_tasks = 0;
   int max_nb = 64;
   double flops_model = 0, flops_proxy = 0;
+  // algorithmic real-field flops (multiply + add = 2) per launch kind:
+  // [0] assembly, [1] cmod, [2] getf2, [3] deep-row replay, [4] panel Schur
+  double kind_flops[6] = {0, 0, 0, 0, 0, 0};
   // device mirrors (uploaded lazily on first factor)
   int device = -1;
   std::vector<std::unique_ptr<void, DFree>> bufs;
@@ -111,8 +116,9 @@ struct rslab_sym_handle {
   long long *d_sp_rp = nullptr, *d_sp_vmap = nullptr;
   int* d_sp_ci = nullptr;
   int4* d_t4 = nullptr;
-  int2* d_t2 = nullptr;
+  int4* d_cpairs = nullptr;
   int* d_t1 = nullptr;
+  long long* d_uoff = nullptr;
   std::mutex mu;
   rslab_analyze_settings settings{};
 
@@ -159,8 +165,9 @@ struct rslab_sym_handle {
     d_sp_ci = up(sp_ci, st);
     d_sp_vmap = up(sp_vmap, st);
     d_t4 = up(t4, st);
-    d_t2 = up(t2, st);
+    d_cpairs = up(cpairs, st);
     d_t1 = up(t1, st);
+    d_uoff = up(uoff, st);
     CK(cudaStreamSynchronize(st));
     device = dev;
   }
@@ -187,6 +194,12 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
     H.flops_proxy += (double)nr * nr * S.sn[s].ncol;
   }
   H.panel_elems = acc;
+  H.uoff.assign(ns, 0);
+  H.urows = 0;
+  for (int s = 0; s < ns; ++s) {
+    H.uoff[s] = H.urows;
+    H.urows += H.nrow[s] - S.sn[s].ncol;
+  }
   // Assembly targets: user (i, j) -> permuted lower (r, c) -> panel slot.
   std::vector<int> col2sn(n);
   for (int s = 0; s < ns; ++s)
@@ -236,14 +249,64 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
   H.max_nb = nb_big;
   auto nb_of = [&](int s) { return S.sn[s].ncol >= 512 ? nb_big : nb_small; };
   for (const auto& lvl : S.by_level) {
-    // cmod tiles (lower part of every panel that has updaters).
+    // cmod tiles of every panel that has updaters, each with its precomputed
+    // list of (updater, row run, column run) pairs in update-list order.
     {
       Launch L{L_CMOD, (long long)H.t4.size(), 0, 0};
       for (int64_t s : lvl) {
         if (S.upd_ptr[s + 1] == S.upd_ptr[s]) continue;
-        int nc = (int)S.sn[s].ncol, nr = H.nrow[s];
-        for (int c0 = 0; c0 < nc; c0 += TILE)
-          for (int r0 = c0; r0 < nr; r0 += TILE) H.t4.push_back(make_int4((int)s, r0, c0, 0));
+        const int nc = (int)S.sn[s].ncol, nr = H.nrow[s];
+        const int64_t first = S.sn[s].first_col;
+        const int64_t* rss = S.rs.data() + S.rs_ptr[s];
+        const int ntc = (nc + TILE - 1) / TILE, ntr = (nr + TILE - 1) / TILE;
+        std::vector<std::vector<int4>> tp((size_t)ntc * ntr);
+        for (int64_t u = S.upd_ptr[s]; u < S.upd_ptr[s + 1]; ++u) {
+          const int64_t k = S.upd[u], p0 = S.upd_p0[u], p1 = S.upd_p1[u];
+          const int64_t nck = S.sn[k].ncol;
+          const int64_t* ok = S.rs.data() + S.rs_ptr[k] + nck;
+          const int64_t nok = S.rs_ptr[k + 1] - S.rs_ptr[k] - nck;
+          // local row position of each of k's rows >= p0 in s (merge walk)
+          std::vector<int> rel(nok - p0);
+          int64_t pos = std::lower_bound(rss, rss + nr, ok[p0]) - rss;
+          for (int64_t r = p0; r < nok; ++r) {
+            while (rss[pos] < ok[r]) ++pos;
+            rel[r - p0] = (int)pos;
+          }
+          int64_t qa = p0;
+          while (qa < p1) {
+            const int64_t ct = (ok[qa] - first) / TILE;
+            int64_t qb = qa;
+            while (qb < p1 && (ok[qb] - first) / TILE == ct) ++qb;
+            int64_t ra = qa;
+            while (ra < nok) {
+              const int rt = rel[ra - p0] / TILE;
+              int64_t rb = ra;
+              while (rb < nok && rel[rb - p0] / TILE == rt) ++rb;
+              tp[(size_t)ct * ntr + rt].push_back(
+                  make_int4((int)k, (int)ra, (int)qa, (int)(((rb - ra) << 16) | (qb - qa))));
+              ra = rb;
+            }
+            qa = qb;
+          }
+        }
+        for (int ct = 0; ct < ntc; ++ct)
+          for (int rt = ct; rt < ntr; ++rt) {
+            const auto& v = tp[(size_t)ct * ntr + rt];
+            if (v.empty()) continue;
+            for (const int4& pq : v) {
+              const double nrr = pq.w >> 16, ncc = pq.w & 0xffff;
+              // (r, c) pairs with r >= c in k's ordering, times nck multiply-adds
+              double cnt = 0;
+              for (int cj = 0; cj < (int)ncc; ++cj) {
+                const int lo = std::max(pq.y, pq.z + cj);
+                cnt += std::max(0, pq.y + (int)nrr - lo);
+              }
+              H.kind_flops[1] += 2.0 * cnt * (double)S.sn[pq.x].ncol;
+            }
+            const int pb = (int)H.cpairs.size();
+            H.cpairs.insert(H.cpairs.end(), v.begin(), v.end());
+            H.t4.push_back(make_int4((int)s, (rt << 16) | ct, pb, (int)H.cpairs.size()));
+          }
       }
       L.ntasks = (int)(H.t4.size() - L.task_off);
       if (L.ntasks) H.fplan.push_back(L);
@@ -265,6 +328,10 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         if (!fuse)
           for (int r0 = ke; r0 < nr; r0 += DEEP_R) deep.push_back(make_int4((int)s, kb, slot, r0));
         int mt = nr - ke, cw = nc - ke;
+        const double pw = ke - kb;
+        H.kind_flops[2] += 2.0 * pw * pw * pw / 3.0;
+        H.kind_flops[3] += 2.0 * (double)(nr - ke) * pw * pw / 2.0;
+        H.kind_flops[4] += 2.0 * ((double)mt * cw - (double)cw * (cw - 1) / 2.0) * pw;
         for (int c0 = 0; c0 < cw; c0 += TILE)
           for (int r0 = c0; r0 < mt; r0 += TILE) schur.push_back(make_int4((int)s, kb, r0, c0));
         ++slot;
@@ -285,15 +352,8 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         H.fplan.push_back(C);
       }
     }
-    // Forward solve launches for this level.
+    // Forward solve launch for this level.
     {
-      Launch L{L_FWD_GATHER, (long long)H.t2.size(), 0, 0};
-      for (int64_t s : lvl) {
-        if (S.upd_ptr[s + 1] == S.upd_ptr[s]) continue;
-        for (int c0 = 0; c0 < S.sn[s].ncol; c0 += SB) H.t2.push_back(make_int2((int)s, c0));
-      }
-      L.ntasks = (int)(H.t2.size() - L.task_off);
-      if (L.ntasks) H.fwdplan.push_back(L);
       Launch Dg{L_FWD_DIAG, (long long)H.t1.size(), (int)lvl.size(), 0};
       for (int64_t s : lvl) H.t1.push_back((int)s);
       H.fwdplan.push_back(Dg);
@@ -326,7 +386,6 @@ struct KernelSetup {
     CK(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
     CK(cudaFuncSetAttribute(k_getf2<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_getf2(es, 128)));
     CK(cudaFuncSetAttribute(k_deep<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep(es, 128)));
-    CK(cudaFuncSetAttribute(k_fwd_gather<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
     CK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
     CK(cudaFuncSetAttribute(k_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
     done = true;
@@ -366,7 +425,7 @@ struct rslab_fac_handle {
   cudaGraphExec_t fgraph = nullptr;
   // solve workspace
   int ws_nrhs = 0;
-  void *Yg = nullptr, *Ze = nullptr, *Xg = nullptr, *bdev = nullptr, *xdev = nullptr;
+  void *Yg = nullptr, *Ze = nullptr, *Xg = nullptr, *Ub = nullptr, *bdev = nullptr, *xdev = nullptr;
   std::vector<std::unique_ptr<void, DFree>> ws;
   cudaGraphExec_t sgraph = nullptr;
   int sgraph_nrhs = -1;
@@ -421,8 +480,23 @@ FactorArgs make_fargs(rslab_fac_handle& F) {
 }
 
 // Enqueue the whole numeric factor of the values in F.aval on F.st.
+struct Prof {
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> kind;
+  void mark(cudaStream_t st, int k) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    CK(cudaEventRecord(e, st));
+    ev.push_back(e);
+    kind.push_back(k);
+  }
+  ~Prof() {
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+};
+
 template <typename T>
-void enqueue_factor(rslab_fac_handle& F) {
+void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
   auto& H = *F.sym;
   const int n = H.n;
   const size_t es = sizeof(T);
@@ -442,10 +516,11 @@ void enqueue_factor(rslab_fac_handle& F) {
                                                 (T*)F.panel);
   FactorArgs fa = make_fargs<T>(F);
   const int nb_small = H.panel_nb, nb_big = std::max(H.panel_nb, 128);
+  if (prof) prof->mark(st, 0);
   for (const Launch& L : H.fplan) {
     switch (L.kind) {
       case L_CMOD:
-        k_cmod<T><<<L.ntasks, TPB, smem_cmod(es), st>>>(fa, H.d_t4 + L.task_off);
+        k_cmod<T><<<L.ntasks, TPB, smem_cmod(es), st>>>(fa, H.d_t4 + L.task_off, H.d_cpairs);
         break;
       case L_GETF2: {
         FactorArgs f2 = fa;
@@ -463,6 +538,7 @@ void enqueue_factor(rslab_fac_handle& F) {
         k_schur<T><<<L.ntasks, TPB, smem_schur(es), st>>>(fa, H.d_t4 + L.task_off, nb_small, nb_big);
         break;
     }
+    if (prof) prof->mark(st, L.kind == L_CMOD ? 1 : L.kind == L_GETF2 ? 2 : L.kind == L_DEEP ? 3 : 4);
   }
   CK(cudaMemsetAsync(F.cnt3, 0, 3 * sizeof(unsigned long long), st));
   k_inertia<T><<<grid1(n), 256, 0, st>>>(n, (const T*)F.d, (const T*)F.dsub, F.kind, F.cnt3);
@@ -527,6 +603,7 @@ void ensure_ws(rslab_fac_handle& F, int nrhs) {
   F.Yg = a(m * es);
   F.Ze = a(m * es);
   F.Xg = a(m * es);
+  F.Ub = a((size_t)std::max(F.sym->urows, 1LL) * nrhs * es);
   F.bdev = a(m * es);
   F.xdev = a(m * es);
   F.ws_nrhs = nrhs;
@@ -559,6 +636,8 @@ SolveArgs make_sargs(rslab_fac_handle& F, int ld, int c0, int nr) {
   a.Yg = F.Yg;
   a.Ze = F.Ze;
   a.Xg = F.Xg;
+  a.U = F.Ub;
+  a.uoff = H.d_uoff;
   a.ld = ld;
   a.c0 = c0;
   a.nrhs = nr;
@@ -577,10 +656,7 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs) {
     const int nr = std::min(RHS_MAX, nrhs - c0);
     SolveArgs sa = make_sargs<T>(F, nrhs, c0, nr);
     for (const Launch& L : H.fwdplan) {
-      if (L.kind == L_FWD_GATHER)
-        k_fwd_gather<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t2 + L.task_off);
-      else
-        k_fwd_diag<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
+      k_fwd_diag<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
     }
     k_dsolve<T><<<grid1((long long)n * nr), 256, 0, st>>>(n, sa);
     for (const Launch& L : H.bwdplan) k_bwd<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
@@ -998,6 +1074,48 @@ int rslab_factor_info(const rslab_fac_handle* F, rslab_factor_info_t* info) {
 
 void* rslab_factor_stream(const rslab_fac_handle* F) { return F ? (void*)F->st : nullptr; }
 
+// One eager (non-graph) refactor of the current values with a CUDA event
+// after every launch: device ms, launch count and algorithmic flops per
+// kernel class ([0] equilibration+assembly, [1] cmod, [2] getf2,
+// [3] deep-row replay, [4] panel Schur, [5] total).
+int rslab_factor_profile(rslab_fac_handle* F, double* kind_ms, int64_t* kind_launches, double* kind_flops) {
+  try {
+    if (!F) throw RslabError(Status::InvalidInput, "null handle");
+    auto& H = *F->sym;
+    Prof prof;
+    dispatch_field(F->dtype, [&](auto z) {
+      using T = decltype(z);
+      KernelSetup<T>::configure();
+      prof.mark(F->st, -1);
+      enqueue_factor<T>(*F, &prof);
+    });
+    CK(cudaStreamSynchronize(F->st));
+    for (int k = 0; k < 6; ++k) {
+      kind_ms[k] = 0;
+      kind_launches[k] = 0;
+    }
+    for (size_t i = 1; i < prof.ev.size(); ++i) {
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, prof.ev[i - 1], prof.ev[i]));
+      int k = prof.kind[i];
+      kind_ms[k] += ms;
+      kind_ms[5] += ms;
+      kind_launches[k] += 1;
+      kind_launches[5] += 1;
+    }
+    const double cplx = (F->dtype == RSLAB_C64 || F->dtype == RSLAB_C32) ? 4.0 : 1.0;
+    double tot = 0;
+    for (int k = 0; k < 5; ++k) {
+      kind_flops[k] = H.kind_flops[k] * cplx;
+      tot += kind_flops[k];
+    }
+    kind_flops[5] = tot;
+    return 0;
+  } catch (const RslabError& e) {
+    return fail(e);
+  }
+}
+
 // Export in the reference LdltFactors layout (src/dense/ldlt_generic.rs:31-66):
 // unit diagonal first, rows sorted, exact zeros dropped, the 2x2 coupling row
 // skipped.  l_col_ptr[n+1]; call with null value arrays to get nnz first via
@@ -1014,26 +1132,41 @@ static void export_counts(const rslab_fac_handle* F, std::vector<unsigned char>&
   CK(cudaMemcpy(kind.data(), F->kind, H.n, cudaMemcpyDeviceToHost));
 }
 
-static bool is_zero_bytes(const unsigned char* p, size_t es) {
+static bool is_zero_value(const unsigned char* p, int dtype) {
   // exact zero of the field (both +0 and -0)
-  if (es == 8) {
-    double v;
-    std::memcpy(&v, p, 8);
-    return v == 0.0;
+  switch (dtype) {
+    case RSLAB_F64: {
+      double v;
+      std::memcpy(&v, p, 8);
+      return v == 0.0;
+    }
+    case RSLAB_C64: {
+      double v[2];
+      std::memcpy(v, p, 16);
+      return v[0] == 0.0 && v[1] == 0.0;
+    }
+    case RSLAB_F32: {
+      float v;
+      std::memcpy(&v, p, 4);
+      return v == 0.0f;
+    }
+    default: {
+      float v[2];
+      std::memcpy(v, p, 8);
+      return v[0] == 0.0f && v[1] == 0.0f;
+    }
   }
-  if (es == 16) {
-    double v[2];
-    std::memcpy(v, p, 16);
-    return v[0] == 0.0 && v[1] == 0.0;
+}
+
+static void write_one(unsigned char* dst, int dtype) {
+  std::memset(dst, 0, elem_size(dtype));
+  if (dtype == RSLAB_F64 || dtype == RSLAB_C64) {
+    double one = 1.0;
+    std::memcpy(dst, &one, 8);
+  } else {
+    float one = 1.0f;
+    std::memcpy(dst, &one, 4);
   }
-  if (es == 4) {
-    float v;
-    std::memcpy(&v, p, 4);
-    return v == 0.0f;
-  }
-  float v[2];
-  std::memcpy(v, p, 8);
-  return v[0] == 0.0f && v[1] == 0.0f;
 }
 
 int rslab_export_factors(const rslab_fac_handle* F, int64_t* l_col_ptr, int64_t* l_row_idx, void* l_values, void* d_diag,
@@ -1064,7 +1197,7 @@ int rslab_export_factors(const rslab_fac_handle* F, int64_t* l_col_ptr, int64_t*
         int64_t i0 = kind[f0 + p] == 1 ? p + 2 : p + 1;
         for (int64_t i = i0; i < nr; ++i) {
           int64_t idx = H.poff[s] + i + p * nr;
-          if (is_zero_bytes(&panel[idx * es], es)) continue;
+          if (is_zero_value(&panel[idx * es], F->dtype)) continue;
           int64_t g = i < nc ? rs[lperm[f0 + i]] : rs[i];
           col.push_back({e_of_g[g], idx});
         }
@@ -1074,17 +1207,7 @@ int rslab_export_factors(const rslab_fac_handle* F, int64_t* l_col_ptr, int64_t*
           if (l_values) {
             unsigned char* dst = (unsigned char*)l_values + nnz * es;
             if (x.second < 0) {
-              std::memset(dst, 0, es);
-              if (es == 8) {
-                double one = 1.0;
-                std::memcpy(dst, &one, 8);
-              } else if (es == 16) {
-                double one = 1.0;
-                std::memcpy(dst, &one, 8);
-              } else {
-                float one = 1.0f;
-                std::memcpy(dst, &one, 4);
-              }
+              write_one(dst, F->dtype);
             } else {
               std::memcpy(dst, &panel[x.second * es], es);
             }

@@ -575,6 +575,19 @@ class MixedLdltSolver:
         return int(N.lib.rslab_factor_stream(self._h) or 0)
 
 
+KINDS = ("assembly", "cmod", "getf2", "deep_replay", "panel_schur", "total")
+
+
+def factor_profile(handle) -> dict:
+    """Per-kernel-class device ms, launches and algorithmic flops of one eager
+    refactor (the measurement aid behind bench.py's roofline line)."""
+    ms = (C.c_double * 6)()
+    nl = (C.c_int64 * 6)()
+    fl = (C.c_double * 6)()
+    _check(N.lib.rslab_factor_profile(handle, ms, nl, fl))
+    return {k: {"ms": ms[i], "launches": int(nl[i]), "flops": fl[i]} for i, k in enumerate(KINDS)}
+
+
 def amd_order(n: int, col_ptr, row_idx) -> tuple:
     """AMD on a full symmetric pattern; returns (perm, stats dict)."""
     cp = _i64(col_ptr)
