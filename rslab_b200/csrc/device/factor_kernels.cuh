@@ -422,6 +422,144 @@ __device__ void replay_rows(T* X, int R, int rows, int kb, int ke, int nb, const
   }
 }
 
+// Warp-per-row replay: lane l holds columns l + 32*j (j < NS) of one deep
+// row in registers; every pivot step's broadcast / interchange goes through
+// shuffles, so a warp replays a whole row with no block barrier.  The
+// per-element op sequence is exactly apply_bk_panel_trailing's.
+template <typename T>
+__device__ __forceinline__ T shfl_t(T v, int src) {
+  if constexpr (Field<T>::complex) {
+    T r;
+    r.re = __shfl_sync(0xffffffffu, v.re, src);
+    r.im = __shfl_sync(0xffffffffu, v.im, src);
+    return r;
+  } else {
+    return __shfl_sync(0xffffffffu, v, src);
+  }
+}
+
+template <typename T, int NS>
+__device__ __forceinline__ T pick(const T (&x)[NS], int slot) {
+  T v = x[0];
+#pragma unroll
+  for (int j = 1; j < NS; ++j)
+    if (j == slot) v = x[j];
+  return v;
+}
+
+template <typename T, int NS>
+__device__ __forceinline__ void put(T (&x)[NS], int slot, T v) {
+#pragma unroll
+  for (int j = 0; j < NS; ++j)
+    if (j == slot) x[j] = v;
+}
+
+template <typename T, int NS>
+__device__ void replay_row_warp(T (&x)[NS], int pw, int nb, const T* __restrict__ snap, const int* __restrict__ swaps,
+                                int kb, const T* __restrict__ d, const T* __restrict__ dsub,
+                                const unsigned char* __restrict__ kind) {
+  using F = Field<T>;
+  const int lane = threadIdx.x & 31;
+  int k = 0;
+  while (k < pw) {
+    const int kp = swaps[k];
+    const bool two = kind[k] == 1;
+    if (kp >= 0) {
+      const int src = two ? k + 1 : k, dst = kp - kb;
+      const T vs = shfl_t(pick(x, src >> 5), src & 31);
+      const T vd = shfl_t(pick(x, dst >> 5), dst & 31);
+      if (lane == (src & 31)) put(x, src >> 5, vd);
+      if (lane == (dst & 31)) put(x, dst >> 5, vs);
+    }
+    const T xk = shfl_t(pick(x, k >> 5), k & 31);
+    if (two) {
+      const T xk1 = shfl_t(pick(x, (k + 1) >> 5), (k + 1) & 31);
+#pragma unroll
+      for (int j = 0; j < NS; ++j) {
+        const int col = lane + 32 * j;
+        if (col >= k + 2 && col < pw) {
+          const T l1 = snap[k * nb + col], l2 = snap[(k + 1) * nb + col];
+          T v = F::sub(x[j], F::mul(xk, l1));
+          x[j] = F::sub(v, F::mul(xk1, l2));
+        }
+      }
+      const T d11 = d[k], d21 = dsub[k], d22 = d[k + 1];
+      const T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
+      const T detinv = F::recip(det);
+      if (lane == (k & 31)) put(x, k >> 5, F::mul(F::sub(F::mul(d22, xk), F::mul(d21, xk1)), detinv));
+      if (lane == ((k + 1) & 31)) put(x, (k + 1) >> 5, F::mul(F::sub(F::mul(d11, xk1), F::mul(d21, xk)), detinv));
+      k += 2;
+    } else {
+#pragma unroll
+      for (int j = 0; j < NS; ++j) {
+        const int col = lane + 32 * j;
+        if (col > k && col < pw) {
+          const T w = snap[k * nb + col];
+          if (!F::is_zero(w)) x[j] = F::sub(x[j], F::mul(xk, w));
+        }
+      }
+      const T dinv = F::recip(d[k]);
+      if (lane == (k & 31)) put(x, k >> 5, F::mul(xk, dinv));
+      k += 1;
+    }
+  }
+}
+
+// Replay a block's pivot steps on deep rows [r_begin, r_end) of a panel:
+// rows staged through shared memory (32 rows x pw, padded stride) so both
+// the global loads / stores and the per-row register fills are conflict-free.
+template <typename T, int NT>
+__device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int nb, int r_begin, int r_end,
+                                 const T* __restrict__ snap, const int* __restrict__ swaps, const T* __restrict__ d,
+                                 const T* __restrict__ dsub, const unsigned char* __restrict__ kind, T* X) {
+  constexpr int R = 32, LDX = 33;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int NW = NT / 32;
+  for (int rs0 = r_begin; rs0 < r_end; rs0 += R) {
+    const int rows = min(R, r_end - rs0);
+    for (int e = threadIdx.x; e < R * pw; e += NT) {
+      const int c = e / R, r = e % R;
+      if (r < rows) X[c * LDX + r] = panel[(rs0 + r) + (long long)(kb + c) * nrow];
+    }
+    __syncthreads();
+    for (int r = warp; r < rows; r += NW) {
+      if (pw <= 64) {
+        T x[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int col = lane + 32 * j;
+          x[j] = col < pw ? X[col * LDX + r] : Field<T>::zero();
+        }
+        replay_row_warp<T, 2>(x, pw, nb, snap, swaps, kb, d, dsub, kind);
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int col = lane + 32 * j;
+          if (col < pw) X[col * LDX + r] = x[j];
+        }
+      } else {
+        T x[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int col = lane + 32 * j;
+          x[j] = col < pw ? X[col * LDX + r] : Field<T>::zero();
+        }
+        replay_row_warp<T, 4>(x, pw, nb, snap, swaps, kb, d, dsub, kind);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int col = lane + 32 * j;
+          if (col < pw) X[col * LDX + r] = x[j];
+        }
+      }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < R * pw; e += NT) {
+      const int c = e / R, r = e % R;
+      if (r < rows) panel[(rs0 + r) + (long long)(kb + c) * nrow] = X[c * LDX + r];
+    }
+    __syncthreads();
+  }
+}
+
 constexpr int DEEP_R = 32;  // deep rows per replay chunk
 
 // ---------------------------------------------------------------------------
@@ -656,38 +794,39 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
     for (int i = j + lane; i < pw; i += 32)
       panel[(kb + i) + (long long)(kb + j) * nrow] = (two && i == j + 1) ? F::zero() : A[pk(i, j, pw)];
   }
-  // Left row segments of each interchange: columns [0, kb) at rows p, q.
+  // Left row segments of the interchanges (columns [0, kb), rows of this
+  // block): the swap sequence composes to one row permutation of the block,
+  // applied as a coalesced gather per column (same final values).
   const int nsw = ctl[2];
   if (nsw > 0 && kb > 0) {
-    for (int j = tid; j < kb; j += NT) {
-      T* col = panel + (long long)j * nrow;
+    int* src_row = reinterpret_cast<int*>(l1);  // pw ints (l1/l2 are free now)
+    __syncthreads();
+    if (tid == 0) {
+      for (int r = 0; r < pw; ++r) src_row[r] = r;
       for (int t = 0; t < nsw; ++t) {
-        int p = swp_p[t], q = swp_q[t];
-        T x = col[p];
-        col[p] = col[q];
-        col[q] = x;
+        const int p = swp_p[t] - kb, q = swp_q[t] - kb;
+        const int x = src_row[p];
+        src_row[p] = src_row[q];
+        src_row[q] = x;
       }
+    }
+    __syncthreads();
+    const int cols_per = NT / pw > 0 ? NT / pw : 1;
+    for (int j0 = 0; j0 < kb; j0 += cols_per) {
+      const int j = j0 + tid / pw, r = tid % pw;
+      T v = F::zero();
+      const bool act = tid < cols_per * pw && j < kb;
+      if (act) v = panel[(kb + src_row[r]) + (long long)j * nrow];
+      __syncthreads();
+      if (act) panel[(kb + r) + (long long)j * nrow] = v;
+      __syncthreads();
     }
   }
   // kind/d written by tid 0 are read by the replay below.
   __syncthreads();
   if (fuse && nrow > ke) {
-    // Replay this block's pivot steps on the deep rows [ke, nrow) in chunks.
-    T* X = A;  // reuse shared memory: DEEP_R x pw
-    for (int rs0 = ke; rs0 < nrow; rs0 += DEEP_R) {
-      const int rows = min(DEEP_R, nrow - rs0);
-      for (int e = tid; e < rows * pw; e += NT) {
-        int c = e / rows, r = e % rows;
-        X[c * DEEP_R + r] = panel[(rs0 + r) + (long long)(kb + c) * nrow];
-      }
-      __syncthreads();
-      replay_rows<T, NT>(X, DEEP_R, rows, kb, ke, nb, snap, swaps, dG, dsG, kindG);
-      for (int e = tid; e < rows * pw; e += NT) {
-        int c = e / rows, r = e % rows;
-        panel[(rs0 + r) + (long long)(kb + c) * nrow] = X[c * DEEP_R + r];
-      }
-      __syncthreads();
-    }
+    // Replay this block's pivot steps on the deep rows [ke, nrow).
+    replay_deep_rows<T, NT>(panel, nrow, kb, pw, nb, ke, nrow, snap, swaps, dG, dsG, kindG, A);
   }
 }
 
@@ -709,19 +848,9 @@ __global__ void __launch_bounds__(NT) k_deep(FactorArgs fa, const int4* __restri
   const T* snap = reinterpret_cast<const T*>(sc);
   const int* swaps = reinterpret_cast<const int*>(snap + (long long)nb * nb);
   T* X = reinterpret_cast<T*>(smem_raw);
-  const int rows = min(DEEP_R, nrow - rs0);
-  const int tid = threadIdx.x;
-  for (int e = tid; e < rows * pw; e += NT) {
-    int c = e / rows, r = e % rows;
-    X[c * DEEP_R + r] = panel[(rs0 + r) + (long long)(kb + c) * nrow];
-  }
-  __syncthreads();
-  replay_rows<T, NT>(X, DEEP_R, rows, kb, ke, nb, snap, swaps, reinterpret_cast<const T*>(fa.d) + first + kb,
-                     reinterpret_cast<const T*>(fa.dsub) + first + kb, fa.kind + first + kb);
-  for (int e = tid; e < rows * pw; e += NT) {
-    int c = e / rows, r = e % rows;
-    panel[(rs0 + r) + (long long)(kb + c) * nrow] = X[c * DEEP_R + r];
-  }
+  replay_deep_rows<T, NT>(panel, nrow, kb, pw, nb, rs0, min(rs0 + DEEP_R, nrow), snap, swaps,
+                          reinterpret_cast<const T*>(fa.d) + first + kb,
+                          reinterpret_cast<const T*>(fa.dsub) + first + kb, fa.kind + first + kb, X);
 }
 
 }  // namespace rsd

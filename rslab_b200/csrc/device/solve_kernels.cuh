@@ -44,6 +44,7 @@ struct SolveArgs {
   void* Ze;   // n x ld, e order
   void* Xg;   // n x ld, g order
   void* U;    // sum_s (nrow_s - ncol_s) x ld: U_s = L21_s z_s
+  void* Wb;   // n x ld, e order: backward off-diagonal dots
   const long long* uoff;  // row offset of U_s
   int ld;     // row stride (total rhs count)
   int c0;     // first rhs column of this pass
@@ -183,26 +184,97 @@ __global__ void __launch_bounds__(SOLVE_NT) k_fwd_diag(SolveArgs a, const int* _
     }
     __syncthreads();
   }
-  // 3. push U_s = L21 z_s: warps take 32-row groups, lanes the rows.
-  T* Us = Uall + a.uoff[s] * a.ld;
+}
+
+// Forward push of supernode s, rows [ncol + r0, ncol + r0 + 64):
+// U_s = L21_s z_s.  Two 32-row lane groups x four q-splits (warps); the
+// q-split partial sums are added in a fixed order (deterministic).
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_NT) k_fwd_push(SolveArgs a, const int2* __restrict__ tasks) {
+  using F = Field<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* red = reinterpret_cast<T*>(smem_raw);  // [4 splits][64 rows][RHS_MAX]
+  const int2 tk = tasks[blockIdx.x];
+  const int s = tk.x, r0 = tk.y;
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
+  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
+  const T* Z = reinterpret_cast<const T*>(a.Ze) + a.c0 + (long long)first * a.ld;
+  T* Us = reinterpret_cast<T*>(a.U) + a.c0 + a.uoff[s] * a.ld;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rg = warp & 1, qs = warp >> 1;  // row group, q split
+  const int rl = rg * 32 + lane;            // local row 0..63
+  const int r = ncol + r0 + rl;
+  const bool ok = r < nrow;
+  T acc[RHS_MAX];
+#pragma unroll
+  for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
+  for (int q = qs; q < ncol; q += 4) {
+    T l = ok ? L[r + (long long)q * nrow] : F::zero();
+    const T* zq = Z + (long long)q * a.ld;
+#pragma unroll
+    for (int c = 0; c < RHS_MAX; ++c)
+      if (c < a.nrhs) acc[c] = F::fma_(l, zq[c], acc[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < RHS_MAX; ++c)
+    if (c < a.nrhs) red[(qs * 64 + rl) * RHS_MAX + c] = acc[c];
+  __syncthreads();
+  for (int e = threadIdx.x; e < 64 * a.nrhs; e += SOLVE_NT) {
+    const int row = e / a.nrhs, c = e % a.nrhs;
+    const int rr = ncol + r0 + row;
+    if (rr >= nrow) continue;
+    T v = red[(0 * 64 + row) * RHS_MAX + c];
+    v = F::add(v, red[(1 * 64 + row) * RHS_MAX + c]);
+    v = F::add(v, red[(2 * 64 + row) * RHS_MAX + c]);
+    v = F::add(v, red[(3 * 64 + row) * RHS_MAX + c]);
+    Us[(long long)(rr - ncol) * a.ld + c] = v;
+  }
+}
+
+// Backward off-diagonal dots of supernode s, pivot columns [c0, c0+32):
+// W[first + p] = sum_{r >= ncol} L[r, p] x[g_r] (warp per column, lanes
+// over rows, fixed-order shuffle reduction).
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_NT) k_bwd_off(SolveArgs a, const int2* __restrict__ tasks) {
+  using F = Field<T>;
+  const int2 tk = tasks[blockIdx.x];
+  const int s = tk.x, c0 = tk.y;
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
+  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
+  const int* rss = a.rs + a.sn_rsoff[s];
+  const T* X = reinterpret_cast<const T*>(a.Xg) + a.c0;
+  T* Wb = reinterpret_cast<T*>(a.Wb) + a.c0 + (long long)first * a.ld;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NW = SOLVE_NT / 32;
-  for (int r0 = ncol + warp * 32; r0 < nrow; r0 += NW * 32) {
-    const int r = r0 + lane;
-    const bool ok = r < nrow;
+  const int cols_here = min(32, ncol - c0);
+  for (int pc = warp; pc < cols_here; pc += NW) {
+    const int p = c0 + pc;
     T acc[RHS_MAX];
 #pragma unroll
     for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
-    for (int q = 0; q < ncol; ++q) {
-      T l = ok ? L[r + (long long)q * nrow] : F::zero();
-      const T* zq = Z + (long long)q * a.ld;
+    const T* Lc = L + (long long)p * nrow;
+    for (int r = ncol + lane; r < nrow; r += 32) {
+      T l = Lc[r];
+      const T* xr = X + (long long)rss[r] * a.ld;
 #pragma unroll
       for (int c = 0; c < RHS_MAX; ++c)
-        if (c < a.nrhs) acc[c] = F::fma_(l, zq[c], acc[c]);
+        if (c < a.nrhs) acc[c] = F::fma_(l, xr[c], acc[c]);
     }
-    if (ok)
 #pragma unroll
-      for (int c = 0; c < RHS_MAX; ++c)
-        if (c < a.nrhs) Us[(long long)(r - ncol) * a.ld + c] = acc[c];
+    for (int c = 0; c < RHS_MAX; ++c) {
+      if (c >= a.nrhs) continue;
+      T x = acc[c];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        if constexpr (Field<T>::complex) {
+          x.re += __shfl_down_sync(0xffffffffu, x.re, o);
+          x.im += __shfl_down_sync(0xffffffffu, x.im, o);
+        } else {
+          x += __shfl_down_sync(0xffffffffu, x, o);
+        }
+      }
+      if (lane == 0) Wb[(long long)p * a.ld + c] = x;
+    }
   }
 }
 
@@ -245,9 +317,8 @@ __global__ void __launch_bounds__(SOLVE_NT) k_bwd(SolveArgs a, const int* __rest
   const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
   const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
   const int* lp = a.lperm + first;
-  const int* rss = a.rs + a.sn_rsoff[s];
   T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  const T* Xall = reinterpret_cast<const T*>(a.Xg) + a.c0;
+  const T* Wb = reinterpret_cast<const T*>(a.Wb) + a.c0 + (long long)first * a.ld;
   T* Xw = reinterpret_cast<T*>(a.Xg) + a.c0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NW = SOLVE_NT / 32;
@@ -261,9 +332,9 @@ __global__ void __launch_bounds__(SOLVE_NT) k_bwd(SolveArgs a, const int* __rest
 #pragma unroll
       for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
       const T* Lc = L + (long long)p * nrow;
-      for (int r = j1 + lane; r < nrow; r += 32) {
+      for (int r = j1 + lane; r < ncol; r += 32) {
         T l = Lc[r];
-        const T* v = r < ncol ? Z + (long long)r * a.ld : Xall + (long long)rss[r] * a.ld;
+        const T* v = Z + (long long)r * a.ld;
 #pragma unroll
         for (int c = 0; c < RHS_MAX; ++c)
           if (c < a.nrhs) acc[c] = F::fma_(l, v[c], acc[c]);
@@ -291,7 +362,9 @@ __global__ void __launch_bounds__(SOLVE_NT) k_bwd(SolveArgs a, const int* __rest
       T v[RHS_MAX];
 #pragma unroll
       for (int c = 0; c < RHS_MAX; ++c)
-        v[c] = (ok && c < a.nrhs) ? F::sub(Z[(long long)p * a.ld + c], vb[lane * RHS_MAX + c]) : F::zero();
+        v[c] = (ok && c < a.nrhs)
+                   ? F::sub(F::sub(Z[(long long)p * a.ld + c], Wb[(long long)p * a.ld + c]), vb[lane * RHS_MAX + c])
+                   : F::zero();
       // Backward inside the block: v[p] -= L[q, p] v[q] for q > p.
       for (int q = nb - 1; q >= 1; --q) {
         const int qq = j0 + q;

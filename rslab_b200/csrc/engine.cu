@@ -65,7 +65,7 @@ size_t elem_size(int dtype) {
   throw RslabError(Status::InvalidInput, "unknown dtype");
 }
 
-enum LaunchKind { L_CMOD, L_GETF2, L_DEEP, L_SCHUR, L_FWD_DIAG, L_BWD };
+enum LaunchKind { L_CMOD, L_GETF2, L_DEEP, L_SCHUR, L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD };
 struct Launch {
   int kind;
   long long task_off;  // into the int4 / int2 / int task arrays
@@ -96,6 +96,7 @@ struct rslab_sym_handle {
   std::vector<int4> t4;
   std::vector<int4> cpairs;   // cmod (k, a, q0, nr << 16 | nc) per tile, in update order
   std::vector<int> t1;
+  std::vector<int2> t2;
   std::vector<long long> uoff;  // forward-push row offsets (nrow - ncol per supernode)
   long long urows = 0;
   std::vector<Launch> fplan, fwdplan, bwdplan;
@@ -118,6 +119,7 @@ struct rslab_sym_handle {
   int4* d_t4 = nullptr;
   int4* d_cpairs = nullptr;
   int* d_t1 = nullptr;
+  int2* d_t2 = nullptr;
   long long* d_uoff = nullptr;
   std::mutex mu;
   rslab_analyze_settings settings{};
@@ -167,6 +169,7 @@ struct rslab_sym_handle {
     d_t4 = up(t4, st);
     d_cpairs = up(cpairs, st);
     d_t1 = up(t1, st);
+    d_t2 = up(t2, st);
     d_uoff = up(uoff, st);
     CK(cudaStreamSynchronize(st));
     device = dev;
@@ -248,6 +251,7 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
   const int nb_small = H.panel_nb, nb_big = std::max(H.panel_nb, 128);
   H.max_nb = nb_big;
   auto nb_of = [&](int s) { return S.sn[s].ncol >= 512 ? nb_big : nb_small; };
+  std::vector<std::pair<Launch, Launch>> lvl_ranges;
   for (const auto& lvl : S.by_level) {
     // cmod tiles of every panel that has updaters, each with its precomputed
     // list of (updater, row run, column run) pairs in update-list order.
@@ -352,29 +356,43 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         H.fplan.push_back(C);
       }
     }
-    // Forward solve launch for this level.
+    // Solve launches for this level: forward = diagonal blocks, then the
+    // row-tiled push; backward (run root first) = column-chunked
+    // off-diagonal dots, then the diagonal blocks.
     {
       Launch Dg{L_FWD_DIAG, (long long)H.t1.size(), (int)lvl.size(), 0};
       for (int64_t s : lvl) H.t1.push_back((int)s);
       H.fwdplan.push_back(Dg);
+      Launch Pu{L_FWD_PUSH, (long long)H.t2.size(), 0, 0};
+      for (int64_t s : lvl)
+        for (int r0 = 0; r0 < H.nrow[s] - S.sn[s].ncol; r0 += 64) H.t2.push_back(make_int2((int)s, r0));
+      Pu.ntasks = (int)(H.t2.size() - Pu.task_off);
+      if (Pu.ntasks) H.fwdplan.push_back(Pu);
+      Launch Bo{L_BWD_OFF, (long long)H.t2.size(), 0, 0};
+      for (int64_t s : lvl)
+        if (H.nrow[s] > S.sn[s].ncol)
+          for (int c0 = 0; c0 < S.sn[s].ncol; c0 += 32) H.t2.push_back(make_int2((int)s, c0));
+      Bo.ntasks = (int)(H.t2.size() - Bo.task_off);
+      lvl_ranges.push_back({Bo, Launch{L_BWD, Dg.task_off, Dg.ntasks, 0}});
     }
   }
-  // Backward: levels root first; the task list reuses the level lists.
-  std::vector<std::pair<long long, int>> lvl_ranges;
-  for (const auto& L : H.fwdplan)
-    if (L.kind == L_FWD_DIAG) lvl_ranges.push_back({L.task_off, L.ntasks});
-  for (auto it = lvl_ranges.rbegin(); it != lvl_ranges.rend(); ++it) H.bwdplan.push_back({L_BWD, it->first, it->second, 0});
+  // Backward: levels root first.
+  for (auto it = lvl_ranges.rbegin(); it != lvl_ranges.rend(); ++it) {
+    if (it->first.ntasks) H.bwdplan.push_back(it->first);
+    H.bwdplan.push_back(it->second);
+  }
 }
 
 size_t smem_cmod(size_t es) { return (size_t)TILE * TILE * es + 2 * 16 * TILE * es + 3 * TILE * 4 + 64; }
 size_t smem_schur(size_t es) { return 2 * 16 * TILE * es; }
 size_t smem_getf2(size_t es, int nb) {
   size_t a = (size_t)nb * (nb + 1) / 2 * es + 2 * nb * es + 16 + 32 * 8 + 32 * 4 + 16 * 4;
-  size_t b = (size_t)DEEP_R * nb * es;
+  size_t b = (size_t)(DEEP_R + 1) * nb * es;
   return std::max(a, b) + 64;
 }
-size_t smem_deep(size_t es, int nb) { return (size_t)DEEP_R * nb * es + 64; }
+size_t smem_deep(size_t es, int nb) { return (size_t)(DEEP_R + 1) * nb * es + 64; }
 size_t smem_solve(size_t es) { return (size_t)(SOLVE_NT / 32) * 32 * RHS_MAX * es + 32 * RHS_MAX * es + 64 * 4; }
+size_t smem_push(size_t es) { return (size_t)4 * 64 * RHS_MAX * es; }
 
 template <typename T>
 struct KernelSetup {
@@ -388,6 +406,7 @@ struct KernelSetup {
     CK(cudaFuncSetAttribute(k_deep<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep(es, 128)));
     CK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
     CK(cudaFuncSetAttribute(k_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
+    CK(cudaFuncSetAttribute(k_fwd_push<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_push(es)));
     done = true;
   }
 };
@@ -425,7 +444,7 @@ struct rslab_fac_handle {
   cudaGraphExec_t fgraph = nullptr;
   // solve workspace
   int ws_nrhs = 0;
-  void *Yg = nullptr, *Ze = nullptr, *Xg = nullptr, *Ub = nullptr, *bdev = nullptr, *xdev = nullptr;
+  void *Yg = nullptr, *Ze = nullptr, *Xg = nullptr, *Ub = nullptr, *Wb = nullptr, *bdev = nullptr, *xdev = nullptr;
   std::vector<std::unique_ptr<void, DFree>> ws;
   cudaGraphExec_t sgraph = nullptr;
   int sgraph_nrhs = -1;
@@ -604,6 +623,7 @@ void ensure_ws(rslab_fac_handle& F, int nrhs) {
   F.Ze = a(m * es);
   F.Xg = a(m * es);
   F.Ub = a((size_t)std::max(F.sym->urows, 1LL) * nrhs * es);
+  F.Wb = a(m * es);
   F.bdev = a(m * es);
   F.xdev = a(m * es);
   F.ws_nrhs = nrhs;
@@ -637,6 +657,7 @@ SolveArgs make_sargs(rslab_fac_handle& F, int ld, int c0, int nr) {
   a.Ze = F.Ze;
   a.Xg = F.Xg;
   a.U = F.Ub;
+  a.Wb = F.Wb;
   a.uoff = H.d_uoff;
   a.ld = ld;
   a.c0 = c0;
@@ -656,10 +677,18 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs) {
     const int nr = std::min(RHS_MAX, nrhs - c0);
     SolveArgs sa = make_sargs<T>(F, nrhs, c0, nr);
     for (const Launch& L : H.fwdplan) {
-      k_fwd_diag<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
+      if (L.kind == L_FWD_DIAG)
+        k_fwd_diag<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
+      else
+        k_fwd_push<T><<<L.ntasks, SOLVE_NT, smem_push(es), st>>>(sa, H.d_t2 + L.task_off);
     }
     k_dsolve<T><<<grid1((long long)n * nr), 256, 0, st>>>(n, sa);
-    for (const Launch& L : H.bwdplan) k_bwd<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
+    for (const Launch& L : H.bwdplan) {
+      if (L.kind == L_BWD_OFF)
+        k_bwd_off<T><<<L.ntasks, SOLVE_NT, 0, st>>>(sa, H.d_t2 + L.task_off);
+      else
+        k_bwd<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
+    }
   }
   k_perm_out<T><<<grid1((long long)n * nrhs), 256, 0, st>>>(n, nrhs, H.d_perm, F.scale, (const T*)F.Xg, x);
   CK(cudaGetLastError());
