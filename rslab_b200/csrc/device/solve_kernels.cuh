@@ -323,6 +323,7 @@ __global__ void __launch_bounds__(SOLVE_NT) k_bwd(SolveArgs a, const int* __rest
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NW = SOLVE_NT / 32;
   const int nblk = (ncol + SB - 1) / SB;
+  const bool has_off = nrow > ncol;  // Wb is written by k_bwd_off only then
   for (int b = nblk - 1; b >= 0; --b) {
     const int j0 = b * SB, nb = min(SB, ncol - j0), j1 = j0 + nb;
     // acc[p][c] = sum_{r >= j1} L[r, p] * v(r): warp per column p, lanes over r.
@@ -363,7 +364,9 @@ __global__ void __launch_bounds__(SOLVE_NT) k_bwd(SolveArgs a, const int* __rest
 #pragma unroll
       for (int c = 0; c < RHS_MAX; ++c)
         v[c] = (ok && c < a.nrhs)
-                   ? F::sub(F::sub(Z[(long long)p * a.ld + c], Wb[(long long)p * a.ld + c]), vb[lane * RHS_MAX + c])
+                   ? F::sub(has_off ? F::sub(Z[(long long)p * a.ld + c], Wb[(long long)p * a.ld + c])
+                                    : Z[(long long)p * a.ld + c],
+                            vb[lane * RHS_MAX + c])
                    : F::zero();
       // Backward inside the block: v[p] -= L[q, p] v[q] for q > p.
       for (int q = nb - 1; q >= 1; --q) {
