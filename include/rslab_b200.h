@@ -167,6 +167,26 @@ uint64_t rslab_rng_units(uint64_t state, int64_t m, double* out);
  * nms_lu, mass eliminations, supervariable merges. */
 int rslab_amd_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, int64_t* perm, double* stats7);
 
+/* Allocation-free dense panel factor.  No counterpart in the reference: an
+ * addition for callers that cannot allocate device memory at factor time
+ * (code running inside a CUDA graph capture or a foreign memory pool, capped
+ * or frozen allocators, real-time loops that must not risk cudaMalloc latency
+ * or an out-of-memory failure).  Factors one caller-owned dense panel
+ * (nrow x ncol column-major device memory: the fully-summed block on top of
+ * the off-diagonal rows, lower part) in place with the same panel-bounded
+ * Bunch-Kaufman kernels as rslab_factor, writing d, dsub, kind (0 = 1x1,
+ * 1/2 = first/second column of a 2x2 block), lperm (pivot position ->
+ * pre-pivot column, ncol each) and status[4] (code, failing block, perturbed
+ * count, unused), all caller-owned device memory.  All scratch lives in one
+ * 1 MiB static device array that every GPU loading the library keeps until
+ * exit: nrow <= 4096, ncol <= 1024 and panel_nb in [8, 64]; larger panels
+ * are rejected with RSLAB_INVALID_INPUT.  Calls no allocator.  The first call
+ * on a device looks up that array's device address, so make it before any
+ * stream capture.  Every call shares the array: calls whose work overlaps
+ * on the GPU (different streams, no ordering between them) race. */
+int rslab_panel_factor_noalloc(int dtype, void* panel, int64_t nrow, int64_t ncol, int64_t panel_nb, void* d,
+                               void* dsub, uint8_t* kind, int32_t* lperm, int32_t* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

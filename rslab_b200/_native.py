@@ -94,6 +94,8 @@ SIGNATURES = {
     "rslab_mixed_solve": (C.c_int, [vp, vp, C.c_int64, C.c_double, vp, C.c_int, C.POINTER(MixedInfoC)]),
     "rslab_rng_units": (C.c_uint64, [C.c_uint64, C.c_int64, C.POINTER(C.c_double)]),
     "rslab_amd_order": (C.c_int, [C.c_int64, i64p, i64p, i64p, C.POINTER(C.c_double)]),
+    "rslab_panel_factor_noalloc": (C.c_int, [C.c_int, vp, C.c_int64, C.c_int64, C.c_int64, vp, vp, vp, vp, vp,
+                                             vp]),
 }
 
 

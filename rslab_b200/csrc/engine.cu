@@ -1317,3 +1317,151 @@ int rslab_amd_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, i
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free dense panel factor.
+//
+// Some callers cannot allocate device memory while they factor: a solver
+// running inside a CUDA graph or another library's memory pool, a process
+// whose allocator is capped or frozen after start-up, or a real-time loop that
+// must not pay cudaMalloc latency or risk an out-of-memory failure mid-run.
+// For them rslab_panel_factor_noalloc runs the blocked Bunch-Kaufman panel
+// kernels (getf2, deep-row replay, in-panel Schur) on one caller-owned dense
+// panel with every piece of scratch (the per-block multiplier snapshot, swap
+// log, the panel's structure and the launch task lists) placed in the
+// file-scope array below instead of memory obtained from an allocator.  The
+// array is 1 MiB and, like every __device__ variable, is held on each GPU that
+// loads this library until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t NOALLOC_MAX_NROW = 4096;
+constexpr int64_t NOALLOC_MAX_NCOL = 1024;
+constexpr size_t NOALLOC_BYTES = size_t(1) << 20;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+// Device address of g_noalloc_scratch on the current device, looked up once
+// per device.  In host code the symbol itself is only a host-side stand-in,
+// never a device address, so kernels always receive this looked-up pointer.
+unsigned char* noalloc_scratch_on_current_device() {
+  static std::mutex mu;
+  static unsigned char* addr[256] = {};
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) throw RslabError(Status::CudaError, "device ordinal out of range");
+  std::lock_guard<std::mutex> g(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    addr[dev] = static_cast<unsigned char*>(p);
+  }
+  return addr[dev];
+}
+
+struct NoallocStruct {  // the one-supernode structure, at offset 0 of the scratch
+  int sn_first, sn_ncol, sn_nrow, pad;
+  long long sn_poff, sn_rsoff;
+};
+
+template <typename T>
+void noalloc_panel(unsigned char* base, T* panel, int nrow, int ncol, int panel_nb, T* d, T* dsub,
+                   unsigned char* kind, int* lperm, int* status, cudaStream_t st) {
+  const size_t es = sizeof(T);
+  const int nb_small = panel_nb, nb_big = std::max(panel_nb, 128);
+  const int nb = ncol >= 512 ? nb_big : nb_small;
+  // Task lists of the whole block sequence, in launch order.
+  std::vector<int4> tasks;
+  struct Seg {
+    int kind, off, cnt;
+  };
+  std::vector<Seg> segs;
+  for (int kb = 0; kb < ncol; kb += nb) {
+    const int ke = std::min(kb + nb, ncol);
+    const bool fuse = (nrow - ke) <= FUSE_DEEP_ROWS;
+    segs.push_back({L_GETF2, (int)tasks.size(), 1});
+    tasks.push_back(make_int4(0, kb, 0, fuse ? 1 : 0));
+    if (!fuse) {
+      Seg sd{L_DEEP, (int)tasks.size(), 0};
+      for (int r0 = ke; r0 < nrow; r0 += DEEP_R) tasks.push_back(make_int4(0, kb, 0, r0));
+      sd.cnt = (int)tasks.size() - sd.off;
+      segs.push_back(sd);
+    }
+    const int mt = nrow - ke, cw = ncol - ke;
+    Seg sc{L_SCHUR, (int)tasks.size(), 0};
+    for (int c0 = 0; c0 < cw; c0 += TILE)
+      for (int r0 = c0; r0 < mt; r0 += TILE) tasks.push_back(make_int4(0, kb, r0, c0));
+    sc.cnt = (int)tasks.size() - sc.off;
+    if (sc.cnt) segs.push_back(sc);
+  }
+  const size_t snap_bytes = ((size_t)nb_big * nb_big * es + 3 * nb_big * 4 + 255) / 256 * 256;
+  const size_t off_snap = 256, off_tasks = off_snap + snap_bytes;
+  const size_t need = off_tasks + tasks.size() * sizeof(int4);
+  if (need > NOALLOC_BYTES)
+    throw RslabError(Status::InvalidInput, "panel needs " + std::to_string(need) +
+                                               " bytes of scratch, more than the allocation-free limit of " +
+                                               std::to_string(NOALLOC_BYTES));
+  NoallocStruct ns{0, ncol, nrow, 0, 0, 0};
+  CK(cudaMemcpyAsync(base, &ns, sizeof(ns), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + off_tasks, tasks.data(), tasks.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(status, 0, 4 * sizeof(int), st));
+  const NoallocStruct* dn = reinterpret_cast<const NoallocStruct*>(base);
+  FactorArgs fa{};
+  fa.sn_first = &dn->sn_first;
+  fa.sn_ncol = &dn->sn_ncol;
+  fa.sn_nrow = &dn->sn_nrow;
+  fa.sn_poff = &dn->sn_poff;
+  fa.sn_rsoff = &dn->sn_rsoff;
+  fa.panel = panel;
+  fa.d = d;
+  fa.dsub = dsub;
+  fa.kind = kind;
+  fa.lperm = lperm;
+  fa.scratch = base + off_snap;
+  fa.scratch_stride = (long long)snap_bytes;
+  fa.status = status;
+  fa.perturb_floor = -1.0;
+  const int4* dt = reinterpret_cast<const int4*>(base + off_tasks);
+  CK(cudaFuncSetAttribute(k_getf2<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_getf2(es, 128)));
+  CK(cudaFuncSetAttribute(k_deep<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep(es, 128)));
+  CK(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
+  for (const Seg& g : segs) {
+    if (g.kind == L_GETF2)
+      k_getf2<T, 256><<<g.cnt, 256, smem_getf2(es, nb), st>>>(fa, dt + g.off, nb_small, nb_big);
+    else if (g.kind == L_DEEP)
+      k_deep<T, 256><<<g.cnt, 256, smem_deep(es, nb), st>>>(fa, dt + g.off, nb_small, nb_big);
+    else
+      k_schur<T><<<g.cnt, TPB, smem_schur(es), st>>>(fa, dt + g.off, nb_small, nb_big);
+  }
+  CK(cudaGetLastError());
+}
+
+}  // namespace
+
+extern "C" int rslab_panel_factor_noalloc(int dtype, void* panel, int64_t nrow, int64_t ncol, int64_t panel_nb,
+                                          void* d, void* dsub, uint8_t* kind, int32_t* lperm, int32_t* status,
+                                          void* stream) {
+  try {
+    if (!panel || !d || !dsub || !kind || !lperm || !status)
+      throw RslabError(Status::InvalidInput, "null device pointer");
+    if (ncol <= 0 || nrow < ncol) throw RslabError(Status::InvalidInput, "need 0 < ncol <= nrow");
+    if (nrow > NOALLOC_MAX_NROW || ncol > NOALLOC_MAX_NCOL)
+      throw RslabError(Status::InvalidInput, "panel " + std::to_string(nrow) + " x " + std::to_string(ncol) +
+                                                 " exceeds the allocation-free maximum of " +
+                                                 std::to_string(NOALLOC_MAX_NROW) + " x " +
+                                                 std::to_string(NOALLOC_MAX_NCOL));
+    if (panel_nb < 8 || panel_nb > 64) throw RslabError(Status::InvalidInput, "panel_nb must lie in [8, 64]");
+    unsigned char* base = noalloc_scratch_on_current_device();
+    cudaStream_t st = (cudaStream_t)stream;
+    dispatch_field(dtype, [&](auto z) {
+      using T = decltype(z);
+      noalloc_panel<T>(base, (T*)panel, (int)nrow, (int)ncol, (int)panel_nb, (T*)d, (T*)dsub, kind, lperm,
+                       status, st);
+    });
+    return 0;
+  } catch (const RslabError& e) {
+    return fail(e);
+  } catch (const std::exception& e) {
+    return fail(RslabError(Status::InvalidInput, e.what()));
+  }
+}
