@@ -277,8 +277,9 @@ def main():
                     "gflops": flops / (ms64 * 1e-3) / 1e9, "backward_error_no_ir": be64}
 
     # Per-kernel-class profile of one eager refactor (events after every launch).
-    from rslab_b200.solver import factor_profile
+    from rslab_b200.solver import factor_profile, solve_profile
     prof_mixed = factor_profile(mixed._h)
+    sprof_mixed = solve_profile(mixed._h, nrhs)
     prof_f64 = factor_profile(f64._h) if out_fp64 is not None else None
     peaks = {}
     try:
@@ -330,6 +331,7 @@ def main():
             "roofline": roofline,
             "profile_mixed": prof_mixed,
             "profile_fp64": prof_f64,
+            "solve_profile_mixed": sprof_mixed,
             "cpu_baseline": cpu_base,
             "gpu_launches": int(info.n_factor_launches),
         }

@@ -147,6 +147,11 @@ void* rslab_factor_stream(const rslab_fac_handle* fac);
  * [2] BK panel getf2, [3] deep-row replay, [4] in-panel Schur, [5] total).
  * A measurement aid with no reference counterpart. */
 int rslab_factor_profile(rslab_fac_handle* fac, double* kind_ms, int64_t* kind_launches, double* kind_flops);
+/* Eager solve with per-launch CUDA events ([0] permute in/out, [1] forward
+ * diagonal, [2] forward push, [3] D solve, [4] backward off-diagonal dots,
+ * [5] backward diagonal, [6] total).  A measurement aid with no reference
+ * counterpart. */
+int rslab_solve_profile(rslab_fac_handle* fac, int64_t nrhs, double* kind_ms, int64_t* kind_launches);
 /* Reference LdltFactors layout; pass NULL arrays to query *nnz_out first. */
 int rslab_export_factors(const rslab_fac_handle* fac, int64_t* l_col_ptr, int64_t* l_row_idx, void* l_values,
                          void* d_diag, void* d_subdiag, uint8_t* two_by_two, int64_t* perm, double* scale,

@@ -117,8 +117,9 @@ __global__ void k_demote<c64, c32>(long long nnz, const c64* __restrict__ a, c32
 // (rows ty + 16*ii, cols tx + 16*jj).
 // ---------------------------------------------------------------------------
 
-template <typename T> struct KChunk { static constexpr int v = 16; };
-template <> struct KChunk<c64> { static constexpr int v = 8; };
+// Inner-dimension chunk of the tile engine (elements of T per A/B row).
+template <typename T> struct KChunk { static constexpr int v = 32; };
+template <> struct KChunk<c64> { static constexpr int v = 16; };
 
 // G(j, t) for column t of a factored panel with block-diagonal D.
 template <typename T>
@@ -136,12 +137,15 @@ __device__ __forceinline__ T ld_G(const T* __restrict__ L, long long ld, int j, 
   return F::add(F::mul(dsub[t - 1], p), F::mul(d[t], a));
 }
 
+// acc[i][j] = sum_t A(i,t) * B(j,t) over t in [0, kdim) for i, j < 64.
 // A rows  : L_A + i (i < arows), column t at stride lda
 // B rows  : L_B + j (j < brows), column t at stride ldb
 // D (indexed by t) multiplies the B operand (D_ON_A = false: the cmod form
 // U = L_k G^T, G = L_k D) or the A operand (D_ON_A = true: the deferred
 // panel Schur tmp = (L21 D) L21^T).  Accumulation is one explicit FMA per t in
-// ascending t, the same order as the oracle.
+// ascending t, the same order as the oracle.  256 threads, 4x4 register
+// micro-tiles (rows ty + 16*ii, cols tx + 16*jj); the next chunk is fetched
+// into registers while the current one is multiplied out of shared memory.
 template <typename T, bool D_ON_A = false>
 __device__ void tile_product(T (&acc)[4][4], const T* __restrict__ LA, long long lda, int arows,
                              const T* __restrict__ LB, long long ldb, int brows, int kdim,
@@ -149,41 +153,69 @@ __device__ void tile_product(T (&acc)[4][4], const T* __restrict__ LA, long long
                              const unsigned char* __restrict__ kind, T* As, T* Bs) {
   using F = Field<T>;
   constexpr int KT = KChunk<T>::v;
+  constexpr int PER = KT * TILE / TPB;  // elements of each operand staged per thread
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = F::zero();
-  for (int t0 = 0; t0 < kdim; t0 += KT) {
+  T ra[PER], rb[PER];
+  auto fetch = [&](int t0) {
     const int kt = min(KT, kdim - t0);
-    // Cooperative chunk loads: element e -> (t = e / 64, r = e % 64).
-    for (int e = tid; e < KT * TILE; e += TPB) {
-      int t = e / TILE, r = e % TILE;
-      T av = F::zero(), gv = F::zero();
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int e = tid + q * TPB;
+      const int t = e / TILE, r = e % TILE;
+      T av = F::zero(), bv = F::zero();
       if (t < kt) {
         if constexpr (D_ON_A) {
           if (r < arows) av = ld_G(LA, lda, r, t0 + t, d, dsub, kind);
-          if (r < brows) gv = LB[r + (long long)(t0 + t) * ldb];
+          if (r < brows) bv = LB[r + (long long)(t0 + t) * ldb];
         } else {
           if (r < arows) av = LA[r + (long long)(t0 + t) * lda];
-          if (r < brows) gv = ld_G(LB, ldb, r, t0 + t, d, dsub, kind);
+          if (r < brows) bv = ld_G(LB, ldb, r, t0 + t, d, dsub, kind);
         }
       }
-      As[t * TILE + r] = av;
-      Bs[t * TILE + r] = gv;
+      ra[q] = av;
+      rb[q] = bv;
+    }
+  };
+  if (kdim > 0) fetch(0);
+  for (int t0 = 0; t0 < kdim; t0 += KT) {
+    const int kt = min(KT, kdim - t0);
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int e = tid + q * TPB;
+      As[e] = ra[q];
+      Bs[e] = rb[q];
     }
     __syncthreads();
-#pragma unroll 4
-    for (int t = 0; t < kt; ++t) {
-      T a[4], b[4];
+    if (t0 + KT < kdim) fetch(t0 + KT);
+    if (kt == KT) {
+#pragma unroll 8
+      for (int t = 0; t < KT; ++t) {
+        T a[4], b[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[t * TILE + ty + 16 * i];
+        for (int i = 0; i < 4; ++i) a[i] = As[t * TILE + ty + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[t * TILE + tx + 16 * j];
+        for (int j = 0; j < 4; ++j) b[j] = Bs[t * TILE + tx + 16 * j];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = F::fma_(a[i], b[j], acc[i][j]);
+          for (int j = 0; j < 4; ++j) acc[i][j] = F::fma_(a[i], b[j], acc[i][j]);
+      }
+    } else {
+      for (int t = 0; t < kt; ++t) {
+        T a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = As[t * TILE + ty + 16 * i];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = Bs[t * TILE + tx + 16 * j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = F::fma_(a[i], b[j], acc[i][j]);
+      }
     }
     __syncthreads();
   }
@@ -618,27 +650,36 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
   __syncthreads();
   const double alpha = (1.0 + sqrt(17.0)) / 8.0;
   int nperturbed = 0;
-  int k = 0;
-  while (k < pw) {
-    // colmax over in-panel rows (k+1)..pw.
-    double v = -1.0;
-    int idx = INT_MAX;
-    for (int i = k + 1 + tid; i < pw; i += NT) argmax_combine(v, idx, F::mag2(A[pk(i, k, pw)]), i);
-    block_argmax<NT>(v, idx, red_v, red_i);
-    if (tid == 0) {
-      double absakk = F::mag(A[pk(k, k, pw)]);
-      double colmax_sq = v > 0.0 ? v : 0.0;
-      int imax = v > 0.0 ? idx : k;
-      double colmax = sqrt(colmax_sq);
+  // The sequential pivot loop runs in warp 0 alone: arg-max / max reductions
+  // and broadcasts are shuffles, ordering is __syncwarp, so a pivot step costs
+  // no block-wide barrier.  Decisions and arithmetic are the reference's.
+  if (warp == 0) {
+    int k = 0;
+    while (k < pw) {
+      double v = -1.0;
+      int idx = INT_MAX;
+      for (int i = k + 1 + lane; i < pw; i += 32) argmax_combine(v, idx, F::mag2(A[pk(i, k, pw)]), i);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
+        argmax_combine(v, idx, v2, i2);
+      }
+      const double absakk = F::mag(A[pk(k, k, pw)]);
+      const double colmax = sqrt(v > 0.0 ? v : 0.0);
+      const int imax = v > 0.0 ? idx : k;
       int kstep = 1, kp = k;
+      bool err = false;
       if (fmax(absakk, colmax) == 0.0) {
-        if (fa.perturb_floor < 0.0) ctl[3] = 1;
+        err = fa.perturb_floor < 0.0;
       } else if (absakk >= alpha * colmax) {
       } else {
         double rmx = 0.0;
-        for (int j = k; j < imax; ++j) rmx = fmax(rmx, F::mag2(A[pk(imax, j, pw)]));
-        for (int i = imax + 1; i < pw; ++i) rmx = fmax(rmx, F::mag2(A[pk(i, imax, pw)]));
-        double rowmax = sqrt(rmx);
+        for (int jj = k + lane; jj < imax; jj += 32) rmx = fmax(rmx, F::mag2(A[pk(imax, jj, pw)]));
+        for (int ii = imax + 1 + lane; ii < pw; ii += 32) rmx = fmax(rmx, F::mag2(A[pk(ii, imax, pw)]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) rmx = fmax(rmx, __shfl_xor_sync(0xffffffffu, rmx, o));
+        const double rowmax = sqrt(rmx);
         if (absakk >= alpha * colmax * (colmax / rowmax)) {
         } else if (F::mag(A[pk(imax, imax, pw)]) >= alpha * rowmax) {
           kp = imax;
@@ -647,137 +688,134 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
           kp = imax;
         }
       }
-      ctl[0] = kstep;
-      ctl[1] = kp;
-    }
-    __syncthreads();
-    if (ctl[3]) break;
-    const int kstep = ctl[0], kp = ctl[1];
-    const int p = kstep == 1 ? k : k + 1;
-    if (kp != p) {
-      // swap_sym_lower_bounded(p, kp) restricted to the block + left segments.
-      const int q = kp;
-      for (int i = q + 1 + tid; i < pw; i += NT) {
-        T t = A[pk(i, p, pw)];
-        A[pk(i, p, pw)] = A[pk(i, q, pw)];
-        A[pk(i, q, pw)] = t;
+      if (err) {
+        if (lane == 0) ctl[3] = 1;
+        break;
       }
-      for (int i = p + 1 + tid; i < q; i += NT) {
-        T t = A[pk(i, p, pw)];
-        A[pk(i, p, pw)] = A[pk(q, i, pw)];
-        A[pk(q, i, pw)] = t;
+      const int p = kstep == 1 ? k : k + 1;
+      if (kp != p) {
+        // swap_sym_lower_bounded(p, kp) restricted to the block + left segments.
+        const int q = kp;
+        for (int i = q + 1 + lane; i < pw; i += 32) {
+          T t = A[pk(i, p, pw)];
+          A[pk(i, p, pw)] = A[pk(i, q, pw)];
+          A[pk(i, q, pw)] = t;
+        }
+        for (int i = p + 1 + lane; i < q; i += 32) {
+          T t = A[pk(i, p, pw)];
+          A[pk(i, p, pw)] = A[pk(q, i, pw)];
+          A[pk(q, i, pw)] = t;
+        }
+        for (int jj = lane; jj < p; jj += 32) {
+          T t = A[pk(p, jj, pw)];
+          A[pk(p, jj, pw)] = A[pk(q, jj, pw)];
+          A[pk(q, jj, pw)] = t;
+        }
+        if (lane == 0) {
+          T t = A[pk(p, p, pw)];
+          A[pk(p, p, pw)] = A[pk(q, q, pw)];
+          A[pk(q, q, pw)] = t;
+          int lpv = lpermG[kb + p];
+          lpermG[kb + p] = lpermG[kb + q];
+          lpermG[kb + q] = lpv;
+          swaps[k] = kb + q;
+          const int ns = ctl[2];
+          swp_p[ns] = kb + p;
+          swp_q[ns] = kb + q;
+          ctl[2] = ns + 1;
+        }
+        __syncwarp();
       }
-      for (int j = tid; j < p; j += NT) {
-        T t = A[pk(p, j, pw)];
-        A[pk(p, j, pw)] = A[pk(q, j, pw)];
-        A[pk(q, j, pw)] = t;
-      }
-      if (tid == 0) {
-        T t = A[pk(p, p, pw)];
-        A[pk(p, p, pw)] = A[pk(q, q, pw)];
-        A[pk(q, q, pw)] = t;
-        int lp = lpermG[kb + p];
-        lpermG[kb + p] = lpermG[kb + q];
-        lpermG[kb + q] = lp;
-        swaps[k] = kb + q;
-        int ns = ctl[2];
-        swp_p[ns] = kb + p;
-        swp_q[ns] = kb + q;
-        ctl[2] = ns + 1;
-      }
-      __syncthreads();
-    }
-    if (kstep == 1) {
-      T dk = A[pk(k, k, pw)];
-      if (fa.perturb_floor >= 0.0) {
-        double m = F::mag(dk);
-        if (m < fa.perturb_floor) {
-          dk = m == 0.0 ? F::from_real(fa.perturb_floor) : F::scale(dk, fa.perturb_floor / m);
-          if (tid == 0) {
-            A[pk(k, k, pw)] = dk;
-            ++nperturbed;
+      if (kstep == 1) {
+        T dk = A[pk(k, k, pw)];
+        if (fa.perturb_floor >= 0.0) {
+          const double m = F::mag(dk);
+          if (m < fa.perturb_floor) {
+            dk = m == 0.0 ? F::from_real(fa.perturb_floor) : F::scale(dk, fa.perturb_floor / m);
+            __syncwarp();
+            if (lane == 0) {
+              A[pk(k, k, pw)] = dk;
+              ++nperturbed;
+            }
+          }
+        } else if (F::is_zero(dk)) {
+          if (lane == 0) ctl[3] = 1;
+          break;
+        }
+        const T dinv = F::recip(dk);
+        if (lane == 0) dG[k] = dk;
+        for (int jj = k + 1 + lane; jj < pw; jj += 32) {
+          const T w = F::mul(A[pk(jj, k, pw)], dinv);
+          l1[jj] = w;
+          snap[k * nb + jj] = w;
+        }
+        __syncwarp();
+        for (int jj = k + 1; jj < pw; ++jj) {
+          const T w = l1[jj];
+          if (F::is_zero(w)) continue;
+          for (int i = jj + lane; i < pw; i += 32) A[pk(i, jj, pw)] = F::sub(A[pk(i, jj, pw)], F::mul(A[pk(i, k, pw)], w));
+        }
+        __syncwarp();
+        for (int i = k + 1 + lane; i < pw; i += 32) A[pk(i, k, pw)] = F::mul(A[pk(i, k, pw)], dinv);
+        __syncwarp();
+        k += 1;
+      } else {
+        T d11 = A[pk(k, k, pw)], d21 = A[pk(k + 1, k, pw)], d22 = A[pk(k + 1, k + 1, pw)];
+        T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
+        const double scale = fmax(fmax(F::mag(d11), F::mag(d22)), F::mag(d21));
+        const double growth_floor = 1e-14 * scale * scale;
+        if (fa.perturb_floor >= 0.0) {
+          const double fl = fmax(fa.perturb_floor * fa.perturb_floor, growth_floor);
+          if (F::mag(det) < fl) {
+            const double lift = fmax(fa.perturb_floor, scale * sqrt(1e-14));
+            d11 = F::add(d11, F::from_real(lift));
+            d22 = F::add(d22, F::from_real(lift));
+            det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
+            if (F::mag(det) < fl) det = F::add(det, F::from_real(fl));
+            if (lane == 0) ++nperturbed;
+          }
+        } else if (F::mag(det) <= growth_floor) {
+          if (lane == 0) ctl[3] = 1;
+          break;
+        }
+        const T detinv = F::recip(det);
+        if (lane == 0) {
+          dG[k] = d11;
+          dsG[k] = d21;
+          dG[k + 1] = d22;
+          kindG[k] = 1;
+          kindG[k + 1] = 2;
+        }
+        for (int i = k + 2 + lane; i < pw; i += 32) {
+          const T wik = A[pk(i, k, pw)], wik1 = A[pk(i, k + 1, pw)];
+          const T a1 = F::mul(F::sub(F::mul(d22, wik), F::mul(d21, wik1)), detinv);
+          const T a2 = F::mul(F::sub(F::mul(d11, wik1), F::mul(d21, wik)), detinv);
+          l1[i] = a1;
+          l2[i] = a2;
+          snap[k * nb + i] = a1;
+          snap[(k + 1) * nb + i] = a2;
+        }
+        __syncwarp();
+        for (int jj = k + 2; jj < pw; ++jj) {
+          const T a1 = l1[jj], a2 = l2[jj];
+          for (int i = jj + lane; i < pw; i += 32) {
+            T x = A[pk(i, jj, pw)];
+            x = F::sub(x, F::mul(A[pk(i, k, pw)], a1));
+            x = F::sub(x, F::mul(A[pk(i, k + 1, pw)], a2));
+            A[pk(i, jj, pw)] = x;
           }
         }
-      } else if (F::is_zero(dk)) {
-        if (tid == 0) ctl[3] = 1;
-        __syncthreads();
-        break;
-      }
-      const T dinv = F::recip(dk);
-      if (tid == 0) dG[k] = dk;
-      // multipliers w_j = A(j,k) / d_k for j > k (snapshot), stored in l1.
-      for (int j = k + 1 + tid; j < pw; j += NT) {
-        T w = F::mul(A[pk(j, k, pw)], dinv);
-        l1[j] = w;
-        snap[k * nb + j] = w;
-      }
-      __syncthreads();
-      // rank-1 trailing update of the block: A(i,j) -= A(i,k) w_j, i >= j > k.
-      for (int j = k + 1 + warp; j < pw; j += NW) {
-        T w = l1[j];
-        if (F::is_zero(w)) continue;
-        for (int i = j + lane; i < pw; i += 32) A[pk(i, j, pw)] = F::sub(A[pk(i, j, pw)], F::mul(A[pk(i, k, pw)], w));
-      }
-      __syncthreads();
-      for (int i = k + 1 + tid; i < pw; i += NT) A[pk(i, k, pw)] = F::mul(A[pk(i, k, pw)], dinv);
-      __syncthreads();
-      k += 1;
-    } else {
-      T d11 = A[pk(k, k, pw)], d21 = A[pk(k + 1, k, pw)], d22 = A[pk(k + 1, k + 1, pw)];
-      T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
-      double scale = fmax(fmax(F::mag(d11), F::mag(d22)), F::mag(d21));
-      double growth_floor = 1e-14 * scale * scale;
-      if (fa.perturb_floor >= 0.0) {
-        double fl = fmax(fa.perturb_floor * fa.perturb_floor, growth_floor);
-        if (F::mag(det) < fl) {
-          double lift = fmax(fa.perturb_floor, scale * sqrt(1e-14));
-          d11 = F::add(d11, F::from_real(lift));
-          d22 = F::add(d22, F::from_real(lift));
-          det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
-          if (F::mag(det) < fl) det = F::add(det, F::from_real(fl));
-          if (tid == 0) ++nperturbed;
+        __syncwarp();
+        for (int i = k + 2 + lane; i < pw; i += 32) {
+          A[pk(i, k, pw)] = l1[i];
+          A[pk(i, k + 1, pw)] = l2[i];
         }
-      } else if (F::mag(det) <= growth_floor) {
-        if (tid == 0) ctl[3] = 1;
-        __syncthreads();
-        break;
+        __syncwarp();
+        k += 2;
       }
-      const T detinv = F::recip(det);
-      if (tid == 0) {
-        dG[k] = d11;
-        dsG[k] = d21;
-        dG[k + 1] = d22;
-        kindG[k] = 1;
-        kindG[k + 1] = 2;
-      }
-      for (int i = k + 2 + tid; i < pw; i += NT) {
-        T wik = A[pk(i, k, pw)], wik1 = A[pk(i, k + 1, pw)];
-        T a1 = F::mul(F::sub(F::mul(d22, wik), F::mul(d21, wik1)), detinv);
-        T a2 = F::mul(F::sub(F::mul(d11, wik1), F::mul(d21, wik)), detinv);
-        l1[i] = a1;
-        l2[i] = a2;
-        snap[k * nb + i] = a1;
-        snap[(k + 1) * nb + i] = a2;
-      }
-      __syncthreads();
-      for (int j = k + 2 + warp; j < pw; j += NW) {
-        T a1 = l1[j], a2 = l2[j];
-        for (int i = j + lane; i < pw; i += 32) {
-          T x = A[pk(i, j, pw)];
-          x = F::sub(x, F::mul(A[pk(i, k, pw)], a1));
-          x = F::sub(x, F::mul(A[pk(i, k + 1, pw)], a2));
-          A[pk(i, j, pw)] = x;
-        }
-      }
-      __syncthreads();
-      for (int i = k + 2 + tid; i < pw; i += NT) {
-        A[pk(i, k, pw)] = l1[i];
-        A[pk(i, k + 1, pw)] = l2[i];
-      }
-      __syncthreads();
-      k += 2;
     }
   }
+  __syncthreads();
   if (ctl[3]) {
     if (tid == 0) {
       if (atomicCAS(&fa.status[0], 0, 1) == 0) fa.status[1] = s;

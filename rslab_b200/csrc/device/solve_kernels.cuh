@@ -22,7 +22,9 @@ namespace rsd {
 
 constexpr int SOLVE_NT = 256;
 constexpr int RHS_MAX = 16;  // right-hand sides per pass (larger counts loop)
-constexpr int SB = 32;       // diagonal-block edge of the blocked solves
+constexpr int SB = 32;       // diagonal-block edge of the in-CTA substitutions
+constexpr int SOLVE_BIG = 128;  // wider supernodes use the multi-CTA blocked diagonal solves
+constexpr int TB = 64;          // block edge of the multi-CTA diagonal solves
 
 struct SolveArgs {
   const int* sn_first;
@@ -112,52 +114,26 @@ __device__ __forceinline__ void reduce_warps(T (&acc)[RHS_MAX], T* red, int nrhs
   __syncthreads();
 }
 
-// Forward step of supernode s (one CTA):
-//  1. pull the descendants' pushes: y[g] -= U_k[r] for every updater k (in
-//     update-list order) and its off-diagonal rows r landing in s's columns;
-//  2. pivot-order unit-lower substitution of the diagonal block in 32-column
-//     blocks (left-looking inside the panel) -> z_s (e order);
-//  3. push: U_s = L21_s z_s for the off-diagonal rows (lanes over rows,
-//     coalesced panel reads), consumed by the ancestors' step 1.
+// Pivot-order unit-lower substitution of columns [j_begin, j_end) of a panel
+// in 32-column blocks (one CTA): z[p] = y[p] - sum_{q in [q_begin, p)} L[p,q] z[q].
+// y comes from the g-ordered RHS through lperm (from_y) or already sits in Z.
 template <typename T>
-__global__ void __launch_bounds__(SOLVE_NT) k_fwd_diag(SolveArgs a, const int* __restrict__ tasks) {
+__device__ void fwd_block_range(const SolveArgs& a, const T* __restrict__ L, int nrow, T* Z, const T* Yfirst,
+                                const int* __restrict__ lp, int j_begin, int j_end, int q_begin, bool from_y, T* red) {
   using F = Field<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* red = reinterpret_cast<T*>(smem_raw);
-  const int s = tasks[blockIdx.x];
-  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
-  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
-  const int* lp = a.lperm + first;
-  T* Y = reinterpret_cast<T*>(a.Yg) + a.c0;
-  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  T* Uall = reinterpret_cast<T*>(a.U) + a.c0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // 1. gather the pushes of the updaters (distinct rows within one updater).
-  for (int u = a.upd_ptr[s]; u < a.upd_ptr[s + 1]; ++u) {
-    const int k = a.upd_k[u], p0 = a.upd_p0[u], p1 = a.upd_p1[u];
-    const int* ok = a.rs + a.sn_rsoff[k] + a.sn_ncol[k];
-    const T* Uk = Uall + a.uoff[k] * a.ld;
-    const int cnt = (p1 - p0) * a.nrhs;
-    for (int e = threadIdx.x; e < cnt; e += SOLVE_NT) {
-      const int r = p0 + e / a.nrhs, c = e % a.nrhs;
-      T* y = Y + (long long)ok[r] * a.ld + c;
-      *y = F::sub(*y, Uk[(long long)r * a.ld + c]);
-    }
-    __syncthreads();
-  }
-  // 2. diagonal block.
-  for (int j0 = 0; j0 < ncol; j0 += SB) {
-    const int nb = min(SB, ncol - j0);
+  for (int j0 = j_begin; j0 < j_end; j0 += SB) {
+    const int nb = min(SB, j_end - j0);
     T acc[RHS_MAX];
 #pragma unroll
     for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
-    lane_row_dot<T>(acc, L + j0 + lane, nrow, 0, j0, Z, a.ld, a.nrhs, lane < nb);
+    lane_row_dot<T>(acc, L + j0 + lane, nrow, q_begin, j0, Z, a.ld, a.nrhs, lane < nb);
     reduce_warps<T>(acc, red, a.nrhs);
     if (warp == 0) {
       T z[RHS_MAX];
       const int p = j0 + lane;
       const bool ok = lane < nb;
-      const T* yrow = Y + (long long)(first + (ok ? lp[p] : 0)) * a.ld;
+      const T* yrow = from_y ? Yfirst + (long long)((ok ? lp[p] : 0)) * a.ld : Z + (long long)(ok ? p : 0) * a.ld;
 #pragma unroll
       for (int c = 0; c < RHS_MAX; ++c) z[c] = (ok && c < a.nrhs) ? F::sub(yrow[c], acc[c]) : F::zero();
       for (int q = 0; q < nb; ++q) {
@@ -184,6 +160,51 @@ __global__ void __launch_bounds__(SOLVE_NT) k_fwd_diag(SolveArgs a, const int* _
     }
     __syncthreads();
   }
+}
+
+// Forward step of supernode s (one CTA):
+//  1. pull the descendants' pushes: y[g] -= U_k[r] for every updater k (in
+//     update-list order) and its off-diagonal rows r landing in s's columns;
+//  2. pivot-order unit-lower substitution of the diagonal block in 32-column
+//     blocks (left-looking inside the panel) -> z_s (e order); supernodes
+//     wider than SOLVE_BIG only stage y here and are solved by the blocked
+//     multi-CTA kernels k_ftrsv_blk / k_ftrsv_upd.
+// The push U_s = L21_s z_s (k_fwd_push) follows as a separate launch.
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_NT) k_fwd_diag(SolveArgs a, const int* __restrict__ tasks) {
+  using F = Field<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* red = reinterpret_cast<T*>(smem_raw);
+  const int s = tasks[blockIdx.x];
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
+  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
+  const int* lp = a.lperm + first;
+  T* Y = reinterpret_cast<T*>(a.Yg) + a.c0;
+  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
+  T* Uall = reinterpret_cast<T*>(a.U) + a.c0;
+  // 1. gather the pushes of the updaters (distinct rows within one updater).
+  for (int u = a.upd_ptr[s]; u < a.upd_ptr[s + 1]; ++u) {
+    const int k = a.upd_k[u], p0 = a.upd_p0[u], p1 = a.upd_p1[u];
+    const int* ok = a.rs + a.sn_rsoff[k] + a.sn_ncol[k];
+    const T* Uk = Uall + a.uoff[k] * a.ld;
+    const int cnt = (p1 - p0) * a.nrhs;
+    for (int e = threadIdx.x; e < cnt; e += SOLVE_NT) {
+      const int r = p0 + e / a.nrhs, c = e % a.nrhs;
+      T* y = Y + (long long)ok[r] * a.ld + c;
+      *y = F::sub(*y, Uk[(long long)r * a.ld + c]);
+    }
+    __syncthreads();
+  }
+  // 2. diagonal block: in this CTA for narrow supernodes; wide ones only
+  //    stage y in pivot order into Z for the blocked multi-CTA solve.
+  if (ncol > SOLVE_BIG) {
+    for (int e = threadIdx.x; e < ncol * a.nrhs; e += SOLVE_NT) {
+      const int p = e / a.nrhs, c = e % a.nrhs;
+      Z[(long long)p * a.ld + c] = Y[(long long)(first + lp[p]) * a.ld + c];
+    }
+    return;
+  }
+  fwd_block_range<T>(a, L, nrow, Z, Y + (long long)first * a.ld, lp, 0, ncol, 0, true, red);
 }
 
 // Forward push of supernode s, rows [ncol + r0, ncol + r0 + 64):
@@ -244,6 +265,7 @@ __global__ void __launch_bounds__(SOLVE_NT) k_bwd_off(SolveArgs a, const int2* _
   const int* rss = a.rs + a.sn_rsoff[s];
   const T* X = reinterpret_cast<const T*>(a.Xg) + a.c0;
   T* Wb = reinterpret_cast<T*>(a.Wb) + a.c0 + (long long)first * a.ld;
+  T* Zs = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NW = SOLVE_NT / 32;
   const int cols_here = min(32, ncol - c0);
@@ -273,7 +295,211 @@ __global__ void __launch_bounds__(SOLVE_NT) k_bwd_off(SolveArgs a, const int2* _
           x += __shfl_down_sync(0xffffffffu, x, o);
         }
       }
-      if (lane == 0) Wb[(long long)p * a.ld + c] = x;
+      if (lane == 0) {
+        if (ncol > SOLVE_BIG) {
+          T* z = Zs + (long long)p * a.ld + c;
+          *z = F::sub(*z, x);
+        } else {
+          Wb[(long long)p * a.ld + c] = x;
+        }
+      }
+    }
+  }
+}
+
+// Blocked forward solve of a wide supernode, block [j0, j0+64): in-block
+// substitution on Z (which already holds y minus the earlier blocks).
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_NT) k_ftrsv_blk(SolveArgs a, const int4* __restrict__ tasks) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* red = reinterpret_cast<T*>(smem_raw);
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, j0 = tk.y;
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
+  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
+  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
+  fwd_block_range<T>(a, L, nrow, Z, nullptr, nullptr, j0, min(j0 + TB, ncol), j0, false, red);
+}
+
+// Right-looking update after forward block [j0, j0+64) of a wide supernode:
+// Z[r] -= sum_{q in block} L[r, q] z[q] for own rows r in [r0, r0+64).
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_NT) k_ftrsv_upd(SolveArgs a, const int4* __restrict__ tasks) {
+  using F = Field<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* red = reinterpret_cast<T*>(smem_raw);  // [4 splits][64 rows][RHS_MAX]
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, j0 = tk.y, r0 = tk.z;
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
+  const int j1 = min(j0 + TB, ncol);
+  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
+  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rg = warp & 1, qs = warp >> 1;
+  const int rl = rg * 32 + lane;
+  const int r = r0 + rl;
+  const bool ok = r < ncol;
+  T acc[RHS_MAX];
+#pragma unroll
+  for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
+  for (int q = j0 + qs; q < j1; q += 4) {
+    T l = ok ? L[r + (long long)q * nrow] : F::zero();
+    const T* zq = Z + (long long)q * a.ld;
+#pragma unroll
+    for (int c = 0; c < RHS_MAX; ++c)
+      if (c < a.nrhs) acc[c] = F::fma_(l, zq[c], acc[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < RHS_MAX; ++c)
+    if (c < a.nrhs) red[(qs * 64 + rl) * RHS_MAX + c] = acc[c];
+  __syncthreads();
+  for (int e = threadIdx.x; e < 64 * a.nrhs; e += SOLVE_NT) {
+    const int row = e / a.nrhs, c = e % a.nrhs;
+    const int rr = r0 + row;
+    if (rr >= ncol) continue;
+    T v = red[(0 * 64 + row) * RHS_MAX + c];
+    v = F::add(v, red[(1 * 64 + row) * RHS_MAX + c]);
+    v = F::add(v, red[(2 * 64 + row) * RHS_MAX + c]);
+    v = F::add(v, red[(3 * 64 + row) * RHS_MAX + c]);
+    T* z = Z + (long long)rr * a.ld + c;
+    *z = F::sub(*z, v);
+  }
+}
+
+// Blocked backward solve of a wide supernode, block [j0, j0+64): in-block
+// substitution with L^T (v already holds w - L21^T x - later blocks), then
+// the block's final values go to X in g order.
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_NT) k_btrsv_blk(SolveArgs a, const int4* __restrict__ tasks) {
+  using F = Field<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* red = reinterpret_cast<T*>(smem_raw);
+  T* vb = red + (SOLVE_NT / 32) * 32 * RHS_MAX;
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, jb = tk.y;
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
+  const int je = min(jb + TB, ncol);
+  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
+  const int* lp = a.lperm + first;
+  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
+  T* Xw = reinterpret_cast<T*>(a.Xg) + a.c0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = SOLVE_NT / 32;
+  const int nblk = (je - jb + SB - 1) / SB;
+  for (int b = nblk - 1; b >= 0; --b) {
+    const int j0 = jb + b * SB, nb = min(SB, je - j0), j1 = j0 + nb;
+    for (int pc = warp; pc < nb; pc += NW) {
+      const int p = j0 + pc;
+      T acc[RHS_MAX];
+#pragma unroll
+      for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
+      const T* Lc = L + (long long)p * nrow;
+      for (int r = j1 + lane; r < je; r += 32) {
+        T l = Lc[r];
+        const T* v = Z + (long long)r * a.ld;
+#pragma unroll
+        for (int c = 0; c < RHS_MAX; ++c)
+          if (c < a.nrhs) acc[c] = F::fma_(l, v[c], acc[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < RHS_MAX; ++c) {
+        if (c >= a.nrhs) continue;
+        T x = acc[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          if constexpr (Field<T>::complex) {
+            x.re += __shfl_down_sync(0xffffffffu, x.re, o);
+            x.im += __shfl_down_sync(0xffffffffu, x.im, o);
+          } else {
+            x += __shfl_down_sync(0xffffffffu, x, o);
+          }
+        }
+        if (lane == 0) vb[pc * RHS_MAX + c] = x;
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {
+      const int p = j0 + lane;
+      const bool ok = lane < nb;
+      T v[RHS_MAX];
+#pragma unroll
+      for (int c = 0; c < RHS_MAX; ++c)
+        v[c] = (ok && c < a.nrhs) ? F::sub(Z[(long long)p * a.ld + c], vb[lane * RHS_MAX + c]) : F::zero();
+      for (int q = nb - 1; q >= 1; --q) {
+        const int qq = j0 + q;
+        T l = F::zero();
+        if (ok && lane < q) l = L[qq + (long long)p * nrow];
+#pragma unroll
+        for (int c = 0; c < RHS_MAX; ++c) {
+          if (c >= a.nrhs) continue;
+          T vq;
+          if constexpr (Field<T>::complex) {
+            vq.re = __shfl_sync(0xffffffffu, v[c].re, q);
+            vq.im = __shfl_sync(0xffffffffu, v[c].im, q);
+          } else {
+            vq = __shfl_sync(0xffffffffu, v[c], q);
+          }
+          v[c] = F::fnma(l, vq, v[c]);
+        }
+      }
+      if (ok) {
+        T* xo = Xw + (long long)(first + lp[p]) * a.ld;
+#pragma unroll
+        for (int c = 0; c < RHS_MAX; ++c)
+          if (c < a.nrhs) {
+            Z[(long long)p * a.ld + c] = v[c];
+            xo[c] = v[c];
+          }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Right-looking backward update after block [jb, jb+64) of a wide supernode:
+// v[p] -= sum_{r in block} L[r, p] v[r] for columns p in [c0, c0+32) < jb.
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_NT) k_btrsv_upd(SolveArgs a, const int4* __restrict__ tasks) {
+  using F = Field<T>;
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, jb = tk.y, c0 = tk.z;
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
+  const int je = min(jb + TB, ncol);
+  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
+  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = SOLVE_NT / 32;
+  const int cols_here = min(32, jb - c0);
+  for (int pc = warp; pc < cols_here; pc += NW) {
+    const int p = c0 + pc;
+    T acc[RHS_MAX];
+#pragma unroll
+    for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
+    const T* Lc = L + (long long)p * nrow;
+    for (int r = jb + lane; r < je; r += 32) {
+      T l = Lc[r];
+      const T* v = Z + (long long)r * a.ld;
+#pragma unroll
+      for (int c = 0; c < RHS_MAX; ++c)
+        if (c < a.nrhs) acc[c] = F::fma_(l, v[c], acc[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < RHS_MAX; ++c) {
+      if (c >= a.nrhs) continue;
+      T x = acc[c];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        if constexpr (Field<T>::complex) {
+          x.re += __shfl_down_sync(0xffffffffu, x.re, o);
+          x.im += __shfl_down_sync(0xffffffffu, x.im, o);
+        } else {
+          x += __shfl_down_sync(0xffffffffu, x, o);
+        }
+      }
+      if (lane == 0) {
+        T* z = Z + (long long)p * a.ld + c;
+        *z = F::sub(*z, x);
+      }
     }
   }
 }

@@ -65,7 +65,11 @@ size_t elem_size(int dtype) {
   throw RslabError(Status::InvalidInput, "unknown dtype");
 }
 
-enum LaunchKind { L_CMOD, L_GETF2, L_DEEP, L_SCHUR, L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD };
+enum LaunchKind {
+  L_CMOD, L_GETF2, L_DEEP, L_SCHUR,
+  L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD,
+  L_FTRSV_BLK, L_FTRSV_UPD, L_BTRSV_BLK, L_BTRSV_UPD
+};
 struct Launch {
   int kind;
   long long task_off;  // into the int4 / int2 / int task arrays
@@ -97,6 +101,7 @@ struct rslab_sym_handle {
   std::vector<int4> cpairs;   // cmod (k, a, q0, nr << 16 | nc) per tile, in update order
   std::vector<int> t1;
   std::vector<int2> t2;
+  std::vector<int4> st4;  // blocked diagonal-solve tasks (s, j0, r0 | c0, 0)
   std::vector<long long> uoff;  // forward-push row offsets (nrow - ncol per supernode)
   long long urows = 0;
   std::vector<Launch> fplan, fwdplan, bwdplan;
@@ -120,6 +125,7 @@ struct rslab_sym_handle {
   int4* d_cpairs = nullptr;
   int* d_t1 = nullptr;
   int2* d_t2 = nullptr;
+  int4* d_st4 = nullptr;
   long long* d_uoff = nullptr;
   std::mutex mu;
   rslab_analyze_settings settings{};
@@ -170,6 +176,7 @@ struct rslab_sym_handle {
     d_cpairs = up(cpairs, st);
     d_t1 = up(t1, st);
     d_t2 = up(t2, st);
+    d_st4 = up(st4, st);
     d_uoff = up(uoff, st);
     CK(cudaStreamSynchronize(st));
     device = dev;
@@ -251,7 +258,7 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
   const int nb_small = H.panel_nb, nb_big = std::max(H.panel_nb, 128);
   H.max_nb = nb_big;
   auto nb_of = [&](int s) { return S.sn[s].ncol >= 512 ? nb_big : nb_small; };
-  std::vector<std::pair<Launch, Launch>> lvl_ranges;
+  std::vector<std::vector<Launch>> bw_levels;
   for (const auto& lvl : S.by_level) {
     // cmod tiles of every panel that has updaters, each with its precomputed
     // list of (updater, row run, column run) pairs in update-list order.
@@ -356,35 +363,75 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         H.fplan.push_back(C);
       }
     }
-    // Solve launches for this level: forward = diagonal blocks, then the
-    // row-tiled push; backward (run root first) = column-chunked
-    // off-diagonal dots, then the diagonal blocks.
+    // Solve launches for this level.  Forward: diagonal blocks (one CTA per
+    // narrow supernode; wide ones get the blocked multi-CTA solve), then the
+    // row-tiled push.  Backward (run root first): column-chunked off-diagonal
+    // dots, narrow diagonal blocks, then the wide ones block by block.
     {
       Launch Dg{L_FWD_DIAG, (long long)H.t1.size(), (int)lvl.size(), 0};
       for (int64_t s : lvl) H.t1.push_back((int)s);
       H.fwdplan.push_back(Dg);
+      int maxb = 0;
+      for (int64_t s : lvl)
+        if (S.sn[s].ncol > SOLVE_BIG) maxb = std::max(maxb, (int)((S.sn[s].ncol + TB - 1) / TB));
+      for (int b = 0; b < maxb; ++b) {
+        Launch Fb{L_FTRSV_BLK, (long long)H.st4.size(), 0, 0};
+        for (int64_t s : lvl)
+          if (S.sn[s].ncol > SOLVE_BIG && b * TB < S.sn[s].ncol) H.st4.push_back(make_int4((int)s, b * TB, 0, 0));
+        Fb.ntasks = (int)(H.st4.size() - Fb.task_off);
+        H.fwdplan.push_back(Fb);
+        Launch Fu{L_FTRSV_UPD, (long long)H.st4.size(), 0, 0};
+        for (int64_t s : lvl) {
+          const int nc = (int)S.sn[s].ncol;
+          if (nc <= SOLVE_BIG) continue;
+          for (int r0 = (b + 1) * TB; r0 < nc; r0 += 64) H.st4.push_back(make_int4((int)s, b * TB, r0, 0));
+        }
+        Fu.ntasks = (int)(H.st4.size() - Fu.task_off);
+        if (Fu.ntasks) H.fwdplan.push_back(Fu);
+      }
       Launch Pu{L_FWD_PUSH, (long long)H.t2.size(), 0, 0};
       for (int64_t s : lvl)
         for (int r0 = 0; r0 < H.nrow[s] - S.sn[s].ncol; r0 += 64) H.t2.push_back(make_int2((int)s, r0));
       Pu.ntasks = (int)(H.t2.size() - Pu.task_off);
       if (Pu.ntasks) H.fwdplan.push_back(Pu);
+
+      std::vector<Launch> bw;
       Launch Bo{L_BWD_OFF, (long long)H.t2.size(), 0, 0};
       for (int64_t s : lvl)
         if (H.nrow[s] > S.sn[s].ncol)
           for (int c0 = 0; c0 < S.sn[s].ncol; c0 += 32) H.t2.push_back(make_int2((int)s, c0));
       Bo.ntasks = (int)(H.t2.size() - Bo.task_off);
-      lvl_ranges.push_back({Bo, Launch{L_BWD, Dg.task_off, Dg.ntasks, 0}});
+      if (Bo.ntasks) bw.push_back(Bo);
+      Launch Bd{L_BWD, (long long)H.t1.size(), 0, 0};
+      for (int64_t s : lvl)
+        if (S.sn[s].ncol <= SOLVE_BIG) H.t1.push_back((int)s);
+      Bd.ntasks = (int)(H.t1.size() - Bd.task_off);
+      if (Bd.ntasks) bw.push_back(Bd);
+      for (int b = maxb - 1; b >= 0; --b) {
+        Launch Bb{L_BTRSV_BLK, (long long)H.st4.size(), 0, 0};
+        for (int64_t s : lvl)
+          if (S.sn[s].ncol > SOLVE_BIG && b * TB < S.sn[s].ncol) H.st4.push_back(make_int4((int)s, b * TB, 0, 0));
+        Bb.ntasks = (int)(H.st4.size() - Bb.task_off);
+        bw.push_back(Bb);
+        Launch Bu{L_BTRSV_UPD, (long long)H.st4.size(), 0, 0};
+        for (int64_t s : lvl)
+          if (S.sn[s].ncol > SOLVE_BIG && b * TB < S.sn[s].ncol)
+            for (int c0 = 0; c0 < b * TB; c0 += 32) H.st4.push_back(make_int4((int)s, b * TB, c0, 0));
+        Bu.ntasks = (int)(H.st4.size() - Bu.task_off);
+        if (Bu.ntasks) bw.push_back(Bu);
+      }
+      bw_levels.push_back(bw);
     }
   }
   // Backward: levels root first.
-  for (auto it = lvl_ranges.rbegin(); it != lvl_ranges.rend(); ++it) {
-    if (it->first.ntasks) H.bwdplan.push_back(it->first);
-    H.bwdplan.push_back(it->second);
-  }
+  for (auto it = bw_levels.rbegin(); it != bw_levels.rend(); ++it)
+    for (const Launch& L : *it) H.bwdplan.push_back(L);
 }
 
-size_t smem_cmod(size_t es) { return (size_t)TILE * TILE * es + 2 * 16 * TILE * es + 3 * TILE * 4 + 64; }
-size_t smem_schur(size_t es) { return 2 * 16 * TILE * es; }
+// Chunk depth of the tile engine for an element size (KChunk<T>::v).
+size_t kchunk(size_t es) { return es == 16 ? 16 : 32; }
+size_t smem_cmod(size_t es) { return (size_t)TILE * TILE * es + 2 * kchunk(es) * TILE * es + 3 * TILE * 4 + 64; }
+size_t smem_schur(size_t es) { return 2 * kchunk(es) * TILE * es; }
 size_t smem_getf2(size_t es, int nb) {
   size_t a = (size_t)nb * (nb + 1) / 2 * es + 2 * nb * es + 16 + 32 * 8 + 32 * 4 + 16 * 4;
   size_t b = (size_t)(DEEP_R + 1) * nb * es;
@@ -407,6 +454,9 @@ struct KernelSetup {
     CK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
     CK(cudaFuncSetAttribute(k_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
     CK(cudaFuncSetAttribute(k_fwd_push<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_push(es)));
+    CK(cudaFuncSetAttribute(k_ftrsv_upd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_push(es)));
+    CK(cudaFuncSetAttribute(k_ftrsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
+    CK(cudaFuncSetAttribute(k_btrsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
     done = true;
   }
 };
@@ -667,30 +717,54 @@ SolveArgs make_sargs(rslab_fac_handle& F, int ld, int c0, int nr) {
 
 // x = A^-1 b on device buffers (row-major n x nrhs) in the factor's field.
 template <typename T>
-void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs) {
+void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof = nullptr) {
   auto& H = *F.sym;
   const int n = H.n;
   const size_t es = sizeof(T);
   cudaStream_t st = F.st;
+  if (prof) prof->mark(st, -1);
   k_perm_in<T><<<grid1((long long)n * nrhs), 256, 0, st>>>(n, nrhs, H.d_perm, F.scale, b, (T*)F.Yg);
+  if (prof) prof->mark(st, 0);
   for (int c0 = 0; c0 < nrhs; c0 += RHS_MAX) {
     const int nr = std::min(RHS_MAX, nrhs - c0);
     SolveArgs sa = make_sargs<T>(F, nrhs, c0, nr);
     for (const Launch& L : H.fwdplan) {
-      if (L.kind == L_FWD_DIAG)
-        k_fwd_diag<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
-      else
-        k_fwd_push<T><<<L.ntasks, SOLVE_NT, smem_push(es), st>>>(sa, H.d_t2 + L.task_off);
+      switch (L.kind) {
+        case L_FWD_DIAG:
+          k_fwd_diag<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
+          break;
+        case L_FTRSV_BLK:
+          k_ftrsv_blk<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_st4 + L.task_off);
+          break;
+        case L_FTRSV_UPD:
+          k_ftrsv_upd<T><<<L.ntasks, SOLVE_NT, smem_push(es), st>>>(sa, H.d_st4 + L.task_off);
+          break;
+        default:
+          k_fwd_push<T><<<L.ntasks, SOLVE_NT, smem_push(es), st>>>(sa, H.d_t2 + L.task_off);
+      }
+      if (prof) prof->mark(st, L.kind == L_FWD_PUSH ? 2 : 1);
     }
     k_dsolve<T><<<grid1((long long)n * nr), 256, 0, st>>>(n, sa);
+    if (prof) prof->mark(st, 3);
     for (const Launch& L : H.bwdplan) {
-      if (L.kind == L_BWD_OFF)
-        k_bwd_off<T><<<L.ntasks, SOLVE_NT, 0, st>>>(sa, H.d_t2 + L.task_off);
-      else
-        k_bwd<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
+      switch (L.kind) {
+        case L_BWD_OFF:
+          k_bwd_off<T><<<L.ntasks, SOLVE_NT, 0, st>>>(sa, H.d_t2 + L.task_off);
+          break;
+        case L_BTRSV_BLK:
+          k_btrsv_blk<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_st4 + L.task_off);
+          break;
+        case L_BTRSV_UPD:
+          k_btrsv_upd<T><<<L.ntasks, SOLVE_NT, 0, st>>>(sa, H.d_st4 + L.task_off);
+          break;
+        default:
+          k_bwd<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
+      }
+      if (prof) prof->mark(st, L.kind == L_BWD_OFF ? 4 : 5);
     }
   }
   k_perm_out<T><<<grid1((long long)n * nrhs), 256, 0, st>>>(n, nrhs, H.d_perm, F.scale, (const T*)F.Xg, x);
+  if (prof) prof->mark(st, 0);
   CK(cudaGetLastError());
 }
 
@@ -1102,6 +1176,40 @@ int rslab_factor_info(const rslab_fac_handle* F, rslab_factor_info_t* info) {
 }
 
 void* rslab_factor_stream(const rslab_fac_handle* F) { return F ? (void*)F->st : nullptr; }
+
+// One eager solve of the workspace RHS (nrhs columns, filled with ones when
+// fill_ones) with a CUDA event after every launch: device ms and launches per
+// class ([0] permute in/out, [1] forward diagonal, [2] forward push,
+// [3] D solve, [4] backward off-diagonal dots, [5] backward diagonal, [6] total).
+int rslab_solve_profile(rslab_fac_handle* F, int64_t nrhs, double* kind_ms, int64_t* kind_launches) {
+  try {
+    if (!F || nrhs <= 0) throw RslabError(Status::InvalidInput, "bad arguments");
+    Prof prof;
+    dispatch_field(F->dtype, [&](auto z) {
+      using T = decltype(z);
+      KernelSetup<T>::configure();
+      ensure_ws<T>(*F, (int)nrhs);
+      CK(cudaMemsetAsync(F->bdev, 0, (size_t)F->sym->n * nrhs * sizeof(T), F->st));
+      enqueue_solve<T>(*F, (const T*)F->bdev, (T*)F->xdev, (int)nrhs, &prof);
+    });
+    CK(cudaStreamSynchronize(F->st));
+    for (int k = 0; k < 7; ++k) {
+      kind_ms[k] = 0;
+      kind_launches[k] = 0;
+    }
+    for (size_t i = 1; i < prof.ev.size(); ++i) {
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, prof.ev[i - 1], prof.ev[i]));
+      kind_ms[prof.kind[i]] += ms;
+      kind_ms[6] += ms;
+      kind_launches[prof.kind[i]] += 1;
+      kind_launches[6] += 1;
+    }
+    return 0;
+  } catch (const RslabError& e) {
+    return fail(e);
+  }
+}
 
 // One eager (non-graph) refactor of the current values with a CUDA event
 // after every launch: device ms, launch count and algorithmic flops per

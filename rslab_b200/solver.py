@@ -588,6 +588,17 @@ def factor_profile(handle) -> dict:
     return {k: {"ms": ms[i], "launches": int(nl[i]), "flops": fl[i]} for i, k in enumerate(KINDS)}
 
 
+SOLVE_KINDS = ("permute", "fwd_diag", "fwd_push", "dsolve", "bwd_off", "bwd_diag", "total")
+
+
+def solve_profile(handle, nrhs: int) -> dict:
+    """Per-kernel-class device ms and launches of one eager solve."""
+    ms = (C.c_double * 7)()
+    nl = (C.c_int64 * 7)()
+    _check(N.lib.rslab_solve_profile(handle, nrhs, ms, nl))
+    return {k: {"ms": ms[i], "launches": int(nl[i])} for i, k in enumerate(SOLVE_KINDS)}
+
+
 def amd_order(n: int, col_ptr, row_idx) -> tuple:
     """AMD on a full symmetric pattern; returns (perm, stats dict)."""
     cp = _i64(col_ptr)
