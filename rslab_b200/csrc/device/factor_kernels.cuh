@@ -650,12 +650,19 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
   __syncthreads();
   const double alpha = (1.0 + sqrt(17.0)) / 8.0;
   int nperturbed = 0;
-  // The sequential pivot loop runs in warp 0 alone: arg-max / max reductions
-  // and broadcasts are shuffles, ordering is __syncwarp, so a pivot step costs
-  // no block-wide barrier.  Decisions and arithmetic are the reference's.
-  if (warp == 0) {
-    int k = 0;
-    while (k < pw) {
+  // Each pivot step: warp 0 alone does the arg-max / max reductions, the BK
+  // decision, the interchange and the multipliers (shuffles + __syncwarp),
+  // then all warps apply the rank-1 / rank-2 trailing update (warp per
+  // column) and finish column k.  Three block barriers per step; decisions
+  // and arithmetic are the reference's.
+  int* ctlk = ctl + 4;  // [0] k [1] kstep
+  T* dinv_s = reinterpret_cast<T*>(ctl + 8);  // pending scale factor
+  if (tid == 0) ctlk[0] = 0;
+  __syncthreads();
+  for (;;) {
+    const int k = ctlk[0];
+    if (k >= pw || ctl[3]) break;
+    if (warp == 0) {
       double v = -1.0;
       int idx = INT_MAX;
       for (int i = k + 1 + lane; i < pw; i += 32) argmax_combine(v, idx, F::mag2(A[pk(i, k, pw)]), i);
@@ -688,134 +695,149 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
           kp = imax;
         }
       }
-      if (err) {
-        if (lane == 0) ctl[3] = 1;
-        break;
-      }
-      const int p = kstep == 1 ? k : k + 1;
-      if (kp != p) {
-        // swap_sym_lower_bounded(p, kp) restricted to the block + left segments.
-        const int q = kp;
-        for (int i = q + 1 + lane; i < pw; i += 32) {
-          T t = A[pk(i, p, pw)];
-          A[pk(i, p, pw)] = A[pk(i, q, pw)];
-          A[pk(i, q, pw)] = t;
+      if (!err) {
+        const int p = kstep == 1 ? k : k + 1;
+        if (kp != p) {
+          // swap_sym_lower_bounded(p, kp) restricted to the block + left segments.
+          const int q = kp;
+          for (int i = q + 1 + lane; i < pw; i += 32) {
+            T t = A[pk(i, p, pw)];
+            A[pk(i, p, pw)] = A[pk(i, q, pw)];
+            A[pk(i, q, pw)] = t;
+          }
+          for (int i = p + 1 + lane; i < q; i += 32) {
+            T t = A[pk(i, p, pw)];
+            A[pk(i, p, pw)] = A[pk(q, i, pw)];
+            A[pk(q, i, pw)] = t;
+          }
+          for (int jj = lane; jj < p; jj += 32) {
+            T t = A[pk(p, jj, pw)];
+            A[pk(p, jj, pw)] = A[pk(q, jj, pw)];
+            A[pk(q, jj, pw)] = t;
+          }
+          if (lane == 0) {
+            T t = A[pk(p, p, pw)];
+            A[pk(p, p, pw)] = A[pk(q, q, pw)];
+            A[pk(q, q, pw)] = t;
+            int lpv = lpermG[kb + p];
+            lpermG[kb + p] = lpermG[kb + q];
+            lpermG[kb + q] = lpv;
+            swaps[k] = kb + q;
+            const int ns = ctl[2];
+            swp_p[ns] = kb + p;
+            swp_q[ns] = kb + q;
+            ctl[2] = ns + 1;
+          }
+          __syncwarp();
         }
-        for (int i = p + 1 + lane; i < q; i += 32) {
-          T t = A[pk(i, p, pw)];
-          A[pk(i, p, pw)] = A[pk(q, i, pw)];
-          A[pk(q, i, pw)] = t;
-        }
-        for (int jj = lane; jj < p; jj += 32) {
-          T t = A[pk(p, jj, pw)];
-          A[pk(p, jj, pw)] = A[pk(q, jj, pw)];
-          A[pk(q, jj, pw)] = t;
-        }
-        if (lane == 0) {
-          T t = A[pk(p, p, pw)];
-          A[pk(p, p, pw)] = A[pk(q, q, pw)];
-          A[pk(q, q, pw)] = t;
-          int lpv = lpermG[kb + p];
-          lpermG[kb + p] = lpermG[kb + q];
-          lpermG[kb + q] = lpv;
-          swaps[k] = kb + q;
-          const int ns = ctl[2];
-          swp_p[ns] = kb + p;
-          swp_q[ns] = kb + q;
-          ctl[2] = ns + 1;
-        }
-        __syncwarp();
-      }
-      if (kstep == 1) {
-        T dk = A[pk(k, k, pw)];
-        if (fa.perturb_floor >= 0.0) {
-          const double m = F::mag(dk);
-          if (m < fa.perturb_floor) {
-            dk = m == 0.0 ? F::from_real(fa.perturb_floor) : F::scale(dk, fa.perturb_floor / m);
-            __syncwarp();
+        if (kstep == 1) {
+          T dk = A[pk(k, k, pw)];
+          if (fa.perturb_floor >= 0.0) {
+            const double m = F::mag(dk);
+            if (m < fa.perturb_floor) {
+              dk = m == 0.0 ? F::from_real(fa.perturb_floor) : F::scale(dk, fa.perturb_floor / m);
+              __syncwarp();
+              if (lane == 0) {
+                A[pk(k, k, pw)] = dk;
+                ++nperturbed;
+              }
+            }
+          } else if (F::is_zero(dk)) {
+            err = true;
+          }
+          if (!err) {
+            const T dinv = F::recip(dk);
+            for (int jj = k + 1 + lane; jj < pw; jj += 32) {
+              const T w = F::mul(A[pk(jj, k, pw)], dinv);
+              l1[jj] = w;
+              snap[k * nb + jj] = w;
+            }
             if (lane == 0) {
-              A[pk(k, k, pw)] = dk;
-              ++nperturbed;
+              dG[k] = dk;
+              *dinv_s = dinv;
             }
           }
-        } else if (F::is_zero(dk)) {
-          if (lane == 0) ctl[3] = 1;
-          break;
-        }
-        const T dinv = F::recip(dk);
-        if (lane == 0) dG[k] = dk;
-        for (int jj = k + 1 + lane; jj < pw; jj += 32) {
-          const T w = F::mul(A[pk(jj, k, pw)], dinv);
-          l1[jj] = w;
-          snap[k * nb + jj] = w;
-        }
-        __syncwarp();
-        for (int jj = k + 1; jj < pw; ++jj) {
-          const T w = l1[jj];
-          if (F::is_zero(w)) continue;
-          for (int i = jj + lane; i < pw; i += 32) A[pk(i, jj, pw)] = F::sub(A[pk(i, jj, pw)], F::mul(A[pk(i, k, pw)], w));
-        }
-        __syncwarp();
-        for (int i = k + 1 + lane; i < pw; i += 32) A[pk(i, k, pw)] = F::mul(A[pk(i, k, pw)], dinv);
-        __syncwarp();
-        k += 1;
-      } else {
-        T d11 = A[pk(k, k, pw)], d21 = A[pk(k + 1, k, pw)], d22 = A[pk(k + 1, k + 1, pw)];
-        T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
-        const double scale = fmax(fmax(F::mag(d11), F::mag(d22)), F::mag(d21));
-        const double growth_floor = 1e-14 * scale * scale;
-        if (fa.perturb_floor >= 0.0) {
-          const double fl = fmax(fa.perturb_floor * fa.perturb_floor, growth_floor);
-          if (F::mag(det) < fl) {
-            const double lift = fmax(fa.perturb_floor, scale * sqrt(1e-14));
-            d11 = F::add(d11, F::from_real(lift));
-            d22 = F::add(d22, F::from_real(lift));
-            det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
-            if (F::mag(det) < fl) det = F::add(det, F::from_real(fl));
-            if (lane == 0) ++nperturbed;
+        } else {
+          T d11 = A[pk(k, k, pw)], d21 = A[pk(k + 1, k, pw)], d22 = A[pk(k + 1, k + 1, pw)];
+          T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
+          const double scale = fmax(fmax(F::mag(d11), F::mag(d22)), F::mag(d21));
+          const double growth_floor = 1e-14 * scale * scale;
+          if (fa.perturb_floor >= 0.0) {
+            const double fl = fmax(fa.perturb_floor * fa.perturb_floor, growth_floor);
+            if (F::mag(det) < fl) {
+              const double lift = fmax(fa.perturb_floor, scale * sqrt(1e-14));
+              d11 = F::add(d11, F::from_real(lift));
+              d22 = F::add(d22, F::from_real(lift));
+              det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
+              if (F::mag(det) < fl) det = F::add(det, F::from_real(fl));
+              if (lane == 0) ++nperturbed;
+            }
+          } else if (F::mag(det) <= growth_floor) {
+            err = true;
           }
-        } else if (F::mag(det) <= growth_floor) {
-          if (lane == 0) ctl[3] = 1;
-          break;
-        }
-        const T detinv = F::recip(det);
-        if (lane == 0) {
-          dG[k] = d11;
-          dsG[k] = d21;
-          dG[k + 1] = d22;
-          kindG[k] = 1;
-          kindG[k + 1] = 2;
-        }
-        for (int i = k + 2 + lane; i < pw; i += 32) {
-          const T wik = A[pk(i, k, pw)], wik1 = A[pk(i, k + 1, pw)];
-          const T a1 = F::mul(F::sub(F::mul(d22, wik), F::mul(d21, wik1)), detinv);
-          const T a2 = F::mul(F::sub(F::mul(d11, wik1), F::mul(d21, wik)), detinv);
-          l1[i] = a1;
-          l2[i] = a2;
-          snap[k * nb + i] = a1;
-          snap[(k + 1) * nb + i] = a2;
-        }
-        __syncwarp();
-        for (int jj = k + 2; jj < pw; ++jj) {
-          const T a1 = l1[jj], a2 = l2[jj];
-          for (int i = jj + lane; i < pw; i += 32) {
-            T x = A[pk(i, jj, pw)];
-            x = F::sub(x, F::mul(A[pk(i, k, pw)], a1));
-            x = F::sub(x, F::mul(A[pk(i, k + 1, pw)], a2));
-            A[pk(i, jj, pw)] = x;
+          if (!err) {
+            const T detinv = F::recip(det);
+            if (lane == 0) {
+              dG[k] = d11;
+              dsG[k] = d21;
+              dG[k + 1] = d22;
+              kindG[k] = 1;
+              kindG[k + 1] = 2;
+            }
+            for (int i = k + 2 + lane; i < pw; i += 32) {
+              const T wik = A[pk(i, k, pw)], wik1 = A[pk(i, k + 1, pw)];
+              const T a1 = F::mul(F::sub(F::mul(d22, wik), F::mul(d21, wik1)), detinv);
+              const T a2 = F::mul(F::sub(F::mul(d11, wik1), F::mul(d21, wik)), detinv);
+              l1[i] = a1;
+              l2[i] = a2;
+              snap[k * nb + i] = a1;
+              snap[(k + 1) * nb + i] = a2;
+            }
           }
         }
-        __syncwarp();
-        for (int i = k + 2 + lane; i < pw; i += 32) {
-          A[pk(i, k, pw)] = l1[i];
-          A[pk(i, k + 1, pw)] = l2[i];
-        }
-        __syncwarp();
-        k += 2;
+      }
+      if (lane == 0) {
+        if (err) ctl[3] = 1;
+        ctlk[1] = kstep;
       }
     }
+    __syncthreads();
+    if (ctl[3]) break;
+    // Trailing update of step k by all warps; the previous 1x1 step's
+    // column scaling rides along (different columns, no conflict).
+    const int kstep = ctlk[1];
+    if (kstep == 1) {
+      for (int jj = k + 1 + warp; jj < pw; jj += NW) {
+        const T w = l1[jj];
+        if (F::is_zero(w)) continue;
+        for (int i = jj + lane; i < pw; i += 32) A[pk(i, jj, pw)] = F::sub(A[pk(i, jj, pw)], F::mul(A[pk(i, k, pw)], w));
+      }
+    } else {
+      for (int jj = k + 2 + warp; jj < pw; jj += NW) {
+        const T a1 = l1[jj], a2 = l2[jj];
+        for (int i = jj + lane; i < pw; i += 32) {
+          T x = A[pk(i, jj, pw)];
+          x = F::sub(x, F::mul(A[pk(i, k, pw)], a1));
+          x = F::sub(x, F::mul(A[pk(i, k + 1, pw)], a2));
+          A[pk(i, jj, pw)] = x;
+        }
+      }
+    }
+    __syncthreads();
+    // Finish column(s) k: 1x1 -> scale by 1/d (deferred from the update);
+    // 2x2 -> store the multipliers.
+    if (kstep == 1) {
+      const T dinv = *dinv_s;
+      for (int i = k + 1 + tid; i < pw; i += NT) A[pk(i, k, pw)] = F::mul(A[pk(i, k, pw)], dinv);
+    } else {
+      for (int i = k + 2 + tid; i < pw; i += NT) {
+        A[pk(i, k, pw)] = l1[i];
+        A[pk(i, k + 1, pw)] = l2[i];
+      }
+    }
+    if (tid == 0) ctlk[0] = k + kstep;
+    __syncthreads();
   }
-  __syncthreads();
   if (ctl[3]) {
     if (tid == 0) {
       if (atomicCAS(&fa.status[0], 0, 1) == 0) fa.status[1] = s;

@@ -252,12 +252,57 @@ __global__ void __launch_bounds__(SOLVE_NT) k_fwd_push(SolveArgs a, const int2* 
   }
 }
 
+// out[p][c] = sum_{r in [r_begin, r_end)} L[r, p] * V(r)[c] for the 32
+// columns p in [p0, p0+32) of a panel, V(r) = the RHS row of panel row r
+// (gathered through rs for ancestor rows).  32-row chunks of V and of the
+// L tile are staged in shared memory and reused by all 32 columns; thread t
+// owns column t % 32 and right-hand sides t / 32 + 8 i; fixed summation order.
+template <typename T, bool GATHER>
+__device__ void dot_cols_tile(const T* __restrict__ L, int nrow, int p0, int ncols, int r_begin, int r_end,
+                              const T* __restrict__ V, const int* __restrict__ rss, int ld, int nrhs,
+                              T (&acc)[RHS_MAX / 8], T* Ls, T* Vs) {
+  using F = Field<T>;
+  constexpr int NRC = RHS_MAX / 8;
+  const int tid = threadIdx.x, pc = tid & 31, cg = tid >> 5;
+#pragma unroll
+  for (int q = 0; q < NRC; ++q) acc[q] = F::zero();
+  for (int r0 = r_begin; r0 < r_end; r0 += 32) {
+    const int rows = min(32, r_end - r0);
+    for (int e = tid; e < 32 * 32; e += SOLVE_NT) {
+      const int c = e >> 5, r = e & 31;  // column c, row r: coalesced along r
+      Ls[r * 33 + c] = (r < rows && c < ncols) ? L[(r0 + r) + (long long)(p0 + c) * nrow] : F::zero();
+    }
+    for (int e = tid; e < 32 * nrhs; e += SOLVE_NT) {
+      const int r = e / nrhs, c = e % nrhs;
+      T v = F::zero();
+      if (r < rows) {
+        const long long row = GATHER ? (long long)rss[r0 + r] : (long long)(r0 + r);
+        v = V[row * ld + c];
+      }
+      Vs[r * RHS_MAX + c] = v;
+    }
+    __syncthreads();
+    for (int r = 0; r < rows; ++r) {
+      const T l = Ls[r * 33 + pc];
+#pragma unroll
+      for (int q = 0; q < NRC; ++q) {
+        const int c = cg + 8 * q;
+        if (c < nrhs) acc[q] = F::fma_(l, Vs[r * RHS_MAX + c], acc[q]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Backward off-diagonal dots of supernode s, pivot columns [c0, c0+32):
-// W[first + p] = sum_{r >= ncol} L[r, p] x[g_r] (warp per column, lanes
-// over rows, fixed-order shuffle reduction).
+// sum_{r >= ncol} L[r, p] x[g_r] -> Wb (narrow supernodes) or subtracted from
+// Z directly (wide supernodes, solved by the blocked kernels).
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_bwd_off(SolveArgs a, const int2* __restrict__ tasks) {
   using F = Field<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Ls = reinterpret_cast<T*>(smem_raw);  // 32 x 33
+  T* Vs = Ls + 32 * 33;                    // 32 x RHS_MAX
   const int2 tk = tasks[blockIdx.x];
   const int s = tk.x, c0 = tk.y;
   const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
@@ -266,42 +311,21 @@ __global__ void __launch_bounds__(SOLVE_NT) k_bwd_off(SolveArgs a, const int2* _
   const T* X = reinterpret_cast<const T*>(a.Xg) + a.c0;
   T* Wb = reinterpret_cast<T*>(a.Wb) + a.c0 + (long long)first * a.ld;
   T* Zs = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int NW = SOLVE_NT / 32;
   const int cols_here = min(32, ncol - c0);
-  for (int pc = warp; pc < cols_here; pc += NW) {
+  T acc[RHS_MAX / 8];
+  dot_cols_tile<T, true>(L, nrow, c0, cols_here, ncol, nrow, X, rss, a.ld, a.nrhs, acc, Ls, Vs);
+  const int pc = threadIdx.x & 31, cg = threadIdx.x >> 5;
+  if (pc < cols_here) {
     const int p = c0 + pc;
-    T acc[RHS_MAX];
 #pragma unroll
-    for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
-    const T* Lc = L + (long long)p * nrow;
-    for (int r = ncol + lane; r < nrow; r += 32) {
-      T l = Lc[r];
-      const T* xr = X + (long long)rss[r] * a.ld;
-#pragma unroll
-      for (int c = 0; c < RHS_MAX; ++c)
-        if (c < a.nrhs) acc[c] = F::fma_(l, xr[c], acc[c]);
-    }
-#pragma unroll
-    for (int c = 0; c < RHS_MAX; ++c) {
+    for (int q = 0; q < RHS_MAX / 8; ++q) {
+      const int c = cg + 8 * q;
       if (c >= a.nrhs) continue;
-      T x = acc[c];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        if constexpr (Field<T>::complex) {
-          x.re += __shfl_down_sync(0xffffffffu, x.re, o);
-          x.im += __shfl_down_sync(0xffffffffu, x.im, o);
-        } else {
-          x += __shfl_down_sync(0xffffffffu, x, o);
-        }
-      }
-      if (lane == 0) {
-        if (ncol > SOLVE_BIG) {
-          T* z = Zs + (long long)p * a.ld + c;
-          *z = F::sub(*z, x);
-        } else {
-          Wb[(long long)p * a.ld + c] = x;
-        }
+      if (ncol > SOLVE_BIG) {
+        T* z = Zs + (long long)p * a.ld + c;
+        *z = F::sub(*z, acc[q]);
+      } else {
+        Wb[(long long)p * a.ld + c] = acc[q];
       }
     }
   }
@@ -461,45 +485,27 @@ __global__ void __launch_bounds__(SOLVE_NT) k_btrsv_blk(SolveArgs a, const int4*
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_btrsv_upd(SolveArgs a, const int4* __restrict__ tasks) {
   using F = Field<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Ls = reinterpret_cast<T*>(smem_raw);
+  T* Vs = Ls + 32 * 33;
   const int4 tk = tasks[blockIdx.x];
   const int s = tk.x, jb = tk.y, c0 = tk.z;
   const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
   const int je = min(jb + TB, ncol);
   const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
   T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int NW = SOLVE_NT / 32;
   const int cols_here = min(32, jb - c0);
-  for (int pc = warp; pc < cols_here; pc += NW) {
+  T acc[RHS_MAX / 8];
+  dot_cols_tile<T, false>(L, nrow, c0, cols_here, jb, je, Z, nullptr, a.ld, a.nrhs, acc, Ls, Vs);
+  const int pc = threadIdx.x & 31, cg = threadIdx.x >> 5;
+  if (pc < cols_here) {
     const int p = c0 + pc;
-    T acc[RHS_MAX];
 #pragma unroll
-    for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
-    const T* Lc = L + (long long)p * nrow;
-    for (int r = jb + lane; r < je; r += 32) {
-      T l = Lc[r];
-      const T* v = Z + (long long)r * a.ld;
-#pragma unroll
-      for (int c = 0; c < RHS_MAX; ++c)
-        if (c < a.nrhs) acc[c] = F::fma_(l, v[c], acc[c]);
-    }
-#pragma unroll
-    for (int c = 0; c < RHS_MAX; ++c) {
+    for (int q = 0; q < RHS_MAX / 8; ++q) {
+      const int c = cg + 8 * q;
       if (c >= a.nrhs) continue;
-      T x = acc[c];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        if constexpr (Field<T>::complex) {
-          x.re += __shfl_down_sync(0xffffffffu, x.re, o);
-          x.im += __shfl_down_sync(0xffffffffu, x.im, o);
-        } else {
-          x += __shfl_down_sync(0xffffffffu, x, o);
-        }
-      }
-      if (lane == 0) {
-        T* z = Z + (long long)p * a.ld + c;
-        *z = F::sub(*z, x);
-      }
+      T* z = Z + (long long)p * a.ld + c;
+      *z = F::sub(*z, acc[q]);
     }
   }
 }

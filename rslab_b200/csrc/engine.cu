@@ -440,6 +440,7 @@ size_t smem_getf2(size_t es, int nb) {
 size_t smem_deep(size_t es, int nb) { return (size_t)(DEEP_R + 1) * nb * es + 64; }
 size_t smem_solve(size_t es) { return (size_t)(SOLVE_NT / 32) * 32 * RHS_MAX * es + 32 * RHS_MAX * es + 64 * 4; }
 size_t smem_push(size_t es) { return (size_t)4 * 64 * RHS_MAX * es; }
+size_t smem_dots(size_t es) { return (size_t)(32 * 33 + 32 * RHS_MAX) * es; }
 
 template <typename T>
 struct KernelSetup {
@@ -457,6 +458,8 @@ struct KernelSetup {
     CK(cudaFuncSetAttribute(k_ftrsv_upd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_push(es)));
     CK(cudaFuncSetAttribute(k_ftrsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
     CK(cudaFuncSetAttribute(k_btrsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
+    CK(cudaFuncSetAttribute(k_bwd_off<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
+    CK(cudaFuncSetAttribute(k_btrsv_upd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
     done = true;
   }
 };
@@ -749,13 +752,13 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
     for (const Launch& L : H.bwdplan) {
       switch (L.kind) {
         case L_BWD_OFF:
-          k_bwd_off<T><<<L.ntasks, SOLVE_NT, 0, st>>>(sa, H.d_t2 + L.task_off);
+          k_bwd_off<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_t2 + L.task_off);
           break;
         case L_BTRSV_BLK:
           k_btrsv_blk<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_st4 + L.task_off);
           break;
         case L_BTRSV_UPD:
-          k_btrsv_upd<T><<<L.ntasks, SOLVE_NT, 0, st>>>(sa, H.d_st4 + L.task_off);
+          k_btrsv_upd<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_st4 + L.task_off);
           break;
         default:
           k_bwd<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
