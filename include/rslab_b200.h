@@ -152,6 +152,14 @@ int rslab_factor_profile(rslab_fac_handle* fac, double* kind_ms, int64_t* kind_l
  * [5] backward diagonal, [6] total).  A measurement aid with no reference
  * counterpart. */
 int rslab_solve_profile(rslab_fac_handle* fac, int64_t nrhs, double* kind_ms, int64_t* kind_launches);
+/* Per-launch rows of the handle's last factor/solve profile: launch kind
+ * (0 cmod, 1 getf2, 2 deep replay, 3 panel Schur, 4 forward diagonal,
+ * 5 forward push, 6 backward dots, 7 backward diagonal, 8/9 blocked forward
+ * diagonal/update, 10/11 blocked backward diagonal/update, -1 other), grid
+ * size and device ms.  *count = rows available; at most cap are written.
+ * A measurement aid with no reference counterpart. */
+int rslab_profile_trace(const rslab_fac_handle* fac, int64_t cap, int32_t* kind, int32_t* grid, float* ms,
+                        int64_t* count);
 /* Reference LdltFactors layout; pass NULL arrays to query *nnz_out first. */
 int rslab_export_factors(const rslab_fac_handle* fac, int64_t* l_col_ptr, int64_t* l_row_idx, void* l_values,
                          void* d_diag, void* d_subdiag, uint8_t* two_by_two, int64_t* perm, double* scale,

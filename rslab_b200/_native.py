@@ -90,6 +90,8 @@ SIGNATURES = {
                                        C.POINTER(C.c_double), i64p]),
     "rslab_factor_profile": (C.c_int, [vp, C.POINTER(C.c_double), i64p, C.POINTER(C.c_double)]),
     "rslab_solve_profile": (C.c_int, [vp, C.c_int64, C.POINTER(C.c_double), i64p]),
+    "rslab_profile_trace": (C.c_int, [vp, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                      C.POINTER(C.c_float), i64p]),
     "rslab_free_factor": (None, [vp]),
     "rslab_mixed_factor": (C.c_int, [vp, C.c_int, vp, C.c_int, C.POINTER(FactorSettings), C.POINTER(vp)]),
     "rslab_mixed_solve": (C.c_int, [vp, vp, C.c_int64, C.c_double, vp, C.c_int, C.POINTER(MixedInfoC)]),

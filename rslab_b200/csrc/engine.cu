@@ -506,6 +506,9 @@ struct rslab_fac_handle {
   int last_status = 0, failing_sn = -1;
   double factor_ms = 0, solve_ms = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // per-launch rows of the last factor/solve profile
+  std::vector<int> tr_kind, tr_grid;
+  std::vector<float> tr_ms;
 
   ~rslab_fac_handle() {
     if (fgraph) cudaGraphExecDestroy(fgraph);
@@ -555,12 +558,29 @@ FactorArgs make_fargs(rslab_fac_handle& F) {
 struct Prof {
   std::vector<cudaEvent_t> ev;
   std::vector<int> kind;
-  void mark(cudaStream_t st, int k) {
+  std::vector<int> grid;
+  std::vector<int> fine;
+  void mark(cudaStream_t st, int k, int ntasks = 0, int launch_kind = -1) {
     cudaEvent_t e;
     CK(cudaEventCreate(&e));
     CK(cudaEventRecord(e, st));
     ev.push_back(e);
     kind.push_back(k);
+    grid.push_back(ntasks);
+    fine.push_back(launch_kind);
+  }
+  // Per-launch rows (launch kind, grid size, device ms) into the handle.
+  void store(std::vector<int>& tk, std::vector<int>& tg, std::vector<float>& tms) const {
+    tk.clear();
+    tg.clear();
+    tms.clear();
+    for (size_t i = 1; i < ev.size(); ++i) {
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, ev[i - 1], ev[i]));
+      tk.push_back(fine[i]);
+      tg.push_back(grid[i]);
+      tms.push_back(ms);
+    }
   }
   ~Prof() {
     for (auto e : ev) cudaEventDestroy(e);
@@ -610,7 +630,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         k_schur<T><<<L.ntasks, TPB, smem_schur(es), st>>>(fa, H.d_t4 + L.task_off, nb_small, nb_big);
         break;
     }
-    if (prof) prof->mark(st, L.kind == L_CMOD ? 1 : L.kind == L_GETF2 ? 2 : L.kind == L_DEEP ? 3 : 4);
+    if (prof) prof->mark(st, L.kind == L_CMOD ? 1 : L.kind == L_GETF2 ? 2 : L.kind == L_DEEP ? 3 : 4, L.ntasks, L.kind);
   }
   CK(cudaMemsetAsync(F.cnt3, 0, 3 * sizeof(unsigned long long), st));
   k_inertia<T><<<grid1(n), 256, 0, st>>>(n, (const T*)F.d, (const T*)F.dsub, F.kind, F.cnt3);
@@ -745,7 +765,7 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
         default:
           k_fwd_push<T><<<L.ntasks, SOLVE_NT, smem_push(es), st>>>(sa, H.d_t2 + L.task_off);
       }
-      if (prof) prof->mark(st, L.kind == L_FWD_PUSH ? 2 : 1);
+      if (prof) prof->mark(st, L.kind == L_FWD_PUSH ? 2 : 1, L.ntasks, L.kind);
     }
     k_dsolve<T><<<grid1((long long)n * nr), 256, 0, st>>>(n, sa);
     if (prof) prof->mark(st, 3);
@@ -763,7 +783,7 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
         default:
           k_bwd<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
       }
-      if (prof) prof->mark(st, L.kind == L_BWD_OFF ? 4 : 5);
+      if (prof) prof->mark(st, L.kind == L_BWD_OFF ? 4 : 5, L.ntasks, L.kind);
     }
   }
   k_perm_out<T><<<grid1((long long)n * nrhs), 256, 0, st>>>(n, nrhs, H.d_perm, F.scale, (const T*)F.Xg, x);
@@ -1196,6 +1216,7 @@ int rslab_solve_profile(rslab_fac_handle* F, int64_t nrhs, double* kind_ms, int6
       enqueue_solve<T>(*F, (const T*)F->bdev, (T*)F->xdev, (int)nrhs, &prof);
     });
     CK(cudaStreamSynchronize(F->st));
+    prof.store(F->tr_kind, F->tr_grid, F->tr_ms);
     for (int k = 0; k < 7; ++k) {
       kind_ms[k] = 0;
       kind_launches[k] = 0;
@@ -1230,6 +1251,7 @@ int rslab_factor_profile(rslab_fac_handle* F, double* kind_ms, int64_t* kind_lau
       enqueue_factor<T>(*F, &prof);
     });
     CK(cudaStreamSynchronize(F->st));
+    prof.store(F->tr_kind, F->tr_grid, F->tr_ms);
     for (int k = 0; k < 6; ++k) {
       kind_ms[k] = 0;
       kind_launches[k] = 0;
@@ -1254,6 +1276,22 @@ int rslab_factor_profile(rslab_fac_handle* F, double* kind_ms, int64_t* kind_lau
   } catch (const RslabError& e) {
     return fail(e);
   }
+}
+
+// Per-launch rows of the last rslab_factor_profile / rslab_solve_profile call:
+// launch kind (LaunchKind code, -1 for permutes / D-solve / assembly), grid
+// size and device ms; *count = rows available, at most `cap` written.
+int rslab_profile_trace(const rslab_fac_handle* F, int64_t cap, int32_t* kind, int32_t* grid, float* ms,
+                        int64_t* count) {
+  if (!F || !count) return fail(RslabError(Status::InvalidInput, "null argument"));
+  const int64_t m = (int64_t)F->tr_ms.size();
+  *count = m;
+  for (int64_t i = 0; i < std::min(m, cap); ++i) {
+    if (kind) kind[i] = F->tr_kind[i];
+    if (grid) grid[i] = F->tr_grid[i];
+    if (ms) ms[i] = F->tr_ms[i];
+  }
+  return 0;
 }
 
 // Export in the reference LdltFactors layout (src/dense/ldlt_generic.rs:31-66):

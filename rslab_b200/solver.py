@@ -599,6 +599,22 @@ def solve_profile(handle, nrhs: int) -> dict:
     return {k: {"ms": ms[i], "launches": int(nl[i])} for i, k in enumerate(SOLVE_KINDS)}
 
 
+LAUNCH_KINDS = ("cmod", "getf2", "deep_replay", "panel_schur", "fwd_diag", "fwd_push", "bwd_off", "bwd_diag",
+                "ftrsv_blk", "ftrsv_upd", "btrsv_blk", "btrsv_upd")
+
+
+def profile_trace(handle) -> list:
+    """Per-launch (kind, grid, ms) rows of the handle's last factor/solve profile."""
+    cnt = C.c_int64(0)
+    _check(N.lib.rslab_profile_trace(handle, 0, None, None, None, C.byref(cnt)))
+    m = int(cnt.value)
+    kind = (C.c_int32 * max(m, 1))()
+    grid = (C.c_int32 * max(m, 1))()
+    ms = (C.c_float * max(m, 1))()
+    _check(N.lib.rslab_profile_trace(handle, m, kind, grid, ms, C.byref(cnt)))
+    return [(LAUNCH_KINDS[kind[i]] if kind[i] >= 0 else "other", int(grid[i]), float(ms[i])) for i in range(m)]
+
+
 def amd_order(n: int, col_ptr, row_idx) -> tuple:
     """AMD on a full symmetric pattern; returns (perm, stats dict)."""
     cp = _i64(col_ptr)
