@@ -6,10 +6,11 @@
 // src/dense/ldlt_generic.rs:556-714).  Two index spaces are used:
 //   g : the analysed (fill-reducing) order — panel row structures live here;
 //   e : pivot order, e = first_col(s) + pivot position inside s.
-// Forward:  per level, k_fwd_gather pulls every descendant's L_k * z_k into
-//           the columns of s (update-list order, no atomics), then
-//           k_fwd_diag solves the unit-lower diagonal block in pivot order and
-//           applies D^-1.
+// Forward:  per level, k_fwd_gather pulls every descendant's push
+//           U_k = L21_k z_k into the columns of s (update-list order, no
+//           atomics), k_fwd_diag (narrow) or k_ftrsv_blk/upd (wide) solve the
+//           unit-lower diagonal block in pivot order, and k_fwd_push forms
+//           U_s; D^-1 follows the whole sweep (k_dsolve).
 // Backward: per level (root first), k_bwd dots each column of s against the
 //           already-solved rows (own pivots in e order, ancestors in g order)
 //           and back-substitutes the diagonal block.
@@ -48,6 +49,8 @@ struct SolveArgs {
   void* U;    // sum_s (nrow_s - ncol_s) x ld: U_s = L21_s z_s
   void* Wb;   // n x ld, e order: backward off-diagonal dots
   const long long* uoff;  // row offset of U_s
+  const int* pull_ptr;    // n + 1: pull list of column g (g order)
+  const int* pull_src;    // U row of each push, update-list order per g
   int ld;     // row stride (total rhs count)
   int c0;     // first rhs column of this pass
   int nrhs;   // rhs columns in this pass (<= RHS_MAX)
@@ -76,7 +79,7 @@ __global__ void k_perm_out(int n, int nrhs, const int* __restrict__ perm, const 
 }
 
 // acc[c] += sum_{q in [q_begin, q_end)} L[r, q] * V[q][c]: one lane per row r,
-// warps split q; result reduced through smem `red` (NW x 32 x RHS_MAX).
+// warps split q (stride NW); the partial sums are reduced through smem.
 template <typename T>
 __device__ __forceinline__ void lane_row_dot(T (&acc)[RHS_MAX], const T* __restrict__ Lrow, long long ld,
                                              int q_begin, int q_end, const T* __restrict__ V, int vld, int nrhs,
@@ -94,162 +97,178 @@ __device__ __forceinline__ void lane_row_dot(T (&acc)[RHS_MAX], const T* __restr
 }
 
 template <typename T>
-__device__ __forceinline__ void reduce_warps(T (&acc)[RHS_MAX], T* red, int nrhs) {
-  using F = Field<T>;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  constexpr int NW = SOLVE_NT / 32;
-#pragma unroll
-  for (int c = 0; c < RHS_MAX; ++c)
-    if (c < nrhs) red[(warp * 32 + lane) * RHS_MAX + c] = acc[c];
-  __syncthreads();
-  if (warp == 0) {
-#pragma unroll
-    for (int c = 0; c < RHS_MAX; ++c) {
-      if (c >= nrhs) continue;
-      T s = F::zero();
-      for (int w = 0; w < NW; ++w) s = F::add(s, red[(w * 32 + lane) * RHS_MAX + c]);
-      acc[c] = s;
-    }
+__device__ __forceinline__ T shfl_T(T v, int src) {
+  if constexpr (Field<T>::complex) {
+    T r;
+    r.re = __shfl_sync(0xffffffffu, v.re, src);
+    r.im = __shfl_sync(0xffffffffu, v.im, src);
+    return r;
+  } else {
+    return __shfl_sync(0xffffffffu, v, src);
   }
-  __syncthreads();
+}
+
+// Ls[i * 33 + j] = L[j0 + i, j0 + j] for j < i < nb (strict lower part of the
+// nb x nb diagonal block), zero elsewhere.  Loads coalesced along i.
+template <typename T>
+__device__ __forceinline__ void stage_diag_block(const T* __restrict__ L, int nrow, int j0, int nb, T* Ls) {
+  for (int e = threadIdx.x; e < SB * SB; e += SOLVE_NT) {
+    const int i = e & (SB - 1), j = e / SB;
+    Ls[i * (SB + 1) + j] = (i < nb && j < i) ? L[(j0 + i) + (long long)(j0 + j) * nrow] : Field<T>::zero();
+  }
 }
 
 // Pivot-order unit-lower substitution of columns [j_begin, j_end) of a panel
-// in 32-column blocks (one CTA): z[p] = y[p] - sum_{q in [q_begin, p)} L[p,q] z[q].
-// y comes from the g-ordered RHS through lperm (from_y) or already sits in Z.
+// in 32-column blocks (one CTA), in place on Z (pivot order, holding y):
+//   z[p] = y[p] - sum_{q in [q_begin, p)} L[p,q] z[q].
+// Per block: the left part [q_begin, j0) is a warp-split dot whose partial
+// sums are added in warp order; the diagonal block is staged in shared memory
+// and every warp substitutes its own right-hand sides (c = warp, warp + NW, ..)
+// with one lane per row, so no warp waits on a global load inside the
+// 32-step dependency chain.  Per (p, c) the operation sequence is fixed:
+// z = y - left; then z -= L[p,q] z[q] for q ascending.
 template <typename T>
-__device__ void fwd_block_range(const SolveArgs& a, const T* __restrict__ L, int nrow, T* Z, const T* Yfirst,
-                                const int* __restrict__ lp, int j_begin, int j_end, int q_begin, bool from_y, T* red) {
+__device__ void fwd_block_range(const SolveArgs& a, const T* __restrict__ L, int nrow, T* Z, int j_begin, int j_end,
+                                int q_begin, T* red, T* Ls, T* zb) {
   using F = Field<T>;
+  constexpr int NW = SOLVE_NT / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int j0 = j_begin; j0 < j_end; j0 += SB) {
     const int nb = min(SB, j_end - j0);
-    T acc[RHS_MAX];
+    const bool left = j0 > q_begin;
+    if (left) {
+      T acc[RHS_MAX];
 #pragma unroll
-    for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
-    lane_row_dot<T>(acc, L + j0 + lane, nrow, q_begin, j0, Z, a.ld, a.nrhs, lane < nb);
-    reduce_warps<T>(acc, red, a.nrhs);
-    if (warp == 0) {
-      T z[RHS_MAX];
-      const int p = j0 + lane;
-      const bool ok = lane < nb;
-      const T* yrow = from_y ? Yfirst + (long long)((ok ? lp[p] : 0)) * a.ld : Z + (long long)(ok ? p : 0) * a.ld;
+      for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
+      lane_row_dot<T>(acc, L + j0 + lane, nrow, q_begin, j0, Z, a.ld, a.nrhs, lane < nb);
 #pragma unroll
-      for (int c = 0; c < RHS_MAX; ++c) z[c] = (ok && c < a.nrhs) ? F::sub(yrow[c], acc[c]) : F::zero();
-      for (int q = 0; q < nb; ++q) {
-        const int qq = j0 + q;
-        T l = F::zero();
-        if (ok && lane > q) l = L[p + (long long)qq * nrow];
-#pragma unroll
-        for (int c = 0; c < RHS_MAX; ++c) {
-          if (c >= a.nrhs) continue;
-          T zq;
-          if constexpr (Field<T>::complex) {
-            zq.re = __shfl_sync(0xffffffffu, z[c].re, q);
-            zq.im = __shfl_sync(0xffffffffu, z[c].im, q);
-          } else {
-            zq = __shfl_sync(0xffffffffu, z[c], q);
-          }
-          z[c] = F::fnma(l, zq, z[c]);
+      for (int c = 0; c < RHS_MAX; ++c)
+        if (c < a.nrhs) red[(warp * 32 + lane) * RHS_MAX + c] = acc[c];
+    }
+    stage_diag_block<T>(L, nrow, j0, nb, Ls);
+    __syncthreads();
+    for (int e = threadIdx.x; e < SB * RHS_MAX; e += SOLVE_NT) {
+      const int i = e & (SB - 1), c = e / SB;
+      if (c >= a.nrhs) continue;
+      T v = F::zero();
+      if (i < nb) {
+        v = Z[(long long)(j0 + i) * a.ld + c];
+        if (left) {
+          T s = F::zero();
+          for (int w = 0; w < NW; ++w) s = F::add(s, red[(w * 32 + i) * RHS_MAX + c]);
+          v = F::sub(v, s);
         }
       }
-      if (ok)
+      zb[i * RHS_MAX + c] = v;
+    }
+    __syncthreads();
+    for (int c = warp; c < a.nrhs; c += NW) {
+      T z = zb[lane * RHS_MAX + c];
 #pragma unroll
-        for (int c = 0; c < RHS_MAX; ++c)
-          if (c < a.nrhs) Z[(long long)p * a.ld + c] = z[c];
+      for (int q = 0; q < SB; ++q) {
+        if (q < nb) {
+          const T zq = shfl_T(z, q);
+          z = F::fnma(Ls[lane * (SB + 1) + q], zq, z);
+        }
+      }
+      if (lane < nb) Z[(long long)(j0 + lane) * a.ld + c] = z;
     }
     __syncthreads();
   }
 }
 
-// Forward step of supernode s (one CTA):
-//  1. pull the descendants' pushes: y[g] -= U_k[r] for every updater k (in
-//     update-list order) and its off-diagonal rows r landing in s's columns;
-//  2. pivot-order unit-lower substitution of the diagonal block in 32-column
-//     blocks (left-looking inside the panel) -> z_s (e order); supernodes
-//     wider than SOLVE_BIG only stage y here and are solved by the blocked
-//     multi-CTA kernels k_ftrsv_blk / k_ftrsv_upd.
-// The push U_s = L21_s z_s (k_fwd_push) follows as a separate launch.
+// Forward gather of supernode s, pivot positions [p0, p0 + 16) (thread =
+// position x right-hand side): Z[p] = Y[g] minus every push U_k[r] that lands
+// on g = first + lperm[p], in update-list order (the pull list of g, built
+// at analysis).  No atomics and no block-wide barrier per updater.
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_NT) k_fwd_gather(SolveArgs a, const int2* __restrict__ tasks) {
+  using F = Field<T>;
+  const int2 tk = tasks[blockIdx.x];
+  const int s = tk.x, p = tk.y + (int)(threadIdx.x / RHS_MAX), c = (int)(threadIdx.x % RHS_MAX);
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s];
+  if (p >= ncol || c >= a.nrhs) return;
+  const int g = first + a.lperm[first + p];
+  const T* U = reinterpret_cast<const T*>(a.U) + a.c0 + c;
+  T y = reinterpret_cast<const T*>(a.Yg)[a.c0 + (long long)g * a.ld + c];
+  const int t0 = a.pull_ptr[g], t1 = a.pull_ptr[g + 1];
+#pragma unroll 4
+  for (int t = t0; t < t1; ++t) y = F::sub(y, U[(long long)a.pull_src[t] * a.ld]);
+  reinterpret_cast<T*>(a.Ze)[a.c0 + (long long)(first + p) * a.ld + c] = y;
+}
+
+// Forward diagonal block of a narrow supernode s (ncol <= SOLVE_BIG, one
+// CTA): Z already holds the gathered y in pivot order; solve in place.
+// Wider supernodes use k_ftrsv_blk / k_ftrsv_upd.
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_fwd_diag(SolveArgs a, const int* __restrict__ tasks) {
-  using F = Field<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* red = reinterpret_cast<T*>(smem_raw);
+  T* red = reinterpret_cast<T*>(smem_raw);        // NW x 32 x RHS_MAX
+  T* Ls = red + (SOLVE_NT / 32) * 32 * RHS_MAX;  // 32 x 33
+  T* zb = Ls + SB * (SB + 1);                    // 32 x RHS_MAX
   const int s = tasks[blockIdx.x];
   const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
   const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
-  const int* lp = a.lperm + first;
-  T* Y = reinterpret_cast<T*>(a.Yg) + a.c0;
   T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  T* Uall = reinterpret_cast<T*>(a.U) + a.c0;
-  // 1. gather the pushes of the updaters (distinct rows within one updater).
-  for (int u = a.upd_ptr[s]; u < a.upd_ptr[s + 1]; ++u) {
-    const int k = a.upd_k[u], p0 = a.upd_p0[u], p1 = a.upd_p1[u];
-    const int* ok = a.rs + a.sn_rsoff[k] + a.sn_ncol[k];
-    const T* Uk = Uall + a.uoff[k] * a.ld;
-    const int cnt = (p1 - p0) * a.nrhs;
-    for (int e = threadIdx.x; e < cnt; e += SOLVE_NT) {
-      const int r = p0 + e / a.nrhs, c = e % a.nrhs;
-      T* y = Y + (long long)ok[r] * a.ld + c;
-      *y = F::sub(*y, Uk[(long long)r * a.ld + c]);
+  fwd_block_range<T>(a, L, nrow, Z, 0, ncol, 0, red, Ls, zb);
+}
+
+// acc[m] = sum_{q in [q0, q1)} L[r, q] * Z[q][c] for the 64 panel rows
+// r = r0 + (tid & 63) (rows >= r_end read as zero) and c = (tid >> 6) + 4 m.
+// 32-column chunks of L and the matching 32 rows of Z are staged in shared
+// memory (coalesced along r); each thread adds q in ascending order.
+template <typename T>
+__device__ void rows_dot_z(const T* __restrict__ L, int nrow, int r0, int r_end, int q0, int q1,
+                           const T* __restrict__ Z, int ld, int nrhs, T (&acc)[RHS_MAX / 4], T* Ls, T* Zs) {
+  using F = Field<T>;
+  const int tid = threadIdx.x, rl = tid & 63, cg = tid >> 6;
+#pragma unroll
+  for (int m = 0; m < RHS_MAX / 4; ++m) acc[m] = F::zero();
+  for (int qc = q0; qc < q1; qc += 32) {
+    const int nq = min(32, q1 - qc);
+    for (int e = tid; e < 64 * 32; e += SOLVE_NT) {
+      const int r = e & 63, q = e >> 6;
+      Ls[q * 64 + r] = (q < nq && r0 + r < r_end) ? L[(r0 + r) + (long long)(qc + q) * nrow] : F::zero();
+    }
+    for (int e = tid; e < 32 * nrhs; e += SOLVE_NT) {
+      const int q = e / nrhs, c = e % nrhs;
+      Zs[q * RHS_MAX + c] = q < nq ? Z[(long long)(qc + q) * ld + c] : F::zero();
+    }
+    __syncthreads();
+    for (int q = 0; q < nq; ++q) {
+      const T l = Ls[q * 64 + rl];
+#pragma unroll
+      for (int m = 0; m < RHS_MAX / 4; ++m) {
+        const int c = cg + 4 * m;
+        if (c < nrhs) acc[m] = F::fma_(l, Zs[q * RHS_MAX + c], acc[m]);
+      }
     }
     __syncthreads();
   }
-  // 2. diagonal block: in this CTA for narrow supernodes; wide ones only
-  //    stage y in pivot order into Z for the blocked multi-CTA solve.
-  if (ncol > SOLVE_BIG) {
-    for (int e = threadIdx.x; e < ncol * a.nrhs; e += SOLVE_NT) {
-      const int p = e / a.nrhs, c = e % a.nrhs;
-      Z[(long long)p * a.ld + c] = Y[(long long)(first + lp[p]) * a.ld + c];
-    }
-    return;
-  }
-  fwd_block_range<T>(a, L, nrow, Z, Y + (long long)first * a.ld, lp, 0, ncol, 0, true, red);
 }
 
-// Forward push of supernode s, rows [ncol + r0, ncol + r0 + 64):
-// U_s = L21_s z_s.  Two 32-row lane groups x four q-splits (warps); the
-// q-split partial sums are added in a fixed order (deterministic).
+// Forward push of supernode s, off-diagonal rows [ncol + r0, ncol + r0 + 64):
+// U_s = L21_s z_s (rows_dot_z over all own columns).
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_fwd_push(SolveArgs a, const int2* __restrict__ tasks) {
-  using F = Field<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* red = reinterpret_cast<T*>(smem_raw);  // [4 splits][64 rows][RHS_MAX]
+  T* Ls = reinterpret_cast<T*>(smem_raw);  // 32 x 64
+  T* Zs = Ls + 32 * 64;                    // 32 x RHS_MAX
   const int2 tk = tasks[blockIdx.x];
   const int s = tk.x, r0 = tk.y;
   const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
   const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
   const T* Z = reinterpret_cast<const T*>(a.Ze) + a.c0 + (long long)first * a.ld;
   T* Us = reinterpret_cast<T*>(a.U) + a.c0 + a.uoff[s] * a.ld;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int rg = warp & 1, qs = warp >> 1;  // row group, q split
-  const int rl = rg * 32 + lane;            // local row 0..63
-  const int r = ncol + r0 + rl;
-  const bool ok = r < nrow;
-  T acc[RHS_MAX];
+  T acc[RHS_MAX / 4];
+  rows_dot_z<T>(L, nrow, ncol + r0, nrow, 0, ncol, Z, a.ld, a.nrhs, acc, Ls, Zs);
+  const int r = ncol + r0 + (threadIdx.x & 63), cg = threadIdx.x >> 6;
+  if (r < nrow)
 #pragma unroll
-  for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
-  for (int q = qs; q < ncol; q += 4) {
-    T l = ok ? L[r + (long long)q * nrow] : F::zero();
-    const T* zq = Z + (long long)q * a.ld;
-#pragma unroll
-    for (int c = 0; c < RHS_MAX; ++c)
-      if (c < a.nrhs) acc[c] = F::fma_(l, zq[c], acc[c]);
-  }
-#pragma unroll
-  for (int c = 0; c < RHS_MAX; ++c)
-    if (c < a.nrhs) red[(qs * 64 + rl) * RHS_MAX + c] = acc[c];
-  __syncthreads();
-  for (int e = threadIdx.x; e < 64 * a.nrhs; e += SOLVE_NT) {
-    const int row = e / a.nrhs, c = e % a.nrhs;
-    const int rr = ncol + r0 + row;
-    if (rr >= nrow) continue;
-    T v = red[(0 * 64 + row) * RHS_MAX + c];
-    v = F::add(v, red[(1 * 64 + row) * RHS_MAX + c]);
-    v = F::add(v, red[(2 * 64 + row) * RHS_MAX + c]);
-    v = F::add(v, red[(3 * 64 + row) * RHS_MAX + c]);
-    Us[(long long)(rr - ncol) * a.ld + c] = v;
-  }
+    for (int m = 0; m < RHS_MAX / 4; ++m) {
+      const int c = cg + 4 * m;
+      if (c < a.nrhs) Us[(long long)(r - ncol) * a.ld + c] = acc[m];
+    }
 }
 
 // out[p][c] = sum_{r in [r_begin, r_end)} L[r, p] * V(r)[c] for the 32
@@ -337,12 +356,14 @@ template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_ftrsv_blk(SolveArgs a, const int4* __restrict__ tasks) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* red = reinterpret_cast<T*>(smem_raw);
+  T* Ls = red + (SOLVE_NT / 32) * 32 * RHS_MAX;
+  T* zb = Ls + SB * (SB + 1);
   const int4 tk = tasks[blockIdx.x];
   const int s = tk.x, j0 = tk.y;
   const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
   const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
   T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  fwd_block_range<T>(a, L, nrow, Z, nullptr, nullptr, j0, min(j0 + TB, ncol), j0, false, red);
+  fwd_block_range<T>(a, L, nrow, Z, j0, min(j0 + TB, ncol), j0, red, Ls, zb);
 }
 
 // Right-looking update after forward block [j0, j0+64) of a wide supernode:
@@ -351,64 +372,41 @@ template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_ftrsv_upd(SolveArgs a, const int4* __restrict__ tasks) {
   using F = Field<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* red = reinterpret_cast<T*>(smem_raw);  // [4 splits][64 rows][RHS_MAX]
+  T* Ls = reinterpret_cast<T*>(smem_raw);
+  T* Zs = Ls + 32 * 64;
   const int4 tk = tasks[blockIdx.x];
   const int s = tk.x, j0 = tk.y, r0 = tk.z;
   const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
-  const int j1 = min(j0 + TB, ncol);
   const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
   T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int rg = warp & 1, qs = warp >> 1;
-  const int rl = rg * 32 + lane;
-  const int r = r0 + rl;
-  const bool ok = r < ncol;
-  T acc[RHS_MAX];
+  T acc[RHS_MAX / 4];
+  rows_dot_z<T>(L, nrow, r0, ncol, j0, min(j0 + TB, ncol), Z, a.ld, a.nrhs, acc, Ls, Zs);
+  const int r = r0 + (threadIdx.x & 63), cg = threadIdx.x >> 6;
+  if (r < ncol)
 #pragma unroll
-  for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
-  for (int q = j0 + qs; q < j1; q += 4) {
-    T l = ok ? L[r + (long long)q * nrow] : F::zero();
-    const T* zq = Z + (long long)q * a.ld;
-#pragma unroll
-    for (int c = 0; c < RHS_MAX; ++c)
-      if (c < a.nrhs) acc[c] = F::fma_(l, zq[c], acc[c]);
-  }
-#pragma unroll
-  for (int c = 0; c < RHS_MAX; ++c)
-    if (c < a.nrhs) red[(qs * 64 + rl) * RHS_MAX + c] = acc[c];
-  __syncthreads();
-  for (int e = threadIdx.x; e < 64 * a.nrhs; e += SOLVE_NT) {
-    const int row = e / a.nrhs, c = e % a.nrhs;
-    const int rr = r0 + row;
-    if (rr >= ncol) continue;
-    T v = red[(0 * 64 + row) * RHS_MAX + c];
-    v = F::add(v, red[(1 * 64 + row) * RHS_MAX + c]);
-    v = F::add(v, red[(2 * 64 + row) * RHS_MAX + c]);
-    v = F::add(v, red[(3 * 64 + row) * RHS_MAX + c]);
-    T* z = Z + (long long)rr * a.ld + c;
-    *z = F::sub(*z, v);
-  }
+    for (int m = 0; m < RHS_MAX / 4; ++m) {
+      const int c = cg + 4 * m;
+      if (c < a.nrhs) {
+        T* z = Z + (long long)r * a.ld + c;
+        *z = F::sub(*z, acc[m]);
+      }
+    }
 }
 
-// Blocked backward solve of a wide supernode, block [j0, j0+64): in-block
-// substitution with L^T (v already holds w - L21^T x - later blocks), then
-// the block's final values go to X in g order.
+// Backward substitution of pivot columns [jb, je) of a panel in 32-column
+// blocks from the last (one CTA), in place on Z; final values also go to X
+// (g order).  Per block: v[p] -= sum_{r in [j1, r_end)} L[r, p] v[r] over
+// the solved rows below it (warp per column, lanes over r, shuffle tree),
+// then the transposed in-block substitution from a shared-memory copy of
+// the diagonal block, warps over right-hand sides, lanes over rows.
+// Per (p, c): v = Z[p] (- Wb[p] when given) - below; then v -= L[q,p] v[q]
+// for q descending.
 template <typename T>
-__global__ void __launch_bounds__(SOLVE_NT) k_btrsv_blk(SolveArgs a, const int4* __restrict__ tasks) {
+__device__ void bwd_block_range(const SolveArgs& a, const T* __restrict__ L, int nrow, T* Z, const T* Wb, T* Xw,
+                                const int* __restrict__ lp, int first, int jb, int je, int r_end, T* vb, T* Ls) {
   using F = Field<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* red = reinterpret_cast<T*>(smem_raw);
-  T* vb = red + (SOLVE_NT / 32) * 32 * RHS_MAX;
-  const int4 tk = tasks[blockIdx.x];
-  const int s = tk.x, jb = tk.y;
-  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
-  const int je = min(jb + TB, ncol);
-  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
-  const int* lp = a.lperm + first;
-  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  T* Xw = reinterpret_cast<T*>(a.Xg) + a.c0;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NW = SOLVE_NT / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nblk = (je - jb + SB - 1) / SB;
   for (int b = nblk - 1; b >= 0; --b) {
     const int j0 = jb + b * SB, nb = min(SB, je - j0), j1 = j0 + nb;
@@ -418,7 +416,7 @@ __global__ void __launch_bounds__(SOLVE_NT) k_btrsv_blk(SolveArgs a, const int4*
 #pragma unroll
       for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
       const T* Lc = L + (long long)p * nrow;
-      for (int r = j1 + lane; r < je; r += 32) {
+      for (int r = j1 + lane; r < r_end; r += 32) {
         T l = Lc[r];
         const T* v = Z + (long long)r * a.ld;
 #pragma unroll
@@ -441,43 +439,48 @@ __global__ void __launch_bounds__(SOLVE_NT) k_btrsv_blk(SolveArgs a, const int4*
         if (lane == 0) vb[pc * RHS_MAX + c] = x;
       }
     }
+    stage_diag_block<T>(L, nrow, j0, nb, Ls);
     __syncthreads();
-    if (warp == 0) {
-      const int p = j0 + lane;
-      const bool ok = lane < nb;
-      T v[RHS_MAX];
+    const int p = j0 + lane;
+    const bool ok = lane < nb;
+    for (int c = warp; c < a.nrhs; c += NW) {
+      T v = F::zero();
+      if (ok) {
+        v = Z[(long long)p * a.ld + c];
+        if (Wb) v = F::sub(v, Wb[(long long)p * a.ld + c]);
+        v = F::sub(v, vb[lane * RHS_MAX + c]);
+      }
 #pragma unroll
-      for (int c = 0; c < RHS_MAX; ++c)
-        v[c] = (ok && c < a.nrhs) ? F::sub(Z[(long long)p * a.ld + c], vb[lane * RHS_MAX + c]) : F::zero();
-      for (int q = nb - 1; q >= 1; --q) {
-        const int qq = j0 + q;
-        T l = F::zero();
-        if (ok && lane < q) l = L[qq + (long long)p * nrow];
-#pragma unroll
-        for (int c = 0; c < RHS_MAX; ++c) {
-          if (c >= a.nrhs) continue;
-          T vq;
-          if constexpr (Field<T>::complex) {
-            vq.re = __shfl_sync(0xffffffffu, v[c].re, q);
-            vq.im = __shfl_sync(0xffffffffu, v[c].im, q);
-          } else {
-            vq = __shfl_sync(0xffffffffu, v[c], q);
-          }
-          v[c] = F::fnma(l, vq, v[c]);
+      for (int q = SB - 1; q >= 1; --q) {
+        if (q < nb) {
+          const T vq = shfl_T(v, q);
+          v = F::fnma(Ls[q * (SB + 1) + lane], vq, v);
         }
       }
       if (ok) {
-        T* xo = Xw + (long long)(first + lp[p]) * a.ld;
-#pragma unroll
-        for (int c = 0; c < RHS_MAX; ++c)
-          if (c < a.nrhs) {
-            Z[(long long)p * a.ld + c] = v[c];
-            xo[c] = v[c];
-          }
+        Z[(long long)p * a.ld + c] = v;
+        Xw[(long long)(first + lp[p]) * a.ld + c] = v;
       }
     }
     __syncthreads();
   }
+}
+
+// Blocked backward solve of a wide supernode, block [jb, jb+64): in-block
+// substitution with L^T (Z already holds w - L21^T x - later blocks).
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_NT) k_btrsv_blk(SolveArgs a, const int4* __restrict__ tasks) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Ls = reinterpret_cast<T*>(smem_raw);  // 32 x 33
+  T* vb = Ls + SB * (SB + 1);              // 32 x RHS_MAX
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, jb = tk.y;
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
+  const int je = min(jb + TB, ncol);
+  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
+  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
+  bwd_block_range<T>(a, L, nrow, Z, nullptr, reinterpret_cast<T*>(a.Xg) + a.c0, a.lperm + first, first, jb, je,
+                     je, vb, Ls);
 }
 
 // Right-looking backward update after block [jb, jb+64) of a wide supernode:
@@ -537,99 +540,21 @@ __global__ void k_dsolve(int n, SolveArgs a) {
   }
 }
 
-// Backward solve of supernode s (one CTA): blocks of 32 pivots from the
-// last; each column dotted against the solved rows below it.
+// Backward solve of a narrow supernode s (one CTA): blocks of 32 pivots
+// from the last; the off-diagonal dots of k_bwd_off (Wb) come first.
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_bwd(SolveArgs a, const int* __restrict__ tasks) {
-  using F = Field<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* red = reinterpret_cast<T*>(smem_raw);
-  T* vb = red + (SOLVE_NT / 32) * 32 * RHS_MAX;  // [32 rows of the block] x RHS_MAX
+  T* Ls = reinterpret_cast<T*>(smem_raw);  // 32 x 33
+  T* vb = Ls + SB * (SB + 1);              // 32 x RHS_MAX
   const int s = tasks[blockIdx.x];
   const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
   const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
-  const int* lp = a.lperm + first;
   T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  const T* Wb = reinterpret_cast<const T*>(a.Wb) + a.c0 + (long long)first * a.ld;
-  T* Xw = reinterpret_cast<T*>(a.Xg) + a.c0;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int NW = SOLVE_NT / 32;
-  const int nblk = (ncol + SB - 1) / SB;
-  const bool has_off = nrow > ncol;  // Wb is written by k_bwd_off only then
-  for (int b = nblk - 1; b >= 0; --b) {
-    const int j0 = b * SB, nb = min(SB, ncol - j0), j1 = j0 + nb;
-    // acc[p][c] = sum_{r >= j1} L[r, p] * v(r): warp per column p, lanes over r.
-    for (int pc = warp; pc < nb; pc += NW) {
-      const int p = j0 + pc;
-      T acc[RHS_MAX];
-#pragma unroll
-      for (int c = 0; c < RHS_MAX; ++c) acc[c] = F::zero();
-      const T* Lc = L + (long long)p * nrow;
-      for (int r = j1 + lane; r < ncol; r += 32) {
-        T l = Lc[r];
-        const T* v = Z + (long long)r * a.ld;
-#pragma unroll
-        for (int c = 0; c < RHS_MAX; ++c)
-          if (c < a.nrhs) acc[c] = F::fma_(l, v[c], acc[c]);
-      }
-#pragma unroll
-      for (int c = 0; c < RHS_MAX; ++c) {
-        if (c >= a.nrhs) continue;
-        T x = acc[c];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          if constexpr (Field<T>::complex) {
-            x.re += __shfl_down_sync(0xffffffffu, x.re, o);
-            x.im += __shfl_down_sync(0xffffffffu, x.im, o);
-          } else {
-            x += __shfl_down_sync(0xffffffffu, x, o);
-          }
-        }
-        if (lane == 0) vb[pc * RHS_MAX + c] = x;
-      }
-    }
-    __syncthreads();
-    if (warp == 0) {
-      const int p = j0 + lane;
-      const bool ok = lane < nb;
-      T v[RHS_MAX];
-#pragma unroll
-      for (int c = 0; c < RHS_MAX; ++c)
-        v[c] = (ok && c < a.nrhs)
-                   ? F::sub(has_off ? F::sub(Z[(long long)p * a.ld + c], Wb[(long long)p * a.ld + c])
-                                    : Z[(long long)p * a.ld + c],
-                            vb[lane * RHS_MAX + c])
-                   : F::zero();
-      // Backward inside the block: v[p] -= L[q, p] v[q] for q > p.
-      for (int q = nb - 1; q >= 1; --q) {
-        const int qq = j0 + q;
-        T l = F::zero();
-        if (ok && lane < q) l = L[qq + (long long)p * nrow];
-#pragma unroll
-        for (int c = 0; c < RHS_MAX; ++c) {
-          if (c >= a.nrhs) continue;
-          T vq;
-          if constexpr (Field<T>::complex) {
-            vq.re = __shfl_sync(0xffffffffu, v[c].re, q);
-            vq.im = __shfl_sync(0xffffffffu, v[c].im, q);
-          } else {
-            vq = __shfl_sync(0xffffffffu, v[c], q);
-          }
-          v[c] = F::fnma(l, vq, v[c]);
-        }
-      }
-      if (ok) {
-        T* xo = Xw + (long long)(first + lp[p]) * a.ld;
-#pragma unroll
-        for (int c = 0; c < RHS_MAX; ++c)
-          if (c < a.nrhs) {
-            Z[(long long)p * a.ld + c] = v[c];
-            xo[c] = v[c];
-          }
-      }
-    }
-    __syncthreads();
-  }
+  // Wb is written by k_bwd_off only when the supernode has off-diagonal rows
+  const T* Wb = nrow > ncol ? reinterpret_cast<const T*>(a.Wb) + a.c0 + (long long)first * a.ld : nullptr;
+  bwd_block_range<T>(a, L, nrow, Z, Wb, reinterpret_cast<T*>(a.Xg) + a.c0, a.lperm + first, first, 0, ncol, ncol,
+                     vb, Ls);
 }
 
 // ---------------------------------------------------------------------------

@@ -68,7 +68,7 @@ size_t elem_size(int dtype) {
 enum LaunchKind {
   L_CMOD, L_GETF2, L_DEEP, L_SCHUR,
   L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD,
-  L_FTRSV_BLK, L_FTRSV_UPD, L_BTRSV_BLK, L_BTRSV_UPD
+  L_FTRSV_BLK, L_FTRSV_UPD, L_BTRSV_BLK, L_BTRSV_UPD, L_FWD_GATHER
 };
 struct Launch {
   int kind;
@@ -104,6 +104,8 @@ struct rslab_sym_handle {
   std::vector<int4> st4;  // blocked diagonal-solve tasks (s, j0, r0 | c0, 0)
   std::vector<long long> uoff;  // forward-push row offsets (nrow - ncol per supernode)
   long long urows = 0;
+  // forward pull lists: for column g, the U rows pushed into it (update order)
+  std::vector<int> pull_ptr, pull_src;
   std::vector<Launch> fplan, fwdplan, bwdplan;
   int max_getf2_tasks = 0;
   int max_nb = 64;
@@ -127,6 +129,7 @@ struct rslab_sym_handle {
   int2* d_t2 = nullptr;
   int4* d_st4 = nullptr;
   long long* d_uoff = nullptr;
+  int *d_pull_ptr = nullptr, *d_pull_src = nullptr;
   std::mutex mu;
   rslab_analyze_settings settings{};
 
@@ -178,6 +181,8 @@ struct rslab_sym_handle {
     d_t2 = up(t2, st);
     d_st4 = up(st4, st);
     d_uoff = up(uoff, st);
+    d_pull_ptr = up(pull_ptr, st);
+    d_pull_src = up(pull_src, st);
     CK(cudaStreamSynchronize(st));
     device = dev;
   }
@@ -209,6 +214,29 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
   for (int s = 0; s < ns; ++s) {
     H.uoff[s] = H.urows;
     H.urows += H.nrow[s] - S.sn[s].ncol;
+  }
+  if (H.urows >= (1LL << 31)) throw RslabError(Status::InvalidInput, "forward push buffer exceeds 2^31 rows");
+  // Pull lists: every off-diagonal row r of updater k (U row uoff[k] + r)
+  // lands on one column g of an ancestor; list the pushes per g in the
+  // ancestor's update-list order so the gather subtracts them in that order.
+  H.pull_ptr.assign(n + 1, 0);
+  for (int s = 0; s < ns; ++s)
+    for (int64_t u = S.upd_ptr[s]; u < S.upd_ptr[s + 1]; ++u) {
+      const int64_t k = S.upd[u];
+      const int64_t base = S.rs_ptr[k] + S.sn[k].ncol;
+      for (int64_t r = S.upd_p0[u]; r < S.upd_p1[u]; ++r) H.pull_ptr[S.rs[base + r] + 1]++;
+    }
+  for (int g = 0; g < n; ++g) H.pull_ptr[g + 1] += H.pull_ptr[g];
+  H.pull_src.assign(std::max(H.pull_ptr[n], 1), 0);
+  {
+    std::vector<int> cur(H.pull_ptr.begin(), H.pull_ptr.end() - 1);
+    for (int s = 0; s < ns; ++s)
+      for (int64_t u = S.upd_ptr[s]; u < S.upd_ptr[s + 1]; ++u) {
+        const int64_t k = S.upd[u];
+        const int64_t base = S.rs_ptr[k] + S.sn[k].ncol;
+        for (int64_t r = S.upd_p0[u]; r < S.upd_p1[u]; ++r)
+          H.pull_src[cur[S.rs[base + r]]++] = (int)(H.uoff[k] + r);
+      }
   }
   // Assembly targets: user (i, j) -> permuted lower (r, c) -> panel slot.
   std::vector<int> col2sn(n);
@@ -368,9 +396,16 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
     // row-tiled push.  Backward (run root first): column-chunked off-diagonal
     // dots, narrow diagonal blocks, then the wide ones block by block.
     {
-      Launch Dg{L_FWD_DIAG, (long long)H.t1.size(), (int)lvl.size(), 0};
-      for (int64_t s : lvl) H.t1.push_back((int)s);
-      H.fwdplan.push_back(Dg);
+      Launch Fg{L_FWD_GATHER, (long long)H.t2.size(), 0, 0};
+      for (int64_t s : lvl)
+        for (int p0 = 0; p0 < S.sn[s].ncol; p0 += SOLVE_NT / RHS_MAX) H.t2.push_back(make_int2((int)s, p0));
+      Fg.ntasks = (int)(H.t2.size() - Fg.task_off);
+      if (Fg.ntasks) H.fwdplan.push_back(Fg);
+      Launch Dg{L_FWD_DIAG, (long long)H.t1.size(), 0, 0};
+      for (int64_t s : lvl)
+        if (S.sn[s].ncol <= SOLVE_BIG) H.t1.push_back((int)s);
+      Dg.ntasks = (int)(H.t1.size() - Dg.task_off);
+      if (Dg.ntasks) H.fwdplan.push_back(Dg);
       int maxb = 0;
       for (int64_t s : lvl)
         if (S.sn[s].ncol > SOLVE_BIG) maxb = std::max(maxb, (int)((S.sn[s].ncol + TB - 1) / TB));
@@ -438,8 +473,8 @@ size_t smem_getf2(size_t es, int nb) {
   return std::max(a, b) + 64;
 }
 size_t smem_deep(size_t es, int nb) { return (size_t)(DEEP_R + 1) * nb * es + 64; }
-size_t smem_solve(size_t es) { return (size_t)(SOLVE_NT / 32) * 32 * RHS_MAX * es + 32 * RHS_MAX * es + 64 * 4; }
-size_t smem_push(size_t es) { return (size_t)4 * 64 * RHS_MAX * es; }
+size_t smem_solve(size_t es) { return ((size_t)(SOLVE_NT / 32) * 32 * RHS_MAX + SB * (SB + 1) + SB * RHS_MAX) * es; }
+size_t smem_push(size_t es) { return (size_t)(32 * 64 + 32 * RHS_MAX) * es; }
 size_t smem_dots(size_t es) { return (size_t)(32 * 33 + 32 * RHS_MAX) * es; }
 
 template <typename T>
@@ -453,11 +488,11 @@ struct KernelSetup {
     CK(cudaFuncSetAttribute(k_getf2<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_getf2(es, 128)));
     CK(cudaFuncSetAttribute(k_deep<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep(es, 128)));
     CK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
-    CK(cudaFuncSetAttribute(k_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
+    CK(cudaFuncSetAttribute(k_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
     CK(cudaFuncSetAttribute(k_fwd_push<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_push(es)));
     CK(cudaFuncSetAttribute(k_ftrsv_upd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_push(es)));
     CK(cudaFuncSetAttribute(k_ftrsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
-    CK(cudaFuncSetAttribute(k_btrsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
+    CK(cudaFuncSetAttribute(k_btrsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
     CK(cudaFuncSetAttribute(k_bwd_off<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
     CK(cudaFuncSetAttribute(k_btrsv_upd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
     done = true;
@@ -732,6 +767,8 @@ SolveArgs make_sargs(rslab_fac_handle& F, int ld, int c0, int nr) {
   a.U = F.Ub;
   a.Wb = F.Wb;
   a.uoff = H.d_uoff;
+  a.pull_ptr = H.d_pull_ptr;
+  a.pull_src = H.d_pull_src;
   a.ld = ld;
   a.c0 = c0;
   a.nrhs = nr;
@@ -753,6 +790,9 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
     SolveArgs sa = make_sargs<T>(F, nrhs, c0, nr);
     for (const Launch& L : H.fwdplan) {
       switch (L.kind) {
+        case L_FWD_GATHER:
+          k_fwd_gather<T><<<L.ntasks, SOLVE_NT, 0, st>>>(sa, H.d_t2 + L.task_off);
+          break;
         case L_FWD_DIAG:
           k_fwd_diag<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
           break;
@@ -775,13 +815,13 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
           k_bwd_off<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_t2 + L.task_off);
           break;
         case L_BTRSV_BLK:
-          k_btrsv_blk<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_st4 + L.task_off);
+          k_btrsv_blk<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_st4 + L.task_off);
           break;
         case L_BTRSV_UPD:
           k_btrsv_upd<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_st4 + L.task_off);
           break;
         default:
-          k_bwd<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
+          k_bwd<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_t1 + L.task_off);
       }
       if (prof) prof->mark(st, L.kind == L_BWD_OFF ? 4 : 5, L.ntasks, L.kind);
     }
