@@ -55,6 +55,35 @@ struct DFree {
   }
 };
 
+// Persistent per-handle device scratch addressed by slot: a slot is
+// reallocated only when a request outgrows it, so repeated refinement
+// solves run without cudaMalloc / cudaFree.
+struct Arena {
+  std::vector<std::unique_ptr<void, DFree>> buf;
+  std::vector<size_t> cap;
+  void* get(int slot, size_t bytes) {
+    bytes = std::max<size_t>(bytes, 256);
+    if ((int)buf.size() <= slot) {
+      buf.resize(slot + 1);
+      cap.resize(slot + 1, 0);
+    }
+    if (cap[slot] < bytes) {
+      buf[slot].reset();
+      cap[slot] = 0;
+      void* p = nullptr;
+      CK(cudaMalloc(&p, bytes));
+      buf[slot].reset(p);
+      cap[slot] = bytes;
+    }
+    return buf[slot].get();
+  }
+};
+// Arena slots of the mixed-precision driver.
+enum ArenaSlot {
+  A_R, A_DX, A_AX, A_NB, A_B, A_X, A_BEST, A_MASK, A_BC, A_XC, A_AXC,
+  A_GM_PART, A_GM_W, A_GM_R, A_GM_V, A_GM_Z
+};
+
 size_t elem_size(int dtype) {
   switch (dtype) {
     case RSLAB_F64: return 8;
@@ -544,6 +573,7 @@ struct rslab_fac_handle {
   // per-launch rows of the last factor/solve profile
   std::vector<int> tr_kind, tr_grid;
   std::vector<float> tr_ms;
+  Arena arena;  // mixed-precision refinement scratch
 
   ~rslab_fac_handle() {
     if (fgraph) cudaGraphExecDestroy(fgraph);
@@ -909,21 +939,14 @@ struct MixedCtx {
   rslab_fac_handle& F;
   int n, nrhs;
   cudaStream_t st;
-  std::vector<std::unique_ptr<void, DFree>> bufs;
   Hi *r = nullptr, *dx = nullptr, *ax = nullptr;
   unsigned long long* nb = nullptr;
   MixedCtx(rslab_fac_handle& f, int nr) : F(f), n(f.sym->n), nrhs(nr), st(f.st) {
-    const long long m = (long long)n * nrhs;
-    auto a = [&](size_t bytes) {
-      void* p = nullptr;
-      CK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
-      bufs.emplace_back(p);
-      return p;
-    };
-    r = (Hi*)a(m * sizeof(Hi));
-    dx = (Hi*)a(m * sizeof(Hi));
-    ax = (Hi*)a(m * sizeof(Hi));
-    nb = (unsigned long long*)a(3 * 64 * sizeof(unsigned long long));
+    const size_t bytes = (size_t)n * nrhs * sizeof(Hi);
+    r = (Hi*)F.arena.get(A_R, bytes);
+    dx = (Hi*)F.arena.get(A_DX, bytes);
+    ax = (Hi*)F.arena.get(A_AX, bytes);
+    nb = (unsigned long long*)F.arena.get(A_NB, (size_t)std::max(nrhs, 3) * 64 * sizeof(unsigned long long));
   }
   // dx = promote(F_lo^-1 demote(r)) for an n x k block (k <= nrhs, ld = k).
   void precond(const Hi* rr, Hi* out, int k) {

@@ -332,8 +332,9 @@ class LdltSymbolic:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            N.lib.rslab_free_symbolic(h)
+        lib = getattr(N, "lib", None)  # None during interpreter shutdown
+        if h and lib is not None:
+            lib.rslab_free_symbolic(h)
             self._h = None
 
     def info(self) -> N.SymbolicInfo:
@@ -400,8 +401,9 @@ class LdltSolver:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            N.lib.rslab_free_factor(h)
+        lib = getattr(N, "lib", None)  # None during interpreter shutdown
+        if h and lib is not None:
+            lib.rslab_free_factor(h)
             self._h = None
 
     @classmethod
@@ -515,8 +517,9 @@ class MixedLdltSolver:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            N.lib.rslab_free_factor(h)
+        lib = getattr(N, "lib", None)  # None during interpreter shutdown
+        if h and lib is not None:
+            lib.rslab_free_factor(h)
             self._h = None
 
     @classmethod
