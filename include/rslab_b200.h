@@ -85,7 +85,15 @@ typedef struct {
   int32_t scaling;             /* RSLAB_SCALING_* */
   int32_t use_graph;           /* capture factor / solve as CUDA graphs (1) */
   void* stream;                /* cudaStream_t to run on, or NULL for a private one */
+  int32_t schur_engine;        /* RSLAB_SCHUR_*: how f32/c32 descendant updates run */
 } rslab_factor_settings;
+
+/* Descendant (cmod) updates of the single-precision fields: 3xTF32 split
+ * products on the tcgen05 tensor cores with fp32 accumulation (default), or
+ * fp32 FMA on the CUDA cores in the oracle's operation order (bit-exact).
+ * FP64 fields always use FP64 FMA. */
+#define RSLAB_SCHUR_TENSOR 0
+#define RSLAB_SCHUR_FMA 1
 
 typedef struct {
   int64_t n, nnz, nsuper, nlevels;

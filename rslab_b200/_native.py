@@ -14,6 +14,7 @@ F64, C64, F32, C32 = 0, 1, 2, 3
 ORDER_AMD, ORDER_METIS_ND, ORDER_NATURAL, ORDER_GIVEN = 0, 1, 2, 3
 PIVOT_FAIL, PIVOT_PERTURB = 0, 1
 SCALING_ONEPASS, SCALING_IDENTITY = 0, 1
+SCHUR_TENSOR, SCHUR_FMA = 0, 1
 
 i64p = C.POINTER(C.c_int64)
 vp = C.c_void_p
@@ -39,6 +40,7 @@ class FactorSettings(C.Structure):
         ("scaling", C.c_int32),
         ("use_graph", C.c_int32),
         ("stream", vp),
+        ("schur_engine", C.c_int32),
     ]
 
 

@@ -18,6 +18,7 @@
 
 #include "../../include/rslab_b200.h"
 #include "device/factor_kernels.cuh"
+#include "device/cmod_tc.cuh"
 #include "device/solve_kernels.cuh"
 #include "host/host.hpp"
 
@@ -97,7 +98,7 @@ size_t elem_size(int dtype) {
 enum LaunchKind {
   L_CMOD, L_GETF2, L_DEEP, L_SCHUR,
   L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD,
-  L_FTRSV_BLK, L_FTRSV_UPD, L_BTRSV_BLK, L_BTRSV_UPD, L_FWD_GATHER
+  L_FTRSV_BLK, L_FTRSV_UPD, L_BTRSV_BLK, L_BTRSV_UPD, L_FWD_GATHER, L_CMOD_TC
 };
 struct Launch {
   int kind;
@@ -128,6 +129,7 @@ struct rslab_sym_handle {
   // plan
   std::vector<int4> t4;
   std::vector<int4> cpairs;   // cmod (k, a, q0, nr << 16 | nc) per tile, in update order
+  std::vector<int4> t4tc, cpairs_tc;  // the same for the 128 x 64 tensor-core tiles
   std::vector<int> t1;
   std::vector<int2> t2;
   std::vector<int4> st4;  // blocked diagonal-solve tasks (s, j0, r0 | c0, 0)
@@ -154,6 +156,7 @@ struct rslab_sym_handle {
   int* d_sp_ci = nullptr;
   int4* d_t4 = nullptr;
   int4* d_cpairs = nullptr;
+  int4 *d_t4tc = nullptr, *d_cpairs_tc = nullptr;
   int* d_t1 = nullptr;
   int2* d_t2 = nullptr;
   int4* d_st4 = nullptr;
@@ -206,6 +209,8 @@ struct rslab_sym_handle {
     d_sp_vmap = up(sp_vmap, st);
     d_t4 = up(t4, st);
     d_cpairs = up(cpairs, st);
+    d_t4tc = up(t4tc, st);
+    d_cpairs_tc = up(cpairs_tc, st);
     d_t1 = up(t1, st);
     d_t2 = up(t2, st);
     d_st4 = up(st4, st);
@@ -218,6 +223,71 @@ struct rslab_sym_handle {
 };
 
 namespace {
+
+// Append the cmod tiles (tr x tc) of every supernode of a level that has
+// updaters: task (s, rt << 16 | ct, pair_begin, pair_end) and its pairs
+// (k, a, q0, nr << 16 | nc) in update-list order.
+void add_cmod_tiles(rslab_sym_handle& H, const std::vector<int64_t>& lvl, int tr, int tcw, std::vector<int4>& tasks,
+                    std::vector<int4>& pairs, bool count_flops) {
+  const auto& S = H.S;
+  for (int64_t s : lvl) {
+    if (S.upd_ptr[s + 1] == S.upd_ptr[s]) continue;
+    const int nc = (int)S.sn[s].ncol, nr = H.nrow[s];
+    const int64_t first = S.sn[s].first_col;
+    const int64_t* rss = S.rs.data() + S.rs_ptr[s];
+    const int ntc = (nc + tcw - 1) / tcw, ntr = (nr + tr - 1) / tr;
+    std::vector<std::vector<int4>> tp((size_t)ntc * ntr);
+    for (int64_t u = S.upd_ptr[s]; u < S.upd_ptr[s + 1]; ++u) {
+      const int64_t k = S.upd[u], p0 = S.upd_p0[u], p1 = S.upd_p1[u];
+      const int64_t nck = S.sn[k].ncol;
+      const int64_t* ok = S.rs.data() + S.rs_ptr[k] + nck;
+      const int64_t nok = S.rs_ptr[k + 1] - S.rs_ptr[k] - nck;
+      // local row position of each of k's rows >= p0 in s (merge walk)
+      std::vector<int> rel(nok - p0);
+      int64_t pos = std::lower_bound(rss, rss + nr, ok[p0]) - rss;
+      for (int64_t r = p0; r < nok; ++r) {
+        while (rss[pos] < ok[r]) ++pos;
+        rel[r - p0] = (int)pos;
+      }
+      int64_t qa = p0;
+      while (qa < p1) {
+        const int64_t ct = (ok[qa] - first) / tcw;
+        int64_t qb = qa;
+        while (qb < p1 && (ok[qb] - first) / tcw == ct) ++qb;
+        // k's rows from the column run's first row on: the lower part
+        int64_t ra = qa;
+        while (ra < nok) {
+          const int rt = rel[ra - p0] / tr;
+          int64_t rb = ra;
+          while (rb < nok && rel[rb - p0] / tr == rt) ++rb;
+          tp[(size_t)ct * ntr + rt].push_back(
+              make_int4((int)k, (int)ra, (int)qa, (int)(((rb - ra) << 16) | (qb - qa))));
+          ra = rb;
+        }
+        qa = qb;
+      }
+    }
+    for (int ct = 0; ct < ntc; ++ct)
+      for (int rt = (ct * tcw) / tr; rt < ntr; ++rt) {
+        const auto& v = tp[(size_t)ct * ntr + rt];
+        if (v.empty()) continue;
+        if (count_flops)
+          for (const int4& pq : v) {
+            const double nrr = pq.w >> 16, ncc = pq.w & 0xffff;
+            // (r, c) pairs with r >= c in k's ordering, times nck multiply-adds
+            double cnt = 0;
+            for (int cj = 0; cj < (int)ncc; ++cj) {
+              const int lo = std::max(pq.y, pq.z + cj);
+              cnt += std::max(0, pq.y + (int)nrr - lo);
+            }
+            H.kind_flops[1] += 2.0 * cnt * (double)S.sn[pq.x].ncol;
+          }
+        const int pb = (int)pairs.size();
+        pairs.insert(pairs.end(), v.begin(), v.end());
+        tasks.push_back(make_int4((int)s, (rt << 16) | ct, pb, (int)pairs.size()));
+      }
+  }
+}
 
 // Build panel offsets, assembly targets, SpMV structure and the launch plan.
 void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_idx) {
@@ -318,66 +388,18 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
   std::vector<std::vector<Launch>> bw_levels;
   for (const auto& lvl : S.by_level) {
     // cmod tiles of every panel that has updaters, each with its precomputed
-    // list of (updater, row run, column run) pairs in update-list order.
+    // list of (updater, row run, column run) pairs in update-list order:
+    // TILE x TILE tiles for the CUDA-core kernel, TC_M x TC_N tiles for the
+    // tensor-core kernel of the single-precision fields.
     {
       Launch L{L_CMOD, (long long)H.t4.size(), 0, 0};
-      for (int64_t s : lvl) {
-        if (S.upd_ptr[s + 1] == S.upd_ptr[s]) continue;
-        const int nc = (int)S.sn[s].ncol, nr = H.nrow[s];
-        const int64_t first = S.sn[s].first_col;
-        const int64_t* rss = S.rs.data() + S.rs_ptr[s];
-        const int ntc = (nc + TILE - 1) / TILE, ntr = (nr + TILE - 1) / TILE;
-        std::vector<std::vector<int4>> tp((size_t)ntc * ntr);
-        for (int64_t u = S.upd_ptr[s]; u < S.upd_ptr[s + 1]; ++u) {
-          const int64_t k = S.upd[u], p0 = S.upd_p0[u], p1 = S.upd_p1[u];
-          const int64_t nck = S.sn[k].ncol;
-          const int64_t* ok = S.rs.data() + S.rs_ptr[k] + nck;
-          const int64_t nok = S.rs_ptr[k + 1] - S.rs_ptr[k] - nck;
-          // local row position of each of k's rows >= p0 in s (merge walk)
-          std::vector<int> rel(nok - p0);
-          int64_t pos = std::lower_bound(rss, rss + nr, ok[p0]) - rss;
-          for (int64_t r = p0; r < nok; ++r) {
-            while (rss[pos] < ok[r]) ++pos;
-            rel[r - p0] = (int)pos;
-          }
-          int64_t qa = p0;
-          while (qa < p1) {
-            const int64_t ct = (ok[qa] - first) / TILE;
-            int64_t qb = qa;
-            while (qb < p1 && (ok[qb] - first) / TILE == ct) ++qb;
-            int64_t ra = qa;
-            while (ra < nok) {
-              const int rt = rel[ra - p0] / TILE;
-              int64_t rb = ra;
-              while (rb < nok && rel[rb - p0] / TILE == rt) ++rb;
-              tp[(size_t)ct * ntr + rt].push_back(
-                  make_int4((int)k, (int)ra, (int)qa, (int)(((rb - ra) << 16) | (qb - qa))));
-              ra = rb;
-            }
-            qa = qb;
-          }
-        }
-        for (int ct = 0; ct < ntc; ++ct)
-          for (int rt = ct; rt < ntr; ++rt) {
-            const auto& v = tp[(size_t)ct * ntr + rt];
-            if (v.empty()) continue;
-            for (const int4& pq : v) {
-              const double nrr = pq.w >> 16, ncc = pq.w & 0xffff;
-              // (r, c) pairs with r >= c in k's ordering, times nck multiply-adds
-              double cnt = 0;
-              for (int cj = 0; cj < (int)ncc; ++cj) {
-                const int lo = std::max(pq.y, pq.z + cj);
-                cnt += std::max(0, pq.y + (int)nrr - lo);
-              }
-              H.kind_flops[1] += 2.0 * cnt * (double)S.sn[pq.x].ncol;
-            }
-            const int pb = (int)H.cpairs.size();
-            H.cpairs.insert(H.cpairs.end(), v.begin(), v.end());
-            H.t4.push_back(make_int4((int)s, (rt << 16) | ct, pb, (int)H.cpairs.size()));
-          }
-      }
+      add_cmod_tiles(H, lvl, TILE, TILE, H.t4, H.cpairs, true);
       L.ntasks = (int)(H.t4.size() - L.task_off);
       if (L.ntasks) H.fplan.push_back(L);
+      Launch Lt{L_CMOD_TC, (long long)H.t4tc.size(), 0, 0};
+      add_cmod_tiles(H, lvl, TC_M, TC_N, H.t4tc, H.cpairs_tc, false);
+      Lt.ntasks = (int)(H.t4tc.size() - Lt.task_off);
+      if (Lt.ntasks) H.fplan.push_back(Lt);
     }
     int maxblocks = 0;
     for (int64_t s : lvl) maxblocks = std::max(maxblocks, (int)((S.sn[s].ncol + nb_of(s) - 1) / nb_of(s)));
@@ -506,12 +528,19 @@ size_t smem_solve(size_t es) { return ((size_t)(SOLVE_NT / 32) * 32 * RHS_MAX + 
 size_t smem_push(size_t es) { return (size_t)(32 * 64 + 32 * RHS_MAX) * es; }
 size_t smem_dots(size_t es) { return (size_t)(32 * 33 + 32 * RHS_MAX) * es; }
 
+// Fields whose descendant updates can run on the tf32 tensor cores.
+template <typename T> struct TensorCmod { static constexpr bool ok = false; };
+template <> struct TensorCmod<float> { static constexpr bool ok = true; };
+template <> struct TensorCmod<c32> { static constexpr bool ok = true; };
+
 template <typename T>
 struct KernelSetup {
   static void configure() {
     static bool done = false;
     if (done) return;
     const size_t es = sizeof(T);
+    if constexpr (TensorCmod<T>::ok)
+      CK(cudaFuncSetAttribute(k_cmod_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_tc_bytes()));
     CK(cudaFuncSetAttribute(k_cmod<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod(es)));
     CK(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
     CK(cudaFuncSetAttribute(k_getf2<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_getf2(es, 128)));
@@ -673,11 +702,21 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
                                                 (T*)F.panel);
   FactorArgs fa = make_fargs<T>(F);
   const int nb_small = H.panel_nb, nb_big = std::max(H.panel_nb, 128);
+  const bool use_tc = TensorCmod<T>::ok && F.set.schur_engine == RSLAB_SCHUR_TENSOR;
   if (prof) prof->mark(st, 0);
   for (const Launch& L : H.fplan) {
     switch (L.kind) {
       case L_CMOD:
+        if (use_tc) continue;
         k_cmod<T><<<L.ntasks, TPB, smem_cmod(es), st>>>(fa, H.d_t4 + L.task_off, H.d_cpairs);
+        break;
+      case L_CMOD_TC:
+        if constexpr (TensorCmod<T>::ok) {
+          if (!use_tc) continue;
+          k_cmod_tc<T><<<L.ntasks, TC_NT, smem_cmod_tc_bytes(), st>>>(fa, H.d_t4tc + L.task_off, H.d_cpairs_tc);
+        } else {
+          continue;
+        }
         break;
       case L_GETF2: {
         FactorArgs f2 = fa;
@@ -695,7 +734,9 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         k_schur<T><<<L.ntasks, TPB, smem_schur(es), st>>>(fa, H.d_t4 + L.task_off, nb_small, nb_big);
         break;
     }
-    if (prof) prof->mark(st, L.kind == L_CMOD ? 1 : L.kind == L_GETF2 ? 2 : L.kind == L_DEEP ? 3 : 4, L.ntasks, L.kind);
+    if (prof)
+      prof->mark(st, (L.kind == L_CMOD || L.kind == L_CMOD_TC) ? 1 : L.kind == L_GETF2 ? 2 : L.kind == L_DEEP ? 3 : 4,
+                 L.ntasks, L.kind);
   }
   CK(cudaMemsetAsync(F.cnt3, 0, 3 * sizeof(unsigned long long), st));
   k_inertia<T><<<grid1(n), 256, 0, st>>>(n, (const T*)F.d, (const T*)F.dsub, F.kind, F.cnt3);
@@ -734,6 +775,11 @@ void run_factor(rslab_fac_handle& F) {
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, F.ev0, F.ev1));
   F.factor_ms = ms;
+  if (F.h_status[0] == 2) {
+    F.last_status = 2;
+    throw RslabError(Status::CudaError, "tensor-core pipeline wait timed out in supernode " +
+                                            std::to_string(F.h_status[1]));
+  }
   F.last_status = F.h_status[0];
   F.failing_sn = F.h_status[0] ? F.h_status[1] : -1;
   F.nperturbed = F.h_status[2];
@@ -1015,6 +1061,7 @@ void rslab_default_factor_settings(rslab_factor_settings* s) {
   s->scaling = RSLAB_SCALING_ONEPASS;
   s->use_graph = 1;
   s->stream = nullptr;
+  s->schur_engine = RSLAB_SCHUR_TENSOR;
 }
 
 int rslab_analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, const rslab_analyze_settings* settings,

@@ -199,6 +199,9 @@ class SolverSettings:
     scaling: str = "onepass"  # or "identity"
     use_graph: bool = True
     given_perm: Optional[np.ndarray] = None
+    # f32/c32 descendant updates: "tensor" (3xTF32 tcgen05) or "fma" (CUDA-core
+    # fp32 in the oracle's operation order, bit-exact)
+    schur_engine: str = "tensor"
 
     @staticmethod
     def exact() -> "SolverSettings":
@@ -259,6 +262,7 @@ class SolverSettings:
         s.scaling = N.SCALING_ONEPASS if self.scaling == "onepass" else N.SCALING_IDENTITY
         s.use_graph = int(self.use_graph)
         s.stream = stream
+        s.schur_engine = N.SCHUR_FMA if self.schur_engine == "fma" else N.SCHUR_TENSOR
         return s
 
 
