@@ -50,6 +50,9 @@ def parse():
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--cpu-sample-side", type=int, default=28)
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--profile-step", action="store_true",
+                   help="one warm-up mixed step, then exactly one mixed step between "
+                        "cudaProfilerStart/Stop (for ncu --profile-from-start off); no JSON line")
     return p.parse_args()
 
 
@@ -224,6 +227,15 @@ def main():
                                      C.c_void_p(x_d.data_ptr()), 1, C.byref(inf))
         assert rc == 0, N.last_error()
         return inf
+
+    if args.profile_step:
+        mixed_step()
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStart()
+        mixed_step()
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStop()
+        return
 
     def timed(fn, steps, warm):
         for _ in range(warm):

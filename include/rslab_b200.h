@@ -164,7 +164,7 @@ int rslab_solve_profile(rslab_fac_handle* fac, int64_t nrhs, double* kind_ms, in
  * (0 cmod, 1 getf2, 2 deep replay, 3 panel Schur, 4 forward diagonal,
  * 5 forward push, 6 backward dots, 7 backward diagonal, 8/9 blocked forward
  * diagonal/update, 10/11 blocked backward diagonal/update, 12 forward
- * gather, -1 other), grid
+ * gather, 13 tensor-core cmod, -1 other), grid
  * size and device ms.  *count = rows available; at most cap are written.
  * A measurement aid with no reference counterpart. */
 int rslab_profile_trace(const rslab_fac_handle* fac, int64_t cap, int32_t* kind, int32_t* grid, float* ms,

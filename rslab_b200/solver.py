@@ -607,7 +607,7 @@ def solve_profile(handle, nrhs: int) -> dict:
 
 
 LAUNCH_KINDS = ("cmod", "getf2", "deep_replay", "panel_schur", "fwd_diag", "fwd_push", "bwd_off", "bwd_diag",
-                "ftrsv_blk", "ftrsv_upd", "btrsv_blk", "btrsv_upd", "fwd_gather")
+                "ftrsv_blk", "ftrsv_upd", "btrsv_blk", "btrsv_upd", "fwd_gather", "cmod_tc")
 
 
 def profile_trace(handle) -> list:
