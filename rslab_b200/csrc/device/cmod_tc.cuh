@@ -1,7 +1,7 @@
 // Tensor-core cmod for the single-precision factor fields (f32, c32):
 // the descendant updates of one 128 x 64 target tile accumulate in TMEM with
-// tcgen05.mma kind::tf32 in the 3xTF32 split (hi*hi + hi*lo + lo*hi, fp32
-// accuracy), and the tile is read-modify-written once at the end.
+// tcgen05.mma kind::tf32 in the 3xTF32 split (hi*hi + hi*lo + lo*hi), and the
+// tile is read-modify-written once at the end.
 //
 // Task (s, rt << 16 | ct, pair_begin, pair_end): tile rows [128 rt, +128) x
 // columns [64 ct, +64) of s's panel.  Pair (k, a, q0, nr << 16 | nc): k's
@@ -14,10 +14,18 @@
 // columns.  Complex operands use the real embedding
 //   A' = [Ar | Ai],  B' = [[Gr, -Gi], [Gi, Gr]]  ->  A' B'^T = [Re | Im],
 // i.e. M = 128, N = 128, and 16 complex columns of k per 32-wide K stage.
-// Two stages: staging of chunk i+1 overlaps the MMAs of chunk i; one thread
-// issues the MMAs and commits them to the stage's mbarrier, which gates the
-// reuse of that stage.  Every wait is bounded; on a timeout the kernel flags
-// status 2, drains what it issued (bounded) and frees its TMEM.
+//
+// Pipeline (512 threads, one CTA per SM): the global loads of K chunk c+1
+// are issued into registers right after chunk c's MMAs, so their latency
+// overlaps the tensor work; two shared-memory stages gated by mbarriers that
+// tcgen05.commit arrives on; the scatter maps of the next pair are built one
+// pair ahead (double-buffered), leaving one block barrier per chunk.
+// Accuracy: the tensor pipe does not round its accumulation to nearest, so
+// the sum runs in windows of TC_WIN chunks over two TMEM accumulators; each
+// finished window is added into per-thread fp32 registers (round to nearest)
+// while the next window runs on the other accumulator.
+// Every wait is bounded; on a timeout the kernel flags status 2, drains what
+// it issued (bounded) and frees its TMEM.
 // Reference: ll_factor_node cmod, src/numeric/multifrontal_ldlt.rs:2452-2728.
 #pragma once
 
@@ -28,10 +36,12 @@ namespace rsd {
 
 constexpr int TC_M = 128;                 // target tile rows = UMMA M
 constexpr int TC_N = 64;                  // target tile columns
-constexpr int TC_NT = 256;                // threads per CTA
+constexpr int TC_NT = 512;                // threads per CTA
 constexpr int TC_OPER = 16384;            // bytes of one 128 x 32 fp32 operand tile
 constexpr int TC_STAGE = 4 * TC_OPER;     // A hi, A lo, B hi, B lo
-constexpr uint32_t TC_TMEM_COLS = 128;
+constexpr int TC_WIN = 4;                 // K chunks per TMEM accumulation window
+constexpr uint32_t TC_ACC_COLS = 128;     // TMEM columns of one accumulator
+constexpr uint32_t TC_TMEM_COLS = 2 * TC_ACC_COLS;
 
 template <typename T> struct TcShape;
 template <> struct TcShape<float> {
@@ -44,130 +54,150 @@ template <> struct TcShape<c32> {
 };
 
 __host__ __device__ constexpr size_t smem_cmod_tc_bytes() {
-  return 1024 + 2 * (size_t)TC_STAGE + (TC_M + TC_M + TC_N) * 4 + 64;
+  return 1024 + 2 * (size_t)TC_STAGE + (TC_M + 2 * TC_M + 2 * TC_N) * 4 + 64;
 }
 
-__device__ __forceinline__ void store_split4(unsigned char* hi_tile, unsigned char* lo_tile, int row, int k4,
-                                             const float (&v)[4]) {
+// Per-thread staging values of one K chunk: A' 8 floats, B' 4 floats.
+struct TcRegs {
+  float a[8];
+  float b[4];
+};
+
+// hi/lo split of 4 (or 2) consecutive K elements starting at element k of an
+// operand row, stored into the hi and lo tiles.
+__device__ __forceinline__ void store_split4(unsigned char* hi_tile, unsigned char* lo_tile, int row, int k,
+                                             float x0, float x1, float x2, float x3) {
   float4 h, l;
-  split_tf32(v[0], h.x, l.x);
-  split_tf32(v[1], h.y, l.y);
-  split_tf32(v[2], h.z, l.z);
-  split_tf32(v[3], h.w, l.w);
-  const uint32_t off = sw128_off((uint32_t)row, (uint32_t)(4 * k4));
+  split_tf32(x0, h.x, l.x);
+  split_tf32(x1, h.y, l.y);
+  split_tf32(x2, h.z, l.z);
+  split_tf32(x3, h.w, l.w);
+  const uint32_t off = sw128_off((uint32_t)row, (uint32_t)k);
   *reinterpret_cast<float4*>(hi_tile + off) = h;
   *reinterpret_cast<float4*>(lo_tile + off) = l;
 }
 
-// Stage one K chunk of pair (k, a, q0) into the operand tiles of a stage.
+__device__ __forceinline__ void store_split2(unsigned char* hi_tile, unsigned char* lo_tile, int row, int k, float x0,
+                                             float x1) {
+  float2 h, l;
+  split_tf32(x0, h.x, l.x);
+  split_tf32(x1, h.y, l.y);
+  const uint32_t off = sw128_off((uint32_t)row, (uint32_t)k);
+  *reinterpret_cast<float2*>(hi_tile + off) = h;
+  *reinterpret_cast<float2*>(lo_tile + off) = l;
+}
+
+// Global loads of K chunk [t0, t0 + kc) of a pair into registers.
+//   c32: A' row tid & 127, complex columns 4 (tid >> 7) .. +4;
+//        B' column tid & 63, complex columns 2 (tid >> 6) .. +2.
+//   f32: A' row tid & 127, columns 8 (tid >> 7) .. +8;
+//        B' column tid & 63, columns 4 (tid >> 6) .. +4.
 template <typename T>
-__device__ __forceinline__ void tc_stage(unsigned char* stg, const T* __restrict__ LA, const T* __restrict__ LB,
-                                         int nrk, int nck, int t0, const int* invrow, const int* invcol,
-                                         const T* __restrict__ dk, const T* __restrict__ dsk,
-                                         const unsigned char* __restrict__ kindk) {
+__device__ __forceinline__ void tc_load(TcRegs& R, const T* __restrict__ LA, const T* __restrict__ LB, int nrk,
+                                        int nck, int t0, const int* invrow, const int* invcol,
+                                        const T* __restrict__ dk, const T* __restrict__ dsk,
+                                        const unsigned char* __restrict__ kindk) {
   using F = Field<T>;
+  const int tid = threadIdx.x;
+  const int row = tid & (TC_M - 1), ga = tid >> 7;
+  const int u = tid & (TC_N - 1), gb = tid >> 6;
+  const int i = invrow[row], j = invcol[u];
+  if constexpr (Field<T>::complex) {
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int t = t0 + 4 * ga + jj;
+      T v = F::zero();
+      if (i >= 0 && t < nck) v = LA[i + (long long)t * nrk];
+      R.a[jj] = v.re;
+      R.a[4 + jj] = v.im;
+    }
+#pragma unroll
+    for (int jj = 0; jj < 2; ++jj) {
+      const int t = t0 + 2 * gb + jj;
+      T v = F::zero();
+      if (j >= 0 && t < nck) v = ld_G(LB, nrk, j, t, dk, dsk, kindk);
+      R.b[2 * jj] = v.re;
+      R.b[2 * jj + 1] = v.im;
+    }
+  } else {
+#pragma unroll
+    for (int jj = 0; jj < 8; ++jj) {
+      const int t = t0 + 8 * ga + jj;
+      R.a[jj] = (i >= 0 && t < nck) ? LA[i + (long long)t * nrk] : 0.0f;
+    }
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int t = t0 + 4 * gb + jj;
+      R.b[jj] = (j >= 0 && t < nck) ? ld_G(LB, nrk, j, t, dk, dsk, kindk) : 0.0f;
+    }
+  }
+}
+
+// Registers -> hi/lo operand tiles of a stage (K-major, 128-byte swizzle).
+template <typename T>
+__device__ __forceinline__ void tc_store(const TcRegs& R, unsigned char* stg) {
   unsigned char* Ah = stg;
   unsigned char* Al = stg + TC_OPER;
   unsigned char* Bh = stg + 2 * TC_OPER;
   unsigned char* Bl = stg + 3 * TC_OPER;
   const int tid = threadIdx.x;
+  const int row = tid & (TC_M - 1), ga = tid >> 7;
+  const int u = tid & (TC_N - 1), gb = tid >> 6;
   if constexpr (Field<T>::complex) {
-    {  // A': row t <- k row invrow[t]; chunks 0-3 real parts, 4-7 imaginary parts
-      const int row = tid & (TC_M - 1), grp = tid >> 7;
-      const int i = invrow[row];
-#pragma unroll
-      for (int gi = 0; gi < 2; ++gi) {
-        const int g = grp + 2 * gi;
-        float re[4], im[4];
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) {
-          const int t = t0 + 4 * g + jj;
-          T v = F::zero();
-          if (i >= 0 && t < nck) v = LA[i + (long long)t * nrk];
-          re[jj] = v.re;
-          im[jj] = v.im;
-        }
-        store_split4(Ah, Al, row, g, re);
-        store_split4(Ah, Al, row, 4 + g, im);
-      }
-    }
-    {  // B': row u (Re out) = [Gr, -Gi], row 64 + u (Im out) = [Gi, Gr]
-      const int u = tid & (TC_N - 1), g = tid >> 6;
-      const int j = invcol[u];
-      float gr[4], gi[4], ngi[4];
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj) {
-        const int t = t0 + 4 * g + jj;
-        T v = F::zero();
-        if (j >= 0 && t < nck) v = ld_G(LB, nrk, j, t, dk, dsk, kindk);
-        gr[jj] = v.re;
-        gi[jj] = v.im;
-        ngi[jj] = -v.im;
-      }
-      store_split4(Bh, Bl, u, g, gr);
-      store_split4(Bh, Bl, u, 4 + g, ngi);
-      store_split4(Bh, Bl, TC_N + u, g, gi);
-      store_split4(Bh, Bl, TC_N + u, 4 + g, gr);
-    }
+    store_split4(Ah, Al, row, 4 * ga, R.a[0], R.a[1], R.a[2], R.a[3]);       // Re(A): K' 0..15
+    store_split4(Ah, Al, row, 16 + 4 * ga, R.a[4], R.a[5], R.a[6], R.a[7]);  // Im(A): K' 16..31
+    const int k = 2 * gb;
+    store_split2(Bh, Bl, u, k, R.b[0], R.b[2]);              // Re out:  Gr
+    store_split2(Bh, Bl, u, 16 + k, -R.b[1], -R.b[3]);       //         -Gi
+    store_split2(Bh, Bl, TC_N + u, k, R.b[1], R.b[3]);       // Im out:  Gi
+    store_split2(Bh, Bl, TC_N + u, 16 + k, R.b[0], R.b[2]);  //          Gr
   } else {
-    {
-      const int row = tid & (TC_M - 1), grp = tid >> 7;
-      const int i = invrow[row];
-#pragma unroll
-      for (int gi = 0; gi < 4; ++gi) {
-        const int g = grp + 2 * gi;
-        float v[4];
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) {
-          const int t = t0 + 4 * g + jj;
-          v[jj] = (i >= 0 && t < nck) ? LA[i + (long long)t * nrk] : 0.0f;
-        }
-        store_split4(Ah, Al, row, g, v);
-      }
-    }
-    {
-      const int u = tid & (TC_N - 1), grp = tid >> 6;
-      const int j = invcol[u];
-#pragma unroll
-      for (int gi = 0; gi < 2; ++gi) {
-        const int g = grp + 4 * gi;
-        float v[4];
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) {
-          const int t = t0 + 4 * g + jj;
-          v[jj] = (j >= 0 && t < nck) ? ld_G(LB, nrk, j, t, dk, dsk, kindk) : 0.0f;
-        }
-        store_split4(Bh, Bl, u, g, v);
-      }
-    }
+    store_split4(Ah, Al, row, 8 * ga, R.a[0], R.a[1], R.a[2], R.a[3]);
+    store_split4(Ah, Al, row, 8 * ga + 4, R.a[4], R.a[5], R.a[6], R.a[7]);
+    store_split4(Bh, Bl, u, 4 * gb, R.b[0], R.b[1], R.b[2], R.b[3]);
   }
+}
+
+template <int NC>
+__device__ __forceinline__ void tmem_ld_cols(uint32_t taddr, float (&v)[NC]);
+template <>
+__device__ __forceinline__ void tmem_ld_cols<32>(uint32_t taddr, float (&v)[32]) {
+  tmem_ld32(taddr, v);
+}
+template <>
+__device__ __forceinline__ void tmem_ld_cols<16>(uint32_t taddr, float (&v)[16]) {
+  tmem_ld16(taddr, v);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4* __restrict__ tasks,
                                                       const int4* __restrict__ pairs) {
-  using F = Field<T>;
   using Sh = TcShape<T>;
+  constexpr int NC = Sh::n / 4;  // accumulator columns per thread
   if (fa.status[0] != 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];  // re-aligned to 1024 below
   const uint32_t sraw = smem_u32(smem_raw);
   unsigned char* sm = smem_raw + (((sraw + 1023u) & ~1023u) - sraw);
-  int* rs_tile = reinterpret_cast<int*>(sm + 2 * TC_STAGE);  // TC_M
-  int* invrow = rs_tile + TC_M;                              // TC_M
-  int* invcol = invrow + TC_M;                               // TC_N
-  uint64_t* bar = reinterpret_cast<uint64_t*>(invcol + TC_N);  // 2
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
+  int* rs_tile = reinterpret_cast<int*>(sm + 2 * TC_STAGE);         // TC_M
+  int* invrow = rs_tile + TC_M;                                     // 2 x TC_M
+  int* invcol = invrow + 2 * TC_M;                                  // 2 x TC_N
+  uint64_t* sbar = reinterpret_cast<uint64_t*>(invcol + 2 * TC_N);  // 2 stage barriers
+  uint64_t* wbar = sbar + 2;                                        // 2 window barriers
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(wbar + 2);
 
   const int4 tk = tasks[blockIdx.x];
   const int s = tk.x, r0 = (tk.y >> 16) * TC_M, c0 = (tk.y & 0xffff) * TC_N;
+  const int pb = tk.z, pe = tk.w;
   const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
   const int rows_here = min(TC_M, nrow - r0), cols_here = min(TC_N, ncol - c0);
   const int* rss = fa.rs + fa.sn_rsoff[s];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid < TC_M) rs_tile[tid] = tid < rows_here ? rss[r0 + tid] : INT_MAX;
   if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    mbar_init(&sbar[0], 1);
+    mbar_init(&sbar[1], 1);
+    mbar_init(&wbar[0], 1);
+    mbar_init(&wbar[1], 1);
     fence_mbar_init();
   }
   if (warp == 0) tmem_alloc(tslot, TC_TMEM_COLS);
@@ -180,96 +210,146 @@ __global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4*
   const T* dall = reinterpret_cast<const T*>(fa.d);
   const T* dsall = reinterpret_cast<const T*>(fa.dsub);
   const T* pall = reinterpret_cast<const T*>(fa.panel);
-  int it = 0;        // K chunks issued
-  bool ok = true;    // every wait so far completed (uniform across the CTA)
-  for (int u = tk.z; u < tk.w && ok; ++u) {
+
+  // Scatter maps of pair u live in buffer (u - pb) & 1: invrow[t] = index of
+  // the k row landing on tile row t (or -1), invcol[v] likewise for columns.
+  // Built in two phases a block barrier apart: clear, then fill.
+  auto clear_maps = [&](int b) {
+    if (tid < TC_M) invrow[b * TC_M + tid] = -1;
+    else if (tid < TC_M + TC_N) invcol[b * TC_N + tid - TC_M] = -1;
+  };
+  auto fill_maps = [&](int u) {
+    const int b = (u - pb) & 1;
     const int4 pr = pairs[u];
     const int k = pr.x, a = pr.y, q0 = pr.z, nr = pr.w >> 16, nc = pr.w & 0xffff;
+    const int* okr = fa.rs + fa.sn_rsoff[k] + fa.sn_ncol[k];
+    if (tid < nr) invrow[b * TC_M + lower_bound_i(rs_tile, 0, rows_here, okr[a + tid])] = tid;
+    else if (tid >= TC_M && tid - TC_M < nc) invcol[b * TC_N + okr[q0 + tid - TC_M] - first - c0] = tid - TC_M;
+  };
+  auto load_chunk = [&](TcRegs& R, int u, int t0) {
+    const int4 pr = pairs[u];
+    const int k = pr.x, a = pr.y, q0 = pr.z;
     const int nck = fa.sn_ncol[k], nrk = fa.sn_nrow[k], fk = fa.sn_first[k];
-    const int* okr = fa.rs + fa.sn_rsoff[k] + nck;
-    __syncthreads();  // the previous pair's staging no longer reads the maps
-    if (tid < TC_M) invrow[tid] = -1;
-    if (tid < TC_N) invcol[tid] = -1;
+    const T* Lk = pall + fa.sn_poff[k] + nck;
+    const int b = (u - pb) & 1;
+    tc_load<T>(R, Lk + a, Lk + q0, nrk, nck, t0, invrow + b * TC_M, invcol + b * TC_N, dall + fk, dsall + fk,
+               fa.kind + fk);
+  };
+
+  float acc[NC];
+#pragma unroll
+  for (int j = 0; j < NC; ++j) acc[j] = 0.0f;
+  const int q = warp & 3, cg = warp >> 2;  // TMEM lane quarter, column group
+  bool ok = true;
+  // Add finished window w into the registers (waits for its MMAs).
+  auto promote = [&](int w) {
+    const bool done = mbar_wait_bounded(&wbar[w & 1], (uint32_t)((w >> 1) & 1));
+    if (__syncthreads_or(!done)) {
+      ok = false;
+      return;
+    }
+    tc_fence_after();
+    float v[NC];
+    tmem_ld_cols<NC>(tmem + (uint32_t)(w & 1) * TC_ACC_COLS + ((uint32_t)(32 * q) << 16) + (uint32_t)(cg * NC), v);
+#pragma unroll
+    for (int j = 0; j < NC; ++j) acc[j] += v[j];
+    tc_fence_before();
+  };
+
+  int c = 0;  // K chunks issued
+  if (pb < pe) {
+    clear_maps(0);
+    if (pb + 1 < pe) clear_maps(1);
     __syncthreads();
-    if (tid < nr) invrow[lower_bound_i(rs_tile, 0, rows_here, okr[a + tid])] = tid;
-    if (tid < nc) invcol[okr[q0 + tid] - first - c0] = tid;
+    fill_maps(pb);
+    if (pb + 1 < pe) fill_maps(pb + 1);
     __syncthreads();
-    const T* Lk = pall + fa.sn_poff[k];
-    for (int t0 = 0; t0 < nck; t0 += Sh::kc) {
-      const int st = it & 1;
-      unsigned char* stg = sm + st * TC_STAGE;
-      if (it >= 2) {
-        const bool done = mbar_wait_bounded(&bar[st], (uint32_t)(((it >> 1) - 1) & 1));
+    TcRegs R;
+    load_chunk(R, pb, 0);
+    int u = pb, t0 = 0;
+    while (u < pe) {
+      const int st = c & 1;
+      if (c >= 2) {
+        const bool done = mbar_wait_bounded(&sbar[st], (uint32_t)(((c >> 1) - 1) & 1));
         if (__syncthreads_or(!done)) {
           ok = false;
           break;
         }
       }
-      tc_stage<T>(stg, Lk + nck + a, Lk + nck + q0, nrk, nck, t0, invrow, invcol, dall + fk, dsall + fk,
-                  fa.kind + fk);
+      unsigned char* stg = sm + st * TC_STAGE;
+      tc_store<T>(R, stg);
+      // next chunk in (pair, column) order
+      int u2 = u, t2 = t0 + Sh::kc;
+      if (t2 >= fa.sn_ncol[pairs[u].x]) {
+        u2 = u + 1;
+        t2 = 0;
+      }
+      const bool last = u2 >= pe;
+      // On the first chunk of pair u > pb, the map buffer of pair u + 1 is
+      // free: its previous user, pair u - 1, read it last one iteration back
+      // (before that iteration's barrier).  Clear it before this barrier and
+      // fill it after; its first reader is the load of pair u + 1's first
+      // chunk, behind the next barrier (or the extra one below when pair u
+      // has a single chunk).
+      const bool mk = t0 == 0 && u > pb && u + 1 < pe;
+      if (mk) clear_maps((u + 1 - pb) & 1);
       fence_proxy_async_smem();
       __syncthreads();
+      const int w = c / TC_WIN;
       if (tid == 0) {
         tc_fence_after();
         const uint32_t sa = smem_u32(stg);
-        uint32_t acc = it > 0 ? 1u : 0u;
+        const uint32_t dacc = tmem + (uint32_t)(w & 1) * TC_ACC_COLS;
+        uint32_t accf = (c % TC_WIN) != 0 ? 1u : 0u;
 #pragma unroll
         for (int p = 0; p < 3; ++p) {
           const uint32_t at = sa + (p == 2 ? TC_OPER : 0);
           const uint32_t bt = sa + 2 * TC_OPER + (p == 1 ? TC_OPER : 0);
 #pragma unroll
           for (int ks = 0; ks < 4; ++ks) {
-            mma_tf32(tmem, desc_sw128(at + 32u * ks), desc_sw128(bt + 32u * ks), idesc, acc);
-            acc = 1u;
+            mma_tf32(dacc, desc_sw128(at + 32u * ks), desc_sw128(bt + 32u * ks), idesc, accf);
+            accf = 1u;
           }
         }
-        mma_commit(&bar[st]);
+        mma_commit(&sbar[st]);
+        if (c % TC_WIN == TC_WIN - 1 || last) mma_commit(&wbar[w & 1]);
       }
-      ++it;
+      if (mk) {
+        fill_maps(u + 1);
+        if (t2 == 0) __syncthreads();  // single-chunk pair: the load below reads those maps
+      }
+      if (!last) load_chunk(R, u2, t2);
+      if (c % TC_WIN == 0 && c >= TC_WIN) promote(w - 1);
+      ++c;
+      u = u2;
+      t0 = t2;
+      if (!ok) break;
     }
   }
-  // Drain: the last commit covers every MMA issued before it.
-  if (it > 0) {
-    const int last = it - 1;
-    const bool done = mbar_wait_bounded(&bar[last & 1], (uint32_t)((last >> 1) & 1));
-    if (__syncthreads_or(!done)) ok = false;
-  }
-  tc_fence_after();
+  if (c > 0 && ok) promote((c - 1) / TC_WIN);
   if (!ok) {
+    // drain what was issued (bounded), then report
+    if (c > 0) (void)mbar_wait_bounded(&sbar[(c - 1) & 1], (uint32_t)(((c - 1) >> 1) & 1));
     if (tid == 0 && atomicCAS(&fa.status[0], 0, 2) == 0) fa.status[1] = s;
-  } else if (it > 0) {
-    // Epilogue: warp w reads TMEM lanes 32 (w & 3) .. +32 (tile rows) and
-    // tile columns 32 (w >> 2) .. +32; P -= U on the lower part only.
-    T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
-    const int q = warp & 3, h = warp >> 2;
+  } else if (c > 0) {
+    // Epilogue: P -= U on the lower part.  Thread (q, cg, lane) holds tile
+    // row 32 q + lane and accumulator columns [cg NC, cg NC + NC): for c32
+    // columns 0-63 are the real parts and 64-127 the imaginary parts of tile
+    // columns 0-63; each thread updates its own component.
     const int row = 32 * q + lane;
-    const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16);
-    float re[32];
-    tmem_ld32(tl + 32u * h, re);
-    if constexpr (Field<T>::complex) {
-      float im[32];
-      tmem_ld32(tl + (uint32_t)TC_N + 32u * h, im);
-      if (row < rows_here) {
-        const int gr = r0 + row;
+    if (row < rows_here) {
+      const int gr = r0 + row;
+      float* pf = reinterpret_cast<float*>(reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s]);
 #pragma unroll
-        for (int jj = 0; jj < 32; ++jj) {
-          const int col = 32 * h + jj, gc = c0 + col;
-          if (col < cols_here && gr >= gc) {
-            T* p = panel + gr + (long long)gc * nrow;
-            T v = *p;
-            v.re -= re[jj];
-            v.im -= im[jj];
-            *p = v;
-          }
-        }
-      }
-    } else {
-      if (row < rows_here) {
-        const int gr = r0 + row;
-#pragma unroll
-        for (int jj = 0; jj < 32; ++jj) {
-          const int col = 32 * h + jj, gc = c0 + col;
-          if (col < cols_here && gr >= gc) panel[gr + (long long)gc * nrow] -= re[jj];
+      for (int jj = 0; jj < NC; ++jj) {
+        const int colj = cg * NC + jj;
+        const int col = Field<T>::complex ? (colj & (TC_N - 1)) : colj;
+        const int comp = Field<T>::complex ? (colj >> 6) : 0;
+        const int gc = c0 + col;
+        if (col < cols_here && gr >= gc) {
+          const long long e = gr + (long long)gc * nrow;
+          float* p = Field<T>::complex ? pf + 2 * e + comp : pf + e;
+          *p -= acc[jj];
         }
       }
     }
