@@ -105,6 +105,9 @@ typedef struct {
   int64_t amd_ncmpa, amd_ndense;
   double amd_ndiv, amd_nms_ldl, amd_nms_lu;
   int64_t n_factor_launches, n_solve_launches;
+  /* tensor-core cmod plan: 128 x 64 tiles, (updater, tile) pairs, and K
+   * chunks staged (16 complex / 32 real updater columns per chunk) */
+  int64_t tc_tiles, tc_pairs, tc_chunks_complex, tc_chunks_real;
 } rslab_symbolic_info_t;
 
 typedef struct {

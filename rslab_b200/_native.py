@@ -53,6 +53,8 @@ class SymbolicInfo(C.Structure):
         ("amd_ncmpa", C.c_int64), ("amd_ndense", C.c_int64),
         ("amd_ndiv", C.c_double), ("amd_nms_ldl", C.c_double), ("amd_nms_lu", C.c_double),
         ("n_factor_launches", C.c_int64), ("n_solve_launches", C.c_int64),
+        ("tc_tiles", C.c_int64), ("tc_pairs", C.c_int64), ("tc_chunks_complex", C.c_int64),
+        ("tc_chunks_real", C.c_int64),
     ]
 
 

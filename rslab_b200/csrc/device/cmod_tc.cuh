@@ -15,11 +15,12 @@
 //   A' = [Ar | Ai],  B' = [[Gr, -Gi], [Gi, Gr]]  ->  A' B'^T = [Re | Im],
 // i.e. M = 128, N = 128, and 16 complex columns of k per 32-wide K stage.
 //
-// Pipeline (512 threads, one CTA per SM): the global loads of K chunk c+1
-// are issued into registers right after chunk c's MMAs, so their latency
-// overlaps the tensor work; two shared-memory stages gated by mbarriers that
-// tcgen05.commit arrives on; the scatter maps of the next pair are built one
-// pair ahead (double-buffered), leaving one block barrier per chunk.
+// Pipeline (512 threads, one CTA per SM): the global loads of K chunk c+2
+// are issued into a second register set right after chunk c's MMAs, so two
+// chunks of loads are in flight behind the tensor work; two shared-memory
+// stages gated by mbarriers that tcgen05.commit arrives on; one block
+// barrier per chunk.  The inverse scatter maps of every pair (tile row ->
+// k row, tile column -> k row, int8) are precomputed at analysis.
 // Accuracy: the tensor pipe does not round its accumulation to nearest, so
 // the sum runs in windows of TC_WIN chunks over two TMEM accumulators; each
 // finished window is added into per-thread fp32 registers (round to nearest)
@@ -53,9 +54,9 @@ template <> struct TcShape<c32> {
   static constexpr int n = 128;
 };
 
-__host__ __device__ constexpr size_t smem_cmod_tc_bytes() {
-  return 1024 + 2 * (size_t)TC_STAGE + (TC_M + 2 * TC_M + 2 * TC_N) * 4 + 64;
-}
+constexpr int TC_MAP = TC_M + TC_N;      // bytes of the inverse maps of one pair
+
+__host__ __device__ constexpr size_t smem_cmod_tc_bytes() { return 1024 + 2 * (size_t)TC_STAGE + 64; }
 
 // Per-thread staging values of one K chunk: A' 8 floats, B' 4 floats.
 struct TcRegs {
@@ -94,14 +95,14 @@ __device__ __forceinline__ void store_split2(unsigned char* hi_tile, unsigned ch
 //        B' column tid & 63, columns 4 (tid >> 6) .. +4.
 template <typename T>
 __device__ __forceinline__ void tc_load(TcRegs& R, const T* __restrict__ LA, const T* __restrict__ LB, int nrk,
-                                        int nck, int t0, const int* invrow, const int* invcol,
+                                        int nck, int t0, const int8_t* __restrict__ map,
                                         const T* __restrict__ dk, const T* __restrict__ dsk,
                                         const unsigned char* __restrict__ kindk) {
   using F = Field<T>;
   const int tid = threadIdx.x;
   const int row = tid & (TC_M - 1), ga = tid >> 7;
   const int u = tid & (TC_N - 1), gb = tid >> 6;
-  const int i = invrow[row], j = invcol[u];
+  const int i = map[row], j = map[TC_M + u];
   if constexpr (Field<T>::complex) {
 #pragma unroll
     for (int jj = 0; jj < 4; ++jj) {
@@ -171,28 +172,24 @@ __device__ __forceinline__ void tmem_ld_cols<16>(uint32_t taddr, float (&v)[16])
 
 template <typename T>
 __global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4* __restrict__ tasks,
-                                                      const int4* __restrict__ pairs) {
+                                                      const int4* __restrict__ pairs,
+                                                      const int8_t* __restrict__ maps) {
   using Sh = TcShape<T>;
   constexpr int NC = Sh::n / 4;  // accumulator columns per thread
   if (fa.status[0] != 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];  // re-aligned to 1024 below
   const uint32_t sraw = smem_u32(smem_raw);
   unsigned char* sm = smem_raw + (((sraw + 1023u) & ~1023u) - sraw);
-  int* rs_tile = reinterpret_cast<int*>(sm + 2 * TC_STAGE);         // TC_M
-  int* invrow = rs_tile + TC_M;                                     // 2 x TC_M
-  int* invcol = invrow + 2 * TC_M;                                  // 2 x TC_N
-  uint64_t* sbar = reinterpret_cast<uint64_t*>(invcol + 2 * TC_N);  // 2 stage barriers
+  uint64_t* sbar = reinterpret_cast<uint64_t*>(sm + 2 * TC_STAGE);  // 2 stage barriers
   uint64_t* wbar = sbar + 2;                                        // 2 window barriers
   uint32_t* tslot = reinterpret_cast<uint32_t*>(wbar + 2);
 
   const int4 tk = tasks[blockIdx.x];
   const int s = tk.x, r0 = (tk.y >> 16) * TC_M, c0 = (tk.y & 0xffff) * TC_N;
   const int pb = tk.z, pe = tk.w;
-  const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
+  const int ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
   const int rows_here = min(TC_M, nrow - r0), cols_here = min(TC_N, ncol - c0);
-  const int* rss = fa.rs + fa.sn_rsoff[s];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  if (tid < TC_M) rs_tile[tid] = tid < rows_here ? rss[r0 + tid] : INT_MAX;
   if (tid == 0) {
     mbar_init(&sbar[0], 1);
     mbar_init(&sbar[1], 1);
@@ -210,30 +207,20 @@ __global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4*
   const T* dall = reinterpret_cast<const T*>(fa.d);
   const T* dsall = reinterpret_cast<const T*>(fa.dsub);
   const T* pall = reinterpret_cast<const T*>(fa.panel);
-
-  // Scatter maps of pair u live in buffer (u - pb) & 1: invrow[t] = index of
-  // the k row landing on tile row t (or -1), invcol[v] likewise for columns.
-  // Built in two phases a block barrier apart: clear, then fill.
-  auto clear_maps = [&](int b) {
-    if (tid < TC_M) invrow[b * TC_M + tid] = -1;
-    else if (tid < TC_M + TC_N) invcol[b * TC_N + tid - TC_M] = -1;
-  };
-  auto fill_maps = [&](int u) {
-    const int b = (u - pb) & 1;
-    const int4 pr = pairs[u];
-    const int k = pr.x, a = pr.y, q0 = pr.z, nr = pr.w >> 16, nc = pr.w & 0xffff;
-    const int* okr = fa.rs + fa.sn_rsoff[k] + fa.sn_ncol[k];
-    if (tid < nr) invrow[b * TC_M + lower_bound_i(rs_tile, 0, rows_here, okr[a + tid])] = tid;
-    else if (tid >= TC_M && tid - TC_M < nc) invcol[b * TC_N + okr[q0 + tid - TC_M] - first - c0] = tid - TC_M;
-  };
   auto load_chunk = [&](TcRegs& R, int u, int t0) {
     const int4 pr = pairs[u];
     const int k = pr.x, a = pr.y, q0 = pr.z;
     const int nck = fa.sn_ncol[k], nrk = fa.sn_nrow[k], fk = fa.sn_first[k];
     const T* Lk = pall + fa.sn_poff[k] + nck;
-    const int b = (u - pb) & 1;
-    tc_load<T>(R, Lk + a, Lk + q0, nrk, nck, t0, invrow + b * TC_M, invcol + b * TC_N, dall + fk, dsall + fk,
-               fa.kind + fk);
+    tc_load<T>(R, Lk + a, Lk + q0, nrk, nck, t0, maps + (long long)u * TC_MAP, dall + fk, dsall + fk, fa.kind + fk);
+  };
+  // (u, t0) -> the next chunk in (pair, updater column) order
+  auto advance = [&](int& u, int& t0) {
+    t0 += Sh::kc;
+    if (t0 >= fa.sn_ncol[pairs[u].x]) {
+      ++u;
+      t0 = 0;
+    }
   };
 
   float acc[NC];
@@ -256,17 +243,15 @@ __global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4*
     tc_fence_before();
   };
 
-  int c = 0;  // K chunks issued
+  int c = 0;   // K chunks issued
+  int pw = 0;  // next window to promote
   if (pb < pe) {
-    clear_maps(0);
-    if (pb + 1 < pe) clear_maps(1);
-    __syncthreads();
-    fill_maps(pb);
-    if (pb + 1 < pe) fill_maps(pb + 1);
-    __syncthreads();
-    TcRegs R;
-    load_chunk(R, pb, 0);
-    int u = pb, t0 = 0;
+    TcRegs R0, R1;  // register sets of the even / odd chunks
+    int ul = pb, tl = 0;  // load cursor: two chunks ahead of the issue cursor
+    load_chunk(R0, ul, tl);
+    advance(ul, tl);
+    if (ul < pe) load_chunk(R1, ul, tl);
+    int u = pb, t0 = 0;  // issue cursor
     while (u < pe) {
       const int st = c & 1;
       if (c >= 2) {
@@ -277,22 +262,12 @@ __global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4*
         }
       }
       unsigned char* stg = sm + st * TC_STAGE;
-      tc_store<T>(R, stg);
-      // next chunk in (pair, column) order
-      int u2 = u, t2 = t0 + Sh::kc;
-      if (t2 >= fa.sn_ncol[pairs[u].x]) {
-        u2 = u + 1;
-        t2 = 0;
-      }
-      const bool last = u2 >= pe;
-      // On the first chunk of pair u > pb, the map buffer of pair u + 1 is
-      // free: its previous user, pair u - 1, read it last one iteration back
-      // (before that iteration's barrier).  Clear it before this barrier and
-      // fill it after; its first reader is the load of pair u + 1's first
-      // chunk, behind the next barrier (or the extra one below when pair u
-      // has a single chunk).
-      const bool mk = t0 == 0 && u > pb && u + 1 < pe;
-      if (mk) clear_maps((u + 1 - pb) & 1);
+      if (st == 0)
+        tc_store<T>(R0, stg);
+      else
+        tc_store<T>(R1, stg);
+      advance(u, t0);
+      const bool last = u >= pe;
       fence_proxy_async_smem();
       __syncthreads();
       const int w = c / TC_WIN;
@@ -314,19 +289,28 @@ __global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4*
         mma_commit(&sbar[st]);
         if (c % TC_WIN == TC_WIN - 1 || last) mma_commit(&wbar[w & 1]);
       }
-      if (mk) {
-        fill_maps(u + 1);
-        if (t2 == 0) __syncthreads();  // single-chunk pair: the load below reads those maps
+      // chunk c + 2 into the register set just stored
+      if (ul < pe) {
+        advance(ul, tl);
+        if (ul < pe) {
+          if (st == 0)
+            load_chunk(R0, ul, tl);
+          else
+            load_chunk(R1, ul, tl);
+        }
       }
-      if (!last) load_chunk(R, u2, t2);
-      if (c % TC_WIN == 0 && c >= TC_WIN) promote(w - 1);
+      // window w - 1 is two chunks behind: its MMAs are (nearly) done, and its
+      // accumulator is next overwritten by window w + 1, TC_WIN - 2 chunks on
+      if (c % TC_WIN == 2 && w >= 1) promote(pw++);
       ++c;
-      u = u2;
-      t0 = t2;
       if (!ok) break;
     }
   }
-  if (c > 0 && ok) promote((c - 1) / TC_WIN);
+  if (ok)
+    while (pw <= (c - 1) / TC_WIN && c > 0) {
+      promote(pw++);
+      if (!ok) break;
+    }
   if (!ok) {
     // drain what was issued (bounded), then report
     if (c > 0) (void)mbar_wait_bounded(&sbar[(c - 1) & 1], (uint32_t)(((c - 1) >> 1) & 1));

@@ -130,6 +130,7 @@ struct rslab_sym_handle {
   std::vector<int4> t4;
   std::vector<int4> cpairs;   // cmod (k, a, q0, nr << 16 | nc) per tile, in update order
   std::vector<int4> t4tc, cpairs_tc;  // the same for the 128 x 64 tensor-core tiles
+  std::vector<int8_t> tcmaps;         // per tensor-core pair: 128 + 64 inverse scatter maps
   std::vector<int> t1;
   std::vector<int2> t2;
   std::vector<int4> st4;  // blocked diagonal-solve tasks (s, j0, r0 | c0, 0)
@@ -157,6 +158,7 @@ struct rslab_sym_handle {
   int4* d_t4 = nullptr;
   int4* d_cpairs = nullptr;
   int4 *d_t4tc = nullptr, *d_cpairs_tc = nullptr;
+  int8_t* d_tcmaps = nullptr;
   int* d_t1 = nullptr;
   int2* d_t2 = nullptr;
   int4* d_st4 = nullptr;
@@ -211,6 +213,7 @@ struct rslab_sym_handle {
     d_cpairs = up(cpairs, st);
     d_t4tc = up(t4tc, st);
     d_cpairs_tc = up(cpairs_tc, st);
+    d_tcmaps = up(tcmaps, st);
     d_t1 = up(t1, st);
     d_t2 = up(t2, st);
     d_st4 = up(st4, st);
@@ -227,8 +230,11 @@ namespace {
 // Append the cmod tiles (tr x tc) of every supernode of a level that has
 // updaters: task (s, rt << 16 | ct, pair_begin, pair_end) and its pairs
 // (k, a, q0, nr << 16 | nc) in update-list order.
+// With `maps`, every pair also gets its inverse scatter maps (tr + tcw
+// bytes: for each tile row / column the index of k's row landing there
+// inside the pair's run, or -1).
 void add_cmod_tiles(rslab_sym_handle& H, const std::vector<int64_t>& lvl, int tr, int tcw, std::vector<int4>& tasks,
-                    std::vector<int4>& pairs, bool count_flops) {
+                    std::vector<int4>& pairs, bool count_flops, std::vector<int8_t>* maps = nullptr) {
   const auto& S = H.S;
   for (int64_t s : lvl) {
     if (S.upd_ptr[s + 1] == S.upd_ptr[s]) continue;
@@ -237,6 +243,7 @@ void add_cmod_tiles(rslab_sym_handle& H, const std::vector<int64_t>& lvl, int tr
     const int64_t* rss = S.rs.data() + S.rs_ptr[s];
     const int ntc = (nc + tcw - 1) / tcw, ntr = (nr + tr - 1) / tr;
     std::vector<std::vector<int4>> tp((size_t)ntc * ntr);
+    std::vector<std::vector<int8_t>> tm(maps ? (size_t)ntc * ntr : 0);
     for (int64_t u = S.upd_ptr[s]; u < S.upd_ptr[s + 1]; ++u) {
       const int64_t k = S.upd[u], p0 = S.upd_p0[u], p1 = S.upd_p1[u];
       const int64_t nck = S.sn[k].ncol;
@@ -262,6 +269,13 @@ void add_cmod_tiles(rslab_sym_handle& H, const std::vector<int64_t>& lvl, int tr
           while (rb < nok && rel[rb - p0] / tr == rt) ++rb;
           tp[(size_t)ct * ntr + rt].push_back(
               make_int4((int)k, (int)ra, (int)qa, (int)(((rb - ra) << 16) | (qb - qa))));
+          if (maps) {
+            auto& m = tm[(size_t)ct * ntr + rt];
+            const size_t base = m.size();
+            m.resize(base + tr + tcw, (int8_t)-1);
+            for (int64_t r = ra; r < rb; ++r) m[base + rel[r - p0] - rt * tr] = (int8_t)(r - ra);
+            for (int64_t qq = qa; qq < qb; ++qq) m[base + tr + (ok[qq] - first - ct * tcw)] = (int8_t)(qq - qa);
+          }
           ra = rb;
         }
         qa = qb;
@@ -284,6 +298,10 @@ void add_cmod_tiles(rslab_sym_handle& H, const std::vector<int64_t>& lvl, int tr
           }
         const int pb = (int)pairs.size();
         pairs.insert(pairs.end(), v.begin(), v.end());
+        if (maps) {
+          const auto& m = tm[(size_t)ct * ntr + rt];
+          maps->insert(maps->end(), m.begin(), m.end());
+        }
         tasks.push_back(make_int4((int)s, (rt << 16) | ct, pb, (int)pairs.size()));
       }
   }
@@ -397,7 +415,7 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       L.ntasks = (int)(H.t4.size() - L.task_off);
       if (L.ntasks) H.fplan.push_back(L);
       Launch Lt{L_CMOD_TC, (long long)H.t4tc.size(), 0, 0};
-      add_cmod_tiles(H, lvl, TC_M, TC_N, H.t4tc, H.cpairs_tc, false);
+      add_cmod_tiles(H, lvl, TC_M, TC_N, H.t4tc, H.cpairs_tc, false, &H.tcmaps);
       Lt.ntasks = (int)(H.t4tc.size() - Lt.task_off);
       if (Lt.ntasks) H.fplan.push_back(Lt);
     }
@@ -713,7 +731,8 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
       case L_CMOD_TC:
         if constexpr (TensorCmod<T>::ok) {
           if (!use_tc) continue;
-          k_cmod_tc<T><<<L.ntasks, TC_NT, smem_cmod_tc_bytes(), st>>>(fa, H.d_t4tc + L.task_off, H.d_cpairs_tc);
+          k_cmod_tc<T><<<L.ntasks, TC_NT, smem_cmod_tc_bytes(), st>>>(fa, H.d_t4tc + L.task_off, H.d_cpairs_tc,
+                                                                      H.d_tcmaps);
         } else {
           continue;
         }
@@ -1119,6 +1138,14 @@ int rslab_symbolic_info(const rslab_sym_handle* h, rslab_symbolic_info_t* info) 
   info->amd_nms_lu = h->S.amd.nms_lu;
   info->n_factor_launches = (int64_t)h->fplan.size();
   info->n_solve_launches = (int64_t)(h->fwdplan.size() + h->bwdplan.size());
+  info->tc_tiles = (int64_t)h->t4tc.size();
+  info->tc_pairs = (int64_t)h->cpairs_tc.size();
+  info->tc_chunks_complex = info->tc_chunks_real = 0;
+  for (const int4& pq : h->cpairs_tc) {
+    const int64_t nck = h->S.sn[pq.x].ncol;
+    info->tc_chunks_complex += (nck + 15) / 16;
+    info->tc_chunks_real += (nck + 31) / 32;
+  }
   return 0;
 }
 
