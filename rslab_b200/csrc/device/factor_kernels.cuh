@@ -49,6 +49,8 @@ struct FactorArgs {
   long long scratch_stride;  // bytes per slot
   int* status;          // [0] = error code, [1] = first failing supernode, [2] = n_perturbed
   double perturb_floor; // < 0: exact mode
+  void* gpool;          // G_k = L21_k D_k, (nrow_k - ncol_k) x ncol_k at goff[k] (tensor-core cmod)
+  const long long* goff;
 };
 
 // ---------------------------------------------------------------------------

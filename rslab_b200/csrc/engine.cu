@@ -98,7 +98,7 @@ size_t elem_size(int dtype) {
 enum LaunchKind {
   L_CMOD, L_GETF2, L_DEEP, L_SCHUR,
   L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD,
-  L_FTRSV_BLK, L_FTRSV_UPD, L_BTRSV_BLK, L_BTRSV_UPD, L_FWD_GATHER, L_CMOD_TC
+  L_FTRSV_BLK, L_FTRSV_UPD, L_BTRSV_BLK, L_BTRSV_UPD, L_FWD_GATHER, L_CMOD_TC, L_MAKE_G
 };
 struct Launch {
   int kind;
@@ -131,6 +131,8 @@ struct rslab_sym_handle {
   std::vector<int4> cpairs;   // cmod (k, a, q0, nr << 16 | nc) per tile, in update order
   std::vector<int4> t4tc, cpairs_tc;  // the same for the 128 x 64 tensor-core tiles
   std::vector<int8_t> tcmaps;         // per tensor-core pair: 128 + 64 inverse scatter maps
+  std::vector<long long> goff;        // G_k = L21_k D_k pool offsets ((nrow - ncol) x ncol each)
+  long long g_elems = 0;
   std::vector<int> t1;
   std::vector<int2> t2;
   std::vector<int4> st4;  // blocked diagonal-solve tasks (s, j0, r0 | c0, 0)
@@ -159,6 +161,7 @@ struct rslab_sym_handle {
   int4* d_cpairs = nullptr;
   int4 *d_t4tc = nullptr, *d_cpairs_tc = nullptr;
   int8_t* d_tcmaps = nullptr;
+  long long* d_goff = nullptr;
   int* d_t1 = nullptr;
   int2* d_t2 = nullptr;
   int4* d_st4 = nullptr;
@@ -214,6 +217,7 @@ struct rslab_sym_handle {
     d_t4tc = up(t4tc, st);
     d_cpairs_tc = up(cpairs_tc, st);
     d_tcmaps = up(tcmaps, st);
+    d_goff = up(goff, st);
     d_t1 = up(t1, st);
     d_t2 = up(t2, st);
     d_st4 = up(st4, st);
@@ -333,6 +337,12 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
     H.urows += H.nrow[s] - S.sn[s].ncol;
   }
   if (H.urows >= (1LL << 31)) throw RslabError(Status::InvalidInput, "forward push buffer exceeds 2^31 rows");
+  H.goff.assign(ns, 0);
+  H.g_elems = 0;
+  for (int s = 0; s < ns; ++s) {
+    H.goff[s] = H.g_elems;
+    H.g_elems += (long long)(H.nrow[s] - S.sn[s].ncol) * S.sn[s].ncol;
+  }
   // Pull lists: every off-diagonal row r of updater k (U row uoff[k] + r)
   // lands on one column g of an ancestor; list the pushes per g in the
   // ancestor's update-list order so the gather subtracts them in that order.
@@ -459,6 +469,16 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         H.t4.insert(H.t4.end(), schur.begin(), schur.end());
         H.fplan.push_back(C);
       }
+    }
+    // G_k = L21_k D_k of this level's updaters, for the tensor-core cmod of
+    // their ancestors (32-column tasks).
+    {
+      Launch Mg{L_MAKE_G, (long long)H.t2.size(), 0, 0};
+      for (int64_t s : lvl)
+        if (H.nrow[s] > S.sn[s].ncol)
+          for (int t0 = 0; t0 < S.sn[s].ncol; t0 += 32) H.t2.push_back(make_int2((int)s, t0));
+      Mg.ntasks = (int)(H.t2.size() - Mg.task_off);
+      if (Mg.ntasks) H.fplan.push_back(Mg);
     }
     // Solve launches for this level.  Forward: diagonal blocks (one CTA per
     // narrow supernode; wide ones get the blocked multi-CTA solve), then the
@@ -604,6 +624,7 @@ struct rslab_fac_handle {
   unsigned long long* cnt3 = nullptr;
   void* scratch = nullptr;
   long long scratch_stride = 0;
+  void* gpool = nullptr;  // G_k = L21_k D_k (tensor-core cmod only)
   // graph of the numeric factor (values read from `aval`)
   cudaGraphExec_t fgraph = nullptr;
   // solve workspace
@@ -663,6 +684,8 @@ FactorArgs make_fargs(rslab_fac_handle& F) {
   a.scratch_stride = F.scratch_stride;
   a.status = F.status;
   a.perturb_floor = F.set.on_zero_pivot == RSLAB_PIVOT_PERTURB ? F.set.abs_floor : -1.0;
+  a.gpool = F.gpool;
+  a.goff = H.d_goff;
   return a;
 }
 
@@ -737,6 +760,10 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
           continue;
         }
         break;
+      case L_MAKE_G:
+        if (!use_tc) continue;
+        k_make_g<T><<<L.ntasks, 256, 0, st>>>(fa, H.d_t2 + L.task_off);
+        break;
       case L_GETF2: {
         FactorArgs f2 = fa;
         f2.scratch_stride = ((long long)L.nb_slot * L.nb_slot * es + 3 * L.nb_slot * 4 + 255) / 256 * 256;
@@ -754,7 +781,11 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         break;
     }
     if (prof)
-      prof->mark(st, (L.kind == L_CMOD || L.kind == L_CMOD_TC) ? 1 : L.kind == L_GETF2 ? 2 : L.kind == L_DEEP ? 3 : 4,
+      prof->mark(st,
+                 (L.kind == L_CMOD || L.kind == L_CMOD_TC || L.kind == L_MAKE_G) ? 1
+                 : L.kind == L_GETF2                                           ? 2
+                 : L.kind == L_DEEP                                            ? 3
+                                                                               : 4,
                  L.ntasks, L.kind);
   }
   CK(cudaMemsetAsync(F.cnt3, 0, 3 * sizeof(unsigned long long), st));
@@ -1213,6 +1244,8 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
     const long long nbm = sym->max_nb;
     F->scratch_stride = (nbm * nbm * (long long)es + 3 * nbm * 4 + 255) / 256 * 256;
     F->scratch = F->al<unsigned char>((size_t)std::max(1, sym->max_getf2_tasks) * F->scratch_stride);
+    if ((dtype == RSLAB_F32 || dtype == RSLAB_C32) && F->set.schur_engine == RSLAB_SCHUR_TENSOR)
+      F->gpool = F->al<unsigned char>((size_t)std::max(sym->g_elems, 1LL) * es);
     if (F->set.scaling != RSLAB_SCALING_ONEPASS) {
       std::vector<double> ones(n, 1.0);
       CK(cudaMemcpyAsync(F->scale, ones.data(), n * 8, cudaMemcpyHostToDevice, F->st));
