@@ -488,52 +488,112 @@ __device__ __forceinline__ void put(T (&x)[NS], int slot, T v) {
     if (j == slot) x[j] = v;
 }
 
-template <typename T, int NS>
-__device__ void replay_row_warp(T (&x)[NS], int pw, int nb, const T* __restrict__ snap, const int* __restrict__ swaps,
-                                int kb, const T* __restrict__ d, const T* __restrict__ dsub,
-                                const unsigned char* __restrict__ kind) {
+// Per-block replay program in shared memory, filled once per CTA: for pivot
+// step k the swap target, the pivot kind and the inverse of the pivot block
+// (1x1: 1/d; 2x2: 1/det with det = d11 d22 - d21^2), plus d and dsub.
+template <typename T>
+struct ReplayProg {
+  int* sw;
+  unsigned char* kd;
+  T* inv;
+  T* dd;
+  T* ds;
+};
+
+template <typename T>
+__host__ __device__ constexpr size_t replay_prog_bytes(int nb) {
+  return (size_t)nb * (3 * sizeof(T) + sizeof(int) + 1) + 16;
+}
+
+// Carve the program out of `mem` (16-byte aligned) and fill it (all threads).
+template <typename T, int NT>
+__device__ ReplayProg<T> load_replay_prog(unsigned char* mem, int pw, int nb, const int* __restrict__ swaps,
+                                          const T* __restrict__ d, const T* __restrict__ dsub,
+                                          const unsigned char* __restrict__ kind) {
+  using F = Field<T>;
+  ReplayProg<T> P;
+  P.inv = reinterpret_cast<T*>(mem);
+  P.dd = P.inv + nb;
+  P.ds = P.dd + nb;
+  P.sw = reinterpret_cast<int*>(P.ds + nb);
+  P.kd = reinterpret_cast<unsigned char*>(P.sw + nb);
+  for (int k = threadIdx.x; k < pw; k += NT) {
+    const unsigned char kk = kind[k];
+    P.sw[k] = swaps[k];
+    P.kd[k] = kk;
+    P.dd[k] = d[k];
+    P.ds[k] = dsub[k];
+    T inv = F::zero();
+    if (kk == 0) {
+      inv = F::recip(d[k]);
+    } else if (kk == 1) {
+      const T d11 = d[k], d21 = dsub[k], d22 = d[k + 1];
+      inv = F::recip(F::sub(F::mul(d11, d22), F::mul(d21, d21)));
+    }
+    P.inv[k] = inv;
+  }
+  return P;
+}
+
+// Replay a block's pivot steps on NR rows held by one warp (x[row][slot],
+// column = lane + 32 slot): the swaps, then per pivot the elimination of the
+// later columns with the snapshot multipliers and the scaling by the inverse
+// pivot block.  The rows are independent, so the NR dependency chains
+// interleave; each row sees the same operation sequence as a lone row.
+template <typename T, int NS, int NR>
+__device__ void replay_rows_warp(T (&x)[NR][NS], int pw, int nb, const T* __restrict__ snap, int kb,
+                                 const ReplayProg<T>& P) {
   using F = Field<T>;
   const int lane = threadIdx.x & 31;
   int k = 0;
   while (k < pw) {
-    const int kp = swaps[k];
-    const bool two = kind[k] == 1;
+    const int kp = P.sw[k];
+    const bool two = P.kd[k] == 1;
     if (kp >= 0) {
       const int src = two ? k + 1 : k, dst = kp - kb;
-      const T vs = shfl_t(pick(x, src >> 5), src & 31);
-      const T vd = shfl_t(pick(x, dst >> 5), dst & 31);
-      if (lane == (src & 31)) put(x, src >> 5, vd);
-      if (lane == (dst & 31)) put(x, dst >> 5, vs);
-    }
-    const T xk = shfl_t(pick(x, k >> 5), k & 31);
-    if (two) {
-      const T xk1 = shfl_t(pick(x, (k + 1) >> 5), (k + 1) & 31);
 #pragma unroll
-      for (int j = 0; j < NS; ++j) {
-        const int col = lane + 32 * j;
-        if (col >= k + 2 && col < pw) {
-          const T l1 = snap[k * nb + col], l2 = snap[(k + 1) * nb + col];
-          T v = F::sub(x[j], F::mul(xk, l1));
-          x[j] = F::sub(v, F::mul(xk1, l2));
-        }
+      for (int r = 0; r < NR; ++r) {
+        const T vs = shfl_t(pick(x[r], src >> 5), src & 31);
+        const T vd = shfl_t(pick(x[r], dst >> 5), dst & 31);
+        if (lane == (src & 31)) put(x[r], src >> 5, vd);
+        if (lane == (dst & 31)) put(x[r], dst >> 5, vs);
       }
-      const T d11 = d[k], d21 = dsub[k], d22 = d[k + 1];
-      const T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
-      const T detinv = F::recip(det);
-      if (lane == (k & 31)) put(x, k >> 5, F::mul(F::sub(F::mul(d22, xk), F::mul(d21, xk1)), detinv));
-      if (lane == ((k + 1) & 31)) put(x, (k + 1) >> 5, F::mul(F::sub(F::mul(d11, xk1), F::mul(d21, xk)), detinv));
+    }
+    if (two) {
+      const T d11 = P.dd[k], d21 = P.ds[k], d22 = P.dd[k + 1], detinv = P.inv[k];
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        const T xk = shfl_t(pick(x[r], k >> 5), k & 31);
+        const T xk1 = shfl_t(pick(x[r], (k + 1) >> 5), (k + 1) & 31);
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+          const int col = lane + 32 * j;
+          if (col >= k + 2 && col < pw) {
+            const T l1 = snap[k * nb + col], l2 = snap[(k + 1) * nb + col];
+            T v = F::sub(x[r][j], F::mul(xk, l1));
+            x[r][j] = F::sub(v, F::mul(xk1, l2));
+          }
+        }
+        if (lane == (k & 31)) put(x[r], k >> 5, F::mul(F::sub(F::mul(d22, xk), F::mul(d21, xk1)), detinv));
+        if (lane == ((k + 1) & 31))
+          put(x[r], (k + 1) >> 5, F::mul(F::sub(F::mul(d11, xk1), F::mul(d21, xk)), detinv));
+      }
       k += 2;
     } else {
+      const T dinv = P.inv[k];
 #pragma unroll
-      for (int j = 0; j < NS; ++j) {
-        const int col = lane + 32 * j;
-        if (col > k && col < pw) {
-          const T w = snap[k * nb + col];
-          if (!F::is_zero(w)) x[j] = F::sub(x[j], F::mul(xk, w));
+      for (int r = 0; r < NR; ++r) {
+        const T xk = shfl_t(pick(x[r], k >> 5), k & 31);
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+          const int col = lane + 32 * j;
+          if (col > k && col < pw) {
+            const T w = snap[k * nb + col];
+            if (!F::is_zero(w)) x[r][j] = F::sub(x[r][j], F::mul(xk, w));
+          }
         }
+        if (lane == (k & 31)) put(x[r], k >> 5, F::mul(xk, dinv));
       }
-      const T dinv = F::recip(d[k]);
-      if (lane == (k & 31)) put(x, k >> 5, F::mul(xk, dinv));
       k += 1;
     }
   }
@@ -541,14 +601,15 @@ __device__ void replay_row_warp(T (&x)[NS], int pw, int nb, const T* __restrict_
 
 // Replay a block's pivot steps on deep rows [r_begin, r_end) of a panel:
 // rows staged through shared memory (32 rows x pw, padded stride) so both
-// the global loads / stores and the per-row register fills are conflict-free.
+// the global loads / stores and the per-row register fills are conflict-free;
+// each warp replays its 32 / NW rows together.  `prog` holds the program.
 template <typename T, int NT>
 __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int nb, int r_begin, int r_end,
-                                 const T* __restrict__ snap, const int* __restrict__ swaps, const T* __restrict__ d,
-                                 const T* __restrict__ dsub, const unsigned char* __restrict__ kind, T* X) {
+                                 const T* __restrict__ snap, const ReplayProg<T>& P, T* X) {
   constexpr int R = 32, LDX = 33;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int NW = NT / 32;
+  constexpr int NR = R / NW;
   for (int rs0 = r_begin; rs0 < r_end; rs0 += R) {
     const int rows = min(R, r_end - rs0);
     for (int e = threadIdx.x; e < R * pw; e += NT) {
@@ -556,34 +617,41 @@ __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int n
       if (r < rows) X[c * LDX + r] = panel[(rs0 + r) + (long long)(kb + c) * nrow];
     }
     __syncthreads();
-    for (int r = warp; r < rows; r += NW) {
-      if (pw <= 64) {
-        T x[2];
+    // rows warp + NW i; rows past `rows` replay zeros and are not stored
+    if (pw <= 64) {
+      T x[NR][2];
+#pragma unroll
+      for (int i = 0; i < NR; ++i)
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-          const int col = lane + 32 * j;
-          x[j] = col < pw ? X[col * LDX + r] : Field<T>::zero();
+          const int col = lane + 32 * j, r = warp + NW * i;
+          x[i][j] = (col < pw && r < rows) ? X[col * LDX + r] : Field<T>::zero();
         }
-        replay_row_warp<T, 2>(x, pw, nb, snap, swaps, kb, d, dsub, kind);
+      replay_rows_warp<T, 2, NR>(x, pw, nb, snap, kb, P);
+#pragma unroll
+      for (int i = 0; i < NR; ++i)
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-          const int col = lane + 32 * j;
-          if (col < pw) X[col * LDX + r] = x[j];
+          const int col = lane + 32 * j, r = warp + NW * i;
+          if (col < pw && r < rows) X[col * LDX + r] = x[i][j];
         }
-      } else {
-        T x[4];
+    } else {
+      T x[NR][4];
+#pragma unroll
+      for (int i = 0; i < NR; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const int col = lane + 32 * j;
-          x[j] = col < pw ? X[col * LDX + r] : Field<T>::zero();
+          const int col = lane + 32 * j, r = warp + NW * i;
+          x[i][j] = (col < pw && r < rows) ? X[col * LDX + r] : Field<T>::zero();
         }
-        replay_row_warp<T, 4>(x, pw, nb, snap, swaps, kb, d, dsub, kind);
+      replay_rows_warp<T, 4, NR>(x, pw, nb, snap, kb, P);
+#pragma unroll
+      for (int i = 0; i < NR; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const int col = lane + 32 * j;
-          if (col < pw) X[col * LDX + r] = x[j];
+          const int col = lane + 32 * j, r = warp + NW * i;
+          if (col < pw && r < rows) X[col * LDX + r] = x[i][j];
         }
-      }
     }
     __syncthreads();
     for (int e = threadIdx.x; e < R * pw; e += NT) {
@@ -888,7 +956,10 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
   __syncthreads();
   if (fuse && nrow > ke) {
     // Replay this block's pivot steps on the deep rows [ke, nrow).
-    replay_deep_rows<T, NT>(panel, nrow, kb, pw, nb, ke, nrow, snap, swaps, dG, dsG, kindG, A);
+    unsigned char* pmem = smem_raw + (((size_t)(DEEP_R + 1) * nb * sizeof(T) + 15) & ~size_t(15));
+    const ReplayProg<T> P = load_replay_prog<T, NT>(pmem, pw, nb, swaps, dG, dsG, kindG);
+    __syncthreads();
+    replay_deep_rows<T, NT>(panel, nrow, kb, pw, nb, ke, nrow, snap, P, A);
   }
 }
 
@@ -910,9 +981,12 @@ __global__ void __launch_bounds__(NT) k_deep(FactorArgs fa, const int4* __restri
   const T* snap = reinterpret_cast<const T*>(sc);
   const int* swaps = reinterpret_cast<const int*>(snap + (long long)nb * nb);
   T* X = reinterpret_cast<T*>(smem_raw);
-  replay_deep_rows<T, NT>(panel, nrow, kb, pw, nb, rs0, min(rs0 + DEEP_R, nrow), snap, swaps,
-                          reinterpret_cast<const T*>(fa.d) + first + kb,
-                          reinterpret_cast<const T*>(fa.dsub) + first + kb, fa.kind + first + kb, X);
+  unsigned char* pmem = smem_raw + (((size_t)(DEEP_R + 1) * nb * sizeof(T) + 15) & ~size_t(15));
+  const ReplayProg<T> P =
+      load_replay_prog<T, NT>(pmem, pw, nb, swaps, reinterpret_cast<const T*>(fa.d) + first + kb,
+                              reinterpret_cast<const T*>(fa.dsub) + first + kb, fa.kind + first + kb);
+  __syncthreads();
+  replay_deep_rows<T, NT>(panel, nrow, kb, pw, nb, rs0, min(rs0 + DEEP_R, nrow), snap, P, X);
 }
 
 }  // namespace rsd

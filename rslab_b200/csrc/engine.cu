@@ -556,12 +556,15 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
 size_t kchunk(size_t es) { return es == 16 ? 16 : 32; }
 size_t smem_cmod(size_t es) { return (size_t)TILE * TILE * es + 2 * kchunk(es) * TILE * es + 3 * TILE * 4 + 64; }
 size_t smem_schur(size_t es) { return 2 * kchunk(es) * TILE * es; }
+// Deep-row staging (DEEP_R + 1) x nb plus the replay program, 16-byte aligned.
+size_t smem_replay(size_t es, int nb) {
+  return (((size_t)(DEEP_R + 1) * nb * es + 15) & ~size_t(15)) + (size_t)nb * (3 * es + 4 + 1) + 16;
+}
 size_t smem_getf2(size_t es, int nb) {
   size_t a = (size_t)nb * (nb + 1) / 2 * es + 2 * nb * es + 16 + 32 * 8 + 32 * 4 + 16 * 4;
-  size_t b = (size_t)(DEEP_R + 1) * nb * es;
-  return std::max(a, b) + 64;
+  return std::max(a, smem_replay(es, nb)) + 64;
 }
-size_t smem_deep(size_t es, int nb) { return (size_t)(DEEP_R + 1) * nb * es + 64; }
+size_t smem_deep(size_t es, int nb) { return smem_replay(es, nb) + 64; }
 size_t smem_solve(size_t es) { return ((size_t)(SOLVE_NT / 32) * 32 * RHS_MAX + SB * (SB + 1) + SB * RHS_MAX) * es; }
 size_t smem_push(size_t es) { return (size_t)(32 * 64 + 32 * RHS_MAX) * es; }
 size_t smem_dots(size_t es) { return (size_t)(32 * 33 + 32 * RHS_MAX) * es; }
