@@ -692,12 +692,15 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
 
   T* A = reinterpret_cast<T*>(smem_raw);              // packed lower pw x pw
   const int npk = pw * (pw + 1) / 2;
-  T* l1 = A + npk;
+  T* l1 = A + npk;   // multipliers of the current step (column k / k+1)
   T* l2 = l1 + pw;
+  T* u1 = l2 + pw;   // the same columns before scaling (read by the update)
+  T* u2 = u1 + pw;
   // 16-byte aligned reduction scratch after the (possibly 4-byte) field arrays.
-  double* red_v = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(l2 + pw) + 15) & ~uintptr_t(15));
+  double* red_v = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(u2 + pw) + 15) & ~uintptr_t(15));
   int* red_i = reinterpret_cast<int*>(red_v + 32);
   int* ctl = red_i + 32;  // [0] kstep [1] kp [2] nswaps [3] error
+  int* lp_s = ctl + 16;   // the block's slice of lperm
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -717,6 +720,8 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
     ctl[2] = 0;
     ctl[3] = 0;
   }
+  __syncthreads();
+  for (int i = tid; i < pw; i += NT) lp_s[i] = lpermG[kb + i];
   __syncthreads();
   const double alpha = (1.0 + sqrt(17.0)) / 8.0;
   int nperturbed = 0;
@@ -789,9 +794,9 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
             T t = A[pk(p, p, pw)];
             A[pk(p, p, pw)] = A[pk(q, q, pw)];
             A[pk(q, q, pw)] = t;
-            int lpv = lpermG[kb + p];
-            lpermG[kb + p] = lpermG[kb + q];
-            lpermG[kb + q] = lpv;
+            const int lpv = lp_s[p];
+            lp_s[p] = lp_s[q];
+            lp_s[q] = lpv;
             swaps[k] = kb + q;
             const int ns = ctl[2];
             swp_p[ns] = kb + p;
@@ -818,7 +823,9 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
           if (!err) {
             const T dinv = F::recip(dk);
             for (int jj = k + 1 + lane; jj < pw; jj += 32) {
-              const T w = F::mul(A[pk(jj, k, pw)], dinv);
+              const T a = A[pk(jj, k, pw)];
+              const T w = F::mul(a, dinv);
+              u1[jj] = a;
               l1[jj] = w;
               snap[k * nb + jj] = w;
             }
@@ -858,6 +865,8 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
               const T wik = A[pk(i, k, pw)], wik1 = A[pk(i, k + 1, pw)];
               const T a1 = F::mul(F::sub(F::mul(d22, wik), F::mul(d21, wik1)), detinv);
               const T a2 = F::mul(F::sub(F::mul(d11, wik1), F::mul(d21, wik)), detinv);
+              u1[i] = wik;
+              u2[i] = wik1;
               l1[i] = a1;
               l2[i] = a2;
               snap[k * nb + i] = a1;
@@ -873,33 +882,28 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
     }
     __syncthreads();
     if (ctl[3]) break;
-    // Trailing update of step k by all warps; the previous 1x1 step's
-    // column scaling rides along (different columns, no conflict).
+    // Trailing update of step k by all warps, reading the unscaled pivot
+    // column(s) from u1/u2, while column(s) k are finished in place (1x1:
+    // scaled by 1/d; 2x2: the multipliers) — disjoint columns, one barrier.
     const int kstep = ctlk[1];
     if (kstep == 1) {
       for (int jj = k + 1 + warp; jj < pw; jj += NW) {
         const T w = l1[jj];
         if (F::is_zero(w)) continue;
-        for (int i = jj + lane; i < pw; i += 32) A[pk(i, jj, pw)] = F::sub(A[pk(i, jj, pw)], F::mul(A[pk(i, k, pw)], w));
+        for (int i = jj + lane; i < pw; i += 32) A[pk(i, jj, pw)] = F::sub(A[pk(i, jj, pw)], F::mul(u1[i], w));
       }
+      const T dinv = *dinv_s;
+      for (int i = k + 1 + tid; i < pw; i += NT) A[pk(i, k, pw)] = F::mul(u1[i], dinv);
     } else {
       for (int jj = k + 2 + warp; jj < pw; jj += NW) {
         const T a1 = l1[jj], a2 = l2[jj];
         for (int i = jj + lane; i < pw; i += 32) {
           T x = A[pk(i, jj, pw)];
-          x = F::sub(x, F::mul(A[pk(i, k, pw)], a1));
-          x = F::sub(x, F::mul(A[pk(i, k + 1, pw)], a2));
+          x = F::sub(x, F::mul(u1[i], a1));
+          x = F::sub(x, F::mul(u2[i], a2));
           A[pk(i, jj, pw)] = x;
         }
       }
-    }
-    __syncthreads();
-    // Finish column(s) k: 1x1 -> scale by 1/d (deferred from the update);
-    // 2x2 -> store the multipliers.
-    if (kstep == 1) {
-      const T dinv = *dinv_s;
-      for (int i = k + 1 + tid; i < pw; i += NT) A[pk(i, k, pw)] = F::mul(A[pk(i, k, pw)], dinv);
-    } else {
       for (int i = k + 2 + tid; i < pw; i += NT) {
         A[pk(i, k, pw)] = l1[i];
         A[pk(i, k + 1, pw)] = l2[i];
@@ -908,6 +912,7 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
     if (tid == 0) ctlk[0] = k + kstep;
     __syncthreads();
   }
+  for (int i = tid; i < pw; i += NT) lpermG[kb + i] = lp_s[i];
   if (ctl[3]) {
     if (tid == 0) {
       if (atomicCAS(&fa.status[0], 0, 1) == 0) fa.status[1] = s;
