@@ -239,26 +239,57 @@ __global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4*
       tc_fence_before();
       mbar_arrive(&pbar[w & 1]);
     };
-    int c = 0, pw = 0;
-    for (int u = pb; u < pe && ok; ++u) {
+    // Chunk cursor: pair u, updater columns [t0, t0 + kc); the loads of the
+    // next chunk are issued before the current one is stored, so their
+    // latency overlaps the stage wait, the split and the stores.
+    struct Cur {
+      int u, t0, nck, nrk, ldg, i, j;
+      const T* Ar;  // A' source row (column stride nrk)
+      const T* Br;  // B' source row of G (column stride ldg)
+    };
+    auto open = [&](Cur& x, int u) {
       const int4 pr = pairs[u];
       const int k = pr.x, a = pr.y, q0 = pr.z;
-      const int nck = fa.sn_ncol[k], nrk = fa.sn_nrow[k], ldg = nrk - nck;
-      const int i = maps[(long long)u * TC_MAP + row], j = maps[(long long)u * TC_MAP + TC_M + ub];
-      const T* Ar = pall + fa.sn_poff[k] + nck + a + i;  // column stride nrk
-      const T* Br = gall + fa.goff[k] + q0 + j;         // column stride ldg
-      for (int t0 = 0; t0 < nck; t0 += Sh::kc, ++c) {
-        T va[NA], vb[NB];
+      x.u = u;
+      x.t0 = 0;
+      x.nck = fa.sn_ncol[k];
+      x.nrk = fa.sn_nrow[k];
+      x.ldg = x.nrk - x.nck;
+      x.i = maps[(long long)u * TC_MAP + row];
+      x.j = maps[(long long)u * TC_MAP + TC_M + ub];
+      x.Ar = pall + fa.sn_poff[k] + x.nck + a + x.i;
+      x.Br = gall + fa.goff[k] + q0 + x.j;
+    };
+    auto load = [&](const Cur& x, T (&va)[NA], T (&vb)[NB]) {
 #pragma unroll
-        for (int jj = 0; jj < NA; ++jj) {
-          const int t = t0 + ta + jj;
-          va[jj] = (i >= 0 && t < nck) ? Ar[(long long)t * nrk] : F::zero();
-        }
+      for (int jj = 0; jj < NA; ++jj) {
+        const int t = x.t0 + ta + jj;
+        va[jj] = (x.i >= 0 && t < x.nck) ? x.Ar[(long long)t * x.nrk] : F::zero();
+      }
 #pragma unroll
-        for (int jj = 0; jj < NB; ++jj) {
-          const int t = t0 + tb + jj;
-          vb[jj] = (j >= 0 && t < nck) ? Br[(long long)t * ldg] : F::zero();
+      for (int jj = 0; jj < NB; ++jj) {
+        const int t = x.t0 + tb + jj;
+        vb[jj] = (x.j >= 0 && t < x.nck) ? x.Br[(long long)t * x.ldg] : F::zero();
+      }
+    };
+    int c = 0, pw = 0;
+    if (pb < pe) {
+      Cur cur;
+      open(cur, pb);
+      T va[NA], vb[NB];
+      load(cur, va, vb);
+      for (;;) {
+        Cur nx = cur;
+        nx.t0 += Sh::kc;
+        bool more = true;
+        if (nx.t0 >= nx.nck) {
+          if (cur.u + 1 < pe)
+            open(nx, cur.u + 1);
+          else
+            more = false;
         }
+        T na[NA], nb2[NB];
+        if (more) load(nx, na, nb2);
         const int st = c % TC_NS;
         if (c >= TC_NS && !mbar_wait_bounded(&empty[st], (uint32_t)(((c / TC_NS) - 1) & 1))) {
           ok = false;
@@ -285,10 +316,14 @@ __global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4*
         mbar_arrive(&full[st]);
         // window w - 1 is two chunks behind: promote it before the MMA warp
         // needs its accumulator again (window w + 1)
-        if (c % TC_WIN == 2 && c >= TC_WIN) {
-          promote(pw++);
-          if (!ok) break;
-        }
+        if (c % TC_WIN == 2 && c >= TC_WIN) promote(pw++);
+        ++c;
+        if (!more || !ok) break;
+        cur = nx;
+#pragma unroll
+        for (int jj = 0; jj < NA; ++jj) va[jj] = na[jj];
+#pragma unroll
+        for (int jj = 0; jj < NB; ++jj) vb[jj] = nb2[jj];
       }
     }
     if (ok && c > 0)
