@@ -58,6 +58,10 @@ extern "C" {
 /* Zero-pivot policy (ZeroPivotAction, src/numeric/multifrontal_ldlt.rs:165). */
 #define RSLAB_PIVOT_FAIL 0
 #define RSLAB_PIVOT_PERTURB 1
+/* ZeroPivotAction::ForceAccept: static pivoting with the floor
+ * max(max|A_scaled|, 1) * eps computed on the device at factor time
+ * (factor_left_looking, src/numeric/multifrontal_ldlt.rs:3355-3358). */
+#define RSLAB_PIVOT_FORCE_ACCEPT 2
 
 /* Equilibration (ScalingStrategy): one-pass inf-norm (default) or identity. */
 #define RSLAB_SCALING_ONEPASS 0
@@ -86,6 +90,8 @@ typedef struct {
   int32_t use_graph;           /* capture factor / solve as CUDA graphs (1) */
   void* stream;                /* cudaStream_t to run on, or NULL for a private one */
   int32_t schur_engine;        /* RSLAB_SCHUR_*: how f32/c32 descendant updates run */
+  double drop_tol;             /* > 0: incomplete factor, drop |L_ip| < drop_tol * max_i |L_ip| per
+                                * column (SolverSettings::drop_tol, multifrontal_ldlt.rs:2359-2367) */
 } rslab_factor_settings;
 
 /* Descendant (cmod) updates of the single-precision fields: 3xTF32 split
@@ -151,6 +157,11 @@ int rslab_factor(rslab_sym_handle* sym, int dtype, const void* values, int value
 int rslab_refactor(rslab_fac_handle* fac, const void* values, int values_on_device);
 /* x = A^-1 b, b and x row-major n x nrhs. */
 int rslab_solve(rslab_fac_handle* fac, const void* b, int64_t nrhs, void* x, int on_device);
+/* LdltSolver::solve_refined (src/numeric/sparse_solver.rs:335-375): solve, then
+ * up to max_iter corrections x += A^-1 (b - A x) against the factored values,
+ * in the factor's field, keeping per column the iterate of smallest ||r||_inf. */
+int rslab_solve_refined(rslab_fac_handle* fac, const void* b, int64_t nrhs, int64_t max_iter, void* x,
+                        int on_device);
 int rslab_factor_info(const rslab_fac_handle* fac, rslab_factor_info_t* info);
 void* rslab_factor_stream(const rslab_fac_handle* fac);
 /* Eager refactor with per-launch CUDA events: device ms, launches and

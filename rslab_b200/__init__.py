@@ -9,10 +9,11 @@ from .solver import (  # noqa: F401
     LdltSolver, LdltSymbolic, MixedInfo, MixedLdltSolver, NumericallyRankDeficient, Ordering, RslabError,
     SolverSettings, ZeroPivotAction, amd_order, device_count,
 )
+from .ldlt import Ldlt, ldlt  # noqa: F401
 
 __all__ = [
     "CscMatrix", "LdltSymbolic", "LdltSolver", "MixedLdltSolver", "SolverSettings", "ZeroPivotAction",
     "Ordering", "Inertia", "MixedInfo", "LdltFactors", "Diagnostics", "RslabError",
     "NumericallyRankDeficient", "InvalidInput", "DimensionMismatch", "CudaError", "amd_order",
-    "device_count", "CERT_FACTOR",
+    "device_count", "CERT_FACTOR", "ldlt", "Ldlt",
 ]

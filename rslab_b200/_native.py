@@ -12,7 +12,7 @@ LIB_PATH = Path(__file__).resolve().parent / "librslab_b200.so"
 
 F64, C64, F32, C32 = 0, 1, 2, 3
 ORDER_AMD, ORDER_METIS_ND, ORDER_NATURAL, ORDER_GIVEN = 0, 1, 2, 3
-PIVOT_FAIL, PIVOT_PERTURB = 0, 1
+PIVOT_FAIL, PIVOT_PERTURB, PIVOT_FORCE_ACCEPT = 0, 1, 2
 SCALING_ONEPASS, SCALING_IDENTITY = 0, 1
 SCHUR_TENSOR, SCHUR_FMA = 0, 1
 
@@ -41,6 +41,7 @@ class FactorSettings(C.Structure):
         ("use_graph", C.c_int32),
         ("stream", vp),
         ("schur_engine", C.c_int32),
+        ("drop_tol", C.c_double),
     ]
 
 
@@ -94,6 +95,7 @@ SIGNATURES = {
                                        C.POINTER(C.c_double), i64p]),
     "rslab_factor_profile": (C.c_int, [vp, C.POINTER(C.c_double), i64p, C.POINTER(C.c_double)]),
     "rslab_solve_profile": (C.c_int, [vp, C.c_int64, C.POINTER(C.c_double), i64p]),
+    "rslab_solve_refined": (C.c_int, [vp, vp, C.c_int64, C.c_int64, vp, C.c_int]),
     "rslab_profile_trace": (C.c_int, [vp, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                       C.POINTER(C.c_float), i64p]),
     "rslab_free_factor": (None, [vp]),

@@ -51,6 +51,7 @@ struct FactorArgs {
   double perturb_floor; // < 0: exact mode
   void* gpool;          // G_k = L21_k D_k, (nrow_k - ncol_k) x ncol_k at goff[k] (tensor-core cmod)
   const long long* goff;
+  const double* floor_dev;  // non-null: static-pivot floor computed on the device (force-accept)
 };
 
 // ---------------------------------------------------------------------------
@@ -673,6 +674,7 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
                                               int nb_big) {
   using F = Field<T>;
   if (fa.status[0] != 0) return;
+  const double pfloor = fa.floor_dev ? *fa.floor_dev : fa.perturb_floor;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int4 tk = tasks[blockIdx.x];
   const int s = tk.x, kb = tk.y, slot = tk.z, fuse = tk.w;
@@ -753,7 +755,7 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
       int kstep = 1, kp = k;
       bool err = false;
       if (fmax(absakk, colmax) == 0.0) {
-        err = fa.perturb_floor < 0.0;
+        err = pfloor < 0.0;
       } else if (absakk >= alpha * colmax) {
       } else {
         double rmx = 0.0;
@@ -807,10 +809,10 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
         }
         if (kstep == 1) {
           T dk = A[pk(k, k, pw)];
-          if (fa.perturb_floor >= 0.0) {
+          if (pfloor >= 0.0) {
             const double m = F::mag(dk);
-            if (m < fa.perturb_floor) {
-              dk = m == 0.0 ? F::from_real(fa.perturb_floor) : F::scale(dk, fa.perturb_floor / m);
+            if (m < pfloor) {
+              dk = m == 0.0 ? F::from_real(pfloor) : F::scale(dk, pfloor / m);
               __syncwarp();
               if (lane == 0) {
                 A[pk(k, k, pw)] = dk;
@@ -839,10 +841,10 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
           T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
           const double scale = fmax(fmax(F::mag(d11), F::mag(d22)), F::mag(d21));
           const double growth_floor = 1e-14 * scale * scale;
-          if (fa.perturb_floor >= 0.0) {
-            const double fl = fmax(fa.perturb_floor * fa.perturb_floor, growth_floor);
+          if (pfloor >= 0.0) {
+            const double fl = fmax(pfloor * pfloor, growth_floor);
             if (F::mag(det) < fl) {
-              const double lift = fmax(fa.perturb_floor, scale * sqrt(1e-14));
+              const double lift = fmax(pfloor, scale * sqrt(1e-14));
               d11 = F::add(d11, F::from_real(lift));
               d22 = F::add(d22, F::from_real(lift));
               det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
@@ -992,6 +994,53 @@ __global__ void __launch_bounds__(NT) k_deep(FactorArgs fa, const int4* __restri
                               reinterpret_cast<const T*>(fa.dsub) + first + kb, fa.kind + first + kb);
   __syncthreads();
   replay_deep_rows<T, NT>(panel, nrow, kb, pw, nb, rs0, min(rs0 + DEEP_R, nrow), snap, P, X);
+}
+
+// ---------------------------------------------------------------------------
+// Force-accept floor: max(max_ij |A_scaled ij|, 1) * eps over the assembled
+// panels (every stored entry of the equilibrated matrix lands in exactly one
+// slot; the other slots are zero).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_panel_absmax(long long m, const T* __restrict__ panel, unsigned long long* __restrict__ out) {
+  double v = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+    v = fmax(v, Field<T>::mag(panel[i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __double_as_longlong(v));
+}
+
+__global__ void k_force_floor(const unsigned long long* __restrict__ amax, double* __restrict__ floor_out) {
+  const double a = __longlong_as_double(*amax);
+  *floor_out = fmax(a, 1.0) * 2.220446049250313e-16;
+}
+
+// ---------------------------------------------------------------------------
+// Incomplete factor (drop_tol): per pivot column p of every panel, drop the
+// multipliers below tau * max |L_ip| (rows below the pivot, the 2x2 coupling
+// slot excluded) — ldlt_emit_and_free, src/numeric/multifrontal_ldlt.rs:2359.
+// One CTA per supernode, one warp per column.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_drop_tol(FactorArgs fa, double tau) {
+  using F = Field<T>;
+  if (fa.status[0] != 0) return;
+  const int s = blockIdx.x;
+  const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
+  T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int p = warp; p < ncol; p += nw) {
+    const int i0 = p + (fa.kind[first + p] == 1 ? 2 : 1);
+    T* col = panel + (long long)p * nrow;
+    double cm = 0.0;
+    for (int i = i0 + lane; i < nrow; i += 32) cm = fmax(cm, F::mag(col[i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, o));
+    const double thresh = tau * cm;
+    for (int i = i0 + lane; i < nrow; i += 32)
+      if (F::mag(col[i]) < thresh) col[i] = F::zero();
+  }
 }
 
 }  // namespace rsd

@@ -625,6 +625,8 @@ struct rslab_fac_handle {
   int* status = nullptr;
   int* h_status = nullptr;  // pinned
   unsigned long long* cnt3 = nullptr;
+  double* floor_dev = nullptr;          // force-accept static-pivot floor (device)
+  unsigned long long* amax_dev = nullptr;
   void* scratch = nullptr;
   long long scratch_stride = 0;
   void* gpool = nullptr;  // G_k = L21_k D_k (tensor-core cmod only)
@@ -689,6 +691,8 @@ FactorArgs make_fargs(rslab_fac_handle& F) {
   a.perturb_floor = F.set.on_zero_pivot == RSLAB_PIVOT_PERTURB ? F.set.abs_floor : -1.0;
   a.gpool = F.gpool;
   a.goff = H.d_goff;
+  a.floor_dev = F.floor_dev;
+  if (F.set.on_zero_pivot == RSLAB_PIVOT_FORCE_ACCEPT) a.perturb_floor = 0.0;
   return a;
 }
 
@@ -747,6 +751,12 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
   FactorArgs fa = make_fargs<T>(F);
   const int nb_small = H.panel_nb, nb_big = std::max(H.panel_nb, 128);
   const bool use_tc = TensorCmod<T>::ok && F.set.schur_engine == RSLAB_SCHUR_TENSOR;
+  if (F.floor_dev) {
+    CK(cudaMemsetAsync(F.amax_dev, 0, sizeof(unsigned long long), st));
+    k_panel_absmax<T><<<(unsigned)std::min<long long>(grid1(H.panel_elems), 148LL * 8), 256, 0, st>>>(
+        H.panel_elems, (const T*)F.panel, F.amax_dev);
+    k_force_floor<<<1, 1, 0, st>>>(F.amax_dev, F.floor_dev);
+  }
   if (prof) prof->mark(st, 0);
   for (const Launch& L : H.fplan) {
     switch (L.kind) {
@@ -791,6 +801,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
                                                                                : 4,
                  L.ntasks, L.kind);
   }
+  if (F.set.drop_tol > 0.0 && H.ns > 0) k_drop_tol<T><<<H.ns, 256, 0, st>>>(fa, F.set.drop_tol);
   CK(cudaMemsetAsync(F.cnt3, 0, 3 * sizeof(unsigned long long), st));
   k_inertia<T><<<grid1(n), 256, 0, st>>>(n, (const T*)F.d, (const T*)F.dsub, F.kind, F.cnt3);
   CK(cudaGetLastError());
@@ -1091,6 +1102,67 @@ static int gmres_column(MixedCtx<Hi>& M, const Hi* b, Hi* x, double tol, int max
 
 #include "engine_gmres.inc"
 
+// LdltSolver::solve_refined (src/numeric/sparse_solver.rs:335-375) in the
+// factor's field: x = A^-1 b, then for it = 0..max_iter: r = b - A x (stored
+// values, full symmetric CSR), keep per column the iterate of smallest
+// ||r||_inf, stop at it == max_iter or when every residual is exactly zero,
+// else x += A^-1 r.
+template <typename T>
+static void refined_solve_impl(rslab_fac_handle& F, const void* bsrc, int nrhs, int max_iter, void* xdst,
+                               bool on_device) {
+  if (F.last_status) throw RslabError(Status::NumericallyRankDeficient, "factor is not valid");
+  auto& H = *F.sym;
+  const int n = H.n;
+  const long long m = (long long)n * nrhs;
+  const size_t es = sizeof(T);
+  cudaStream_t st = F.st;
+  KernelSetup<T>::configure();
+  ensure_ws<T>(F, nrhs);
+  T* bb = (T*)F.arena.get(A_B, m * es);
+  T* xx = (T*)F.arena.get(A_X, m * es);
+  T* best = (T*)F.arena.get(A_BEST, m * es);
+  T* r = (T*)F.arena.get(A_R, m * es);
+  unsigned char* mask = (unsigned char*)F.arena.get(A_MASK, 64 + nrhs);
+  unsigned long long* nbits = (unsigned long long*)F.arena.get(A_NB, (size_t)std::max(nrhs, 3) * 64 * 8);
+  CK(cudaMemcpyAsync(bb, bsrc, m * es, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  auto solve_into = [&](const T* rhs, T* out) {
+    CK(cudaMemcpyAsync(F.bdev, rhs, m * es, cudaMemcpyDeviceToDevice, st));
+    solve_ws<T>(F, nrhs);
+    CK(cudaMemcpyAsync(out, F.xdev, m * es, cudaMemcpyDeviceToDevice, st));
+  };
+  solve_into(bb, xx);
+  std::vector<double> best_res(nrhs, INFINITY), res(nrhs);
+  std::vector<unsigned char> hmask(nrhs);
+  std::vector<unsigned long long> hb(nrhs);
+  for (int it = 0; it <= max_iter; ++it) {
+    k_residual<T><<<grid1(m), 256, 0, st>>>(n, nrhs, H.d_sp_rp, H.d_sp_ci, H.d_sp_vmap, (const T*)F.aval, xx, bb, r);
+    CK(cudaMemsetAsync(nbits, 0, nrhs * sizeof(unsigned long long), st));
+    dim3 g(std::min<unsigned>(grid1(n), 1024u), nrhs);
+    k_colmax<T><<<g, 256, 0, st>>>(n, nrhs, r, nbits);
+    CK(cudaMemcpyAsync(hb.data(), nbits, nrhs * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    bool any = false, all_zero = true;
+    for (int c = 0; c < nrhs; ++c) {
+      std::memcpy(&res[c], &hb[c], 8);
+      hmask[c] = res[c] < best_res[c];
+      if (hmask[c]) {
+        best_res[c] = res[c];
+        any = true;
+      }
+      if (res[c] != 0.0) all_zero = false;
+    }
+    if (any) {
+      CK(cudaMemcpyAsync(mask, hmask.data(), nrhs, cudaMemcpyHostToDevice, st));
+      k_copy_cols<T><<<grid1(m), 256, 0, st>>>(m, nrhs, mask, xx, best);
+    }
+    if (all_zero || it == max_iter) break;
+    solve_into(r, r);
+    k_axpy1<T><<<grid1(m), 256, 0, st>>>(m, r, xx);
+  }
+  CK(cudaMemcpyAsync(xdst, best, m * es, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+}
+
 extern "C" {
 
 const char* rslab_last_error(void) { return g_last_error.c_str(); }
@@ -1115,6 +1187,7 @@ void rslab_default_factor_settings(rslab_factor_settings* s) {
   s->use_graph = 1;
   s->stream = nullptr;
   s->schur_engine = RSLAB_SCHUR_TENSOR;
+  s->drop_tol = 0.0;
 }
 
 int rslab_analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, const rslab_analyze_settings* settings,
@@ -1247,6 +1320,10 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
     const long long nbm = sym->max_nb;
     F->scratch_stride = (nbm * nbm * (long long)es + 3 * nbm * 4 + 255) / 256 * 256;
     F->scratch = F->al<unsigned char>((size_t)std::max(1, sym->max_getf2_tasks) * F->scratch_stride);
+    if (F->set.on_zero_pivot == RSLAB_PIVOT_FORCE_ACCEPT) {
+      F->floor_dev = F->al<double>(1);
+      F->amax_dev = F->al<unsigned long long>(1);
+    }
     if ((dtype == RSLAB_F32 || dtype == RSLAB_C32) && F->set.schur_engine == RSLAB_SCHUR_TENSOR)
       F->gpool = F->al<unsigned char>((size_t)std::max(sym->g_elems, 1LL) * es);
     if (F->set.scaling != RSLAB_SCALING_ONEPASS) {
@@ -1315,6 +1392,22 @@ int rslab_refactor(rslab_fac_handle* F, const void* values, int values_on_device
       CK(cudaMemcpyAsync(F->aval, values, H.nnz * elem_size(F->dtype), kd, F->st));
     }
     dispatch_field(F->dtype, [&](auto z) { run_factor<decltype(z)>(*F); });
+    return 0;
+  } catch (const RslabError& e) {
+    return fail(e);
+  } catch (const std::exception& e) {
+    return fail(RslabError(Status::InvalidInput, e.what()));
+  }
+}
+
+int rslab_solve_refined(rslab_fac_handle* F, const void* b, int64_t nrhs, int64_t max_iter, void* x,
+                        int on_device) {
+  try {
+    if (!F || nrhs <= 0) throw RslabError(Status::DimensionMismatch, "nrhs must be positive");
+    if (max_iter < 0) throw RslabError(Status::InvalidInput, "max_iter must be non-negative");
+    dispatch_field(F->dtype, [&](auto z) {
+      refined_solve_impl<decltype(z)>(*F, b, (int)nrhs, (int)max_iter, x, on_device != 0);
+    });
     return 0;
   } catch (const RslabError& e) {
     return fail(e);

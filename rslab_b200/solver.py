@@ -187,6 +187,12 @@ class ZeroPivotAction:
     def perturb_to_eps(abs_floor: float) -> "ZeroPivotAction":
         return ZeroPivotAction("perturb", float(abs_floor))
 
+    @staticmethod
+    def force_accept() -> "ZeroPivotAction":
+        """Accept tiny pivots: static pivoting at max(max|A_scaled|, 1) * eps
+        (the left-looking path, multifrontal_ldlt.rs:3355-3358)."""
+        return ZeroPivotAction("force_accept")
+
 
 @dataclass
 class SolverSettings:
@@ -202,6 +208,8 @@ class SolverSettings:
     # f32/c32 descendant updates: "tensor" (3xTF32 tcgen05) or "fma" (CUDA-core
     # fp32 in the oracle's operation order, bit-exact)
     schur_engine: str = "tensor"
+    # incomplete factor: drop |L_ip| < drop_tol * max_i |L_ip| per column
+    drop_tol: Optional[float] = None
 
     @staticmethod
     def exact() -> "SolverSettings":
@@ -259,6 +267,9 @@ class SolverSettings:
         if self.on_zero_pivot.kind == "perturb":
             s.on_zero_pivot = N.PIVOT_PERTURB
             s.abs_floor = self.on_zero_pivot.abs_floor
+        elif self.on_zero_pivot.kind == "force_accept":
+            s.on_zero_pivot = N.PIVOT_FORCE_ACCEPT
+        s.drop_tol = float(self.drop_tol) if self.drop_tol else 0.0
         s.scaling = N.SCALING_ONEPASS if self.scaling == "onepass" else N.SCALING_IDENTITY
         s.use_graph = int(self.use_graph)
         s.stream = stream
@@ -471,22 +482,19 @@ class LdltSolver:
         _check(N.lib.rslab_solve(self._h, C.c_void_p(b_ptr), nrhs, C.c_void_p(x_ptr), 1))
 
     def solve_refined(self, a: CscMatrix, rhs, max_iter: int) -> np.ndarray:
-        """Iterative refinement against the original A (sparse_solver.rs:335-375)."""
+        """Iterative refinement against the factored matrix (sparse_solver.rs:335-375),
+        on the GPU: residuals from the stored values, per-column best iterate."""
         if a.n != self.n:
             raise DimensionMismatch(self.n, a.n)
-        rhs = np.ascontiguousarray(rhs, dtype=self.dtype)
-        A = a.to_scipy_full()
-        x = self.solve(rhs)
-        best_x, best_res = x.copy(), np.inf
-        for it in range(max_iter + 1):
-            r = rhs - A @ x
-            res = float(np.max(np.abs(r))) if len(r) else 0.0
-            if res < best_res:
-                best_res, best_x = res, x.copy()
-            if res == 0.0 or it == max_iter:
-                break
-            x = x + self.solve(r)
-        return best_x
+        self._sym._check_pattern(a)
+        b = np.ascontiguousarray(rhs, dtype=self.dtype)
+        nrhs = 1 if b.ndim == 1 else b.shape[1]
+        if b.shape[0] != self.n:
+            raise DimensionMismatch(self.n, b.shape[0])
+        x = np.empty_like(b)
+        _check(N.lib.rslab_solve_refined(self._h, b.ctypes.data_as(C.c_void_p), nrhs, int(max_iter),
+                                         x.ctypes.data_as(C.c_void_p), 0))
+        return x
 
     def export_factors(self) -> LdltFactors:
         n = self.n
