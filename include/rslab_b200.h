@@ -148,6 +148,25 @@ int rslab_symbolic_export(const rslab_sym_handle* sym, int64_t* perm, int64_t* s
                           int64_t* col_counts, int64_t* parent);
 void rslab_free_symbolic(rslab_sym_handle* sym);
 
+/* Independent systems as one analysis (no reference counterpart: the
+ * reference factors them one call at a time; `rslab_factor_batch` of the
+ * design sketch is this entry plus rslab_factor on the concatenated values).
+ * System i keeps its own LdltSymbolic::analyze result (orderings, supernodes
+ * and update lists identical to a lone analysis); the systems are laid out
+ * block-diagonally (columns and stored entries concatenated in input order)
+ * so one launch per assembly-tree level covers that level of every system.
+ * Values / right-hand sides of the batch are the systems' arrays
+ * concatenated; rslab_mixed_solve on a batch handle certifies every
+ * (system, column) unit separately. */
+int rslab_analyze_batch(int64_t count, const int64_t* n, const int64_t* const* col_ptr,
+                        const int64_t* const* row_idx, const rslab_analyze_settings* settings,
+                        rslab_sym_handle** out);
+/* count systems; seg_begin[count+1] column offsets; nnz_begin[count+1] value offsets. */
+int rslab_batch_layout(const rslab_sym_handle* sym, int64_t* count, int64_t* seg_begin, int64_t* nnz_begin);
+/* Per (system, column) backward errors of the handle's last rslab_mixed_solve,
+ * index system * nrhs + column; *count = systems * nrhs (at most cap written). */
+int rslab_mixed_batch_result(const rslab_fac_handle* fac, int64_t cap, double* backward_error, int64_t* count);
+
 /* Phases 2-3: equilibrate + numeric factor on the GPU.  `values` follow the
  * analysed pattern's row_idx order; host memory unless values_on_device.  On a
  * singular pivot returns RSLAB_NUMERICALLY_RANK_DEFICIENT and still hands

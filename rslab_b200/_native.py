@@ -95,6 +95,10 @@ SIGNATURES = {
                                        C.POINTER(C.c_double), i64p]),
     "rslab_factor_profile": (C.c_int, [vp, C.POINTER(C.c_double), i64p, C.POINTER(C.c_double)]),
     "rslab_solve_profile": (C.c_int, [vp, C.c_int64, C.POINTER(C.c_double), i64p]),
+    "rslab_analyze_batch": (C.c_int, [C.c_int64, i64p, C.POINTER(i64p), C.POINTER(i64p),
+                                      C.POINTER(AnalyzeSettings), C.POINTER(vp)]),
+    "rslab_batch_layout": (C.c_int, [vp, i64p, i64p, i64p]),
+    "rslab_mixed_batch_result": (C.c_int, [vp, C.c_int64, C.POINTER(C.c_double), i64p]),
     "rslab_solve_refined": (C.c_int, [vp, vp, C.c_int64, C.c_int64, vp, C.c_int]),
     "rslab_profile_trace": (C.c_int, [vp, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                       C.POINTER(C.c_float), i64p]),

@@ -82,7 +82,7 @@ struct Arena {
 // Arena slots of the mixed-precision driver.
 enum ArenaSlot {
   A_R, A_DX, A_AX, A_NB, A_B, A_X, A_BEST, A_MASK, A_BC, A_XC, A_AXC,
-  A_GM_PART, A_GM_W, A_GM_R, A_GM_V, A_GM_Z
+  A_GM_PART, A_GM_W, A_GM_R, A_GM_V, A_GM_Z, A_SEGNORM
 };
 
 size_t elem_size(int dtype) {
@@ -114,6 +114,11 @@ struct Launch {
 // ---------------------------------------------------------------------------
 struct rslab_sym_handle {
   rslab::Symbolic S;
+  // independent systems (rslab_analyze_batch): system i owns user columns
+  // [seg_begin[i], seg_begin[i+1]) and stored entries [nnz_begin[i], ...);
+  // one system otherwise
+  std::vector<long long> seg_begin, nnz_begin;
+  std::vector<int> seg_of_g;  // system of every analysed (g-order) column
   int panel_nb = 64;
   int n = 0, ns = 0;
   long long nnz = 0;
@@ -167,6 +172,8 @@ struct rslab_sym_handle {
   int4* d_st4 = nullptr;
   long long* d_uoff = nullptr;
   int *d_pull_ptr = nullptr, *d_pull_src = nullptr;
+  int* d_seg_of_row = nullptr;  // system of every user row (batch handles)
+  long long* d_seg_begin = nullptr;
   std::mutex mu;
   rslab_analyze_settings settings{};
 
@@ -224,6 +231,13 @@ struct rslab_sym_handle {
     d_uoff = up(uoff, st);
     d_pull_ptr = up(pull_ptr, st);
     d_pull_src = up(pull_src, st);
+    if (seg_begin.size() > 2) {
+      std::vector<int> sr(n);
+      for (size_t i = 0; i + 1 < seg_begin.size(); ++i)
+        for (long long r = seg_begin[i]; r < seg_begin[i + 1]; ++r) sr[r] = (int)i;
+      d_seg_of_row = up(sr, st);
+    }
+    d_seg_begin = up(seg_begin, st);
     CK(cudaStreamSynchronize(st));
     device = dev;
   }
@@ -647,6 +661,9 @@ struct rslab_fac_handle {
   std::vector<int> tr_kind, tr_grid;
   std::vector<float> tr_ms;
   Arena arena;  // mixed-precision refinement scratch
+  // per (system, column) backward errors of the last mixed solve
+  std::vector<double> last_be;
+  int last_be_nrhs = 0;
 
   ~rslab_fac_handle() {
     if (fgraph) cudaGraphExecDestroy(fgraph);
@@ -1215,6 +1232,8 @@ int rslab_analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, con
     H->settings = st;
     H->panel_nb = (int)std::max<int64_t>(st.panel_nb, 8);
     H->S = rslab::analyze(n, col_ptr, row_idx, o);
+    H->seg_begin = {0, (long long)n};
+    H->nnz_begin = {0, (long long)col_ptr[n]};
     build_plan(*H, col_ptr, row_idx);
     *out = H.release();
     return 0;
@@ -1223,6 +1242,77 @@ int rslab_analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, con
   } catch (const std::exception& e) {
     return fail(RslabError(Status::InvalidInput, e.what()));
   }
+}
+
+int rslab_analyze_batch(int64_t count, const int64_t* n, const int64_t* const* col_ptr,
+                        const int64_t* const* row_idx, const rslab_analyze_settings* settings,
+                        rslab_sym_handle** out) {
+  try {
+    if (!out || count <= 0 || !n || !col_ptr || !row_idx) throw RslabError(Status::InvalidInput, "bad batch arguments");
+    *out = nullptr;
+    rslab_analyze_settings st;
+    if (settings)
+      st = *settings;
+    else
+      rslab_default_analyze_settings(&st);
+    if (st.ordering == RSLAB_ORDER_GIVEN) throw RslabError(Status::InvalidInput, "batch analysis takes no given permutation");
+    rslab::AnalyzeOptions o;
+    o.ordering = (rslab::Ordering)st.ordering;
+    o.nemin = st.nemin;
+    o.relax = st.relax != 0;
+    o.relax_max_width = st.relax_max_width;
+    o.relax_max_extra_rows = st.relax_max_extra_rows;
+    o.hybrid_liu = st.hybrid_liu != 0;
+    o.given_perm = nullptr;
+    std::vector<rslab::Symbolic> parts((size_t)count);
+    std::vector<long long> seg{0}, nz{0};
+    for (int64_t i = 0; i < count; ++i) {
+      if (n[i] < 0 || !col_ptr[i] || (n[i] > 0 && !row_idx[i] && col_ptr[i][n[i]] > 0))
+        throw RslabError(Status::InvalidInput, "bad CSC of system " + std::to_string(i));
+      rslab::validate_lower_csc(n[i], col_ptr[i], row_idx[i], col_ptr[i][n[i]]);
+      parts[i] = rslab::analyze(n[i], col_ptr[i], row_idx[i], o);
+      seg.push_back(seg.back() + n[i]);
+      nz.push_back(nz.back() + col_ptr[i][n[i]]);
+    }
+    if (seg.back() >= (1LL << 31)) throw RslabError(Status::InvalidInput, "batch too large");
+    // block-diagonal lower CSC of the whole batch (user order)
+    std::vector<int64_t> cp{0}, ri;
+    ri.reserve(nz.back());
+    for (int64_t i = 0; i < count; ++i) {
+      for (int64_t j = 0; j < n[i]; ++j) {
+        for (int64_t k = col_ptr[i][j]; k < col_ptr[i][j + 1]; ++k) ri.push_back(row_idx[i][k] + seg[i]);
+        cp.push_back((int64_t)ri.size());
+      }
+    }
+    auto H = std::make_unique<rslab_sym_handle>();
+    H->settings = st;
+    H->panel_nb = (int)std::max<int64_t>(st.panel_nb, 8);
+    H->S = rslab::merge_independent(parts);
+    H->seg_begin = seg;
+    H->nnz_begin = nz;
+    build_plan(*H, cp.data(), ri.data());
+    *out = H.release();
+    return 0;
+  } catch (const RslabError& e) {
+    return fail(e);
+  } catch (const std::exception& e) {
+    return fail(RslabError(Status::InvalidInput, e.what()));
+  }
+}
+
+int rslab_batch_layout(const rslab_sym_handle* h, int64_t* count, int64_t* seg_begin, int64_t* nnz_begin) {
+  if (!h || !count) return fail(RslabError(Status::InvalidInput, "null argument"));
+  *count = (int64_t)h->seg_begin.size() - 1;
+  if (seg_begin) std::copy(h->seg_begin.begin(), h->seg_begin.end(), seg_begin);
+  if (nnz_begin) std::copy(h->nnz_begin.begin(), h->nnz_begin.end(), nnz_begin);
+  return 0;
+}
+
+int rslab_mixed_batch_result(const rslab_fac_handle* F, int64_t cap, double* backward_error, int64_t* count) {
+  if (!F || !count) return fail(RslabError(Status::InvalidInput, "null argument"));
+  *count = (int64_t)F->last_be.size();
+  for (int64_t i = 0; i < std::min<int64_t>(cap, *count); ++i) backward_error[i] = F->last_be[i];
+  return 0;
 }
 
 void rslab_free_symbolic(rslab_sym_handle* h) { delete h; }

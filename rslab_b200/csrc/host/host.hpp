@@ -104,6 +104,13 @@ struct Symbolic {
 Symbolic analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx,
                  const AnalyzeOptions& opt);
 
+// Independent systems as one block-diagonal analysis: system i occupies
+// columns [col_off[i], col_off[i+1]); its supernodes, row structures, update
+// lists and levels are its own analysis shifted by the offsets, so the
+// assembly forest has one tree (or more) per system and level l collects the
+// level-l supernodes of every system.
+Symbolic merge_independent(const std::vector<Symbolic>& parts);
+
 // Dense partial BK flop model per supernode: F(r,c) = sum_{m=r-c+1}^{r}(m^2-1).
 double supernode_flops(int64_t r, int64_t c);
 

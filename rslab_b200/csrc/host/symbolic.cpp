@@ -579,4 +579,56 @@ Symbolic analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, cons
   return S;
 }
 
+Symbolic merge_independent(const std::vector<Symbolic>& parts) {
+  Symbolic M;
+  int64_t coff = 0, soff = 0, nlev = 0;
+  for (const auto& P : parts) nlev = std::max<int64_t>(nlev, (int64_t)P.by_level.size());
+  M.by_level.assign(nlev, {});
+  M.permuted.col_ptr.push_back(0);
+  M.rs_ptr.push_back(0);
+  M.upd_ptr.push_back(0);
+  M.resolved_ordering = parts.empty() ? 0 : parts[0].resolved_ordering;
+  for (const auto& P : parts) {
+    M.n += P.n;
+    M.nnz += P.nnz;
+    for (int64_t v : P.perm) M.perm.push_back(v + coff);
+    for (int64_t v : P.perm_inv) M.perm_inv.push_back(v + coff);
+    for (int64_t v : P.parent) M.parent.push_back(v < 0 ? -1 : v + coff);
+    M.col_counts.insert(M.col_counts.end(), P.col_counts.begin(), P.col_counts.end());
+    const int64_t pbase = (int64_t)M.permuted.row_idx.size();
+    for (size_t j = 1; j < P.permuted.col_ptr.size(); ++j) M.permuted.col_ptr.push_back(P.permuted.col_ptr[j] + pbase);
+    for (int64_t r : P.permuted.row_idx) M.permuted.row_idx.push_back(r + coff);
+    const int64_t ns = (int64_t)P.sn.size();
+    for (int64_t s = 0; s < ns; ++s) {
+      Supernode x = P.sn[s];
+      x.first_col += coff;
+      for (auto& c : x.children) c += soff;
+      M.sn.push_back(std::move(x));
+      const int64_t rb = (int64_t)M.rs.size();
+      for (int64_t q = P.rs_ptr[s]; q < P.rs_ptr[s + 1]; ++q) M.rs.push_back(P.rs[q] + coff);
+      (void)rb;
+      M.rs_ptr.push_back((int64_t)M.rs.size());
+      for (int64_t q = P.upd_ptr[s]; q < P.upd_ptr[s + 1]; ++q) {
+        M.upd.push_back(P.upd[q] + soff);
+        M.upd_p0.push_back(P.upd_p0[q]);
+        M.upd_p1.push_back(P.upd_p1[q]);
+      }
+      M.upd_ptr.push_back((int64_t)M.upd.size());
+      M.level.push_back(P.level[s]);
+      M.by_level[P.level[s]].push_back(s + soff);
+    }
+    M.factor_nnz_sym += P.factor_nnz_sym;
+    M.renumbered |= P.renumbered;
+    M.amd.ncmpa += P.amd.ncmpa;
+    M.amd.n_dense += P.amd.n_dense;
+    M.amd.ndiv += P.amd.ndiv;
+    M.amd.nms_lu += P.amd.nms_lu;
+    M.amd.nms_ldl += P.amd.nms_ldl;
+    coff += P.n;
+    soff += ns;
+  }
+  M.permuted.n = M.n;
+  return M;
+}
+
 }  // namespace rslab

@@ -156,6 +156,17 @@ def c3_matrix(side: int) -> CscMatrix:
     return shifted_laplacian(dims, 0.1 * lambda_max(dims))
 
 
+def c3_sides(count: int = 512, seed: int = 2, lo: int = 12, hi: int = 40) -> list:
+    """Cube sides of the batched workload: uniform integers in [lo, hi] from Rng(seed)."""
+    rng = Rng(seed)
+    return [lo + min(int(u * (hi - lo + 1)), hi - lo) for u in rng.units(count)]
+
+
+def c3_batch(count: int = 512, seed: int = 2, lo: int = 12, hi: int = 40) -> list:
+    """The batched workload: `count` shifted 3D Laplacians (shift 0.1 lambda_max)."""
+    return [c3_matrix(s) for s in c3_sides(count, seed, lo, hi)]
+
+
 def negative_eigs_shifted_laplacian(dims, sigma: float) -> int:
     """Exact count of eigenvalues of -Delta_h - sigma I below zero (separable spectrum)."""
     ev = None
