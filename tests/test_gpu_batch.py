@@ -63,5 +63,7 @@ def test_batch_mixed_certifies_every_system():
     for a, r, x, be in zip(sy, rhs, xs, res.backward_error):
         for c in range(4):
             got = backward_error(a, x[:, c], r[:, c])
-            assert got <= 1e-14
-            assert got == pytest.approx(be[c], rel=1e-6, abs=1e-18)
+            assert got <= 1e-14 and be[c] <= 1e-14
+            # at ~1e-16 the residual itself is rounding noise of b - A x: the
+            # device and host evaluations agree to within that noise
+            assert abs(got - be[c]) <= 1e-15
