@@ -51,6 +51,8 @@ struct SolveArgs {
   const long long* uoff;  // row offset of U_s
   const int* pull_ptr;    // n + 1: pull list of column g (g order)
   const int* pull_src;    // U row of each push, update-list order per g
+  const void* linv;       // inverses of the TB x TB diagonal blocks of wide supernodes
+  const long long* linv_off;
   int ld;     // row stride (total rhs count)
   int c0;     // first rhs column of this pass
   int nrhs;   // rhs columns in this pass (<= RHS_MAX)
@@ -350,20 +352,84 @@ __global__ void __launch_bounds__(SOLVE_NT) k_bwd_off(SolveArgs a, const int2* _
   }
 }
 
-// Blocked forward solve of a wide supernode, block [j0, j0+64): in-block
-// substitution on Z (which already holds y minus the earlier blocks).
+// Inverse of the unit lower TB x TB diagonal block [j0, j0+nb) of a wide
+// supernode's panel (task (s, j0)), column-major into its TB x TB slot;
+// thread j forms column j by forward substitution, x_i = -sum_k L_ik x_k.
+// Runs once per factor, after the supernode's panel factorization.
+template <typename T>
+__global__ void __launch_bounds__(TB) k_diag_inv(const int2* __restrict__ tasks, const int* __restrict__ sn_ncol,
+                                                 const int* __restrict__ sn_nrow, const long long* __restrict__ sn_poff,
+                                                 const T* __restrict__ panel, const int* __restrict__ status,
+                                                 T* __restrict__ linv, const long long* __restrict__ linv_off) {
+  using F = Field<T>;
+  if (status[0] != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Ls = reinterpret_cast<T*>(smem_raw);  // TB x (TB + 1), row i at i * (TB + 1)
+  T* Xs = Ls + TB * (TB + 1);               // TB x (TB + 1)
+  const int2 tk = tasks[blockIdx.x];
+  const int s = tk.x, j0 = tk.y;
+  const int ncol = sn_ncol[s], nrow = sn_nrow[s];
+  const int nb = min(TB, ncol - j0);
+  const T* L = panel + sn_poff[s];
+  for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
+    const int i = e % TB, j = e / TB;
+    Ls[i * (TB + 1) + j] = (i < nb && j < i) ? L[(j0 + i) + (long long)(j0 + j) * nrow] : F::zero();
+  }
+  __syncthreads();
+  const int j = threadIdx.x;
+  if (j < TB) {
+    for (int i = 0; i < TB; ++i) Xs[i * (TB + 1) + j] = (i == j && j < nb) ? F::one() : F::zero();
+    if (j < nb)
+      for (int i = j + 1; i < nb; ++i) {
+        T acc = F::zero();
+        for (int k = j; k < i; ++k) acc = F::fma_(Ls[i * (TB + 1) + k], Xs[k * (TB + 1) + j], acc);
+        Xs[i * (TB + 1) + j] = F::sub(F::zero(), acc);
+      }
+  }
+  __syncthreads();
+  T* out = linv + linv_off[s] + (long long)(j0 / TB) * TB * TB;
+  for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
+    const int i = e % TB, jj = e / TB;
+    out[i + (long long)jj * TB] = Xs[i * (TB + 1) + jj];
+  }
+}
+
+// Blocked forward solve of a wide supernode, block [j0, j0+nb): Z holds y
+// minus the earlier blocks; z = Linv y with the precomputed inverse
+// (thread: row i = tid % TB, right-hand sides tid / TB + 4 m; k ascending).
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_ftrsv_blk(SolveArgs a, const int4* __restrict__ tasks) {
+  using F = Field<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* red = reinterpret_cast<T*>(smem_raw);
-  T* Ls = red + (SOLVE_NT / 32) * 32 * RHS_MAX;
-  T* zb = Ls + SB * (SB + 1);
+  T* Ys = reinterpret_cast<T*>(smem_raw);  // TB x RHS_MAX
   const int4 tk = tasks[blockIdx.x];
   const int s = tk.x, j0 = tk.y;
-  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
-  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
-  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  fwd_block_range<T>(a, L, nrow, Z, j0, min(j0 + TB, ncol), j0, red, Ls, zb);
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s];
+  const int nb = min(TB, ncol - j0);
+  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)(first + j0) * a.ld;
+  const T* Li = reinterpret_cast<const T*>(a.linv) + a.linv_off[s] + (long long)(j0 / TB) * TB * TB;
+  for (int e = threadIdx.x; e < TB * RHS_MAX; e += SOLVE_NT) {
+    const int k = e / RHS_MAX, c = e % RHS_MAX;
+    Ys[e] = (k < nb && c < a.nrhs) ? Z[(long long)k * a.ld + c] : F::zero();
+  }
+  __syncthreads();
+  const int i = threadIdx.x % TB, cg = threadIdx.x / TB;
+  constexpr int NCG = SOLVE_NT / TB;
+  T acc[RHS_MAX / NCG];
+#pragma unroll
+  for (int m = 0; m < RHS_MAX / NCG; ++m) acc[m] = F::zero();
+  if (i < nb)
+    for (int k = 0; k <= i; ++k) {
+      const T l = Li[i + (long long)k * TB];
+#pragma unroll
+      for (int m = 0; m < RHS_MAX / NCG; ++m) acc[m] = F::fma_(l, Ys[k * RHS_MAX + cg + NCG * m], acc[m]);
+    }
+  if (i < nb)
+#pragma unroll
+    for (int m = 0; m < RHS_MAX / NCG; ++m) {
+      const int c = cg + NCG * m;
+      if (c < a.nrhs) Z[(long long)i * a.ld + c] = acc[m];
+    }
 }
 
 // Right-looking update after forward block [j0, j0+64) of a wide supernode:
@@ -466,21 +532,55 @@ __device__ void bwd_block_range(const SolveArgs& a, const T* __restrict__ L, int
   }
 }
 
-// Blocked backward solve of a wide supernode, block [jb, jb+64): in-block
-// substitution with L^T (Z already holds w - L21^T x - later blocks).
+// Blocked backward solve of a wide supernode, block [jb, jb+nb): Z holds w
+// minus the off-diagonal and later blocks' contributions; v = Linv^T w with
+// the precomputed inverse (staged in shared memory), then the block's final
+// values go to Z and to X in g order.
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_btrsv_blk(SolveArgs a, const int4* __restrict__ tasks) {
+  using F = Field<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* Ls = reinterpret_cast<T*>(smem_raw);  // 32 x 33
-  T* vb = Ls + SB * (SB + 1);              // 32 x RHS_MAX
+  T* Ls = reinterpret_cast<T*>(smem_raw);  // TB x (TB + 1): Ls[k * (TB + 1) + i] = Linv[k, i]
+  T* Ws = Ls + TB * (TB + 1);              // TB x RHS_MAX
   const int4 tk = tasks[blockIdx.x];
   const int s = tk.x, jb = tk.y;
-  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
-  const int je = min(jb + TB, ncol);
-  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
-  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  bwd_block_range<T>(a, L, nrow, Z, nullptr, reinterpret_cast<T*>(a.Xg) + a.c0, a.lperm + first, first, jb, je,
-                     je, vb, Ls);
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s];
+  const int nb = min(TB, ncol - jb);
+  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)(first + jb) * a.ld;
+  T* Xw = reinterpret_cast<T*>(a.Xg) + a.c0;
+  const int* lp = a.lperm + first + jb;
+  const T* Li = reinterpret_cast<const T*>(a.linv) + a.linv_off[s] + (long long)(jb / TB) * TB * TB;
+  for (int e = threadIdx.x; e < TB * TB; e += SOLVE_NT) {
+    const int k = e % TB, i = e / TB;  // column-major read: Linv[k, i]
+    Ls[k * (TB + 1) + i] = Li[k + (long long)i * TB];
+  }
+  for (int e = threadIdx.x; e < TB * RHS_MAX; e += SOLVE_NT) {
+    const int k = e / RHS_MAX, c = e % RHS_MAX;
+    Ws[e] = (k < nb && c < a.nrhs) ? Z[(long long)k * a.ld + c] : F::zero();
+  }
+  __syncthreads();
+  const int i = threadIdx.x % TB, cg = threadIdx.x / TB;
+  constexpr int NCG = SOLVE_NT / TB;
+  T acc[RHS_MAX / NCG];
+#pragma unroll
+  for (int m = 0; m < RHS_MAX / NCG; ++m) acc[m] = F::zero();
+  if (i < nb)
+    for (int k = i; k < nb; ++k) {
+      const T l = Ls[k * (TB + 1) + i];
+#pragma unroll
+      for (int m = 0; m < RHS_MAX / NCG; ++m) acc[m] = F::fma_(l, Ws[k * RHS_MAX + cg + NCG * m], acc[m]);
+    }
+  if (i < nb) {
+    T* xo = Xw + (long long)(first + lp[i]) * a.ld;
+#pragma unroll
+    for (int m = 0; m < RHS_MAX / NCG; ++m) {
+      const int c = cg + NCG * m;
+      if (c < a.nrhs) {
+        Z[(long long)i * a.ld + c] = acc[m];
+        xo[c] = acc[m];
+      }
+    }
+  }
 }
 
 // Right-looking backward update after block [jb, jb+64) of a wide supernode:

@@ -98,7 +98,7 @@ size_t elem_size(int dtype) {
 enum LaunchKind {
   L_CMOD, L_GETF2, L_DEEP, L_SCHUR,
   L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD,
-  L_FTRSV_BLK, L_FTRSV_UPD, L_BTRSV_BLK, L_BTRSV_UPD, L_FWD_GATHER, L_CMOD_TC, L_MAKE_G
+  L_FTRSV_BLK, L_FTRSV_UPD, L_BTRSV_BLK, L_BTRSV_UPD, L_FWD_GATHER, L_CMOD_TC, L_MAKE_G, L_DIAG_INV
 };
 struct Launch {
   int kind;
@@ -138,6 +138,8 @@ struct rslab_sym_handle {
   std::vector<int8_t> tcmaps;         // per tensor-core pair: 128 + 64 inverse scatter maps
   std::vector<long long> goff;        // G_k = L21_k D_k pool offsets ((nrow - ncol) x ncol each)
   long long g_elems = 0;
+  std::vector<long long> linv_off;    // wide supernodes: inverses of their TB x TB diagonal blocks
+  long long linv_elems = 0;
   std::vector<int> t1;
   std::vector<int2> t2;
   std::vector<int4> st4;  // blocked diagonal-solve tasks (s, j0, r0 | c0, 0)
@@ -167,6 +169,7 @@ struct rslab_sym_handle {
   int4 *d_t4tc = nullptr, *d_cpairs_tc = nullptr;
   int8_t* d_tcmaps = nullptr;
   long long* d_goff = nullptr;
+  long long* d_linv_off = nullptr;
   int* d_t1 = nullptr;
   int2* d_t2 = nullptr;
   int4* d_st4 = nullptr;
@@ -225,6 +228,7 @@ struct rslab_sym_handle {
     d_cpairs_tc = up(cpairs_tc, st);
     d_tcmaps = up(tcmaps, st);
     d_goff = up(goff, st);
+    d_linv_off = up(linv_off, st);
     d_t1 = up(t1, st);
     d_t2 = up(t2, st);
     d_st4 = up(st4, st);
@@ -356,6 +360,12 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
   for (int s = 0; s < ns; ++s) {
     H.goff[s] = H.g_elems;
     H.g_elems += (long long)(H.nrow[s] - S.sn[s].ncol) * S.sn[s].ncol;
+  }
+  H.linv_off.assign(ns, 0);
+  H.linv_elems = 0;
+  for (int s = 0; s < ns; ++s) {
+    H.linv_off[s] = H.linv_elems;
+    if (S.sn[s].ncol > SOLVE_BIG) H.linv_elems += (long long)((S.sn[s].ncol + TB - 1) / TB) * TB * TB;
   }
   // Pull lists: every off-diagonal row r of updater k (U row uoff[k] + r)
   // lands on one column g of an ancestor; list the pushes per g in the
@@ -493,6 +503,14 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
           for (int t0 = 0; t0 < S.sn[s].ncol; t0 += 32) H.t2.push_back(make_int2((int)s, t0));
       Mg.ntasks = (int)(H.t2.size() - Mg.task_off);
       if (Mg.ntasks) H.fplan.push_back(Mg);
+      // inverses of the diagonal TB-blocks of this level's wide supernodes
+      // (used by the blocked triangular solves)
+      Launch Dv{L_DIAG_INV, (long long)H.t2.size(), 0, 0};
+      for (int64_t s : lvl)
+        if (S.sn[s].ncol > SOLVE_BIG)
+          for (int j0 = 0; j0 < S.sn[s].ncol; j0 += TB) H.t2.push_back(make_int2((int)s, j0));
+      Dv.ntasks = (int)(H.t2.size() - Dv.task_off);
+      if (Dv.ntasks) H.fplan.push_back(Dv);
     }
     // Solve launches for this level.  Forward: diagonal blocks (one CTA per
     // narrow supernode; wide ones get the blocked multi-CTA solve), then the
@@ -582,6 +600,8 @@ size_t smem_deep(size_t es, int nb) { return smem_replay(es, nb) + 64; }
 size_t smem_solve(size_t es) { return ((size_t)(SOLVE_NT / 32) * 32 * RHS_MAX + SB * (SB + 1) + SB * RHS_MAX) * es; }
 size_t smem_push(size_t es) { return (size_t)(32 * 64 + 32 * RHS_MAX) * es; }
 size_t smem_dots(size_t es) { return (size_t)(32 * 33 + 32 * RHS_MAX) * es; }
+size_t smem_diag_inv(size_t es) { return (size_t)TB * (TB + 1) * 2 * es; }
+size_t smem_blk_inv(size_t es) { return (size_t)(TB * (TB + 1) + TB * RHS_MAX) * es; }
 
 // Fields whose descendant updates can run on the tf32 tensor cores.
 template <typename T> struct TensorCmod { static constexpr bool ok = false; };
@@ -604,8 +624,9 @@ struct KernelSetup {
     CK(cudaFuncSetAttribute(k_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
     CK(cudaFuncSetAttribute(k_fwd_push<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_push(es)));
     CK(cudaFuncSetAttribute(k_ftrsv_upd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_push(es)));
-    CK(cudaFuncSetAttribute(k_ftrsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
-    CK(cudaFuncSetAttribute(k_btrsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
+    CK(cudaFuncSetAttribute(k_ftrsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_blk_inv(es)));
+    CK(cudaFuncSetAttribute(k_diag_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_diag_inv(es)));
+    CK(cudaFuncSetAttribute(k_btrsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_blk_inv(es)));
     CK(cudaFuncSetAttribute(k_bwd_off<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
     CK(cudaFuncSetAttribute(k_btrsv_upd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
     done = true;
@@ -644,6 +665,7 @@ struct rslab_fac_handle {
   void* scratch = nullptr;
   long long scratch_stride = 0;
   void* gpool = nullptr;  // G_k = L21_k D_k (tensor-core cmod only)
+  void* linv = nullptr;   // inverse diagonal blocks of the wide supernodes
   // graph of the numeric factor (values read from `aval`)
   cudaGraphExec_t fgraph = nullptr;
   // solve workspace
@@ -794,6 +816,11 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         if (!use_tc) continue;
         k_make_g<T><<<L.ntasks, 256, 0, st>>>(fa, H.d_t2 + L.task_off);
         break;
+      case L_DIAG_INV:
+        k_diag_inv<T><<<L.ntasks, TB, smem_diag_inv(es), st>>>(H.d_t2 + L.task_off, H.d_sn_ncol, H.d_sn_nrow,
+                                                                 H.d_poff, (const T*)F.panel, F.status, (T*)F.linv,
+                                                                 H.d_linv_off);
+        break;
       case L_GETF2: {
         FactorArgs f2 = fa;
         f2.scratch_stride = ((long long)L.nb_slot * L.nb_slot * es + 3 * L.nb_slot * 4 + 255) / 256 * 256;
@@ -813,6 +840,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
     if (prof)
       prof->mark(st,
                  (L.kind == L_CMOD || L.kind == L_CMOD_TC || L.kind == L_MAKE_G) ? 1
+                 : L.kind == L_DIAG_INV                                        ? 4
                  : L.kind == L_GETF2                                           ? 2
                  : L.kind == L_DEEP                                            ? 3
                                                                                : 4,
@@ -926,6 +954,8 @@ SolveArgs make_sargs(rslab_fac_handle& F, int ld, int c0, int nr) {
   a.uoff = H.d_uoff;
   a.pull_ptr = H.d_pull_ptr;
   a.pull_src = H.d_pull_src;
+  a.linv = F.linv;
+  a.linv_off = H.d_linv_off;
   a.ld = ld;
   a.c0 = c0;
   a.nrhs = nr;
@@ -954,7 +984,7 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
           k_fwd_diag<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
           break;
         case L_FTRSV_BLK:
-          k_ftrsv_blk<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_st4 + L.task_off);
+          k_ftrsv_blk<T><<<L.ntasks, SOLVE_NT, smem_blk_inv(es), st>>>(sa, H.d_st4 + L.task_off);
           break;
         case L_FTRSV_UPD:
           k_ftrsv_upd<T><<<L.ntasks, SOLVE_NT, smem_push(es), st>>>(sa, H.d_st4 + L.task_off);
@@ -972,7 +1002,7 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
           k_bwd_off<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_t2 + L.task_off);
           break;
         case L_BTRSV_BLK:
-          k_btrsv_blk<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_st4 + L.task_off);
+          k_btrsv_blk<T><<<L.ntasks, SOLVE_NT, smem_blk_inv(es), st>>>(sa, H.d_st4 + L.task_off);
           break;
         case L_BTRSV_UPD:
           k_btrsv_upd<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_st4 + L.task_off);
@@ -1410,6 +1440,7 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
     const long long nbm = sym->max_nb;
     F->scratch_stride = (nbm * nbm * (long long)es + 3 * nbm * 4 + 255) / 256 * 256;
     F->scratch = F->al<unsigned char>((size_t)std::max(1, sym->max_getf2_tasks) * F->scratch_stride);
+    F->linv = F->al<unsigned char>((size_t)std::max(sym->linv_elems, 1LL) * es);
     if (F->set.on_zero_pivot == RSLAB_PIVOT_FORCE_ACCEPT) {
       F->floor_dev = F->al<double>(1);
       F->amax_dev = F->al<unsigned long long>(1);
