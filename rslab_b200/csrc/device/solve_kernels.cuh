@@ -26,6 +26,7 @@ constexpr int RHS_MAX = 16;  // right-hand sides per pass (larger counts loop)
 constexpr int SB = 32;       // diagonal-block edge of the in-CTA substitutions
 constexpr int SOLVE_BIG = 128;  // wider supernodes use the multi-CTA blocked diagonal solves
 constexpr int TB = 64;          // block edge of the multi-CTA diagonal solves
+constexpr int BWD_ROWS = 1024;  // off-diagonal rows per backward-dot task
 
 struct SolveArgs {
   const int* sn_first;
@@ -53,6 +54,7 @@ struct SolveArgs {
   const int* pull_src;    // U row of each push, update-list order per g
   const void* linv;       // inverses of the TB x TB diagonal blocks of wide supernodes
   const long long* linv_off;
+  void* Wp;               // slots x 32 x ld partial sums of the split backward dots
   int ld;     // row stride (total rhs count)
   int c0;     // first rhs column of this pass
   int nrhs;   // rhs columns in this pass (<= RHS_MAX)
@@ -315,39 +317,80 @@ __device__ void dot_cols_tile(const T* __restrict__ L, int nrow, int p0, int nco
   }
 }
 
-// Backward off-diagonal dots of supernode s, pivot columns [c0, c0+32):
-// sum_{r >= ncol} L[r, p] x[g_r] -> Wb (narrow supernodes) or subtracted from
-// Z directly (wide supernodes, solved by the blocked kernels).
+// Backward off-diagonal dots of supernode s, pivot columns [c0, c0+32),
+// off-diagonal rows [ncol + r0, ncol + r0 + BWD_ROWS): sum_r L[r, p] x[g_r].
+// Task (s, c0, r0, slot): slot < 0 (the only row chunk) writes the result —
+// to Wb for narrow supernodes, subtracted from Z for wide ones (solved by
+// the blocked kernels); otherwise the partial sum goes to slot `slot`.
 template <typename T>
-__global__ void __launch_bounds__(SOLVE_NT) k_bwd_off(SolveArgs a, const int2* __restrict__ tasks) {
+__global__ void __launch_bounds__(SOLVE_NT) k_bwd_off(SolveArgs a, const int4* __restrict__ tasks) {
   using F = Field<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* Ls = reinterpret_cast<T*>(smem_raw);  // 32 x 33
   T* Vs = Ls + 32 * 33;                    // 32 x RHS_MAX
-  const int2 tk = tasks[blockIdx.x];
-  const int s = tk.x, c0 = tk.y;
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, c0 = tk.y, r0 = tk.z, slot = tk.w;
   const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
   const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
   const int* rss = a.rs + a.sn_rsoff[s];
   const T* X = reinterpret_cast<const T*>(a.Xg) + a.c0;
-  T* Wb = reinterpret_cast<T*>(a.Wb) + a.c0 + (long long)first * a.ld;
-  T* Zs = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
   const int cols_here = min(32, ncol - c0);
+  const int rb = ncol + r0, re = min(nrow, rb + BWD_ROWS);
   T acc[RHS_MAX / 8];
-  dot_cols_tile<T, true>(L, nrow, c0, cols_here, ncol, nrow, X, rss, a.ld, a.nrhs, acc, Ls, Vs);
+  dot_cols_tile<T, true>(L, nrow, c0, cols_here, rb, re, X, rss, a.ld, a.nrhs, acc, Ls, Vs);
   const int pc = threadIdx.x & 31, cg = threadIdx.x >> 5;
-  if (pc < cols_here) {
-    const int p = c0 + pc;
+  if (pc >= cols_here) return;
+  const int p = c0 + pc;
+  if (slot >= 0) {
+    T* part = reinterpret_cast<T*>(a.Wp) + (long long)slot * 32 * a.ld;
 #pragma unroll
     for (int q = 0; q < RHS_MAX / 8; ++q) {
       const int c = cg + 8 * q;
-      if (c >= a.nrhs) continue;
-      if (ncol > SOLVE_BIG) {
-        T* z = Zs + (long long)p * a.ld + c;
-        *z = F::sub(*z, acc[q]);
-      } else {
-        Wb[(long long)p * a.ld + c] = acc[q];
-      }
+      if (c < a.nrhs) part[pc * a.ld + c] = acc[q];
+    }
+    return;
+  }
+  T* Wb = reinterpret_cast<T*>(a.Wb) + a.c0 + (long long)first * a.ld;
+  T* Zs = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
+#pragma unroll
+  for (int q = 0; q < RHS_MAX / 8; ++q) {
+    const int c = cg + 8 * q;
+    if (c >= a.nrhs) continue;
+    if (ncol > SOLVE_BIG) {
+      T* z = Zs + (long long)p * a.ld + c;
+      *z = F::sub(*z, acc[q]);
+    } else {
+      Wb[(long long)p * a.ld + c] = acc[q];
+    }
+  }
+}
+
+// Reduce the row-chunk partial sums of one (s, c0) in chunk order and write
+// them like the single-chunk case.  Task (s, c0, slot0, nchunks).
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_NT) k_bwd_off_reduce(SolveArgs a, const int4* __restrict__ tasks) {
+  using F = Field<T>;
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, c0 = tk.y, slot0 = tk.z, nch = tk.w;
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s];
+  const int cols_here = min(32, ncol - c0);
+  const int pc = threadIdx.x & 31, cg = threadIdx.x >> 5;
+  if (pc >= cols_here) return;
+  const int p = c0 + pc;
+  const T* part = reinterpret_cast<const T*>(a.Wp) + (long long)slot0 * 32 * a.ld;
+  T* Wb = reinterpret_cast<T*>(a.Wb) + a.c0 + (long long)first * a.ld;
+  T* Zs = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
+#pragma unroll
+  for (int q = 0; q < RHS_MAX / 8; ++q) {
+    const int c = cg + 8 * q;
+    if (c >= a.nrhs) continue;
+    T v = part[pc * a.ld + c];
+    for (int k = 1; k < nch; ++k) v = F::add(v, part[(long long)k * 32 * a.ld + pc * a.ld + c]);
+    if (ncol > SOLVE_BIG) {
+      T* z = Zs + (long long)p * a.ld + c;
+      *z = F::sub(*z, v);
+    } else {
+      Wb[(long long)p * a.ld + c] = v;
     }
   }
 }

@@ -98,7 +98,8 @@ size_t elem_size(int dtype) {
 enum LaunchKind {
   L_CMOD, L_GETF2, L_DEEP, L_SCHUR,
   L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD,
-  L_FTRSV_BLK, L_FTRSV_UPD, L_BTRSV_BLK, L_BTRSV_UPD, L_FWD_GATHER, L_CMOD_TC, L_MAKE_G, L_DIAG_INV
+  L_FTRSV_BLK, L_FTRSV_UPD, L_BTRSV_BLK, L_BTRSV_UPD, L_FWD_GATHER, L_CMOD_TC, L_MAKE_G, L_DIAG_INV,
+  L_BWD_OFF_RED
 };
 struct Launch {
   int kind;
@@ -138,6 +139,7 @@ struct rslab_sym_handle {
   std::vector<int8_t> tcmaps;         // per tensor-core pair: 128 + 64 inverse scatter maps
   std::vector<long long> goff;        // G_k = L21_k D_k pool offsets ((nrow - ncol) x ncol each)
   long long g_elems = 0;
+  int bwd_slots = 0;                  // partial-sum slots of the split backward dots (max per level)
   std::vector<long long> linv_off;    // wide supernodes: inverses of their TB x TB diagonal blocks
   long long linv_elems = 0;
   std::vector<int> t1;
@@ -552,12 +554,34 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       if (Pu.ntasks) H.fwdplan.push_back(Pu);
 
       std::vector<Launch> bw;
-      Launch Bo{L_BWD_OFF, (long long)H.t2.size(), 0, 0};
-      for (int64_t s : lvl)
-        if (H.nrow[s] > S.sn[s].ncol)
-          for (int c0 = 0; c0 < S.sn[s].ncol; c0 += 32) H.t2.push_back(make_int2((int)s, c0));
-      Bo.ntasks = (int)(H.t2.size() - Bo.task_off);
+      // Off-diagonal dots: tasks (s, c0, row chunk, slot) over chunks of
+      // BWD_ROWS off-diagonal rows; a column chunk with several row chunks
+      // writes partial sums to slots, reduced in row-chunk order next.
+      Launch Bo{L_BWD_OFF, (long long)H.st4.size(), 0, 0};
+      Launch Br{L_BWD_OFF_RED, (long long)H.st4.size(), 0, 0};
+      std::vector<int4> red;
+      int slot = 0;
+      for (int64_t s : lvl) {
+        const int off = H.nrow[s] - (int)S.sn[s].ncol;
+        if (off <= 0) continue;
+        const int nch = (off + BWD_ROWS - 1) / BWD_ROWS;
+        for (int c0 = 0; c0 < S.sn[s].ncol; c0 += 32) {
+          if (nch == 1) {
+            H.st4.push_back(make_int4((int)s, c0, 0, -1));
+          } else {
+            red.push_back(make_int4((int)s, c0, slot, nch));
+            for (int q = 0; q < nch; ++q) H.st4.push_back(make_int4((int)s, c0, q * BWD_ROWS, slot + q));
+            slot += nch;
+          }
+        }
+      }
+      Bo.ntasks = (int)(H.st4.size() - Bo.task_off);
       if (Bo.ntasks) bw.push_back(Bo);
+      H.bwd_slots = std::max(H.bwd_slots, slot);
+      Br.task_off = (long long)H.st4.size();
+      H.st4.insert(H.st4.end(), red.begin(), red.end());
+      Br.ntasks = (int)red.size();
+      if (Br.ntasks) bw.push_back(Br);
       Launch Bd{L_BWD, (long long)H.t1.size(), 0, 0};
       for (int64_t s : lvl)
         if (S.sn[s].ncol <= SOLVE_BIG) H.t1.push_back((int)s);
@@ -671,6 +695,7 @@ struct rslab_fac_handle {
   // solve workspace
   int ws_nrhs = 0;
   void *Yg = nullptr, *Ze = nullptr, *Xg = nullptr, *Ub = nullptr, *Wb = nullptr, *bdev = nullptr, *xdev = nullptr;
+  void* Wp = nullptr;  // partial sums of the split backward dots
   std::vector<std::unique_ptr<void, DFree>> ws;
   cudaGraphExec_t sgraph = nullptr;
   int sgraph_nrhs = -1;
@@ -917,6 +942,7 @@ void ensure_ws(rslab_fac_handle& F, int nrhs) {
   F.Xg = a(m * es);
   F.Ub = a((size_t)std::max(F.sym->urows, 1LL) * nrhs * es);
   F.Wb = a(m * es);
+  F.Wp = a((size_t)std::max(F.sym->bwd_slots, 1) * 32 * nrhs * es);
   F.bdev = a(m * es);
   F.xdev = a(m * es);
   F.ws_nrhs = nrhs;
@@ -956,6 +982,7 @@ SolveArgs make_sargs(rslab_fac_handle& F, int ld, int c0, int nr) {
   a.pull_src = H.d_pull_src;
   a.linv = F.linv;
   a.linv_off = H.d_linv_off;
+  a.Wp = F.Wp;
   a.ld = ld;
   a.c0 = c0;
   a.nrhs = nr;
@@ -999,7 +1026,10 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
     for (const Launch& L : H.bwdplan) {
       switch (L.kind) {
         case L_BWD_OFF:
-          k_bwd_off<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_t2 + L.task_off);
+          k_bwd_off<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_st4 + L.task_off);
+          break;
+        case L_BWD_OFF_RED:
+          k_bwd_off_reduce<T><<<L.ntasks, SOLVE_NT, 0, st>>>(sa, H.d_st4 + L.task_off);
           break;
         case L_BTRSV_BLK:
           k_btrsv_blk<T><<<L.ntasks, SOLVE_NT, smem_blk_inv(es), st>>>(sa, H.d_st4 + L.task_off);
@@ -1010,7 +1040,7 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
         default:
           k_bwd<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_t1 + L.task_off);
       }
-      if (prof) prof->mark(st, L.kind == L_BWD_OFF ? 4 : 5, L.ntasks, L.kind);
+      if (prof) prof->mark(st, (L.kind == L_BWD_OFF || L.kind == L_BWD_OFF_RED) ? 4 : 5, L.ntasks, L.kind);
     }
   }
   k_perm_out<T><<<grid1((long long)n * nrhs), 256, 0, st>>>(n, nrhs, H.d_perm, F.scale, (const T*)F.Xg, x);
