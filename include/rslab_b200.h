@@ -78,7 +78,7 @@ typedef struct {
   int64_t relax_max_width;     /* 256 */
   int64_t relax_max_extra_rows;/* 64 */
   int32_t hybrid_liu;          /* child reordering (scheduling only) */
-  int64_t panel_nb;            /* BK panel width, 64 (128 when ncol >= 512) */
+  int64_t panel_nb;            /* BK panel width, 64 (128 when ncol >= 512); clamped to [8, 128] */
   const int64_t* given_perm;   /* RSLAB_ORDER_GIVEN: new-to-old permutation */
 } rslab_analyze_settings;
 

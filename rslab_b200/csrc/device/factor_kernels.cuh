@@ -613,9 +613,11 @@ __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int n
   constexpr int NR = R / NW;
   for (int rs0 = r_begin; rs0 < r_end; rs0 += R) {
     const int rows = min(R, r_end - rs0);
-    for (int e = threadIdx.x; e < R * pw; e += NT) {
+    // fixed trip count (panel blocks are at most 128 wide): all loads in flight
+#pragma unroll 16
+    for (int e = threadIdx.x; e < R * 128; e += NT) {
       const int c = e / R, r = e % R;
-      if (r < rows) X[c * LDX + r] = panel[(rs0 + r) + (long long)(kb + c) * nrow];
+      if (r < rows && c < pw) X[c * LDX + r] = panel[(rs0 + r) + (long long)(kb + c) * nrow];
     }
     __syncthreads();
     // rows warp + NW i; rows past `rows` replay zeros and are not stored
@@ -707,8 +709,12 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   constexpr int NW = NT / 32;
-  for (int j = warp; j < pw; j += NW)
-    for (int i = j + lane; i < pw; i += 32) A[pk(i, j, pw)] = panel[(kb + i) + (long long)(kb + j) * nrow];
+  // flat fixed-count load of the lower block (at most 128 x 128): loads in flight
+#pragma unroll 8
+  for (int e = tid; e < 128 * 128; e += NT) {
+    const int i = e & 127, j = e >> 7;
+    if (i < pw && j <= i) A[pk(i, j, pw)] = panel[(kb + i) + (long long)(kb + j) * nrow];
+  }
   if (kb == 0)
     for (int p = tid; p < ncol; p += NT) lpermG[p] = p;
   for (int e = tid; e < pw; e += NT) {

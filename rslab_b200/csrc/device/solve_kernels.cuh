@@ -116,6 +116,7 @@ __device__ __forceinline__ T shfl_T(T v, int src) {
 // nb x nb diagonal block), zero elsewhere.  Loads coalesced along i.
 template <typename T>
 __device__ __forceinline__ void stage_diag_block(const T* __restrict__ L, int nrow, int j0, int nb, T* Ls) {
+#pragma unroll
   for (int e = threadIdx.x; e < SB * SB; e += SOLVE_NT) {
     const int i = e & (SB - 1), j = e / SB;
     Ls[i * (SB + 1) + j] = (i < nb && j < i) ? L[(j0 + i) + (long long)(j0 + j) * nrow] : Field<T>::zero();
@@ -230,13 +231,15 @@ __device__ void rows_dot_z(const T* __restrict__ L, int nrow, int r0, int r_end,
   for (int m = 0; m < RHS_MAX / 4; ++m) acc[m] = F::zero();
   for (int qc = q0; qc < q1; qc += 32) {
     const int nq = min(32, q1 - qc);
+#pragma unroll
     for (int e = tid; e < 64 * 32; e += SOLVE_NT) {
       const int r = e & 63, q = e >> 6;
       Ls[q * 64 + r] = (q < nq && r0 + r < r_end) ? L[(r0 + r) + (long long)(qc + q) * nrow] : F::zero();
     }
-    for (int e = tid; e < 32 * nrhs; e += SOLVE_NT) {
-      const int q = e / nrhs, c = e % nrhs;
-      Zs[q * RHS_MAX + c] = q < nq ? Z[(long long)(qc + q) * ld + c] : F::zero();
+#pragma unroll
+    for (int e = tid; e < 32 * RHS_MAX; e += SOLVE_NT) {
+      const int q = e / RHS_MAX, c = e % RHS_MAX;
+      Zs[e] = (q < nq && c < nrhs) ? Z[(long long)(qc + q) * ld + c] : F::zero();
     }
     __syncthreads();
     for (int q = 0; q < nq; ++q) {
@@ -291,18 +294,20 @@ __device__ void dot_cols_tile(const T* __restrict__ L, int nrow, int p0, int nco
   for (int q = 0; q < NRC; ++q) acc[q] = F::zero();
   for (int r0 = r_begin; r0 < r_end; r0 += 32) {
     const int rows = min(32, r_end - r0);
+#pragma unroll
     for (int e = tid; e < 32 * 32; e += SOLVE_NT) {
       const int c = e >> 5, r = e & 31;  // column c, row r: coalesced along r
       Ls[r * 33 + c] = (r < rows && c < ncols) ? L[(r0 + r) + (long long)(p0 + c) * nrow] : F::zero();
     }
-    for (int e = tid; e < 32 * nrhs; e += SOLVE_NT) {
-      const int r = e / nrhs, c = e % nrhs;
+#pragma unroll
+    for (int e = tid; e < 32 * RHS_MAX; e += SOLVE_NT) {
+      const int r = e / RHS_MAX, c = e % RHS_MAX;
       T v = F::zero();
-      if (r < rows) {
+      if (r < rows && c < nrhs) {
         const long long row = GATHER ? (long long)rss[r0 + r] : (long long)(r0 + r);
         v = V[row * ld + c];
       }
-      Vs[r * RHS_MAX + c] = v;
+      Vs[e] = v;
     }
     __syncthreads();
     for (int r = 0; r < rows; ++r) {
@@ -444,13 +449,20 @@ template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_ftrsv_blk(SolveArgs a, const int4* __restrict__ tasks) {
   using F = Field<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* Ys = reinterpret_cast<T*>(smem_raw);  // TB x RHS_MAX
+  T* Ls = reinterpret_cast<T*>(smem_raw);  // TB x (TB + 1): Ls[k * (TB + 1) + i] = Linv[i, k]
+  T* Ys = Ls + TB * (TB + 1);              // TB x RHS_MAX
   const int4 tk = tasks[blockIdx.x];
   const int s = tk.x, j0 = tk.y;
   const int first = a.sn_first[s], ncol = a.sn_ncol[s];
   const int nb = min(TB, ncol - j0);
   T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)(first + j0) * a.ld;
   const T* Li = reinterpret_cast<const T*>(a.linv) + a.linv_off[s] + (long long)(j0 / TB) * TB * TB;
+#pragma unroll
+  for (int e = threadIdx.x; e < TB * TB; e += SOLVE_NT) {
+    const int i = e % TB, k = e / TB;  // column-major read: Linv[i, k]
+    Ls[k * (TB + 1) + i] = Li[i + (long long)k * TB];
+  }
+#pragma unroll
   for (int e = threadIdx.x; e < TB * RHS_MAX; e += SOLVE_NT) {
     const int k = e / RHS_MAX, c = e % RHS_MAX;
     Ys[e] = (k < nb && c < a.nrhs) ? Z[(long long)k * a.ld + c] : F::zero();
@@ -463,7 +475,7 @@ __global__ void __launch_bounds__(SOLVE_NT) k_ftrsv_blk(SolveArgs a, const int4*
   for (int m = 0; m < RHS_MAX / NCG; ++m) acc[m] = F::zero();
   if (i < nb)
     for (int k = 0; k <= i; ++k) {
-      const T l = Li[i + (long long)k * TB];
+      const T l = Ls[k * (TB + 1) + i];
 #pragma unroll
       for (int m = 0; m < RHS_MAX / NCG; ++m) acc[m] = F::fma_(l, Ys[k * RHS_MAX + cg + NCG * m], acc[m]);
     }
@@ -593,10 +605,12 @@ __global__ void __launch_bounds__(SOLVE_NT) k_btrsv_blk(SolveArgs a, const int4*
   T* Xw = reinterpret_cast<T*>(a.Xg) + a.c0;
   const int* lp = a.lperm + first + jb;
   const T* Li = reinterpret_cast<const T*>(a.linv) + a.linv_off[s] + (long long)(jb / TB) * TB * TB;
+#pragma unroll
   for (int e = threadIdx.x; e < TB * TB; e += SOLVE_NT) {
     const int k = e % TB, i = e / TB;  // column-major read: Linv[k, i]
     Ls[k * (TB + 1) + i] = Li[k + (long long)i * TB];
   }
+#pragma unroll
   for (int e = threadIdx.x; e < TB * RHS_MAX; e += SOLVE_NT) {
     const int k = e / RHS_MAX, c = e % RHS_MAX;
     Ws[e] = (k < nb && c < a.nrhs) ? Z[(long long)k * a.ld + c] : F::zero();

@@ -1290,7 +1290,7 @@ int rslab_analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, con
     o.given_perm = st.given_perm;
     auto H = std::make_unique<rslab_sym_handle>();
     H->settings = st;
-    H->panel_nb = (int)std::max<int64_t>(st.panel_nb, 8);
+    H->panel_nb = (int)std::min<int64_t>(std::max<int64_t>(st.panel_nb, 8), 128);  // panel kernels hold <= 128 columns
     H->S = rslab::analyze(n, col_ptr, row_idx, o);
     H->seg_begin = {0, (long long)n};
     H->nnz_begin = {0, (long long)col_ptr[n]};
@@ -1346,7 +1346,7 @@ int rslab_analyze_batch(int64_t count, const int64_t* n, const int64_t* const* c
     }
     auto H = std::make_unique<rslab_sym_handle>();
     H->settings = st;
-    H->panel_nb = (int)std::max<int64_t>(st.panel_nb, 8);
+    H->panel_nb = (int)std::min<int64_t>(std::max<int64_t>(st.panel_nb, 8), 128);  // panel kernels hold <= 128 columns
     H->S = rslab::merge_independent(parts);
     H->seg_begin = seg;
     H->nnz_begin = nz;
