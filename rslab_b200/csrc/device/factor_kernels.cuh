@@ -691,8 +691,6 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
   unsigned char* sc = reinterpret_cast<unsigned char*>(fa.scratch) + (long long)slot * fa.scratch_stride;
   T* snap = reinterpret_cast<T*>(sc);                      // nb x nb
   int* swaps = reinterpret_cast<int*>(snap + (long long)nb * nb);  // nb
-  int* swp_p = swaps + nb;                                  // nb (row pairs for left swaps)
-  int* swp_q = swp_p + nb;
 
   T* A = reinterpret_cast<T*>(smem_raw);              // packed lower pw x pw
   const int npk = pw * (pw + 1) / 2;
@@ -705,6 +703,9 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
   int* red_i = reinterpret_cast<int*>(red_v + 32);
   int* ctl = red_i + 32;  // [0] kstep [1] kp [2] nswaps [3] error
   int* lp_s = ctl + 16;   // the block's slice of lperm
+  int* swp_p = lp_s + nb; // swap log of this block (row pairs for the left segments)
+  int* swp_q = swp_p + nb;
+  int* supp = swp_q + nb; // rows moved by the composed permutation
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -938,8 +939,9 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
       panel[(kb + i) + (long long)(kb + j) * nrow] = (two && i == j + 1) ? F::zero() : A[pk(i, j, pw)];
   }
   // Left row segments of the interchanges (columns [0, kb), rows of this
-  // block): the swap sequence composes to one row permutation of the block,
-  // applied as a coalesced gather per column (same final values).
+  // block): the swap sequence composes to one row permutation of the block;
+  // only the rows it moves are copied, in column chunks whose loads are all
+  // in flight before the barrier that precedes the stores (same final values).
   const int nsw = ctl[2];
   if (nsw > 0 && kb > 0) {
     int* src_row = reinterpret_cast<int*>(l1);  // pw ints (l1/l2 are free now)
@@ -952,17 +954,38 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
         src_row[p] = src_row[q];
         src_row[q] = x;
       }
+      int m = 0;
+      for (int r = 0; r < pw; ++r)
+        if (src_row[r] != r) supp[m++] = r;
+      ctl[1] = m;
     }
     __syncthreads();
-    const int cols_per = NT / pw > 0 ? NT / pw : 1;
-    for (int j0 = 0; j0 < kb; j0 += cols_per) {
-      const int j = j0 + tid / pw, r = tid % pw;
-      T v = F::zero();
-      const bool act = tid < cols_per * pw && j < kb;
-      if (act) v = panel[(kb + src_row[r]) + (long long)j * nrow];
-      __syncthreads();
-      if (act) panel[(kb + r) + (long long)j * nrow] = v;
-      __syncthreads();
+    const int ns = ctl[1];
+    if (ns > 0) {
+      constexpr int PER = 8;  // elements per thread per chunk
+      const int cols = max(1, (NT * PER) / ns);
+      for (int j0 = 0; j0 < kb; j0 += cols) {
+        const int jn = min(cols, kb - j0);
+        T v[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+          const int idx = tid + u * NT;
+          if (idx < ns * jn) {
+            const int r = supp[idx % ns], j = j0 + idx / ns;
+            v[u] = panel[(kb + src_row[r]) + (long long)j * nrow];
+          }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+          const int idx = tid + u * NT;
+          if (idx < ns * jn) {
+            const int r = supp[idx % ns], j = j0 + idx / ns;
+            panel[(kb + r) + (long long)j * nrow] = v[u];
+          }
+        }
+        __syncthreads();
+      }
     }
   }
   // kind/d written by tid 0 are read by the replay below.
