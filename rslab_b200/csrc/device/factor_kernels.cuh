@@ -749,7 +749,12 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
     if (warp == 0) {
       double v = -1.0;
       int idx = INT_MAX;
-      for (int i = k + 1 + lane; i < pw; i += 32) argmax_combine(v, idx, F::mag2(A[pk(i, k, pw)]), i);
+      // blocks are at most 128 wide: four predicated lanes-strided slots
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int i = k + 1 + lane + 32 * t;
+        if (i < pw) argmax_combine(v, idx, F::mag2(A[pk(i, k, pw)]), i);
+      }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
@@ -831,12 +836,16 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
           }
           if (!err) {
             const T dinv = F::recip(dk);
-            for (int jj = k + 1 + lane; jj < pw; jj += 32) {
-              const T a = A[pk(jj, k, pw)];
-              const T w = F::mul(a, dinv);
-              u1[jj] = a;
-              l1[jj] = w;
-              snap[k * nb + jj] = w;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+              const int jj = k + 1 + lane + 32 * t;
+              if (jj < pw) {
+                const T a = A[pk(jj, k, pw)];
+                const T w = F::mul(a, dinv);
+                u1[jj] = a;
+                l1[jj] = w;
+                snap[k * nb + jj] = w;
+              }
             }
             if (lane == 0) {
               dG[k] = dk;
@@ -899,18 +908,28 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
       for (int jj = k + 1 + warp; jj < pw; jj += NW) {
         const T w = l1[jj];
         if (F::is_zero(w)) continue;
-        for (int i = jj + lane; i < pw; i += 32) A[pk(i, jj, pw)] = F::sub(A[pk(i, jj, pw)], F::mul(u1[i], w));
+        const int base = pk(jj, jj, pw) - jj;  // packed index of (i, jj) = base + i
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int i = jj + lane + 32 * t;
+          if (i < pw) A[base + i] = F::sub(A[base + i], F::mul(u1[i], w));
+        }
       }
       const T dinv = *dinv_s;
       for (int i = k + 1 + tid; i < pw; i += NT) A[pk(i, k, pw)] = F::mul(u1[i], dinv);
     } else {
       for (int jj = k + 2 + warp; jj < pw; jj += NW) {
         const T a1 = l1[jj], a2 = l2[jj];
-        for (int i = jj + lane; i < pw; i += 32) {
-          T x = A[pk(i, jj, pw)];
-          x = F::sub(x, F::mul(u1[i], a1));
-          x = F::sub(x, F::mul(u2[i], a2));
-          A[pk(i, jj, pw)] = x;
+        const int base = pk(jj, jj, pw) - jj;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int i = jj + lane + 32 * t;
+          if (i < pw) {
+            T x = A[base + i];
+            x = F::sub(x, F::mul(u1[i], a1));
+            x = F::sub(x, F::mul(u2[i], a2));
+            A[base + i] = x;
+          }
         }
       }
       for (int i = k + 2 + tid; i < pw; i += NT) {
