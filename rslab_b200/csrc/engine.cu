@@ -627,6 +627,10 @@ size_t smem_dots(size_t es) { return (size_t)(32 * 33 + 32 * RHS_MAX) * es; }
 size_t smem_diag_inv(size_t es) { return (size_t)TB * (TB + 1) * 2 * es; }
 size_t smem_blk_inv(size_t es) { return (size_t)(TB * (TB + 1) + TB * RHS_MAX) * es; }
 
+// Threads of the BK panel kernel: its per-step trailing update is
+// latency-bound, so 16 warps hide more of it than 8.
+constexpr int GETF2_NT = 512;
+
 // Fields whose descendant updates can run on the tf32 tensor cores.
 template <typename T> struct TensorCmod { static constexpr bool ok = false; };
 template <> struct TensorCmod<float> { static constexpr bool ok = true; };
@@ -642,7 +646,8 @@ struct KernelSetup {
       CK(cudaFuncSetAttribute(k_cmod_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_tc_bytes()));
     CK(cudaFuncSetAttribute(k_cmod<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod(es)));
     CK(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
-    CK(cudaFuncSetAttribute(k_getf2<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_getf2(es, 128)));
+    CK(cudaFuncSetAttribute(k_getf2<T, GETF2_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)smem_getf2(es, 128)));
     CK(cudaFuncSetAttribute(k_deep<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep(es, 128)));
     CK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
     CK(cudaFuncSetAttribute(k_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
@@ -849,7 +854,8 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
       case L_GETF2: {
         FactorArgs f2 = fa;
         f2.scratch_stride = ((long long)L.nb_slot * L.nb_slot * es + 3 * L.nb_slot * 4 + 255) / 256 * 256;
-        k_getf2<T, 256><<<L.ntasks, 256, smem_getf2(es, L.nb_slot), st>>>(f2, H.d_t4 + L.task_off, nb_small, nb_big);
+        k_getf2<T, GETF2_NT><<<L.ntasks, GETF2_NT, smem_getf2(es, L.nb_slot), st>>>(f2, H.d_t4 + L.task_off,
+                                                                                  nb_small, nb_big);
         break;
       }
       case L_DEEP: {
