@@ -116,15 +116,34 @@ __global__ void __launch_bounds__(256) k_make_g(FactorArgs fa, const int2* __res
   }
 }
 
+// The producer / MMA pipeline of one 128 x 64 target tile, generic over the
+// operand source: `Src` enumerates the (A, B) K-ranges that accumulate into
+// the tile (npairs(), ncols(u)) and opens them (open(Cur&, u, row, col)):
+// pointers to the A' source row of tile row `row` and to the B' source row of
+// tile column `col` (or -1 when no source row lands there), with their column
+// strides.  B' is read from G (plain loads) or formed as L D on the fly
+// (Src::kBonfly).  The tile is panel rows [rbase + r0, +128) x columns
+// [cbase + c0, +64) of supernode s, rows_here x cols_here of them real;
+// P -= U is applied on rows >= columns.
 template <typename T>
-__global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4* __restrict__ tasks,
-                                                      const int4* __restrict__ pairs,
-                                                      const int8_t* __restrict__ maps) {
+struct TcCur {
+  int u, t0, nck, i, j;
+  long long lda, ldb;
+  const T* Ar;  // A' source row (column stride lda)
+  const T* Br;  // B' source row (column stride ldb)
+  const T* dk;  // D of the B' source (on-the-fly G only)
+  const T* dsk;
+  const unsigned char* kk;
+};
+
+template <typename T, typename Src>
+__device__ __forceinline__ void tc_tile_pipeline(const FactorArgs& fa, const Src& src, int s, int rbase, int cbase,
+                                                 int r0, int c0, int rows_here, int cols_here,
+                                                 unsigned char* smem_raw) {
   using F = Field<T>;
   using Sh = TcShape<T>;
+  using Cur = TcCur<T>;
   constexpr int NC = Sh::n / 4;  // accumulator columns per producer thread
-  if (fa.status[0] != 0) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];  // re-aligned to 1024 below
   const uint32_t sraw = smem_u32(smem_raw);
   unsigned char* sm = smem_raw + (((sraw + 1023u) & ~1023u) - sraw);
   uint64_t* full = reinterpret_cast<uint64_t*>(sm + TC_NS * TC_STAGE);  // TC_NS
@@ -133,9 +152,7 @@ __global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4*
   uint64_t* pbar = wbar + 2;                                            // 2: window promoted
   uint32_t* tslot = reinterpret_cast<uint32_t*>(pbar + 2);
 
-  const int4 tk = tasks[blockIdx.x];
-  const int s = tk.x, r0 = (tk.y >> 16) * TC_M, c0 = (tk.y & 0xffff) * TC_N;
-  const int pb = tk.z, pe = tk.w;
+  const int pb = 0, pe = src.npairs();
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
     for (int i = 0; i < TC_NS; ++i) {
@@ -167,7 +184,7 @@ __global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4*
       const uint32_t sbase = smem_u32(sm);
       int c = 0;
       for (int u = pb; u < pe && ok; ++u) {
-        const int nck = fa.sn_ncol[pairs[u].x];
+        const int nck = src.ncols(u);
         for (int t0 = 0; t0 < nck; t0 += Sh::kc, ++c) {
           const int st = c % TC_NS, w = c / TC_WIN;
           if (c % TC_WIN == 0 && w >= 2 && !mbar_wait_bounded(&pbar[w & 1], (uint32_t)(((w - 2) >> 1) & 1))) {
@@ -224,8 +241,6 @@ __global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4*
     constexpr int NA = Field<T>::complex ? 4 : 8;  // A columns per thread
     constexpr int NB = Field<T>::complex ? 2 : 4;  // B columns per thread
     const int ta = NA * ga, tb = NB * gb;          // column offsets inside the chunk
-    const T* pall = reinterpret_cast<const T*>(fa.panel);
-    const T* gall = reinterpret_cast<const T*>(fa.gpool);
     auto promote = [&](int w) {
       if (!mbar_wait_bounded(&wbar[w & 1], (uint32_t)((w >> 1) & 1))) {
         ok = false;
@@ -239,37 +254,28 @@ __global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4*
       tc_fence_before();
       mbar_arrive(&pbar[w & 1]);
     };
-    // Chunk cursor: pair u, updater columns [t0, t0 + kc); the loads of the
+    // Chunk cursor: pair u, source columns [t0, t0 + kc); the loads of the
     // next chunk are issued before the current one is stored, so their
     // latency overlaps the stage wait, the split and the stores.
-    struct Cur {
-      int u, t0, nck, nrk, ldg, i, j;
-      const T* Ar;  // A' source row (column stride nrk)
-      const T* Br;  // B' source row of G (column stride ldg)
-    };
     auto open = [&](Cur& x, int u) {
-      const int4 pr = pairs[u];
-      const int k = pr.x, a = pr.y, q0 = pr.z;
+      src.open(x, u, row, ub);
       x.u = u;
       x.t0 = 0;
-      x.nck = fa.sn_ncol[k];
-      x.nrk = fa.sn_nrow[k];
-      x.ldg = x.nrk - x.nck;
-      x.i = maps[(long long)u * TC_MAP + row];
-      x.j = maps[(long long)u * TC_MAP + TC_M + ub];
-      x.Ar = pall + fa.sn_poff[k] + x.nck + a + x.i;
-      x.Br = gall + fa.goff[k] + q0 + x.j;
+      x.nck = src.ncols(u);
     };
     auto load = [&](const Cur& x, T (&va)[NA], T (&vb)[NB]) {
 #pragma unroll
       for (int jj = 0; jj < NA; ++jj) {
         const int t = x.t0 + ta + jj;
-        va[jj] = (x.i >= 0 && t < x.nck) ? x.Ar[(long long)t * x.nrk] : F::zero();
+        va[jj] = (x.i >= 0 && t < x.nck) ? x.Ar[(long long)t * x.lda] : F::zero();
       }
 #pragma unroll
       for (int jj = 0; jj < NB; ++jj) {
         const int t = x.t0 + tb + jj;
-        vb[jj] = (x.j >= 0 && t < x.nck) ? x.Br[(long long)t * x.ldg] : F::zero();
+        if constexpr (Src::kBonfly)
+          vb[jj] = (x.j >= 0 && t < x.nck) ? ld_G(x.Br, x.ldb, 0, t, x.dk, x.dsk, x.kk) : F::zero();
+        else
+          vb[jj] = (x.j >= 0 && t < x.nck) ? x.Br[(long long)t * x.ldb] : F::zero();
       }
     };
     int c = 0, pw = 0;
@@ -341,18 +347,17 @@ __global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4*
       // 32 q + lane and accumulator columns [cg NC, cg NC + NC): for c32
       // columns 0-63 are the real parts and 64-127 the imaginary parts of
       // tile columns 0-63; each thread updates its own component.
-      const int ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
-      const int rows_here = min(TC_M, nrow - r0), cols_here = min(TC_N, ncol - c0);
+      const int nrow = fa.sn_nrow[s];
       const int trow = 32 * q + lane;
       if (trow < rows_here) {
-        const int gr = r0 + trow;
+        const int gr = rbase + r0 + trow;
         float* pf = reinterpret_cast<float*>(reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s]);
 #pragma unroll
         for (int jj = 0; jj < NC; ++jj) {
           const int colj = cg * NC + jj;
           const int col = Field<T>::complex ? (colj & (TC_N - 1)) : colj;
           const int comp = Field<T>::complex ? (colj >> 6) : 0;
-          const int gc = c0 + col;
+          const int gc = cbase + c0 + col;
           if (col < cols_here && gr >= gc) {
             const long long e = gr + (long long)gc * nrow;
             float* p = Field<T>::complex ? pf + 2 * e + comp : pf + e;
@@ -369,6 +374,98 @@ __global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4*
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, TC_TMEM_COLS);
+}
+
+
+// cmod source: the (updater, tile) pairs of the task; A' = updater rows from
+// its panel, B' = rows of its precomputed G_k, through the int8 inverse maps.
+template <typename T>
+struct CmodSrc {
+  static constexpr bool kBonfly = false;
+  const FactorArgs* fa;
+  const int4* pairs;
+  const int8_t* maps;
+  int pb, pe;
+  __device__ int npairs() const { return pe - pb; }
+  __device__ int ncols(int u) const { return fa->sn_ncol[pairs[pb + u].x]; }
+  __device__ void open(TcCur<T>& x, int u, int row, int col) const {
+    const int4 pr = pairs[pb + u];
+    const int k = pr.x, a = pr.y, q0 = pr.z;
+    const int nck = fa->sn_ncol[k], nrk = fa->sn_nrow[k];
+    const int8_t* m = maps + (long long)(pb + u) * TC_MAP;
+    x.i = m[row];
+    x.j = m[TC_M + col];
+    x.lda = nrk;
+    x.ldb = nrk - nck;
+    x.Ar = reinterpret_cast<const T*>(fa->panel) + fa->sn_poff[k] + nck + a + x.i;
+    x.Br = reinterpret_cast<const T*>(fa->gpool) + fa->goff[k] + q0 + x.j;
+    x.dk = nullptr;
+    x.dsk = nullptr;
+    x.kk = nullptr;
+  }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4* __restrict__ tasks,
+                                                      const int4* __restrict__ pairs,
+                                                      const int8_t* __restrict__ maps) {
+  if (fa.status[0] != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];  // re-aligned to 1024 inside
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, r0 = (tk.y >> 16) * TC_M, c0 = (tk.y & 0xffff) * TC_N;
+  const int ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
+  CmodSrc<T> src{&fa, pairs, maps, tk.z, tk.w};
+  tc_tile_pipeline<T>(fa, src, s, 0, 0, r0, c0, min(TC_M, nrow - r0), min(TC_N, ncol - c0), smem_raw);
+}
+
+// In-panel (deferred) Schur source of block [kb, ke) of supernode s: one
+// K-range of pw columns; A' = L21 rows [ke + r0, ...) of the panel (every
+// row real), B' = (L21 D) rows [ke + c0, ...) formed on the fly with the
+// block's D.  Reference: ll_cdiv_emit deferred Schur,
+// src/numeric/multifrontal_ldlt.rs:3085-3167.
+template <typename T>
+struct SchurSrc {
+  static constexpr bool kBonfly = true;
+  const T* L21;  // panel + ke + kb * nrow
+  long long nrow;
+  int pw, r0, c0, rows_here, cols_here;
+  const T* d;
+  const T* ds;
+  const unsigned char* kd;
+  __device__ int npairs() const { return 1; }
+  __device__ int ncols(int) const { return pw; }
+  __device__ void open(TcCur<T>& x, int, int row, int col) const {
+    x.i = row < rows_here ? 0 : -1;
+    x.j = col < cols_here ? 0 : -1;
+    x.lda = nrow;
+    x.ldb = nrow;
+    x.Ar = L21 + r0 + row;
+    x.Br = L21 + c0 + col;
+    x.dk = d;
+    x.dsk = ds;
+    x.kk = kd;
+  }
+};
+
+// Task (s, kb, r0, c0): trailing-part tile rows [ke + r0, +128) x columns
+// [ke + c0, +64) of block [kb, ke) of supernode s.
+template <typename T>
+__global__ void __launch_bounds__(TC_NT, 1) k_schur_tc(FactorArgs fa, const int4* __restrict__ tasks, int nb_small,
+                                                       int nb_big) {
+  if (fa.status[0] != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];  // re-aligned to 1024 inside
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, kb = tk.y, r0 = tk.z, c0 = tk.w;
+  const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
+  const int nb = ncol >= 512 ? nb_big : nb_small;
+  const int ke = min(kb + nb, ncol);
+  const int mt = nrow - ke, cw = ncol - ke;
+  const T* panel = reinterpret_cast<const T*>(fa.panel) + fa.sn_poff[s];
+  SchurSrc<T> src{panel + ke + (long long)kb * nrow, (long long)nrow, ke - kb, r0, c0,
+                  min(TC_M, mt - r0), min(TC_N, cw - c0),
+                  reinterpret_cast<const T*>(fa.d) + first + kb, reinterpret_cast<const T*>(fa.dsub) + first + kb,
+                  fa.kind + first + kb};
+  tc_tile_pipeline<T>(fa, src, s, ke, ke, r0, c0, min(TC_M, mt - r0), min(TC_N, cw - c0), smem_raw);
 }
 
 }  // namespace rsd

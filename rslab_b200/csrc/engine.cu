@@ -99,7 +99,7 @@ enum LaunchKind {
   L_CMOD, L_GETF2, L_DEEP, L_SCHUR,
   L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD,
   L_FTRSV_BLK, L_FTRSV_UPD, L_BTRSV_BLK, L_BTRSV_UPD, L_FWD_GATHER, L_CMOD_TC, L_MAKE_G, L_DIAG_INV,
-  L_BWD_OFF_RED
+  L_BWD_OFF_RED, L_SCHUR_TC
 };
 struct Launch {
   int kind;
@@ -459,7 +459,7 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
     for (int64_t s : lvl) maxblocks = std::max(maxblocks, (int)((S.sn[s].ncol + nb_of(s) - 1) / nb_of(s)));
     for (int b = 0; b < maxblocks; ++b) {
       Launch G{L_GETF2, (long long)H.t4.size(), 0, 0};
-      std::vector<int4> deep, schur;
+      std::vector<int4> deep, schur, schur_tc;
       int slot = 0, launch_nb = 0;
       for (int64_t s : lvl) {
         int nb = nb_of(s), nc = (int)S.sn[s].ncol, nr = H.nrow[s];
@@ -478,6 +478,8 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         H.kind_flops[4] += 2.0 * ((double)mt * cw - (double)cw * (cw - 1) / 2.0) * pw;
         for (int c0 = 0; c0 < cw; c0 += TILE)
           for (int r0 = c0; r0 < mt; r0 += TILE) schur.push_back(make_int4((int)s, kb, r0, c0));
+        for (int c0 = 0; c0 < cw; c0 += TC_N)
+          for (int r0 = (c0 / TC_M) * TC_M; r0 < mt; r0 += TC_M) schur_tc.push_back(make_int4((int)s, kb, r0, c0));
         ++slot;
       }
       G.ntasks = slot;
@@ -494,6 +496,9 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         Launch C{L_SCHUR, (long long)H.t4.size(), (int)schur.size(), 0};
         H.t4.insert(H.t4.end(), schur.begin(), schur.end());
         H.fplan.push_back(C);
+        Launch Ct{L_SCHUR_TC, (long long)H.t4.size(), (int)schur_tc.size(), 0};
+        H.t4.insert(H.t4.end(), schur_tc.begin(), schur_tc.end());
+        H.fplan.push_back(Ct);
       }
     }
     // G_k = L21_k D_k of this level's updaters, for the tensor-core cmod of
@@ -642,8 +647,10 @@ struct KernelSetup {
     static bool done = false;
     if (done) return;
     const size_t es = sizeof(T);
-    if constexpr (TensorCmod<T>::ok)
+    if constexpr (TensorCmod<T>::ok) {
       CK(cudaFuncSetAttribute(k_cmod_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_tc_bytes()));
+      CK(cudaFuncSetAttribute(k_schur_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_tc_bytes()));
+    }
     CK(cudaFuncSetAttribute(k_cmod<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod(es)));
     CK(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
     CK(cudaFuncSetAttribute(k_getf2<T, GETF2_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -865,13 +872,22 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         break;
       }
       case L_SCHUR:
+        if (use_tc) continue;
         k_schur<T><<<L.ntasks, TPB, smem_schur(es), st>>>(fa, H.d_t4 + L.task_off, nb_small, nb_big);
+        break;
+      case L_SCHUR_TC:
+        if constexpr (TensorCmod<T>::ok) {
+          if (!use_tc) continue;
+          k_schur_tc<T><<<L.ntasks, TC_NT, smem_cmod_tc_bytes(), st>>>(fa, H.d_t4 + L.task_off, nb_small, nb_big);
+        } else {
+          continue;
+        }
         break;
     }
     if (prof)
       prof->mark(st,
                  (L.kind == L_CMOD || L.kind == L_CMOD_TC || L.kind == L_MAKE_G) ? 1
-                 : L.kind == L_DIAG_INV                                        ? 4
+                 : (L.kind == L_DIAG_INV || L.kind == L_SCHUR_TC)             ? 4
                  : L.kind == L_GETF2                                           ? 2
                  : L.kind == L_DEEP                                            ? 3
                                                                                : 4,
