@@ -446,13 +446,10 @@ __global__ void __launch_bounds__(TB) k_diag_inv(const int2* __restrict__ tasks,
 // minus the earlier blocks; z = Linv y with the precomputed inverse
 // (thread: row i = tid % TB, right-hand sides tid / TB + 4 m; k ascending).
 template <typename T>
-__global__ void __launch_bounds__(SOLVE_NT) k_ftrsv_blk(SolveArgs a, const int4* __restrict__ tasks) {
+__device__ void fwd_blk_inv(const SolveArgs& a, int s, int j0, unsigned char* smem_raw) {
   using F = Field<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   T* Ls = reinterpret_cast<T*>(smem_raw);  // TB x (TB + 1): Ls[k * (TB + 1) + i] = Linv[i, k]
   T* Ys = Ls + TB * (TB + 1);              // TB x RHS_MAX
-  const int4 tk = tasks[blockIdx.x];
-  const int s = tk.x, j0 = tk.y;
   const int first = a.sn_first[s], ncol = a.sn_ncol[s];
   const int nb = min(TB, ncol - j0);
   T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)(first + j0) * a.ld;
@@ -487,8 +484,17 @@ __global__ void __launch_bounds__(SOLVE_NT) k_ftrsv_blk(SolveArgs a, const int4*
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_NT) k_ftrsv_blk(SolveArgs a, const int4* __restrict__ tasks) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int4 tk = tasks[blockIdx.x];
+  fwd_blk_inv<T>(a, tk.x, tk.y, smem_raw);
+}
+
 // Right-looking update after forward block [j0, j0+64) of a wide supernode:
-// Z[r] -= sum_{q in block} L[r, q] z[q] for own rows r in [r0, r0+64).
+// Z[r] -= sum_{q in block} L[r, q] z[q] for own rows r in [r0, r0+64); task
+// (s, j0, r0, solve_next): with solve_next the rows are the next block's,
+// which this CTA then solves.
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_ftrsv_upd(SolveArgs a, const int4* __restrict__ tasks) {
   using F = Field<T>;
@@ -512,6 +518,12 @@ __global__ void __launch_bounds__(SOLVE_NT) k_ftrsv_upd(SolveArgs a, const int4*
         *z = F::sub(*z, acc[m]);
       }
     }
+  // The CTA that owns the next block's rows has just completed their update:
+  // it solves that block too (no separate launch on the critical path).
+  if (tk.w) {
+    __syncthreads();
+    fwd_blk_inv<T>(a, s, r0, smem_raw);
+  }
 }
 
 // Backward substitution of pivot columns [jb, je) of a panel in 32-column
@@ -592,13 +604,10 @@ __device__ void bwd_block_range(const SolveArgs& a, const T* __restrict__ L, int
 // the precomputed inverse (staged in shared memory), then the block's final
 // values go to Z and to X in g order.
 template <typename T>
-__global__ void __launch_bounds__(SOLVE_NT) k_btrsv_blk(SolveArgs a, const int4* __restrict__ tasks) {
+__device__ void bwd_blk_inv(const SolveArgs& a, int s, int jb, unsigned char* smem_raw) {
   using F = Field<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   T* Ls = reinterpret_cast<T*>(smem_raw);  // TB x (TB + 1): Ls[k * (TB + 1) + i] = Linv[k, i]
   T* Ws = Ls + TB * (TB + 1);              // TB x RHS_MAX
-  const int4 tk = tasks[blockIdx.x];
-  const int s = tk.x, jb = tk.y;
   const int first = a.sn_first[s], ncol = a.sn_ncol[s];
   const int nb = min(TB, ncol - jb);
   T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)(first + jb) * a.ld;
@@ -640,8 +649,17 @@ __global__ void __launch_bounds__(SOLVE_NT) k_btrsv_blk(SolveArgs a, const int4*
   }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_NT) k_btrsv_blk(SolveArgs a, const int4* __restrict__ tasks) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int4 tk = tasks[blockIdx.x];
+  bwd_blk_inv<T>(a, tk.x, tk.y, smem_raw);
+}
+
 // Right-looking backward update after block [jb, jb+64) of a wide supernode:
-// v[p] -= sum_{r in block} L[r, p] v[r] for columns p in [c0, c0+32) < jb.
+// v[p] -= sum_{r in block} L[r, p] v[r] for columns p in [c0, c0+32) < jb;
+// task (s, jb, c0, solve_prev): with solve_prev, c0 = jb - 64 and the task
+// covers the whole previous block, which it then solves.
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_btrsv_upd(SolveArgs a, const int4* __restrict__ tasks) {
   using F = Field<T>;
@@ -649,24 +667,32 @@ __global__ void __launch_bounds__(SOLVE_NT) k_btrsv_upd(SolveArgs a, const int4*
   T* Ls = reinterpret_cast<T*>(smem_raw);
   T* Vs = Ls + 32 * 33;
   const int4 tk = tasks[blockIdx.x];
-  const int s = tk.x, jb = tk.y, c0 = tk.z;
+  const int s = tk.x, jb = tk.y, c0 = tk.z, solve_prev = tk.w;
   const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
   const int je = min(jb + TB, ncol);
   const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
   T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  const int cols_here = min(32, jb - c0);
-  T acc[RHS_MAX / 8];
-  dot_cols_tile<T, false>(L, nrow, c0, cols_here, jb, je, Z, nullptr, a.ld, a.nrhs, acc, Ls, Vs);
   const int pc = threadIdx.x & 31, cg = threadIdx.x >> 5;
-  if (pc < cols_here) {
-    const int p = c0 + pc;
+  // one 32-column chunk, or (solve_prev) the two chunks of the previous block
+  for (int cc = c0; cc < (solve_prev ? jb : c0 + 32); cc += 32) {
+    const int cols_here = min(32, jb - cc);
+    T acc[RHS_MAX / 8];
+    dot_cols_tile<T, false>(L, nrow, cc, cols_here, jb, je, Z, nullptr, a.ld, a.nrhs, acc, Ls, Vs);
+    if (pc < cols_here) {
+      const int p = cc + pc;
 #pragma unroll
-    for (int q = 0; q < RHS_MAX / 8; ++q) {
-      const int c = cg + 8 * q;
-      if (c >= a.nrhs) continue;
-      T* z = Z + (long long)p * a.ld + c;
-      *z = F::sub(*z, acc[q]);
+      for (int q = 0; q < RHS_MAX / 8; ++q) {
+        const int c = cg + 8 * q;
+        if (c >= a.nrhs) continue;
+        T* z = Z + (long long)p * a.ld + c;
+        *z = F::sub(*z, acc[q]);
+      }
     }
+  }
+  // The previous block's columns are now complete: solve it here.
+  if (solve_prev) {
+    __syncthreads();
+    bwd_blk_inv<T>(a, s, c0, smem_raw);
   }
 }
 

@@ -537,17 +537,23 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       int maxb = 0;
       for (int64_t s : lvl)
         if (S.sn[s].ncol > SOLVE_BIG) maxb = std::max(maxb, (int)((S.sn[s].ncol + TB - 1) / TB));
-      for (int b = 0; b < maxb; ++b) {
+      // Wide supernodes: block 0 is solved by k_ftrsv_blk; afterwards each
+      // launch updates the rows below block b and the CTA owning block b+1's
+      // rows solves it (one launch per block step).
+      if (maxb > 0) {
         Launch Fb{L_FTRSV_BLK, (long long)H.st4.size(), 0, 0};
         for (int64_t s : lvl)
-          if (S.sn[s].ncol > SOLVE_BIG && b * TB < S.sn[s].ncol) H.st4.push_back(make_int4((int)s, b * TB, 0, 0));
+          if (S.sn[s].ncol > SOLVE_BIG) H.st4.push_back(make_int4((int)s, 0, 0, 0));
         Fb.ntasks = (int)(H.st4.size() - Fb.task_off);
         H.fwdplan.push_back(Fb);
+      }
+      for (int b = 0; b < maxb; ++b) {
         Launch Fu{L_FTRSV_UPD, (long long)H.st4.size(), 0, 0};
         for (int64_t s : lvl) {
           const int nc = (int)S.sn[s].ncol;
           if (nc <= SOLVE_BIG) continue;
-          for (int r0 = (b + 1) * TB; r0 < nc; r0 += 64) H.st4.push_back(make_int4((int)s, b * TB, r0, 0));
+          for (int r0 = (b + 1) * TB; r0 < nc; r0 += TB)
+            H.st4.push_back(make_int4((int)s, b * TB, r0, r0 == (b + 1) * TB ? 1 : 0));
         }
         Fu.ntasks = (int)(H.st4.size() - Fu.task_off);
         if (Fu.ntasks) H.fwdplan.push_back(Fu);
@@ -592,16 +598,23 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         if (S.sn[s].ncol <= SOLVE_BIG) H.t1.push_back((int)s);
       Bd.ntasks = (int)(H.t1.size() - Bd.task_off);
       if (Bd.ntasks) bw.push_back(Bd);
+      // Backward, last block first: k_btrsv_blk solves each wide supernode's
+      // last block; each update launch after block b also solves block b-1
+      // in the task that covers it.
       for (int b = maxb - 1; b >= 0; --b) {
         Launch Bb{L_BTRSV_BLK, (long long)H.st4.size(), 0, 0};
-        for (int64_t s : lvl)
-          if (S.sn[s].ncol > SOLVE_BIG && b * TB < S.sn[s].ncol) H.st4.push_back(make_int4((int)s, b * TB, 0, 0));
+        for (int64_t s : lvl) {
+          const int nc = (int)S.sn[s].ncol;
+          if (nc > SOLVE_BIG && b == (nc - 1) / TB) H.st4.push_back(make_int4((int)s, b * TB, 0, 0));
+        }
         Bb.ntasks = (int)(H.st4.size() - Bb.task_off);
-        bw.push_back(Bb);
+        if (Bb.ntasks) bw.push_back(Bb);
         Launch Bu{L_BTRSV_UPD, (long long)H.st4.size(), 0, 0};
         for (int64_t s : lvl)
-          if (S.sn[s].ncol > SOLVE_BIG && b * TB < S.sn[s].ncol)
-            for (int c0 = 0; c0 < b * TB; c0 += 32) H.st4.push_back(make_int4((int)s, b * TB, c0, 0));
+          if (S.sn[s].ncol > SOLVE_BIG && b * TB < S.sn[s].ncol && b > 0) {
+            H.st4.push_back(make_int4((int)s, b * TB, (b - 1) * TB, 1));
+            for (int c0 = 0; c0 < (b - 1) * TB; c0 += 32) H.st4.push_back(make_int4((int)s, b * TB, c0, 0));
+          }
         Bu.ntasks = (int)(H.st4.size() - Bu.task_off);
         if (Bu.ntasks) bw.push_back(Bu);
       }
@@ -659,12 +672,12 @@ struct KernelSetup {
     CK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
     CK(cudaFuncSetAttribute(k_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
     CK(cudaFuncSetAttribute(k_fwd_push<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_push(es)));
-    CK(cudaFuncSetAttribute(k_ftrsv_upd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_push(es)));
+    CK(cudaFuncSetAttribute(k_ftrsv_upd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_blk_inv(es)));
     CK(cudaFuncSetAttribute(k_ftrsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_blk_inv(es)));
     CK(cudaFuncSetAttribute(k_diag_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_diag_inv(es)));
     CK(cudaFuncSetAttribute(k_btrsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_blk_inv(es)));
     CK(cudaFuncSetAttribute(k_bwd_off<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
-    CK(cudaFuncSetAttribute(k_btrsv_upd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
+    CK(cudaFuncSetAttribute(k_btrsv_upd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_blk_inv(es)));
     done = true;
   }
 };
@@ -1036,7 +1049,7 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
           k_ftrsv_blk<T><<<L.ntasks, SOLVE_NT, smem_blk_inv(es), st>>>(sa, H.d_st4 + L.task_off);
           break;
         case L_FTRSV_UPD:
-          k_ftrsv_upd<T><<<L.ntasks, SOLVE_NT, smem_push(es), st>>>(sa, H.d_st4 + L.task_off);
+          k_ftrsv_upd<T><<<L.ntasks, SOLVE_NT, smem_blk_inv(es), st>>>(sa, H.d_st4 + L.task_off);
           break;
         default:
           k_fwd_push<T><<<L.ntasks, SOLVE_NT, smem_push(es), st>>>(sa, H.d_t2 + L.task_off);
@@ -1057,7 +1070,7 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
           k_btrsv_blk<T><<<L.ntasks, SOLVE_NT, smem_blk_inv(es), st>>>(sa, H.d_st4 + L.task_off);
           break;
         case L_BTRSV_UPD:
-          k_btrsv_upd<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_st4 + L.task_off);
+          k_btrsv_upd<T><<<L.ntasks, SOLVE_NT, smem_blk_inv(es), st>>>(sa, H.d_st4 + L.task_off);
           break;
         default:
           k_bwd<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_t1 + L.task_off);
