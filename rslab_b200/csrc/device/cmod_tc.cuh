@@ -17,19 +17,16 @@
 //
 // G_k = L21_k D_k is formed once per updater (k_make_g, after k's level is
 // factored), so staging is plain loads plus the hi/lo split.
-// Pipeline (one CTA per SM, 16 warps): every warp loads, splits and stores
-// its slots of each K chunk into one of three shared-memory stages, with the
-// loads of the next two chunks in flight in registers; the warp whose
-// arrival completes a stage (a shared-memory counter with release / acquire
-// fences) issues the chunk's 12 tcgen05.mma and commits them to the stage's
-// `empty` mbarrier, which gates the stage's reuse.  No block-wide barrier in
-// the main loop and no dedicated issue warp (so 128 registers per thread).
+// Warp-specialised pipeline (one CTA per SM): 16 producer warps load, split
+// and store K chunks into three shared-memory stages and arrive on the
+// stage's `full` mbarrier; one MMA warp waits on `full`, issues the 12
+// tcgen05.mma of the chunk and commits to the stage's `empty` mbarrier,
+// which gates the stage's reuse.  No block-wide barrier in the main loop.
 // Accuracy: the tensor pipe does not round its accumulation to nearest, so
-// the sum runs in windows of TC_WIN chunks over two TMEM accumulators; each
-// warp adds every finished window into per-thread fp32 registers (round to
-// nearest) while the next window runs on the other accumulator; a window's
-// accumulator is reused only by the window after next, whose first issue
-// comes after every warp has promoted it.
+// the sum runs in windows of TC_WIN chunks over two TMEM accumulators; the
+// producers add each finished window into per-thread fp32 registers (round
+// to nearest) while the next window runs on the other accumulator, and
+// signal the MMA warp (`promoted` mbarrier) before the accumulator is reused.
 // Every wait is bounded; on a timeout the kernel flags status 2, drains what
 // it issued (bounded) and frees its TMEM.
 // Reference: ll_factor_node cmod, src/numeric/multifrontal_ldlt.rs:2452-2728.
@@ -42,8 +39,9 @@ namespace rsd {
 
 constexpr int TC_M = 128;                 // target tile rows = UMMA M
 constexpr int TC_N = 64;                  // target tile columns
-constexpr int TC_PW = 16;                 // warps (all stage operands; the last to arrive issues)
-constexpr int TC_NT = TC_PW * 32;         // threads per CTA
+constexpr int TC_PW = 16;                 // producer warps
+constexpr int TC_NP = TC_PW * 32;         // producer threads
+constexpr int TC_NT = TC_NP + 32;         // + one MMA-issue warp
 constexpr int TC_NS = 3;                  // shared-memory stages
 constexpr int TC_OPER = 16384;            // bytes of one 128 x 32 fp32 operand tile
 constexpr int TC_STAGE = 4 * TC_OPER;     // A hi, A lo, B hi, B lo
@@ -64,7 +62,6 @@ template <> struct TcShape<c32> {
 constexpr int TC_MAP = TC_M + TC_N;      // bytes of the inverse maps of one pair
 
 __host__ __device__ constexpr size_t smem_cmod_tc_bytes() { return 1024 + TC_NS * (size_t)TC_STAGE + 128; }
-static_assert(TC_NS * 8 + 2 * 8 + TC_NS * 4 + 4 <= 128, "barrier area");
 
 // hi/lo split of 4 (or 2) consecutive K elements of an operand row, stored
 // at byte offset `off` of the hi and lo tiles.
@@ -146,23 +143,26 @@ __device__ __forceinline__ void tc_tile_pipeline(const FactorArgs& fa, const Src
   using F = Field<T>;
   using Sh = TcShape<T>;
   using Cur = TcCur<T>;
-  constexpr int NC = Sh::n / 4;  // accumulator columns per thread
+  constexpr int NC = Sh::n / 4;  // accumulator columns per producer thread
   const uint32_t sraw = smem_u32(smem_raw);
   unsigned char* sm = smem_raw + (((sraw + 1023u) & ~1023u) - sraw);
-  uint64_t* empty = reinterpret_cast<uint64_t*>(sm + TC_NS * TC_STAGE);  // TC_NS: stage MMAs done
-  uint64_t* wbar = empty + TC_NS;                                        // 2: window MMAs done
-  int* cnt = reinterpret_cast<int*>(wbar + 2);                           // TC_NS: warp arrivals per stage
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(cnt + TC_NS);
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + TC_NS * TC_STAGE);  // TC_NS
+  uint64_t* empty = full + TC_NS;                                       // TC_NS
+  uint64_t* wbar = empty + TC_NS;                                       // 2: window MMAs done
+  uint64_t* pbar = wbar + 2;                                            // 2: window promoted
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(pbar + 2);
 
-  const int pe = src.npairs();
+  const int pb = 0, pe = src.npairs();
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
     for (int i = 0; i < TC_NS; ++i) {
+      mbar_init(&full[i], TC_NP);
       mbar_init(&empty[i], 1);
-      cnt[i] = 0;
     }
     mbar_init(&wbar[0], 1);
     mbar_init(&wbar[1], 1);
+    mbar_init(&pbar[0], TC_NP);
+    mbar_init(&pbar[1], TC_NP);
     fence_mbar_init();
   }
   if (warp == 0) tmem_alloc(tslot, TC_TMEM_COLS);
@@ -170,214 +170,212 @@ __device__ __forceinline__ void tc_tile_pipeline(const FactorArgs& fa, const Src
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  constexpr uint32_t idesc = idesc_tf32(TC_M, Sh::n);
   bool ok = true;
-  int c = 0;                               // chunks this thread took part in
-  const int q = warp & 3, cg = warp >> 2;  // TMEM lane quarter, column group
-  float acc[NC];                           // finished windows, fp32
+  int nchunks = 0;                         // chunks this thread took part in
+  const int q = warp & 3, cg = warp >> 2;  // producers: TMEM lane quarter, column group
+  float acc[NC];                           // producers: finished windows, fp32
 #pragma unroll
   for (int j = 0; j < NC; ++j) acc[j] = 0.0f;
 
-  // Fixed per-thread element slots (see the operand layouts above):
-  //   c32: A' row tid & 127, complex columns 4 (tid >> 7) .. +4;
-  //        B' column tid & 63, complex columns 2 (tid >> 6) .. +2.
-  //   f32: A' row tid & 127, columns 8 (tid >> 7) .. +8;
-  //        B' column tid & 63, columns 4 (tid >> 6) .. +4.
-  const int row = tid & (TC_M - 1), ga = tid >> 7;
-  const int ub = tid & (TC_N - 1), gb = tid >> 6;
-  uint32_t oa0, oa1, ob0, ob1 = 0, ob2 = 0, ob3 = 0;
-  if constexpr (Field<T>::complex) {
-    oa0 = sw128_off(row, 4 * ga);
-    oa1 = sw128_off(row, 16 + 4 * ga);
-    ob0 = sw128_off(ub, 2 * gb);
-    ob1 = sw128_off(ub, 16 + 2 * gb);
-    ob2 = sw128_off(TC_N + ub, 2 * gb);
-    ob3 = sw128_off(TC_N + ub, 16 + 2 * gb);
-  } else {
-    oa0 = sw128_off(row, 8 * ga);
-    oa1 = sw128_off(row, 8 * ga + 4);
-    ob0 = sw128_off(ub, 4 * gb);
-  }
-  constexpr int NA = Field<T>::complex ? 4 : 8;  // A columns per thread
-  constexpr int NB = Field<T>::complex ? 2 : 4;  // B columns per thread
-  const int ta = NA * ga, tb = NB * gb;          // column offsets inside the chunk
-
-  auto open = [&](Cur& x, int u) {
-    src.open(x, u, row, ub);
-    x.u = u;
-    x.t0 = 0;
-    x.nck = src.ncols(u);
-  };
-  // (x -> y): the next chunk in (source range, column) order; false at the end
-  auto advance = [&](const Cur& x, Cur& y) -> bool {
-    y = x;
-    y.t0 += Sh::kc;
-    if (y.t0 < y.nck) return true;
-    if (x.u + 1 >= pe) return false;
-    open(y, x.u + 1);
-    return true;
-  };
-  auto load = [&](const Cur& x, T (&va)[NA], T (&vb)[NB]) {
+  if (warp == TC_PW) {
+    // ---------------- MMA-issue warp ----------------
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_tf32(TC_M, Sh::n);
+      const uint32_t sbase = smem_u32(sm);
+      int c = 0;
+      for (int u = pb; u < pe && ok; ++u) {
+        const int nck = src.ncols(u);
+        for (int t0 = 0; t0 < nck; t0 += Sh::kc, ++c) {
+          const int st = c % TC_NS, w = c / TC_WIN;
+          if (c % TC_WIN == 0 && w >= 2 && !mbar_wait_bounded(&pbar[w & 1], (uint32_t)(((w - 2) >> 1) & 1))) {
+            ok = false;
+            break;
+          }
+          if (!mbar_wait_bounded(&full[st], (uint32_t)((c / TC_NS) & 1))) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sa = sbase + (uint32_t)(st * TC_STAGE);
+          const uint32_t dacc = tmem + (uint32_t)(w & 1) * TC_ACC_COLS;
+          uint32_t accf = (c % TC_WIN) != 0 ? 1u : 0u;
 #pragma unroll
-    for (int jj = 0; jj < NA; ++jj) {
-      const int t = x.t0 + ta + jj;
-      va[jj] = (x.i >= 0 && t < x.nck) ? x.Ar[(long long)t * x.lda] : F::zero();
-    }
+          for (int p = 0; p < 3; ++p) {
+            const uint32_t at = sa + (p == 2 ? TC_OPER : 0);
+            const uint32_t bt = sa + 2 * TC_OPER + (p == 1 ? TC_OPER : 0);
 #pragma unroll
-    for (int jj = 0; jj < NB; ++jj) {
-      const int t = x.t0 + tb + jj;
-      if constexpr (Src::kBonfly)
-        vb[jj] = (x.j >= 0 && t < x.nck) ? ld_G(x.Br, x.ldb, 0, t, x.dk, x.dsk, x.kk) : F::zero();
-      else
-        vb[jj] = (x.j >= 0 && t < x.nck) ? x.Br[(long long)t * x.ldb] : F::zero();
-    }
-  };
-  // Add finished window w into the registers (waits for its MMAs).
-  auto promote = [&](int w) {
-    if (!mbar_wait_bounded(&wbar[w & 1], (uint32_t)((w >> 1) & 1))) {
-      ok = false;
-      return;
-    }
-    tc_fence_after();
-    float v[NC];
-    tmem_ld_cols<NC>(tmem + (uint32_t)(w & 1) * TC_ACC_COLS + ((uint32_t)(32 * q) << 16) + (uint32_t)(cg * NC), v);
-#pragma unroll
-    for (int j = 0; j < NC; ++j) acc[j] += v[j];
-    tc_fence_before();
-  };
-  // The warp whose arrival completes a stage issues its MMAs: the stage's
-  // writes of every warp are ordered before it by the release / acquire
-  // fences around the shared-memory counter.
-  auto issue = [&](int st, int cc, bool last) {
-    const int w = cc / TC_WIN;
-    tc_fence_after();
-    const uint32_t sa = smem_u32(sm + st * TC_STAGE);
-    const uint32_t dacc = tmem + (uint32_t)(w & 1) * TC_ACC_COLS;
-    uint32_t accf = (cc % TC_WIN) != 0 ? 1u : 0u;
-#pragma unroll
-    for (int p = 0; p < 3; ++p) {
-      const uint32_t at = sa + (p == 2 ? TC_OPER : 0);
-      const uint32_t bt = sa + 2 * TC_OPER + (p == 1 ? TC_OPER : 0);
-#pragma unroll
-      for (int ks = 0; ks < 4; ++ks) {
-        mma_tf32(dacc, desc_sw128(at + 32u * ks), desc_sw128(bt + 32u * ks), idesc, accf);
-        accf = 1u;
-      }
-    }
-    mma_commit(&empty[st]);
-    if (cc % TC_WIN == TC_WIN - 1 || last) mma_commit(&wbar[w & 1]);
-  };
-
-  int pw = 0;  // next window to promote
-  if (pe > 0) {
-    // three register sets: chunk c (stored now), c + 1 and c + 2 (in flight)
-    Cur cur, n1, n2;
-    open(cur, 0);
-    T va[NA], vb[NB], a1[NA], b1[NB], a2[NA], b2[NB];
-    load(cur, va, vb);
-    bool more1 = advance(cur, n1), more2 = false;
-    if (more1) {
-      load(n1, a1, b1);
-      more2 = advance(n1, n2);
-    }
-    for (;;) {
-      if (more2) load(n2, a2, b2);
-      const int st = c % TC_NS;
-      if (c >= TC_NS && !mbar_wait_bounded(&empty[st], (uint32_t)(((c / TC_NS) - 1) & 1))) {
-        ok = false;
-        break;
-      }
-      unsigned char* stg = sm + st * TC_STAGE;
-      unsigned char* Ah = stg;
-      unsigned char* Al = stg + TC_OPER;
-      unsigned char* Bh = stg + 2 * TC_OPER;
-      unsigned char* Bl = stg + 3 * TC_OPER;
-      if constexpr (Field<T>::complex) {
-        store_split4(Ah, Al, oa0, va[0].re, va[1].re, va[2].re, va[3].re);  // Re(A): K' 0..15
-        store_split4(Ah, Al, oa1, va[0].im, va[1].im, va[2].im, va[3].im);  // Im(A): K' 16..31
-        store_split2(Bh, Bl, ob0, vb[0].re, vb[1].re);                      // Re out:  Gr
-        store_split2(Bh, Bl, ob1, -vb[0].im, -vb[1].im);                    //         -Gi
-        store_split2(Bh, Bl, ob2, vb[0].im, vb[1].im);                      // Im out:  Gi
-        store_split2(Bh, Bl, ob3, vb[0].re, vb[1].re);                      //          Gr
-      } else {
-        store_split4(Ah, Al, oa0, va[0], va[1], va[2], va[3]);
-        store_split4(Ah, Al, oa1, va[4], va[5], va[6], va[7]);
-        store_split4(Bh, Bl, ob0, vb[0], vb[1], vb[2], vb[3]);
-      }
-      fence_proxy_async_smem();
-      __syncwarp();
-      if (lane == 0) {
-        // the counter of a stage only grows: use u of stage st completes at
-        // 16 (u + 1) arrivals, so no reset has to be ordered against reuse
-        __threadfence_block();
-        if (atomicAdd(&cnt[st], 1) == TC_PW * (c / TC_NS + 1) - 1) {
-          __threadfence_block();
-          issue(st, c, !more1);
+            for (int ks = 0; ks < 4; ++ks) {
+              mma_tf32(dacc, desc_sw128(at + 32u * ks), desc_sw128(bt + 32u * ks), idesc, accf);
+              accf = 1u;
+            }
+          }
+          mma_commit(&empty[st]);
+          const bool last = (t0 + Sh::kc >= nck) && (u + 1 == pe);
+          if (c % TC_WIN == TC_WIN - 1 || last) mma_commit(&wbar[w & 1]);
         }
       }
-      __syncwarp();
-      // window w - 1 is two chunks behind: promote it before its accumulator
-      // is reused by window w + 1 (whose first issue needs every warp past here)
-      if (c % TC_WIN == 2 && c >= TC_WIN) promote(pw++);
-      ++c;
-      if (!more1 || !ok) break;
+      nchunks = c;
+    }
+  } else {
+    // ---------------- producer warps ----------------
+    // Fixed per-thread element slots (see the operand layouts above):
+    //   c32: A' row tid & 127, complex columns 4 (tid >> 7) .. +4;
+    //        B' column tid & 63, complex columns 2 (tid >> 6) .. +2.
+    //   f32: A' row tid & 127, columns 8 (tid >> 7) .. +8;
+    //        B' column tid & 63, columns 4 (tid >> 6) .. +4.
+    const int row = tid & (TC_M - 1), ga = tid >> 7;
+    const int ub = tid & (TC_N - 1), gb = tid >> 6;
+    uint32_t oa0, oa1, ob0, ob1 = 0, ob2 = 0, ob3 = 0;
+    if constexpr (Field<T>::complex) {
+      oa0 = sw128_off(row, 4 * ga);
+      oa1 = sw128_off(row, 16 + 4 * ga);
+      ob0 = sw128_off(ub, 2 * gb);
+      ob1 = sw128_off(ub, 16 + 2 * gb);
+      ob2 = sw128_off(TC_N + ub, 2 * gb);
+      ob3 = sw128_off(TC_N + ub, 16 + 2 * gb);
+    } else {
+      oa0 = sw128_off(row, 8 * ga);
+      oa1 = sw128_off(row, 8 * ga + 4);
+      ob0 = sw128_off(ub, 4 * gb);
+    }
+    constexpr int NA = Field<T>::complex ? 4 : 8;  // A columns per thread
+    constexpr int NB = Field<T>::complex ? 2 : 4;  // B columns per thread
+    const int ta = NA * ga, tb = NB * gb;          // column offsets inside the chunk
+    auto promote = [&](int w) {
+      if (!mbar_wait_bounded(&wbar[w & 1], (uint32_t)((w >> 1) & 1))) {
+        ok = false;
+        return;
+      }
+      tc_fence_after();
+      float v[NC];
+      tmem_ld_cols<NC>(tmem + (uint32_t)(w & 1) * TC_ACC_COLS + ((uint32_t)(32 * q) << 16) + (uint32_t)(cg * NC), v);
+#pragma unroll
+      for (int j = 0; j < NC; ++j) acc[j] += v[j];
+      tc_fence_before();
+      mbar_arrive(&pbar[w & 1]);
+    };
+    // Chunk cursor: pair u, source columns [t0, t0 + kc); the loads of the
+    // next chunk are issued before the current one is stored, so their
+    // latency overlaps the stage wait, the split and the stores.
+    auto open = [&](Cur& x, int u) {
+      src.open(x, u, row, ub);
+      x.u = u;
+      x.t0 = 0;
+      x.nck = src.ncols(u);
+    };
+    auto load = [&](const Cur& x, T (&va)[NA], T (&vb)[NB]) {
 #pragma unroll
       for (int jj = 0; jj < NA; ++jj) {
-        va[jj] = a1[jj];
-        a1[jj] = a2[jj];
+        const int t = x.t0 + ta + jj;
+        va[jj] = (x.i >= 0 && t < x.nck) ? x.Ar[(long long)t * x.lda] : F::zero();
       }
 #pragma unroll
       for (int jj = 0; jj < NB; ++jj) {
-        vb[jj] = b1[jj];
-        b1[jj] = b2[jj];
+        const int t = x.t0 + tb + jj;
+        if constexpr (Src::kBonfly)
+          vb[jj] = (x.j >= 0 && t < x.nck) ? ld_G(x.Br, x.ldb, 0, t, x.dk, x.dsk, x.kk) : F::zero();
+        else
+          vb[jj] = (x.j >= 0 && t < x.nck) ? x.Br[(long long)t * x.ldb] : F::zero();
       }
-      cur = n1;
-      more1 = more2;
-      if (more2) {
-        n1 = n2;
-        more2 = advance(n1, n2);
-      }
-    }
-  }
-  if (ok && c > 0)
-    while (pw <= (c - 1) / TC_WIN) {
-      promote(pw++);
-      if (!ok) break;
-    }
-  // Every warp agrees on the outcome before the epilogue.
-  const bool all_ok = __syncthreads_or(!ok) == 0;
-  if (all_ok && c > 0) {
-    // P -= U on the lower part.  Thread (q, cg, lane) holds tile row
-    // 32 q + lane and accumulator columns [cg NC, cg NC + NC): for c32
-    // columns 0-63 are the real parts and 64-127 the imaginary parts of
-    // tile columns 0-63; each thread updates its own component.
-    const int nrow = fa.sn_nrow[s];
-    const int trow = 32 * q + lane;
-    if (trow < rows_here) {
-      const int gr = rbase + r0 + trow;
-      float* pf = reinterpret_cast<float*>(reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s]);
+    };
+    int c = 0, pw = 0;
+    if (pb < pe) {
+      Cur cur;
+      open(cur, pb);
+      T va[NA], vb[NB];
+      load(cur, va, vb);
+      for (;;) {
+        Cur nx = cur;
+        nx.t0 += Sh::kc;
+        bool more = true;
+        if (nx.t0 >= nx.nck) {
+          if (cur.u + 1 < pe)
+            open(nx, cur.u + 1);
+          else
+            more = false;
+        }
+        T na[NA], nb2[NB];
+        if (more) load(nx, na, nb2);
+        const int st = c % TC_NS;
+        if (c >= TC_NS && !mbar_wait_bounded(&empty[st], (uint32_t)(((c / TC_NS) - 1) & 1))) {
+          ok = false;
+          break;
+        }
+        unsigned char* stg = sm + st * TC_STAGE;
+        unsigned char* Ah = stg;
+        unsigned char* Al = stg + TC_OPER;
+        unsigned char* Bh = stg + 2 * TC_OPER;
+        unsigned char* Bl = stg + 3 * TC_OPER;
+        if constexpr (Field<T>::complex) {
+          store_split4(Ah, Al, oa0, va[0].re, va[1].re, va[2].re, va[3].re);  // Re(A): K' 0..15
+          store_split4(Ah, Al, oa1, va[0].im, va[1].im, va[2].im, va[3].im);  // Im(A): K' 16..31
+          store_split2(Bh, Bl, ob0, vb[0].re, vb[1].re);                      // Re out:  Gr
+          store_split2(Bh, Bl, ob1, -vb[0].im, -vb[1].im);                    //         -Gi
+          store_split2(Bh, Bl, ob2, vb[0].im, vb[1].im);                      // Im out:  Gi
+          store_split2(Bh, Bl, ob3, vb[0].re, vb[1].re);                      //          Gr
+        } else {
+          store_split4(Ah, Al, oa0, va[0], va[1], va[2], va[3]);
+          store_split4(Ah, Al, oa1, va[4], va[5], va[6], va[7]);
+          store_split4(Bh, Bl, ob0, vb[0], vb[1], vb[2], vb[3]);
+        }
+        fence_proxy_async_smem();
+        mbar_arrive(&full[st]);
+        // window w - 1 is two chunks behind: promote it before the MMA warp
+        // needs its accumulator again (window w + 1)
+        if (c % TC_WIN == 2 && c >= TC_WIN) promote(pw++);
+        ++c;
+        if (!more || !ok) break;
+        cur = nx;
 #pragma unroll
-      for (int jj = 0; jj < NC; ++jj) {
-        const int colj = cg * NC + jj;
-        const int col = Field<T>::complex ? (colj & (TC_N - 1)) : colj;
-        const int comp = Field<T>::complex ? (colj >> 6) : 0;
-        const int gc = cbase + c0 + col;
-        if (col < cols_here && gr >= gc) {
-          const long long e = gr + (long long)gc * nrow;
-          float* p = Field<T>::complex ? pf + 2 * e + comp : pf + e;
-          *p -= acc[jj];
+        for (int jj = 0; jj < NA; ++jj) va[jj] = na[jj];
+#pragma unroll
+        for (int jj = 0; jj < NB; ++jj) vb[jj] = nb2[jj];
+      }
+    }
+    if (ok && c > 0)
+      while (pw <= (c - 1) / TC_WIN) {
+        promote(pw++);
+        if (!ok) break;
+      }
+    nchunks = c;
+  }
+  // Every role agrees on the outcome before the epilogue.
+  const bool all_ok = __syncthreads_or(!ok) == 0;
+  if (warp < TC_PW) {
+    if (all_ok && nchunks > 0) {
+      // P -= U on the lower part.  Thread (q, cg, lane) holds tile row
+      // 32 q + lane and accumulator columns [cg NC, cg NC + NC): for c32
+      // columns 0-63 are the real parts and 64-127 the imaginary parts of
+      // tile columns 0-63; each thread updates its own component.
+      const int nrow = fa.sn_nrow[s];
+      const int trow = 32 * q + lane;
+      if (trow < rows_here) {
+        const int gr = rbase + r0 + trow;
+        float* pf = reinterpret_cast<float*>(reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s]);
+#pragma unroll
+        for (int jj = 0; jj < NC; ++jj) {
+          const int colj = cg * NC + jj;
+          const int col = Field<T>::complex ? (colj & (TC_N - 1)) : colj;
+          const int comp = Field<T>::complex ? (colj >> 6) : 0;
+          const int gc = cbase + c0 + col;
+          if (col < cols_here && gr >= gc) {
+            const long long e = gr + (long long)gc * nrow;
+            float* p = Field<T>::complex ? pf + 2 * e + comp : pf + e;
+            *p -= acc[jj];
+          }
         }
       }
     }
-  } else if (!all_ok && c > 0 && tid == 0) {
-    // drain (bounded): wait for the last stage used to finish its MMAs
-    (void)mbar_wait_bounded(&empty[(c - 1) % TC_NS], (uint32_t)(((c - 1) / TC_NS) & 1));
+  } else if (!all_ok && lane == 0 && nchunks > 0) {
+    // drain (bounded): the last commit covers every MMA issued before it
+    (void)mbar_wait_bounded(&empty[(nchunks - 1) % TC_NS], (uint32_t)(((nchunks - 1) / TC_NS) & 1));
   }
   if (!all_ok && tid == 0 && atomicCAS(&fa.status[0], 0, 2) == 0) fa.status[1] = s;
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, TC_TMEM_COLS);
 }
+
 
 // cmod source: the (updater, tile) pairs of the task; A' = updater rows from
 // its panel, B' = rows of its precomputed G_k, through the int8 inverse maps.
