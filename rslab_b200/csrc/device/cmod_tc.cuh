@@ -42,9 +42,7 @@ constexpr int TC_N = 64;                  // target tile columns
 constexpr int TC_PW = 16;                 // producer warps
 constexpr int TC_NP = TC_PW * 32;         // producer threads
 constexpr int TC_NT = TC_NP + 32;         // + one MMA-issue warp
-constexpr int TC_NS = 3;                  // operand stages (register-staged sources)
-constexpr int TC_NS_ASYNC = 2;            // operand stages (copy-staged sources)
-constexpr int TC_RAW = 4;                 // raw copy slots in flight (copy-staged sources)
+constexpr int TC_NS = 3;                  // shared-memory stages
 constexpr int TC_OPER = 16384;            // bytes of one 128 x 32 fp32 operand tile
 constexpr int TC_STAGE = 4 * TC_OPER;     // A hi, A lo, B hi, B lo
 constexpr int TC_WIN = 4;                 // K chunks per TMEM accumulation window
@@ -63,14 +61,7 @@ template <> struct TcShape<c32> {
 
 constexpr int TC_MAP = TC_M + TC_N;      // bytes of the inverse maps of one pair
 
-// Raw slot of one K chunk, element-major per thread (A then B):
-// 512 threads x (4 A + 2 B) complex or (8 A + 4 B) real values = 24 KB.
-constexpr int TC_RAW_SLOT = 24576;
-// barriers after max(3 stages, 2 stages + 4 raw slots)
-constexpr int TC_BAR_OFF = (TC_NS * TC_STAGE > TC_NS_ASYNC * TC_STAGE + TC_RAW * TC_RAW_SLOT)
-                               ? TC_NS * TC_STAGE
-                               : TC_NS_ASYNC * TC_STAGE + TC_RAW * TC_RAW_SLOT;
-__host__ __device__ constexpr size_t smem_cmod_tc_bytes() { return 1024 + (size_t)TC_BAR_OFF + 128; }
+__host__ __device__ constexpr size_t smem_cmod_tc_bytes() { return 1024 + TC_NS * (size_t)TC_STAGE + 128; }
 
 // hi/lo split of 4 (or 2) consecutive K elements of an operand row, stored
 // at byte offset `off` of the hi and lo tiles.
@@ -155,11 +146,8 @@ __device__ __forceinline__ void tc_tile_pipeline(const FactorArgs& fa, const Src
   constexpr int NC = Sh::n / 4;  // accumulator columns per producer thread
   const uint32_t sraw = smem_u32(smem_raw);
   unsigned char* sm = smem_raw + (((sraw + 1023u) & ~1023u) - sraw);
-  // operand stages: register-staged sources use TC_NS, copy-staged ones
-  // TC_NS_ASYNC (the raw copy ring follows them)
-  constexpr int NS = Src::kBonfly ? TC_NS : TC_NS_ASYNC;
-  uint64_t* full = reinterpret_cast<uint64_t*>(sm + TC_BAR_OFF);  // NS
-  uint64_t* empty = full + TC_NS;                                 // NS
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + TC_NS * TC_STAGE);  // TC_NS
+  uint64_t* empty = full + TC_NS;                                       // TC_NS
   uint64_t* wbar = empty + TC_NS;                                       // 2: window MMAs done
   uint64_t* pbar = wbar + 2;                                            // 2: window promoted
   uint32_t* tslot = reinterpret_cast<uint32_t*>(pbar + 2);
@@ -167,7 +155,7 @@ __device__ __forceinline__ void tc_tile_pipeline(const FactorArgs& fa, const Src
   const int pb = 0, pe = src.npairs();
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
-    for (int i = 0; i < NS; ++i) {
+    for (int i = 0; i < TC_NS; ++i) {
       mbar_init(&full[i], TC_NP);
       mbar_init(&empty[i], 1);
     }
@@ -198,12 +186,12 @@ __device__ __forceinline__ void tc_tile_pipeline(const FactorArgs& fa, const Src
       for (int u = pb; u < pe && ok; ++u) {
         const int nck = src.ncols(u);
         for (int t0 = 0; t0 < nck; t0 += Sh::kc, ++c) {
-          const int st = c % NS, w = c / TC_WIN;
+          const int st = c % TC_NS, w = c / TC_WIN;
           if (c % TC_WIN == 0 && w >= 2 && !mbar_wait_bounded(&pbar[w & 1], (uint32_t)(((w - 2) >> 1) & 1))) {
             ok = false;
             break;
           }
-          if (!mbar_wait_bounded(&full[st], (uint32_t)((c / NS) & 1))) {
+          if (!mbar_wait_bounded(&full[st], (uint32_t)((c / TC_NS) & 1))) {
             ok = false;
             break;
           }
@@ -291,145 +279,57 @@ __device__ __forceinline__ void tc_tile_pipeline(const FactorArgs& fa, const Src
       }
     };
     int c = 0, pw = 0;
-    if constexpr (!Src::kBonfly) {
-      // Copy-staged producer: register-free cp.async copies of chunk c + 3
-      // into the raw ring while chunk c is converted; every thread reads back
-      // exactly the elements it copied, so the copy group wait is the only
-      // synchronisation on the raw ring.
-      unsigned char* raw = sm + NS * TC_STAGE;
-      const T* zero_src = reinterpret_cast<const T*>(fa.panel);  // any valid address for zero-fill
-      auto issue = [&](const Cur& x, int slot) {
-        T* ra = reinterpret_cast<T*>(raw + slot * TC_RAW_SLOT);
-        T* rb = ra + NA * TC_NP;
-#pragma unroll
-        for (int jj = 0; jj < NA; ++jj) {
-          const int t = x.t0 + ta + jj;
-          const bool v = x.i >= 0 && t < x.nck;
-          cp_async<sizeof(T)>(ra + jj * TC_NP + tid, v ? x.Ar + (long long)t * x.lda : zero_src, v ? (int)sizeof(T) : 0);
-        }
-#pragma unroll
-        for (int jj = 0; jj < NB; ++jj) {
-          const int t = x.t0 + tb + jj;
-          const bool v = x.j >= 0 && t < x.nck;
-          cp_async<sizeof(T)>(rb + jj * TC_NP + tid, v ? x.Br + (long long)t * x.ldb : zero_src, v ? (int)sizeof(T) : 0);
-        }
-      };
-      auto advance = [&](Cur& x) -> bool {
-        x.t0 += Sh::kc;
-        if (x.t0 < x.nck) return true;
-        if (x.u + 1 >= pe) return false;
-        open(x, x.u + 1);
-        return true;
-      };
-      if (pb < pe) {
-        Cur lc, cc;  // copy cursor (TC_RAW - 1 chunks ahead), consume cursor
-        open(lc, pb);
-        open(cc, pb);
-        bool lmore = true;
-        for (int k = 0; k < TC_RAW - 1; ++k) {
-          if (lmore) {
-            issue(lc, k);
-            lmore = advance(lc);
-          }
-          cp_async_commit();
-        }
-        for (;;) {
-          if (lmore) {
-            issue(lc, (c + TC_RAW - 1) % TC_RAW);
-            lmore = advance(lc);
-          }
-          cp_async_commit();
-          cp_async_wait<TC_RAW - 1>();  // chunk c's copies have landed
-          const int st = c % NS;
-          if (c >= NS && !mbar_wait_bounded(&empty[st], (uint32_t)(((c / NS) - 1) & 1))) {
-            ok = false;
-            break;
-          }
-          const T* ra = reinterpret_cast<const T*>(raw + (c % TC_RAW) * TC_RAW_SLOT);
-          const T* rb = ra + NA * TC_NP;
-          T va[NA], vb[NB];
-#pragma unroll
-          for (int jj = 0; jj < NA; ++jj) va[jj] = ra[jj * TC_NP + tid];
-#pragma unroll
-          for (int jj = 0; jj < NB; ++jj) vb[jj] = rb[jj * TC_NP + tid];
-          unsigned char* stg = sm + st * TC_STAGE;
-          unsigned char* Ah = stg;
-          unsigned char* Al = stg + TC_OPER;
-          unsigned char* Bh = stg + 2 * TC_OPER;
-          unsigned char* Bl = stg + 3 * TC_OPER;
-          if constexpr (Field<T>::complex) {
-            store_split4(Ah, Al, oa0, va[0].re, va[1].re, va[2].re, va[3].re);
-            store_split4(Ah, Al, oa1, va[0].im, va[1].im, va[2].im, va[3].im);
-            store_split2(Bh, Bl, ob0, vb[0].re, vb[1].re);
-            store_split2(Bh, Bl, ob1, -vb[0].im, -vb[1].im);
-            store_split2(Bh, Bl, ob2, vb[0].im, vb[1].im);
-            store_split2(Bh, Bl, ob3, vb[0].re, vb[1].re);
-          } else {
-            store_split4(Ah, Al, oa0, va[0], va[1], va[2], va[3]);
-            store_split4(Ah, Al, oa1, va[4], va[5], va[6], va[7]);
-            store_split4(Bh, Bl, ob0, vb[0], vb[1], vb[2], vb[3]);
-          }
-          fence_proxy_async_smem();
-          mbar_arrive(&full[st]);
-          if (c % TC_WIN == 2 && c >= TC_WIN) promote(pw++);
-          ++c;
-          if (!advance(cc) || !ok) break;
-        }
-        cp_async_wait<0>();
-      }
-    } else {
     if (pb < pe) {
-        Cur cur;
-        open(cur, pb);
-        T va[NA], vb[NB];
-        load(cur, va, vb);
-        for (;;) {
-          Cur nx = cur;
-          nx.t0 += Sh::kc;
-          bool more = true;
-          if (nx.t0 >= nx.nck) {
-            if (cur.u + 1 < pe)
-              open(nx, cur.u + 1);
-            else
-              more = false;
-          }
-          T na[NA], nb2[NB];
-          if (more) load(nx, na, nb2);
-          const int st = c % NS;
-          if (c >= NS && !mbar_wait_bounded(&empty[st], (uint32_t)(((c / NS) - 1) & 1))) {
-            ok = false;
-            break;
-          }
-          unsigned char* stg = sm + st * TC_STAGE;
-          unsigned char* Ah = stg;
-          unsigned char* Al = stg + TC_OPER;
-          unsigned char* Bh = stg + 2 * TC_OPER;
-          unsigned char* Bl = stg + 3 * TC_OPER;
-          if constexpr (Field<T>::complex) {
-            store_split4(Ah, Al, oa0, va[0].re, va[1].re, va[2].re, va[3].re);  // Re(A): K' 0..15
-            store_split4(Ah, Al, oa1, va[0].im, va[1].im, va[2].im, va[3].im);  // Im(A): K' 16..31
-            store_split2(Bh, Bl, ob0, vb[0].re, vb[1].re);                      // Re out:  Gr
-            store_split2(Bh, Bl, ob1, -vb[0].im, -vb[1].im);                    //         -Gi
-            store_split2(Bh, Bl, ob2, vb[0].im, vb[1].im);                      // Im out:  Gi
-            store_split2(Bh, Bl, ob3, vb[0].re, vb[1].re);                      //          Gr
-          } else {
-            store_split4(Ah, Al, oa0, va[0], va[1], va[2], va[3]);
-            store_split4(Ah, Al, oa1, va[4], va[5], va[6], va[7]);
-            store_split4(Bh, Bl, ob0, vb[0], vb[1], vb[2], vb[3]);
-          }
-          fence_proxy_async_smem();
-          mbar_arrive(&full[st]);
-          // window w - 1 is two chunks behind: promote it before the MMA warp
-          // needs its accumulator again (window w + 1)
-          if (c % TC_WIN == 2 && c >= TC_WIN) promote(pw++);
-          ++c;
-          if (!more || !ok) break;
-          cur = nx;
-  #pragma unroll
-          for (int jj = 0; jj < NA; ++jj) va[jj] = na[jj];
-  #pragma unroll
-          for (int jj = 0; jj < NB; ++jj) vb[jj] = nb2[jj];
+      Cur cur;
+      open(cur, pb);
+      T va[NA], vb[NB];
+      load(cur, va, vb);
+      for (;;) {
+        Cur nx = cur;
+        nx.t0 += Sh::kc;
+        bool more = true;
+        if (nx.t0 >= nx.nck) {
+          if (cur.u + 1 < pe)
+            open(nx, cur.u + 1);
+          else
+            more = false;
         }
+        T na[NA], nb2[NB];
+        if (more) load(nx, na, nb2);
+        const int st = c % TC_NS;
+        if (c >= TC_NS && !mbar_wait_bounded(&empty[st], (uint32_t)(((c / TC_NS) - 1) & 1))) {
+          ok = false;
+          break;
+        }
+        unsigned char* stg = sm + st * TC_STAGE;
+        unsigned char* Ah = stg;
+        unsigned char* Al = stg + TC_OPER;
+        unsigned char* Bh = stg + 2 * TC_OPER;
+        unsigned char* Bl = stg + 3 * TC_OPER;
+        if constexpr (Field<T>::complex) {
+          store_split4(Ah, Al, oa0, va[0].re, va[1].re, va[2].re, va[3].re);  // Re(A): K' 0..15
+          store_split4(Ah, Al, oa1, va[0].im, va[1].im, va[2].im, va[3].im);  // Im(A): K' 16..31
+          store_split2(Bh, Bl, ob0, vb[0].re, vb[1].re);                      // Re out:  Gr
+          store_split2(Bh, Bl, ob1, -vb[0].im, -vb[1].im);                    //         -Gi
+          store_split2(Bh, Bl, ob2, vb[0].im, vb[1].im);                      // Im out:  Gi
+          store_split2(Bh, Bl, ob3, vb[0].re, vb[1].re);                      //          Gr
+        } else {
+          store_split4(Ah, Al, oa0, va[0], va[1], va[2], va[3]);
+          store_split4(Ah, Al, oa1, va[4], va[5], va[6], va[7]);
+          store_split4(Bh, Bl, ob0, vb[0], vb[1], vb[2], vb[3]);
+        }
+        fence_proxy_async_smem();
+        mbar_arrive(&full[st]);
+        // window w - 1 is two chunks behind: promote it before the MMA warp
+        // needs its accumulator again (window w + 1)
+        if (c % TC_WIN == 2 && c >= TC_WIN) promote(pw++);
+        ++c;
+        if (!more || !ok) break;
+        cur = nx;
+#pragma unroll
+        for (int jj = 0; jj < NA; ++jj) va[jj] = na[jj];
+#pragma unroll
+        for (int jj = 0; jj < NB; ++jj) vb[jj] = nb2[jj];
       }
     }
     if (ok && c > 0)
@@ -468,7 +368,7 @@ __device__ __forceinline__ void tc_tile_pipeline(const FactorArgs& fa, const Src
     }
   } else if (!all_ok && lane == 0 && nchunks > 0) {
     // drain (bounded): the last commit covers every MMA issued before it
-    (void)mbar_wait_bounded(&empty[(nchunks - 1) % NS], (uint32_t)(((nchunks - 1) / NS) & 1));
+    (void)mbar_wait_bounded(&empty[(nchunks - 1) % TC_NS], (uint32_t)(((nchunks - 1) / TC_NS) & 1));
   }
   if (!all_ok && tid == 0 && atomicCAS(&fa.status[0], 0, 2) == 0) fa.status[1] = s;
   tc_fence_before();

@@ -68,20 +68,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return false;
 }
 
-// Asynchronous global -> shared copy of `bytes` (4, 8 or 16) bytes; with
-// src_bytes = 0 nothing is read and the destination is zero-filled.
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void* smem_dst, const void* gsrc, int src_bytes) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(smem_u32(smem_dst)), "l"(gsrc), "n"(BYTES),
-               "r"(src_bytes)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
 // Arrive once on `bar` (release, CTA scope).
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
