@@ -42,12 +42,15 @@ constexpr int TC_N = 64;                  // target tile columns
 constexpr int TC_PW = 16;                 // producer warps
 constexpr int TC_NP = TC_PW * 32;         // producer threads
 constexpr int TC_NT = TC_NP + 32;         // + one MMA-issue warp
-constexpr int TC_NS = 3;                  // shared-memory stages
+constexpr int TC_NS = 4;                  // operand stages
 constexpr int TC_OPER = 16384;            // bytes of one 128 x 32 fp32 operand tile
-constexpr int TC_STAGE = 4 * TC_OPER;     // A hi, A lo, B hi, B lo
+constexpr int TC_STAGE = 2 * TC_OPER;     // B hi, B lo in shared memory (A hi / lo live in TMEM)
 constexpr int TC_WIN = 4;                 // K chunks per TMEM accumulation window
 constexpr uint32_t TC_ACC_COLS = 128;     // TMEM columns of one accumulator
-constexpr uint32_t TC_TMEM_COLS = 2 * TC_ACC_COLS;
+constexpr uint32_t TC_A_BASE = 2 * TC_ACC_COLS;   // A stages after the two accumulators
+constexpr uint32_t TC_A_COLS = 64;                // A hi (32 columns) + A lo (32 columns) per stage
+constexpr uint32_t TC_TMEM_COLS = 512;            // 2 x 128 accumulator + 4 x 64 A stage columns
+static_assert(TC_A_BASE + TC_NS * TC_A_COLS <= TC_TMEM_COLS, "TMEM budget");
 
 template <typename T> struct TcShape;
 template <> struct TcShape<float> {
@@ -198,14 +201,15 @@ __device__ __forceinline__ void tc_tile_pipeline(const FactorArgs& fa, const Src
           tc_fence_after();
           const uint32_t sa = sbase + (uint32_t)(st * TC_STAGE);
           const uint32_t dacc = tmem + (uint32_t)(w & 1) * TC_ACC_COLS;
+          const uint32_t ahi = tmem + TC_A_BASE + (uint32_t)st * TC_A_COLS;
           uint32_t accf = (c % TC_WIN) != 0 ? 1u : 0u;
 #pragma unroll
           for (int p = 0; p < 3; ++p) {
-            const uint32_t at = sa + (p == 2 ? TC_OPER : 0);
-            const uint32_t bt = sa + 2 * TC_OPER + (p == 1 ? TC_OPER : 0);
+            const uint32_t at = ahi + (p == 2 ? 32u : 0u);  // A hi, A hi, A lo
+            const uint32_t bt = sa + (p == 1 ? TC_OPER : 0);  // B hi, B lo, B hi
 #pragma unroll
             for (int ks = 0; ks < 4; ++ks) {
-              mma_tf32(dacc, desc_sw128(at + 32u * ks), desc_sw128(bt + 32u * ks), idesc, accf);
+              mma_tf32_at(dacc, at + 8u * ks, desc_sw128(bt + 32u * ks), idesc, accf);
               accf = 1u;
             }
           }
@@ -225,17 +229,13 @@ __device__ __forceinline__ void tc_tile_pipeline(const FactorArgs& fa, const Src
     //        B' column tid & 63, columns 4 (tid >> 6) .. +4.
     const int row = tid & (TC_M - 1), ga = tid >> 7;
     const int ub = tid & (TC_N - 1), gb = tid >> 6;
-    uint32_t oa0, oa1, ob0, ob1 = 0, ob2 = 0, ob3 = 0;
+    uint32_t ob0, ob1 = 0, ob2 = 0, ob3 = 0;
     if constexpr (Field<T>::complex) {
-      oa0 = sw128_off(row, 4 * ga);
-      oa1 = sw128_off(row, 16 + 4 * ga);
       ob0 = sw128_off(ub, 2 * gb);
       ob1 = sw128_off(ub, 16 + 2 * gb);
       ob2 = sw128_off(TC_N + ub, 2 * gb);
       ob3 = sw128_off(TC_N + ub, 16 + 2 * gb);
     } else {
-      oa0 = sw128_off(row, 8 * ga);
-      oa1 = sw128_off(row, 8 * ga + 4);
       ob0 = sw128_off(ub, 4 * gb);
     }
     constexpr int NA = Field<T>::complex ? 4 : 8;  // A columns per thread
@@ -302,22 +302,36 @@ __device__ __forceinline__ void tc_tile_pipeline(const FactorArgs& fa, const Src
           break;
         }
         unsigned char* stg = sm + st * TC_STAGE;
-        unsigned char* Ah = stg;
-        unsigned char* Al = stg + TC_OPER;
-        unsigned char* Bh = stg + 2 * TC_OPER;
-        unsigned char* Bl = stg + 3 * TC_OPER;
+        unsigned char* Bh = stg;
+        unsigned char* Bl = stg + TC_OPER;
+        // A' hi / lo into this warp's TMEM lanes (row = lane), B' into smem
+        tc_fence_after();  // the stage's previous MMAs (empty barrier) precede these stores
+        const uint32_t tA = tmem + ((uint32_t)(32 * q) << 16) + TC_A_BASE + (uint32_t)st * TC_A_COLS;
         if constexpr (Field<T>::complex) {
-          store_split4(Ah, Al, oa0, va[0].re, va[1].re, va[2].re, va[3].re);  // Re(A): K' 0..15
-          store_split4(Ah, Al, oa1, va[0].im, va[1].im, va[2].im, va[3].im);  // Im(A): K' 16..31
-          store_split2(Bh, Bl, ob0, vb[0].re, vb[1].re);                      // Re out:  Gr
-          store_split2(Bh, Bl, ob1, -vb[0].im, -vb[1].im);                    //         -Gi
-          store_split2(Bh, Bl, ob2, vb[0].im, vb[1].im);                      // Im out:  Gi
-          store_split2(Bh, Bl, ob3, vb[0].re, vb[1].re);                      //          Gr
+          float h[8], l[8];
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) {
+            split_tf32(va[jj].re, h[jj], l[jj]);
+            split_tf32(va[jj].im, h[4 + jj], l[4 + jj]);
+          }
+          tmem_st4(tA + 4u * ga, h[0], h[1], h[2], h[3]);              // Re(A): K' 0..15
+          tmem_st4(tA + 16u + 4u * ga, h[4], h[5], h[6], h[7]);        // Im(A): K' 16..31
+          tmem_st4(tA + 32u + 4u * ga, l[0], l[1], l[2], l[3]);
+          tmem_st4(tA + 48u + 4u * ga, l[4], l[5], l[6], l[7]);
+          store_split2(Bh, Bl, ob0, vb[0].re, vb[1].re);                // Re out:  Gr
+          store_split2(Bh, Bl, ob1, -vb[0].im, -vb[1].im);              //         -Gi
+          store_split2(Bh, Bl, ob2, vb[0].im, vb[1].im);                // Im out:  Gi
+          store_split2(Bh, Bl, ob3, vb[0].re, vb[1].re);                //          Gr
         } else {
-          store_split4(Ah, Al, oa0, va[0], va[1], va[2], va[3]);
-          store_split4(Ah, Al, oa1, va[4], va[5], va[6], va[7]);
+          float h[8], l[8];
+#pragma unroll
+          for (int jj = 0; jj < 8; ++jj) split_tf32(va[jj], h[jj], l[jj]);
+          tmem_st8(tA + 8u * ga, h);
+          tmem_st8(tA + 32u + 8u * ga, l);
           store_split4(Bh, Bl, ob0, vb[0], vb[1], vb[2], vb[3]);
         }
+        tmem_wait_st();
+        tc_fence_before();
         fence_proxy_async_smem();
         mbar_arrive(&full[st]);
         // window w - 1 is two chunks behind: promote it before the MMA warp
