@@ -398,65 +398,6 @@ __device__ void block_argmax(double& v, int& idx, double* red_v, int* red_i) {
 // Packed lower-triangle index of (i, j), i >= j, in a pw x pw block.
 __device__ __forceinline__ int pk(int i, int j, int pw) { return j * pw - (j * (j - 1)) / 2 + (i - j); }
 
-// Apply one recorded pivot step of a block to R deep rows held in smem
-// (column-major, stride R): the exact per-row op sequence of
-// apply_bk_panel_trailing.
-template <typename T, int NT>
-__device__ void replay_rows(T* X, int R, int rows, int kb, int ke, int nb, const T* __restrict__ snap,
-                            const int* __restrict__ swaps, const T* __restrict__ d, const T* __restrict__ dsub,
-                            const unsigned char* __restrict__ kind) {
-  using F = Field<T>;
-  const int pw = ke - kb;
-  int k = 0;
-  while (k < pw) {
-    int kp = swaps[k];
-    bool two = kind[k] == 1;
-    if (kp >= 0) {
-      int src = two ? k + 1 : k;
-      for (int r = threadIdx.x; r < rows; r += NT) {
-        T t = X[src * R + r];
-        X[src * R + r] = X[(kp - kb) * R + r];
-        X[(kp - kb) * R + r] = t;
-      }
-      __syncthreads();
-    }
-    if (two) {
-      T d11 = d[k], d21 = dsub[k], d22 = d[k + 1];
-      T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
-      T detinv = F::recip(det);
-      int ncols = pw - (k + 2);
-      for (int e = threadIdx.x; e < ncols * rows; e += NT) {
-        int j = k + 2 + e / rows, r = e % rows;
-        T l1 = snap[k * nb + j], l2 = snap[(k + 1) * nb + j];
-        T x = X[j * R + r];
-        x = F::sub(x, F::mul(X[k * R + r], l1));
-        x = F::sub(x, F::mul(X[(k + 1) * R + r], l2));
-        X[j * R + r] = x;
-      }
-      __syncthreads();
-      for (int r = threadIdx.x; r < rows; r += NT) {
-        T wik = X[k * R + r], wik1 = X[(k + 1) * R + r];
-        X[k * R + r] = F::mul(F::sub(F::mul(d22, wik), F::mul(d21, wik1)), detinv);
-        X[(k + 1) * R + r] = F::mul(F::sub(F::mul(d11, wik1), F::mul(d21, wik)), detinv);
-      }
-      __syncthreads();
-      k += 2;
-    } else {
-      T dinv = F::recip(d[k]);
-      int ncols = pw - (k + 1);
-      for (int e = threadIdx.x; e < ncols * rows; e += NT) {
-        int j = k + 1 + e / rows, r = e % rows;
-        T w = snap[k * nb + j];
-        if (!F::is_zero(w)) X[j * R + r] = F::sub(X[j * R + r], F::mul(X[k * R + r], w));
-      }
-      __syncthreads();
-      for (int r = threadIdx.x; r < rows; r += NT) X[k * R + r] = F::mul(X[k * R + r], dinv);
-      __syncthreads();
-      k += 1;
-    }
-  }
-}
-
 // Warp-per-row replay: lane l holds columns l + 32*j (j < NS) of one deep
 // row in registers; every pivot step's broadcast / interchange goes through
 // shuffles, so a warp replays a whole row with no block barrier.  The
@@ -536,18 +477,20 @@ __device__ ReplayProg<T> load_replay_prog(unsigned char* mem, int pw, int nb, co
   return P;
 }
 
-// Replay a block's pivot steps on NR rows held by one warp (x[row][slot],
-// column = lane + 32 slot): the swaps, then per pivot the elimination of the
-// later columns with the snapshot multipliers and the scaling by the inverse
-// pivot block.  The rows are independent, so the NR dependency chains
-// interleave; each row sees the same operation sequence as a lone row.
+// Replay pivot steps [k_begin, k_end) of a block on NR rows held by one warp
+// (x[row][slot], column = lane + 32 slot): the swaps, then per pivot the
+// elimination of the later columns with the snapshot multipliers and the
+// scaling by the inverse pivot block.  S holds snapshot rows k_begin ..
+// k_end - 1 (row stride `lds`).  The rows are independent, so the NR
+// dependency chains interleave; each row sees the same operation sequence as
+// a lone row.
 template <typename T, int NS, int NR>
-__device__ void replay_rows_warp(T (&x)[NR][NS], int pw, int nb, const T* __restrict__ snap, int kb,
+__device__ void replay_rows_warp(T (&x)[NR][NS], int pw, const T* S, int lds, int k_begin, int k_end, int kb,
                                  const ReplayProg<T>& P) {
   using F = Field<T>;
   const int lane = threadIdx.x & 31;
-  int k = 0;
-  while (k < pw) {
+  int k = k_begin;
+  while (k < k_end) {
     const int kp = P.sw[k];
     const bool two = P.kd[k] == 1;
     if (kp >= 0) {
@@ -570,7 +513,7 @@ __device__ void replay_rows_warp(T (&x)[NR][NS], int pw, int nb, const T* __rest
         for (int j = 0; j < NS; ++j) {
           const int col = lane + 32 * j;
           if (col >= k + 2 && col < pw) {
-            const T l1 = snap[k * nb + col], l2 = snap[(k + 1) * nb + col];
+            const T l1 = S[(k - k_begin) * lds + col], l2 = S[(k + 1 - k_begin) * lds + col];
             T v = F::sub(x[r][j], F::mul(xk, l1));
             x[r][j] = F::sub(v, F::mul(xk1, l2));
           }
@@ -589,7 +532,7 @@ __device__ void replay_rows_warp(T (&x)[NR][NS], int pw, int nb, const T* __rest
         for (int j = 0; j < NS; ++j) {
           const int col = lane + 32 * j;
           if (col > k && col < pw) {
-            const T w = snap[k * nb + col];
+            const T w = S[(k - k_begin) * lds + col];
             if (!F::is_zero(w)) x[r][j] = F::sub(x[r][j], F::mul(xk, w));
           }
         }
@@ -600,10 +543,39 @@ __device__ void replay_rows_warp(T (&x)[NR][NS], int pw, int nb, const T* __rest
   }
 }
 
+// Snapshot rows staged per slice of pivot steps (one more when a 2x2 pivot
+// straddles the slice end).
+constexpr int REPLAY_SL = 16;
+
+// All of a block's pivot steps on the warp's rows, the snapshot multipliers
+// read from shared memory: per slice of REPLAY_SL steps the CTA copies the
+// slice's snapshot rows (all columns < pw, stride nb) into S, then every warp
+// replays those steps.  S holds (REPLAY_SL + 1) x nb elements; every thread
+// of the CTA calls this (it synchronises the block).
+template <typename T, int NT, int NS, int NR>
+__device__ void replay_rows_sliced(T (&x)[NR][NS], int pw, int nb, const T* __restrict__ snap, int kb,
+                                   const ReplayProg<T>& P, T* S) {
+  for (int k0 = 0; k0 < pw;) {
+    int k1 = min(k0 + REPLAY_SL, pw);
+    if (k1 < pw && P.kd[k1 - 1] == 1) ++k1;
+    __syncthreads();
+    const int cnt = (k1 - k0) * pw;
+    for (int e = threadIdx.x; e < cnt; e += NT) {
+      const int r = e / pw, c = e - r * pw;
+      S[r * nb + c] = snap[(long long)(k0 + r) * nb + c];
+    }
+    __syncthreads();
+    replay_rows_warp<T, NS, NR>(x, pw, S, nb, k0, k1, kb, P);
+    k0 = k1;
+  }
+  __syncthreads();
+}
+
 // Replay a block's pivot steps on deep rows [r_begin, r_end) of a panel:
 // rows staged through shared memory (32 rows x pw, padded stride) so both
 // the global loads / stores and the per-row register fills are conflict-free;
-// each warp replays its 32 / NW rows together.  `prog` holds the program.
+// each warp replays its 32 / NW rows together.  `P` holds the program.  While
+// the rows sit in registers the staging buffer X carries the snapshot slices.
 template <typename T, int NT>
 __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int nb, int r_begin, int r_end,
                                  const T* __restrict__ snap, const ReplayProg<T>& P, T* X) {
@@ -630,7 +602,7 @@ __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int n
           const int col = lane + 32 * j, r = warp + NW * i;
           x[i][j] = (col < pw && r < rows) ? X[col * LDX + r] : Field<T>::zero();
         }
-      replay_rows_warp<T, 2, NR>(x, pw, nb, snap, kb, P);
+      replay_rows_sliced<T, NT, 2, NR>(x, pw, nb, snap, kb, P, X);
 #pragma unroll
       for (int i = 0; i < NR; ++i)
 #pragma unroll
@@ -647,7 +619,7 @@ __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int n
           const int col = lane + 32 * j, r = warp + NW * i;
           x[i][j] = (col < pw && r < rows) ? X[col * LDX + r] : Field<T>::zero();
         }
-      replay_rows_warp<T, 4, NR>(x, pw, nb, snap, kb, P);
+      replay_rows_sliced<T, NT, 4, NR>(x, pw, nb, snap, kb, P, X);
 #pragma unroll
       for (int i = 0; i < NR; ++i)
 #pragma unroll
