@@ -195,9 +195,10 @@ int rslab_factor_profile(rslab_fac_handle* fac, double* kind_ms, int64_t* kind_l
 int rslab_solve_profile(rslab_fac_handle* fac, int64_t nrhs, double* kind_ms, int64_t* kind_launches);
 /* Per-launch rows of the handle's last factor/solve profile: launch kind
  * (0 cmod, 1 getf2, 2 deep replay, 3 panel Schur, 4 forward diagonal,
- * 5 forward push, 6 backward dots, 7 backward diagonal, 8/9 blocked forward
- * diagonal/update, 10/11 blocked backward diagonal/update, 12 forward
- * gather, 13 tensor-core cmod, -1 other), grid
+ * 5 forward push, 6 backward dots, 7 backward diagonal, 8-11 unused, 12
+ * forward gather, 13 tensor-core cmod, 14 G = L21 D, 15 diagonal-block
+ * inverses, 16 backward partial-sum reduction, 17 tensor-core panel Schur,
+ * 18/19 forward/backward block-chain solve, 20 backward gather, -1 other), grid
  * size and device ms.  *count = rows available; at most cap are written.
  * A measurement aid with no reference counterpart. */
 int rslab_profile_trace(const rslab_fac_handle* fac, int64_t cap, int32_t* kind, int32_t* grid, float* ms,

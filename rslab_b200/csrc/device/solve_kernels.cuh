@@ -8,12 +8,12 @@
 //   e : pivot order, e = first_col(s) + pivot position inside s.
 // Forward:  per level, k_fwd_gather pulls every descendant's push
 //           U_k = L21_k z_k into the columns of s (update-list order, no
-//           atomics), k_fwd_diag (narrow) or k_ftrsv_blk/upd (wide) solve the
-//           unit-lower diagonal block in pivot order, and k_fwd_push forms
-//           U_s; D^-1 follows the whole sweep (k_dsolve).
-// Backward: per level (root first), k_bwd dots each column of s against the
-//           already-solved rows (own pivots in e order, ancestors in g order)
-//           and back-substitutes the diagonal block.
+//           atomics), k_fwd_diag (narrow) or k_chain (wide, wave_solve.cuh)
+//           solve the unit-lower diagonal block in pivot order, and
+//           k_stream forms U_s; D^-1 follows the whole sweep (k_dsolve).
+// Backward: per level (root first), k_bwd_gather / k_stream form the
+//           off-diagonal dots against the ancestors' x, then k_bwd (narrow)
+//           or k_chain (wide) back-substitute the diagonal block.
 // Reference: solve_ldlt_block (src/dense/ldlt_generic.rs:618-714).
 #pragma once
 
@@ -26,7 +26,6 @@ constexpr int RHS_MAX = 16;  // right-hand sides per pass (larger counts loop)
 constexpr int SB = 32;       // diagonal-block edge of the in-CTA substitutions
 constexpr int SOLVE_BIG = 128;  // wider supernodes use the multi-CTA blocked diagonal solves
 constexpr int TB = 64;          // block edge of the multi-CTA diagonal solves
-constexpr int BWD_ROWS = 1024;  // off-diagonal rows per backward-dot task
 
 struct SolveArgs {
   const int* sn_first;
@@ -55,6 +54,7 @@ struct SolveArgs {
   const void* linv;       // inverses of the TB x TB diagonal blocks of wide supernodes
   const long long* linv_off;
   void* Wp;               // slots x 32 x ld partial sums of the split backward dots
+  int* wstate;            // wavefront solves: status, abort word, ticket counters, block flags
   int ld;     // row stride (total rhs count)
   int c0;     // first rhs column of this pass
   int nrhs;   // rhs columns in this pass (<= RHS_MAX)
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(SOLVE_NT) k_fwd_gather(SolveArgs a, const int2
 
 // Forward diagonal block of a narrow supernode s (ncol <= SOLVE_BIG, one
 // CTA): Z already holds the gathered y in pivot order; solve in place.
-// Wider supernodes use k_ftrsv_blk / k_ftrsv_upd.
+// Wider supernodes use the block chain (k_chain).
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_fwd_diag(SolveArgs a, const int* __restrict__ tasks) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -216,188 +216,6 @@ __global__ void __launch_bounds__(SOLVE_NT) k_fwd_diag(SolveArgs a, const int* _
   const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
   T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
   fwd_block_range<T>(a, L, nrow, Z, 0, ncol, 0, red, Ls, zb);
-}
-
-// acc[m] = sum_{q in [q0, q1)} L[r, q] * Z[q][c] for the 64 panel rows
-// r = r0 + (tid & 63) (rows >= r_end read as zero) and c = (tid >> 6) + 4 m.
-// 32-column chunks of L and the matching 32 rows of Z are staged in shared
-// memory (coalesced along r); each thread adds q in ascending order.
-template <typename T>
-__device__ void rows_dot_z(const T* __restrict__ L, int nrow, int r0, int r_end, int q0, int q1,
-                           const T* __restrict__ Z, int ld, int nrhs, T (&acc)[RHS_MAX / 4], T* Ls, T* Zs) {
-  using F = Field<T>;
-  const int tid = threadIdx.x, rl = tid & 63, cg = tid >> 6;
-#pragma unroll
-  for (int m = 0; m < RHS_MAX / 4; ++m) acc[m] = F::zero();
-  for (int qc = q0; qc < q1; qc += 32) {
-    const int nq = min(32, q1 - qc);
-#pragma unroll
-    for (int e = tid; e < 64 * 32; e += SOLVE_NT) {
-      const int r = e & 63, q = e >> 6;
-      Ls[q * 64 + r] = (q < nq && r0 + r < r_end) ? L[(r0 + r) + (long long)(qc + q) * nrow] : F::zero();
-    }
-#pragma unroll
-    for (int e = tid; e < 32 * RHS_MAX; e += SOLVE_NT) {
-      const int q = e / RHS_MAX, c = e % RHS_MAX;
-      Zs[e] = (q < nq && c < nrhs) ? Z[(long long)(qc + q) * ld + c] : F::zero();
-    }
-    __syncthreads();
-    for (int q = 0; q < nq; ++q) {
-      const T l = Ls[q * 64 + rl];
-#pragma unroll
-      for (int m = 0; m < RHS_MAX / 4; ++m) {
-        const int c = cg + 4 * m;
-        if (c < nrhs) acc[m] = F::fma_(l, Zs[q * RHS_MAX + c], acc[m]);
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// Forward push of supernode s, off-diagonal rows [ncol + r0, ncol + r0 + 64):
-// U_s = L21_s z_s (rows_dot_z over all own columns).
-template <typename T>
-__global__ void __launch_bounds__(SOLVE_NT) k_fwd_push(SolveArgs a, const int2* __restrict__ tasks) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* Ls = reinterpret_cast<T*>(smem_raw);  // 32 x 64
-  T* Zs = Ls + 32 * 64;                    // 32 x RHS_MAX
-  const int2 tk = tasks[blockIdx.x];
-  const int s = tk.x, r0 = tk.y;
-  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
-  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
-  const T* Z = reinterpret_cast<const T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  T* Us = reinterpret_cast<T*>(a.U) + a.c0 + a.uoff[s] * a.ld;
-  T acc[RHS_MAX / 4];
-  rows_dot_z<T>(L, nrow, ncol + r0, nrow, 0, ncol, Z, a.ld, a.nrhs, acc, Ls, Zs);
-  const int r = ncol + r0 + (threadIdx.x & 63), cg = threadIdx.x >> 6;
-  if (r < nrow)
-#pragma unroll
-    for (int m = 0; m < RHS_MAX / 4; ++m) {
-      const int c = cg + 4 * m;
-      if (c < a.nrhs) Us[(long long)(r - ncol) * a.ld + c] = acc[m];
-    }
-}
-
-// out[p][c] = sum_{r in [r_begin, r_end)} L[r, p] * V(r)[c] for the 32
-// columns p in [p0, p0+32) of a panel, V(r) = the RHS row of panel row r
-// (gathered through rs for ancestor rows).  32-row chunks of V and of the
-// L tile are staged in shared memory and reused by all 32 columns; thread t
-// owns column t % 32 and right-hand sides t / 32 + 8 i; fixed summation order.
-template <typename T, bool GATHER>
-__device__ void dot_cols_tile(const T* __restrict__ L, int nrow, int p0, int ncols, int r_begin, int r_end,
-                              const T* __restrict__ V, const int* __restrict__ rss, int ld, int nrhs,
-                              T (&acc)[RHS_MAX / 8], T* Ls, T* Vs) {
-  using F = Field<T>;
-  constexpr int NRC = RHS_MAX / 8;
-  const int tid = threadIdx.x, pc = tid & 31, cg = tid >> 5;
-#pragma unroll
-  for (int q = 0; q < NRC; ++q) acc[q] = F::zero();
-  for (int r0 = r_begin; r0 < r_end; r0 += 32) {
-    const int rows = min(32, r_end - r0);
-#pragma unroll
-    for (int e = tid; e < 32 * 32; e += SOLVE_NT) {
-      const int c = e >> 5, r = e & 31;  // column c, row r: coalesced along r
-      Ls[r * 33 + c] = (r < rows && c < ncols) ? L[(r0 + r) + (long long)(p0 + c) * nrow] : F::zero();
-    }
-#pragma unroll
-    for (int e = tid; e < 32 * RHS_MAX; e += SOLVE_NT) {
-      const int r = e / RHS_MAX, c = e % RHS_MAX;
-      T v = F::zero();
-      if (r < rows && c < nrhs) {
-        const long long row = GATHER ? (long long)rss[r0 + r] : (long long)(r0 + r);
-        v = V[row * ld + c];
-      }
-      Vs[e] = v;
-    }
-    __syncthreads();
-    for (int r = 0; r < rows; ++r) {
-      const T l = Ls[r * 33 + pc];
-#pragma unroll
-      for (int q = 0; q < NRC; ++q) {
-        const int c = cg + 8 * q;
-        if (c < nrhs) acc[q] = F::fma_(l, Vs[r * RHS_MAX + c], acc[q]);
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// Backward off-diagonal dots of supernode s, pivot columns [c0, c0+32),
-// off-diagonal rows [ncol + r0, ncol + r0 + BWD_ROWS): sum_r L[r, p] x[g_r].
-// Task (s, c0, r0, slot): slot < 0 (the only row chunk) writes the result —
-// to Wb for narrow supernodes, subtracted from Z for wide ones (solved by
-// the blocked kernels); otherwise the partial sum goes to slot `slot`.
-template <typename T>
-__global__ void __launch_bounds__(SOLVE_NT) k_bwd_off(SolveArgs a, const int4* __restrict__ tasks) {
-  using F = Field<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* Ls = reinterpret_cast<T*>(smem_raw);  // 32 x 33
-  T* Vs = Ls + 32 * 33;                    // 32 x RHS_MAX
-  const int4 tk = tasks[blockIdx.x];
-  const int s = tk.x, c0 = tk.y, r0 = tk.z, slot = tk.w;
-  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
-  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
-  const int* rss = a.rs + a.sn_rsoff[s];
-  const T* X = reinterpret_cast<const T*>(a.Xg) + a.c0;
-  const int cols_here = min(32, ncol - c0);
-  const int rb = ncol + r0, re = min(nrow, rb + BWD_ROWS);
-  T acc[RHS_MAX / 8];
-  dot_cols_tile<T, true>(L, nrow, c0, cols_here, rb, re, X, rss, a.ld, a.nrhs, acc, Ls, Vs);
-  const int pc = threadIdx.x & 31, cg = threadIdx.x >> 5;
-  if (pc >= cols_here) return;
-  const int p = c0 + pc;
-  if (slot >= 0) {
-    T* part = reinterpret_cast<T*>(a.Wp) + (long long)slot * 32 * a.ld;
-#pragma unroll
-    for (int q = 0; q < RHS_MAX / 8; ++q) {
-      const int c = cg + 8 * q;
-      if (c < a.nrhs) part[pc * a.ld + c] = acc[q];
-    }
-    return;
-  }
-  T* Wb = reinterpret_cast<T*>(a.Wb) + a.c0 + (long long)first * a.ld;
-  T* Zs = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-#pragma unroll
-  for (int q = 0; q < RHS_MAX / 8; ++q) {
-    const int c = cg + 8 * q;
-    if (c >= a.nrhs) continue;
-    if (ncol > SOLVE_BIG) {
-      T* z = Zs + (long long)p * a.ld + c;
-      *z = F::sub(*z, acc[q]);
-    } else {
-      Wb[(long long)p * a.ld + c] = acc[q];
-    }
-  }
-}
-
-// Reduce the row-chunk partial sums of one (s, c0) in chunk order and write
-// them like the single-chunk case.  Task (s, c0, slot0, nchunks).
-template <typename T>
-__global__ void __launch_bounds__(SOLVE_NT) k_bwd_off_reduce(SolveArgs a, const int4* __restrict__ tasks) {
-  using F = Field<T>;
-  const int4 tk = tasks[blockIdx.x];
-  const int s = tk.x, c0 = tk.y, slot0 = tk.z, nch = tk.w;
-  const int first = a.sn_first[s], ncol = a.sn_ncol[s];
-  const int cols_here = min(32, ncol - c0);
-  const int pc = threadIdx.x & 31, cg = threadIdx.x >> 5;
-  if (pc >= cols_here) return;
-  const int p = c0 + pc;
-  const T* part = reinterpret_cast<const T*>(a.Wp) + (long long)slot0 * 32 * a.ld;
-  T* Wb = reinterpret_cast<T*>(a.Wb) + a.c0 + (long long)first * a.ld;
-  T* Zs = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-#pragma unroll
-  for (int q = 0; q < RHS_MAX / 8; ++q) {
-    const int c = cg + 8 * q;
-    if (c >= a.nrhs) continue;
-    T v = part[pc * a.ld + c];
-    for (int k = 1; k < nch; ++k) v = F::add(v, part[(long long)k * 32 * a.ld + pc * a.ld + c]);
-    if (ncol > SOLVE_BIG) {
-      T* z = Zs + (long long)p * a.ld + c;
-      *z = F::sub(*z, v);
-    } else {
-      Wb[(long long)p * a.ld + c] = v;
-    }
-  }
 }
 
 // Inverse of the unit lower TB x TB diagonal block [j0, j0+nb) of a wide
@@ -439,90 +257,6 @@ __global__ void __launch_bounds__(TB) k_diag_inv(const int2* __restrict__ tasks,
   for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
     const int i = e % TB, jj = e / TB;
     out[i + (long long)jj * TB] = Xs[i * (TB + 1) + jj];
-  }
-}
-
-// Blocked forward solve of a wide supernode, block [j0, j0+nb): Z holds y
-// minus the earlier blocks; z = Linv y with the precomputed inverse
-// (thread: row i = tid % TB, right-hand sides tid / TB + 4 m; k ascending).
-template <typename T>
-__device__ void fwd_blk_inv(const SolveArgs& a, int s, int j0, unsigned char* smem_raw) {
-  using F = Field<T>;
-  T* Ls = reinterpret_cast<T*>(smem_raw);  // TB x (TB + 1): Ls[k * (TB + 1) + i] = Linv[i, k]
-  T* Ys = Ls + TB * (TB + 1);              // TB x RHS_MAX
-  const int first = a.sn_first[s], ncol = a.sn_ncol[s];
-  const int nb = min(TB, ncol - j0);
-  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)(first + j0) * a.ld;
-  const T* Li = reinterpret_cast<const T*>(a.linv) + a.linv_off[s] + (long long)(j0 / TB) * TB * TB;
-#pragma unroll
-  for (int e = threadIdx.x; e < TB * TB; e += SOLVE_NT) {
-    const int i = e % TB, k = e / TB;  // column-major read: Linv[i, k]
-    Ls[k * (TB + 1) + i] = Li[i + (long long)k * TB];
-  }
-#pragma unroll
-  for (int e = threadIdx.x; e < TB * RHS_MAX; e += SOLVE_NT) {
-    const int k = e / RHS_MAX, c = e % RHS_MAX;
-    Ys[e] = (k < nb && c < a.nrhs) ? Z[(long long)k * a.ld + c] : F::zero();
-  }
-  __syncthreads();
-  const int i = threadIdx.x % TB, cg = threadIdx.x / TB;
-  constexpr int NCG = SOLVE_NT / TB;
-  T acc[RHS_MAX / NCG];
-#pragma unroll
-  for (int m = 0; m < RHS_MAX / NCG; ++m) acc[m] = F::zero();
-  if (i < nb)
-    for (int k = 0; k <= i; ++k) {
-      const T l = Ls[k * (TB + 1) + i];
-#pragma unroll
-      for (int m = 0; m < RHS_MAX / NCG; ++m) acc[m] = F::fma_(l, Ys[k * RHS_MAX + cg + NCG * m], acc[m]);
-    }
-  if (i < nb)
-#pragma unroll
-    for (int m = 0; m < RHS_MAX / NCG; ++m) {
-      const int c = cg + NCG * m;
-      if (c < a.nrhs) Z[(long long)i * a.ld + c] = acc[m];
-    }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(SOLVE_NT) k_ftrsv_blk(SolveArgs a, const int4* __restrict__ tasks) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int4 tk = tasks[blockIdx.x];
-  fwd_blk_inv<T>(a, tk.x, tk.y, smem_raw);
-}
-
-// Right-looking update after forward block [j0, j0+64) of a wide supernode:
-// Z[r] -= sum_{q in block} L[r, q] z[q] for own rows r in [r0, r0+64); task
-// (s, j0, r0, solve_next): with solve_next the rows are the next block's,
-// which this CTA then solves.
-template <typename T>
-__global__ void __launch_bounds__(SOLVE_NT) k_ftrsv_upd(SolveArgs a, const int4* __restrict__ tasks) {
-  using F = Field<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* Ls = reinterpret_cast<T*>(smem_raw);
-  T* Zs = Ls + 32 * 64;
-  const int4 tk = tasks[blockIdx.x];
-  const int s = tk.x, j0 = tk.y, r0 = tk.z;
-  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
-  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
-  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  T acc[RHS_MAX / 4];
-  rows_dot_z<T>(L, nrow, r0, ncol, j0, min(j0 + TB, ncol), Z, a.ld, a.nrhs, acc, Ls, Zs);
-  const int r = r0 + (threadIdx.x & 63), cg = threadIdx.x >> 6;
-  if (r < ncol)
-#pragma unroll
-    for (int m = 0; m < RHS_MAX / 4; ++m) {
-      const int c = cg + 4 * m;
-      if (c < a.nrhs) {
-        T* z = Z + (long long)r * a.ld + c;
-        *z = F::sub(*z, acc[m]);
-      }
-    }
-  // The CTA that owns the next block's rows has just completed their update:
-  // it solves that block too (no separate launch on the critical path).
-  if (tk.w) {
-    __syncthreads();
-    fwd_blk_inv<T>(a, s, r0, smem_raw);
   }
 }
 
@@ -599,103 +333,6 @@ __device__ void bwd_block_range(const SolveArgs& a, const T* __restrict__ L, int
   }
 }
 
-// Blocked backward solve of a wide supernode, block [jb, jb+nb): Z holds w
-// minus the off-diagonal and later blocks' contributions; v = Linv^T w with
-// the precomputed inverse (staged in shared memory), then the block's final
-// values go to Z and to X in g order.
-template <typename T>
-__device__ void bwd_blk_inv(const SolveArgs& a, int s, int jb, unsigned char* smem_raw) {
-  using F = Field<T>;
-  T* Ls = reinterpret_cast<T*>(smem_raw);  // TB x (TB + 1): Ls[k * (TB + 1) + i] = Linv[k, i]
-  T* Ws = Ls + TB * (TB + 1);              // TB x RHS_MAX
-  const int first = a.sn_first[s], ncol = a.sn_ncol[s];
-  const int nb = min(TB, ncol - jb);
-  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)(first + jb) * a.ld;
-  T* Xw = reinterpret_cast<T*>(a.Xg) + a.c0;
-  const int* lp = a.lperm + first + jb;
-  const T* Li = reinterpret_cast<const T*>(a.linv) + a.linv_off[s] + (long long)(jb / TB) * TB * TB;
-#pragma unroll
-  for (int e = threadIdx.x; e < TB * TB; e += SOLVE_NT) {
-    const int k = e % TB, i = e / TB;  // column-major read: Linv[k, i]
-    Ls[k * (TB + 1) + i] = Li[k + (long long)i * TB];
-  }
-#pragma unroll
-  for (int e = threadIdx.x; e < TB * RHS_MAX; e += SOLVE_NT) {
-    const int k = e / RHS_MAX, c = e % RHS_MAX;
-    Ws[e] = (k < nb && c < a.nrhs) ? Z[(long long)k * a.ld + c] : F::zero();
-  }
-  __syncthreads();
-  const int i = threadIdx.x % TB, cg = threadIdx.x / TB;
-  constexpr int NCG = SOLVE_NT / TB;
-  T acc[RHS_MAX / NCG];
-#pragma unroll
-  for (int m = 0; m < RHS_MAX / NCG; ++m) acc[m] = F::zero();
-  if (i < nb)
-    for (int k = i; k < nb; ++k) {
-      const T l = Ls[k * (TB + 1) + i];
-#pragma unroll
-      for (int m = 0; m < RHS_MAX / NCG; ++m) acc[m] = F::fma_(l, Ws[k * RHS_MAX + cg + NCG * m], acc[m]);
-    }
-  if (i < nb) {
-    T* xo = Xw + (long long)(first + lp[i]) * a.ld;
-#pragma unroll
-    for (int m = 0; m < RHS_MAX / NCG; ++m) {
-      const int c = cg + NCG * m;
-      if (c < a.nrhs) {
-        Z[(long long)i * a.ld + c] = acc[m];
-        xo[c] = acc[m];
-      }
-    }
-  }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(SOLVE_NT) k_btrsv_blk(SolveArgs a, const int4* __restrict__ tasks) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int4 tk = tasks[blockIdx.x];
-  bwd_blk_inv<T>(a, tk.x, tk.y, smem_raw);
-}
-
-// Right-looking backward update after block [jb, jb+64) of a wide supernode:
-// v[p] -= sum_{r in block} L[r, p] v[r] for columns p in [c0, c0+32) < jb;
-// task (s, jb, c0, solve_prev): with solve_prev, c0 = jb - 64 and the task
-// covers the whole previous block, which it then solves.
-template <typename T>
-__global__ void __launch_bounds__(SOLVE_NT) k_btrsv_upd(SolveArgs a, const int4* __restrict__ tasks) {
-  using F = Field<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* Ls = reinterpret_cast<T*>(smem_raw);
-  T* Vs = Ls + 32 * 33;
-  const int4 tk = tasks[blockIdx.x];
-  const int s = tk.x, jb = tk.y, c0 = tk.z, solve_prev = tk.w;
-  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
-  const int je = min(jb + TB, ncol);
-  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
-  T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  const int pc = threadIdx.x & 31, cg = threadIdx.x >> 5;
-  // one 32-column chunk, or (solve_prev) the two chunks of the previous block
-  for (int cc = c0; cc < (solve_prev ? jb : c0 + 32); cc += 32) {
-    const int cols_here = min(32, jb - cc);
-    T acc[RHS_MAX / 8];
-    dot_cols_tile<T, false>(L, nrow, cc, cols_here, jb, je, Z, nullptr, a.ld, a.nrhs, acc, Ls, Vs);
-    if (pc < cols_here) {
-      const int p = cc + pc;
-#pragma unroll
-      for (int q = 0; q < RHS_MAX / 8; ++q) {
-        const int c = cg + 8 * q;
-        if (c >= a.nrhs) continue;
-        T* z = Z + (long long)p * a.ld + c;
-        *z = F::sub(*z, acc[q]);
-      }
-    }
-  }
-  // The previous block's columns are now complete: solve it here.
-  if (solve_prev) {
-    __syncthreads();
-    bwd_blk_inv<T>(a, s, c0, smem_raw);
-  }
-}
-
 // D^-1 on the e-indexed forward solution, after the whole forward sweep
 // (ancestors' gathers need z, not D^-1 z).  1x1 and 2x2 blocks.
 template <typename T>
@@ -724,7 +361,7 @@ __global__ void k_dsolve(int n, SolveArgs a) {
 }
 
 // Backward solve of a narrow supernode s (one CTA): blocks of 32 pivots
-// from the last; the off-diagonal dots of k_bwd_off (Wb) come first.
+// from the last; the off-diagonal dots (Wb, k_stream) come first.
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_NT) k_bwd(SolveArgs a, const int* __restrict__ tasks) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -734,7 +371,7 @@ __global__ void __launch_bounds__(SOLVE_NT) k_bwd(SolveArgs a, const int* __rest
   const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
   const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
   T* Z = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * a.ld;
-  // Wb is written by k_bwd_off only when the supernode has off-diagonal rows
+  // Wb is written by the dots only when the supernode has off-diagonal rows
   const T* Wb = nrow > ncol ? reinterpret_cast<const T*>(a.Wb) + a.c0 + (long long)first * a.ld : nullptr;
   bwd_block_range<T>(a, L, nrow, Z, Wb, reinterpret_cast<T*>(a.Xg) + a.c0, a.lperm + first, first, 0, ncol, ncol,
                      vb, Ls);

@@ -1,0 +1,471 @@
+// Triangular-solve kernels of the supernodal solve that stream the panels
+// at memory bandwidth, and the dependency-chain solve of the wide
+// supernodes' diagonal blocks.
+//
+// Streaming (k_stream): the forward push U_s = L21_s z_s and the backward
+// off-diagonal dots L21_s^T x_anc.  An item owns 64 outputs and loops over
+// 32-wide reduction units; each unit's 2048-element panel tile and its 32
+// right-hand-side rows are copied global -> shared with cp.async (zero
+// filled outside the panel), `st_stages<T>()` units in flight, one CTA
+// barrier per unit.  Tile layouts keep every lane on consecutive or odd
+// strided shared memory:
+//   forward  : 64 output rows x 32 reduction columns, S[q * 65 + r]
+//   backward : 32 reduction rows x 64 output columns, S[p * 33 + r]
+// Thread (x = tid & 63, g = tid >> 6) owns output x and the reduction slice
+// [8g, 8g + 8) of every unit; the four slice partials are added in order
+// g = 0..3 at the end, so results are deterministic.  The right-hand sides
+// read here are final before the launch (forward: z of this level, solved
+// by an earlier launch; backward: the ancestors' x gathered into a
+// contiguous buffer by k_bwd_gather).
+//
+// Chain (k_chain): a wide supernode (ncol > SOLVE_BIG) is cut into TB = 64
+// column blocks whose solves form a chain (forward: block i needs z of
+// blocks j < i; backward: x of blocks j > i).  One CTA per block:
+//   forward : z_i = Linv_i (y_i - sum_{j<i} L_ij z_j)
+//   backward: x_i = Linv_i^T (w_i - W_i - sum_{j>i, descending} L_ji^T x_j)
+// with Linv_i the precomputed inverse of the unit-lower diagonal block and
+// W_i the off-diagonal dots.  The 64 x 64 tiles stream through shared
+// memory ahead of the chain; z_j / x_j are read (L2 only) after block j's
+// flag.  Items are handed out in ticket order (an atomic counter per launch,
+// not blockIdx) and every item waits only on items with smaller tickets,
+// whose CTAs have therefore started, so the chain progresses whatever the
+// number of resident CTAs.  A finished block is published by one thread
+// after a CTA barrier: fence, then a gpu-scope release store of the flag; a
+// waiting CTA polls with acquire loads a bounded number of times and on
+// timeout raises the launch-wide abort word and a sticky status that the
+// host reads after the solve.
+// Reference: the column-block substitution of solve_ldlt_block
+// (src/dense/ldlt_generic.rs:618-714), reorganised as a dependency chain.
+#pragma once
+
+#include "solve_kernels.cuh"
+
+namespace rsd {
+
+constexpr int WV_NT = 256;
+constexpr long WV_POLL_LIMIT = 1L << 21;  // flag polls before a wait gives up
+constexpr int ST_UNIT = 2112;             // streamed tile elements (max of 32 x 65 and 64 x 33)
+constexpr int CH_UNIT = 64 * 65;          // chain tile elements
+constexpr int BWD_CH = 1024;              // off-diagonal rows per backward-dot item
+
+template <typename T>
+__host__ __device__ constexpr int st_stages() {
+  return sizeof(T) >= 16 ? 3 : 4;
+}
+
+// Right-hand-side buffers are sized by the pass's column count nr (<=
+// RHS_MAX), so a one-column solve keeps several CTAs resident per SM; the
+// kernels are instantiated for NR = 1, 4 and 16 register columns (the
+// smallest NR >= nr runs) so the inner loops carry no dead columns.
+// Streaming: stages of (tile + 32 x nr right-hand sides), then the slice
+// partials (4 x 64 x nr).
+template <typename T>
+__host__ __device__ constexpr size_t st_stage_elems(int nr) {
+  return (size_t)ST_UNIT + 32 * nr;
+}
+template <typename T>
+__host__ __device__ constexpr size_t st_smem_bytes(int nr) {
+  return ((size_t)st_stages<T>() * st_stage_elems<T>(nr) + 4 * 64 * nr) * sizeof(T) + 16;
+}
+// Chain: one tile slot (its copy overlaps the wait for the dependency's
+// flag; after the chain it holds the slice partials), the inverse block,
+// right-hand sides (64 x nr) and the block vector (64 x nr).
+template <typename T>
+__host__ __device__ constexpr size_t ch_smem_bytes(int nr) {
+  return ((size_t)2 * CH_UNIT + 64 * nr + 64 * nr) * sizeof(T) + 16;
+}
+
+// Wave state (ints): [0] sticky status (nonzero after a timed-out wait;
+// cleared by the host when read), then the per-pass region cleared before
+// every pass: [1] abort word, [2, 2 + nchain) ticket counters, then the
+// forward and the backward block flags.
+constexpr int WV_STATE_ABORT = 1;
+constexpr int WV_STATE_CTR = 2;
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async_zfill(void* dst, const void* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES),
+               "r"(valid ? BYTES : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_gpu(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_volatile(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
+
+// L2-only loads of vectors written by other CTAs of the same launch.
+__device__ __forceinline__ double ld_cg(const double* p) { return __ldcg(p); }
+__device__ __forceinline__ float ld_cg(const float* p) { return __ldcg(p); }
+__device__ __forceinline__ c64 ld_cg(const c64* p) {
+  const double2 v = __ldcg(reinterpret_cast<const double2*>(p));
+  return c64{v.x, v.y};
+}
+__device__ __forceinline__ c32 ld_cg(const c32* p) {
+  const float2 v = __ldcg(reinterpret_cast<const float2*>(p));
+  return c32{v.x, v.y};
+}
+
+// The sum of the four slice partials red[(g * 64 + x) * nr + c] in order
+// g = 0..3.
+template <typename T>
+__device__ __forceinline__ T slice_sum(const T* red, int x, int c, int nr) {
+  using F = Field<T>;
+  T s = red[x * nr + c];
+  s = F::add(s, red[(64 + x) * nr + c]);
+  s = F::add(s, red[(128 + x) * nr + c]);
+  return F::add(s, red[(192 + x) * nr + c]);
+}
+
+// ---------------------------------------------------------------------------
+// Streaming items.  Forward push (s, r0, nrb): U rows [r0, r0 + 64 nrb) of s
+// = L[ncol + r, :] z_s, one 64-row block after another (narrow supernodes
+// take several blocks per item so an item streams a few units at least).
+// Backward dots (s, i, r0, slot): for the columns of block i, sum over
+// off-diagonal rows [ncol + r0, ncol + r0 + BWD_CH) of L[r, p] x_anc[r];
+// slot < 0 (the only chunk) writes Wb, else partial sums go to slot `slot`
+// (64 x ld each).
+// ---------------------------------------------------------------------------
+template <typename T, bool FWD>
+struct StItem {
+  const T* L;
+  long long ld;       // panel leading dimension (nrow)
+  int r0, rlim;       // tile rows
+  int c0, clim;       // tile columns
+  const T* V;         // right-hand-side row 0 of the item (row stride a.ld)
+  int vlim;           // right-hand-side rows valid < vlim (relative)
+  int cu;             // forward: column units per 64-row block
+  int nunits;
+};
+
+template <typename T, bool FWD>
+__device__ __forceinline__ StItem<T, FWD> st_item(const SolveArgs& a, int4 tk) {
+  const int s = tk.x;
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
+  StItem<T, FWD> it;
+  it.L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
+  it.ld = nrow;
+  if (FWD) {
+    it.r0 = ncol + tk.y; it.rlim = nrow;
+    it.c0 = 0; it.clim = ncol;
+    it.V = reinterpret_cast<const T*>(a.Ze) + a.c0 + (long long)first * a.ld;
+    it.vlim = ncol;
+    it.cu = (ncol + 31) / 32;
+    const int nrb = min(tk.z, (nrow - it.r0 + 63) / 64);
+    it.nunits = nrb * it.cu;
+  } else {
+    it.r0 = ncol + tk.z; it.rlim = min(nrow, it.r0 + BWD_CH);
+    it.c0 = tk.y * TB; it.clim = ncol;
+    it.V = reinterpret_cast<const T*>(a.U) + a.c0 + (a.uoff[s] + tk.z) * a.ld;
+    it.vlim = it.rlim - it.r0;
+    it.cu = 1;
+    it.nunits = (it.vlim + 31) / 32;
+  }
+  return it;
+}
+
+template <typename T, bool FWD>
+__device__ __forceinline__ void st_issue(T* S, T* Vs, const StItem<T, FWD>& it, int u, int ld, int nr) {
+  int rr0, cc0, vr0;
+  if constexpr (FWD) {
+    const int rb = u / it.cu, cb = u - rb * it.cu;
+    rr0 = it.r0 + 64 * rb; cc0 = 32 * cb; vr0 = 32 * cb;
+  } else {
+    rr0 = it.r0 + 32 * u; cc0 = it.c0; vr0 = 32 * u;
+  }
+#pragma unroll
+  for (int m = 0; m < 2048 / WV_NT; ++m) {
+    const int e = threadIdx.x + WV_NT * m;
+    int r, c, dst;
+    if constexpr (FWD) {
+      r = rr0 + (e & 63); c = cc0 + (e >> 6); dst = (e >> 6) * 65 + (e & 63);
+    } else {
+      r = rr0 + (e & 31); c = cc0 + (e >> 5); dst = (e >> 5) * 33 + (e & 31);
+    }
+    const bool ok = r < it.rlim && c < it.clim;
+    const T* g = ok ? it.L + r + (long long)c * it.ld : it.L;
+    cp_async_zfill<sizeof(T)>(S + dst, g, ok);
+  }
+  for (int e = threadIdx.x; e < 32 * nr; e += WV_NT) {
+    const int k = e / nr, c = e - k * nr, row = vr0 + k;
+    const bool ok = row < it.vlim;
+    const T* g = ok ? it.V + (long long)row * ld + c : it.V;
+    cp_async_zfill<sizeof(T)>(Vs + e, g, ok);
+  }
+}
+
+template <typename T, bool FWD, int NR>
+__global__ void __launch_bounds__(WV_NT) k_stream(SolveArgs a, const int4* __restrict__ tasks) {
+  using F = Field<T>;
+  constexpr int NST = st_stages<T>();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nr = a.nrhs, ld = a.ld;
+  const int SE = (int)st_stage_elems<T>(nr);
+  T* stages = reinterpret_cast<T*>(smem_raw);  // NST x (tile, V)
+  T* red = stages + NST * SE;                  // 4 x 64 x nr
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x;
+  const StItem<T, FWD> it = st_item<T, FWD>(a, tk);
+  const int tid = threadIdx.x, x = tid & 63, g = tid >> 6;
+  T acc[NR];
+#pragma unroll
+  for (int c = 0; c < NR; ++c) acc[c] = F::zero();
+  // slice partials of the finished output block -> U (forward) / Wb / slot
+  auto flush = [&](int rb) {
+#pragma unroll
+    for (int c = 0; c < NR; ++c)
+      if (c < nr) {
+        red[(g * 64 + x) * nr + c] = acc[c];
+        acc[c] = F::zero();
+      }
+    __syncthreads();
+    for (int e = tid; e < 64 * nr; e += WV_NT) {
+      const int r = e / nr, c = e - r * nr;
+      const T v = slice_sum(red, r, c, nr);
+      if (FWD) {
+        const int row = it.r0 + 64 * rb + r;
+        if (row < it.rlim) {
+          T* Us = reinterpret_cast<T*>(a.U) + a.c0 + a.uoff[s] * ld;
+          Us[(long long)(row - a.sn_ncol[s]) * ld + c] = v;
+        }
+      } else if (it.c0 + r < it.clim) {
+        if (tk.w < 0) {
+          T* Wb = reinterpret_cast<T*>(a.Wb) + a.c0 + (long long)a.sn_first[s] * ld;
+          Wb[(long long)(it.c0 + r) * ld + c] = v;
+        } else {
+          T* part = reinterpret_cast<T*>(a.Wp) + (long long)tk.w * 64 * ld;
+          part[(long long)r * ld + c] = v;
+        }
+      }
+    }
+  };
+#pragma unroll 1
+  for (int u = 0; u < NST - 1; ++u) {
+    T* S = stages + u * SE;
+    if (u < it.nunits) st_issue<T, FWD>(S, S + ST_UNIT, it, u, ld, nr);
+    cp_async_commit();
+  }
+#pragma unroll 1
+  for (int u = 0; u < it.nunits; ++u) {
+    if (FWD && u > 0 && u % it.cu == 0) flush(u / it.cu - 1);
+    cp_async_wait<NST - 2>();
+    __syncthreads();  // unit u landed everywhere; unit u - 1's stage and the partials are free
+    {
+      const int un = u + NST - 1;
+      T* Sn = stages + (un % NST) * SE;
+      if (un < it.nunits) st_issue<T, FWD>(Sn, Sn + ST_UNIT, it, un, ld, nr);
+      cp_async_commit();
+    }
+    const T* S = stages + (u % NST) * SE;
+    const T* V = S + ST_UNIT;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int q = 8 * g + k;
+      const T l = FWD ? S[q * 65 + x] : S[x * 33 + q];
+#pragma unroll
+      for (int c = 0; c < NR; ++c)
+        if (c < nr) acc[c] = F::fma_(l, V[q * nr + c], acc[c]);
+    }
+  }
+  cp_async_wait<0>();
+  if (it.nunits > 0) flush(FWD ? (it.nunits - 1) / it.cu : 0);
+}
+
+// Backward: sum the row-chunk partials of (s, block i) in chunk order into
+// Wb.  Task (s, i, slot0, nchunks).
+template <typename T>
+__global__ void __launch_bounds__(WV_NT) k_dots_reduce(SolveArgs a, const int4* __restrict__ tasks) {
+  using F = Field<T>;
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, i = tk.y, slot0 = tk.z, nch = tk.w;
+  const int ncol = a.sn_ncol[s];
+  const int ld = a.ld, nr = a.nrhs;
+  const T* part = reinterpret_cast<const T*>(a.Wp) + (long long)slot0 * 64 * ld;
+  T* Wb = reinterpret_cast<T*>(a.Wb) + a.c0 + (long long)a.sn_first[s] * ld;
+  for (int e = threadIdx.x; e < 64 * nr; e += WV_NT) {
+    const int p = e / nr, c = e - p * nr;
+    if (i * TB + p >= ncol) continue;
+    T v = part[(long long)p * ld + c];
+    for (int k = 1; k < nch; ++k) v = F::add(v, part[((long long)k * 64 + p) * ld + c]);
+    Wb[(long long)(i * TB + p) * ld + c] = v;
+  }
+}
+
+// Backward: the ancestors' x of every off-diagonal row of the level's
+// supernodes, gathered (g order -> row order) into the push buffer U, which
+// the backward dots stream contiguously.  Task (s, r0): rows [r0, r0 + 256).
+template <typename T>
+__global__ void __launch_bounds__(WV_NT) k_bwd_gather(SolveArgs a, const int2* __restrict__ tasks) {
+  const int2 tk = tasks[blockIdx.x];
+  const int s = tk.x;
+  const int ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
+  const int nr = a.nrhs;
+  const int* rss = a.rs + a.sn_rsoff[s];
+  const T* Xg = reinterpret_cast<const T*>(a.Xg) + a.c0;
+  T* U = reinterpret_cast<T*>(a.U) + a.c0 + a.uoff[s] * a.ld;
+  for (int e = threadIdx.x; e < 256 * nr; e += WV_NT) {
+    const int k = e / nr, c = e - k * nr, r = tk.y + k;
+    if (ncol + r >= nrow) continue;
+    U[(long long)r * a.ld + c] = Xg[(long long)rss[ncol + r] * a.ld + c];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Chain items (s, 0 / 1 = forward / backward, block i, first flag of s).
+// ---------------------------------------------------------------------------
+
+// Wait (thread 0) until flag `f` is set; false on timeout or abort.
+__device__ __forceinline__ bool wv_wait(const int* flags, int f, int* state) {
+  for (long it = 0; it < WV_POLL_LIMIT; ++it) {
+    if (ld_acquire_gpu(flags + f) != 0) return true;
+    if (ld_volatile(state + WV_STATE_ABORT) != 0) return false;
+  }
+  atomicExch(state + WV_STATE_ABORT, 1);
+  atomicExch(state, 1);
+  return false;
+}
+
+// Copy the 64 x 64 tile at (r0, c0) of a column-major source (rows < rlim,
+// columns < clim, zero elsewhere) into S[c * 65 + r].
+template <typename T>
+__device__ __forceinline__ void ch_issue(T* S, const T* src, long long ld, int r0, int rlim, int c0, int clim) {
+#pragma unroll
+  for (int m = 0; m < 4096 / WV_NT; ++m) {
+    const int e = threadIdx.x + WV_NT * m;
+    const int r = e & 63, c = e >> 6;
+    const bool ok = r0 + r < rlim && c0 + c < clim;
+    const T* g = ok ? src + (r0 + r) + (long long)(c0 + c) * ld : src;
+    cp_async_zfill<sizeof(T)>(S + c * 65 + r, g, ok);
+  }
+}
+
+// acc[c] += sum over the thread's 16 reduction entries of the 64 x 64 tile
+// S (forward: S[q * 65 + x] = A[x, q]; backward: S[x * 65 + q] = A[q, x])
+// times V[q * nr + c].
+template <typename T, bool FWD, int NR>
+__device__ __forceinline__ void ch_tile_mv(T (&acc)[NR], const T* S, const T* V, int x, int g, int nr) {
+  using F = Field<T>;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const int q = 16 * g + k;
+    const T l = FWD ? S[q * 65 + x] : S[x * 65 + q];
+#pragma unroll
+    for (int c = 0; c < NR; ++c)
+      if (c < nr) acc[c] = F::fma_(l, V[q * nr + c], acc[c]);
+  }
+}
+
+template <typename T, bool FWD, int NR>
+__global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __restrict__ tasks, int ctr, int flag_base) {
+  using F = Field<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int sh_t, sh_abort;
+  const int nr = a.nrhs, ld = a.ld;
+  T* S = reinterpret_cast<T*>(smem_raw);  // dependency tile; later the slice partials (4 x 64 x nr)
+  T* red = S;
+  T* Lv = S + CH_UNIT;                    // the inverse block
+  T* Vs = Lv + CH_UNIT;                   // 64 x nr
+  T* wv = Vs + 64 * nr;                   // 64 x nr
+  const int tid = threadIdx.x, x = tid & 63, g = tid >> 6;
+  if (tid == 0) {
+    sh_t = atomicAdd(a.wstate + WV_STATE_CTR + ctr, 1);
+    sh_abort = 0;
+  }
+  __syncthreads();
+  if (ld_volatile(a.wstate + WV_STATE_ABORT) != 0) return;
+  const int4 tk = tasks[sh_t];
+  const int s = tk.x, i = tk.z, fb = tk.w;
+  int* flags = a.wstate + flag_base + fb;
+  const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
+  const int nblk = (ncol + TB - 1) / TB, nb = min(TB, ncol - i * TB);
+  const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
+  const T* Li = reinterpret_cast<const T*>(a.linv) + a.linv_off[s] + (long long)i * TB * TB;
+  T* Ze = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * ld;
+  // dependency blocks in chain order: step u is block dep(u)
+  const int nd = FWD ? i : nblk - 1 - i;
+  auto dep = [&](int u) { return FWD ? u : nblk - 1 - u; };
+  auto issue = [&](int u) {
+    const int j = dep(u);
+    if (FWD) ch_issue<T>(S, L, nrow, i * TB, ncol, j * TB, ncol);
+    else ch_issue<T>(S, L, nrow, j * TB, ncol, i * TB, ncol);
+  };
+  ch_issue<T>(Lv, Li, TB, 0, nb, 0, nb);
+  if (nd > 0) issue(0);
+  cp_async_commit();
+  // block vector: y_i (forward) or w_i - W_i (backward; W_i = off-diagonal dots)
+  const T* Wb = (!FWD && nrow > ncol) ? reinterpret_cast<const T*>(a.Wb) + a.c0 + (long long)first * ld : nullptr;
+  for (int e = tid; e < 64 * nr; e += WV_NT) {
+    const int r = e / nr, c = e - r * nr;
+    T v = F::zero();
+    if (r < nb) {
+      v = ld_cg(Ze + (long long)(i * TB + r) * ld + c);
+      if (Wb) v = F::sub(v, Wb[(long long)(i * TB + r) * ld + c]);
+    }
+    wv[e] = v;
+  }
+  T acc[NR];
+#pragma unroll
+  for (int c = 0; c < NR; ++c) acc[c] = F::zero();
+#pragma unroll 1
+  for (int u = 0; u < nd; ++u) {
+    const int j = dep(u);
+    if (tid == 0 && !wv_wait(flags, j, a.wstate)) sh_abort = 1;
+    cp_async_wait<0>();
+    __syncthreads();  // tile u landed; flag j observed
+    if (sh_abort) return;
+    for (int e = tid; e < 64 * nr; e += WV_NT) {
+      const int r = e / nr, c = e - r * nr;
+      Vs[e] = j * TB + r < ncol ? ld_cg(Ze + (long long)(j * TB + r) * ld + c) : F::zero();
+    }
+    __syncthreads();
+    ch_tile_mv<T, FWD, NR>(acc, S, Vs, x, g, nr);
+    __syncthreads();  // tile and right-hand sides consumed
+    if (u + 1 < nd) issue(u + 1);
+    cp_async_commit();
+  }
+  cp_async_wait<0>();
+  // wv -= sum of the slice partials, then the inverse block
+#pragma unroll
+  for (int c = 0; c < NR; ++c)
+    if (c < nr) {
+      red[(g * 64 + x) * nr + c] = acc[c];
+      acc[c] = F::zero();
+    }
+  __syncthreads();
+  for (int e = tid; e < 64 * nr; e += WV_NT) {
+    const int r = e / nr, c = e - r * nr;
+    wv[e] = r < nb ? F::sub(wv[e], slice_sum(red, r, c, nr)) : F::zero();
+  }
+  __syncthreads();
+  ch_tile_mv<T, FWD, NR>(acc, Lv, wv, x, g, nr);
+#pragma unroll
+  for (int c = 0; c < NR; ++c)
+    if (c < nr) red[(g * 64 + x) * nr + c] = acc[c];
+  __syncthreads();
+  for (int e = tid; e < 64 * nr; e += WV_NT) {
+    const int r = e / nr, c = e - r * nr;
+    if (r >= nb) continue;
+    const T v = slice_sum(red, r, c, nr);
+    Ze[(long long)(i * TB + r) * ld + c] = v;
+    if (!FWD) {
+      T* Xw = reinterpret_cast<T*>(a.Xg) + a.c0;
+      Xw[(long long)(first + a.lperm[first + i * TB + r]) * ld + c] = v;
+    }
+  }
+  __syncthreads();
+  // the release store orders the CTA's stores above (barrier, then a
+  // cumulative gpu-scope release)
+  if (tid == 0) st_release_gpu(flags + i, 1);
+}
+
+}  // namespace rsd

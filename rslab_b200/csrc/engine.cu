@@ -20,6 +20,7 @@
 #include "device/factor_kernels.cuh"
 #include "device/cmod_tc.cuh"
 #include "device/solve_kernels.cuh"
+#include "device/wave_solve.cuh"
 #include "host/host.hpp"
 
 using namespace rsd;
@@ -98,14 +99,14 @@ size_t elem_size(int dtype) {
 enum LaunchKind {
   L_CMOD, L_GETF2, L_DEEP, L_SCHUR,
   L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD,
-  L_FTRSV_BLK, L_FTRSV_UPD, L_BTRSV_BLK, L_BTRSV_UPD, L_FWD_GATHER, L_CMOD_TC, L_MAKE_G, L_DIAG_INV,
-  L_BWD_OFF_RED, L_SCHUR_TC
+  L_UNUSED8, L_UNUSED9, L_UNUSED10, L_UNUSED11, L_FWD_GATHER, L_CMOD_TC, L_MAKE_G, L_DIAG_INV,
+  L_BWD_OFF_RED, L_SCHUR_TC, L_FWD_CHAIN, L_BWD_CHAIN, L_BWD_GATHER
 };
 struct Launch {
   int kind;
   long long task_off;  // into the int4 / int2 / int task arrays
   int ntasks;
-  int nb_slot;         // getf2/deep: scratch stride nb
+  int nb_slot;         // getf2/deep: scratch stride nb; chain solves: ticket counter
 };
 
 }  // namespace
@@ -142,6 +143,10 @@ struct rslab_sym_handle {
   int bwd_slots = 0;                  // partial-sum slots of the split backward dots (max per level)
   std::vector<long long> linv_off;    // wide supernodes: inverses of their TB x TB diagonal blocks
   long long linv_elems = 0;
+  // chain solves: per wide supernode the index of its block-0 flag (-1 for
+  // narrow ones), flags per direction, and ticket counters (launches)
+  std::vector<int> flag_off;
+  int nflags = 0, nwave = 0;
   std::vector<int> t1;
   std::vector<int2> t2;
   std::vector<int4> st4;  // blocked diagonal-solve tasks (s, j0, r0 | c0, 0)
@@ -369,6 +374,14 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
     H.linv_off[s] = H.linv_elems;
     if (S.sn[s].ncol > SOLVE_BIG) H.linv_elems += (long long)((S.sn[s].ncol + TB - 1) / TB) * TB * TB;
   }
+  H.flag_off.assign(ns, -1);
+  H.nflags = 0;
+  H.nwave = 0;
+  for (int s = 0; s < ns; ++s)
+    if (S.sn[s].ncol > SOLVE_BIG) {
+      H.flag_off[s] = H.nflags;
+      H.nflags += (int)((S.sn[s].ncol + TB - 1) / TB);
+    }
   // Pull lists: every off-diagonal row r of updater k (U row uoff[k] + r)
   // lands on one column g of an ancestor; list the pushes per g in the
   // ancestor's update-list order so the gather subtracts them in that order.
@@ -519,10 +532,13 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       Dv.ntasks = (int)(H.t2.size() - Dv.task_off);
       if (Dv.ntasks) H.fplan.push_back(Dv);
     }
-    // Solve launches for this level.  Forward: diagonal blocks (one CTA per
-    // narrow supernode; wide ones get the blocked multi-CTA solve), then the
-    // row-tiled push.  Backward (run root first): column-chunked off-diagonal
-    // dots, narrow diagonal blocks, then the wide ones block by block.
+    // Solve launches for this level.
+    // Forward: gather the descendants' pushes into y (all supernodes), solve
+    // the narrow diagonal blocks (one CTA each) and the wide ones (block
+    // chain, one launch), then stream the push U_s = L21_s z_s.
+    // Backward (levels root first): gather the ancestors' x into row order,
+    // stream the off-diagonal dots W_s = L21_s^T x_anc (row-chunk partials
+    // reduced in chunk order), then the narrow and the wide diagonal solves.
     {
       Launch Fg{L_FWD_GATHER, (long long)H.t2.size(), 0, 0};
       for (int64_t s : lvl)
@@ -537,51 +553,48 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       int maxb = 0;
       for (int64_t s : lvl)
         if (S.sn[s].ncol > SOLVE_BIG) maxb = std::max(maxb, (int)((S.sn[s].ncol + TB - 1) / TB));
-      // Wide supernodes: block 0 is solved by k_ftrsv_blk; afterwards each
-      // launch updates the rows below block b and the CTA owning block b+1's
-      // rows solves it (one launch per block step).
+      // chain items in block order across the level's wide supernodes
+      // (ticket order = dependency order)
       if (maxb > 0) {
-        Launch Fb{L_FTRSV_BLK, (long long)H.st4.size(), 0, 0};
-        for (int64_t s : lvl)
-          if (S.sn[s].ncol > SOLVE_BIG) H.st4.push_back(make_int4((int)s, 0, 0, 0));
-        Fb.ntasks = (int)(H.st4.size() - Fb.task_off);
-        H.fwdplan.push_back(Fb);
+        Launch W{L_FWD_CHAIN, (long long)H.st4.size(), 0, H.nwave++};
+        for (int b = 0; b < maxb; ++b)
+          for (int64_t s : lvl)
+            if (S.sn[s].ncol > SOLVE_BIG && b * TB < S.sn[s].ncol)
+              H.st4.push_back(make_int4((int)s, 0, b, H.flag_off[s]));
+        W.ntasks = (int)(H.st4.size() - W.task_off);
+        H.fwdplan.push_back(W);
       }
-      for (int b = 0; b < maxb; ++b) {
-        Launch Fu{L_FTRSV_UPD, (long long)H.st4.size(), 0, 0};
-        for (int64_t s : lvl) {
-          const int nc = (int)S.sn[s].ncol;
-          if (nc <= SOLVE_BIG) continue;
-          for (int r0 = (b + 1) * TB; r0 < nc; r0 += TB)
-            H.st4.push_back(make_int4((int)s, b * TB, r0, r0 == (b + 1) * TB ? 1 : 0));
-        }
-        Fu.ntasks = (int)(H.st4.size() - Fu.task_off);
-        if (Fu.ntasks) H.fwdplan.push_back(Fu);
+      // push items: 64-row blocks, several per item for narrow supernodes
+      // (about 8 column units per item)
+      Launch Pu{L_FWD_PUSH, (long long)H.st4.size(), 0, 0};
+      for (int64_t s : lvl) {
+        const int cu = (int)((S.sn[s].ncol + 31) / 32), nrb = std::max(1, 8 / cu);
+        for (int r0 = 0; r0 < H.nrow[s] - S.sn[s].ncol; r0 += 64 * nrb) H.st4.push_back(make_int4((int)s, r0, nrb, 0));
       }
-      Launch Pu{L_FWD_PUSH, (long long)H.t2.size(), 0, 0};
-      for (int64_t s : lvl)
-        for (int r0 = 0; r0 < H.nrow[s] - S.sn[s].ncol; r0 += 64) H.t2.push_back(make_int2((int)s, r0));
-      Pu.ntasks = (int)(H.t2.size() - Pu.task_off);
+      Pu.ntasks = (int)(H.st4.size() - Pu.task_off);
       if (Pu.ntasks) H.fwdplan.push_back(Pu);
 
       std::vector<Launch> bw;
-      // Off-diagonal dots: tasks (s, c0, row chunk, slot) over chunks of
-      // BWD_ROWS off-diagonal rows; a column chunk with several row chunks
-      // writes partial sums to slots, reduced in row-chunk order next.
+      Launch Bg{L_BWD_GATHER, (long long)H.t2.size(), 0, 0};
+      for (int64_t s : lvl)
+        for (int r0 = 0; r0 < H.nrow[s] - S.sn[s].ncol; r0 += 256) H.t2.push_back(make_int2((int)s, r0));
+      Bg.ntasks = (int)(H.t2.size() - Bg.task_off);
+      if (Bg.ntasks) bw.push_back(Bg);
+      // dots items (s, block, row chunk, slot); a block with several row
+      // chunks writes partial sums to slots, reduced in chunk order next
       Launch Bo{L_BWD_OFF, (long long)H.st4.size(), 0, 0};
-      Launch Br{L_BWD_OFF_RED, (long long)H.st4.size(), 0, 0};
       std::vector<int4> red;
       int slot = 0;
       for (int64_t s : lvl) {
         const int off = H.nrow[s] - (int)S.sn[s].ncol;
         if (off <= 0) continue;
-        const int nch = (off + BWD_ROWS - 1) / BWD_ROWS;
-        for (int c0 = 0; c0 < S.sn[s].ncol; c0 += 32) {
+        const int nch = (off + BWD_CH - 1) / BWD_CH;
+        for (int i = 0; i * TB < S.sn[s].ncol; ++i) {
           if (nch == 1) {
-            H.st4.push_back(make_int4((int)s, c0, 0, -1));
+            H.st4.push_back(make_int4((int)s, i, 0, -1));
           } else {
-            red.push_back(make_int4((int)s, c0, slot, nch));
-            for (int q = 0; q < nch; ++q) H.st4.push_back(make_int4((int)s, c0, q * BWD_ROWS, slot + q));
+            red.push_back(make_int4((int)s, i, slot, nch));
+            for (int q = 0; q < nch; ++q) H.st4.push_back(make_int4((int)s, i, q * BWD_CH, slot + q));
             slot += nch;
           }
         }
@@ -589,34 +602,23 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       Bo.ntasks = (int)(H.st4.size() - Bo.task_off);
       if (Bo.ntasks) bw.push_back(Bo);
       H.bwd_slots = std::max(H.bwd_slots, slot);
-      Br.task_off = (long long)H.st4.size();
+      Launch Br{L_BWD_OFF_RED, (long long)H.st4.size(), (int)red.size(), 0};
       H.st4.insert(H.st4.end(), red.begin(), red.end());
-      Br.ntasks = (int)red.size();
       if (Br.ntasks) bw.push_back(Br);
       Launch Bd{L_BWD, (long long)H.t1.size(), 0, 0};
       for (int64_t s : lvl)
         if (S.sn[s].ncol <= SOLVE_BIG) H.t1.push_back((int)s);
       Bd.ntasks = (int)(H.t1.size() - Bd.task_off);
       if (Bd.ntasks) bw.push_back(Bd);
-      // Backward, last block first: k_btrsv_blk solves each wide supernode's
-      // last block; each update launch after block b also solves block b-1
-      // in the task that covers it.
-      for (int b = maxb - 1; b >= 0; --b) {
-        Launch Bb{L_BTRSV_BLK, (long long)H.st4.size(), 0, 0};
-        for (int64_t s : lvl) {
-          const int nc = (int)S.sn[s].ncol;
-          if (nc > SOLVE_BIG && b == (nc - 1) / TB) H.st4.push_back(make_int4((int)s, b * TB, 0, 0));
-        }
-        Bb.ntasks = (int)(H.st4.size() - Bb.task_off);
-        if (Bb.ntasks) bw.push_back(Bb);
-        Launch Bu{L_BTRSV_UPD, (long long)H.st4.size(), 0, 0};
-        for (int64_t s : lvl)
-          if (S.sn[s].ncol > SOLVE_BIG && b * TB < S.sn[s].ncol && b > 0) {
-            H.st4.push_back(make_int4((int)s, b * TB, (b - 1) * TB, 1));
-            for (int c0 = 0; c0 < (b - 1) * TB; c0 += 32) H.st4.push_back(make_int4((int)s, b * TB, c0, 0));
+      if (maxb > 0) {
+        Launch W{L_BWD_CHAIN, (long long)H.st4.size(), 0, H.nwave++};
+        for (int dd = 0; dd < maxb; ++dd)
+          for (int64_t s : lvl) {
+            const int nc = (int)S.sn[s].ncol, nblk = (nc + TB - 1) / TB;
+            if (nc > SOLVE_BIG && dd < nblk) H.st4.push_back(make_int4((int)s, 1, nblk - 1 - dd, H.flag_off[s]));
           }
-        Bu.ntasks = (int)(H.st4.size() - Bu.task_off);
-        if (Bu.ntasks) bw.push_back(Bu);
+        W.ntasks = (int)(H.st4.size() - W.task_off);
+        bw.push_back(W);
       }
       bw_levels.push_back(bw);
     }
@@ -640,10 +642,8 @@ size_t smem_getf2(size_t es, int nb) {
 }
 size_t smem_deep(size_t es, int nb) { return smem_replay(es, nb) + 64; }
 size_t smem_solve(size_t es) { return ((size_t)(SOLVE_NT / 32) * 32 * RHS_MAX + SB * (SB + 1) + SB * RHS_MAX) * es; }
-size_t smem_push(size_t es) { return (size_t)(32 * 64 + 32 * RHS_MAX) * es; }
 size_t smem_dots(size_t es) { return (size_t)(32 * 33 + 32 * RHS_MAX) * es; }
 size_t smem_diag_inv(size_t es) { return (size_t)TB * (TB + 1) * 2 * es; }
-size_t smem_blk_inv(size_t es) { return (size_t)(TB * (TB + 1) + TB * RHS_MAX) * es; }
 
 // Threads of the BK panel kernel: its per-step trailing update is
 // latency-bound, so 16 warps hide more of it than 8.
@@ -653,6 +653,37 @@ constexpr int GETF2_NT = 512;
 template <typename T> struct TensorCmod { static constexpr bool ok = false; };
 template <> struct TensorCmod<float> { static constexpr bool ok = true; };
 template <> struct TensorCmod<c32> { static constexpr bool ok = true; };
+
+// Shared-memory limits of the streamed / chain solve kernels for NR
+// right-hand-side columns (NR = 1, 4, RHS_MAX instantiated).
+template <typename T, int NR>
+void solve_nr_attrs() {
+  CK(cudaFuncSetAttribute(k_stream<T, true, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st_smem_bytes<T>(NR)));
+  CK(cudaFuncSetAttribute(k_stream<T, false, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st_smem_bytes<T>(NR)));
+  CK(cudaFuncSetAttribute(k_chain<T, true, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ch_smem_bytes<T>(NR)));
+  CK(cudaFuncSetAttribute(k_chain<T, false, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ch_smem_bytes<T>(NR)));
+}
+
+// Launch a streamed (kind 0) or chain (kind 1) solve kernel instantiated for
+// the smallest NR in {1, 4, RHS_MAX} that holds nr columns.
+template <typename T, bool FWD, int NR>
+void launch_solve_nr(int kind, int grid, int nr, const SolveArgs& sa, const int4* tasks, int ctr, int flags,
+                     cudaStream_t st) {
+  if (kind == 0)
+    k_stream<T, FWD, NR><<<grid, WV_NT, st_smem_bytes<T>(nr), st>>>(sa, tasks);
+  else
+    k_chain<T, FWD, NR><<<grid, WV_NT, ch_smem_bytes<T>(nr), st>>>(sa, tasks, ctr, flags);
+}
+template <typename T, bool FWD>
+void launch_solve(int kind, int grid, int nr, const SolveArgs& sa, const int4* tasks, int ctr = 0, int flags = 0,
+                  cudaStream_t st = nullptr) {
+  if (nr <= 1)
+    launch_solve_nr<T, FWD, 1>(kind, grid, nr, sa, tasks, ctr, flags, st);
+  else if (nr <= 4)
+    launch_solve_nr<T, FWD, 4>(kind, grid, nr, sa, tasks, ctr, flags, st);
+  else
+    launch_solve_nr<T, FWD, RHS_MAX>(kind, grid, nr, sa, tasks, ctr, flags, st);
+}
 
 template <typename T>
 struct KernelSetup {
@@ -671,13 +702,10 @@ struct KernelSetup {
     CK(cudaFuncSetAttribute(k_deep<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep(es, 128)));
     CK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
     CK(cudaFuncSetAttribute(k_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
-    CK(cudaFuncSetAttribute(k_fwd_push<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_push(es)));
-    CK(cudaFuncSetAttribute(k_ftrsv_upd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_blk_inv(es)));
-    CK(cudaFuncSetAttribute(k_ftrsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_blk_inv(es)));
     CK(cudaFuncSetAttribute(k_diag_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_diag_inv(es)));
-    CK(cudaFuncSetAttribute(k_btrsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_blk_inv(es)));
-    CK(cudaFuncSetAttribute(k_bwd_off<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
-    CK(cudaFuncSetAttribute(k_btrsv_upd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_blk_inv(es)));
+    solve_nr_attrs<T, 1>();
+    solve_nr_attrs<T, 4>();
+    solve_nr_attrs<T, RHS_MAX>();
     done = true;
   }
 };
@@ -721,6 +749,8 @@ struct rslab_fac_handle {
   int ws_nrhs = 0;
   void *Yg = nullptr, *Ze = nullptr, *Xg = nullptr, *Ub = nullptr, *Wb = nullptr, *bdev = nullptr, *xdev = nullptr;
   void* Wp = nullptr;  // partial sums of the split backward dots
+  int* wstate = nullptr;   // wavefront solves: sticky status, abort word, ticket counters, block flags
+  int* h_wstat = nullptr;  // pinned copy of the sticky status after each solve
   std::vector<std::unique_ptr<void, DFree>> ws;
   cudaGraphExec_t sgraph = nullptr;
   int sgraph_nrhs = -1;
@@ -741,6 +771,7 @@ struct rslab_fac_handle {
     if (fgraph) cudaGraphExecDestroy(fgraph);
     if (sgraph) cudaGraphExecDestroy(sgraph);
     if (h_status) cudaFreeHost(h_status);
+    if (h_wstat) cudaFreeHost(h_wstat);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (own_stream && st) cudaStreamDestroy(st);
@@ -960,6 +991,20 @@ void run_factor(rslab_fac_handle& F) {
                                       "numerically rank deficient pivot in supernode " + std::to_string(F.failing_sn));
 }
 
+// Wave state: sticky status, abort word, one ticket counter per wavefront
+// launch, forward and backward block flags.
+size_t wave_state_ints(const rslab_sym_handle& H) { return (size_t)WV_STATE_CTR + H.nwave + 2 * (size_t)H.nflags; }
+
+// After a synchronised solve: a timed-out wavefront wait (sticky status set
+// by the kernels) is reported and the status cleared.
+void wave_check(rslab_fac_handle& F) {
+  if (!F.h_wstat || *F.h_wstat == 0) return;
+  *F.h_wstat = 0;
+  CK(cudaMemsetAsync(F.wstate, 0, sizeof(int), F.st));
+  CK(cudaStreamSynchronize(F.st));
+  throw RslabError(Status::CudaError, "triangular solve: a wavefront dependency wait timed out");
+}
+
 template <typename T>
 void ensure_ws(rslab_fac_handle& F, int nrhs) {
   if (F.ws_nrhs >= nrhs) return;
@@ -977,9 +1022,15 @@ void ensure_ws(rslab_fac_handle& F, int nrhs) {
   F.Xg = a(m * es);
   F.Ub = a((size_t)std::max(F.sym->urows, 1LL) * nrhs * es);
   F.Wb = a(m * es);
-  F.Wp = a((size_t)std::max(F.sym->bwd_slots, 1) * 32 * nrhs * es);
+  F.Wp = a((size_t)std::max(F.sym->bwd_slots, 1) * 64 * nrhs * es);
   F.bdev = a(m * es);
   F.xdev = a(m * es);
+  F.wstate = (int*)a(wave_state_ints(*F.sym) * sizeof(int));
+  CK(cudaMemsetAsync(F.wstate, 0, wave_state_ints(*F.sym) * sizeof(int), F.st));
+  if (!F.h_wstat) {
+    CK(cudaMallocHost(&F.h_wstat, sizeof(int)));
+    *F.h_wstat = 0;
+  }
   F.ws_nrhs = nrhs;
   if (F.sgraph) {
     cudaGraphExecDestroy(F.sgraph);
@@ -1018,6 +1069,7 @@ SolveArgs make_sargs(rslab_fac_handle& F, int ld, int c0, int nr) {
   a.linv = F.linv;
   a.linv_off = H.d_linv_off;
   a.Wp = F.Wp;
+  a.wstate = F.wstate;
   a.ld = ld;
   a.c0 = c0;
   a.nrhs = nr;
@@ -1037,6 +1089,8 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
   for (int c0 = 0; c0 < nrhs; c0 += RHS_MAX) {
     const int nr = std::min(RHS_MAX, nrhs - c0);
     SolveArgs sa = make_sargs<T>(F, nrhs, c0, nr);
+    CK(cudaMemsetAsync(F.wstate + 1, 0, (wave_state_ints(H) - 1) * sizeof(int), st));
+    const int fwd_flags = WV_STATE_CTR + H.nwave, bwd_flags = fwd_flags + H.nflags;
     for (const Launch& L : H.fwdplan) {
       switch (L.kind) {
         case L_FWD_GATHER:
@@ -1045,14 +1099,11 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
         case L_FWD_DIAG:
           k_fwd_diag<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
           break;
-        case L_FTRSV_BLK:
-          k_ftrsv_blk<T><<<L.ntasks, SOLVE_NT, smem_blk_inv(es), st>>>(sa, H.d_st4 + L.task_off);
-          break;
-        case L_FTRSV_UPD:
-          k_ftrsv_upd<T><<<L.ntasks, SOLVE_NT, smem_blk_inv(es), st>>>(sa, H.d_st4 + L.task_off);
+        case L_FWD_CHAIN:
+          launch_solve<T, true>(1, L.ntasks, nr, sa, H.d_st4 + L.task_off, L.nb_slot, fwd_flags, st);
           break;
         default:
-          k_fwd_push<T><<<L.ntasks, SOLVE_NT, smem_push(es), st>>>(sa, H.d_t2 + L.task_off);
+          launch_solve<T, true>(0, L.ntasks, nr, sa, H.d_st4 + L.task_off, 0, 0, st);
       }
       if (prof) prof->mark(st, L.kind == L_FWD_PUSH ? 2 : 1, L.ntasks, L.kind);
     }
@@ -1060,26 +1111,29 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
     if (prof) prof->mark(st, 3);
     for (const Launch& L : H.bwdplan) {
       switch (L.kind) {
+        case L_BWD_GATHER:
+          k_bwd_gather<T><<<L.ntasks, WV_NT, 0, st>>>(sa, H.d_t2 + L.task_off);
+          break;
         case L_BWD_OFF:
-          k_bwd_off<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_st4 + L.task_off);
+          launch_solve<T, false>(0, L.ntasks, nr, sa, H.d_st4 + L.task_off, 0, 0, st);
           break;
         case L_BWD_OFF_RED:
-          k_bwd_off_reduce<T><<<L.ntasks, SOLVE_NT, 0, st>>>(sa, H.d_st4 + L.task_off);
+          k_dots_reduce<T><<<L.ntasks, WV_NT, 0, st>>>(sa, H.d_st4 + L.task_off);
           break;
-        case L_BTRSV_BLK:
-          k_btrsv_blk<T><<<L.ntasks, SOLVE_NT, smem_blk_inv(es), st>>>(sa, H.d_st4 + L.task_off);
-          break;
-        case L_BTRSV_UPD:
-          k_btrsv_upd<T><<<L.ntasks, SOLVE_NT, smem_blk_inv(es), st>>>(sa, H.d_st4 + L.task_off);
+        case L_BWD_CHAIN:
+          launch_solve<T, false>(1, L.ntasks, nr, sa, H.d_st4 + L.task_off, L.nb_slot, bwd_flags, st);
           break;
         default:
           k_bwd<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_t1 + L.task_off);
       }
-      if (prof) prof->mark(st, (L.kind == L_BWD_OFF || L.kind == L_BWD_OFF_RED) ? 4 : 5, L.ntasks, L.kind);
+      if (prof)
+        prof->mark(st, (L.kind == L_BWD_OFF || L.kind == L_BWD_OFF_RED || L.kind == L_BWD_GATHER) ? 4 : 5, L.ntasks,
+                   L.kind);
     }
   }
   k_perm_out<T><<<grid1((long long)n * nrhs), 256, 0, st>>>(n, nrhs, H.d_perm, F.scale, (const T*)F.Xg, x);
   if (prof) prof->mark(st, 0);
+  CK(cudaMemcpyAsync(F.h_wstat, F.wstate, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaGetLastError());
 }
 
@@ -1122,6 +1176,7 @@ void do_solve(rslab_fac_handle& F, const void* b, void* x, int nrhs, bool on_dev
   CK(cudaEventRecord(F.ev1, F.st));
   CK(cudaMemcpyAsync(x, F.xdev, m * es, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, F.st));
   CK(cudaStreamSynchronize(F.st));
+  wave_check(F);
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, F.ev0, F.ev1));
   F.solve_ms = ms;
@@ -1273,6 +1328,7 @@ static void refined_solve_impl(rslab_fac_handle& F, const void* bsrc, int nrhs, 
   }
   CK(cudaMemcpyAsync(xdst, best, m * es, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  wave_check(F);
 }
 
 extern "C" {
