@@ -19,6 +19,7 @@
 // Reference: src/numeric/multifrontal_ldlt.rs:2400-3256, 1347-1408.
 #pragma once
 
+#include "async_copy.cuh"
 #include "scalar.cuh"
 
 namespace rsd {
@@ -45,14 +46,24 @@ struct FactorArgs {
   void* dsub;
   unsigned char* kind;
   int* lperm;
-  void* scratch;        // per getf2 slot: snap[nb*nb] T + swaps[nb] int
+  void* scratch;        // per getf2 slot: snap[nb*nb] T + swaps[nb] int, then the block transform M[nb*nb] T
   long long scratch_stride;  // bytes per slot
   int* status;          // [0] = error code, [1] = first failing supernode, [2] = n_perturbed
   double perturb_floor; // < 0: exact mode
   void* gpool;          // G_k = L21_k D_k, (nrow_k - ncol_k) x ncol_k at goff[k] (tensor-core cmod)
   const long long* goff;
   const double* floor_dev;  // non-null: static-pivot floor computed on the device (force-accept)
+  int deep_mm;              // tall panels: getf2 forms the block transform M, k_deep_mm applies it
 };
+
+// Byte offset of the block transform M in a getf2 scratch slot, and the slot
+// size, for panel width nb and element size es.
+__host__ __device__ constexpr long long replay_mm_off(long long nb, long long es) {
+  return (nb * nb * es + 3 * nb * 4 + 255) / 256 * 256;
+}
+__host__ __device__ constexpr long long getf2_scratch_stride(long long nb, long long es) {
+  return (replay_mm_off(nb, es) + nb * nb * es + 255) / 256 * 256;
+}
 
 // ---------------------------------------------------------------------------
 // Equilibration + assembly.
@@ -576,10 +587,20 @@ __device__ void replay_rows_sliced(T (&x)[NR][NS], int pw, int nb, const T* __re
 // the global loads / stores and the per-row register fills are conflict-free;
 // each warp replays its 32 / NW rows together.  `P` holds the program.  While
 // the rows sit in registers the staging buffer X carries the snapshot slices.
-template <typename T, int NT>
+//
+// IDENT: the rows are those of the pw x pw identity instead (rows
+// [r_begin, r_end) of it), and the results go to M (row-major, stride nb):
+// the replay is linear in the row, so M is the block's transform and every
+// deep row x becomes x M.
+// R rows per pass (a multiple of the warp count).  The snapshot slices use
+// S (default: X, free while the rows sit in registers; it must hold
+// (REPLAY_SL + 1) x nb elements).
+template <typename T, int NT, bool IDENT = false, int R = 32>
 __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int nb, int r_begin, int r_end,
-                                 const T* __restrict__ snap, const ReplayProg<T>& P, T* X) {
-  constexpr int R = 32, LDX = 33;
+                                 const T* __restrict__ snap, const ReplayProg<T>& P, T* X, T* M = nullptr,
+                                 T* S = nullptr) {
+  constexpr int LDX = R + 1;
+  if (!S) S = X;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int NW = NT / 32;
   constexpr int NR = R / NW;
@@ -589,7 +610,12 @@ __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int n
 #pragma unroll 16
     for (int e = threadIdx.x; e < R * 128; e += NT) {
       const int c = e / R, r = e % R;
-      if (r < rows && c < pw) X[c * LDX + r] = panel[(rs0 + r) + (long long)(kb + c) * nrow];
+      if (r < rows && c < pw) {
+        if constexpr (IDENT)
+          X[c * LDX + r] = c == rs0 + r ? Field<T>::one() : Field<T>::zero();
+        else
+          X[c * LDX + r] = panel[(rs0 + r) + (long long)(kb + c) * nrow];
+      }
     }
     __syncthreads();
     // rows warp + NW i; rows past `rows` replay zeros and are not stored
@@ -602,7 +628,7 @@ __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int n
           const int col = lane + 32 * j, r = warp + NW * i;
           x[i][j] = (col < pw && r < rows) ? X[col * LDX + r] : Field<T>::zero();
         }
-      replay_rows_sliced<T, NT, 2, NR>(x, pw, nb, snap, kb, P, X);
+      replay_rows_sliced<T, NT, 2, NR>(x, pw, nb, snap, kb, P, S);
 #pragma unroll
       for (int i = 0; i < NR; ++i)
 #pragma unroll
@@ -619,7 +645,7 @@ __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int n
           const int col = lane + 32 * j, r = warp + NW * i;
           x[i][j] = (col < pw && r < rows) ? X[col * LDX + r] : Field<T>::zero();
         }
-      replay_rows_sliced<T, NT, 4, NR>(x, pw, nb, snap, kb, P, X);
+      replay_rows_sliced<T, NT, 4, NR>(x, pw, nb, snap, kb, P, S);
 #pragma unroll
       for (int i = 0; i < NR; ++i)
 #pragma unroll
@@ -630,8 +656,13 @@ __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int n
     }
     __syncthreads();
     for (int e = threadIdx.x; e < R * pw; e += NT) {
-      const int c = e / R, r = e % R;
-      if (r < rows) panel[(rs0 + r) + (long long)(kb + c) * nrow] = X[c * LDX + r];
+      if constexpr (IDENT) {
+        const int r = e / pw, c = e % pw;  // row-major M: coalesced along c
+        if (r < rows) M[(long long)(rs0 + r) * nb + c] = X[c * LDX + r];
+      } else {
+        const int c = e / R, r = e % R;
+        if (r < rows) panel[(rs0 + r) + (long long)(kb + c) * nrow] = X[c * LDX + r];
+      }
     }
     __syncthreads();
   }
@@ -1014,6 +1045,132 @@ __global__ void __launch_bounds__(NT) k_deep(FactorArgs fa, const int4* __restri
                               reinterpret_cast<const T*>(fa.dsub) + first + kb, fa.kind + first + kb);
   __syncthreads();
   replay_deep_rows<T, NT>(panel, nrow, kb, pw, nb, rs0, min(rs0 + DEEP_R, nrow), snap, P, X);
+}
+
+// ---------------------------------------------------------------------------
+// Block transform of a tall panel: rows [i0, i0 + MM_RB) of M = the replay of
+// the same rows of the pw x pw identity (one row per warp, so each step's
+// dependency chain is short).  Task (s, kb, slot, i0).
+// ---------------------------------------------------------------------------
+constexpr int MM_RB = 8;
+
+__host__ __device__ constexpr size_t smem_make_m_off_prog(size_t es, int nb) {
+  return (((size_t)(MM_RB + 1) * nb * es + 15) & ~size_t(15));
+}
+__host__ __device__ constexpr size_t smem_make_m_off_slice(size_t es, int nb) {
+  return ((smem_make_m_off_prog(es, nb) + (size_t)nb * (3 * es + 4 + 1) + 16) + 15) & ~size_t(15);
+}
+__host__ __device__ constexpr size_t smem_make_m_bytes(size_t es, int nb) {
+  return smem_make_m_off_slice(es, nb) + (size_t)(REPLAY_SL + 1) * nb * es + 64;
+}
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_make_m(FactorArgs fa, const int4* __restrict__ tasks, int nb_small,
+                                               int nb_big) {
+  static_assert(MM_RB == NT / 32, "one identity row per warp");
+  if (fa.status[0] != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, kb = tk.y, slot = tk.z, i0 = tk.w;
+  const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
+  const int nb = ncol >= 512 ? nb_big : nb_small;
+  const int ke = min(kb + nb, ncol), pw = ke - kb;
+  T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
+  unsigned char* sc = reinterpret_cast<unsigned char*>(fa.scratch) + (long long)slot * fa.scratch_stride;
+  const T* snap = reinterpret_cast<const T*>(sc);
+  const int* swaps = reinterpret_cast<const int*>(snap + (long long)nb * nb);
+  T* M = reinterpret_cast<T*>(sc + replay_mm_off(nb, sizeof(T)));
+  T* X = reinterpret_cast<T*>(smem_raw);
+  const ReplayProg<T> P =
+      load_replay_prog<T, NT>(smem_raw + smem_make_m_off_prog(sizeof(T), nb), pw, nb, swaps,
+                              reinterpret_cast<const T*>(fa.d) + first + kb,
+                              reinterpret_cast<const T*>(fa.dsub) + first + kb, fa.kind + first + kb);
+  T* S = reinterpret_cast<T*>(smem_raw + smem_make_m_off_slice(sizeof(T), nb));
+  __syncthreads();
+  replay_deep_rows<T, NT, true, MM_RB>(panel, nrow, kb, pw, nb, i0, min(i0 + MM_RB, pw), snap, P, X, M, S);
+}
+
+// ---------------------------------------------------------------------------
+// Deep rows of a tall panel as one product: rows [r0, r0 + 64) of the panel
+// columns [kb, ke) become A21 M, M the block transform formed by getf2 (the
+// replay of the identity rows; the replay is linear in the row).  The 64-row
+// block is staged in shared memory first (the product overwrites it in
+// place), M streams through in MM_CW-column chunks; thread (r = tid & 63,
+// g = tid >> 6) owns row r and MM_CW / 4 columns of each chunk, summing over
+// k in ascending order.  Task (s, kb, slot, r0).  Used with the tensor-core
+// engine of the single-precision fields (the FMA engine replays row by row,
+// in the oracle's operation order).
+// ---------------------------------------------------------------------------
+template <typename T>
+__host__ __device__ constexpr int mm_cw() {
+  return sizeof(T) >= 16 ? 16 : 32;
+}
+template <typename T>
+__host__ __device__ constexpr size_t smem_deep_mm_bytes() {
+  return ((size_t)128 * 65 + 2 * 128 * mm_cw<T>()) * sizeof(T) + 16;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_deep_mm(FactorArgs fa, const int4* __restrict__ tasks, int nb_small,
+                                                 int nb_big) {
+  using F = Field<T>;
+  constexpr int CW = mm_cw<T>(), NO = CW / 4;
+  if (fa.status[0] != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* As = reinterpret_cast<T*>(smem_raw);  // As[k * 65 + r]
+  T* Ms = As + 128 * 65;                   // 2 x (128 x CW), row-major chunks
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, kb = tk.y, slot = tk.z, r0 = tk.w;
+  const int ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
+  const int nb = ncol >= 512 ? nb_big : nb_small;
+  const int ke = min(kb + nb, ncol), pw = ke - kb;
+  T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
+  const unsigned char* sc = reinterpret_cast<const unsigned char*>(fa.scratch) + (long long)slot * fa.scratch_stride;
+  const T* M = reinterpret_cast<const T*>(sc + replay_mm_off(nb, sizeof(T)));
+  const int tid = threadIdx.x, r = tid & 63, g = tid >> 6;
+  const int rows = min(64, nrow - r0);
+  auto load_chunk = [&](int j0, T* dst) {
+    for (int e = tid; e < 128 * CW; e += 256) {
+      const int k = e / CW, j = e % CW;
+      const bool ok = k < pw && j0 + j < pw;
+      const T* src = ok ? M + (long long)k * nb + j0 + j : M;
+      cp_async_zfill<sizeof(T)>(dst + e, src, ok);
+    }
+  };
+  for (int e = tid; e < 64 * 128; e += 256) {
+    const int rr = e & 63, k = e >> 6;
+    const bool ok = rr < rows && k < pw;
+    const T* src = ok ? panel + (r0 + rr) + (long long)(kb + k) * nrow : panel;
+    cp_async_zfill<sizeof(T)>(As + k * 65 + rr, src, ok);
+  }
+  load_chunk(0, Ms);
+  cp_async_commit();
+  const int nch = (pw + CW - 1) / CW;
+  for (int ch = 0; ch < nch; ++ch) {
+    if (ch + 1 < nch) load_chunk((ch + 1) * CW, Ms + ((ch + 1) & 1) * 128 * CW);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const T* Mc = Ms + (ch & 1) * 128 * CW + g * NO;
+    T acc[NO];
+#pragma unroll
+    for (int j = 0; j < NO; ++j) acc[j] = F::zero();
+#pragma unroll 4
+    for (int k = 0; k < pw; ++k) {
+      const T a = As[k * 65 + r];
+      T m[NO];
+      lds_row<T, NO>(Mc + k * CW, m);
+#pragma unroll
+      for (int j = 0; j < NO; ++j) acc[j] = F::fma_(a, m[j], acc[j]);
+    }
+    if (r < rows)
+#pragma unroll
+      for (int j = 0; j < NO; ++j) {
+        const int col = ch * CW + g * NO + j;
+        if (col < pw) panel[(r0 + r) + (long long)(kb + col) * nrow] = acc[j];
+      }
+    __syncthreads();  // chunk consumed before its buffer is refilled
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -38,6 +38,7 @@
 // (src/dense/ldlt_generic.rs:618-714), reorganised as a dependency chain.
 #pragma once
 
+#include "async_copy.cuh"
 #include "solve_kernels.cuh"
 
 namespace rsd {
@@ -58,14 +59,14 @@ __host__ __device__ constexpr int st_stages() {
 // kernels are instantiated for NR = 1, 4 and 16 register columns (the
 // smallest NR >= nr runs) so the inner loops carry no dead columns.
 // Streaming: stages of (tile + 32 x nr right-hand sides), then the slice
-// partials (4 x 64 x nr).
+// partials (4 x nr x 65).
 template <typename T>
 __host__ __device__ constexpr size_t st_stage_elems(int nr) {
   return (size_t)ST_UNIT + 32 * nr;
 }
 template <typename T>
 __host__ __device__ constexpr size_t st_smem_bytes(int nr) {
-  return ((size_t)st_stages<T>() * st_stage_elems<T>(nr) + 4 * 64 * nr) * sizeof(T) + 16;
+  return ((size_t)st_stages<T>() * st_stage_elems<T>(nr) + 4 * 65 * nr) * sizeof(T) + 16;
 }
 // Chain: one tile slot (its copy overlaps the wait for the dependency's
 // flag; after the chain it holds the slice partials), the inverse block,
@@ -81,18 +82,6 @@ __host__ __device__ constexpr size_t ch_smem_bytes(int nr) {
 // forward and the backward block flags.
 constexpr int WV_STATE_ABORT = 1;
 constexpr int WV_STATE_CTR = 2;
-
-template <int BYTES>
-__device__ __forceinline__ void cp_async_zfill(void* dst, const void* src, bool valid) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES),
-               "r"(valid ? BYTES : 0)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
   int v;
@@ -116,15 +105,20 @@ __device__ __forceinline__ c32 ld_cg(const c32* p) {
   return c32{v.x, v.y};
 }
 
-// The sum of the four slice partials red[(g * 64 + x) * nr + c] in order
-// g = 0..3.
-template <typename T>
-__device__ __forceinline__ T slice_sum(const T* red, int x, int c, int nr) {
+// Slice partials live at red[(g * NR + c) * 65 + x] (lanes over x write
+// consecutive words).  The sum over g = 0..3 in order:
+template <typename T, int NR>
+__device__ __forceinline__ T slice_sum(const T* red, int x, int c) {
   using F = Field<T>;
-  T s = red[x * nr + c];
-  s = F::add(s, red[(64 + x) * nr + c]);
-  s = F::add(s, red[(128 + x) * nr + c]);
-  return F::add(s, red[(192 + x) * nr + c]);
+  T s = red[c * 65 + x];
+  s = F::add(s, red[(NR + c) * 65 + x]);
+  s = F::add(s, red[(2 * NR + c) * 65 + x]);
+  return F::add(s, red[(3 * NR + c) * 65 + x]);
+}
+template <typename T, int NR>
+__device__ __forceinline__ void store_partials(T* red, const T (&acc)[NR], int x, int g) {
+#pragma unroll
+  for (int c = 0; c < NR; ++c) red[(g * NR + c) * 65 + x] = acc[c];
 }
 
 // ---------------------------------------------------------------------------
@@ -174,7 +168,7 @@ __device__ __forceinline__ StItem<T, FWD> st_item(const SolveArgs& a, int4 tk) {
   return it;
 }
 
-template <typename T, bool FWD>
+template <typename T, bool FWD, int NR>
 __device__ __forceinline__ void st_issue(T* S, T* Vs, const StItem<T, FWD>& it, int u, int ld, int nr) {
   int rr0, cc0, vr0;
   if constexpr (FWD) {
@@ -200,7 +194,7 @@ __device__ __forceinline__ void st_issue(T* S, T* Vs, const StItem<T, FWD>& it, 
     const int k = e / nr, c = e - k * nr, row = vr0 + k;
     const bool ok = row < it.vlim;
     const T* g = ok ? it.V + (long long)row * ld + c : it.V;
-    cp_async_zfill<sizeof(T)>(Vs + e, g, ok);
+    cp_async_zfill<sizeof(T)>(Vs + k * NR + c, g, ok);
   }
 }
 
@@ -210,9 +204,9 @@ __global__ void __launch_bounds__(WV_NT) k_stream(SolveArgs a, const int4* __res
   constexpr int NST = st_stages<T>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nr = a.nrhs, ld = a.ld;
-  const int SE = (int)st_stage_elems<T>(nr);
-  T* stages = reinterpret_cast<T*>(smem_raw);  // NST x (tile, V)
-  T* red = stages + NST * SE;                  // 4 x 64 x nr
+  constexpr int SE = (int)st_stage_elems<T>(NR);
+  T* stages = reinterpret_cast<T*>(smem_raw);  // NST x (tile, V rows of stride NR)
+  T* red = stages + NST * SE;                  // slice partials, 4 x NR x 65
   const int4 tk = tasks[blockIdx.x];
   const int s = tk.x;
   const StItem<T, FWD> it = st_item<T, FWD>(a, tk);
@@ -222,16 +216,13 @@ __global__ void __launch_bounds__(WV_NT) k_stream(SolveArgs a, const int4* __res
   for (int c = 0; c < NR; ++c) acc[c] = F::zero();
   // slice partials of the finished output block -> U (forward) / Wb / slot
   auto flush = [&](int rb) {
+    store_partials<T, NR>(red, acc, x, g);
 #pragma unroll
-    for (int c = 0; c < NR; ++c)
-      if (c < nr) {
-        red[(g * 64 + x) * nr + c] = acc[c];
-        acc[c] = F::zero();
-      }
+    for (int c = 0; c < NR; ++c) acc[c] = F::zero();
     __syncthreads();
     for (int e = tid; e < 64 * nr; e += WV_NT) {
       const int r = e / nr, c = e - r * nr;
-      const T v = slice_sum(red, r, c, nr);
+      const T v = slice_sum<T, NR>(red, r, c);
       if (FWD) {
         const int row = it.r0 + 64 * rb + r;
         if (row < it.rlim) {
@@ -252,7 +243,7 @@ __global__ void __launch_bounds__(WV_NT) k_stream(SolveArgs a, const int4* __res
 #pragma unroll 1
   for (int u = 0; u < NST - 1; ++u) {
     T* S = stages + u * SE;
-    if (u < it.nunits) st_issue<T, FWD>(S, S + ST_UNIT, it, u, ld, nr);
+    if (u < it.nunits) st_issue<T, FWD, NR>(S, S + ST_UNIT, it, u, ld, nr);
     cp_async_commit();
   }
 #pragma unroll 1
@@ -263,7 +254,7 @@ __global__ void __launch_bounds__(WV_NT) k_stream(SolveArgs a, const int4* __res
     {
       const int un = u + NST - 1;
       T* Sn = stages + (un % NST) * SE;
-      if (un < it.nunits) st_issue<T, FWD>(Sn, Sn + ST_UNIT, it, un, ld, nr);
+      if (un < it.nunits) st_issue<T, FWD, NR>(Sn, Sn + ST_UNIT, it, un, ld, nr);
       cp_async_commit();
     }
     const T* S = stages + (u % NST) * SE;
@@ -272,9 +263,10 @@ __global__ void __launch_bounds__(WV_NT) k_stream(SolveArgs a, const int4* __res
     for (int k = 0; k < 8; ++k) {
       const int q = 8 * g + k;
       const T l = FWD ? S[q * 65 + x] : S[x * 33 + q];
+      T v[NR];
+      lds_row<T, NR>(V + q * NR, v);
 #pragma unroll
-      for (int c = 0; c < NR; ++c)
-        if (c < nr) acc[c] = F::fma_(l, V[q * nr + c], acc[c]);
+      for (int c = 0; c < NR; ++c) acc[c] = F::fma_(l, v[c], acc[c]);
     }
   }
   cp_async_wait<0>();
@@ -353,15 +345,16 @@ __device__ __forceinline__ void ch_issue(T* S, const T* src, long long ld, int r
 // S (forward: S[q * 65 + x] = A[x, q]; backward: S[x * 65 + q] = A[q, x])
 // times V[q * nr + c].
 template <typename T, bool FWD, int NR>
-__device__ __forceinline__ void ch_tile_mv(T (&acc)[NR], const T* S, const T* V, int x, int g, int nr) {
+__device__ __forceinline__ void ch_tile_mv(T (&acc)[NR], const T* S, const T* V, int x, int g) {
   using F = Field<T>;
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
     const int q = 16 * g + k;
     const T l = FWD ? S[q * 65 + x] : S[x * 65 + q];
+    T v[NR];
+    lds_row<T, NR>(V + q * NR, v);
 #pragma unroll
-    for (int c = 0; c < NR; ++c)
-      if (c < nr) acc[c] = F::fma_(l, V[q * nr + c], acc[c]);
+    for (int c = 0; c < NR; ++c) acc[c] = F::fma_(l, v[c], acc[c]);
   }
 }
 
@@ -371,11 +364,11 @@ __global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __rest
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int sh_t, sh_abort;
   const int nr = a.nrhs, ld = a.ld;
-  T* S = reinterpret_cast<T*>(smem_raw);  // dependency tile; later the slice partials (4 x 64 x nr)
+  T* S = reinterpret_cast<T*>(smem_raw);  // dependency tile; later the slice partials (4 x NR x 65)
   T* red = S;
   T* Lv = S + CH_UNIT;                    // the inverse block
-  T* Vs = Lv + CH_UNIT;                   // 64 x nr
-  T* wv = Vs + 64 * nr;                   // 64 x nr
+  T* Vs = Lv + CH_UNIT;                   // 64 x NR
+  T* wv = Vs + 64 * NR;                   // 64 x NR
   const int tid = threadIdx.x, x = tid & 63, g = tid >> 6;
   if (tid == 0) {
     sh_t = atomicAdd(a.wstate + WV_STATE_CTR + ctr, 1);
@@ -404,10 +397,10 @@ __global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __rest
   cp_async_commit();
   // block vector: y_i (forward) or w_i - W_i (backward; W_i = off-diagonal dots)
   const T* Wb = (!FWD && nrow > ncol) ? reinterpret_cast<const T*>(a.Wb) + a.c0 + (long long)first * ld : nullptr;
-  for (int e = tid; e < 64 * nr; e += WV_NT) {
-    const int r = e / nr, c = e - r * nr;
+  for (int e = tid; e < 64 * NR; e += WV_NT) {
+    const int r = e / NR, c = e % NR;
     T v = F::zero();
-    if (r < nb) {
+    if (r < nb && c < nr) {
       v = ld_cg(Ze + (long long)(i * TB + r) * ld + c);
       if (Wb) v = F::sub(v, Wb[(long long)(i * TB + r) * ld + c]);
     }
@@ -423,39 +416,34 @@ __global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __rest
     cp_async_wait<0>();
     __syncthreads();  // tile u landed; flag j observed
     if (sh_abort) return;
-    for (int e = tid; e < 64 * nr; e += WV_NT) {
-      const int r = e / nr, c = e - r * nr;
-      Vs[e] = j * TB + r < ncol ? ld_cg(Ze + (long long)(j * TB + r) * ld + c) : F::zero();
+    for (int e = tid; e < 64 * NR; e += WV_NT) {
+      const int r = e / NR, c = e % NR;
+      Vs[e] = (c < nr && j * TB + r < ncol) ? ld_cg(Ze + (long long)(j * TB + r) * ld + c) : F::zero();
     }
     __syncthreads();
-    ch_tile_mv<T, FWD, NR>(acc, S, Vs, x, g, nr);
+    ch_tile_mv<T, FWD, NR>(acc, S, Vs, x, g);
     __syncthreads();  // tile and right-hand sides consumed
     if (u + 1 < nd) issue(u + 1);
     cp_async_commit();
   }
   cp_async_wait<0>();
   // wv -= sum of the slice partials, then the inverse block
+  store_partials<T, NR>(red, acc, x, g);
 #pragma unroll
-  for (int c = 0; c < NR; ++c)
-    if (c < nr) {
-      red[(g * 64 + x) * nr + c] = acc[c];
-      acc[c] = F::zero();
-    }
+  for (int c = 0; c < NR; ++c) acc[c] = F::zero();
   __syncthreads();
-  for (int e = tid; e < 64 * nr; e += WV_NT) {
-    const int r = e / nr, c = e - r * nr;
-    wv[e] = r < nb ? F::sub(wv[e], slice_sum(red, r, c, nr)) : F::zero();
+  for (int e = tid; e < 64 * NR; e += WV_NT) {
+    const int r = e / NR, c = e % NR;
+    wv[e] = (r < nb && c < nr) ? F::sub(wv[e], slice_sum<T, NR>(red, r, c)) : F::zero();
   }
   __syncthreads();
-  ch_tile_mv<T, FWD, NR>(acc, Lv, wv, x, g, nr);
-#pragma unroll
-  for (int c = 0; c < NR; ++c)
-    if (c < nr) red[(g * 64 + x) * nr + c] = acc[c];
+  ch_tile_mv<T, FWD, NR>(acc, Lv, wv, x, g);
+  store_partials<T, NR>(red, acc, x, g);
   __syncthreads();
   for (int e = tid; e < 64 * nr; e += WV_NT) {
     const int r = e / nr, c = e - r * nr;
     if (r >= nb) continue;
-    const T v = slice_sum(red, r, c, nr);
+    const T v = slice_sum<T, NR>(red, r, c);
     Ze[(long long)(i * TB + r) * ld + c] = v;
     if (!FWD) {
       T* Xw = reinterpret_cast<T*>(a.Xg) + a.c0;

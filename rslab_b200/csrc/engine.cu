@@ -100,7 +100,7 @@ enum LaunchKind {
   L_CMOD, L_GETF2, L_DEEP, L_SCHUR,
   L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD,
   L_UNUSED8, L_UNUSED9, L_UNUSED10, L_UNUSED11, L_FWD_GATHER, L_CMOD_TC, L_MAKE_G, L_DIAG_INV,
-  L_BWD_OFF_RED, L_SCHUR_TC, L_FWD_CHAIN, L_BWD_CHAIN, L_BWD_GATHER
+  L_BWD_OFF_RED, L_SCHUR_TC, L_FWD_CHAIN, L_BWD_CHAIN, L_BWD_GATHER, L_DEEP_MM, L_MAKE_M
 };
 struct Launch {
   int kind;
@@ -472,7 +472,7 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
     for (int64_t s : lvl) maxblocks = std::max(maxblocks, (int)((S.sn[s].ncol + nb_of(s) - 1) / nb_of(s)));
     for (int b = 0; b < maxblocks; ++b) {
       Launch G{L_GETF2, (long long)H.t4.size(), 0, 0};
-      std::vector<int4> deep, schur, schur_tc;
+      std::vector<int4> deep, make_m, deep_mm, schur, schur_tc;
       int slot = 0, launch_nb = 0;
       for (int64_t s : lvl) {
         int nb = nb_of(s), nc = (int)S.sn[s].ncol, nr = H.nrow[s];
@@ -482,8 +482,11 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         bool fuse = (nr - ke) <= FUSE_DEEP_ROWS;
         H.t4.push_back(make_int4((int)s, kb, slot, fuse ? 1 : 0));
         launch_nb = std::max(launch_nb, nb);
-        if (!fuse)
+        if (!fuse) {
           for (int r0 = ke; r0 < nr; r0 += DEEP_R) deep.push_back(make_int4((int)s, kb, slot, r0));
+          for (int r0 = ke; r0 < nr; r0 += 64) deep_mm.push_back(make_int4((int)s, kb, slot, r0));
+          for (int i0 = 0; i0 < ke - kb; i0 += MM_RB) make_m.push_back(make_int4((int)s, kb, slot, i0));
+        }
         int mt = nr - ke, cw = nc - ke;
         const double pw = ke - kb;
         H.kind_flops[2] += 2.0 * pw * pw * pw / 3.0;
@@ -504,6 +507,14 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         Launch D{L_DEEP, (long long)H.t4.size(), (int)deep.size(), launch_nb};
         H.t4.insert(H.t4.end(), deep.begin(), deep.end());
         H.fplan.push_back(D);
+        // the same rows as one product with the block transform (tensor-core
+        // engine of the single-precision fields): M, then A21 M
+        Launch Mm{L_MAKE_M, (long long)H.t4.size(), (int)make_m.size(), launch_nb};
+        H.t4.insert(H.t4.end(), make_m.begin(), make_m.end());
+        H.fplan.push_back(Mm);
+        Launch Dm{L_DEEP_MM, (long long)H.t4.size(), (int)deep_mm.size(), launch_nb};
+        H.t4.insert(H.t4.end(), deep_mm.begin(), deep_mm.end());
+        H.fplan.push_back(Dm);
       }
       if (!schur.empty()) {
         Launch C{L_SCHUR, (long long)H.t4.size(), (int)schur.size(), 0};
@@ -670,9 +681,9 @@ template <typename T, bool FWD, int NR>
 void launch_solve_nr(int kind, int grid, int nr, const SolveArgs& sa, const int4* tasks, int ctr, int flags,
                      cudaStream_t st) {
   if (kind == 0)
-    k_stream<T, FWD, NR><<<grid, WV_NT, st_smem_bytes<T>(nr), st>>>(sa, tasks);
+    k_stream<T, FWD, NR><<<grid, WV_NT, st_smem_bytes<T>(NR), st>>>(sa, tasks);
   else
-    k_chain<T, FWD, NR><<<grid, WV_NT, ch_smem_bytes<T>(nr), st>>>(sa, tasks, ctr, flags);
+    k_chain<T, FWD, NR><<<grid, WV_NT, ch_smem_bytes<T>(NR), st>>>(sa, tasks, ctr, flags);
 }
 template <typename T, bool FWD>
 void launch_solve(int kind, int grid, int nr, const SolveArgs& sa, const int4* tasks, int ctr = 0, int flags = 0,
@@ -703,6 +714,8 @@ struct KernelSetup {
     CK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
     CK(cudaFuncSetAttribute(k_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
     CK(cudaFuncSetAttribute(k_diag_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_diag_inv(es)));
+    if constexpr (TensorCmod<T>::ok)
+      CK(cudaFuncSetAttribute(k_deep_mm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep_mm_bytes<T>()));
     solve_nr_attrs<T, 1>();
     solve_nr_attrs<T, 4>();
     solve_nr_attrs<T, RHS_MAX>();
@@ -789,7 +802,7 @@ namespace {
 template <typename T>
 FactorArgs make_fargs(rslab_fac_handle& F) {
   auto& H = *F.sym;
-  FactorArgs a;
+  FactorArgs a{};
   a.sn_first = H.d_sn_first;
   a.sn_ncol = H.d_sn_ncol;
   a.sn_nrow = H.d_sn_nrow;
@@ -871,6 +884,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
   FactorArgs fa = make_fargs<T>(F);
   const int nb_small = H.panel_nb, nb_big = std::max(H.panel_nb, 128);
   const bool use_tc = TensorCmod<T>::ok && F.set.schur_engine == RSLAB_SCHUR_TENSOR;
+  fa.deep_mm = use_tc ? 1 : 0;
   if (F.floor_dev) {
     CK(cudaMemsetAsync(F.amax_dev, 0, sizeof(unsigned long long), st));
     k_panel_absmax<T><<<(unsigned)std::min<long long>(grid1(H.panel_elems), 148LL * 8), 256, 0, st>>>(
@@ -904,15 +918,33 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         break;
       case L_GETF2: {
         FactorArgs f2 = fa;
-        f2.scratch_stride = ((long long)L.nb_slot * L.nb_slot * es + 3 * L.nb_slot * 4 + 255) / 256 * 256;
+        f2.scratch_stride = getf2_scratch_stride(L.nb_slot, (long long)es);
         k_getf2<T, GETF2_NT><<<L.ntasks, GETF2_NT, smem_getf2(es, L.nb_slot), st>>>(f2, H.d_t4 + L.task_off,
                                                                                   nb_small, nb_big);
         break;
       }
       case L_DEEP: {
+        if (fa.deep_mm) continue;
         FactorArgs f2 = fa;
-        f2.scratch_stride = ((long long)L.nb_slot * L.nb_slot * es + 3 * L.nb_slot * 4 + 255) / 256 * 256;
+        f2.scratch_stride = getf2_scratch_stride(L.nb_slot, (long long)es);
         k_deep<T, 256><<<L.ntasks, 256, smem_deep(es, L.nb_slot), st>>>(f2, H.d_t4 + L.task_off, nb_small, nb_big);
+        break;
+      }
+      case L_MAKE_M: {
+        if (!fa.deep_mm) continue;
+        FactorArgs f2 = fa;
+        f2.scratch_stride = getf2_scratch_stride(L.nb_slot, (long long)es);
+        k_make_m<T, 32 * MM_RB><<<L.ntasks, 32 * MM_RB, smem_make_m_bytes(es, L.nb_slot), st>>>(
+            f2, H.d_t4 + L.task_off, nb_small, nb_big);
+        break;
+      }
+      case L_DEEP_MM: {
+        if (!fa.deep_mm) continue;
+        if constexpr (TensorCmod<T>::ok) {
+          FactorArgs f2 = fa;
+          f2.scratch_stride = getf2_scratch_stride(L.nb_slot, (long long)es);
+          k_deep_mm<T><<<L.ntasks, 256, smem_deep_mm_bytes<T>(), st>>>(f2, H.d_t4 + L.task_off, nb_small, nb_big);
+        }
         break;
       }
       case L_SCHUR:
@@ -933,7 +965,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
                  (L.kind == L_CMOD || L.kind == L_CMOD_TC || L.kind == L_MAKE_G) ? 1
                  : (L.kind == L_DIAG_INV || L.kind == L_SCHUR_TC)             ? 4
                  : L.kind == L_GETF2                                           ? 2
-                 : L.kind == L_DEEP                                            ? 3
+                 : (L.kind == L_DEEP || L.kind == L_DEEP_MM || L.kind == L_MAKE_M) ? 3
                                                                                : 4,
                  L.ntasks, L.kind);
   }
@@ -1559,7 +1591,7 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
     F->aval = F->al<unsigned char>(sym->nnz * es);
     CK(cudaMallocHost(&F->h_status, 4 * sizeof(int)));
     const long long nbm = sym->max_nb;
-    F->scratch_stride = (nbm * nbm * (long long)es + 3 * nbm * 4 + 255) / 256 * 256;
+    F->scratch_stride = getf2_scratch_stride(nbm, (long long)es);
     F->scratch = F->al<unsigned char>((size_t)std::max(1, sym->max_getf2_tasks) * F->scratch_stride);
     F->linv = F->al<unsigned char>((size_t)std::max(sym->linv_elems, 1LL) * es);
     if (F->set.on_zero_pivot == RSLAB_PIVOT_FORCE_ACCEPT) {
