@@ -99,24 +99,27 @@ __device__ __forceinline__ void tmem_ld_cols<16>(uint32_t taddr, float (&v)[16])
   tmem_ld16(taddr, v);
 }
 
-// G_k[r, t] = (L21_k D_k)[r, t] for off-diagonal rows r of k and columns
-// [t0, t0 + 32): task (k, t0).  Same arithmetic as ld_G.
+// G_k[r, t] = (L21_k D_k)[r, t] for off-diagonal rows [r0, r0 + MG_ROWS)
+// of k and columns [t0, t0 + 32): task (k, t0, r0).  Same arithmetic as
+// ld_G; consecutive threads take consecutive rows of one column (coalesced
+// loads of L and stores of G).
+constexpr int MG_ROWS = 1024;
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_make_g(FactorArgs fa, const int2* __restrict__ tasks) {
+__global__ void __launch_bounds__(256) k_make_g(FactorArgs fa, const int4* __restrict__ tasks) {
   if (fa.status[0] != 0) return;
-  const int2 tk = tasks[blockIdx.x];
-  const int k = tk.x, t0 = tk.y;
+  const int4 tk = tasks[blockIdx.x];
+  const int k = tk.x, t0 = tk.y, r0 = tk.z;
   const int first = fa.sn_first[k], ncol = fa.sn_ncol[k], nrow = fa.sn_nrow[k];
-  const int off = nrow - ncol, tw = min(32, ncol - t0);
+  const int off = nrow - ncol, tw = min(32, ncol - t0), r1 = min(off, r0 + MG_ROWS);
   const T* L = reinterpret_cast<const T*>(fa.panel) + fa.sn_poff[k] + ncol;
   T* G = reinterpret_cast<T*>(fa.gpool) + fa.goff[k];
   const T* d = reinterpret_cast<const T*>(fa.d) + first;
   const T* ds = reinterpret_cast<const T*>(fa.dsub) + first;
   const unsigned char* kd = fa.kind + first;
-  for (long long e = threadIdx.x; e < (long long)off * tw; e += blockDim.x) {
-    const int r = (int)(e % off), t = t0 + (int)(e / off);
-    G[r + (long long)t * off] = ld_G(L, nrow, r, t, d, ds, kd);
-  }
+  for (int t = t0; t < t0 + tw; ++t)
+#pragma unroll 4
+    for (int r = r0 + (int)threadIdx.x; r < r1; r += 256) G[r + (long long)t * off] = ld_G(L, nrow, r, t, d, ds, kd);
 }
 
 // The producer / MMA pipeline of one 128 x 64 target tile, generic over the

@@ -18,9 +18,9 @@
 // by an earlier launch; backward: the ancestors' x gathered into a
 // contiguous buffer by k_bwd_gather).
 //
-// Chain (k_chain): a wide supernode (ncol > SOLVE_BIG) is cut into TB = 64
-// column blocks whose solves form a chain (forward: block i needs z of
-// blocks j < i; backward: x of blocks j > i).  One CTA per block:
+// Chain (k_chain): every supernode is cut into TB = 64 column blocks whose
+// solves form a chain (forward: block i needs z of blocks j < i; backward:
+// x of blocks j > i).  One CTA per block:
 //   forward : z_i = Linv_i (y_i - sum_{j<i} L_ij z_j)
 //   backward: x_i = Linv_i^T (w_i - W_i - sum_{j>i, descending} L_ji^T x_j)
 // with Linv_i the precomputed inverse of the unit-lower diagonal block and
@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __rest
     if (FWD) ch_issue<T>(S, L, nrow, i * TB, ncol, j * TB, ncol);
     else ch_issue<T>(S, L, nrow, j * TB, ncol, i * TB, ncol);
   };
-  ch_issue<T>(Lv, Li, TB, 0, nb, 0, nb);
+  ch_issue<T>(Lv, Li, ncol <= TB ? ncol : TB, 0, nb, 0, nb);
   if (nd > 0) issue(0);
   cp_async_commit();
   // block vector: y_i (forward) or w_i - W_i (backward; W_i = off-diagonal dots)

@@ -102,6 +102,13 @@ enum LaunchKind {
   L_UNUSED8, L_UNUSED9, L_UNUSED10, L_UNUSED11, L_FWD_GATHER, L_CMOD_TC, L_MAKE_G, L_DIAG_INV,
   L_BWD_OFF_RED, L_SCHUR_TC, L_FWD_CHAIN, L_BWD_CHAIN, L_BWD_GATHER, L_DEEP_MM, L_MAKE_M
 };
+// Inverse diagonal blocks of a supernode with ncol columns: TB x TB per
+// block, or ncol x ncol when it is a single block (leading dimension
+// linv_ld).
+inline long long linv_elems_of(int ncol) {
+  return ncol <= TB ? (long long)ncol * ncol : (long long)((ncol + TB - 1) / TB) * TB * TB;
+}
+
 struct Launch {
   int kind;
   long long task_off;  // into the int4 / int2 / int task arrays
@@ -372,16 +379,15 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
   H.linv_elems = 0;
   for (int s = 0; s < ns; ++s) {
     H.linv_off[s] = H.linv_elems;
-    if (S.sn[s].ncol > SOLVE_BIG) H.linv_elems += (long long)((S.sn[s].ncol + TB - 1) / TB) * TB * TB;
+    H.linv_elems += linv_elems_of((int)S.sn[s].ncol);
   }
   H.flag_off.assign(ns, -1);
   H.nflags = 0;
   H.nwave = 0;
-  for (int s = 0; s < ns; ++s)
-    if (S.sn[s].ncol > SOLVE_BIG) {
-      H.flag_off[s] = H.nflags;
-      H.nflags += (int)((S.sn[s].ncol + TB - 1) / TB);
-    }
+  for (int s = 0; s < ns; ++s) {
+    H.flag_off[s] = H.nflags;
+    H.nflags += (int)((S.sn[s].ncol + TB - 1) / TB);
+  }
   // Pull lists: every off-diagonal row r of updater k (U row uoff[k] + r)
   // lands on one column g of an ancestor; list the pushes per g in the
   // ancestor's update-list order so the gather subtracts them in that order.
@@ -528,50 +534,44 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
     // G_k = L21_k D_k of this level's updaters, for the tensor-core cmod of
     // their ancestors (32-column tasks).
     {
-      Launch Mg{L_MAKE_G, (long long)H.t2.size(), 0, 0};
-      for (int64_t s : lvl)
-        if (H.nrow[s] > S.sn[s].ncol)
-          for (int t0 = 0; t0 < S.sn[s].ncol; t0 += 32) H.t2.push_back(make_int2((int)s, t0));
-      Mg.ntasks = (int)(H.t2.size() - Mg.task_off);
+      Launch Mg{L_MAKE_G, (long long)H.t4.size(), 0, 0};
+      for (int64_t s : lvl) {
+        const int off = H.nrow[s] - (int)S.sn[s].ncol;
+        for (int t0 = 0; off > 0 && t0 < S.sn[s].ncol; t0 += 32)
+          for (int r0 = 0; r0 < off; r0 += MG_ROWS) H.t4.push_back(make_int4((int)s, t0, r0, 0));
+      }
+      Mg.ntasks = (int)(H.t4.size() - Mg.task_off);
       if (Mg.ntasks) H.fplan.push_back(Mg);
-      // inverses of the diagonal TB-blocks of this level's wide supernodes
-      // (used by the blocked triangular solves)
+      // inverses of the diagonal TB-blocks of this level's supernodes (used
+      // by the block-chain triangular solves)
       Launch Dv{L_DIAG_INV, (long long)H.t2.size(), 0, 0};
       for (int64_t s : lvl)
-        if (S.sn[s].ncol > SOLVE_BIG)
-          for (int j0 = 0; j0 < S.sn[s].ncol; j0 += TB) H.t2.push_back(make_int2((int)s, j0));
+        for (int j0 = 0; j0 < S.sn[s].ncol; j0 += TB) H.t2.push_back(make_int2((int)s, j0));
       Dv.ntasks = (int)(H.t2.size() - Dv.task_off);
       if (Dv.ntasks) H.fplan.push_back(Dv);
     }
     // Solve launches for this level.
-    // Forward: gather the descendants' pushes into y (all supernodes), solve
-    // the narrow diagonal blocks (one CTA each) and the wide ones (block
-    // chain, one launch), then stream the push U_s = L21_s z_s.
+    // Forward: gather the descendants' pushes into y, solve every
+    // supernode's diagonal blocks (block chain, one launch), then stream the
+    // push U_s = L21_s z_s.
     // Backward (levels root first): gather the ancestors' x into row order,
     // stream the off-diagonal dots W_s = L21_s^T x_anc (row-chunk partials
-    // reduced in chunk order), then the narrow and the wide diagonal solves.
+    // reduced in chunk order), then the diagonal blocks (block chain).
     {
       Launch Fg{L_FWD_GATHER, (long long)H.t2.size(), 0, 0};
       for (int64_t s : lvl)
         for (int p0 = 0; p0 < S.sn[s].ncol; p0 += SOLVE_NT / RHS_MAX) H.t2.push_back(make_int2((int)s, p0));
       Fg.ntasks = (int)(H.t2.size() - Fg.task_off);
       if (Fg.ntasks) H.fwdplan.push_back(Fg);
-      Launch Dg{L_FWD_DIAG, (long long)H.t1.size(), 0, 0};
-      for (int64_t s : lvl)
-        if (S.sn[s].ncol <= SOLVE_BIG) H.t1.push_back((int)s);
-      Dg.ntasks = (int)(H.t1.size() - Dg.task_off);
-      if (Dg.ntasks) H.fwdplan.push_back(Dg);
       int maxb = 0;
-      for (int64_t s : lvl)
-        if (S.sn[s].ncol > SOLVE_BIG) maxb = std::max(maxb, (int)((S.sn[s].ncol + TB - 1) / TB));
-      // chain items in block order across the level's wide supernodes
-      // (ticket order = dependency order)
+      for (int64_t s : lvl) maxb = std::max(maxb, (int)((S.sn[s].ncol + TB - 1) / TB));
+      // diagonal blocks: chain items in block order across the level's
+      // supernodes (ticket order = dependency order)
       if (maxb > 0) {
         Launch W{L_FWD_CHAIN, (long long)H.st4.size(), 0, H.nwave++};
         for (int b = 0; b < maxb; ++b)
           for (int64_t s : lvl)
-            if (S.sn[s].ncol > SOLVE_BIG && b * TB < S.sn[s].ncol)
-              H.st4.push_back(make_int4((int)s, 0, b, H.flag_off[s]));
+            if (b * TB < S.sn[s].ncol) H.st4.push_back(make_int4((int)s, 0, b, H.flag_off[s]));
         W.ntasks = (int)(H.st4.size() - W.task_off);
         H.fwdplan.push_back(W);
       }
@@ -616,17 +616,12 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       Launch Br{L_BWD_OFF_RED, (long long)H.st4.size(), (int)red.size(), 0};
       H.st4.insert(H.st4.end(), red.begin(), red.end());
       if (Br.ntasks) bw.push_back(Br);
-      Launch Bd{L_BWD, (long long)H.t1.size(), 0, 0};
-      for (int64_t s : lvl)
-        if (S.sn[s].ncol <= SOLVE_BIG) H.t1.push_back((int)s);
-      Bd.ntasks = (int)(H.t1.size() - Bd.task_off);
-      if (Bd.ntasks) bw.push_back(Bd);
       if (maxb > 0) {
         Launch W{L_BWD_CHAIN, (long long)H.st4.size(), 0, H.nwave++};
         for (int dd = 0; dd < maxb; ++dd)
           for (int64_t s : lvl) {
-            const int nc = (int)S.sn[s].ncol, nblk = (nc + TB - 1) / TB;
-            if (nc > SOLVE_BIG && dd < nblk) H.st4.push_back(make_int4((int)s, 1, nblk - 1 - dd, H.flag_off[s]));
+            const int nblk = (int)((S.sn[s].ncol + TB - 1) / TB);
+            if (dd < nblk) H.st4.push_back(make_int4((int)s, 1, nblk - 1 - dd, H.flag_off[s]));
           }
         W.ntasks = (int)(H.st4.size() - W.task_off);
         bw.push_back(W);
@@ -652,8 +647,6 @@ size_t smem_getf2(size_t es, int nb) {
   return std::max(a, smem_replay(es, nb)) + 64;
 }
 size_t smem_deep(size_t es, int nb) { return smem_replay(es, nb) + 64; }
-size_t smem_solve(size_t es) { return ((size_t)(SOLVE_NT / 32) * 32 * RHS_MAX + SB * (SB + 1) + SB * RHS_MAX) * es; }
-size_t smem_dots(size_t es) { return (size_t)(32 * 33 + 32 * RHS_MAX) * es; }
 size_t smem_diag_inv(size_t es) { return (size_t)TB * (TB + 1) * 2 * es; }
 
 // Threads of the BK panel kernel: its per-step trailing update is
@@ -711,8 +704,6 @@ struct KernelSetup {
     CK(cudaFuncSetAttribute(k_getf2<T, GETF2_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)smem_getf2(es, 128)));
     CK(cudaFuncSetAttribute(k_deep<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep(es, 128)));
-    CK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve(es)));
-    CK(cudaFuncSetAttribute(k_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dots(es)));
     CK(cudaFuncSetAttribute(k_diag_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_diag_inv(es)));
     if constexpr (TensorCmod<T>::ok)
       CK(cudaFuncSetAttribute(k_deep_mm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep_mm_bytes<T>()));
@@ -909,10 +900,10 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         break;
       case L_MAKE_G:
         if (!use_tc) continue;
-        k_make_g<T><<<L.ntasks, 256, 0, st>>>(fa, H.d_t2 + L.task_off);
+        k_make_g<T><<<L.ntasks, 256, 0, st>>>(fa, H.d_t4 + L.task_off);
         break;
       case L_DIAG_INV:
-        k_diag_inv<T><<<L.ntasks, TB, smem_diag_inv(es), st>>>(H.d_t2 + L.task_off, H.d_sn_ncol, H.d_sn_nrow,
+        k_diag_inv<T><<<L.ntasks, DI_NT, smem_diag_inv(es), st>>>(H.d_t2 + L.task_off, H.d_sn_ncol, H.d_sn_nrow,
                                                                  H.d_poff, (const T*)F.panel, F.status, (T*)F.linv,
                                                                  H.d_linv_off);
         break;
@@ -1113,7 +1104,6 @@ template <typename T>
 void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof = nullptr) {
   auto& H = *F.sym;
   const int n = H.n;
-  const size_t es = sizeof(T);
   cudaStream_t st = F.st;
   if (prof) prof->mark(st, -1);
   k_perm_in<T><<<grid1((long long)n * nrhs), 256, 0, st>>>(n, nrhs, H.d_perm, F.scale, b, (T*)F.Yg);
@@ -1127,9 +1117,6 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
       switch (L.kind) {
         case L_FWD_GATHER:
           k_fwd_gather<T><<<L.ntasks, SOLVE_NT, 0, st>>>(sa, H.d_t2 + L.task_off);
-          break;
-        case L_FWD_DIAG:
-          k_fwd_diag<T><<<L.ntasks, SOLVE_NT, smem_solve(es), st>>>(sa, H.d_t1 + L.task_off);
           break;
         case L_FWD_CHAIN:
           launch_solve<T, true>(1, L.ntasks, nr, sa, H.d_st4 + L.task_off, L.nb_slot, fwd_flags, st);
@@ -1152,11 +1139,8 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
         case L_BWD_OFF_RED:
           k_dots_reduce<T><<<L.ntasks, WV_NT, 0, st>>>(sa, H.d_st4 + L.task_off);
           break;
-        case L_BWD_CHAIN:
+        default:  // L_BWD_CHAIN
           launch_solve<T, false>(1, L.ntasks, nr, sa, H.d_st4 + L.task_off, L.nb_slot, bwd_flags, st);
-          break;
-        default:
-          k_bwd<T><<<L.ntasks, SOLVE_NT, smem_dots(es), st>>>(sa, H.d_t1 + L.task_off);
       }
       if (prof)
         prof->mark(st, (L.kind == L_BWD_OFF || L.kind == L_BWD_OFF_RED || L.kind == L_BWD_GATHER) ? 4 : 5, L.ntasks,
