@@ -697,12 +697,11 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
 
   T* A = reinterpret_cast<T*>(smem_raw);              // packed lower pw x pw
   const int npk = pw * (pw + 1) / 2;
-  T* l1 = A + npk;   // multipliers of the current step (column k / k+1)
-  T* l2 = l1 + pw;
-  T* u1 = l2 + pw;   // the same columns before scaling (read by the update)
-  T* u2 = u1 + pw;
+  // Two sets (by step parity) of the step's multipliers l1 / l2 (column k /
+  // k+1) and the same columns before scaling u1 / u2 (read by the update).
+  T* l1 = A + npk;
   // 16-byte aligned reduction scratch after the (possibly 4-byte) field arrays.
-  double* red_v = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(u2 + pw) + 15) & ~uintptr_t(15));
+  double* red_v = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(l1 + 8 * pw) + 15) & ~uintptr_t(15));
   int* red_i = reinterpret_cast<int*>(red_v + 32);
   int* ctl = red_i + 32;  // [0] kstep [1] kp [2] nswaps [3] error
   int* lp_s = ctl + 16;   // the block's slice of lperm
@@ -737,210 +736,244 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
   __syncthreads();
   const double alpha = (1.0 + sqrt(17.0)) / 8.0;
   int nperturbed = 0;
-  // Each pivot step: warp 0 alone does the arg-max / max reductions, the BK
-  // decision, the interchange and the multipliers (shuffles + __syncwarp),
-  // then all warps apply the rank-1 / rank-2 trailing update (warp per
-  // column) and finish column k.  Three block barriers per step; decisions
-  // and arithmetic are the reference's.
-  int* ctlk = ctl + 4;  // [0] k [1] kstep
-  T* dinv_s = reinterpret_cast<T*>(ctl + 8);  // pending scale factor
-  if (tid == 0) ctlk[0] = 0;
-  __syncthreads();
-  for (;;) {
-    const int k = ctlk[0];
-    if (k >= pw || ctl[3]) break;
-    if (warp == 0) {
-      double v = -1.0;
-      int idx = INT_MAX;
-      // blocks are at most 128 wide: four predicated lanes-strided slots
+  // Pipelined pivot steps.  Warp 0 decides step k (arg-max / max
+  // reductions, BK test, interchange, multipliers, the finished column(s) k)
+  // into the multiplier set of the step's parity; then warps 1.. apply the
+  // rank-1 / rank-2 trailing update of step k to the columns beyond the next
+  // pivot column kn = k + kstep, while warp 0 updates column kn itself and
+  // already decides step kn.  That early decision completes when the BK test
+  // needs no row maximum (so no interchange either: both would read or move
+  // entries other warps are still updating); otherwise it is redone in full
+  // after the step's barrier.  One block barrier per step on the fast path;
+  // per element the operation sequence, and every decision, are unchanged.
+  // Control slots by iteration parity: {k, kstep, pending}.
+  int* cslot = ctl + 4;
+  auto bufs = [&](int par, T*& L1, T*& L2, T*& U1, T*& U2) {
+    L1 = l1 + 4 * par * pw;
+    L2 = L1 + pw;
+    U1 = L2 + pw;
+    U2 = U1 + pw;
+  };
+  // Warp 0: decide step k into multiplier set / control slot `par`.  With
+  // `full` false, returns false (writing nothing) when the row-maximum test
+  // is needed.
+  auto decide = [&](int k, int par, bool full) -> bool {
+    T *L1, *L2, *U1, *U2;
+    bufs(par, L1, L2, U1, U2);
+    double v = -1.0;
+    int idx = INT_MAX;
+    // blocks are at most 128 wide: four predicated lanes-strided slots
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int i = k + 1 + lane + 32 * t;
+      if (i < pw) argmax_combine(v, idx, F::mag2(A[pk(i, k, pw)]), i);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+      const int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
+      argmax_combine(v, idx, v2, i2);
+    }
+    const double absakk = F::mag(A[pk(k, k, pw)]);
+    const double colmax = sqrt(v > 0.0 ? v : 0.0);
+    const int imax = v > 0.0 ? idx : k;
+    int kstep = 1, kp = k;
+    bool err = false;
+    if (fmax(absakk, colmax) == 0.0) {
+      err = pfloor < 0.0;
+    } else if (absakk >= alpha * colmax) {
+    } else {
+      if (!full) return false;
+      double rmx = 0.0;
+      for (int jj = k + lane; jj < imax; jj += 32) rmx = fmax(rmx, F::mag2(A[pk(imax, jj, pw)]));
+      for (int ii = imax + 1 + lane; ii < pw; ii += 32) rmx = fmax(rmx, F::mag2(A[pk(ii, imax, pw)]));
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) rmx = fmax(rmx, __shfl_xor_sync(0xffffffffu, rmx, o));
+      const double rowmax = sqrt(rmx);
+      if (absakk >= alpha * colmax * (colmax / rowmax)) {
+      } else if (F::mag(A[pk(imax, imax, pw)]) >= alpha * rowmax) {
+        kp = imax;
+      } else {
+        kstep = 2;
+        kp = imax;
+      }
+    }
+    if (!err) {
+      const int p = kstep == 1 ? k : k + 1;
+      if (kp != p) {
+        // swap_sym_lower_bounded(p, kp) restricted to the block + left segments.
+        const int q = kp;
+        for (int i = q + 1 + lane; i < pw; i += 32) {
+          T t = A[pk(i, p, pw)];
+          A[pk(i, p, pw)] = A[pk(i, q, pw)];
+          A[pk(i, q, pw)] = t;
+        }
+        for (int i = p + 1 + lane; i < q; i += 32) {
+          T t = A[pk(i, p, pw)];
+          A[pk(i, p, pw)] = A[pk(q, i, pw)];
+          A[pk(q, i, pw)] = t;
+        }
+        for (int jj = lane; jj < p; jj += 32) {
+          T t = A[pk(p, jj, pw)];
+          A[pk(p, jj, pw)] = A[pk(q, jj, pw)];
+          A[pk(q, jj, pw)] = t;
+        }
+        if (lane == 0) {
+          T t = A[pk(p, p, pw)];
+          A[pk(p, p, pw)] = A[pk(q, q, pw)];
+          A[pk(q, q, pw)] = t;
+          const int lpv = lp_s[p];
+          lp_s[p] = lp_s[q];
+          lp_s[q] = lpv;
+          swaps[k] = kb + q;
+          const int ns = ctl[2];
+          swp_p[ns] = kb + p;
+          swp_q[ns] = kb + q;
+          ctl[2] = ns + 1;
+        }
+        __syncwarp();
+      }
+      if (kstep == 1) {
+        T dk = A[pk(k, k, pw)];
+        if (pfloor >= 0.0) {
+          const double m = F::mag(dk);
+          if (m < pfloor) {
+            dk = m == 0.0 ? F::from_real(pfloor) : F::scale(dk, pfloor / m);
+            __syncwarp();
+            if (lane == 0) {
+              A[pk(k, k, pw)] = dk;
+              ++nperturbed;
+            }
+          }
+        } else if (F::is_zero(dk)) {
+          err = true;
+        }
+        if (!err) {
+          const T dinv = F::recip(dk);
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const int jj = k + 1 + lane + 32 * t;
+            if (jj < pw) {
+              const T a = A[pk(jj, k, pw)];
+              const T w = F::mul(a, dinv);
+              U1[jj] = a;
+              L1[jj] = w;
+              snap[k * nb + jj] = w;
+              A[pk(jj, k, pw)] = w;  // column k finished: the multipliers
+            }
+          }
+          if (lane == 0) dG[k] = dk;
+        }
+      } else {
+        T d11 = A[pk(k, k, pw)], d21 = A[pk(k + 1, k, pw)], d22 = A[pk(k + 1, k + 1, pw)];
+        T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
+        const double scale = fmax(fmax(F::mag(d11), F::mag(d22)), F::mag(d21));
+        const double growth_floor = 1e-14 * scale * scale;
+        if (pfloor >= 0.0) {
+          const double fl = fmax(pfloor * pfloor, growth_floor);
+          if (F::mag(det) < fl) {
+            const double lift = fmax(pfloor, scale * sqrt(1e-14));
+            d11 = F::add(d11, F::from_real(lift));
+            d22 = F::add(d22, F::from_real(lift));
+            det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
+            if (F::mag(det) < fl) det = F::add(det, F::from_real(fl));
+            if (lane == 0) ++nperturbed;
+          }
+        } else if (F::mag(det) <= growth_floor) {
+          err = true;
+        }
+        if (!err) {
+          const T detinv = F::recip(det);
+          if (lane == 0) {
+            dG[k] = d11;
+            dsG[k] = d21;
+            dG[k + 1] = d22;
+            kindG[k] = 1;
+            kindG[k + 1] = 2;
+          }
+          for (int i = k + 2 + lane; i < pw; i += 32) {
+            const T wik = A[pk(i, k, pw)], wik1 = A[pk(i, k + 1, pw)];
+            const T a1 = F::mul(F::sub(F::mul(d22, wik), F::mul(d21, wik1)), detinv);
+            const T a2 = F::mul(F::sub(F::mul(d11, wik1), F::mul(d21, wik)), detinv);
+            U1[i] = wik;
+            U2[i] = wik1;
+            L1[i] = a1;
+            L2[i] = a2;
+            snap[k * nb + i] = a1;
+            snap[(k + 1) * nb + i] = a2;
+            A[pk(i, k, pw)] = a1;  // columns k, k+1 finished
+            A[pk(i, k + 1, pw)] = a2;
+          }
+        }
+      }
+    }
+    if (lane == 0) {
+      if (err) ctl[3] = 1;
+      int* cs = cslot + 3 * par;
+      cs[0] = k;
+      cs[1] = kstep;
+      cs[2] = 0;
+    }
+    return true;
+  };
+  // Column jj of the trailing update of a step (one warp, lanes over rows):
+  // rank-1 with U1 / L1[jj] (skipped for a zero multiplier) or rank-2.
+  auto upd_col = [&](int jj, int kstep, const T* L1, const T* L2, const T* U1, const T* U2) {
+    const int base = pk(jj, jj, pw) - jj;  // packed index of (i, jj) = base + i
+    if (kstep == 1) {
+      const T w = L1[jj];
+      if (F::is_zero(w)) return;
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
-        const int i = k + 1 + lane + 32 * t;
-        if (i < pw) argmax_combine(v, idx, F::mag2(A[pk(i, k, pw)]), i);
+        const int i = jj + lane + 32 * t;
+        if (i < pw) A[base + i] = F::sub(A[base + i], F::mul(U1[i], w));
       }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
-        const int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
-        argmax_combine(v, idx, v2, i2);
-      }
-      const double absakk = F::mag(A[pk(k, k, pw)]);
-      const double colmax = sqrt(v > 0.0 ? v : 0.0);
-      const int imax = v > 0.0 ? idx : k;
-      int kstep = 1, kp = k;
-      bool err = false;
-      if (fmax(absakk, colmax) == 0.0) {
-        err = pfloor < 0.0;
-      } else if (absakk >= alpha * colmax) {
-      } else {
-        double rmx = 0.0;
-        for (int jj = k + lane; jj < imax; jj += 32) rmx = fmax(rmx, F::mag2(A[pk(imax, jj, pw)]));
-        for (int ii = imax + 1 + lane; ii < pw; ii += 32) rmx = fmax(rmx, F::mag2(A[pk(ii, imax, pw)]));
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) rmx = fmax(rmx, __shfl_xor_sync(0xffffffffu, rmx, o));
-        const double rowmax = sqrt(rmx);
-        if (absakk >= alpha * colmax * (colmax / rowmax)) {
-        } else if (F::mag(A[pk(imax, imax, pw)]) >= alpha * rowmax) {
-          kp = imax;
-        } else {
-          kstep = 2;
-          kp = imax;
-        }
-      }
-      if (!err) {
-        const int p = kstep == 1 ? k : k + 1;
-        if (kp != p) {
-          // swap_sym_lower_bounded(p, kp) restricted to the block + left segments.
-          const int q = kp;
-          for (int i = q + 1 + lane; i < pw; i += 32) {
-            T t = A[pk(i, p, pw)];
-            A[pk(i, p, pw)] = A[pk(i, q, pw)];
-            A[pk(i, q, pw)] = t;
-          }
-          for (int i = p + 1 + lane; i < q; i += 32) {
-            T t = A[pk(i, p, pw)];
-            A[pk(i, p, pw)] = A[pk(q, i, pw)];
-            A[pk(q, i, pw)] = t;
-          }
-          for (int jj = lane; jj < p; jj += 32) {
-            T t = A[pk(p, jj, pw)];
-            A[pk(p, jj, pw)] = A[pk(q, jj, pw)];
-            A[pk(q, jj, pw)] = t;
-          }
-          if (lane == 0) {
-            T t = A[pk(p, p, pw)];
-            A[pk(p, p, pw)] = A[pk(q, q, pw)];
-            A[pk(q, q, pw)] = t;
-            const int lpv = lp_s[p];
-            lp_s[p] = lp_s[q];
-            lp_s[q] = lpv;
-            swaps[k] = kb + q;
-            const int ns = ctl[2];
-            swp_p[ns] = kb + p;
-            swp_q[ns] = kb + q;
-            ctl[2] = ns + 1;
-          }
-          __syncwarp();
-        }
-        if (kstep == 1) {
-          T dk = A[pk(k, k, pw)];
-          if (pfloor >= 0.0) {
-            const double m = F::mag(dk);
-            if (m < pfloor) {
-              dk = m == 0.0 ? F::from_real(pfloor) : F::scale(dk, pfloor / m);
-              __syncwarp();
-              if (lane == 0) {
-                A[pk(k, k, pw)] = dk;
-                ++nperturbed;
-              }
-            }
-          } else if (F::is_zero(dk)) {
-            err = true;
-          }
-          if (!err) {
-            const T dinv = F::recip(dk);
-#pragma unroll
-            for (int t = 0; t < 4; ++t) {
-              const int jj = k + 1 + lane + 32 * t;
-              if (jj < pw) {
-                const T a = A[pk(jj, k, pw)];
-                const T w = F::mul(a, dinv);
-                u1[jj] = a;
-                l1[jj] = w;
-                snap[k * nb + jj] = w;
-              }
-            }
-            if (lane == 0) {
-              dG[k] = dk;
-              *dinv_s = dinv;
-            }
-          }
-        } else {
-          T d11 = A[pk(k, k, pw)], d21 = A[pk(k + 1, k, pw)], d22 = A[pk(k + 1, k + 1, pw)];
-          T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
-          const double scale = fmax(fmax(F::mag(d11), F::mag(d22)), F::mag(d21));
-          const double growth_floor = 1e-14 * scale * scale;
-          if (pfloor >= 0.0) {
-            const double fl = fmax(pfloor * pfloor, growth_floor);
-            if (F::mag(det) < fl) {
-              const double lift = fmax(pfloor, scale * sqrt(1e-14));
-              d11 = F::add(d11, F::from_real(lift));
-              d22 = F::add(d22, F::from_real(lift));
-              det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
-              if (F::mag(det) < fl) det = F::add(det, F::from_real(fl));
-              if (lane == 0) ++nperturbed;
-            }
-          } else if (F::mag(det) <= growth_floor) {
-            err = true;
-          }
-          if (!err) {
-            const T detinv = F::recip(det);
-            if (lane == 0) {
-              dG[k] = d11;
-              dsG[k] = d21;
-              dG[k + 1] = d22;
-              kindG[k] = 1;
-              kindG[k + 1] = 2;
-            }
-            for (int i = k + 2 + lane; i < pw; i += 32) {
-              const T wik = A[pk(i, k, pw)], wik1 = A[pk(i, k + 1, pw)];
-              const T a1 = F::mul(F::sub(F::mul(d22, wik), F::mul(d21, wik1)), detinv);
-              const T a2 = F::mul(F::sub(F::mul(d11, wik1), F::mul(d21, wik)), detinv);
-              u1[i] = wik;
-              u2[i] = wik1;
-              l1[i] = a1;
-              l2[i] = a2;
-              snap[k * nb + i] = a1;
-              snap[(k + 1) * nb + i] = a2;
-            }
-          }
-        }
-      }
-      if (lane == 0) {
-        if (err) ctl[3] = 1;
-        ctlk[1] = kstep;
-      }
-    }
-    __syncthreads();
-    if (ctl[3]) break;
-    // Trailing update of step k by all warps, reading the unscaled pivot
-    // column(s) from u1/u2, while column(s) k are finished in place (1x1:
-    // scaled by 1/d; 2x2: the multipliers) — disjoint columns, one barrier.
-    const int kstep = ctlk[1];
-    if (kstep == 1) {
-      for (int jj = k + 1 + warp; jj < pw; jj += NW) {
-        const T w = l1[jj];
-        if (F::is_zero(w)) continue;
-        const int base = pk(jj, jj, pw) - jj;  // packed index of (i, jj) = base + i
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const int i = jj + lane + 32 * t;
-          if (i < pw) A[base + i] = F::sub(A[base + i], F::mul(u1[i], w));
-        }
-      }
-      const T dinv = *dinv_s;
-      for (int i = k + 1 + tid; i < pw; i += NT) A[pk(i, k, pw)] = F::mul(u1[i], dinv);
     } else {
-      for (int jj = k + 2 + warp; jj < pw; jj += NW) {
-        const T a1 = l1[jj], a2 = l2[jj];
-        const int base = pk(jj, jj, pw) - jj;
+      const T a1 = L1[jj], a2 = L2[jj];
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const int i = jj + lane + 32 * t;
-          if (i < pw) {
-            T x = A[base + i];
-            x = F::sub(x, F::mul(u1[i], a1));
-            x = F::sub(x, F::mul(u2[i], a2));
-            A[base + i] = x;
-          }
+      for (int t = 0; t < 4; ++t) {
+        const int i = jj + lane + 32 * t;
+        if (i < pw) {
+          T x = A[base + i];
+          x = F::sub(x, F::mul(U1[i], a1));
+          x = F::sub(x, F::mul(U2[i], a2));
+          A[base + i] = x;
         }
       }
-      for (int i = k + 2 + tid; i < pw; i += NT) {
-        A[pk(i, k, pw)] = l1[i];
-        A[pk(i, k + 1, pw)] = l2[i];
-      }
     }
-    if (tid == 0) ctlk[0] = k + kstep;
+  };
+  if (warp == 0) decide(0, 0, true);
+  __syncthreads();
+  for (int it = 0;; ++it) {
+    const int par = it & 1;
+    int k = cslot[3 * par], kstep = cslot[3 * par + 1];
+    if (k >= pw || ctl[3]) break;
+    if (cslot[3 * par + 2]) {
+      // the early decision of step k needed the row maximum: redo it in full
+      __syncthreads();
+      if (warp == 0) decide(k, par, true);
+      __syncthreads();
+      if (ctl[3]) break;
+      kstep = cslot[3 * par + 1];
+    }
+    T *L1, *L2, *U1, *U2;
+    bufs(par, L1, L2, U1, U2);
+    const int kn = k + kstep;
+    if (warp == 0) {
+      if (kn < pw) {
+        upd_col(kn, kstep, L1, L2, U1, U2);
+        __syncwarp();
+        if (!decide(kn, par ^ 1, false) && lane == 0) {
+          int* cs = cslot + 3 * (par ^ 1);
+          cs[0] = kn;
+          cs[2] = 1;
+        }
+      } else if (lane == 0) {
+        cslot[3 * (par ^ 1)] = kn;
+      }
+    } else {
+      for (int jj = kn + 1 + (warp - 1); jj < pw; jj += NW - 1) upd_col(jj, kstep, L1, L2, U1, U2);
+    }
     __syncthreads();
   }
   for (int i = tid; i < pw; i += NT) lpermG[kb + i] = lp_s[i];

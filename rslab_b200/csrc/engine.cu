@@ -643,7 +643,7 @@ size_t smem_replay(size_t es, int nb) {
   return (((size_t)(DEEP_R + 1) * nb * es + 15) & ~size_t(15)) + (size_t)nb * (3 * es + 4 + 1) + 16;
 }
 size_t smem_getf2(size_t es, int nb) {
-  size_t a = (size_t)nb * (nb + 1) / 2 * es + 4 * nb * es + 16 + 32 * 8 + 32 * 4 + 16 * 4 + 4 * nb * 4;
+  size_t a = (size_t)nb * (nb + 1) / 2 * es + 8 * nb * es + 16 + 32 * 8 + 32 * 4 + 16 * 4 + 4 * nb * 4;
   return std::max(a, smem_replay(es, nb)) + 64;
 }
 size_t smem_deep(size_t es, int nb) { return smem_replay(es, nb) + 64; }
