@@ -48,7 +48,7 @@ def parse():
     p.add_argument("--nrhs", type=int, default=16)
     p.add_argument("--target", type=float, default=1e-14)
     p.add_argument("--no-fp64", action="store_true")
-    p.add_argument("--cpu-sample-side", type=int, default=28)
+    p.add_argument("--cpu-sample-side", type=int, default=36)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--profile-step", action="store_true",
                    help="one warm-up mixed step, then exactly one mixed step between "
@@ -342,7 +342,6 @@ def main():
                 "traffic": (bpf * cm["flops"] / max(tc_n, 1)) if bpf else None,
                 "traffic_note": "dram bytes per launch: ncu bytes per algorithmic flop (profiles/"
                                 "k_cmod_tc_helmholtz48.md) x this run's flops per launch",
-                "algorithmic_bytes_per_launch": None,
                 "peak_source": ("MEASURED_PEAKS.json bf16_tflops (burst), of measured" if "bf16_tflops" in peaks
                                 else "fallback 1590 TFLOP/s"),
                 "launches": tc_n, "avg_launch_ms": tc_ms / max(tc_n, 1),
