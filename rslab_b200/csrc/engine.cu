@@ -114,6 +114,8 @@ struct Launch {
   long long task_off;  // into the int4 / int2 / int task arrays
   int ntasks;
   int nb_slot;         // getf2/deep: scratch stride nb; chain solves: ticket counter
+  int side = 0;        // factor: may run on the side stream, overlapping the next block's
+                       // getf2 / deep-row launches (Schur update beyond the next block)
 };
 
 }  // namespace
@@ -478,7 +480,7 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
     for (int64_t s : lvl) maxblocks = std::max(maxblocks, (int)((S.sn[s].ncol + nb_of(s) - 1) / nb_of(s)));
     for (int b = 0; b < maxblocks; ++b) {
       Launch G{L_GETF2, (long long)H.t4.size(), 0, 0};
-      std::vector<int4> deep, make_m, deep_mm, schur, schur_tc;
+      std::vector<int4> deep, make_m, deep_mm, schur, schur_tc, schur_r, schur_tc_r;
       int slot = 0, launch_nb = 0;
       for (int64_t s : lvl) {
         int nb = nb_of(s), nc = (int)S.sn[s].ncol, nr = H.nrow[s];
@@ -498,10 +500,14 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         H.kind_flops[2] += 2.0 * pw * pw * pw / 3.0;
         H.kind_flops[3] += 2.0 * (double)(nr - ke) * pw * pw / 2.0;
         H.kind_flops[4] += 2.0 * ((double)mt * cw - (double)cw * (cw - 1) / 2.0) * pw;
+        // Schur tiles of the next block's columns [ke, ke + nb) first; the
+        // rest may overlap the next block's panel factorization
+        const int nxt = std::min(nb, cw);
         for (int c0 = 0; c0 < cw; c0 += TILE)
-          for (int r0 = c0; r0 < mt; r0 += TILE) schur.push_back(make_int4((int)s, kb, r0, c0));
+          for (int r0 = c0; r0 < mt; r0 += TILE) (c0 < nxt ? schur : schur_r).push_back(make_int4((int)s, kb, r0, c0));
         for (int c0 = 0; c0 < cw; c0 += TC_N)
-          for (int r0 = (c0 / TC_M) * TC_M; r0 < mt; r0 += TC_M) schur_tc.push_back(make_int4((int)s, kb, r0, c0));
+          for (int r0 = (c0 / TC_M) * TC_M; r0 < mt; r0 += TC_M)
+            (c0 < nxt ? schur_tc : schur_tc_r).push_back(make_int4((int)s, kb, r0, c0));
         ++slot;
       }
       G.ntasks = slot;
@@ -528,6 +534,14 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         H.fplan.push_back(C);
         Launch Ct{L_SCHUR_TC, (long long)H.t4.size(), (int)schur_tc.size(), 0};
         H.t4.insert(H.t4.end(), schur_tc.begin(), schur_tc.end());
+        H.fplan.push_back(Ct);
+      }
+      if (!schur_r.empty()) {
+        Launch C{L_SCHUR, (long long)H.t4.size(), (int)schur_r.size(), 0, 1};
+        H.t4.insert(H.t4.end(), schur_r.begin(), schur_r.end());
+        H.fplan.push_back(C);
+        Launch Ct{L_SCHUR_TC, (long long)H.t4.size(), (int)schur_tc_r.size(), 0, 1};
+        H.t4.insert(H.t4.end(), schur_tc_r.begin(), schur_tc_r.end());
         H.fplan.push_back(Ct);
       }
     }
@@ -763,6 +777,9 @@ struct rslab_fac_handle {
   int last_status = 0, failing_sn = -1;
   double factor_ms = 0, solve_ms = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // side stream of the factor (lowest priority) and its fork / join events
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // per-launch rows of the last factor/solve profile
   std::vector<int> tr_kind, tr_grid;
   std::vector<float> tr_ms;
@@ -776,6 +793,9 @@ struct rslab_fac_handle {
     if (sgraph) cudaGraphExecDestroy(sgraph);
     if (h_status) cudaFreeHost(h_status);
     if (h_wstat) cudaFreeHost(h_wstat);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (st2) cudaStreamDestroy(st2);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (own_stream && st) cudaStreamDestroy(st);
@@ -883,16 +903,44 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
     k_force_floor<<<1, 1, 0, st>>>(F.amax_dev, F.floor_dev);
   }
   if (prof) prof->mark(st, 0);
+  // Launches marked `side` (the Schur update beyond the next block) run on
+  // the side stream when not profiling; every later launch except the next
+  // block's getf2 / deep-row launches waits for them first.
+  const bool overlap = prof == nullptr && F.st2 != nullptr;
+  bool side_pending = false;
+  auto runs = [&](const Launch& L) {
+    switch (L.kind) {
+      case L_CMOD: return !use_tc;
+      case L_CMOD_TC: return use_tc;
+      case L_MAKE_G: return use_tc;
+      case L_DEEP: return !fa.deep_mm;
+      case L_MAKE_M: case L_DEEP_MM: return fa.deep_mm != 0;
+      case L_SCHUR: return !use_tc;
+      case L_SCHUR_TC: return use_tc;
+      default: return true;
+    }
+  };
   for (const Launch& L : H.fplan) {
+    if (!runs(L)) continue;
+    cudaStream_t ls = st;
+    if (overlap && L.side) {
+      CK(cudaEventRecord(F.ev_fork, st));
+      CK(cudaStreamWaitEvent(F.st2, F.ev_fork, 0));
+      ls = F.st2;
+    } else if (side_pending && L.kind != L_GETF2 && L.kind != L_DEEP && L.kind != L_MAKE_M &&
+               L.kind != L_DEEP_MM) {
+      CK(cudaStreamWaitEvent(st, F.ev_join, 0));
+      side_pending = false;
+    }
     switch (L.kind) {
       case L_CMOD:
         if (use_tc) continue;
-        k_cmod<T><<<L.ntasks, TPB, smem_cmod(es), st>>>(fa, H.d_t4 + L.task_off, H.d_cpairs);
+        k_cmod<T><<<L.ntasks, TPB, smem_cmod(es), ls>>>(fa, H.d_t4 + L.task_off, H.d_cpairs);
         break;
       case L_CMOD_TC:
         if constexpr (TensorCmod<T>::ok) {
           if (!use_tc) continue;
-          k_cmod_tc<T><<<L.ntasks, TC_NT, smem_cmod_tc_bytes(), st>>>(fa, H.d_t4tc + L.task_off, H.d_cpairs_tc,
+          k_cmod_tc<T><<<L.ntasks, TC_NT, smem_cmod_tc_bytes(), ls>>>(fa, H.d_t4tc + L.task_off, H.d_cpairs_tc,
                                                                       H.d_tcmaps);
         } else {
           continue;
@@ -900,17 +948,17 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         break;
       case L_MAKE_G:
         if (!use_tc) continue;
-        k_make_g<T><<<L.ntasks, 256, 0, st>>>(fa, H.d_t4 + L.task_off);
+        k_make_g<T><<<L.ntasks, 256, 0, ls>>>(fa, H.d_t4 + L.task_off);
         break;
       case L_DIAG_INV:
-        k_diag_inv<T><<<L.ntasks, DI_NT, smem_diag_inv(es), st>>>(H.d_t2 + L.task_off, H.d_sn_ncol, H.d_sn_nrow,
+        k_diag_inv<T><<<L.ntasks, DI_NT, smem_diag_inv(es), ls>>>(H.d_t2 + L.task_off, H.d_sn_ncol, H.d_sn_nrow,
                                                                  H.d_poff, (const T*)F.panel, F.status, (T*)F.linv,
                                                                  H.d_linv_off);
         break;
       case L_GETF2: {
         FactorArgs f2 = fa;
         f2.scratch_stride = getf2_scratch_stride(L.nb_slot, (long long)es);
-        k_getf2<T, GETF2_NT><<<L.ntasks, GETF2_NT, smem_getf2(es, L.nb_slot), st>>>(f2, H.d_t4 + L.task_off,
+        k_getf2<T, GETF2_NT><<<L.ntasks, GETF2_NT, smem_getf2(es, L.nb_slot), ls>>>(f2, H.d_t4 + L.task_off,
                                                                                   nb_small, nb_big);
         break;
       }
@@ -918,14 +966,14 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         if (fa.deep_mm) continue;
         FactorArgs f2 = fa;
         f2.scratch_stride = getf2_scratch_stride(L.nb_slot, (long long)es);
-        k_deep<T, 256><<<L.ntasks, 256, smem_deep(es, L.nb_slot), st>>>(f2, H.d_t4 + L.task_off, nb_small, nb_big);
+        k_deep<T, 256><<<L.ntasks, 256, smem_deep(es, L.nb_slot), ls>>>(f2, H.d_t4 + L.task_off, nb_small, nb_big);
         break;
       }
       case L_MAKE_M: {
         if (!fa.deep_mm) continue;
         FactorArgs f2 = fa;
         f2.scratch_stride = getf2_scratch_stride(L.nb_slot, (long long)es);
-        k_make_m<T, 32 * MM_RB><<<L.ntasks, 32 * MM_RB, smem_make_m_bytes(es, L.nb_slot), st>>>(
+        k_make_m<T, 32 * MM_RB><<<L.ntasks, 32 * MM_RB, smem_make_m_bytes(es, L.nb_slot), ls>>>(
             f2, H.d_t4 + L.task_off, nb_small, nb_big);
         break;
       }
@@ -934,18 +982,18 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         if constexpr (TensorCmod<T>::ok) {
           FactorArgs f2 = fa;
           f2.scratch_stride = getf2_scratch_stride(L.nb_slot, (long long)es);
-          k_deep_mm<T><<<L.ntasks, 256, smem_deep_mm_bytes<T>(), st>>>(f2, H.d_t4 + L.task_off, nb_small, nb_big);
+          k_deep_mm<T><<<L.ntasks, 256, smem_deep_mm_bytes<T>(), ls>>>(f2, H.d_t4 + L.task_off, nb_small, nb_big);
         }
         break;
       }
       case L_SCHUR:
         if (use_tc) continue;
-        k_schur<T><<<L.ntasks, TPB, smem_schur(es), st>>>(fa, H.d_t4 + L.task_off, nb_small, nb_big);
+        k_schur<T><<<L.ntasks, TPB, smem_schur(es), ls>>>(fa, H.d_t4 + L.task_off, nb_small, nb_big);
         break;
       case L_SCHUR_TC:
         if constexpr (TensorCmod<T>::ok) {
           if (!use_tc) continue;
-          k_schur_tc<T><<<L.ntasks, TC_NT, smem_cmod_tc_bytes(), st>>>(fa, H.d_t4 + L.task_off, nb_small, nb_big);
+          k_schur_tc<T><<<L.ntasks, TC_NT, smem_cmod_tc_bytes(), ls>>>(fa, H.d_t4 + L.task_off, nb_small, nb_big);
         } else {
           continue;
         }
@@ -959,7 +1007,12 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
                  : (L.kind == L_DEEP || L.kind == L_DEEP_MM || L.kind == L_MAKE_M) ? 3
                                                                                : 4,
                  L.ntasks, L.kind);
+    if (ls != st) {
+      CK(cudaEventRecord(F.ev_join, ls));
+      side_pending = true;
+    }
   }
+  if (side_pending) CK(cudaStreamWaitEvent(st, F.ev_join, 0));
   if (F.set.drop_tol > 0.0 && H.ns > 0) k_drop_tol<T><<<H.ns, 256, 0, st>>>(fa, F.set.drop_tol);
   CK(cudaMemsetAsync(F.cnt3, 0, 3 * sizeof(unsigned long long), st));
   k_inertia<T><<<grid1(n), 256, 0, st>>>(n, (const T*)F.d, (const T*)F.dsub, F.kind, F.cnt3);
@@ -982,7 +1035,9 @@ void run_factor(rslab_fac_handle& F) {
         throw;
       }
       CK(cudaStreamEndCapture(F.st, &g));
-      CK(cudaGraphInstantiate(&F.fgraph, g, 0));
+      // per-node priorities: the panel chain's launches go ahead of the
+      // overlapping Schur update when SMs free up
+      CK(cudaGraphInstantiate(&F.fgraph, g, cudaGraphInstantiateFlagUseNodePriority));
       cudaGraphDestroy(g);
     }
     CK(cudaGraphLaunch(F.fgraph, F.st));
@@ -1552,14 +1607,20 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
       F->set = *settings;
     else
       rslab_default_factor_settings(&F->set);
+    int prio_lo = 0, prio_hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     if (F->set.stream) {
       F->st = (cudaStream_t)F->set.stream;
     } else {
-      CK(cudaStreamCreateWithFlags(&F->st, cudaStreamNonBlocking));
+      // the panel chain (getf2, deep rows) runs here: highest priority
+      CK(cudaStreamCreateWithPriority(&F->st, cudaStreamNonBlocking, prio_hi));
       F->own_stream = true;
     }
+    CK(cudaStreamCreateWithPriority(&F->st2, cudaStreamNonBlocking, prio_lo));
     CK(cudaEventCreate(&F->ev0));
     CK(cudaEventCreate(&F->ev1));
+    CK(cudaEventCreateWithFlags(&F->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&F->ev_join, cudaEventDisableTiming));
     sym->ensure_device(F->st);
     const size_t es = elem_size(dtype);
     const int n = sym->n;
