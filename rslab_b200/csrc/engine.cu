@@ -100,7 +100,8 @@ enum LaunchKind {
   L_CMOD, L_GETF2, L_DEEP, L_SCHUR,
   L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD,
   L_UNUSED8, L_UNUSED9, L_UNUSED10, L_UNUSED11, L_FWD_GATHER, L_CMOD_TC, L_MAKE_G, L_DIAG_INV,
-  L_BWD_OFF_RED, L_SCHUR_TC, L_FWD_CHAIN, L_BWD_CHAIN, L_BWD_GATHER, L_DEEP_MM, L_MAKE_M
+  L_BWD_OFF_RED, L_SCHUR_TC, L_FWD_CHAIN, L_BWD_CHAIN, L_BWD_GATHER, L_DEEP_MM, L_MAKE_M,
+  L_JOIN_CM  // no kernel: the level's early cmod updates must be complete from here on
 };
 // Inverse diagonal blocks of a supernode with ncol columns: TB x TB per
 // block, or ncol x ncol when it is a single block (leading dimension
@@ -114,8 +115,10 @@ struct Launch {
   long long task_off;  // into the int4 / int2 / int task arrays
   int ntasks;
   int nb_slot;         // getf2/deep: scratch stride nb; chain solves: ticket counter
-  int side = 0;        // factor: may run on the side stream, overlapping the next block's
-                       // getf2 / deep-row launches (Schur update beyond the next block)
+  int side = 0;        // factor: 1 = may run on the side stream, overlapping the next block's
+                       // getf2 / deep-row launches (Schur update beyond the next block);
+                       // 2 = on the cmod stream, overlapping the whole level (early
+                       // tensor-core cmod of the next level, tagged by nb_slot)
 };
 
 }  // namespace
@@ -271,8 +274,12 @@ namespace {
 // With `maps`, every pair also gets its inverse scatter maps (tr + tcw
 // bytes: for each tile row / column the index of k's row landing there
 // inside the pair's run, or -1).
+// `lv_of` / [lv_lo, lv_hi]: when given, only updaters whose tree level lies
+// in that range contribute pairs (the tensor-core cmod splits a level's
+// updates into those final one level earlier and the rest).
 void add_cmod_tiles(rslab_sym_handle& H, const std::vector<int64_t>& lvl, int tr, int tcw, std::vector<int4>& tasks,
-                    std::vector<int4>& pairs, bool count_flops, std::vector<int8_t>* maps = nullptr) {
+                    std::vector<int4>& pairs, bool count_flops, std::vector<int8_t>* maps = nullptr,
+                    const std::vector<int>* lv_of = nullptr, int lv_lo = 0, int lv_hi = 0) {
   const auto& S = H.S;
   for (int64_t s : lvl) {
     if (S.upd_ptr[s + 1] == S.upd_ptr[s]) continue;
@@ -284,6 +291,7 @@ void add_cmod_tiles(rslab_sym_handle& H, const std::vector<int64_t>& lvl, int tr
     std::vector<std::vector<int8_t>> tm(maps ? (size_t)ntc * ntr : 0);
     for (int64_t u = S.upd_ptr[s]; u < S.upd_ptr[s + 1]; ++u) {
       const int64_t k = S.upd[u], p0 = S.upd_p0[u], p1 = S.upd_p1[u];
+      if (lv_of && ((*lv_of)[k] < lv_lo || (*lv_of)[k] > lv_hi)) continue;
       const int64_t nck = S.sn[k].ncol;
       const int64_t* ok = S.rs.data() + S.rs_ptr[k] + nck;
       const int64_t nok = S.rs_ptr[k + 1] - S.rs_ptr[k] - nck;
@@ -461,18 +469,34 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
   H.max_nb = nb_big;
   auto nb_of = [&](int s) { return S.sn[s].ncol >= 512 ? nb_big : nb_small; };
   std::vector<std::vector<Launch>> bw_levels;
-  for (const auto& lvl : S.by_level) {
+  std::vector<int> lv_of(ns, 0);
+  for (size_t li = 0; li < S.by_level.size(); ++li)
+    for (int64_t s : S.by_level[li]) lv_of[s] = (int)li;
+  const int nlev = (int)S.by_level.size();
+  for (int li = 0; li < nlev; ++li) {
+    const auto& lvl = S.by_level[li];
     // cmod tiles of every panel that has updaters, each with its precomputed
     // list of (updater, row run, column run) pairs in update-list order:
     // TILE x TILE tiles for the CUDA-core kernel, TC_M x TC_N tiles for the
-    // tensor-core kernel of the single-precision fields.
+    // tensor-core kernel of the single-precision fields.  The tensor-core
+    // updates of the NEXT level from updaters two or more levels below it
+    // are final now: they go first, marked to overlap this level (side 2,
+    // tag = their level); this level's own launch then adds the updates
+    // from the level just below.
     {
+      if (li + 1 < nlev) {
+        Launch Le{L_CMOD_TC, (long long)H.t4tc.size(), 0, li + 1, 2};
+        add_cmod_tiles(H, S.by_level[li + 1], TC_M, TC_N, H.t4tc, H.cpairs_tc, false, &H.tcmaps, &lv_of, 0, li - 1);
+        Le.ntasks = (int)(H.t4tc.size() - Le.task_off);
+        if (Le.ntasks) H.fplan.push_back(Le);
+      }
+      H.fplan.push_back(Launch{L_JOIN_CM, 0, 0, li});
       Launch L{L_CMOD, (long long)H.t4.size(), 0, 0};
       add_cmod_tiles(H, lvl, TILE, TILE, H.t4, H.cpairs, true);
       L.ntasks = (int)(H.t4.size() - L.task_off);
       if (L.ntasks) H.fplan.push_back(L);
-      Launch Lt{L_CMOD_TC, (long long)H.t4tc.size(), 0, 0};
-      add_cmod_tiles(H, lvl, TC_M, TC_N, H.t4tc, H.cpairs_tc, false, &H.tcmaps);
+      Launch Lt{L_CMOD_TC, (long long)H.t4tc.size(), 0, li};
+      add_cmod_tiles(H, lvl, TC_M, TC_N, H.t4tc, H.cpairs_tc, false, &H.tcmaps, &lv_of, li - 1, li - 1);
       Lt.ntasks = (int)(H.t4tc.size() - Lt.task_off);
       if (Lt.ntasks) H.fplan.push_back(Lt);
     }
@@ -778,8 +802,8 @@ struct rslab_fac_handle {
   double factor_ms = 0, solve_ms = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // side stream of the factor (lowest priority) and its fork / join events
-  cudaStream_t st2 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t st2 = nullptr, st3 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_cm[2] = {nullptr, nullptr};
   // per-launch rows of the last factor/solve profile
   std::vector<int> tr_kind, tr_grid;
   std::vector<float> tr_ms;
@@ -795,7 +819,10 @@ struct rslab_fac_handle {
     if (h_wstat) cudaFreeHost(h_wstat);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    for (cudaEvent_t e : ev_cm)
+      if (e) cudaEventDestroy(e);
     if (st2) cudaStreamDestroy(st2);
+    if (st3) cudaStreamDestroy(st3);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (own_stream && st) cudaStreamDestroy(st);
@@ -920,10 +947,21 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
       default: return true;
     }
   };
+  bool cm_pending[2] = {false, false};
   for (const Launch& L : H.fplan) {
     if (!runs(L)) continue;
     cudaStream_t ls = st;
-    if (overlap && L.side) {
+    if (L.kind == L_JOIN_CM) {
+      // this level's early updates (forked one level ago) precede all of its work
+      if (cm_pending[L.nb_slot & 1]) CK(cudaStreamWaitEvent(st, F.ev_cm[L.nb_slot & 1], 0));
+      cm_pending[L.nb_slot & 1] = false;
+      continue;
+    }
+    if (overlap && L.side == 2) {
+      CK(cudaEventRecord(F.ev_fork, st));
+      CK(cudaStreamWaitEvent(F.st3, F.ev_fork, 0));
+      ls = F.st3;
+    } else if (overlap && L.side == 1) {
       CK(cudaEventRecord(F.ev_fork, st));
       CK(cudaStreamWaitEvent(F.st2, F.ev_fork, 0));
       ls = F.st2;
@@ -1007,12 +1045,17 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
                  : (L.kind == L_DEEP || L.kind == L_DEEP_MM || L.kind == L_MAKE_M) ? 3
                                                                                : 4,
                  L.ntasks, L.kind);
-    if (ls != st) {
+    if (ls == F.st3) {
+      CK(cudaEventRecord(F.ev_cm[L.nb_slot & 1], ls));
+      cm_pending[L.nb_slot & 1] = true;
+    } else if (ls != st) {
       CK(cudaEventRecord(F.ev_join, ls));
       side_pending = true;
     }
   }
   if (side_pending) CK(cudaStreamWaitEvent(st, F.ev_join, 0));
+  for (int q = 0; q < 2; ++q)
+    if (cm_pending[q]) CK(cudaStreamWaitEvent(st, F.ev_cm[q], 0));
   if (F.set.drop_tol > 0.0 && H.ns > 0) k_drop_tol<T><<<H.ns, 256, 0, st>>>(fa, F.set.drop_tol);
   CK(cudaMemsetAsync(F.cnt3, 0, 3 * sizeof(unsigned long long), st));
   k_inertia<T><<<grid1(n), 256, 0, st>>>(n, (const T*)F.d, (const T*)F.dsub, F.kind, F.cnt3);
@@ -1617,6 +1660,8 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
       F->own_stream = true;
     }
     CK(cudaStreamCreateWithPriority(&F->st2, cudaStreamNonBlocking, prio_lo));
+    CK(cudaStreamCreateWithPriority(&F->st3, cudaStreamNonBlocking, prio_lo));
+    for (cudaEvent_t& e : F->ev_cm) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     CK(cudaEventCreate(&F->ev0));
     CK(cudaEventCreate(&F->ev1));
     CK(cudaEventCreateWithFlags(&F->ev_fork, cudaEventDisableTiming));
