@@ -142,6 +142,11 @@ void rslab_default_factor_settings(rslab_factor_settings* s);
 /* Phase 1: analyze a lower-triangle CSC pattern (n, col_ptr[n+1], row_idx). */
 int rslab_analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx,
                   const rslab_analyze_settings* settings, rslab_sym_handle** out);
+/* CscMatrix::validate (src/sparse/csc.rs:157) for a lower-triangular CSC: col_ptr
+ * starts at 0, ends at nnz and never decreases; row indices in [0, n), on or
+ * below the diagonal and strictly increasing in each column.  Returns
+ * RSLAB_INVALID_INPUT with a message naming the first offending column. */
+int rslab_validate_lower_csc(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, int64_t nnz);
 int rslab_symbolic_info(const rslab_sym_handle* sym, rslab_symbolic_info_t* info);
 int rslab_symbolic_export(const rslab_sym_handle* sym, int64_t* perm, int64_t* sn_first, int64_t* sn_ncol,
                           int64_t* sn_nrow, int64_t* sn_level, int64_t* child_ptr, int64_t* child_idx,

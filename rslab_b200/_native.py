@@ -83,6 +83,7 @@ SIGNATURES = {
     "rslab_default_analyze_settings": (None, [C.POINTER(AnalyzeSettings)]),
     "rslab_default_factor_settings": (None, [C.POINTER(FactorSettings)]),
     "rslab_analyze": (C.c_int, [C.c_int64, i64p, i64p, C.POINTER(AnalyzeSettings), C.POINTER(vp)]),
+    "rslab_validate_lower_csc": (C.c_int, [C.c_int64, i64p, i64p, C.c_int64]),
     "rslab_symbolic_info": (C.c_int, [vp, C.POINTER(SymbolicInfo)]),
     "rslab_symbolic_export": (C.c_int, [vp, i64p, i64p, i64p, i64p, i64p, i64p, i64p, i64p, i64p]),
     "rslab_free_symbolic": (None, [vp]),

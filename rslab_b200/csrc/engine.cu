@@ -1472,6 +1472,16 @@ void rslab_default_factor_settings(rslab_factor_settings* s) {
   s->drop_tol = 0.0;
 }
 
+int rslab_validate_lower_csc(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, int64_t nnz) {
+  try {
+    if (n < 0 || !col_ptr || (nnz > 0 && !row_idx)) throw RslabError(Status::InvalidInput, "bad CSC arrays");
+    rslab::validate_lower_csc(n, col_ptr, row_idx, nnz);
+    return 0;
+  } catch (const RslabError& e) {
+    return fail(e);
+  }
+}
+
 int rslab_analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, const rslab_analyze_settings* settings,
                   rslab_sym_handle** out) {
   try {

@@ -135,17 +135,11 @@ class CscMatrix:
             raise InvalidInput(f"col_ptr[0] must be 0, got {self.col_ptr[0]}")
         if self.col_ptr[n] != self.row_idx.shape[0]:
             raise InvalidInput("col_ptr[n] != nnz")
-        if np.any(np.diff(self.col_ptr) < 0):
-            raise InvalidInput("col_ptr not monotonically non-decreasing")
-        cols = np.repeat(np.arange(n), np.diff(self.col_ptr))
-        r = self.row_idx
-        if len(r) and (r.min() < 0 or r.max() >= n):
-            raise InvalidInput("row index out of bounds")
-        if np.any(r < cols):
-            raise InvalidInput("row index in upper triangle; CscMatrix stores only the lower triangle")
-        same = cols[1:] == cols[:-1]
-        if np.any(r[1:][same] <= r[:-1][same]):
-            raise InvalidInput("row indices not sorted in column")
+        # monotone col_ptr, row bounds, lower triangle, sorted columns: one
+        # native pass (rslab_validate_lower_csc)
+        cp = np.ascontiguousarray(self.col_ptr, np.int64)
+        ri = np.ascontiguousarray(self.row_idx, np.int64)
+        _check(N.lib.rslab_validate_lower_csc(n, _p64(cp), _p64(ri), int(ri.shape[0])))
 
     def astype(self, dtype) -> "CscMatrix":
         return CscMatrix(self.n, self.col_ptr, self.row_idx, self.values.astype(dtype))
@@ -562,14 +556,22 @@ class MixedLdltSolver:
     def solve(self, a: CscMatrix, b) -> tuple:
         return self.solve_to(a, b, CERT_FACTOR * EPS_F64)
 
-    def solve_to(self, a: CscMatrix, b, target_backward_error: float) -> tuple:
+    def solve_to(self, a: CscMatrix, b, target_backward_error: float, out: Optional[np.ndarray] = None) -> tuple:
+        """`out` (optional, not in the reference API): a C-contiguous array of
+        b's shape and dtype that receives the solution, e.g. page-locked
+        host memory so the device-to-host copy runs at full speed."""
         if a.n != self._sym.n:
             raise DimensionMismatch(self._sym.n, a.n)
         b = np.ascontiguousarray(b, dtype=self.dtype)
         nrhs = 1 if b.ndim == 1 else b.shape[1]
         if b.shape[0] != self._sym.n:
             raise DimensionMismatch(self._sym.n, b.shape[0])
-        x = np.empty_like(b)
+        if out is not None:
+            if out.shape != b.shape or out.dtype != b.dtype or not out.flags["C_CONTIGUOUS"]:
+                raise InvalidInput("out must be C-contiguous with the shape and dtype of b")
+            x = out
+        else:
+            x = np.empty_like(b)
         info = N.MixedInfoC()
         _check(N.lib.rslab_mixed_solve(self._h, b.ctypes.data_as(C.c_void_p), nrhs, float(target_backward_error),
                                        x.ctypes.data_as(C.c_void_p), 0, C.byref(info)))
