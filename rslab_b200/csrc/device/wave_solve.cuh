@@ -20,7 +20,8 @@
 //
 // Chain (k_chain): every supernode is cut into TB = 64 column blocks whose
 // solves form a chain (forward: block i needs z of blocks j < i; backward:
-// x of blocks j > i).  One CTA per block:
+// x of blocks j > i).  One CTA per block and group of at most CH_NR
+// right-hand-side columns (the columns' chains are independent):
 //   forward : z_i = Linv_i (y_i - sum_{j<i} L_ij z_j)
 //   backward: x_i = Linv_i^T (w_i - W_i - sum_{j>i, descending} L_ji^T x_j)
 // with Linv_i the precomputed inverse of the unit-lower diagonal block and
@@ -48,6 +49,10 @@ constexpr long WV_POLL_LIMIT = 1L << 21;  // flag polls before a wait gives up
 constexpr int ST_UNIT = 2112;             // streamed tile elements (max of 32 x 65 and 64 x 33)
 constexpr int CH_UNIT = 64 * 65;          // chain tile elements
 constexpr int BWD_CH = 1024;              // off-diagonal rows per backward-dot item
+// The right-hand sides of a pass are solved as CH_GROUPS independent chains
+// of at most CH_NR columns (more CTAs, shorter per-block products).
+constexpr int CH_NR = 4;
+constexpr int CH_GROUPS = RHS_MAX / CH_NR;
 
 template <typename T>
 __host__ __device__ constexpr int st_stages() {
@@ -363,7 +368,7 @@ __global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __rest
   using F = Field<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int sh_t, sh_abort;
-  const int nr = a.nrhs, ld = a.ld;
+  const int ld = a.ld;
   T* S = reinterpret_cast<T*>(smem_raw);  // dependency tile; later the slice partials (4 x NR x 65)
   T* red = S;
   T* Lv = S + CH_UNIT;                    // the inverse block
@@ -378,12 +383,19 @@ __global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __rest
   if (ld_volatile(a.wstate + WV_STATE_ABORT) != 0) return;
   const int4 tk = tasks[sh_t];
   const int s = tk.x, i = tk.z, fb = tk.w;
-  int* flags = a.wstate + flag_base + fb;
+  // column group: columns [cg0, cg0 + nr) of the pass; a group with no
+  // columns in this pass has nothing to do (its dependents are in the same
+  // group)
+  const int cg0 = CH_NR * (tk.y >> 1);
+  const int nr = min(CH_NR, a.nrhs - cg0);
+  if (nr <= 0) return;
+  // flags of group g: flag index (fb + block) * CH_GROUPS + g
+  int* flags = a.wstate + flag_base + (long long)fb * CH_GROUPS + (tk.y >> 1);
   const int first = a.sn_first[s], ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
   const int nblk = (ncol + TB - 1) / TB, nb = min(TB, ncol - i * TB);
   const T* L = reinterpret_cast<const T*>(a.panel) + a.sn_poff[s];
   const T* Li = reinterpret_cast<const T*>(a.linv) + a.linv_off[s] + (long long)i * TB * TB;
-  T* Ze = reinterpret_cast<T*>(a.Ze) + a.c0 + (long long)first * ld;
+  T* Ze = reinterpret_cast<T*>(a.Ze) + a.c0 + cg0 + (long long)first * ld;
   // dependency blocks in chain order: step u is block dep(u)
   const int nd = FWD ? i : nblk - 1 - i;
   auto dep = [&](int u) { return FWD ? u : nblk - 1 - u; };
@@ -396,7 +408,7 @@ __global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __rest
   if (nd > 0) issue(0);
   cp_async_commit();
   // block vector: y_i (forward) or w_i - W_i (backward; W_i = off-diagonal dots)
-  const T* Wb = (!FWD && nrow > ncol) ? reinterpret_cast<const T*>(a.Wb) + a.c0 + (long long)first * ld : nullptr;
+  const T* Wb = (!FWD && nrow > ncol) ? reinterpret_cast<const T*>(a.Wb) + a.c0 + cg0 + (long long)first * ld : nullptr;
   for (int e = tid; e < 64 * NR; e += WV_NT) {
     const int r = e / NR, c = e % NR;
     T v = F::zero();
@@ -412,7 +424,7 @@ __global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __rest
 #pragma unroll 1
   for (int u = 0; u < nd; ++u) {
     const int j = dep(u);
-    if (tid == 0 && !wv_wait(flags, j, a.wstate)) sh_abort = 1;
+    if (tid == 0 && !wv_wait(flags, j * CH_GROUPS, a.wstate)) sh_abort = 1;
     cp_async_wait<0>();
     __syncthreads();  // tile u landed; flag j observed
     if (sh_abort) return;
@@ -446,14 +458,14 @@ __global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __rest
     const T v = slice_sum<T, NR>(red, r, c);
     Ze[(long long)(i * TB + r) * ld + c] = v;
     if (!FWD) {
-      T* Xw = reinterpret_cast<T*>(a.Xg) + a.c0;
+      T* Xw = reinterpret_cast<T*>(a.Xg) + a.c0 + cg0;
       Xw[(long long)(first + a.lperm[first + i * TB + r]) * ld + c] = v;
     }
   }
   __syncthreads();
   // the release store orders the CTA's stores above (barrier, then a
   // cumulative gpu-scope release)
-  if (tid == 0) st_release_gpu(flags + i, 1);
+  if (tid == 0) st_release_gpu(flags + (long long)i * CH_GROUPS, 1);
 }
 
 }  // namespace rsd

@@ -609,7 +609,8 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         Launch W{L_FWD_CHAIN, (long long)H.st4.size(), 0, H.nwave++};
         for (int b = 0; b < maxb; ++b)
           for (int64_t s : lvl)
-            if (b * TB < S.sn[s].ncol) H.st4.push_back(make_int4((int)s, 0, b, H.flag_off[s]));
+            if (b * TB < S.sn[s].ncol)
+              for (int g = 0; g < CH_GROUPS; ++g) H.st4.push_back(make_int4((int)s, 2 * g, b, H.flag_off[s]));
         W.ntasks = (int)(H.st4.size() - W.task_off);
         H.fwdplan.push_back(W);
       }
@@ -659,7 +660,9 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         for (int dd = 0; dd < maxb; ++dd)
           for (int64_t s : lvl) {
             const int nblk = (int)((S.sn[s].ncol + TB - 1) / TB);
-            if (dd < nblk) H.st4.push_back(make_int4((int)s, 1, nblk - 1 - dd, H.flag_off[s]));
+            if (dd < nblk)
+              for (int g = 0; g < CH_GROUPS; ++g)
+                H.st4.push_back(make_int4((int)s, 1 + 2 * g, nblk - 1 - dd, H.flag_off[s]));
           }
         W.ntasks = (int)(H.st4.size() - W.task_off);
         bw.push_back(W);
@@ -719,6 +722,13 @@ void launch_solve_nr(int kind, int grid, int nr, const SolveArgs& sa, const int4
 template <typename T, bool FWD>
 void launch_solve(int kind, int grid, int nr, const SolveArgs& sa, const int4* tasks, int ctr = 0, int flags = 0,
                   cudaStream_t st = nullptr) {
+  if (kind == 1) {  // chain items carry at most CH_NR columns each
+    if (nr <= 1)
+      launch_solve_nr<T, FWD, 1>(kind, grid, nr, sa, tasks, ctr, flags, st);
+    else
+      launch_solve_nr<T, FWD, CH_NR>(kind, grid, nr, sa, tasks, ctr, flags, st);
+    return;
+  }
   if (nr <= 1)
     launch_solve_nr<T, FWD, 1>(kind, grid, nr, sa, tasks, ctr, flags, st);
   else if (nr <= 4)
@@ -1114,7 +1124,9 @@ void run_factor(rslab_fac_handle& F) {
 
 // Wave state: sticky status, abort word, one ticket counter per wavefront
 // launch, forward and backward block flags.
-size_t wave_state_ints(const rslab_sym_handle& H) { return (size_t)WV_STATE_CTR + H.nwave + 2 * (size_t)H.nflags; }
+size_t wave_state_ints(const rslab_sym_handle& H) {
+  return (size_t)WV_STATE_CTR + H.nwave + 2 * (size_t)CH_GROUPS * H.nflags;
+}
 
 // After a synchronised solve: a timed-out wavefront wait (sticky status set
 // by the kernels) is reported and the status cleared.
@@ -1210,7 +1222,7 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
     const int nr = std::min(RHS_MAX, nrhs - c0);
     SolveArgs sa = make_sargs<T>(F, nrhs, c0, nr);
     CK(cudaMemsetAsync(F.wstate + 1, 0, (wave_state_ints(H) - 1) * sizeof(int), st));
-    const int fwd_flags = WV_STATE_CTR + H.nwave, bwd_flags = fwd_flags + H.nflags;
+    const int fwd_flags = WV_STATE_CTR + H.nwave, bwd_flags = fwd_flags + CH_GROUPS * H.nflags;
     for (const Launch& L : H.fwdplan) {
       switch (L.kind) {
         case L_FWD_GATHER:
