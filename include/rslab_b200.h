@@ -204,7 +204,8 @@ int rslab_solve_profile(rslab_fac_handle* fac, int64_t nrhs, double* kind_ms, in
  * forward gather, 13 tensor-core cmod, 14 G = L21 D, 15 diagonal-block
  * inverses, 16 backward partial-sum reduction, 17 tensor-core panel Schur,
  * 18/19 forward/backward block-chain solve, 20 backward gather, 21 deep rows
- * as a product with the block transform, 22 block transform, -1 other), grid
+ * as a product with the block transform, 22 block transform, 23 forward push
+ * partial-sum reduction, -1 other), grid
  * size and device ms.  *count = rows available; at most cap are written.
  * A measurement aid with no reference counterpart. */
 int rslab_profile_trace(const rslab_fac_handle* fac, int64_t cap, int32_t* kind, int32_t* grid, float* ms,

@@ -6,7 +6,7 @@
 // off-diagonal dots L21_s^T x_anc.  An item owns 64 outputs and loops over
 // 32-wide reduction units; each unit's 2048-element panel tile and its 32
 // right-hand-side rows are copied global -> shared with cp.async (zero
-// filled outside the panel), `st_stages<T>()` units in flight, one CTA
+// filled outside the panel), `st_stages<T>(NR)` units in flight, one CTA
 // barrier per unit.  Tile layouts keep every lane on consecutive or odd
 // strided shared memory:
 //   forward  : 64 output rows x 32 reduction columns, S[q * 65 + r]
@@ -48,15 +48,18 @@ constexpr int WV_NT = 256;
 constexpr long WV_POLL_LIMIT = 1L << 21;  // flag polls before a wait gives up
 constexpr int ST_UNIT = 2112;             // streamed tile elements (max of 32 x 65 and 64 x 33)
 constexpr int CH_UNIT = 64 * 65;          // chain tile elements
-constexpr int BWD_CH = 1024;              // off-diagonal rows per backward-dot item
+constexpr int BWD_CH = 512;               // off-diagonal rows per backward-dot item
+constexpr int PUSH_KS = 16;               // column units (of 32) per forward-push item of a wide supernode
 // The right-hand sides of a pass are solved as CH_GROUPS independent chains
 // of at most CH_NR columns (more CTAs, shorter per-block products).
 constexpr int CH_NR = 4;
 constexpr int CH_GROUPS = RHS_MAX / CH_NR;
 
+// Stages in flight: 4, or 3 where the wide elements of 16 right-hand sides
+// would otherwise keep a second CTA off the SM.
 template <typename T>
-__host__ __device__ constexpr int st_stages() {
-  return sizeof(T) >= 16 ? 3 : 4;
+__host__ __device__ constexpr int st_stages(int nr) {
+  return (sizeof(T) >= 16 || (sizeof(T) >= 8 && nr >= 16)) ? 3 : 4;
 }
 
 // Right-hand-side buffers are sized by the pass's column count nr (<=
@@ -71,7 +74,7 @@ __host__ __device__ constexpr size_t st_stage_elems(int nr) {
 }
 template <typename T>
 __host__ __device__ constexpr size_t st_smem_bytes(int nr) {
-  return ((size_t)st_stages<T>() * st_stage_elems<T>(nr) + 4 * 65 * nr) * sizeof(T) + 16;
+  return ((size_t)st_stages<T>(nr) * st_stage_elems<T>(nr) + 4 * 65 * nr) * sizeof(T) + 16;
 }
 // Chain: one tile slot (its copy overlaps the wait for the dependency's
 // flag; after the chain it holds the slice partials), the inverse block,
@@ -143,7 +146,8 @@ struct StItem {
   int c0, clim;       // tile columns
   const T* V;         // right-hand-side row 0 of the item (row stride a.ld)
   int vlim;           // right-hand-side rows valid < vlim (relative)
-  int cu;             // forward: column units per 64-row block
+  int cu;             // forward: column units per 64-row block (of this item's column chunk)
+  int cb0;            // forward: first column unit of the item
   int nunits;
 };
 
@@ -159,8 +163,12 @@ __device__ __forceinline__ StItem<T, FWD> st_item(const SolveArgs& a, int4 tk) {
     it.c0 = 0; it.clim = ncol;
     it.V = reinterpret_cast<const T*>(a.Ze) + a.c0 + (long long)first * a.ld;
     it.vlim = ncol;
-    it.cu = (ncol + 31) / 32;
-    const int nrb = min(tk.z, (nrow - it.r0 + 63) / 64);
+    // z = nrb | first column unit << 8; wide supernodes' items take
+    // PUSH_KS column units each (partial sums to slot w)
+    it.cb0 = tk.z >> 8;
+    it.cu = min(PUSH_KS, (ncol + 31) / 32 - it.cb0);
+    if (tk.w < 0) it.cu = (ncol + 31) / 32;
+    const int nrb = min(tk.z & 255, (nrow - it.r0 + 63) / 64);
     it.nunits = nrb * it.cu;
   } else {
     it.r0 = ncol + tk.z; it.rlim = min(nrow, it.r0 + BWD_CH);
@@ -168,6 +176,7 @@ __device__ __forceinline__ StItem<T, FWD> st_item(const SolveArgs& a, int4 tk) {
     it.V = reinterpret_cast<const T*>(a.U) + a.c0 + (a.uoff[s] + tk.z) * a.ld;
     it.vlim = it.rlim - it.r0;
     it.cu = 1;
+    it.cb0 = 0;
     it.nunits = (it.vlim + 31) / 32;
   }
   return it;
@@ -177,7 +186,7 @@ template <typename T, bool FWD, int NR>
 __device__ __forceinline__ void st_issue(T* S, T* Vs, const StItem<T, FWD>& it, int u, int ld, int nr) {
   int rr0, cc0, vr0;
   if constexpr (FWD) {
-    const int rb = u / it.cu, cb = u - rb * it.cu;
+    const int rb = u / it.cu, cb = it.cb0 + u - rb * it.cu;
     rr0 = it.r0 + 64 * rb; cc0 = 32 * cb; vr0 = 32 * cb;
   } else {
     rr0 = it.r0 + 32 * u; cc0 = it.c0; vr0 = 32 * u;
@@ -206,7 +215,7 @@ __device__ __forceinline__ void st_issue(T* S, T* Vs, const StItem<T, FWD>& it, 
 template <typename T, bool FWD, int NR>
 __global__ void __launch_bounds__(WV_NT) k_stream(SolveArgs a, const int4* __restrict__ tasks) {
   using F = Field<T>;
-  constexpr int NST = st_stages<T>();
+  constexpr int NST = st_stages<T>(NR);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nr = a.nrhs, ld = a.ld;
   constexpr int SE = (int)st_stage_elems<T>(NR);
@@ -231,8 +240,13 @@ __global__ void __launch_bounds__(WV_NT) k_stream(SolveArgs a, const int4* __res
       if (FWD) {
         const int row = it.r0 + 64 * rb + r;
         if (row < it.rlim) {
-          T* Us = reinterpret_cast<T*>(a.U) + a.c0 + a.uoff[s] * ld;
-          Us[(long long)(row - a.sn_ncol[s]) * ld + c] = v;
+          if (tk.w < 0) {
+            T* Us = reinterpret_cast<T*>(a.U) + a.c0 + a.uoff[s] * ld;
+            Us[(long long)(row - a.sn_ncol[s]) * ld + c] = v;
+          } else {
+            T* part = reinterpret_cast<T*>(a.Wp) + (long long)tk.w * 64 * ld;
+            part[(long long)r * ld + c] = v;
+          }
         }
       } else if (it.c0 + r < it.clim) {
         if (tk.w < 0) {
@@ -295,6 +309,26 @@ __global__ void __launch_bounds__(WV_NT) k_dots_reduce(SolveArgs a, const int4* 
     T v = part[(long long)p * ld + c];
     for (int k = 1; k < nch; ++k) v = F::add(v, part[((long long)k * 64 + p) * ld + c]);
     Wb[(long long)(i * TB + p) * ld + c] = v;
+  }
+}
+
+// Forward: sum the column-chunk partials of (s, 64-row block r0) in chunk
+// order into U.  Task (s, r0, slot0, nchunks).
+template <typename T>
+__global__ void __launch_bounds__(WV_NT) k_push_reduce(SolveArgs a, const int4* __restrict__ tasks) {
+  using F = Field<T>;
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, r0 = tk.y, slot0 = tk.z, nch = tk.w;
+  const int off = a.sn_nrow[s] - a.sn_ncol[s];
+  const int ld = a.ld, nr = a.nrhs;
+  const T* part = reinterpret_cast<const T*>(a.Wp) + (long long)slot0 * 64 * ld;
+  T* Us = reinterpret_cast<T*>(a.U) + a.c0 + a.uoff[s] * ld;
+  for (int e = threadIdx.x; e < 64 * nr; e += WV_NT) {
+    const int r = e / nr, c = e - r * nr;
+    if (r0 + r >= off) continue;
+    T v = part[(long long)r * ld + c];
+    for (int k = 1; k < nch; ++k) v = F::add(v, part[((long long)k * 64 + r) * ld + c]);
+    Us[(long long)(r0 + r) * ld + c] = v;
   }
 }
 

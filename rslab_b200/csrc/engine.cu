@@ -101,6 +101,7 @@ enum LaunchKind {
   L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD,
   L_UNUSED8, L_UNUSED9, L_UNUSED10, L_UNUSED11, L_FWD_GATHER, L_CMOD_TC, L_MAKE_G, L_DIAG_INV,
   L_BWD_OFF_RED, L_SCHUR_TC, L_FWD_CHAIN, L_BWD_CHAIN, L_BWD_GATHER, L_DEEP_MM, L_MAKE_M,
+  L_FWD_PUSH_RED,
   L_JOIN_CM  // no kernel: the level's early cmod updates must be complete from here on
 };
 // Inverse diagonal blocks of a supernode with ncol columns: TB x TB per
@@ -152,7 +153,7 @@ struct rslab_sym_handle {
   std::vector<int8_t> tcmaps;         // per tensor-core pair: 128 + 64 inverse scatter maps
   std::vector<long long> goff;        // G_k = L21_k D_k pool offsets ((nrow - ncol) x ncol each)
   long long g_elems = 0;
-  int bwd_slots = 0;                  // partial-sum slots of the split backward dots (max per level)
+  int bwd_slots = 0;                  // partial-sum slots of the split push / backward dots (max per level)
   std::vector<long long> linv_off;    // wide supernodes: inverses of their TB x TB diagonal blocks
   long long linv_elems = 0;
   // chain solves: per wide supernode the index of its block-0 flag (-1 for
@@ -616,13 +617,31 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       }
       // push items: 64-row blocks, several per item for narrow supernodes
       // (about 8 column units per item)
+      // (wide supernodes: PUSH_KS column units per item, partial sums
+      // reduced in chunk order by the next launch)
       Launch Pu{L_FWD_PUSH, (long long)H.st4.size(), 0, 0};
+      std::vector<int4> pred;
+      int pslot = 0;
       for (int64_t s : lvl) {
-        const int cu = (int)((S.sn[s].ncol + 31) / 32), nrb = std::max(1, 8 / cu);
-        for (int r0 = 0; r0 < H.nrow[s] - S.sn[s].ncol; r0 += 64 * nrb) H.st4.push_back(make_int4((int)s, r0, nrb, 0));
+        const int cu = (int)((S.sn[s].ncol + 31) / 32), off = H.nrow[s] - (int)S.sn[s].ncol;
+        if (cu <= PUSH_KS) {
+          const int nrb = std::max(1, 8 / cu);
+          for (int r0 = 0; r0 < off; r0 += 64 * nrb) H.st4.push_back(make_int4((int)s, r0, nrb, -1));
+        } else {
+          const int nch = (cu + PUSH_KS - 1) / PUSH_KS;
+          for (int r0 = 0; r0 < off; r0 += 64) {
+            pred.push_back(make_int4((int)s, r0, pslot, nch));
+            for (int q = 0; q < nch; ++q) H.st4.push_back(make_int4((int)s, r0, 1 | ((q * PUSH_KS) << 8), pslot + q));
+            pslot += nch;
+          }
+        }
       }
       Pu.ntasks = (int)(H.st4.size() - Pu.task_off);
       if (Pu.ntasks) H.fwdplan.push_back(Pu);
+      H.bwd_slots = std::max(H.bwd_slots, pslot);
+      Launch Pr{L_FWD_PUSH_RED, (long long)H.st4.size(), (int)pred.size(), 0};
+      H.st4.insert(H.st4.end(), pred.begin(), pred.end());
+      if (Pr.ntasks) H.fwdplan.push_back(Pr);
 
       std::vector<Launch> bw;
       Launch Bg{L_BWD_GATHER, (long long)H.t2.size(), 0, 0};
@@ -1231,10 +1250,13 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
         case L_FWD_CHAIN:
           launch_solve<T, true>(1, L.ntasks, nr, sa, H.d_st4 + L.task_off, L.nb_slot, fwd_flags, st);
           break;
+        case L_FWD_PUSH_RED:
+          k_push_reduce<T><<<L.ntasks, WV_NT, 0, st>>>(sa, H.d_st4 + L.task_off);
+          break;
         default:
           launch_solve<T, true>(0, L.ntasks, nr, sa, H.d_st4 + L.task_off, 0, 0, st);
       }
-      if (prof) prof->mark(st, L.kind == L_FWD_PUSH ? 2 : 1, L.ntasks, L.kind);
+      if (prof) prof->mark(st, (L.kind == L_FWD_PUSH || L.kind == L_FWD_PUSH_RED) ? 2 : 1, L.ntasks, L.kind);
     }
     k_dsolve<T><<<grid1((long long)n * nr), 256, 0, st>>>(n, sa);
     if (prof) prof->mark(st, 3);

@@ -618,7 +618,8 @@ def solve_profile(handle, nrhs: int) -> dict:
 
 LAUNCH_KINDS = ("cmod", "getf2", "deep_replay", "panel_schur", "fwd_diag", "fwd_push", "bwd_off", "bwd_diag",
                 "unused8", "unused9", "unused10", "unused11", "fwd_gather", "cmod_tc", "make_g", "diag_inv",
-                "bwd_off_reduce", "schur_tc", "fwd_chain", "bwd_chain", "bwd_gather", "deep_mm", "make_m")
+                "bwd_off_reduce", "schur_tc", "fwd_chain", "bwd_chain", "bwd_gather", "deep_mm", "make_m", "push_reduce",
+                "join")
 
 
 def profile_trace(handle) -> list:
