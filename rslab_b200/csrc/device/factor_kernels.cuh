@@ -563,18 +563,20 @@ constexpr int REPLAY_SL = 16;
 // slice's snapshot rows (all columns < pw, stride nb) into S, then every warp
 // replays those steps.  S holds (REPLAY_SL + 1) x nb elements; every thread
 // of the CTA calls this (it synchronises the block).
-template <typename T, int NT, int NS, int NR>
+template <typename T, int NT, int NS, int NR, int SL = REPLAY_SL>
 __device__ void replay_rows_sliced(T (&x)[NR][NS], int pw, int nb, const T* __restrict__ snap, int kb,
                                    const ReplayProg<T>& P, T* S) {
   for (int k0 = 0; k0 < pw;) {
-    int k1 = min(k0 + REPLAY_SL, pw);
+    int k1 = min(k0 + SL, pw);
     if (k1 < pw && P.kd[k1 - 1] == 1) ++k1;
     __syncthreads();
     const int cnt = (k1 - k0) * pw;
     for (int e = threadIdx.x; e < cnt; e += NT) {
       const int r = e / pw, c = e - r * pw;
-      S[r * nb + c] = snap[(long long)(k0 + r) * nb + c];
+      cp_async_zfill<sizeof(T)>(S + r * nb + c, snap + (long long)(k0 + r) * nb + c, true);
     }
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
     replay_rows_warp<T, NS, NR>(x, pw, S, nb, k0, k1, kb, P);
     k0 = k1;
@@ -592,10 +594,10 @@ __device__ void replay_rows_sliced(T (&x)[NR][NS], int pw, int nb, const T* __re
 // [r_begin, r_end) of it), and the results go to M (row-major, stride nb):
 // the replay is linear in the row, so M is the block's transform and every
 // deep row x becomes x M.
-// R rows per pass (a multiple of the warp count).  The snapshot slices use
-// S (default: X, free while the rows sit in registers; it must hold
-// (REPLAY_SL + 1) x nb elements).
-template <typename T, int NT, bool IDENT = false, int R = 32>
+// R rows per pass (a multiple of the warp count).  The snapshot slices of SL
+// steps use S (default: X, free while the rows sit in registers; it must
+// hold (SL + 1) x nb elements, or pw x nb when SL >= pw).
+template <typename T, int NT, bool IDENT = false, int R = 32, int SL = REPLAY_SL>
 __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int nb, int r_begin, int r_end,
                                  const T* __restrict__ snap, const ReplayProg<T>& P, T* X, T* M = nullptr,
                                  T* S = nullptr) {
@@ -628,7 +630,7 @@ __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int n
           const int col = lane + 32 * j, r = warp + NW * i;
           x[i][j] = (col < pw && r < rows) ? X[col * LDX + r] : Field<T>::zero();
         }
-      replay_rows_sliced<T, NT, 2, NR>(x, pw, nb, snap, kb, P, S);
+      replay_rows_sliced<T, NT, 2, NR, SL>(x, pw, nb, snap, kb, P, S);
 #pragma unroll
       for (int i = 0; i < NR; ++i)
 #pragma unroll
@@ -645,7 +647,7 @@ __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int n
           const int col = lane + 32 * j, r = warp + NW * i;
           x[i][j] = (col < pw && r < rows) ? X[col * LDX + r] : Field<T>::zero();
         }
-      replay_rows_sliced<T, NT, 4, NR>(x, pw, nb, snap, kb, P, S);
+      replay_rows_sliced<T, NT, 4, NR, SL>(x, pw, nb, snap, kb, P, S);
 #pragma unroll
       for (int i = 0; i < NR; ++i)
 #pragma unroll
@@ -1094,7 +1096,7 @@ __host__ __device__ constexpr size_t smem_make_m_off_slice(size_t es, int nb) {
   return ((smem_make_m_off_prog(es, nb) + (size_t)nb * (3 * es + 4 + 1) + 16) + 15) & ~size_t(15);
 }
 __host__ __device__ constexpr size_t smem_make_m_bytes(size_t es, int nb) {
-  return smem_make_m_off_slice(es, nb) + (size_t)(REPLAY_SL + 1) * nb * es + 64;
+  return smem_make_m_off_slice(es, nb) + (size_t)nb * nb * es + 64;
 }
 
 template <typename T, int NT>
@@ -1120,17 +1122,18 @@ __global__ void __launch_bounds__(NT) k_make_m(FactorArgs fa, const int4* __rest
                               reinterpret_cast<const T*>(fa.dsub) + first + kb, fa.kind + first + kb);
   T* S = reinterpret_cast<T*>(smem_raw + smem_make_m_off_slice(sizeof(T), nb));
   __syncthreads();
-  replay_deep_rows<T, NT, true, MM_RB>(panel, nrow, kb, pw, nb, i0, min(i0 + MM_RB, pw), snap, P, X, M, S);
+  // the whole snapshot in one slice: no staging round trips inside the steps
+  replay_deep_rows<T, NT, true, MM_RB, 128>(panel, nrow, kb, pw, nb, i0, min(i0 + MM_RB, pw), snap, P, X, M, S);
 }
 
 // ---------------------------------------------------------------------------
-// Deep rows of a tall panel as one product: rows [r0, r0 + 64) of the panel
-// columns [kb, ke) become A21 M, M the block transform formed by getf2 (the
-// replay of the identity rows; the replay is linear in the row).  The 64-row
+// Deep rows of a tall panel as one product: rows [r0, r0 + MM_ROWS) of the
+// panel columns [kb, ke) become A21 M, M the block transform (k_make_m: the
+// replay of the identity rows; the replay is linear in the row).  The row
 // block is staged in shared memory first (the product overwrites it in
-// place), M streams through in MM_CW-column chunks; thread (r = tid & 63,
-// g = tid >> 6) owns row r and MM_CW / 4 columns of each chunk, summing over
-// k in ascending order.  Task (s, kb, slot, r0).  Used with the tensor-core
+// place), M streams through in mm_cw-column chunks; thread (r = tid %
+// MM_ROWS, g = tid / MM_ROWS) owns row r and a contiguous group of columns of
+// each chunk, summing over k in ascending order.  Task (s, kb, slot, r0).  Used with the tensor-core
 // engine of the single-precision fields (the FMA engine replays row by row,
 // in the oracle's operation order).
 // ---------------------------------------------------------------------------
@@ -1138,20 +1141,21 @@ template <typename T>
 __host__ __device__ constexpr int mm_cw() {
   return sizeof(T) >= 16 ? 16 : 32;
 }
+constexpr int MM_ROWS = 32;  // deep rows per product task
 template <typename T>
 __host__ __device__ constexpr size_t smem_deep_mm_bytes() {
-  return ((size_t)128 * 65 + 2 * 128 * mm_cw<T>()) * sizeof(T) + 16;
+  return ((size_t)128 * (MM_ROWS + 1) + 2 * 128 * mm_cw<T>()) * sizeof(T) + 16;
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_deep_mm(FactorArgs fa, const int4* __restrict__ tasks, int nb_small,
                                                  int nb_big) {
   using F = Field<T>;
-  constexpr int CW = mm_cw<T>(), NO = CW / 4;
+  constexpr int CW = mm_cw<T>(), NG = 256 / MM_ROWS, NO = CW / NG, LDA = MM_ROWS + 1;
   if (fa.status[0] != 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* As = reinterpret_cast<T*>(smem_raw);  // As[k * 65 + r]
-  T* Ms = As + 128 * 65;                   // 2 x (128 x CW), row-major chunks
+  T* As = reinterpret_cast<T*>(smem_raw);  // As[k * LDA + r]
+  T* Ms = As + 128 * LDA;                  // 2 x (128 x CW), row-major chunks
   const int4 tk = tasks[blockIdx.x];
   const int s = tk.x, kb = tk.y, slot = tk.z, r0 = tk.w;
   const int ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
@@ -1160,8 +1164,8 @@ __global__ void __launch_bounds__(256) k_deep_mm(FactorArgs fa, const int4* __re
   T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
   const unsigned char* sc = reinterpret_cast<const unsigned char*>(fa.scratch) + (long long)slot * fa.scratch_stride;
   const T* M = reinterpret_cast<const T*>(sc + replay_mm_off(nb, sizeof(T)));
-  const int tid = threadIdx.x, r = tid & 63, g = tid >> 6;
-  const int rows = min(64, nrow - r0);
+  const int tid = threadIdx.x, r = tid % MM_ROWS, g = tid / MM_ROWS;
+  const int rows = min(MM_ROWS, nrow - r0);
   auto load_chunk = [&](int j0, T* dst) {
     for (int e = tid; e < 128 * CW; e += 256) {
       const int k = e / CW, j = e % CW;
@@ -1170,11 +1174,11 @@ __global__ void __launch_bounds__(256) k_deep_mm(FactorArgs fa, const int4* __re
       cp_async_zfill<sizeof(T)>(dst + e, src, ok);
     }
   };
-  for (int e = tid; e < 64 * 128; e += 256) {
-    const int rr = e & 63, k = e >> 6;
+  for (int e = tid; e < MM_ROWS * 128; e += 256) {
+    const int rr = e % MM_ROWS, k = e / MM_ROWS;
     const bool ok = rr < rows && k < pw;
     const T* src = ok ? panel + (r0 + rr) + (long long)(kb + k) * nrow : panel;
-    cp_async_zfill<sizeof(T)>(As + k * 65 + rr, src, ok);
+    cp_async_zfill<sizeof(T)>(As + k * LDA + rr, src, ok);
   }
   load_chunk(0, Ms);
   cp_async_commit();
@@ -1190,7 +1194,7 @@ __global__ void __launch_bounds__(256) k_deep_mm(FactorArgs fa, const int4* __re
     for (int j = 0; j < NO; ++j) acc[j] = F::zero();
 #pragma unroll 4
     for (int k = 0; k < pw; ++k) {
-      const T a = As[k * 65 + r];
+      const T a = As[k * LDA + r];
       T m[NO];
       lds_row<T, NO>(Mc + k * CW, m);
 #pragma unroll
