@@ -517,7 +517,7 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         launch_nb = std::max(launch_nb, nb);
         if (!fuse) {
           for (int r0 = ke; r0 < nr; r0 += DEEP_R) deep.push_back(make_int4((int)s, kb, slot, r0));
-          for (int r0 = ke; r0 < nr; r0 += 64) deep_mm.push_back(make_int4((int)s, kb, slot, r0));
+          for (int r0 = ke; r0 < nr; r0 += MM_ROWS) deep_mm.push_back(make_int4((int)s, kb, slot, r0));
           for (int i0 = 0; i0 < ke - kb; i0 += MM_RB) make_m.push_back(make_int4((int)s, kb, slot, i0));
         }
         int mt = nr - ke, cw = nc - ke;
@@ -772,8 +772,11 @@ struct KernelSetup {
                             (int)smem_getf2(es, 128)));
     CK(cudaFuncSetAttribute(k_deep<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep(es, 128)));
     CK(cudaFuncSetAttribute(k_diag_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_diag_inv(es)));
-    if constexpr (TensorCmod<T>::ok)
+    if constexpr (TensorCmod<T>::ok) {
       CK(cudaFuncSetAttribute(k_deep_mm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep_mm_bytes<T>()));
+      CK(cudaFuncSetAttribute(k_make_m<T, 32 * MM_RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_make_m_bytes(es, 128)));
+    }
     solve_nr_attrs<T, 1>();
     solve_nr_attrs<T, 4>();
     solve_nr_attrs<T, RHS_MAX>();
