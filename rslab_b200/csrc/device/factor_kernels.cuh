@@ -372,6 +372,21 @@ __device__ __forceinline__ void argmax_combine(double& v, int& i, double v2, int
   }
 }
 
+// Warp-wide argmax_combine of every lane's (v, i), v >= 0 or -1 (none): the
+// same result (largest v, then smallest i) from three warp reductions on an
+// order-preserving key (bits of v + 1; 0 for none), instead of a shuffle tree.
+__device__ __forceinline__ void warp_argmax(double& v, int& i) {
+  const unsigned long long key = v >= 0.0 ? (unsigned long long)__double_as_longlong(v) + 1ull : 0ull;
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  const bool win = hi == mhi && lo == mlo;
+  const int mi = (int)__reduce_min_sync(0xffffffffu, win ? (unsigned)i : 0xffffffffu);
+  const unsigned long long mk = ((unsigned long long)mhi << 32) | mlo;
+  v = mk == 0ull ? -1.0 : __longlong_as_double((long long)(mk - 1ull));
+  i = mk == 0ull ? INT_MAX : mi;
+}
+
 template <int NT>
 __device__ void block_argmax(double& v, int& idx, double* red_v, int* red_i) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -762,6 +777,8 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
   auto decide = [&](int k, int par, bool full) -> bool {
     T *L1, *L2, *U1, *U2;
     bufs(par, L1, L2, U1, U2);
+    // |a_kk| first: independent of the column scan, its latency overlaps it
+    const double absakk = F::mag(A[pk(k, k, pw)]);
     double v = -1.0;
     int idx = INT_MAX;
     // blocks are at most 128 wide: four predicated lanes-strided slots
@@ -770,13 +787,7 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
       const int i = k + 1 + lane + 32 * t;
       if (i < pw) argmax_combine(v, idx, F::mag2(A[pk(i, k, pw)]), i);
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
-      const int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
-      argmax_combine(v, idx, v2, i2);
-    }
-    const double absakk = F::mag(A[pk(k, k, pw)]);
+    warp_argmax(v, idx);
     const double colmax = sqrt(v > 0.0 ? v : 0.0);
     const int imax = v > 0.0 ? idx : k;
     int kstep = 1, kp = k;
