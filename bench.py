@@ -50,6 +50,13 @@ def parse():
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--cpu-sample-side", type=int, default=36)
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--workload", default="helmholtz", choices=["helmholtz", "sweep"],
+                   help="helmholtz: the 64^3 Helmholtz factor+solve step (default); sweep: the "
+                        "same-pattern frequency sweep, 48^3 27-point K - w^2 M + i w C, 64 frequencies")
+    p.add_argument("--sweep-side", type=int, default=48)
+    p.add_argument("--sweep-count", type=int, default=64)
+    p.add_argument("--sweep-fp64-count", type=int, default=4,
+                   help="frequencies (evenly spread) timed on the plain FP64 path for the ratio")
     p.add_argument("--profile-step", action="store_true",
                    help="one warm-up mixed step, then exactly one mixed step between "
                         "cudaProfilerStart/Stop (for ncu --profile-from-start off); no JSON line")
@@ -215,11 +222,193 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def sweep_cpu_sample(side: int = 24, count: int = 4):
+    """The oracle on a bounded sample of the sweep: the same 27-point
+    K - w^2 M + i w C family on a side^3 grid, FP64 factor + 8-RHS solve at
+    `count` frequencies spread over the band."""
+    from oracle.oracle import OracleSolver, backward_error
+    from rslab_b200 import LdltSymbolic, matgen
+    from rslab_b200.sweep import sweep_settings
+    c4 = matgen.C4System(side, 3)
+    om = c4.omegas(64)[np.linspace(0, 63, count).round().astype(int)]
+    b = matgen.uniform_rhs(c4.n, 8, 4, complex_=True)
+    sym = LdltSymbolic.analyze_with(c4.matrix(om[0]), sweep_settings())
+    flops = 4.0 * sym.info().flops_model
+    ex = sym.export()
+    t = 0.0
+    be = 0.0
+    for w in om:
+        a = c4.matrix(w)
+        t0 = time.perf_counter()
+        x = OracleSolver(a, ex).solve_many(b, 8)
+        t += time.perf_counter() - t0
+        be = max(be, backward_error(a, x, b))
+    return {"value": flops * len(om) / t / 1e9, "unit": "GFLOP/s", "cores": os.cpu_count(), "kind": "port",
+            "seconds": t,
+            "sample": f"FP64 factor + 8-RHS solve of the {side}^3 27-point sweep matrix at {len(om)} frequencies "
+                      f"(n={c4.n}, model flops {flops:.3g} each); max backward error {be:.2e}"}
+
+
+def run_sweep(args, ws, rank, local):
+    """Same-pattern frequency sweep: A(w) = K - w^2 M + i w C on a 48^3
+    27-point grid (n = 110,592), 64 frequencies, 8 right-hand sides, each
+    solved to normwise backward error <= 1e-14.  Analysis and the factor
+    handle are made once outside the timed region; a step is the whole sweep
+    of this rank's frequencies (round-robin over ranks, no exchange): per
+    frequency a c32 refactor (captured factor graph replayed on the new
+    values) and the mixed solve refined in FP64.  The plain FP64 path is
+    timed on `--sweep-fp64-count` frequencies spread over the band."""
+    import ctypes as C
+
+    import torch
+
+    from rslab_b200 import CscMatrix, LdltSymbolic, MixedLdltSolver, matgen
+    from rslab_b200 import _native as N
+    from rslab_b200.sweep import sweep_settings
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    c4 = matgen.C4System(args.sweep_side, 3)
+    om_all = c4.omegas(args.sweep_count)
+    mine = list(range(rank, len(om_all), ws))
+    nrhs = 8
+    b = matgen.uniform_rhs(c4.n, nrhs, 4, complex_=True)
+    st = sweep_settings()
+    mats = [c4.matrix(om_all[i]) for i in mine]
+    sym = LdltSymbolic.analyze_with(mats[0], st)
+    info = sym.info()
+    flops = 4.0 * info.flops_model
+    vals_d = [torch.from_numpy(np.ascontiguousarray(a.values)).to(dev) for a in mats]
+    b_d = torch.from_numpy(np.ascontiguousarray(b)).to(dev)
+    x_d = torch.empty_like(b_d)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    mixed = MixedLdltSolver.factor_with(mats[0], st, sym=sym)
+    stream = torch.cuda.ExternalStream(mixed.stream())
+
+    def sweep_step():
+        infos = []
+        for v in vals_d:
+            rc = N.lib.rslab_refactor(mixed._h, C.c_void_p(v.data_ptr()), 1)
+            assert rc == 0, N.last_error()
+            inf = N.MixedInfoC()
+            rc = N.lib.rslab_mixed_solve(mixed._h, C.c_void_p(b_d.data_ptr()), nrhs, args.target,
+                                         C.c_void_p(x_d.data_ptr()), 1, C.byref(inf))
+            assert rc == 0, N.last_error()
+            infos.append((inf.certified, inf.backward_error, inf.ir_iters, inf.gmres_iters))
+        return infos
+
+    def timed(fn, strm, steps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        barrier(ws)
+        tot, last = 0.0, None
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(strm)
+            last = fn()
+            e1.record(strm)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        barrier(ws)
+        return tot / steps, last
+
+    clk = ClockSampler(local)
+    clk.start()
+    ms_sweep, infos = timed(sweep_step, stream, args.steps, args.warmup)
+    clocks = clk.stop()
+    ms_sweep = allmax(ms_sweep, ws)
+
+    # Plain FP64 factor + solve + FP64 refinement on a spread of frequencies.
+    out_fp64 = None
+    if not args.no_fp64 and args.sweep_fp64_count > 0:
+        pick = np.unique(np.linspace(0, len(mats) - 1, args.sweep_fp64_count).round().astype(int))
+        f64 = sym.factor(mats[0], st)
+        s64 = torch.cuda.ExternalStream(f64.stream())
+        res = []
+
+        def fp64_some():
+            for i in pick:
+                rc = N.lib.rslab_refactor(f64._h, C.c_void_p(vals_d[i].data_ptr()), 1)
+                assert rc == 0, N.last_error()
+                rc = N.lib.rslab_solve(f64._h, C.c_void_p(b_d.data_ptr()), nrhs, C.c_void_p(x_d.data_ptr()), 1)
+                assert rc == 0, N.last_error()
+
+        ms64, _ = timed(fp64_some, s64, 1, 1)
+        ms64 = allmax(ms64 / len(pick), ws)
+        from oracle.oracle import backward_error
+        for i in pick[-1:]:
+            res.append(backward_error(mats[i], x_d.cpu().numpy(), b))
+        out_fp64 = {"ms_per_frequency": ms64, "frequencies_timed": int(len(pick)),
+                    "ms_per_sweep_projected": ms64 * len(om_all) / ws,
+                    "gflops": flops / (ms64 * 1e-3) / 1e9,
+                    "backward_error_no_ir_last": res[-1] if res else None}
+
+    # End to end through the public API with page-locked host buffers: every
+    # frequency's values and the right-hand sides copied in, solutions out.
+    def pinned(arr):
+        t = torch.empty(arr.shape, dtype={np.complex128: torch.complex128}[arr.dtype.type], pin_memory=True)
+        v = t.numpy()
+        v[...] = arr
+        return t, v
+    keep = []
+    mats_h = []
+    for a in mats:
+        t, v = pinned(np.ascontiguousarray(a.values))
+        keep.append(t)
+        mats_h.append(CscMatrix(a.n, a.col_ptr, a.row_idx, v))
+    _pb, b_h = pinned(np.ascontiguousarray(b))
+    _px, x_h = pinned(np.zeros_like(np.ascontiguousarray(b)))
+    cert_h = 0
+    t0 = time.perf_counter()
+    for a_h in mats_h:
+        mixed.refactor(a_h)
+        x_h, inf_h = mixed.solve_to(a_h, b_h, args.target, out=x_h)
+        cert_h += int(bool(inf_h.certified))
+    e2e_s = allmax(time.perf_counter() - t0, ws)
+
+    cpu_base = sweep_cpu_sample() if (rank == 0 and ws == 1 and not args.no_cpu) else None
+    total_flops = flops * len(om_all)
+    if rank == 0:
+        line = {
+            "metric": "LDLT factor+solve GFLOP/s at bwd err <= 1e-14 (mixed/batched vs FP64 GPU)",
+            "value": total_flops / (ms_sweep * 1e-3) / 1e9, "unit": "GFLOP/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_sweep, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "c32 factor / f64 refinement", "data": "synthetic",
+            "config": {"workload": f"freq_sweep_{args.sweep_side}^3_27pt_c32_nrhs{nrhs}_{len(om_all)}w",
+                       "n": c4.n, "nnz_lower": mats[0].nnz, "frequencies": len(om_all), "nrhs": nrhs,
+                       "ordering": "AMD", "static_pivot": 1e-10, "target_backward_error": args.target,
+                       "model_flops_per_frequency": flops, "parallelism": f"frequencies round-robin over {ws}",
+                       "l2": "flushed between steps (256 MB write)"},
+            "sweep": {"ms_per_frequency": ms_sweep / len(mine),
+                      "certified": int(sum(1 for c, *_ in infos if c)), "of": len(infos),
+                      "max_backward_error": max(be for _, be, _, _ in infos),
+                      "ir_iters_max": max(i for _, _, i, _ in infos),
+                      "gmres_iters_max": max(g for *_, g in infos)},
+            "fp64_gpu": out_fp64,
+            "e2e": {"value": flops * len(mine) / e2e_s / 1e9 * ws, "unit": "GFLOP/s", "seconds_per_step": e2e_s,
+                    "h2d_bytes_per_step": int(sum(a.values.nbytes for a in mats) + len(mats) * b.nbytes),
+                    "d2h_bytes_per_step": int(len(mats) * b.nbytes), "certified": cert_h,
+                    "host_buffers": "page-locked (torch pin_memory) numpy views"},
+            "clocks": clocks,
+            "cpu_baseline": cpu_base,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init(args)
     if args.impl == "reference":
         run_reference(args, ws, rank)
+        return
+    if args.workload == "sweep":
+        run_sweep(args, ws, rank, local)
         return
     import torch
 

@@ -167,6 +167,38 @@ def c3_batch(count: int = 512, seed: int = 2, lo: int = 12, hi: int = 40) -> lis
     return [c3_matrix(s) for s in c3_sides(count, seed, lo, hi)]
 
 
+class C4System:
+    """The same-pattern frequency-sweep workload A(w) = K - w^2 M + i w C:
+    K the 3D 27-point stencil on a side^3 grid (off-diagonal -1, diagonal
+    26 + U[0, 0.1]), M diagonal U[0.5, 1.5], C = 0.01 K, complex symmetric.
+    The frequencies are `count` points evenly spaced in [0.1, 2] sqrt(l_mid),
+    l_mid the centre of K's Gershgorin interval (the stencil's spectrum lies
+    inside it).  Draws: K's diagonal, then M's, from Rng(seed)."""
+
+    def __init__(self, side: int = 48, seed: int = 3):
+        rng = Rng(seed)
+        diag, rows, cols, w = stencil27(side, rng)
+        self.side = side
+        self.n = side ** 3
+        self.mdiag = 0.5 + rng.units(self.n)
+        self.K = _lower_csc(self.n, diag, rows, cols, w)
+        # Gershgorin: K_ii -/+ (number of stencil neighbours of i)
+        deg = np.bincount(rows, minlength=self.n) + np.bincount(cols, minlength=self.n)
+        self.lambda_mid = 0.5 * (float(np.min(diag - deg)) + float(np.max(diag + deg)))
+        cp = self.K.col_ptr
+        self._diag_pos = np.asarray(cp[:-1], np.int64)  # (j, j) is the first entry of column j
+        assert np.array_equal(np.asarray(self.K.row_idx)[self._diag_pos], np.arange(self.n))
+
+    def omegas(self, count: int = 64) -> np.ndarray:
+        return np.linspace(0.1, 2.0, count) * math.sqrt(self.lambda_mid)
+
+    def matrix(self, omega: float) -> CscMatrix:
+        """A(omega) on K's lower-triangle pattern (complex128)."""
+        v = np.asarray(self.K.values, np.float64) * (1.0 + 0.01j * omega)
+        v[self._diag_pos] -= omega * omega * self.mdiag
+        return CscMatrix(self.n, self.K.col_ptr, self.K.row_idx, v)
+
+
 def negative_eigs_shifted_laplacian(dims, sigma: float) -> int:
     """Exact count of eigenvalues of -Delta_h - sigma I below zero (separable spectrum)."""
     ev = None

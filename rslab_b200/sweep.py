@@ -1,0 +1,40 @@
+"""Same-pattern frequency sweeps: one analysis, one low-precision factor
+handle, then per frequency a refactor (the captured factor graph replayed on
+the new values) and a solve refined in FP64 to the target backward error.
+
+The reference factors every frequency from scratch through
+`MixedLdltSolver::factor` (src/numeric/mixed.rs:234) and `solve_to` (:267);
+here the symbolic analysis and the launch plan are reused and each refactor
+replays the factor graph, which is what keeps a 64-point sweep cheap.  Zero
+pivots follow the settings' `on_zero_pivot` (static pivoting by default, as
+the workload asks).
+"""
+from __future__ import annotations
+
+from typing import Iterator, Optional, Sequence, Tuple
+
+import numpy as np
+
+from .solver import CscMatrix, LdltSymbolic, MixedInfo, MixedLdltSolver, SolverSettings
+
+
+def sweep_settings() -> SolverSettings:
+    """Static pivoting: a pivot below 1e-10 (scaled matrix) is perturbed to
+    that floor instead of failing the factor; IR certifies the result."""
+    return SolverSettings.preconditioner(1e-10)
+
+
+def frequency_sweep(matrices, b: np.ndarray, target: float = 1e-14,
+                    settings: Optional[SolverSettings] = None) -> Iterator[Tuple[int, np.ndarray, MixedInfo]]:
+    """Yield (index, x, info) for every matrix of `matrices` (an iterable of
+    CscMatrix on one pattern), solving A_i x = b to `target`."""
+    st = settings or sweep_settings()
+    solver = None
+    for i, a in enumerate(matrices):
+        if solver is None:
+            sym = LdltSymbolic.analyze_with(a, st)
+            solver = MixedLdltSolver.factor_with(a, st, sym=sym)
+        else:
+            solver.refactor(a)
+        x, info = solver.solve_to(a, b, target)
+        yield i, x, info
