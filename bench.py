@@ -50,9 +50,12 @@ def parse():
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--cpu-sample-side", type=int, default=36)
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--workload", default="helmholtz", choices=["helmholtz", "sweep"],
+    p.add_argument("--workload", default="helmholtz", choices=["helmholtz", "sweep", "tiers"],
                    help="helmholtz: the 64^3 Helmholtz factor+solve step (default); sweep: the "
-                        "same-pattern frequency sweep, 48^3 27-point K - w^2 M + i w C, 64 frequencies")
+                        "same-pattern frequency sweep, 48^3 27-point K - w^2 M + i w C, 64 frequencies; "
+                        "tiers: the learned precision tier on the held-out 80^3 27-point complex Helmholtz")
+    p.add_argument("--tiers-side", type=int, default=80)
+    p.add_argument("--tier-model", default=None, help="tier network .npz (default: the package's trained one)")
     p.add_argument("--sweep-side", type=int, default=48)
     p.add_argument("--sweep-count", type=int, default=64)
     p.add_argument("--sweep-fp64-count", type=int, default=4,
@@ -401,6 +404,138 @@ def run_sweep(args, ws, rank, local):
         dist.destroy_process_group()
 
 
+def run_tiers(args, ws, rank, local):
+    """Learned precision tier on the held-out matrix: 27-point complex
+    Helmholtz K - k2 (1 + 0.02 i) I on an 80^3 grid (n = 512,000), k2 =
+    0.15 lambda_max, 4 right-hand sides, backward error <= 1e-14.  The tier
+    network picks the factor's precision from the matrix's features (outside
+    the timed region, with the analysis); a step is refactor + refined solve
+    in that tier, plus the FP64 refactor + solve if it did not certify.  The
+    plain FP64 tier is timed on the same matrix for the ratio."""
+    import ctypes as C
+
+    import torch
+
+    from rslab_b200 import CscMatrix, LdltSymbolic, MixedLdltSolver, matgen
+    from rslab_b200 import _native as N
+    from rslab_b200.tiers import TIERS, TierModel, tier_features, tier_settings
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    a = matgen.c5_heldout(args.tiers_side, 6)
+    nrhs = 4
+    b = matgen.uniform_rhs(a.n, nrhs, 6, complex_=True)
+    st = tier_settings()
+    t0 = time.perf_counter()
+    sym = LdltSymbolic.analyze_with(a, st)
+    t_an = time.perf_counter() - t0
+    info = sym.info()
+    flops = 4.0 * info.flops_model
+    model = TierModel.load(args.tier_model) if args.tier_model else TierModel.load()
+    feats = tier_features(a, sym)
+    probs = model.predict_proba(feats)[0]
+    tier = int(np.argmax(probs))
+    vals_d = torch.from_numpy(np.ascontiguousarray(a.values)).to(dev)
+    b_d = torch.from_numpy(np.ascontiguousarray(b)).to(dev)
+    x_d = torch.empty_like(b_d)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    h = MixedLdltSolver.factor_tier(a, tier, st, sym)
+    h64 = MixedLdltSolver.factor_tier(a, N.TIER_FP64, st, sym) if tier != N.TIER_FP64 else h
+
+    def one(handle):
+        rc = N.lib.rslab_refactor(handle._h, C.c_void_p(vals_d.data_ptr()), 1)
+        assert rc == 0, N.last_error()
+        inf = N.MixedInfoC()
+        rc = N.lib.rslab_mixed_solve(handle._h, C.c_void_p(b_d.data_ptr()), nrhs, args.target,
+                                     C.c_void_p(x_d.data_ptr()), 1, C.byref(inf))
+        assert rc == 0, N.last_error()
+        return inf
+
+    def learned_step():
+        inf = one(h)
+        if not inf.certified and h is not h64:
+            return one(h64), True
+        return inf, False
+
+    def timed(fn, strm, steps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        barrier(ws)
+        tot, last = 0.0, None
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(strm)
+            last = fn()
+            e1.record(strm)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        barrier(ws)
+        return tot / steps, last
+
+    clk = ClockSampler(local)
+    clk.start()
+    ms, (minfo, fell) = timed(learned_step, torch.cuda.ExternalStream(h.stream()), args.steps, args.warmup)
+    clocks = clk.stop()
+    ms = allmax(ms, ws)
+    out64 = None
+    if not args.no_fp64:
+        ms64, inf64 = timed(lambda: one(h64), torch.cuda.ExternalStream(h64.stream()), max(1, args.steps // 2), 1)
+        ms64 = allmax(ms64, ws)
+        out64 = {"ms_per_step": ms64, "gflops": flops / (ms64 * 1e-3) / 1e9, "certified": bool(inf64.certified),
+                 "backward_error": inf64.backward_error, "ir_iters": inf64.ir_iters}
+    # end to end: host values and right-hand sides in page-locked memory
+    def pinned(arr):
+        t = torch.empty(arr.shape, dtype=torch.complex128, pin_memory=True)
+        v = t.numpy()
+        v[...] = arr
+        return t, v
+    _pa, vals_h = pinned(np.ascontiguousarray(a.values))
+    _pb, b_h = pinned(np.ascontiguousarray(b))
+    _px, x_h = pinned(np.zeros_like(np.ascontiguousarray(b)))
+    a_h = CscMatrix(a.n, a.col_ptr, a.row_idx, vals_h)
+    te = []
+    for it in range(2):
+        t0 = time.perf_counter()
+        h.refactor(a_h)
+        x_h, inf_h = h.solve_to(a_h, b_h, args.target, out=x_h)
+        if not inf_h.certified and h is not h64:
+            h64.refactor(a_h)
+            x_h, inf_h = h64.solve_to(a_h, b_h, args.target, out=x_h)
+        if it:
+            te.append(time.perf_counter() - t0)
+    e2e_s = allmax(float(np.mean(te)), ws)
+    if rank == 0:
+        line = {
+            "metric": "LDLT factor+solve GFLOP/s at bwd err <= 1e-14 (mixed/batched vs FP64 GPU)",
+            "value": flops / (ms * 1e-3) / 1e9 * ws, "unit": "GFLOP/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": f"{TIERS[tier]} factor / f64 refinement", "data": "synthetic",
+            "config": {"workload": f"learned_tier_helmholtz27_{args.tiers_side}^3_c64_nrhs{nrhs}", "n": a.n,
+                       "nnz_lower": a.nnz, "nrhs": nrhs, "ordering": "AMD", "static_pivot": 1e-10,
+                       "target_backward_error": args.target, "model_flops": flops,
+                       "factor_nnz_panels": info.panel_elems, "analysis_s": t_an,
+                       "parallelism": f"replicas{ws}", "l2": "flushed between steps (256 MB write)"},
+            "tier": {"chosen": TIERS[tier], "probabilities": [float(p) for p in probs],
+                     "features": [float(f) for f in feats], "fell_back_to_fp64": bool(fell),
+                     "certified": bool(minfo.certified), "backward_error": minfo.backward_error,
+                     "ir_iters": minfo.ir_iters, "gmres_iters": minfo.gmres_iters},
+            "fp64_gpu": out64,
+            "e2e": {"value": flops / e2e_s / 1e9 * ws, "unit": "GFLOP/s", "seconds_per_step": e2e_s,
+                    "h2d_bytes_per_step": int(a.values.nbytes + b.nbytes), "d2h_bytes_per_step": int(b.nbytes),
+                    "certified": bool(inf_h.certified), "host_buffers": "page-locked (torch pin_memory) numpy views"},
+            "clocks": clocks,
+            "cpu_baseline": {"value": None, "unit": "GFLOP/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"not timed: {flops:.3g} model flops per factor is hours of host work"},
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init(args)
@@ -409,6 +544,9 @@ def main():
         return
     if args.workload == "sweep":
         run_sweep(args, ws, rank, local)
+        return
+    if args.workload == "tiers":
+        run_tiers(args, ws, rank, local)
         return
     import torch
 

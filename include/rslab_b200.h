@@ -17,6 +17,9 @@
  *   rslab_solve          LdltSolver::solve / solve_many (src/numeric/sparse_solver.rs:274,302)
  *   rslab_mixed_factor   MixedLdltSolver::factor / factor_with (src/numeric/mixed.rs:234,245)
  *   rslab_mixed_solve    MixedLdltSolver::solve / solve_to (src/numeric/mixed.rs:258,267)
+ *   rslab_tier_factor    MixedLdltSolver::factor with the precision chosen per
+ *                        matrix (src/numeric/mixed.rs:234); rslab_tier_mlp_*
+ *                        (the network that chooses it) have no counterpart
  *   rslab_factor_info    LdltSolver::inertia / n_perturbed / diagnostics
  *                        (src/numeric/sparse_solver.rs:81,72,57)
  *   rslab_export_factors LdltFactors (src/dense/ldlt_generic.rs:31-66), the
@@ -221,6 +224,46 @@ int rslab_mixed_factor(rslab_sym_handle* sym, int dtype_hi, const void* values_h
                        const rslab_factor_settings* settings, rslab_fac_handle** out);
 int rslab_mixed_solve(rslab_fac_handle* fac, const void* b, int64_t nrhs, double target, void* x, int on_device,
                       rslab_mixed_info* info);
+
+/* Precision tiers of a refined factor.  The tier fixes the precision the
+ * factor is computed and stored in; refinement always runs against the
+ * original FP64 matrix and certifies the normwise backward error. */
+#define RSLAB_TIER_FP64 0   /* factor in the matrix's own field (f64 / c64) */
+#define RSLAB_TIER_FP32 1   /* f32 / c32 factor, CUDA-core descendant updates */
+#define RSLAB_TIER_TF32X3 2 /* f32 / c32 factor, 3xTF32 tensor-core descendant updates */
+
+/* Refined factor in a chosen precision tier: rslab_mixed_factor generalised
+ * (src/numeric/mixed.rs:234-256 factors in f32 / c32 only).  The handle is
+ * solved with rslab_mixed_solve whatever the tier; RSLAB_TIER_FP64 makes the
+ * plain FP64 factor the preconditioner of the same refinement ladder (the
+ * fallback when a low tier does not certify). */
+int rslab_tier_factor(rslab_sym_handle* sym, int dtype_hi, int tier, const void* values_hi, int values_on_device,
+                      const rslab_factor_settings* settings, rslab_fac_handle** out);
+
+/* Tier network: 8 features -> 64 -> 64 -> 3 tier probabilities (ReLU hidden
+ * layers, softmax output), FP32.  No counterpart in the reference: it picks
+ * the precision tier above per matrix, trained on labels the solver makes by
+ * running every tier and keeping the cheapest one that certifies.  Parameters
+ * (RSLAB_TIER_MLP_PARAMS floats): W1[64][8], b1[64], W2[64][64], b2[64],
+ * W3[3][64], b3[3], rows = output units.  x is m x 8 row-major (already
+ * standardised), y holds labels 0..2, w optional per-sample weights (NULL =
+ * 1).  on_device = 1: every array is device memory. */
+#define RSLAB_TIER_FEATURES 8
+#define RSLAB_TIER_HIDDEN 64
+#define RSLAB_TIER_COUNT 3
+#define RSLAB_TIER_MLP_PARAMS 4931
+/* probs: m x 3 softmax outputs. */
+int rslab_tier_mlp_forward(const float* params, const float* x, int64_t m, float* probs, int on_device);
+/* Gradient of the weighted mean cross-entropy sum_s w_s CE_s / sum_s w_s
+ * with respect to the parameters (grad: RSLAB_TIER_MLP_PARAMS floats), and
+ * that loss. */
+int rslab_tier_mlp_grad(const float* params, const float* x, const int32_t* y, const float* w, int64_t m,
+                        float* grad, float* loss, int on_device);
+/* `epochs` full-batch Adam steps (beta 0.9 / 0.999, eps 1e-8, rate lr) on the
+ * same loss, params updated in place; loss_curve[e] (optional) = the loss
+ * before step e. */
+int rslab_tier_mlp_train(float* params, const float* x, const int32_t* y, const float* w, int64_t m, int64_t epochs,
+                         float lr, float* loss_curve, int on_device);
 
 /* Synthetic-workload generator: m unit draws of the xorshift64* state
  * `state`; returns the advanced state. */

@@ -15,8 +15,12 @@ ORDER_AMD, ORDER_METIS_ND, ORDER_NATURAL, ORDER_GIVEN = 0, 1, 2, 3
 PIVOT_FAIL, PIVOT_PERTURB, PIVOT_FORCE_ACCEPT = 0, 1, 2
 SCALING_ONEPASS, SCALING_IDENTITY = 0, 1
 SCHUR_TENSOR, SCHUR_FMA = 0, 1
+TIER_FP64, TIER_FP32, TIER_TF32X3 = 0, 1, 2
+TIER_MLP_PARAMS = 4931
 
 i64p = C.POINTER(C.c_int64)
+i32p = C.POINTER(C.c_int32)
+fp = C.POINTER(C.c_float)
 vp = C.c_void_p
 
 
@@ -106,6 +110,10 @@ SIGNATURES = {
     "rslab_free_factor": (None, [vp]),
     "rslab_mixed_factor": (C.c_int, [vp, C.c_int, vp, C.c_int, C.POINTER(FactorSettings), C.POINTER(vp)]),
     "rslab_mixed_solve": (C.c_int, [vp, vp, C.c_int64, C.c_double, vp, C.c_int, C.POINTER(MixedInfoC)]),
+    "rslab_tier_factor": (C.c_int, [vp, C.c_int, C.c_int, vp, C.c_int, C.POINTER(FactorSettings), C.POINTER(vp)]),
+    "rslab_tier_mlp_forward": (C.c_int, [fp, fp, C.c_int64, fp, C.c_int]),
+    "rslab_tier_mlp_grad": (C.c_int, [fp, fp, i32p, fp, C.c_int64, fp, fp, C.c_int]),
+    "rslab_tier_mlp_train": (C.c_int, [fp, fp, i32p, fp, C.c_int64, C.c_int64, C.c_float, fp, C.c_int]),
     "rslab_rng_units": (C.c_uint64, [C.c_uint64, C.c_int64, C.POINTER(C.c_double)]),
     "rslab_amd_order": (C.c_int, [C.c_int64, i64p, i64p, i64p, C.POINTER(C.c_double)]),
     "rslab_panel_factor_noalloc": (C.c_int, [C.c_int, vp, C.c_int64, C.c_int64, C.c_int64, vp, vp, vp, vp, vp,

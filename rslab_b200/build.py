@@ -35,7 +35,7 @@ def nvcc() -> str:
 
 
 def sources() -> list[Path]:
-    return sorted((CSRC / "host").glob("*.cpp")) + [CSRC / "engine.cu"]
+    return sorted((CSRC / "host").glob("*.cpp")) + [CSRC / "engine.cu", CSRC / "tier_mlp.cu"]
 
 
 def deps() -> list[Path]:

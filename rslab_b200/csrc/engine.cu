@@ -1379,6 +1379,13 @@ struct MixedCtx {
   // dx = promote(F_lo^-1 demote(r)) for an n x k block (k <= nrhs, ld = k).
   void precond(const Hi* rr, Hi* out, int k) {
     const long long m = (long long)n * k;
+    if (F.dtype == F.dtype_hi) {  // FP64 tier: the factor is in the matrix's own field
+      ensure_ws<Hi>(F, k);
+      CK(cudaMemcpyAsync(F.bdev, rr, m * sizeof(Hi), cudaMemcpyDeviceToDevice, st));
+      solve_ws<Hi>(F, k);
+      CK(cudaMemcpyAsync(out, F.xdev, m * sizeof(Hi), cudaMemcpyDeviceToDevice, st));
+      return;
+    }
     ensure_ws<Lo>(F, k);
     k_cast_down<Hi, Lo><<<grid1(m), 256, 0, st>>>(m, rr, (Lo*)F.bdev);
     solve_ws<Lo>(F, k);
@@ -1481,6 +1488,12 @@ static void refined_solve_impl(rslab_fac_handle& F, const void* bsrc, int nrhs, 
   CK(cudaStreamSynchronize(st));
   wave_check(F);
 }
+
+namespace rslab {
+// Sets the calling thread's last-error message (for entry points defined in
+// other translation units of the library).
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace rslab
 
 extern "C" {
 
@@ -1684,6 +1697,24 @@ int rslab_symbolic_export(const rslab_sym_handle* h, int64_t* perm, int64_t* sn_
   return 0;
 }
 
+// The matrix values into the handle: straight into the factor's input, or,
+// for a refined handle, into the original (FP64) copy and from there demoted
+// (or, for the FP64 tier, copied) into the factor's input.
+static void load_values(rslab_fac_handle& F, const void* values, cudaMemcpyKind kd) {
+  const long long nnz = F.sym->nnz;
+  if (F.dtype_hi < 0) {
+    CK(cudaMemcpyAsync(F.aval, values, nnz * elem_size(F.dtype), kd, F.st));
+    return;
+  }
+  CK(cudaMemcpyAsync(F.aval_hi, values, nnz * elem_size(F.dtype_hi), kd, F.st));
+  if (F.dtype == F.dtype_hi)
+    CK(cudaMemcpyAsync(F.aval, F.aval_hi, nnz * elem_size(F.dtype), cudaMemcpyDeviceToDevice, F.st));
+  else if (F.dtype_hi == RSLAB_F64)
+    k_demote<double, float><<<grid1(nnz), 256, 0, F.st>>>(nnz, (const double*)F.aval_hi, (float*)F.aval);
+  else
+    k_demote<c64, c32><<<grid1(nnz), 256, 0, F.st>>>(nnz, (const c64*)F.aval_hi, (c32*)F.aval);
+}
+
 static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const void* values, int on_device,
                        const rslab_factor_settings* settings, rslab_fac_handle** out) {
   try {
@@ -1743,18 +1774,8 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
       CK(cudaStreamSynchronize(F->st));
     }
     const cudaMemcpyKind kd = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    if (dtype_hi >= 0) {
-      const size_t eh = elem_size(dtype_hi);
-      F->aval_hi = F->al<unsigned char>(sym->nnz * eh);
-      CK(cudaMemcpyAsync(F->aval_hi, values, sym->nnz * eh, kd, F->st));
-      if (dtype_hi == RSLAB_F64)
-        k_demote<double, float><<<grid1(sym->nnz), 256, 0, F->st>>>(sym->nnz, (const double*)F->aval_hi,
-                                                                    (float*)F->aval);
-      else
-        k_demote<c64, c32><<<grid1(sym->nnz), 256, 0, F->st>>>(sym->nnz, (const c64*)F->aval_hi, (c32*)F->aval);
-    } else {
-      CK(cudaMemcpyAsync(F->aval, values, sym->nnz * es, kd, F->st));
-    }
+    if (dtype_hi >= 0) F->aval_hi = F->al<unsigned char>(sym->nnz * elem_size(dtype_hi));
+    load_values(*F, values, kd);
     rslab_fac_handle* raw = F.get();
     int rc = 0;
     try {
@@ -1787,21 +1808,34 @@ int rslab_mixed_factor(rslab_sym_handle* sym, int dtype_hi, const void* values_h
   return factor_impl(sym, lo, dtype_hi, values_hi, values_on_device, settings, out);
 }
 
+int rslab_tier_factor(rslab_sym_handle* sym, int dtype_hi, int tier, const void* values_hi, int values_on_device,
+                      const rslab_factor_settings* settings, rslab_fac_handle** out) {
+  if (dtype_hi != RSLAB_F64 && dtype_hi != RSLAB_C64) {
+    g_last_error = "tier factor needs an f64 or c64 matrix";
+    return (int)Status::InvalidInput;
+  }
+  if (tier < RSLAB_TIER_FP64 || tier > RSLAB_TIER_TF32X3) {
+    g_last_error = "tier must be RSLAB_TIER_FP64, RSLAB_TIER_FP32 or RSLAB_TIER_TF32X3";
+    return (int)Status::InvalidInput;
+  }
+  rslab_factor_settings s;
+  if (settings)
+    s = *settings;
+  else
+    rslab_default_factor_settings(&s);
+  if (tier == RSLAB_TIER_FP64)
+    return factor_impl(sym, dtype_hi, dtype_hi, values_hi, values_on_device, &s, out);
+  s.schur_engine = tier == RSLAB_TIER_FP32 ? RSLAB_SCHUR_FMA : RSLAB_SCHUR_TENSOR;
+  const int lo = dtype_hi == RSLAB_F64 ? RSLAB_F32 : RSLAB_C32;
+  return factor_impl(sym, lo, dtype_hi, values_hi, values_on_device, &s, out);
+}
+
 int rslab_refactor(rslab_fac_handle* F, const void* values, int values_on_device) {
   try {
     if (!F) throw RslabError(Status::InvalidInput, "null handle");
     auto& H = *F->sym;
-    const cudaMemcpyKind kd = values_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    if (F->dtype_hi >= 0) {
-      const size_t eh = elem_size(F->dtype_hi);
-      CK(cudaMemcpyAsync(F->aval_hi, values, H.nnz * eh, kd, F->st));
-      if (F->dtype_hi == RSLAB_F64)
-        k_demote<double, float><<<grid1(H.nnz), 256, 0, F->st>>>(H.nnz, (const double*)F->aval_hi, (float*)F->aval);
-      else
-        k_demote<c64, c32><<<grid1(H.nnz), 256, 0, F->st>>>(H.nnz, (const c64*)F->aval_hi, (c32*)F->aval);
-    } else {
-      CK(cudaMemcpyAsync(F->aval, values, H.nnz * elem_size(F->dtype), kd, F->st));
-    }
+    (void)H;
+    load_values(*F, values, values_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
     dispatch_field(F->dtype, [&](auto z) { run_factor<decltype(z)>(*F); });
     return 0;
   } catch (const RslabError& e) {

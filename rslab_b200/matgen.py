@@ -199,6 +199,97 @@ class C4System:
         return CscMatrix(self.n, self.K.col_ptr, self.K.row_idx, v)
 
 
+def stencil27_lambda_max(side: int) -> float:
+    """Largest eigenvalue of the 27-point operator 26 I - (neighbour sum) with
+    Dirichlet ends: 27 - prod_d (1 + 2 cos t_d), minimised at one t_d =
+    side pi/(side+1) and two t_d = pi/(side+1)."""
+    c = math.cos(math.pi / (side + 1))
+    return 27.0 - (1.0 - 2.0 * c) * (1.0 + 2.0 * c) ** 2
+
+
+def normals(rng: Rng, m: int) -> np.ndarray:
+    """m N(0, 1) draws by the Box-Muller transform of 2m unit draws."""
+    u = rng.units(2 * m).reshape(m, 2)
+    return np.sqrt(-2.0 * np.log1p(-u[:, 0])) * np.cos(2.0 * math.pi * u[:, 1])
+
+
+def random_sparse_symmetric(n: int, rng: Rng, shift: float) -> CscMatrix:
+    """Symmetric n x n: every row draws 8-30 partner columns (uniform) with
+    N(0, 1) values (the symmetric pair shares the value; repeats add), the
+    diagonal is N(0, 1) + shift."""
+    k = 8 + np.minimum((rng.units(n) * 23).astype(np.int64), 22)
+    rows = np.repeat(np.arange(n), k)
+    cols = np.minimum((rng.units(int(k.sum())) * n).astype(np.int64), n - 1)
+    vals = normals(rng, len(rows))
+    keep = rows != cols
+    r, c, v = np.maximum(rows, cols)[keep], np.minimum(rows, cols)[keep], vals[keep]
+    diag = normals(rng, n) + shift
+    return _lower_csc(n, diag, r, c, v)
+
+
+C5_FAMILIES = ("laplacian2d", "laplacian3d", "stencil27", "random_sparse", "helmholtz27", "helmholtz7")
+
+
+def c5_corpus(count: int = 2000, seed: int = 5):
+    """The precision-tier training corpus: `count` seeded matrices, yielded
+    as (family, CscMatrix).  Family uniform over C5_FAMILIES, parameters from
+    Rng(seed) in order:
+      laplacian2d   side U{16..160}, -Delta_h - s lambda_max I, s U[0, 0.6]
+      laplacian3d   side U{8..40},   s U[0, 0.4]
+      stencil27     side U{8..32},   27-point K - s lambda_max I, s U[0, 0.5]
+      random_sparse n U{500..8000},  8-30 N(0,1) entries per row, shift U[-1, 1] sqrt(19)
+      helmholtz27   side U{8..32},   K - k2 (1 + i eta) I, k2 = U[0.05, 0.3] lambda_max, eta U[0, 0.05]
+      helmholtz7    side U{8..40},   7-point, same k2 / eta draws (complex)
+    The stencils' random diagonals and the random patterns draw from
+    Rng(seed * 1000003 + index)."""
+    rng = Rng(seed)
+
+    def uint(lo, hi):
+        return lo + min(int(rng.unit() * (hi - lo + 1)), hi - lo)
+
+    for idx in range(count):
+        fam = C5_FAMILIES[uint(0, len(C5_FAMILIES) - 1)]
+        sub = Rng(seed * 1000003 + idx)
+        if fam == "laplacian2d":
+            side = uint(16, 160)
+            dims = (side, side)
+            a = shifted_laplacian(dims, rng.range(0.0, 0.6) * lambda_max(dims))
+        elif fam == "laplacian3d":
+            side = uint(8, 40)
+            dims = (side, side, side)
+            a = shifted_laplacian(dims, rng.range(0.0, 0.4) * lambda_max(dims))
+        elif fam == "stencil27":
+            side = uint(8, 32)
+            s = rng.range(0.0, 0.5)
+            diag, rows, cols, w = stencil27(side, sub)
+            a = _lower_csc(side ** 3, diag - s * stencil27_lambda_max(side), rows, cols, w)
+        elif fam == "random_sparse":
+            n = uint(500, 8000)
+            a = random_sparse_symmetric(n, sub, rng.range(-1.0, 1.0) * math.sqrt(19.0))
+        else:
+            side = uint(8, 32) if fam == "helmholtz27" else uint(8, 40)
+            k2 = rng.range(0.05, 0.3)
+            eta = rng.range(0.0, 0.05)
+            if fam == "helmholtz27":
+                diag, rows, cols, w = stencil27(side, sub)
+                lam = stencil27_lambda_max(side)
+            else:
+                diag, rows, cols, w = laplacian_weights((side, side, side))
+                lam = lambda_max((side, side, side))
+            shift = k2 * lam * (1.0 + 1j * eta)
+            a = _lower_csc(side ** 3, diag.astype(np.complex128) - shift, rows, cols, w.astype(np.complex128))
+        yield fam, a
+
+
+def c5_heldout(side: int = 80, seed: int = 6) -> CscMatrix:
+    """The held-out evaluation matrix of the precision-tier network: 27-point
+    complex Helmholtz K - k2 (1 + 0.02 i) I on a side^3 grid, k2 = 0.15
+    lambda_max (K's diagonal 26 + U[0, 0.1] from Rng(seed))."""
+    diag, rows, cols, w = stencil27(side, Rng(seed))
+    shift = 0.15 * stencil27_lambda_max(side) * (1.0 + 0.02j)
+    return _lower_csc(side ** 3, diag.astype(np.complex128) - shift, rows, cols, w.astype(np.complex128))
+
+
 def negative_eigs_shifted_laplacian(dims, sigma: float) -> int:
     """Exact count of eigenvalues of -Delta_h - sigma I below zero (separable spectrum)."""
     ev = None

@@ -548,6 +548,26 @@ class MixedLdltSolver:
         _check(rc)
         return out
 
+    @classmethod
+    def factor_tier(cls, a: CscMatrix, tier: int, opts: Optional[SolverSettings] = None,
+                    sym: Optional[LdltSymbolic] = None, stream=None) -> "MixedLdltSolver":
+        """The refined factor in precision tier `tier` (N.TIER_FP64 / TIER_FP32 /
+        TIER_TF32X3; the tier sets the descendant-update engine).  TIER_FP64
+        factors in the matrix's own field and refines with the same ladder."""
+        opts = opts or SolverSettings()
+        sym = sym or LdltSymbolic.analyze_with(a, opts)
+        sym._check_pattern(a)
+        vals = np.ascontiguousarray(a.values)
+        if vals.dtype not in (np.dtype(np.float64), np.dtype(np.complex128)):
+            raise InvalidInput("tier factor needs an f64 or c64 matrix")
+        fs = opts._factor_c(stream)
+        h = C.c_void_p()
+        rc = N.lib.rslab_tier_factor(sym._h, _DT[vals.dtype], int(tier), vals.ctypes.data_as(C.c_void_p), 0,
+                                     C.byref(fs), C.byref(h))
+        out = cls(h, sym, vals.dtype) if h else None
+        _check(rc)
+        return out
+
     def refactor(self, a: CscMatrix) -> None:
         self._sym._check_pattern(a)
         vals = np.ascontiguousarray(a.values, dtype=self.dtype)
