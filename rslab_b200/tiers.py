@@ -118,10 +118,12 @@ def effective_cost(times: np.ndarray, certified: np.ndarray, tier: int) -> float
 
 
 def sample_weight(times: np.ndarray, certified: np.ndarray) -> float:
-    """Training weight: how much a wrong choice costs on this matrix
-    (worst / best effective cost - 1, capped at 10), floor 0.05."""
+    """Training weight: the seconds a wrong choice can cost on this matrix
+    (worst minus best effective cost) + 1e-4 s, so that the weighted
+    cross-entropy follows the total time of the policy (matrices whose tier
+    hardly matters carry little weight)."""
     eff = np.array([effective_cost(times, certified, k) for k in range(len(TIERS))])
-    return float(min(10.0, eff.max() / eff.min() - 1.0) + 0.05)
+    return float(eff.max() - eff.min() + 1e-4)
 
 
 def label_corpus(count: int = 2000, seed: int = 5, nrhs: int = 4, target: float = 1e-14, reps: int = 1,
@@ -195,7 +197,7 @@ class TierModel:
     def standardise(self, x: np.ndarray) -> np.ndarray:
         return np.ascontiguousarray((np.asarray(x, np.float64) - self.mu) / self.sd, np.float32)
 
-    def fit(self, x: np.ndarray, y: np.ndarray, w: Optional[np.ndarray] = None, epochs: int = 1500,
+    def fit(self, x: np.ndarray, y: np.ndarray, w: Optional[np.ndarray] = None, epochs: int = 200,
             lr: float = 3e-3) -> np.ndarray:
         """Set the standardisation from x, then train on the GPU; returns the
         loss before every epoch."""
@@ -272,9 +274,12 @@ def solve_learned(a: CscMatrix, b: np.ndarray, model: Optional[TierModel] = None
     return x, info, tier, tier != N.TIER_FP64
 
 
-def train_from_corpus(corpus: dict, epochs: int = 1500, lr: float = 3e-3, seed: int = 7):
+def train_from_corpus(corpus: dict, epochs: int = 200, lr: float = 3e-3, seed: int = 7):
     """Train on the corpus's training split; returns (model, loss curve,
-    held-out report)."""
+    held-out report).  200 full-batch epochs at 3e-3 with regret weights:
+    chosen by 4-fold cross-validation of the policy cost on the training
+    split (longer training fits the training matrices' timing outliers and
+    costs more on unseen ones)."""
     count = len(corpus["labels"])
     tr, te = split(count)
     w = np.array([sample_weight(corpus["times"][i], corpus["certified"][i]) for i in range(count)])
@@ -299,7 +304,7 @@ def _main():
     p2 = sub.add_parser("train", help="train the network on a labelled corpus (GPU)")
     p2.add_argument("--corpus", required=True)
     p2.add_argument("--out", required=True)
-    p2.add_argument("--epochs", type=int, default=1500)
+    p2.add_argument("--epochs", type=int, default=200)
     p2.add_argument("--lr", type=float, default=3e-3)
     args = ap.parse_args()
     if args.cmd == "label":
