@@ -225,6 +225,20 @@ int rslab_mixed_factor(rslab_sym_handle* sym, int dtype_hi, const void* values_h
 int rslab_mixed_solve(rslab_fac_handle* fac, const void* b, int64_t nrhs, double target, void* x, int on_device,
                       rslab_mixed_info* info);
 
+/* Right-preconditioned restarted block GMRES (gmres_block,
+ * src/numeric/iterative.rs:1881) on the handle's FP64 matrix (the original
+ * matrix of a refined handle, the input of an f64 / c64 factor) with the
+ * handle's factor as the preconditioner (Preconditioner for LdltSolver,
+ * iterative.rs:178-190).  b, x0 (optional: NULL = zero start) and x are
+ * row-major n x s, the layout of rslab_solve (the reference's block API is
+ * column-major).  Columns run in groups of 16 in lockstep, one block
+ * preconditioner apply and one block product per step; block classical
+ * Gram-Schmidt with a per-column second pass, in-cycle deflation of
+ * converged columns.  iters = block steps of the longest group, final_res[s]
+ * = ||b_c - A x_c||_2 / ||b_c||_2, *converged = every column reached tol. */
+int rslab_gmres_block(rslab_fac_handle* fac, const void* b, int64_t s, double tol, int64_t max_iter, int64_t restart,
+                      const void* x0, void* x, int on_device, int64_t* iters, double* final_res, int* converged);
+
 /* Precision tiers of a refined factor.  The tier fixes the precision the
  * factor is computed and stored in; refinement always runs against the
  * original FP64 matrix and certifies the normwise backward error. */

@@ -110,6 +110,8 @@ SIGNATURES = {
     "rslab_free_factor": (None, [vp]),
     "rslab_mixed_factor": (C.c_int, [vp, C.c_int, vp, C.c_int, C.POINTER(FactorSettings), C.POINTER(vp)]),
     "rslab_mixed_solve": (C.c_int, [vp, vp, C.c_int64, C.c_double, vp, C.c_int, C.POINTER(MixedInfoC)]),
+    "rslab_gmres_block": (C.c_int, [vp, vp, C.c_int64, C.c_double, C.c_int64, C.c_int64, vp, vp, C.c_int, i64p,
+                                    C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     "rslab_tier_factor": (C.c_int, [vp, C.c_int, C.c_int, vp, C.c_int, C.POINTER(FactorSettings), C.POINTER(vp)]),
     "rslab_tier_mlp_forward": (C.c_int, [fp, fp, C.c_int64, fp, C.c_int]),
     "rslab_tier_mlp_grad": (C.c_int, [fp, fp, i32p, fp, C.c_int64, fp, fp, C.c_int]),

@@ -83,7 +83,10 @@ struct Arena {
 // Arena slots of the mixed-precision driver.
 enum ArenaSlot {
   A_R, A_DX, A_AX, A_NB, A_B, A_X, A_BEST, A_MASK, A_BC, A_XC, A_AXC,
-  A_GM_PART, A_GM_W, A_GM_R, A_GM_V, A_GM_Z, A_SEGNORM
+  A_GM_PART, A_GM_W, A_GM_R, A_GM_V, A_GM_Z, A_SEGNORM,
+  // block GMRES
+  A_BG_V0, A_BG_V1, A_BG_Z, A_BG_W, A_BG_AX, A_BG_XC, A_BG_PART, A_BG_DPART, A_BG_PROJ, A_BG_Y, A_BG_NRM,
+  A_BG_SCALE, A_BG_COLS, A_BG_B, A_BG_X, A_BG_R, A_BG_CL, A_BG_IB, A_BG_IX
 };
 
 size_t elem_size(int dtype) {
@@ -1379,7 +1382,7 @@ struct MixedCtx {
   // dx = promote(F_lo^-1 demote(r)) for an n x k block (k <= nrhs, ld = k).
   void precond(const Hi* rr, Hi* out, int k) {
     const long long m = (long long)n * k;
-    if (F.dtype == F.dtype_hi) {  // FP64 tier: the factor is in the matrix's own field
+    if (F.dtype_hi < 0 || F.dtype == F.dtype_hi) {  // FP64 tier / plain factor: the matrix's own field
       ensure_ws<Hi>(F, k);
       CK(cudaMemcpyAsync(F.bdev, rr, m * sizeof(Hi), cudaMemcpyDeviceToDevice, st));
       solve_ws<Hi>(F, k);
@@ -1394,13 +1397,16 @@ struct MixedCtx {
   void residual(const Hi* x, const Hi* b, Hi* rr, int k) {
     auto& H = *F.sym;
     k_residual<Hi><<<grid1((long long)n * k), 256, 0, st>>>(n, k, H.d_sp_rp, H.d_sp_ci, H.d_sp_vmap,
-                                                          (const Hi*)F.aval_hi, x, b, rr);
+                                                          op_values(), x, b, rr);
   }
   void spmv(const Hi* x, Hi* y, int k) {
     auto& H = *F.sym;
     k_spmv<Hi><<<grid1((long long)n * k), 256, 0, st>>>(n, k, H.d_sp_rp, H.d_sp_ci, H.d_sp_vmap,
-                                                      (const Hi*)F.aval_hi, x, y);
+                                                      op_values(), x, y);
   }
+  // the FP64 operator: the original matrix of a refined handle, the input
+  // values of a plain FP64 factor
+  const Hi* op_values() const { return (const Hi*)(F.aval_hi ? F.aval_hi : F.aval); }
   // per-column inf norms of up to 3 vectors -> host
   void colmax(const Hi* v, int k, double* out) {
     CK(cudaMemsetAsync(nb, 0, k * sizeof(unsigned long long), st));
@@ -1488,6 +1494,52 @@ static void refined_solve_impl(rslab_fac_handle& F, const void* bsrc, int nrhs, 
   CK(cudaStreamSynchronize(st));
   wave_check(F);
 }
+
+namespace {
+
+template <typename Hi>
+static void gmres_block_entry(rslab_fac_handle& F, const void* b, int s, double tol, int max_iter, int restart,
+                              const void* x0, void* x, bool on_device, int64_t* iters, double* final_res,
+                              int* converged) {
+  MixedCtx<Hi> M(F, std::min(s, BG_SMAX));
+  const long long n = M.n;
+  const size_t bytes = (size_t)n * s * sizeof(Hi);
+  const cudaMemcpyKind kin = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  Hi* bd = (Hi*)F.arena.get(A_BG_IB, bytes);
+  Hi* xd = (Hi*)F.arena.get(A_BG_IX, bytes);
+  CK(cudaMemcpyAsync(bd, b, bytes, kin, M.st));
+  if (x0)
+    CK(cudaMemcpyAsync(xd, x0, bytes, kin, M.st));
+  else
+    CK(cudaMemsetAsync(xd, 0, bytes, M.st));
+  const int gk = std::min(s, BG_SMAX);
+  Hi* bk = (Hi*)F.arena.get(A_BG_B, (size_t)n * gk * sizeof(Hi));
+  Hi* xk = (Hi*)F.arena.get(A_BG_X, (size_t)n * gk * sizeof(Hi));
+  int* dcl = (int*)F.arena.get(A_BG_CL, BG_SMAX * sizeof(int));
+  int64_t it = 0;
+  bool conv = true;
+  for (int g0 = 0; g0 < s; g0 += BG_SMAX) {
+    const int k = std::min(BG_SMAX, s - g0);
+    std::vector<int> cols(k);
+    for (int a = 0; a < k; ++a) cols[a] = g0 + a;
+    CK(cudaMemcpyAsync(dcl, cols.data(), k * sizeof(int), cudaMemcpyHostToDevice, M.st));
+    k_bg_gather<Hi><<<grid1(n * k), 256, 0, M.st>>>(n, s, k, dcl, bd, bk);
+    k_bg_gather<Hi><<<grid1(n * k), 256, 0, M.st>>>(n, s, k, dcl, xd, xk);
+    const BlockGmresResult r = gmres_block<Hi>(M, bk, xk, k, tol, max_iter, restart);
+    k_bg_scatter<Hi><<<grid1(n * k), 256, 0, M.st>>>(n, s, k, dcl, xk, xd);
+    it = std::max<int64_t>(it, r.iters);
+    conv = conv && r.converged;
+    if (final_res)
+      for (int a = 0; a < k; ++a) final_res[g0 + a] = r.final_res[a];
+  }
+  CK(cudaMemcpyAsync(x, xd, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, M.st));
+  CK(cudaStreamSynchronize(M.st));
+  wave_check(F);
+  if (iters) *iters = it;
+  if (converged) *converged = conv ? 1 : 0;
+}
+
+}  // namespace
 
 namespace rslab {
 // Sets the calling thread's last-error message (for entry points defined in
@@ -1887,6 +1939,32 @@ int rslab_mixed_solve(rslab_fac_handle* F, const void* b, int64_t nrhs, double t
       rc = mixed_solve_impl<c64>(*F, b, (int)nrhs, target, x, on_device != 0, info);
     F->solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return rc;
+  } catch (const RslabError& e) {
+    return fail(e);
+  } catch (const std::exception& e) {
+    return fail(RslabError(Status::InvalidInput, e.what()));
+  }
+}
+
+int rslab_gmres_block(rslab_fac_handle* F, const void* b, int64_t s, double tol, int64_t max_iter, int64_t restart,
+                      const void* x0, void* x, int on_device, int64_t* iters, double* final_res, int* converged) {
+  try {
+    if (!F || !b || !x) throw RslabError(Status::InvalidInput, "null handle or vector");
+    if (s <= 0) throw RslabError(Status::DimensionMismatch, "s must be positive");
+    if (!(tol > 0.0) || max_iter < 0 || restart < 1)
+      throw RslabError(Status::InvalidInput, "tol > 0, max_iter >= 0 and restart >= 1 required");
+    if (F->last_status) throw RslabError(Status::NumericallyRankDeficient, "factor is not valid");
+    const int op = F->dtype_hi >= 0 ? F->dtype_hi : F->dtype;
+    if (op == RSLAB_F64)
+      gmres_block_entry<double>(*F, b, (int)s, tol, (int)max_iter, (int)restart, x0, x, on_device != 0, iters,
+                                final_res, converged);
+    else if (op == RSLAB_C64)
+      gmres_block_entry<c64>(*F, b, (int)s, tol, (int)max_iter, (int)restart, x0, x, on_device != 0, iters,
+                             final_res, converged);
+    else
+      throw RslabError(Status::InvalidInput,
+                       "block GMRES needs an FP64 operator: a refined handle or an f64 / c64 factor");
+    return 0;
   } catch (const RslabError& e) {
     return fail(e);
   } catch (const std::exception& e) {
