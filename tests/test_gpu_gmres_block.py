@@ -53,7 +53,8 @@ def test_matches_the_oracle_with_the_same_preconditioner():
     full = _full(a)
 
     def pre(rr):
-        return lo.solve_many(np.ascontiguousarray(rr).astype(np.complex64), rr.shape[1]).astype(np.complex128)
+        z = lo.solve_many(np.ascontiguousarray(rr).astype(np.complex64), rr.shape[1])
+        return np.asarray(z).reshape(rr.shape).astype(np.complex128)
 
     xo, ito, convo, fro = oracle_gmres_block(lambda v: full @ v, pre, b, 1e-13, 120, 8)
     assert convo and r.converged
