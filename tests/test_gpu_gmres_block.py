@@ -93,9 +93,9 @@ def test_f32_factor_is_rejected_as_operator():
         gmres_block(f32, np.ones(a.n, np.float32), 1e-10)
 
 
-def test_ladder_block_gmres_certifies_a_hard_matrix():
+def test_ladder_gmres_ir_certifies_a_hard_matrix():
     """A random sparse symmetric matrix from the tier corpus on which plain
-    IR stagnates with the c32 factor: the ladder's block GMRES-IR stage runs
+    IR stagnates with the c32 factor: the ladder's GMRES-IR stage runs
     (gmres_iters > 0) and certifies every column."""
     fam, a = list(matgen.c5_corpus(202, 5))[201]
     assert fam == "random_sparse"
