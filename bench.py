@@ -5,8 +5,10 @@ A = -Delta_h - k^2 (1 + 0.05 i) I on a side^3 grid (default 64^3, n = 262,144),
 k^2 = 0.2 lambda_max, 16 right-hand sides with U[-1, 1) real and imaginary
 parts (seed 1).  Analysis (ordering + symbolic) is done once, outside the
 timed region, as in the reference's methodology.
-  * headline (`value`): the mixed-precision path — c32 numeric factor on the
-    GPU + FP64 refinement against the original A (IR -> GMRES-IR) until every
+  * headline (`value`): the mixed-precision path — the numeric factor in the
+    precision tier the tier network picks from the matrix's features (c32 with
+    tensor-core updates on this matrix) + FP64 refinement against the
+    original A (IR -> GMRES-IR) until every
     right-hand side's normwise backward error is <= 1e-14; GFLOP/s counts the
     model flops of the FP64-equivalent factor (sum_s sum_m (m^2 - 1), x4 for
     complex) per step time;
@@ -566,7 +568,13 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     st = SolverSettings()
-    mixed = MixedLdltSolver.factor_with(a, st, sym=sym)
+    # The tier network picks the factor's precision tier from the matrix's
+    # features, outside the timed region like the analysis.
+    from rslab_b200.tiers import TIERS, TierModel, tier_features
+    tier_feats = tier_features(a, sym)
+    tier_probs = TierModel.load().predict_proba(tier_feats)[0]
+    tier = int(np.argmax(tier_probs))
+    mixed = MixedLdltSolver.factor_tier(a, tier, st, sym=sym)
     stream = torch.cuda.ExternalStream(mixed.stream())
     import ctypes as C
 
@@ -707,11 +715,14 @@ def main():
             "metric": "LDLT factor+solve GFLOP/s at bwd err <= 1e-14 (mixed/batched vs FP64 GPU)",
             "value": gflops, "unit": "GFLOP/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "c32 factor / f64 refinement", "data": "synthetic",
+            "dtype": f"{TIERS[tier]} factor / f64 refinement", "data": "synthetic",
             "config": {"workload": f"helmholtz3d_{args.side}^3_c64_nrhs{nrhs}", "n": n, "nnz_lower": a.nnz,
                        "nrhs": nrhs, "ordering": "AMD", "target_backward_error": args.target,
                        "model_flops": flops, "factor_nnz_panels": info.panel_elems,
                        "parallelism": f"replicas{ws}", "l2": "flushed between steps (256 MB write)"},
+            "tier": {"chosen": TIERS[tier], "probabilities": [float(p) for p in tier_probs],
+                     "features": [float(f) for f in tier_feats],
+                     "note": "picked by the tier network (rslab_tier_mlp_forward) before the timed region"},
             "mixed": {"certified": bool(minfo.certified), "backward_error": minfo.backward_error,
                       "ir_iters": minfo.ir_iters, "gmres_iters": minfo.gmres_iters,
                       "last_factor_ms": fi.factor_ms},
