@@ -274,7 +274,8 @@ def run_sweep(args, ws, rank, local):
     dev = torch.device("cuda", local)
     c4 = matgen.C4System(args.sweep_side, 3)
     om_all = c4.omegas(args.sweep_count)
-    mine = list(range(rank, len(om_all), ws))
+    from rslab_b200.sweep import shard_frequencies
+    mine = shard_frequencies(len(om_all), rank, ws)
     nrhs = 8
     b = matgen.uniform_rhs(c4.n, nrhs, 4, complex_=True)
     st = sweep_settings()

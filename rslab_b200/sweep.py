@@ -38,3 +38,21 @@ def frequency_sweep(matrices, b: np.ndarray, target: float = 1e-14,
             solver.refactor(a)
         x, info = solver.solve_to(a, b, target)
         yield i, x, info
+
+
+def shard_frequencies(count: int, rank: int, world_size: int) -> list:
+    """The frequency indices one rank sweeps: index i goes to rank
+    i mod world_size.  Every frequency costs the same (one pattern, one
+    factor graph), so round-robin balances to within one frequency; the
+    ranks need no exchange until the per-frequency certificates are gathered
+    (`gather_certificates`)."""
+    if world_size <= 0 or not 0 <= rank < world_size:
+        raise ValueError("need 0 <= rank < world_size")
+    return list(range(rank, count, world_size))
+
+
+def gather_certificates(local: dict, world_size: int) -> list:
+    """Every rank's per-frequency records (a host-side all-gather of small
+    dicts, the only communication of a sharded sweep)."""
+    from .batch import gather_stats
+    return gather_stats(local, world_size)
