@@ -179,6 +179,23 @@ def cpu_sample(args):
                       f"{flops:.3g}), mean of 2 warm runs; backward error {be:.2e}"}
 
 
+def host_backward_error(a, x, b) -> float:
+    """Normwise backward error max|b - A x| / (||A||_inf max|x| + max|b|) over
+    all columns, A the symmetric matrix of the stored lower triangle (the
+    certificate of MixedInfo, recomputed on the host)."""
+    import scipy.sparse as sp
+    n = a.n
+    cp = np.asarray(a.col_ptr)
+    col = np.repeat(np.arange(n), np.diff(cp))
+    low = sp.csr_matrix((np.asarray(a.values), (np.asarray(a.row_idx), col)), shape=(n, n))
+    full = low + low.T - sp.diags(low.diagonal())
+    x2 = x.reshape(n, -1)
+    b2 = np.asarray(b).reshape(n, -1)
+    r = b2 - full @ x2
+    anorm = float(np.abs(full).sum(axis=1).max())
+    return float(np.max(np.abs(r).max(axis=0) / (anorm * np.abs(x2).max(axis=0) + np.abs(b2).max(axis=0))))
+
+
 def cmod_tc_bytes_per_flop():
     """DRAM bytes per algorithmic flop of k_cmod_tc from the committed ncu
     summary (line 'dram_bytes_per_flop: X'), or None."""
@@ -344,9 +361,8 @@ def run_sweep(args, ws, rank, local):
 
         ms64, _ = timed(fp64_some, s64, 1, 1)
         ms64 = allmax(ms64 / len(pick), ws)
-        from oracle.oracle import backward_error
         for i in pick[-1:]:
-            res.append(backward_error(mats[i], x_d.cpu().numpy(), b))
+            res.append(host_backward_error(mats[i], x_d.cpu().numpy(), b))
         out_fp64 = {"ms_per_frequency": ms64, "frequencies_timed": int(len(pick)),
                     "ms_per_sweep_projected": ms64 * len(om_all) / ws,
                     "gflops": flops / (ms64 * 1e-3) / 1e9,
@@ -624,6 +640,7 @@ def main():
     ms_mixed, minfo = timed(mixed_step, args.steps, args.warmup)
     clocks = clk.stop()
     ms_mixed = allmax(ms_mixed, ws)
+    x_mixed = x_d.cpu().numpy()  # the last timed step's solution
 
     out_fp64 = None
     if not args.no_fp64:
@@ -643,12 +660,12 @@ def main():
         stream = stream_save
         ms64 = allmax(ms64, ws)
         x64 = x_d.cpu().numpy()
-        from oracle.oracle import backward_error
-        be64 = backward_error(a, x64, b)
+        be64 = host_backward_error(a, x64, b)
         fi = N.FactorInfo()
         N.lib.rslab_factor_info(f64._h, C.byref(fi))
         out_fp64 = {"ms_per_step": ms64, "factor_ms": fi.factor_ms, "solve_ms": fi.solve_ms,
-                    "gflops": flops / (ms64 * 1e-3) / 1e9, "backward_error_no_ir": be64}
+                    "gflops": flops / (ms64 * 1e-3) / 1e9, "backward_error_no_ir": be64,
+                    "mixed_forward_error_vs_fp64": float(np.abs(x_mixed - x64).max() / np.abs(x64).max())}
 
     # Per-kernel-class profile of one eager refactor (events after every launch).
     from rslab_b200.solver import factor_profile, solve_profile
