@@ -2,7 +2,7 @@
 
 `gmres_block(solver, b, tol, max_iter, restart, x0)` mirrors the reference's
 `gmres_block(op, b, s, precond, tol, max_iter, restart, x0)`
-(src/numeric/iterative.rs:1881) for the case the survey names: the operator
+(src/numeric/iterative.rs:1881) for a factored solver used as preconditioner: the operator
 is the handle's FP64 matrix and the preconditioner its factor
 (`impl Preconditioner for LdltSolver`, iterative.rs:178-190).  The iteration
 runs on the GPU (rslab_gmres_block); `b` is an n x s array (a 1-D b is one

@@ -1,7 +1,7 @@
 """Learned precision tier: a small network picks, per matrix, the precision
 the refined factor is computed in (FP64 / FP32 / TF32x3), trained on labels
 the solver makes itself by running every tier and keeping the cheapest one
-that certifies; the FP64 tier is the fallback and the judge (a matrix whose
+that certifies; the FP64 tier is the fallback and the arbiter (a matrix whose
 chosen tier does not certify is refactored in FP64).
 
 Tiers (include/rslab_b200.h RSLAB_TIER_*), all refined in FP64 against the
