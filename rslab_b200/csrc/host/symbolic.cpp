@@ -417,6 +417,9 @@ Symbolic analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, cons
     case Ordering::Amd:
       ord = amd_order(full, &S.amd);
       break;
+    case Ordering::MetisND:
+      ord = metis_nd_order(full);
+      break;
     case Ordering::Natural:
       std::iota(ord.begin(), ord.end(), 0);
       break;

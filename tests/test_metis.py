@@ -1,0 +1,56 @@
+"""MetisND ordering (host, no GPU): valid and deterministic permutations,
+AMD on graphs at or below the leaf size, contiguous components, and the fill
+reduction nested dissection gives on 3D grids.  The reference's own crate
+cannot be run here, so the permutation itself is not pinned to it."""
+import numpy as np
+import pytest
+
+from rslab_b200 import LdltSymbolic, Ordering, SolverSettings, matgen
+from rslab_b200.solver import CscMatrix
+
+
+def _sym(a, o):
+    return LdltSymbolic.analyze_with(a, SolverSettings().with_ordering(o))
+
+
+def _perm(a, o):
+    p = np.asarray(_sym(a, o).export()["perm"])
+    assert sorted(p.tolist()) == list(range(a.n))
+    return p
+
+
+@pytest.mark.parametrize("make", [lambda: matgen.c1_matrix(40), lambda: matgen.c2_matrix(14),
+                                  lambda: matgen.random_sparse_symmetric(900, matgen.Rng(3), 1.0),
+                                  lambda: matgen.C4System(9).matrix(1.0)])
+def test_valid_and_deterministic(make):
+    a = make()
+    assert np.array_equal(_perm(a, Ordering.METIS_ND), _perm(a, Ordering.METIS_ND))
+
+
+def test_small_graph_is_one_amd_leaf():
+    a = matgen.c3_matrix(5)  # n = 125 <= 200: the whole graph goes to AMD
+    assert np.array_equal(_perm(a, Ordering.METIS_ND), _perm(a, Ordering.AMD))
+    ia, ib = _sym(a, Ordering.METIS_ND).info(), _sym(a, Ordering.AMD).info()
+    assert ia.factor_nnz_sym == ib.factor_nnz_sym and ia.nsuper == ib.nsuper
+
+
+def test_nested_dissection_cuts_3d_fill():
+    a = matgen.c3_matrix(32)
+    nd, amd = _sym(a, Ordering.METIS_ND).info(), _sym(a, Ordering.AMD).info()
+    assert nd.flops_model < 0.75 * amd.flops_model
+    assert nd.factor_nnz_sym < 0.9 * amd.factor_nnz_sym
+
+
+def test_disconnected_components():
+    """Two disjoint grids: the dissection splits components first, the
+    permutation stays valid and the elimination forest has a tree per grid."""
+    g1 = matgen.c3_matrix(12)
+    g2 = matgen.c1_matrix(30)
+    n1 = g1.n
+    r1, c1 = np.asarray(g1.row_idx), np.repeat(np.arange(n1), np.diff(np.asarray(g1.col_ptr)))
+    r2, c2 = np.asarray(g2.row_idx), np.repeat(np.arange(g2.n), np.diff(np.asarray(g2.col_ptr)))
+    a = CscMatrix.from_triplets(n1 + g2.n, np.concatenate([r1, r2 + n1]), np.concatenate([c1, c2 + n1]),
+                                np.concatenate([np.asarray(g1.values), np.asarray(g2.values)]))
+    _perm(a, Ordering.METIS_ND)
+    parent = np.asarray(_sym(a, Ordering.METIS_ND).export()["parent"])
+    assert int(np.sum(parent < 0)) >= 2
