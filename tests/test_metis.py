@@ -54,3 +54,17 @@ def test_disconnected_components():
     _perm(a, Ordering.METIS_ND)
     parent = np.asarray(_sym(a, Ordering.METIS_ND).export()["parent"])
     assert int(np.sum(parent < 0)) >= 2
+
+
+@pytest.mark.parametrize("side,nnz_m,digits", [(24, 1.53, 2), (40, 14.00, 2), (56, 63.8, 1)])
+def test_fill_matches_the_reference_crates_recorded_fill(side, nnz_m, digits):
+    """The reference recorded the exact scalar nnz(L) (diagonal included,
+    elimination-tree column counts, no supernode padding) of its crate's
+    default MetisND on 7-point grids: 24^3 1.53 M, 40^3 14.00 M, 56^3 63.8 M,
+    and the 40^3 flop proxy sum(cc^2) 1.53e10
+    (dev/research/metis-node-separator-2026-07.md:3-4, 72-74)."""
+    a = matgen.c3_matrix(side)
+    cc = np.asarray(_sym(a, Ordering.METIS_ND).export()["col_counts"], np.float64)
+    assert round(cc.sum() / 1e6, digits) == nnz_m
+    if side == 40:
+        assert round((cc ** 2).sum() / 1e10, 2) == 1.53
