@@ -56,6 +56,8 @@ def parse():
                    help="helmholtz: the 64^3 Helmholtz factor+solve step (default); sweep: the "
                         "same-pattern frequency sweep, 48^3 27-point K - w^2 M + i w C, 64 frequencies; "
                         "tiers: the learned precision tier on the held-out 80^3 27-point complex Helmholtz")
+    p.add_argument("--ordering", default="amd", choices=["amd", "metis"],
+                   help="fill-reducing ordering of the helmholtz workload (metis: the MetisND restatement)")
     p.add_argument("--tiers-side", type=int, default=80)
     p.add_argument("--tier-model", default=None, help="tier network .npz (default: the package's trained one)")
     p.add_argument("--sweep-side", type=int, default=48)
@@ -575,7 +577,11 @@ def main():
 
     a = matgen.c2_matrix(args.side)
     n, nrhs = a.n, args.nrhs
-    sym = LdltSymbolic.analyze(a)
+    if args.ordering == "metis":
+        from rslab_b200 import Ordering
+        sym = LdltSymbolic.analyze_with(a, SolverSettings().with_ordering(Ordering.METIS_ND))
+    else:
+        sym = LdltSymbolic.analyze(a)
     info = sym.info()
     flops = 4.0 * info.flops_model  # complex: 4 real flops per complex multiply-add pair
     b = matgen.uniform_rhs(n, nrhs, 1, complex_=True)
@@ -735,7 +741,8 @@ def main():
             "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": f"{TIERS[tier]} factor / f64 refinement", "data": "synthetic",
             "config": {"workload": f"helmholtz3d_{args.side}^3_c64_nrhs{nrhs}", "n": n, "nnz_lower": a.nnz,
-                       "nrhs": nrhs, "ordering": "AMD", "target_backward_error": args.target,
+                       "nrhs": nrhs, "ordering": "MetisND" if args.ordering == "metis" else "AMD",
+                       "target_backward_error": args.target,
                        "model_flops": flops, "factor_nnz_panels": info.panel_elems,
                        "parallelism": f"replicas{ws}", "l2": "flushed between steps (256 MB write)"},
             "tier": {"chosen": TIERS[tier], "probabilities": [float(p) for p in tier_probs],
