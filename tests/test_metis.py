@@ -68,3 +68,20 @@ def test_fill_matches_the_reference_crates_recorded_fill(side, nnz_m, digits):
     assert round(cc.sum() / 1e6, digits) == nnz_m
     if side == 40:
         assert round((cc ** 2).sum() / 1e10, 2) == 1.53
+
+
+def test_oracle_factor_on_the_dissection_structure():
+    """The CPU oracle factors and solves on the MetisND structure: same
+    solution as a direct sparse solve, inertia of the shifted Laplacian."""
+    import scipy.sparse.linalg as spla
+
+    from oracle.oracle import OracleSolver
+    a = matgen.c3_matrix(14)
+    sym = _sym(a, Ordering.METIS_ND)
+    o = OracleSolver(a, sym.export())
+    b = matgen.uniform_rhs(a.n, 2, 5)
+    x = o.solve_many(b, 2)
+    xr = spla.spsolve(a.to_scipy_full().tocsc(), b)
+    assert np.abs(x - xr).max() <= 1e-10 * np.abs(xr).max()
+    neg = matgen.negative_eigs_shifted_laplacian((14, 14, 14), 0.1 * matgen.lambda_max((14, 14, 14)))
+    assert o.factors().inertia == (a.n - neg, neg, 0)
