@@ -53,8 +53,8 @@ extern "C" {
 #define RSLAB_C32 3
 
 /* Orderings (OrderingMethod, src/symbolic/mod.rs:28). */
-#define RSLAB_ORDER_AMD 0
-#define RSLAB_ORDER_METIS_ND 1
+#define RSLAB_ORDER_AMD 0      /* rslab_amd::amd_order (crates/rslab-amd/src/lib.rs:66) */
+#define RSLAB_ORDER_METIS_ND 1 /* rslab_metis::metis_order (crates/rslab-metis/src/lib.rs:184) */
 #define RSLAB_ORDER_NATURAL 2
 #define RSLAB_ORDER_GIVEN 3
 
