@@ -25,6 +25,7 @@
  *   rslab_export_factors LdltFactors (src/dense/ldlt_generic.rs:31-66), the
  *                        factor_numeric return value
  *   rslab_amd_order      rslab_amd::amd_order (crates/rslab-amd/src/lib.rs:66)
+ *   rslab_metis_order    rslab_metis::metis_order_full (crates/rslab-metis/src/lib.rs:204)
  */
 #ifndef RSLAB_B200_H
 #define RSLAB_B200_H
@@ -286,6 +287,11 @@ uint64_t rslab_rng_units(uint64_t state, int64_t m, double* out);
 /* AMD on a full symmetric pattern; stats7 = ncmpa, ndense, ndiv, nms_ldl,
  * nms_lu, mass eliminations, supervariable merges. */
 int rslab_amd_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, int64_t* perm, double* stats7);
+
+/* MetisND on a full symmetric pattern with the given seed and otherwise
+ * default options: rslab_metis::metis_order_full (crates/rslab-metis/src/
+ * lib.rs:204; seed 1 = metis_order, :184).  perm = new-to-old. */
+int rslab_metis_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, uint64_t seed, int64_t* perm);
 
 /* Allocation-free dense panel factor.  No counterpart in the reference: an
  * addition for callers that cannot allocate device memory at factor time

@@ -48,9 +48,10 @@ struct AmdStats {
 };
 std::vector<int64_t> amd_order(const CscPattern& pat, AmdStats* stats = nullptr,
                                double dense_alpha = 10.0, bool aggressive = true);
-// Multilevel nested dissection with AMD leaves, default options
-// (crates/rslab-metis/src/lib.rs:184 metis_order); new-to-old permutation.
-std::vector<int64_t> metis_nd_order(const CscPattern& pat);
+// Multilevel nested dissection with AMD leaves, default options except the
+// seed (crates/rslab-metis/src/lib.rs:184 metis_order, :204 metis_order_full);
+// new-to-old permutation.
+std::vector<int64_t> metis_nd_order(const CscPattern& pat, uint64_t seed = 1);
 
 // Elimination tree: parent[j] > j or -1 (src/ordering/elimination_tree.rs:28-64).
 std::vector<int64_t> etree_from_pattern(const CscPattern& pat);

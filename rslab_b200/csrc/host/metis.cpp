@@ -846,8 +846,9 @@ void push_components(std::vector<Work>& work, const Graph& g, const std::vector<
 
 }  // namespace
 
-std::vector<int64_t> metis_nd_order(const CscPattern& full) {
-  const Opts o;
+std::vector<int64_t> metis_nd_order(const CscPattern& full, uint64_t seed) {
+  Opts o;
+  o.seed = seed;
   const Graph g = graph_of(full);
   const int n = g.n;
   std::vector<int64_t> iperm(n, -1);

@@ -665,6 +665,15 @@ def amd_order(n: int, col_ptr, row_idx) -> tuple:
     return perm, {k: st[i] for i, k in enumerate(keys)}
 
 
+def metis_order(n: int, col_ptr, row_idx, seed: int = 1) -> np.ndarray:
+    """MetisND on a full symmetric pattern (new-to-old permutation)."""
+    cp = _i64(col_ptr)
+    ri = _i64(row_idx)
+    perm = np.zeros(n, np.int64)
+    _check(N.lib.rslab_metis_order(n, _p64(cp), _p64(ri), C.c_uint64(seed), _p64(perm)))
+    return perm
+
+
 def device_count() -> int:
     c = C.c_int(0)
     N.lib.rslab_device_count(C.byref(c))

@@ -85,3 +85,25 @@ def test_oracle_factor_on_the_dissection_structure():
     assert np.abs(x - xr).max() <= 1e-10 * np.abs(xr).max()
     neg = matgen.negative_eigs_shifted_laplacian((14, 14, 14), 0.1 * matgen.lambda_max((14, 14, 14)))
     assert o.factors().inertia == (a.n - neg, neg, 0)
+
+
+def test_seeded_fill_on_40_cubed_grid():
+    """Other seeds of the same crate, 40^3 grid: the reference recorded 14.3,
+    14.5 and 14.9 M for seeds 2-4 (dev/research/metis-node-separator-2026-07.md:72).
+    Ours: 14.25, 14.45 and 14.96 M.  Seeds 2 and 3 match the note's one
+    decimal; seed 4 reads 0.06 M above it, which is checked here as a bound
+    rather than claimed as a match."""
+    from rslab_b200.solver import metis_order
+    a = matgen.c3_matrix(40)
+    full = a.to_scipy_full().tocsc()
+    full.sort_indices()
+    got = {}
+    for seed in (1, 2, 3, 4):
+        perm = metis_order(a.n, full.indptr, full.indices, seed)
+        assert sorted(perm.tolist()) == list(range(a.n))
+        st = SolverSettings().with_ordering(Ordering.GIVEN)
+        st.given_perm = perm
+        got[seed] = np.asarray(LdltSymbolic.analyze_with(a, st).export()["col_counts"]).sum() / 1e6
+    assert round(got[1], 2) == 14.00
+    assert round(got[2], 1) == 14.3 and round(got[3], 1) == 14.5
+    assert abs(got[4] - 14.9) < 0.1
