@@ -107,3 +107,28 @@ def test_seeded_fill_on_40_cubed_grid():
     assert round(got[1], 2) == 14.00
     assert round(got[2], 1) == 14.3 and round(got[3], 1) == 14.5
     assert abs(got[4] - 14.9) < 0.1
+
+
+@pytest.mark.parametrize("shape", ["empty", "one", "diag", "star", "path", "dense", "random", "two_blocks"])
+def test_degenerate_graphs_give_permutations(shape):
+    import scipy.sparse as sp
+
+    from rslab_b200.solver import metis_order
+    n = 3000
+    if shape == "empty":
+        assert metis_order(0, np.zeros(1, np.int64), np.zeros(0, np.int64)).shape == (0,)
+        return
+    if shape == "one":
+        assert metis_order(1, np.array([0, 1]), np.array([0])).tolist() == [0]
+        return
+    r = np.arange(1, n)
+    a = {"diag": sp.csr_matrix((n, n)),
+         "star": sp.csr_matrix((np.ones(n - 1), (r, np.zeros(n - 1))), shape=(n, n)),
+         "path": sp.diags([np.ones(n - 1)], [-1]),
+         "dense": sp.csr_matrix(np.tril(np.ones((400, 400)), -1)),
+         "random": sp.random(n, n, density=5 / n, random_state=1),
+         "two_blocks": sp.block_diag([sp.diags([np.ones(1999)], [-1]), np.tril(np.ones((300, 300)), -1)])}[shape]
+    a = (a + a.T + sp.eye(a.shape[0])).tocsc()
+    a.sort_indices()
+    p = metis_order(a.shape[0], a.indptr, a.indices)
+    assert sorted(p.tolist()) == list(range(a.shape[0]))
