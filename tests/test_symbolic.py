@@ -103,3 +103,13 @@ def test_given_and_natural_orderings():
     perm = np.random.default_rng(0).permutation(40)
     giv = LdltSymbolic.analyze_with(a, SolverSettings(ordering=3, given_perm=perm)).export()
     assert sorted(giv["perm"]) == list(range(40))
+
+
+@pytest.mark.parametrize("make", [lambda: random_sym(400, 0.008, 4), lambda: matgen.c3_matrix(8)])
+def test_column_counts_exact_under_nested_dissection(make):
+    """The same exactness on MetisND structures (graphs above the AMD leaf
+    size, so the dissection and its separators are exercised)."""
+    a = make()
+    ex = LdltSymbolic.analyze_with(a, SolverSettings(ordering=1)).export()
+    L = brute_force_l_pattern(a, ex["perm"])
+    assert np.array_equal(L.sum(axis=0), ex["col_counts"])
