@@ -288,10 +288,14 @@ uint64_t rslab_rng_units(uint64_t state, int64_t m, double* out);
  * nms_lu, mass eliminations, supervariable merges. */
 int rslab_amd_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, int64_t* perm, double* stats7);
 
-/* MetisND on a full symmetric pattern with the given seed and otherwise
- * default options: rslab_metis::metis_order_full (crates/rslab-metis/src/
- * lib.rs:204; seed 1 = metis_order, :184).  perm = new-to-old. */
-int rslab_metis_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, uint64_t seed, int64_t* perm);
+/* MetisND on a full symmetric pattern: rslab_metis::metis_order_full
+ * (crates/rslab-metis/src/lib.rs:204) with the given seed, the opt-in
+ * quasi-dense column quotient (dense_quotient != 0; columns of off-diagonal
+ * degree above dense_threshold, or max(40, ceil(10 sqrt(n))) when it is < 0,
+ * are ordered last, densest first) and otherwise default options; seed 1
+ * without the quotient = metis_order (:184).  perm = new-to-old. */
+int rslab_metis_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, uint64_t seed, int dense_quotient,
+                      int64_t dense_threshold, int64_t* perm);
 
 /* Allocation-free dense panel factor.  No counterpart in the reference: an
  * addition for callers that cannot allocate device memory at factor time

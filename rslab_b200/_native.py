@@ -118,7 +118,7 @@ SIGNATURES = {
     "rslab_tier_mlp_train": (C.c_int, [fp, fp, i32p, fp, C.c_int64, C.c_int64, C.c_float, fp, C.c_int]),
     "rslab_rng_units": (C.c_uint64, [C.c_uint64, C.c_int64, C.POINTER(C.c_double)]),
     "rslab_amd_order": (C.c_int, [C.c_int64, i64p, i64p, i64p, C.POINTER(C.c_double)]),
-    "rslab_metis_order": (C.c_int, [C.c_int64, i64p, i64p, C.c_uint64, i64p]),
+    "rslab_metis_order": (C.c_int, [C.c_int64, i64p, i64p, C.c_uint64, C.c_int, C.c_int64, i64p]),
     "rslab_panel_factor_noalloc": (C.c_int, [C.c_int, vp, C.c_int64, C.c_int64, C.c_int64, vp, vp, vp, vp, vp,
                                              vp]),
 }

@@ -2254,14 +2254,15 @@ int rslab_amd_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, i
   }
 }
 
-int rslab_metis_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, uint64_t seed, int64_t* perm) {
+int rslab_metis_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, uint64_t seed, int dense_quotient,
+                      int64_t dense_threshold, int64_t* perm) {
   try {
     if (n < 0 || (n > 0 && (!col_ptr || !row_idx || !perm))) throw RslabError(Status::InvalidInput, "null pattern");
     rslab::CscPattern p;
     p.n = n;
     p.col_ptr.assign(col_ptr, col_ptr + n + 1);
     p.row_idx.assign(row_idx, row_idx + col_ptr[n]);
-    std::vector<int64_t> pr = rslab::metis_nd_order(p, seed);
+    std::vector<int64_t> pr = rslab::metis_nd_order(p, seed, dense_quotient != 0, dense_threshold);
     std::copy(pr.begin(), pr.end(), perm);
     return 0;
   } catch (const RslabError& e) {

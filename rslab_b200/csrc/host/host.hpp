@@ -51,7 +51,10 @@ std::vector<int64_t> amd_order(const CscPattern& pat, AmdStats* stats = nullptr,
 // Multilevel nested dissection with AMD leaves, default options except the
 // seed (crates/rslab-metis/src/lib.rs:184 metis_order, :204 metis_order_full);
 // new-to-old permutation.
-std::vector<int64_t> metis_nd_order(const CscPattern& pat, uint64_t seed = 1);
+// dense_quotient: the opt-in quasi-dense column quotient (off in the
+// reference's defaults), dense_threshold < 0 = max(40, ceil(10 sqrt(n))).
+std::vector<int64_t> metis_nd_order(const CscPattern& pat, uint64_t seed = 1, bool dense_quotient = false,
+                                    int64_t dense_threshold = -1);
 
 // Elimination tree: parent[j] > j or -1 (src/ordering/elimination_tree.rs:28-64).
 std::vector<int64_t> etree_from_pattern(const CscPattern& pat);

@@ -844,11 +844,7 @@ void push_components(std::vector<Work>& work, const Graph& g, const std::vector<
   }
 }
 
-}  // namespace
-
-std::vector<int64_t> metis_nd_order(const CscPattern& full, uint64_t seed) {
-  Opts o;
-  o.seed = seed;
+std::vector<int64_t> nd_order(const CscPattern& full, const Opts& o) {
   const Graph g = graph_of(full);
   const int n = g.n;
   std::vector<int64_t> iperm(n, -1);
@@ -898,6 +894,58 @@ std::vector<int64_t> metis_nd_order(const CscPattern& full, uint64_t seed) {
     if (p < 0 || p >= n || perm[p] >= 0) throw RslabError(Status::InvalidInput, "nested dissection: invalid order");
     perm[p] = v;
   }
+  return perm;
+}
+
+}  // namespace
+
+std::vector<int64_t> metis_nd_order(const CscPattern& full, uint64_t seed, bool dense_quotient,
+                                    int64_t dense_threshold) {
+  Opts o;
+  o.seed = seed;
+  const int64_t n = full.n;
+  if (!dense_quotient || n == 0) return nd_order(full, o);
+  // Opt-in quasi-dense column quotient (lib.rs:282-404): columns of
+  // off-diagonal degree above max(40, ceil(10 sqrt(n))) (or the given
+  // threshold) leave the graph and are appended last, densest first.
+  const int64_t thresh =
+      dense_threshold >= 0 ? dense_threshold : std::max<int64_t>(40, (int64_t)std::ceil(10.0 * std::sqrt((double)n)));
+  std::vector<int64_t> deg(n, 0), dense;
+  for (int64_t c = 0; c < n; ++c) {
+    for (int64_t k = full.col_ptr[c]; k < full.col_ptr[c + 1]; ++k) deg[c] += full.row_idx[k] != c;
+    if (deg[c] > thresh) dense.push_back(c);
+  }
+  if (dense.empty()) return nd_order(full, o);
+  std::sort(dense.begin(), dense.end(), [&](int64_t a, int64_t b) { return deg[a] != deg[b] ? deg[a] > deg[b] : a < b; });
+  std::vector<char> is_dense(n, 0);
+  for (int64_t c : dense) is_dense[c] = 1;
+  std::vector<int64_t> to_orig, local(n, -1);
+  for (int64_t c = 0; c < n; ++c)
+    if (!is_dense[c]) {
+      local[c] = (int64_t)to_orig.size();
+      to_orig.push_back(c);
+    }
+  CscPattern sub;
+  sub.n = (int64_t)to_orig.size();
+  sub.col_ptr.assign(1, 0);
+  for (int64_t c : to_orig) {
+    bool diag = false;
+    for (int64_t k = full.col_ptr[c]; k < full.col_ptr[c + 1]; ++k) {
+      const int64_t r = full.row_idx[k];
+      if (r == c || local[r] < 0) continue;
+      if (!diag && local[r] > local[c]) {
+        sub.row_idx.push_back(local[c]);
+        diag = true;
+      }
+      sub.row_idx.push_back(local[r]);
+    }
+    if (!diag) sub.row_idx.push_back(local[c]);
+    sub.col_ptr.push_back((int64_t)sub.row_idx.size());
+  }
+  std::vector<int64_t> perm;
+  perm.reserve(n);
+  for (int64_t l : nd_order(sub, o)) perm.push_back(to_orig[l]);
+  perm.insert(perm.end(), dense.begin(), dense.end());
   return perm;
 }
 

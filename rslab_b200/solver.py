@@ -665,12 +665,16 @@ def amd_order(n: int, col_ptr, row_idx) -> tuple:
     return perm, {k: st[i] for i, k in enumerate(keys)}
 
 
-def metis_order(n: int, col_ptr, row_idx, seed: int = 1) -> np.ndarray:
-    """MetisND on a full symmetric pattern (new-to-old permutation)."""
+def metis_order(n: int, col_ptr, row_idx, seed: int = 1, dense_quotient: bool = False,
+                dense_threshold: Optional[int] = None) -> np.ndarray:
+    """MetisND on a full symmetric pattern (new-to-old permutation); the
+    keywords are MetisOptions' seed, dense_quotient_enabled and
+    dense_quotient_threshold (crates/rslab-metis/src/lib.rs:90-122)."""
     cp = _i64(col_ptr)
     ri = _i64(row_idx)
     perm = np.zeros(n, np.int64)
-    _check(N.lib.rslab_metis_order(n, _p64(cp), _p64(ri), C.c_uint64(seed), _p64(perm)))
+    _check(N.lib.rslab_metis_order(n, _p64(cp), _p64(ri), C.c_uint64(seed), int(dense_quotient),
+                                   -1 if dense_threshold is None else int(dense_threshold), _p64(perm)))
     return perm
 
 

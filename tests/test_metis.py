@@ -132,3 +132,61 @@ def test_degenerate_graphs_give_permutations(shape):
     a.sort_indices()
     p = metis_order(a.shape[0], a.indptr, a.indices)
     assert sorted(p.tolist()) == list(range(a.shape[0]))
+
+
+# The reference's dense-quotient tests (crates/rslab-metis/tests/dense_quotient.rs):
+# full symmetric pattern of a banded graph plus one near-dense column.
+
+def _pattern(n, edges):
+    import scipy.sparse as sp
+    r = np.array([e[0] for e in edges] + list(range(n)))
+    c = np.array([e[1] for e in edges] + list(range(n)))
+    a = sp.csc_matrix((np.ones(len(r)), (r, c)), shape=(n, n))
+    a = ((a + a.T) != 0).astype(np.float64).tocsc()
+    a.sort_indices()
+    return a.indptr, a.indices
+
+
+def _banded(n, band):
+    return [(r, r + 1) for r in range(n - 1)] + [(r, r + band) for r in range(n - band)]
+
+
+def _with_dense(n, band, col, deg):
+    e = _banded(n, band)
+    added, step = set(), 1
+    while len(added) < deg:
+        r = (col + step) % n
+        if r != col and r not in added:
+            e.append((col, r))
+            added.add(r)
+        step += 1
+    return e
+
+
+def test_dense_column_lands_at_end_of_perm():
+    from rslab_b200.solver import metis_order
+    cp, ri = _pattern(1000, _with_dense(1000, 7, 500, 800))
+    p = metis_order(1000, cp, ri, dense_quotient=True)
+    assert sorted(p.tolist()) == list(range(1000)) and p[-1] == 500
+
+
+def test_no_dense_column_matches_the_plain_order():
+    from rslab_b200.solver import metis_order
+    cp, ri = _pattern(600, _banded(600, 11))
+    assert np.array_equal(metis_order(600, cp, ri), metis_order(600, cp, ri, dense_quotient=True))
+
+
+def test_quotient_off_keeps_the_dense_column_inside():
+    from rslab_b200.solver import metis_order
+    cp, ri = _pattern(1000, _with_dense(1000, 7, 500, 800))
+    off = metis_order(1000, cp, ri)
+    assert sorted(off.tolist()) == list(range(1000))
+    assert metis_order(1000, cp, ri, dense_quotient=True)[-1] == 500
+
+
+def test_threshold_override_promotes_a_lower_degree_column():
+    from rslab_b200.solver import metis_order
+    cp, ri = _pattern(200, _with_dense(200, 5, 73, 50))
+    assert sorted(metis_order(200, cp, ri).tolist()) == list(range(200))
+    p = metis_order(200, cp, ri, dense_quotient=True, dense_threshold=30)
+    assert sorted(p.tolist()) == list(range(200)) and p[-1] == 73
