@@ -299,9 +299,9 @@ int rslab_metis_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx,
 
 /* Allocation-free dense panel factor.  No counterpart in the reference: an
  * addition for callers that cannot allocate device memory at factor time
- * (code running inside a CUDA graph capture or a foreign memory pool, capped
- * or frozen allocators, real-time loops that must not risk cudaMalloc latency
- * or an out-of-memory failure).  Factors one caller-owned dense panel
+ * (code embedded in another library's memory pool, capped or frozen
+ * allocators, real-time loops that must not risk cudaMalloc latency or an
+ * out-of-memory failure).  Factors one caller-owned dense panel
  * (nrow x ncol column-major device memory: the fully-summed block on top of
  * the off-diagonal rows, lower part) in place with the same panel-bounded
  * Bunch-Kaufman kernels as rslab_factor, writing d, dsub, kind (0 = 1x1,

@@ -2232,10 +2232,8 @@ uint64_t rslab_rng_units(uint64_t state, int64_t m, double* out) {
 // AMD ordering of a full symmetric pattern, for golden-vector checks.
 int rslab_amd_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, int64_t* perm, double* stats7) {
   try {
-    rslab::CscPattern p;
-    p.n = n;
-    p.col_ptr.assign(col_ptr, col_ptr + n + 1);
-    p.row_idx.assign(row_idx, row_idx + col_ptr[n]);
+    if (n > 0 && !perm) throw RslabError(Status::InvalidInput, "null perm");
+    const rslab::CscPattern p = rslab::checked_full_pattern(n, col_ptr, row_idx);
     rslab::AmdStats st;
     std::vector<int64_t> pr = rslab::amd_order(p, &st);
     std::copy(pr.begin(), pr.end(), perm);
@@ -2257,11 +2255,8 @@ int rslab_amd_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, i
 int rslab_metis_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, uint64_t seed, int dense_quotient,
                       int64_t dense_threshold, int64_t* perm) {
   try {
-    if (n < 0 || (n > 0 && (!col_ptr || !row_idx || !perm))) throw RslabError(Status::InvalidInput, "null pattern");
-    rslab::CscPattern p;
-    p.n = n;
-    p.col_ptr.assign(col_ptr, col_ptr + n + 1);
-    p.row_idx.assign(row_idx, row_idx + col_ptr[n]);
+    if (n > 0 && !perm) throw RslabError(Status::InvalidInput, "null perm");
+    const rslab::CscPattern p = rslab::checked_full_pattern(n, col_ptr, row_idx);
     std::vector<int64_t> pr = rslab::metis_nd_order(p, seed, dense_quotient != 0, dense_threshold);
     std::copy(pr.begin(), pr.end(), perm);
     return 0;
@@ -2276,16 +2271,18 @@ int rslab_metis_order(int64_t n, const int64_t* col_ptr, const int64_t* row_idx,
 // Allocation-free dense panel factor.
 //
 // Some callers cannot allocate device memory while they factor: a solver
-// running inside a CUDA graph or another library's memory pool, a process
-// whose allocator is capped or frozen after start-up, or a real-time loop that
-// must not pay cudaMalloc latency or risk an out-of-memory failure mid-run.
-// For them rslab_panel_factor_noalloc runs the blocked Bunch-Kaufman panel
-// kernels (getf2, deep-row replay, in-panel Schur) on one caller-owned dense
-// panel with every piece of scratch (the per-block multiplier snapshot, swap
-// log, the panel's structure and the launch task lists) placed in the
-// file-scope array below instead of memory obtained from an allocator.  The
-// array is 1 MiB and, like every __device__ variable, is held on each GPU that
-// loads this library until the process exits.
+// embedded in another library's memory pool, a process whose allocator is
+// capped or frozen after start-up, or a real-time loop that must not pay
+// cudaMalloc latency or risk an out-of-memory failure mid-run.  For them
+// rslab_panel_factor_noalloc runs the blocked Bunch-Kaufman panel kernels
+// (getf2, deep-row replay, in-panel Schur) on one caller-owned dense panel
+// with every piece of scratch (the per-block multiplier snapshot, swap log,
+// the panel's structure and the launch task lists) placed in the file-scope
+// array below instead of memory obtained from an allocator.  The structure
+// and the task lists are written into that array by a small kernel, so no
+// host buffer has to outlive the call.  The array is 1 MiB and, like every
+// __device__ variable, is held on each GPU that loads this library until the
+// process exits.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -2318,46 +2315,105 @@ struct NoallocStruct {  // the one-supernode structure, at offset 0 of the scrat
   long long sn_poff, sn_rsoff;
 };
 
+// The block sequence of one panel, in launch order: for every column block
+// its getf2 task, then (unless getf2 replays the deep rows itself) the
+// deep-row chunks, then the in-panel Schur tiles.  noalloc_count walks it on
+// the host for the launch segments; k_noalloc_plan writes the same tasks on
+// the device.
+struct NoallocSeg {
+  int kind, off, cnt;
+};
+
+__host__ __device__ inline int noalloc_schur_tiles(int mt, int cw) {
+  int c = 0;
+  for (int c0 = 0; c0 < cw && c0 < mt; c0 += TILE) c += (mt - c0 + TILE - 1) / TILE;
+  return c;
+}
+
+int noalloc_count(int nrow, int ncol, int nb, std::vector<NoallocSeg>& segs) {
+  int t = 0;
+  for (int kb = 0; kb < ncol; kb += nb) {
+    const int ke = std::min(kb + nb, ncol);
+    const bool fuse = (nrow - ke) <= FUSE_DEEP_ROWS;
+    segs.push_back({L_GETF2, t, 1});
+    t += 1;
+    if (!fuse) {
+      const int cnt = (nrow - ke + DEEP_R - 1) / DEEP_R;
+      segs.push_back({L_DEEP, t, cnt});
+      t += cnt;
+    }
+    const int cnt = noalloc_schur_tiles(nrow - ke, ncol - ke);
+    if (cnt) segs.push_back({L_SCHUR, t, cnt});
+    t += cnt;
+  }
+  return t;
+}
+
+// One CTA: the blocks run in order (every thread keeps the same running
+// offset), the tasks of a block are written by all threads.
+__global__ void k_noalloc_plan(NoallocStruct* ns, int4* tasks, int nrow, int ncol, int nb) {
+  if (threadIdx.x == 0) {
+    ns->sn_first = 0;
+    ns->sn_ncol = ncol;
+    ns->sn_nrow = nrow;
+    ns->pad = 0;
+    ns->sn_poff = 0;
+    ns->sn_rsoff = 0;
+  }
+  int t = 0;
+  for (int kb = 0; kb < ncol; kb += nb) {
+    const int ke = min(kb + nb, ncol);
+    const bool fuse = (nrow - ke) <= FUSE_DEEP_ROWS;
+    if (threadIdx.x == 0) tasks[t] = make_int4(0, kb, 0, fuse ? 1 : 0);
+    t += 1;
+    if (!fuse) {
+      const int cnt = (nrow - ke + DEEP_R - 1) / DEEP_R;
+      for (int i = threadIdx.x; i < cnt; i += blockDim.x) tasks[t + i] = make_int4(0, kb, 0, ke + i * DEEP_R);
+      t += cnt;
+    }
+    const int mt = nrow - ke, cw = ncol - ke;
+    for (int c0 = 0; c0 < cw && c0 < mt; c0 += TILE) {
+      const int cnt = (mt - c0 + TILE - 1) / TILE;
+      for (int i = threadIdx.x; i < cnt; i += blockDim.x) tasks[t + i] = make_int4(0, kb, c0 + i * TILE, c0);
+      t += cnt;
+    }
+  }
+}
+
+// The kernels' shared-memory limits are raised once per device.
+template <typename T>
+void noalloc_attrs() {
+  static std::mutex mu;
+  static bool done[256] = {};
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  if (done[dev]) return;
+  const size_t es = sizeof(T);
+  CK(cudaFuncSetAttribute(k_getf2<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_getf2(es, 128)));
+  CK(cudaFuncSetAttribute(k_deep<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep(es, 128)));
+  CK(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
+  done[dev] = true;
+}
+
 template <typename T>
 void noalloc_panel(unsigned char* base, T* panel, int nrow, int ncol, int panel_nb, T* d, T* dsub,
                    unsigned char* kind, int* lperm, int* status, cudaStream_t st) {
   const size_t es = sizeof(T);
   const int nb_small = panel_nb, nb_big = std::max(panel_nb, 128);
   const int nb = ncol >= 512 ? nb_big : nb_small;
-  // Task lists of the whole block sequence, in launch order.
-  std::vector<int4> tasks;
-  struct Seg {
-    int kind, off, cnt;
-  };
-  std::vector<Seg> segs;
-  for (int kb = 0; kb < ncol; kb += nb) {
-    const int ke = std::min(kb + nb, ncol);
-    const bool fuse = (nrow - ke) <= FUSE_DEEP_ROWS;
-    segs.push_back({L_GETF2, (int)tasks.size(), 1});
-    tasks.push_back(make_int4(0, kb, 0, fuse ? 1 : 0));
-    if (!fuse) {
-      Seg sd{L_DEEP, (int)tasks.size(), 0};
-      for (int r0 = ke; r0 < nrow; r0 += DEEP_R) tasks.push_back(make_int4(0, kb, 0, r0));
-      sd.cnt = (int)tasks.size() - sd.off;
-      segs.push_back(sd);
-    }
-    const int mt = nrow - ke, cw = ncol - ke;
-    Seg sc{L_SCHUR, (int)tasks.size(), 0};
-    for (int c0 = 0; c0 < cw; c0 += TILE)
-      for (int r0 = c0; r0 < mt; r0 += TILE) tasks.push_back(make_int4(0, kb, r0, c0));
-    sc.cnt = (int)tasks.size() - sc.off;
-    if (sc.cnt) segs.push_back(sc);
-  }
+  std::vector<NoallocSeg> segs;
+  const int ntasks = noalloc_count(nrow, ncol, nb, segs);
   const size_t snap_bytes = ((size_t)nb_big * nb_big * es + 3 * nb_big * 4 + 255) / 256 * 256;
   const size_t off_snap = 256, off_tasks = off_snap + snap_bytes;
-  const size_t need = off_tasks + tasks.size() * sizeof(int4);
+  const size_t need = off_tasks + (size_t)ntasks * sizeof(int4);
   if (need > NOALLOC_BYTES)
     throw RslabError(Status::InvalidInput, "panel needs " + std::to_string(need) +
                                                " bytes of scratch, more than the allocation-free limit of " +
                                                std::to_string(NOALLOC_BYTES));
-  NoallocStruct ns{0, ncol, nrow, 0, 0, 0};
-  CK(cudaMemcpyAsync(base, &ns, sizeof(ns), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(base + off_tasks, tasks.data(), tasks.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+  noalloc_attrs<T>();
+  k_noalloc_plan<<<1, 256, 0, st>>>(reinterpret_cast<NoallocStruct*>(base),
+                                    reinterpret_cast<int4*>(base + off_tasks), nrow, ncol, nb);
   CK(cudaMemsetAsync(status, 0, 4 * sizeof(int), st));
   const NoallocStruct* dn = reinterpret_cast<const NoallocStruct*>(base);
   FactorArgs fa{};
@@ -2376,10 +2432,7 @@ void noalloc_panel(unsigned char* base, T* panel, int nrow, int ncol, int panel_
   fa.status = status;
   fa.perturb_floor = -1.0;
   const int4* dt = reinterpret_cast<const int4*>(base + off_tasks);
-  CK(cudaFuncSetAttribute(k_getf2<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_getf2(es, 128)));
-  CK(cudaFuncSetAttribute(k_deep<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep(es, 128)));
-  CK(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
-  for (const Seg& g : segs) {
+  for (const NoallocSeg& g : segs) {
     if (g.kind == L_GETF2)
       k_getf2<T, 256><<<g.cnt, 256, smem_getf2(es, nb), st>>>(fa, dt + g.off, nb_small, nb_big);
     else if (g.kind == L_DEEP)

@@ -36,6 +36,13 @@ struct CscPattern {
 
 // Validation of a lower-triangle CSC (src/sparse/csc.rs:157-237).
 void validate_lower_csc(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, int64_t nnz);
+// Validation of a full symmetric pattern given to an ordering entry point, as
+// Graph::from_csc_pattern (crates/rslab-metis/src/graph.rs:51-86) and
+// CscPattern::new check it: col_ptr starts at 0 and never decreases, n and
+// nnz fit 32-bit indices, rows lie in [0, n) sorted within each column, and
+// the pattern is structurally symmetric.  Returns the pattern with adjacent
+// duplicate rows dropped; throws InvalidInput otherwise.
+CscPattern checked_full_pattern(int64_t n, const int64_t* col_ptr, const int64_t* row_idx);
 // Lower triangle -> full symmetric pattern (src/sparse/csc.rs:240-291).
 CscPattern symmetric_pattern(int64_t n, const int64_t* col_ptr, const int64_t* row_idx);
 // Relabel a full symmetric pattern by a new-to-old permutation

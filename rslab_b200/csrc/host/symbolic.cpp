@@ -16,6 +16,7 @@
 #include "host.hpp"
 
 #include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <numeric>
 
@@ -42,6 +43,51 @@ void validate_lower_csc(int64_t n, const int64_t* col_ptr, const int64_t* row_id
         throw RslabError(Status::InvalidInput, "row indices not sorted in column " + std::to_string(j));
     }
   }
+}
+
+CscPattern checked_full_pattern(int64_t n, const int64_t* col_ptr, const int64_t* row_idx) {
+  if (n < 0) throw RslabError(Status::InvalidInput, "n must be non-negative");
+  if (n > INT32_MAX) throw RslabError(Status::InvalidInput, "n exceeds the 32-bit index range");
+  if (!col_ptr) throw RslabError(Status::InvalidInput, "null col_ptr");
+  if (col_ptr[0] != 0) throw RslabError(Status::InvalidInput, "col_ptr[0] must be 0");
+  for (int64_t j = 0; j < n; ++j)
+    if (col_ptr[j + 1] < col_ptr[j])
+      throw RslabError(Status::InvalidInput,
+                       "col_ptr not monotonically non-decreasing at column " + std::to_string(j));
+  if (col_ptr[n] > INT32_MAX) throw RslabError(Status::InvalidInput, "nnz exceeds the 32-bit index range");
+  if (col_ptr[n] > 0 && !row_idx) throw RslabError(Status::InvalidInput, "null row_idx");
+  CscPattern p;
+  p.n = n;
+  p.col_ptr.assign(n + 1, 0);
+  p.row_idx.reserve(col_ptr[n]);
+  for (int64_t j = 0; j < n; ++j) {
+    int64_t last = -1;
+    for (int64_t k = col_ptr[j]; k < col_ptr[j + 1]; ++k) {
+      const int64_t i = row_idx[k];
+      if (i < 0 || i >= n)
+        throw RslabError(Status::InvalidInput,
+                         "row index " + std::to_string(i) + " out of bounds in column " + std::to_string(j));
+      if (i < last) throw RslabError(Status::InvalidInput, "row indices not sorted in column " + std::to_string(j));
+      if (i != last) p.row_idx.push_back(i);  // sorted input: duplicates are adjacent
+      last = i;
+    }
+    p.col_ptr[j + 1] = (int64_t)p.row_idx.size();
+  }
+  // structural symmetry: entry (i, j) needs (j, i).  The transpose of a
+  // column-sorted pattern, filled column by column, is row-sorted too, so the
+  // two index arrays must be equal.
+  std::vector<int64_t> tp(n + 1, 0), ti(p.row_idx.size());
+  for (int64_t i : p.row_idx) tp[i + 1]++;
+  for (int64_t j = 0; j < n; ++j) tp[j + 1] += tp[j];
+  std::vector<int64_t> fill(tp.begin(), tp.end() - 1);
+  for (int64_t j = 0; j < n; ++j)
+    for (int64_t k = p.col_ptr[j]; k < p.col_ptr[j + 1]; ++k) ti[fill[p.row_idx[k]]++] = j;
+  for (int64_t j = 0; j < n; ++j)
+    if (tp[j + 1] != p.col_ptr[j + 1] ||
+        !std::equal(ti.begin() + tp[j], ti.begin() + tp[j + 1], p.row_idx.begin() + p.col_ptr[j]))
+      throw RslabError(Status::InvalidInput,
+                       "pattern is not structurally symmetric (first at column " + std::to_string(j) + ")");
+  return p;
 }
 
 CscPattern symmetric_pattern(int64_t n, const int64_t* col_ptr, const int64_t* row_idx) {

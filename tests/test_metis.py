@@ -190,3 +190,41 @@ def test_threshold_override_promotes_a_lower_degree_column():
     assert sorted(metis_order(200, cp, ri).tolist()) == list(range(200))
     p = metis_order(200, cp, ri, dense_quotient=True, dense_threshold=30)
     assert sorted(p.tolist()) == list(range(200)) and p[-1] == 73
+
+
+@pytest.mark.parametrize("which", ["amd", "metis"])
+def test_ordering_entry_points_reject_malformed_patterns(which):
+    """The ordering entry points validate their full symmetric pattern as the
+    reference's Graph::from_csc_pattern / CscPattern::new do, and return
+    InvalidInput instead of reading or writing outside the arrays."""
+    from rslab_b200.solver import InvalidInput, amd_order, metis_order
+
+    def run(n, cp, ri):
+        cp, ri = np.asarray(cp, np.int64), np.asarray(ri, np.int64)
+        return amd_order(n, cp, ri) if which == "amd" else metis_order(n, cp, ri)
+
+    # 3-vertex path 0-1-2 with diagonals: valid
+    ok_cp, ok_ri = [0, 2, 5, 7], [0, 1, 0, 1, 2, 1, 2]
+    run(3, ok_cp, ok_ri)
+    bad = {
+        "row out of range": ([0, 2, 5, 7], [0, 1, 0, 1, 9, 1, 2]),
+        "negative row": ([0, 2, 5, 7], [0, -1, 0, 1, 2, 1, 2]),
+        "col_ptr decreasing": ([0, 5, 2, 7], [0, 1, 0, 1, 2, 1, 2]),
+        "col_ptr[0] != 0": ([1, 2, 5, 7], [0, 1, 0, 1, 2, 1, 2]),
+        "unsorted column": ([0, 2, 5, 7], [1, 0, 0, 1, 2, 1, 2]),
+        "not symmetric": ([0, 2, 4, 6], [0, 1, 1, 2, 1, 2]),
+    }
+    for what, (cp, ri) in bad.items():
+        with pytest.raises(InvalidInput):
+            run(3, cp, ri)
+        assert what  # message names the case on failure
+
+
+def test_ordering_entry_points_drop_adjacent_duplicates():
+    from rslab_b200.solver import amd_order, metis_order
+
+    cp = np.array([0, 3, 7, 9], np.int64)
+    ri = np.array([0, 1, 1, 0, 1, 1, 2, 1, 2], np.int64)
+    p, _ = amd_order(3, cp, ri)
+    assert sorted(p.tolist()) == [0, 1, 2]
+    assert sorted(metis_order(3, cp, ri).tolist()) == [0, 1, 2]
