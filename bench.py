@@ -56,8 +56,9 @@ def parse():
                    help="helmholtz: the 64^3 Helmholtz factor+solve step (default); sweep: the "
                         "same-pattern frequency sweep, 48^3 27-point K - w^2 M + i w C, 64 frequencies; "
                         "tiers: the learned precision tier on the held-out 80^3 27-point complex Helmholtz")
-    p.add_argument("--ordering", default="amd", choices=["amd", "metis"],
-                   help="fill-reducing ordering of the helmholtz workload (metis: the MetisND restatement)")
+    p.add_argument("--ordering", default="tuned", choices=["tuned", "amd", "metis"],
+                   help="fill-reducing ordering of the helmholtz workload: tuned = the default pick of "
+                        "LdltSolver::factor (nested-dissection bakeoff; MetisND on this matrix), amd, metis")
     p.add_argument("--tiers-side", type=int, default=80)
     p.add_argument("--tier-model", default=None, help="tier network .npz (default: the package's trained one)")
     p.add_argument("--sweep-side", type=int, default=48)
@@ -196,19 +197,6 @@ def host_backward_error(a, x, b) -> float:
     r = b2 - full @ x2
     anorm = float(np.abs(full).sum(axis=1).max())
     return float(np.max(np.abs(r).max(axis=0) / (anorm * np.abs(x2).max(axis=0) + np.abs(b2).max(axis=0))))
-
-
-def cmod_tc_bytes_per_flop():
-    """DRAM bytes per algorithmic flop of k_cmod_tc from the committed ncu
-    summary (line 'dram_bytes_per_flop: X'), or None."""
-    f = ROOT / "profiles" / "k_cmod_tc_helmholtz48.md"
-    try:
-        for line in f.read_text().splitlines():
-            if line.strip().startswith("dram_bytes_per_flop:"):
-                return float(line.split(":", 1)[1])
-    except OSError:
-        pass
-    return None
 
 
 def launches_per_step(prof_mixed, sprof, minfo):
@@ -577,12 +565,25 @@ def main():
 
     a = matgen.c2_matrix(args.side)
     n, nrhs = a.n, args.nrhs
+    from rslab_b200 import Ordering
+    t_an = time.perf_counter()
     if args.ordering == "metis":
-        from rslab_b200 import Ordering
         sym = LdltSymbolic.analyze_with(a, SolverSettings().with_ordering(Ordering.METIS_ND))
-    else:
+        ordering = Ordering.METIS_ND
+    elif args.ordering == "amd":
         sym = LdltSymbolic.analyze(a)
+        ordering = Ordering.AMD
+    else:
+        sym, st_tuned = LdltSymbolic.tuned(a)
+        ordering = st_tuned.ordering
+    t_an = time.perf_counter() - t_an
     info = sym.info()
+    ex = sym.export()
+    sn_c = ex["sn_ncol"].astype(np.float64)
+    sn_r = ex["sn_nrow"].astype(np.float64)
+    # algorithmic bytes of one solve of nrhs columns (forward + backward panel
+    # reads, right-hand sides in / out twice, D), in the factor's field
+    solve_entries = float(np.sum(sn_c * (sn_c + 1) / 2 + (sn_r - sn_c) * sn_c))
     flops = 4.0 * info.flops_model  # complex: 4 real flops per complex multiply-add pair
     b = matgen.uniform_rhs(n, nrhs, 1, complex_=True)
     vals_d = torch.from_numpy(np.ascontiguousarray(a.values)).to(dev)
@@ -695,12 +696,11 @@ def main():
     tc_n = sum(1 for k, _, _ in tr if k == "cmod_tc")
     cm = prof_mixed["cmod"]
     ach = cm["flops"] / (tc_ms * 1e-3) / 1e12 if tc_ms > 0 else 0.0
-    bpf = cmod_tc_bytes_per_flop()
     roofline = {"bound": "tensor", "kernel": "k_cmod_tc (c32, tcgen05 kind::tf32, 3xTF32 split)",
                 "achieved": ach, "peak": peak_tf, "unit": "TFLOP/s", "frac": ach / peak_tf,
-                "traffic": (bpf * cm["flops"] / max(tc_n, 1)) if bpf else None,
-                "traffic_note": "dram bytes per launch: ncu bytes per algorithmic flop (profiles/"
-                                "k_cmod_tc_helmholtz48.md) x this run's flops per launch",
+                "traffic": None,
+                "traffic_note": "not measured by this run: dram bytes per launch come from an ncu capture "
+                                "of the kernel (profiles/)",
                 "peak_source": ("MEASURED_PEAKS.json bf16_tflops (burst), of measured" if "bf16_tflops" in peaks
                                 else "fallback 1590 TFLOP/s"),
                 "launches": tc_n, "avg_launch_ms": tc_ms / max(tc_n, 1),
@@ -733,6 +733,19 @@ def main():
     fi = N.FactorInfo()
     N.lib.rslab_factor_info(mixed._h, C.byref(fi))
     gflops = flops / (ms_mixed * 1e-3) / 1e9 * ws
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+
+    def solve_bw(prof, esize):
+        byt = 2.0 * solve_entries * esize + 4.0 * n * nrhs * esize + 2.0 * n * esize
+        ms = prof["total"]["ms"]
+        return {"bytes": byt, "ms": ms, "gbs": byt / (ms * 1e-3) / 1e9 if ms > 0 else None,
+                "frac_of_hbm": (byt / (ms * 1e-3) / 1e9 / hbm) if ms > 0 else None,
+                "hbm_peak_gbs": hbm}
+    solve_gbs = {"mixed_c32": solve_bw(sprof_mixed, 8)}
+    if prof_f64 is not None:
+        solve_gbs["fp64_c64"] = solve_bw(solve_profile(f64._h, nrhs), 16)
+    solve_gbs["note"] = ("algorithmic bytes 2 sum_s(c(c+1)/2 + (r-c)c) + 4 n nrhs + 2 n scalars per solve, "
+                         "eager solve with per-launch events (no graph), of measured hbm_gbs")
     cpu_base = cpu_sample(args) if (rank == 0 and ws == 1 and not args.no_cpu) else None
     if rank == 0:
         line = {
@@ -741,7 +754,8 @@ def main():
             "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": f"{TIERS[tier]} factor / f64 refinement", "data": "synthetic",
             "config": {"workload": f"helmholtz3d_{args.side}^3_c64_nrhs{nrhs}", "n": n, "nnz_lower": a.nnz,
-                       "nrhs": nrhs, "ordering": "MetisND" if args.ordering == "metis" else "AMD",
+                       "nrhs": nrhs, "ordering": "MetisND" if ordering == Ordering.METIS_ND else "AMD",
+                       "ordering_pick": args.ordering, "analysis_s": t_an,
                        "target_backward_error": args.target,
                        "model_flops": flops, "factor_nnz_panels": info.panel_elems,
                        "parallelism": f"replicas{ws}", "l2": "flushed between steps (256 MB write)"},
@@ -761,6 +775,7 @@ def main():
             "profile_mixed": prof_mixed,
             "profile_fp64": prof_f64,
             "solve_profile_mixed": sprof_mixed,
+            "solve_gbs": solve_gbs,
             "cpu_baseline": cpu_base,
             "gpu_launches": launches_per_step(prof_mixed, sprof_mixed, minfo),
         }

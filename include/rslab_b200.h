@@ -10,6 +10,9 @@
  *   rslab_analyze        LdltSymbolic::analyze / analyze_with
  *                        (src/numeric/sparse_solver.rs:493,506) ->
  *                        multifrontal_ldlt::analyze_with (src/numeric/multifrontal_ldlt.rs:1667)
+ *   rslab_analyze_tuned  LdltSolver::tuned + nd_bakeoff (src/numeric/sparse_solver.rs:108-131,231-266)
+ *   rslab_symbolic_estimate LdltSymbolic::estimate_memory / symbolic_factor_nnz
+ *                        (src/numeric/sparse_solver.rs:550-660)
  *   rslab_factor         LdltSymbolic::factor (src/numeric/sparse_solver.rs:677) ->
  *                        factor_numeric (src/numeric/multifrontal_ldlt.rs:1851)
  *   rslab_refactor       LdltSymbolic::factor on a new value set of the same
@@ -127,6 +130,8 @@ typedef struct {
   int64_t n_perturbed;
   double factor_ms, solve_ms;  /* device time of the last factor / solve */
   int32_t dtype, dtype_hi;
+  int32_t multiprocessors;     /* SMs of the handle's device (the reference's Diagnostics::threads
+                                * counts CPU workers) */
 } rslab_factor_info_t;
 
 typedef struct {
@@ -152,6 +157,35 @@ int rslab_analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx,
  * RSLAB_INVALID_INPUT with a message naming the first offending column. */
 int rslab_validate_lower_csc(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, int64_t nnz);
 int rslab_symbolic_info(const rslab_sym_handle* sym, rslab_symbolic_info_t* info);
+
+/* A-priori memory and work estimate of an analysis for a scalar of
+ * value_bytes bytes: LdltSymbolic::estimate_memory
+ * (src/numeric/sparse_solver.rs:561-660; estimate_left_looking,
+ * src/diagnostics.rs:116-175) and LdltSymbolic::symbolic_factor_nnz (:550).
+ * panel_live_peak_bytes is the live-panel peak of the left-looking refcount
+ * free schedule; factor_flops = sum_s nrow^2 ncol. */
+typedef struct {
+  int64_t value_bytes, factor_nnz, factor_bytes, panels_all_bytes;
+  int64_t panel_live_peak_bytes, transient_peak_bytes;
+  uint64_t factor_flops, critical_path_flops;
+  int64_t max_tree_width;
+  int64_t symbolic_factor_nnz; /* exact column-count fill x 1.2 (src/symbolic/mod.rs:1189,1202) */
+} rslab_memory_estimate_t;
+int rslab_symbolic_estimate(const rslab_sym_handle* sym, int64_t value_bytes, rslab_memory_estimate_t* est);
+
+/* The default settings pick behind LdltSolver::factor: LdltSolver::tuned
+ * (src/numeric/sparse_solver.rs:108-131) with the nested-dissection bakeoff
+ * nd_bakeoff (:231-266).  Analyses with the default settings (AMD); when
+ * n >= 10,000 and that analysis predicts factor_flops >= 5e9 for a scalar
+ * of value_bytes bytes, analyses again with MetisND and adopts it only if its
+ * factor_flops is below 0.75x, its symbolic_factor_nnz is not larger and its
+ * live-panel peak is not larger (constants :31-36).  *ordering_used gets the
+ * RSLAB_ORDER_* of the returned analysis. */
+#define RSLAB_ND_BAKEOFF_MIN_FLOPS 5000000000LL
+#define RSLAB_ND_BAKEOFF_MIN_N 10000
+#define RSLAB_ND_BAKEOFF_ADOPT_RATIO 0.75
+int rslab_analyze_tuned(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, int64_t value_bytes,
+                        rslab_sym_handle** out, int32_t* ordering_used);
 int rslab_symbolic_export(const rslab_sym_handle* sym, int64_t* perm, int64_t* sn_first, int64_t* sn_ncol,
                           int64_t* sn_nrow, int64_t* sn_level, int64_t* child_ptr, int64_t* child_idx,
                           int64_t* col_counts, int64_t* parent);

@@ -68,7 +68,16 @@ class FactorInfo(C.Structure):
         ("status", C.c_int32), ("failing_supernode", C.c_int64),
         ("inertia_pos", C.c_int64), ("inertia_neg", C.c_int64), ("inertia_zero", C.c_int64),
         ("n_perturbed", C.c_int64), ("factor_ms", C.c_double), ("solve_ms", C.c_double),
-        ("dtype", C.c_int32), ("dtype_hi", C.c_int32),
+        ("dtype", C.c_int32), ("dtype_hi", C.c_int32), ("multiprocessors", C.c_int32),
+    ]
+
+
+class MemoryEstimateC(C.Structure):
+    _fields_ = [
+        ("value_bytes", C.c_int64), ("factor_nnz", C.c_int64), ("factor_bytes", C.c_int64),
+        ("panels_all_bytes", C.c_int64), ("panel_live_peak_bytes", C.c_int64), ("transient_peak_bytes", C.c_int64),
+        ("factor_flops", C.c_uint64), ("critical_path_flops", C.c_uint64), ("max_tree_width", C.c_int64),
+        ("symbolic_factor_nnz", C.c_int64),
     ]
 
 
@@ -87,6 +96,8 @@ SIGNATURES = {
     "rslab_default_analyze_settings": (None, [C.POINTER(AnalyzeSettings)]),
     "rslab_default_factor_settings": (None, [C.POINTER(FactorSettings)]),
     "rslab_analyze": (C.c_int, [C.c_int64, i64p, i64p, C.POINTER(AnalyzeSettings), C.POINTER(vp)]),
+    "rslab_analyze_tuned": (C.c_int, [C.c_int64, i64p, i64p, C.c_int64, C.POINTER(vp), C.POINTER(C.c_int32)]),
+    "rslab_symbolic_estimate": (C.c_int, [vp, C.c_int64, C.POINTER(MemoryEstimateC)]),
     "rslab_validate_lower_csc": (C.c_int, [C.c_int64, i64p, i64p, C.c_int64]),
     "rslab_symbolic_info": (C.c_int, [vp, C.POINTER(SymbolicInfo)]),
     "rslab_symbolic_export": (C.c_int, [vp, i64p, i64p, i64p, i64p, i64p, i64p, i64p, i64p, i64p]),

@@ -1584,35 +1584,120 @@ int rslab_validate_lower_csc(int64_t n, const int64_t* col_ptr, const int64_t* r
   }
 }
 
+}  // extern "C"
+
+namespace {
+
+void check_lower_input(int64_t n, const int64_t* col_ptr, const int64_t* row_idx) {
+  if (n < 0 || !col_ptr || (n > 0 && !row_idx && col_ptr[n] > 0)) throw RslabError(Status::InvalidInput, "bad CSC");
+  if (n >= (int64_t)1 << 31) throw RslabError(Status::InvalidInput, "n too large");
+  rslab::validate_lower_csc(n, col_ptr, row_idx, col_ptr[n]);
+}
+
+rslab::AnalyzeOptions analyze_options(const rslab_analyze_settings& st) {
+  rslab::AnalyzeOptions o;
+  o.ordering = (rslab::Ordering)st.ordering;
+  o.nemin = st.nemin;
+  o.relax = st.relax != 0;
+  o.relax_max_width = st.relax_max_width;
+  o.relax_max_extra_rows = st.relax_max_extra_rows;
+  o.hybrid_liu = st.hybrid_liu != 0;
+  o.given_perm = st.given_perm;
+  return o;
+}
+
+// A handle around a finished host analysis: the device plan is built here.
+rslab_sym_handle* make_sym_handle(rslab::Symbolic&& S, const rslab_analyze_settings& st, int64_t n,
+                                  const int64_t* col_ptr, const int64_t* row_idx) {
+  auto H = std::make_unique<rslab_sym_handle>();
+  H->settings = st;
+  H->panel_nb = (int)std::min<int64_t>(std::max<int64_t>(st.panel_nb, 8), 128);  // panel kernels hold <= 128 columns
+  H->S = std::move(S);
+  H->seg_begin = {0, (long long)n};
+  H->nnz_begin = {0, (long long)col_ptr[n]};
+  build_plan(*H, col_ptr, row_idx);
+  return H.release();
+}
+
+void fill_estimate(const rslab::MemoryEstimate& e, const rslab::Symbolic& S, rslab_memory_estimate_t* out) {
+  out->value_bytes = e.value_bytes;
+  out->factor_nnz = e.factor_nnz;
+  out->factor_bytes = e.factor_bytes;
+  out->panels_all_bytes = e.panels_all_bytes;
+  out->panel_live_peak_bytes = e.panel_live_peak_bytes;
+  out->transient_peak_bytes = e.transient_peak_bytes;
+  out->factor_flops = e.factor_flops;
+  out->critical_path_flops = e.critical_path_flops;
+  out->max_tree_width = e.max_tree_width;
+  out->symbolic_factor_nnz = rslab::symbolic_factor_nnz(S);
+}
+
+}  // namespace
+
+extern "C" {
+
 int rslab_analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, const rslab_analyze_settings* settings,
                   rslab_sym_handle** out) {
   try {
     if (!out) throw RslabError(Status::InvalidInput, "null output handle");
     *out = nullptr;
-    if (n < 0 || !col_ptr || (n > 0 && !row_idx && col_ptr[n] > 0)) throw RslabError(Status::InvalidInput, "bad CSC");
-    if (n >= (int64_t)1 << 31) throw RslabError(Status::InvalidInput, "n too large");
-    rslab::validate_lower_csc(n, col_ptr, row_idx, col_ptr[n]);
+    check_lower_input(n, col_ptr, row_idx);
     rslab_analyze_settings st;
     if (settings)
       st = *settings;
     else
       rslab_default_analyze_settings(&st);
-    rslab::AnalyzeOptions o;
-    o.ordering = (rslab::Ordering)st.ordering;
-    o.nemin = st.nemin;
-    o.relax = st.relax != 0;
-    o.relax_max_width = st.relax_max_width;
-    o.relax_max_extra_rows = st.relax_max_extra_rows;
-    o.hybrid_liu = st.hybrid_liu != 0;
-    o.given_perm = st.given_perm;
-    auto H = std::make_unique<rslab_sym_handle>();
-    H->settings = st;
-    H->panel_nb = (int)std::min<int64_t>(std::max<int64_t>(st.panel_nb, 8), 128);  // panel kernels hold <= 128 columns
-    H->S = rslab::analyze(n, col_ptr, row_idx, o);
-    H->seg_begin = {0, (long long)n};
-    H->nnz_begin = {0, (long long)col_ptr[n]};
-    build_plan(*H, col_ptr, row_idx);
-    *out = H.release();
+    *out = make_sym_handle(rslab::analyze(n, col_ptr, row_idx, analyze_options(st)), st, n, col_ptr, row_idx);
+    return 0;
+  } catch (const RslabError& e) {
+    return fail(e);
+  } catch (const std::exception& e) {
+    return fail(RslabError(Status::InvalidInput, e.what()));
+  }
+}
+
+int rslab_symbolic_estimate(const rslab_sym_handle* h, int64_t value_bytes, rslab_memory_estimate_t* est) {
+  if (!h || !est || value_bytes <= 0) return fail(RslabError(Status::InvalidInput, "bad estimate arguments"));
+  fill_estimate(rslab::estimate_memory(h->S, value_bytes), h->S, est);
+  return 0;
+}
+
+int rslab_analyze_tuned(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, int64_t value_bytes,
+                        rslab_sym_handle** out, int32_t* ordering_used) {
+  try {
+    if (!out) throw RslabError(Status::InvalidInput, "null output handle");
+    *out = nullptr;
+    if (value_bytes <= 0) throw RslabError(Status::InvalidInput, "value_bytes must be positive");
+    check_lower_input(n, col_ptr, row_idx);
+    rslab_analyze_settings st;
+    rslab_default_analyze_settings(&st);
+    rslab::Symbolic S = rslab::analyze(n, col_ptr, row_idx, analyze_options(st));
+    if (n >= RSLAB_ND_BAKEOFF_MIN_N) {
+      const rslab::MemoryEstimate est = rslab::estimate_memory(S, value_bytes);
+      if (est.factor_flops >= (uint64_t)RSLAB_ND_BAKEOFF_MIN_FLOPS) {
+        rslab_analyze_settings st_nd = st;
+        st_nd.ordering = RSLAB_ORDER_METIS_ND;
+        bool nd_ok = true;
+        rslab::Symbolic S_nd;
+        try {
+          S_nd = rslab::analyze(n, col_ptr, row_idx, analyze_options(st_nd));
+        } catch (const std::exception&) {
+          nd_ok = false;  // the ND analysis failed: keep the first pick
+        }
+        if (nd_ok) {
+          const rslab::MemoryEstimate est_nd = rslab::estimate_memory(S_nd, value_bytes);
+          const bool flops_win = (double)est_nd.factor_flops < (double)est.factor_flops * RSLAB_ND_BAKEOFF_ADOPT_RATIO;
+          const bool fill_ok = rslab::symbolic_factor_nnz(S_nd) <= rslab::symbolic_factor_nnz(S);
+          const bool mem_ok = est_nd.panel_live_peak_bytes <= est.panel_live_peak_bytes;
+          if (flops_win && fill_ok && mem_ok) {
+            S = std::move(S_nd);
+            st = st_nd;
+          }
+        }
+      }
+    }
+    if (ordering_used) *ordering_used = st.ordering;
+    *out = make_sym_handle(std::move(S), st, n, col_ptr, row_idx);
     return 0;
   } catch (const RslabError& e) {
     return fail(e);
@@ -1984,6 +2069,9 @@ int rslab_factor_info(const rslab_fac_handle* F, rslab_factor_info_t* info) {
   info->solve_ms = F->solve_ms;
   info->dtype = F->dtype;
   info->dtype_hi = F->dtype_hi;
+  info->multiprocessors = 0;
+  if (F->sym && F->sym->device >= 0)
+    cudaDeviceGetAttribute(&info->multiprocessors, cudaDevAttrMultiProcessorCount, F->sym->device);
   return 0;
 }
 

@@ -125,6 +125,22 @@ Symbolic analyze(int64_t n, const int64_t* col_ptr, const int64_t* row_idx,
 // level-l supernodes of every system.
 Symbolic merge_independent(const std::vector<Symbolic>& parts);
 
+// A-priori memory and work estimate of an analysis for a scalar of
+// value_bytes bytes (LdltSymbolic::estimate_memory,
+// src/numeric/sparse_solver.rs:561-660, with estimate_left_looking,
+// src/diagnostics.rs:116-175): the refcount free schedule of the left-looking
+// factor gives the live panel peak; factor_flops = sum_s nrow^2 ncol.
+struct MemoryEstimate {
+  int64_t value_bytes = 0, factor_nnz = 0, factor_bytes = 0, panels_all_bytes = 0;
+  int64_t panel_live_peak_bytes = 0, transient_peak_bytes = 0;
+  uint64_t factor_flops = 0, critical_path_flops = 0;
+  int64_t max_tree_width = 0;
+};
+MemoryEstimate estimate_memory(const Symbolic& S, int64_t value_bytes);
+// symbolic_factor_nnz (src/numeric/sparse_solver.rs:550-555): the exact
+// column-count fill times the 1.2 slack (src/symbolic/mod.rs:1189, 1202).
+inline int64_t symbolic_factor_nnz(const Symbolic& S) { return (int64_t)((double)S.factor_nnz_sym * 1.2); }
+
 // Dense partial BK flop model per supernode: F(r,c) = sum_{m=r-c+1}^{r}(m^2-1).
 double supernode_flops(int64_t r, int64_t c);
 

@@ -680,4 +680,78 @@ Symbolic merge_independent(const std::vector<Symbolic>& parts) {
   return M;
 }
 
+MemoryEstimate estimate_memory(const Symbolic& S, int64_t value_bytes) {
+  MemoryEstimate e;
+  e.value_bytes = value_bytes;
+  const int64_t ns = (int64_t)S.sn.size();
+  auto nrow = [&](int64_t s) { return S.rs_ptr[s + 1] - S.rs_ptr[s]; };
+  // the descendants k whose off-diagonal rows land in s, once each (rows are
+  // ascending, so the supernodes they land in come in runs)
+  std::vector<int64_t> col_sn(S.n, 0);
+  for (int64_t s = 0; s < ns; ++s)
+    std::fill(col_sn.begin() + S.sn[s].first_col, col_sn.begin() + S.sn[s].first_col + S.sn[s].ncol, s);
+  std::vector<std::vector<int64_t>> upd(ns);
+  std::vector<int64_t> refc(ns, 0);
+  for (int64_t k = 0; k < ns; ++k) {
+    int64_t last = -1;
+    for (int64_t q = S.rs_ptr[k] + S.sn[k].ncol; q < S.rs_ptr[k + 1]; ++q) {
+      const int64_t s = col_sn[S.rs[q]];
+      if (s != last) {
+        upd[s].push_back(k);
+        refc[k]++;
+        last = s;
+      }
+    }
+  }
+  auto panel_bytes = [&](int64_t s) { return nrow(s) * S.sn[s].ncol * value_bytes; };
+  auto compact_bytes = [&](int64_t s) {
+    const int64_t nc = S.sn[s].ncol;
+    return (nc * (nc + 1) / 2 + (nrow(s) - nc) * nc) * (value_bytes + 8);
+  };
+  int64_t panels_all = 0, factor_bytes = 0;
+  for (int64_t s = 0; s < ns; ++s) {
+    panels_all += panel_bytes(s);
+    factor_bytes += compact_bytes(s);
+  }
+  // the refcount free schedule of the left-looking factor, in postorder
+  int64_t live = 0, compact = 0, peak = 0;
+  for (int64_t s = 0; s < ns; ++s) {
+    live += panel_bytes(s);
+    for (int64_t k : upd[s])
+      if (--refc[k] == 0) {
+        live -= panel_bytes(k);
+        compact += compact_bytes(k);
+      }
+    if (refc[s] == 0) {
+      live -= panel_bytes(s);
+      compact += compact_bytes(s);
+    }
+    peak = std::max(peak, live + compact);
+  }
+  const int64_t input_bytes = S.nnz * (value_bytes + 8);
+  const int64_t scratch = (panels_all + factor_bytes) / 4 + 32000000;
+  e.panels_all_bytes = panels_all;
+  e.factor_bytes = factor_bytes;
+  e.factor_nnz = factor_bytes / std::max<int64_t>(value_bytes + 8, 1);
+  e.panel_live_peak_bytes = std::max<int64_t>(peak, 0);
+  e.transient_peak_bytes = panels_all + factor_bytes + input_bytes + scratch;
+  std::vector<uint64_t> crit(ns, 0);
+  uint64_t cp = 0, flops = 0;
+  for (int64_t s = 0; s < ns; ++s) {
+    const uint64_t nc = (uint64_t)S.sn[s].ncol, nr = (uint64_t)nrow(s);
+    const uint64_t ff = nr * nr * nc;
+    flops += ff;
+    uint64_t cmax = 0;
+    for (int64_t c : S.sn[s].children) cmax = std::max(cmax, crit[c]);
+    crit[s] = ff + cmax;
+    cp = std::max(cp, crit[s]);
+  }
+  e.factor_flops = flops;
+  e.critical_path_flops = cp;
+  int64_t width = ns ? 1 : 0;
+  for (const auto& l : S.by_level) width = std::max<int64_t>(width, (int64_t)l.size());
+  e.max_tree_width = width;
+  return e;
+}
+
 }  // namespace rslab

@@ -286,7 +286,37 @@ class MixedInfo:
 
 
 @dataclass
+class MemoryEstimate:
+    """A-priori memory / work estimate of an analysis (MemoryEstimate,
+    src/diagnostics.rs:14-53; computed as LdltSymbolic::estimate_memory,
+    src/numeric/sparse_solver.rs:561-660)."""
+    value_bytes: int
+    factor_nnz: int
+    factor_bytes: int
+    panels_all_bytes: int
+    panel_live_peak_bytes: int
+    transient_peak_bytes: int
+    factor_flops: int
+    critical_path_flops: int
+    max_tree_width: int
+
+
+@dataclass
+class StageReport:
+    """One timed stage of a factorization (StageReport, src/diagnostics.rs:220-228)."""
+    name: str
+    wall_ms: float
+    flops: int
+    bytes: int
+
+
+@dataclass
 class Diagnostics:
+    """Per-call factor diagnostics (Diagnostics, src/diagnostics.rs:235-240):
+    the reference's stages / threads / factor_nnz / estimate, plus the
+    device-side figures of this build.  `threads` is the number of
+    multiprocessors of the GPU the factor ran on (the reference reports its
+    CPU worker count)."""
     factor_ms: float
     solve_ms: float
     factor_nnz: int
@@ -294,6 +324,12 @@ class Diagnostics:
     flops_proxy: float
     n_supernodes: int
     n_levels: int
+    threads: int = 0
+    estimate: Optional[MemoryEstimate] = None
+    stages: list = field(default_factory=list)
+
+    def total_ms(self) -> float:
+        return sum(s.wall_ms for s in self.stages)
 
 
 @dataclass
@@ -353,6 +389,35 @@ class LdltSymbolic:
 
     def n_levels(self) -> int:
         return int(self.info().nlevels)
+
+    def estimate_memory(self, dtype=np.float64) -> MemoryEstimate:
+        """A-priori estimate for a scalar of `dtype` (estimate_memory::<T>)."""
+        e = N.MemoryEstimateC()
+        _check(N.lib.rslab_symbolic_estimate(self._h, np.dtype(dtype).itemsize, C.byref(e)))
+        return MemoryEstimate(int(e.value_bytes), int(e.factor_nnz), int(e.factor_bytes), int(e.panels_all_bytes),
+                              int(e.panel_live_peak_bytes), int(e.transient_peak_bytes), int(e.factor_flops),
+                              int(e.critical_path_flops), int(e.max_tree_width))
+
+    def symbolic_factor_nnz(self) -> int:
+        """Exact symbolic fill x 1.2 slack (sparse_solver.rs:550-555)."""
+        e = N.MemoryEstimateC()
+        _check(N.lib.rslab_symbolic_estimate(self._h, 8, C.byref(e)))
+        return int(e.symbolic_factor_nnz)
+
+    @classmethod
+    def tuned(cls, a: CscMatrix) -> tuple:
+        """LdltSolver::tuned (sparse_solver.rs:108-131): the default analysis,
+        then on large systems the nested-dissection bakeoff (:231-266) that
+        adopts MetisND only on a clear predicted-flops win with no regression
+        in exact fill or live-panel peak.  Returns (analysis, settings)."""
+        a.validate()
+        vals = np.asarray(a.values)
+        vb = vals.dtype.itemsize if vals.dtype in _DT else 8
+        h = C.c_void_p()
+        used = C.c_int32(0)
+        _check(N.lib.rslab_analyze_tuned(a.n, _p64(a.col_ptr), _p64(a.row_idx), vb, C.byref(h), C.byref(used)))
+        s = SolverSettings(ordering=int(used.value))
+        return cls(h, a.n, a.nnz, s), s
 
     def export(self) -> dict:
         inf = self.info()
@@ -417,7 +482,9 @@ class LdltSolver:
 
     @classmethod
     def factor(cls, a: CscMatrix) -> "LdltSolver":
-        return LdltSymbolic.analyze(a).factor(a, SolverSettings())
+        """Settings from the heuristic pick LdltSolver::tuned (sparse_solver.rs:94-97)."""
+        sym, s = LdltSymbolic.tuned(a)
+        return sym.factor(a, s)
 
     @classmethod
     def factor_with(cls, a: CscMatrix, opts: SolverSettings) -> "LdltSolver":
@@ -450,10 +517,16 @@ class LdltSolver:
         return int(nnz.value)
 
     def diagnostics(self) -> Diagnostics:
+        """Diagnostics of this factor (LdltSolver::diagnostics, sparse_solver.rs:57;
+        filled as LdltSymbolic::factor does, :692-705)."""
         i = self._info()
         si = self._sym.info()
-        return Diagnostics(i.factor_ms, i.solve_ms, -1, si.flops_model, si.flops_proxy, int(si.nsuper),
-                           int(si.nlevels))
+        nnz = self.factor_nnz()
+        entry_bytes = self.dtype.itemsize + 8
+        return Diagnostics(i.factor_ms, i.solve_ms, nnz, si.flops_model, si.flops_proxy, int(si.nsuper),
+                           int(si.nlevels), threads=int(i.multiprocessors),
+                           estimate=self._sym.estimate_memory(self.dtype),
+                           stages=[StageReport("factor", float(i.factor_ms), int(si.flops_model), nnz * entry_bytes)])
 
     def stream(self) -> int:
         return int(N.lib.rslab_factor_stream(self._h) or 0)
@@ -530,7 +603,13 @@ class MixedLdltSolver:
 
     @classmethod
     def factor(cls, a: CscMatrix) -> "MixedLdltSolver":
-        return cls.factor_with(a, SolverSettings())
+        """Factor cast(A) with the heuristic pick LdltSolver::tuned on the
+        low-precision matrix (mixed.rs:232-243)."""
+        vals = np.asarray(a.values)
+        lo = np.complex64 if np.iscomplexobj(vals) else np.float32
+        sym, s = LdltSymbolic.tuned(a.astype(lo))
+        sym.nnz = a.nnz
+        return cls.factor_with(a, s, sym=sym)
 
     @classmethod
     def factor_with(cls, a: CscMatrix, opts: SolverSettings, sym: Optional[LdltSymbolic] = None,
