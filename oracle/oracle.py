@@ -22,8 +22,8 @@ vp = C.c_void_p
 
 
 def build() -> Path:
-    src = HERE / "oracle.cpp"
-    if not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+    srcs = [HERE / "oracle.cpp", HERE / "symbolic.cpp", HERE / "build_oracle.sh"]
+    if not LIB.exists() or any(LIB.stat().st_mtime < s.stat().st_mtime for s in srcs):
         subprocess.run(["bash", str(HERE / "build_oracle.sh")], check=True, stdout=subprocess.DEVNULL)
     return LIB
 
@@ -48,6 +48,9 @@ def _load():
     lib.oracle_symv.argtypes = [C.c_int, C.c_int64, i64p, i64p, vp, vp, vp]
     lib.oracle_free.restype = None
     lib.oracle_free.argtypes = [vp]
+    lib.oracle_symbolic.restype = C.c_int64
+    lib.oracle_symbolic.argtypes = [C.c_int64, i64p, i64p, i64p, C.c_int64, C.c_int64, C.c_int64] + [i64p] * 9 + \
+        [C.POINTER(C.c_int32)]
     return lib
 
 
@@ -63,6 +66,45 @@ def lib():
 
 def _p(a):
     return a.ctypes.data_as(i64p)
+
+
+def oracle_structure(a, ordering: np.ndarray, nemin: int = 16, relax=(256, 64)) -> dict:
+    """The reference's symbolic analysis (oracle/symbolic.cpp) of the lower
+    CSC pattern of `a` for the ordering output `ordering` (new-to-old, before
+    the postorder): a dict with the keys of LdltSymbolic.export() (perm,
+    parent, col_counts, sn_first, sn_ncol, sn_nrow = row-structure heights,
+    sn_level, child_ptr, child_idx) plus `renumbered`."""
+    n = a.n
+    cp = np.ascontiguousarray(a.col_ptr, np.int64)
+    ri = np.ascontiguousarray(a.row_idx, np.int64)
+    o = np.ascontiguousarray(ordering, np.int64)
+    out = {k: np.zeros(max(n, 1), np.int64) for k in ("perm", "parent", "col_counts", "sn_first", "sn_ncol",
+                                                      "sn_nrow", "sn_level", "child_idx")}
+    out["child_ptr"] = np.zeros(n + 1, np.int64)
+    ren = C.c_int32(0)
+    rw, rr = (relax if relax is not None else (0, 0))
+    ns = lib().oracle_symbolic(n, _p(cp), _p(ri), _p(o), nemin, rw, rr, _p(out["perm"]), _p(out["parent"]),
+                               _p(out["col_counts"]), _p(out["sn_first"]), _p(out["sn_ncol"]), _p(out["sn_nrow"]),
+                               _p(out["sn_level"]), _p(out["child_ptr"]), _p(out["child_idx"]), C.byref(ren))
+    for k in ("perm", "parent", "col_counts"):
+        out[k] = out[k][:n]
+    for k in ("sn_first", "sn_ncol", "sn_nrow", "sn_level"):
+        out[k] = out[k][:ns]
+    out["child_ptr"] = out["child_ptr"][: ns + 1]
+    out["child_idx"] = out["child_idx"][: int(out["child_ptr"][-1])]
+    out["renumbered"] = bool(ren.value)
+    return out
+
+
+def supernode_parent(ex: dict) -> np.ndarray:
+    """Parent supernode of every supernode (-1 for roots) from a structure
+    dict's child lists (their order is a scheduling choice, the sets are not)."""
+    ns = len(ex["sn_first"])
+    par = np.full(ns, -1, np.int64)
+    cp, ci = ex["child_ptr"], ex["child_idx"]
+    for s in range(ns):
+        par[ci[cp[s]:cp[s + 1]]] = s
+    return par
 
 
 @dataclass
