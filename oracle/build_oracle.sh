@@ -6,7 +6,7 @@
 set -euo pipefail
 here="$(cd "$(dirname "$0")" && pwd)"
 mkdir -p "$here/_build"
-g++ -O2 -std=c++17 -march=x86-64-v3 -ffp-contract=off -fopenmp -fPIC -shared \
+g++ -O3 -std=c++17 -march=x86-64-v3 -ffp-contract=off -fopenmp -fPIC -shared \
     "$here/oracle.cpp" "$here/symbolic.cpp" -o "$here/_build/liboracle.so.tmp"
 mv "$here/_build/liboracle.so.tmp" "$here/_build/liboracle.so"
 echo "$here/_build/liboracle.so"

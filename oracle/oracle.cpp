@@ -27,7 +27,18 @@
 // norm = hypot).  The reference's Schur GEMMs run in the `gemm` crate 0.18.2
 // whose per-element rounding is shape dependent; the oracle computes the same
 // products with plain loops, so GEMM-level results agree to rounding only.
+// Timing mode (oracle_set_parallel): the same factor with the two Schur
+// products (cmod and the deferred in-panel update) computed by a BLAS GEMM
+// (OpenBLAS, loaded at run time) and the assembly forest scheduled level by
+// level with independent supernodes on different threads, as the reference
+// runs sibling subtrees concurrently on rayon and its GEMMs in the gemm crate
+// (multifrontal_ldlt.rs:847-866, 3264-3297).  Its results equal the exact
+// mode's to rounding (the GEMM summation order differs); it is the timed CPU
+// baseline, the exact mode is the checker.
 // Build: oracle/build_oracle.sh (g++ -O2 -ffp-contract=off -fopenmp).
+#include <dlfcn.h>
+#include <omp.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -305,7 +316,49 @@ struct FactorOpts {
   bool drop = false;
   double drop_tol = 0;
   int64_t panel_nb = 64;
+  bool fast = false;  // timing mode: BLAS products + level-parallel schedule
 };
+
+// CBLAS of an ILP64 OpenBLAS (64-bit dimensions), resolved by name from the
+// library path given to oracle_set_parallel.
+struct Blas {
+  using real_gemm_d = void (*)(int, int, int, int64_t, int64_t, int64_t, double, const double*, int64_t,
+                               const double*, int64_t, double, double*, int64_t);
+  using real_gemm_s = void (*)(int, int, int, int64_t, int64_t, int64_t, float, const float*, int64_t,
+                               const float*, int64_t, float, float*, int64_t);
+  using cplx_gemm = void (*)(int, int, int, int64_t, int64_t, int64_t, const void*, const void*, int64_t,
+                             const void*, int64_t, const void*, void*, int64_t);
+  real_gemm_d dgemm = nullptr;
+  real_gemm_s sgemm = nullptr;
+  cplx_gemm zgemm = nullptr, cgemm = nullptr;
+  void (*set_threads)(int) = nullptr;
+  int threads = 1;
+  bool ok() const { return dgemm && sgemm && zgemm && cgemm && set_threads; }
+};
+static Blas g_blas;
+static bool g_fast = false;
+
+constexpr int kColMajor = 102, kNoTrans = 111, kTrans = 112;
+
+// C = A B^T, A m x k (lda), B n x k (ldb), C m x n (ldc), column-major.
+inline void gemm_nt(int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B, int64_t ldb,
+                    double* C, int64_t ldc) {
+  g_blas.dgemm(kColMajor, kNoTrans, kTrans, m, n, k, 1.0, A, lda, B, ldb, 0.0, C, ldc);
+}
+inline void gemm_nt(int64_t m, int64_t n, int64_t k, const float* A, int64_t lda, const float* B, int64_t ldb,
+                    float* C, int64_t ldc) {
+  g_blas.sgemm(kColMajor, kNoTrans, kTrans, m, n, k, 1.0f, A, lda, B, ldb, 0.0f, C, ldc);
+}
+inline void gemm_nt(int64_t m, int64_t n, int64_t k, const Cx<double>* A, int64_t lda, const Cx<double>* B,
+                    int64_t ldb, Cx<double>* C, int64_t ldc) {
+  const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+  g_blas.zgemm(kColMajor, kNoTrans, kTrans, m, n, k, one, A, lda, B, ldb, zero, C, ldc);
+}
+inline void gemm_nt(int64_t m, int64_t n, int64_t k, const Cx<float>* A, int64_t lda, const Cx<float>* B,
+                    int64_t ldb, Cx<float>* C, int64_t ldc) {
+  const float one[2] = {1.0f, 0.0f}, zero[2] = {0.0f, 0.0f};
+  g_blas.cgemm(kColMajor, kNoTrans, kTrans, m, n, k, one, A, lda, B, ldb, zero, C, ldc);
+}
 
 template <typename T>
 struct Panel {
@@ -448,7 +501,22 @@ int cdiv(Panel<T>& P, int64_t nrow, int64_t ncol, const FactorOpts& o, int64_t& 
         k += 2;
       }
     }
-    if (nrow > ke) apply_bk_panel_trailing(panel.data(), nrow, kb, ke, d, dsub, two, deep, snap, nb, ke, nrow);
+    if (nrow > ke) {
+      // rows are replayed independently: as the reference does above
+      // deep * pw^2 >= 8e6 (DEFAULT_PAR_CDIV, gemm_tuning.rs:22;
+      // multifrontal_ldlt.rs:3022-3056), one contiguous chunk of rows per
+      // thread gives the same values as one pass
+      const int64_t deep_rows = nrow - ke, pw = ke - kb;
+      const int64_t nth = omp_get_max_threads();
+      const bool par = o.fast && deep_rows * pw * pw >= 8000000 && nth > 1 && !omp_in_parallel();
+      const int64_t cs = par ? (deep_rows + nth - 1) / nth : deep_rows;
+      const int64_t chunks = (deep_rows + cs - 1) / cs;
+#pragma omp parallel for schedule(static, 1) if (par)
+      for (int64_t c = 0; c < chunks; ++c) {
+        const int64_t r0 = ke + c * cs, r1 = std::min<int64_t>(r0 + cs, nrow);
+        apply_bk_panel_trailing(panel.data(), nrow, kb, ke, d, dsub, two, deep, snap, nb, r0, r1);
+      }
+    }
     // Deferred panel Schur: panel[ke.., ke..ncol] -= L21 D R^T (lower part).
     int64_t pw = ke - kb, cw = ncol - ke, mt = nrow - ke;
     if (pw > 0 && cw > 0 && mt > 0) {
@@ -474,6 +542,16 @@ int cdiv(Panel<T>& P, int64_t nrow, int64_t ncol, const FactorOpts& o, int64_t& 
       }
       // tmp = G L21^T (FMA accumulation in ascending q), then the lower part
       // of tmp is subtracted from the panel.
+      if (o.fast) {
+        std::vector<T> tmp(mt * cw);
+        gemm_nt(mt, cw, pw, g.data(), mt, l21.data(), mt, tmp.data(), mt);
+        for (int64_t c2 = 0; c2 < cw; ++c2) {
+          T* col = panel.data() + (ke + c2) * nrow + ke;
+          for (int64_t rr = c2; rr < mt; ++rr) col[rr] = col[rr] - tmp[rr + c2 * mt];
+        }
+        kb = ke;
+        continue;
+      }
 #pragma omp parallel for schedule(dynamic, 16) if (mt * cw * pw > 4000000)
       for (int64_t c2 = 0; c2 < cw; ++c2) {
         T* col = panel.data() + (ke + c2) * nrow + ke;
@@ -555,8 +633,6 @@ int factor_left_looking(const SymIn& sym, const Csc<T>& a, const FactorOpts& o, 
     }
   }
   std::vector<Panel<T>> store(ns);
-  std::vector<int64_t> gloc(n, -1);
-  int64_t nperturbed = 0;
   std::vector<int64_t> e_offset(ns, 0);
   {
     int64_t acc = 0;
@@ -571,8 +647,12 @@ int factor_left_looking(const SymIn& sym, const Csc<T>& a, const FactorOpts& o, 
   out.dsub.assign(n, S<T>::zero());
   out.two.assign(n, 0);
   std::vector<int64_t> e_of_g(n, -1);
-  // Supernodes are in postorder: sequential 0..ns is a valid schedule.
-  for (int64_t s = 0; s < ns; ++s) {
+  // per-supernode results, summed in supernode order at the end
+  std::vector<int64_t> sn_pert(ns, 0), sn_ipos(ns, 0), sn_ineg(ns, 0), sn_izero(ns, 0);
+  // One supernode: assembly, cmod from its updaters, cdiv, emit maps and
+  // inertia.  `gloc` (global row -> panel row, -1 elsewhere) is the caller's
+  // scratch; updaters are complete when this runs.
+  auto process = [&](int64_t s, std::vector<int64_t>& gloc) -> int {
     const int64_t first = sym.first[s], ncol = sym.ncol[s], nrow = (int64_t)rs[s].size();
     Panel<T>& P = store[s];
     P.p.assign(nrow * ncol, S<T>::zero());
@@ -612,6 +692,23 @@ int factor_left_looking(const SymIn& sym, const Csc<T>& a, const FactorOpts& o, 
           ck += 1;
         }
       }
+      if (o.fast) {
+        // W = L_k[p0 + c0 .., :] G[c0 .. c0 + cb, :]^T by BLAS, 512 target
+        // columns at a time, then the rows r >= c are scattered.
+        for (int64_t c0 = 0; c0 < npk; c0 += 512) {
+          const int64_t cb = std::min<int64_t>(512, npk - c0), m = nok - p0 - c0;
+          std::vector<T> W(m * cb);
+          gemm_nt(m, cb, nck, K.p.data() + nck + p0 + c0, nrk, vd.data() + c0, npk, W.data(), m);
+          for (int64_t c = 0; c < cb; ++c) {
+            T* dst = P.p.data() + (ok[p0 + c0 + c] - first) * nrow;
+            for (int64_t r = c; r < m; ++r) {
+              const int64_t tr = gloc[ok[p0 + c0 + r]];
+              dst[tr] = dst[tr] - W[r + c * m];
+            }
+          }
+        }
+        continue;
+      }
       // U[r, c] = sum_q L_k[p0 + r, q] * G[c, q] (FMA accumulation in
       // ascending q, as the gemm crate's FMA kernels); rows r >= c only.
 #pragma omp parallel for schedule(dynamic, 8) if ((nok - p0) * npk * nck > 4000000)
@@ -626,7 +723,7 @@ int factor_left_looking(const SymIn& sym, const Csc<T>& a, const FactorOpts& o, 
         }
       }
     }
-    int st = cdiv(P, nrow, ncol, o, nperturbed);
+    int st = cdiv(P, nrow, ncol, o, sn_pert[s]);
     for (int64_t li = 0; li < nrow; ++li) gloc[rs[s][li]] = -1;
     if (st != OK) return st;
     // Emit maps + inertia.
@@ -648,36 +745,83 @@ int factor_left_looking(const SymIn& sym, const Csc<T>& a, const FactorOpts& o, 
         double det_r = S<T>::real(P.d[pp] * P.d[pp + 1] - P.dsub[pp] * P.dsub[pp]);
         double tr_r = S<T>::real(P.d[pp] + P.d[pp + 1]);
         if (det_r < 0.0) {
-          out.ipos++;
-          out.ineg++;
+          sn_ipos[s]++;
+          sn_ineg[s]++;
         } else if (det_r > 0.0) {
           if (tr_r >= 0.0)
-            out.ipos += 2;
+            sn_ipos[s] += 2;
           else
-            out.ineg += 2;
+            sn_ineg[s] += 2;
         } else {
-          out.izero++;
+          sn_izero[s]++;
           if (tr_r >= 0.0)
-            out.ipos++;
+            sn_ipos[s]++;
           else
-            out.ineg++;
+            sn_ineg[s]++;
         }
         pp += 2;
       } else {
         double r = S<T>::real(P.d[pp]);
         if (r > 0.0)
-          out.ipos++;
+          sn_ipos[s]++;
         else if (r < 0.0)
-          out.ineg++;
+          sn_ineg[s]++;
         else
-          out.izero++;
+          sn_izero[s]++;
         pp += 1;
       }
     }
+    return OK;
+  };
+  if (!o.fast) {
+    // Supernodes are in postorder: sequential 0..ns is a valid schedule.
+    std::vector<int64_t> gloc(n, -1);
+    for (int64_t s = 0; s < ns; ++s) {
+      const int st = process(s, gloc);
+      if (st != OK) return st;
+    }
+  } else {
+    // Assembly-tree levels (children before parents); a level's supernodes
+    // are independent.  Wide levels: one supernode per thread, one-thread
+    // BLAS; narrow levels: one supernode at a time, all threads in BLAS.
+    std::vector<int64_t> level(ns, 0);
+    int64_t nlev = 0;
+    for (int64_t s = 0; s < ns; ++s) {
+      for (int64_t c : sym.children[s]) level[s] = std::max(level[s], level[c] + 1);
+      nlev = std::max(nlev, level[s] + 1);
+    }
+    std::vector<std::vector<int64_t>> by_level(nlev);
+    for (int64_t s = 0; s < ns; ++s) by_level[level[s]].push_back(s);
+    const int nth = omp_get_max_threads();
+    std::vector<std::vector<int64_t>> glocs(nth, std::vector<int64_t>(n, -1));
+    std::vector<int> sn_st(ns, OK);
+    for (const auto& L : by_level) {
+      if ((int64_t)L.size() >= nth && nth > 1) {
+        g_blas.set_threads(1);
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int64_t i = 0; i < (int64_t)L.size(); ++i) sn_st[L[i]] = process(L[i], glocs[omp_get_thread_num()]);
+      } else {
+        g_blas.set_threads(g_blas.threads);
+        for (int64_t s : L) sn_st[s] = process(s, glocs[0]);
+      }
+      for (int64_t s : L)
+        if (sn_st[s] != OK) return sn_st[s];
+    }
+    g_blas.set_threads(g_blas.threads);
   }
-  // Emit compact L (every row's e index is known once all panels are done).
-  out.lcp.assign(1, 0);
+  int64_t nperturbed = 0;
   for (int64_t s = 0; s < ns; ++s) {
+    nperturbed += sn_pert[s];
+    out.ipos += sn_ipos[s];
+    out.ineg += sn_ineg[s];
+    out.izero += sn_izero[s];
+  }
+  // Emit compact L (every row's e index is known once all panels are done):
+  // each supernode's columns into its own buffer (in parallel in timing
+  // mode), then concatenated in supernode order.
+  std::vector<std::vector<int64_t>> sn_ri(ns), sn_cnt(ns);
+  std::vector<std::vector<T>> sn_v(ns);
+  auto emit = [&](int64_t s) {
     const Panel<T>& P = store[s];
     const int64_t ncol = sym.ncol[s], nrow = (int64_t)rs[s].size();
     std::vector<std::pair<int64_t, T>> col;
@@ -702,11 +846,25 @@ int factor_left_looking(const SymIn& sym, const Csc<T>& a, const FactorOpts& o, 
       }
       std::stable_sort(col.begin(), col.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
       for (auto& x : col) {
-        out.lri.push_back(x.first);
-        out.lv.push_back(x.second);
+        sn_ri[s].push_back(x.first);
+        sn_v[s].push_back(x.second);
       }
-      out.lcp.push_back((int64_t)out.lri.size());
+      sn_cnt[s].push_back((int64_t)col.size());
     }
+  };
+#pragma omp parallel for schedule(dynamic, 4) if (o.fast)
+  for (int64_t s = 0; s < ns; ++s) emit(s);
+  out.lcp.assign(1, 0);
+  int64_t total = 0;
+  for (int64_t s = 0; s < ns; ++s) total += (int64_t)sn_ri[s].size();
+  out.lri.reserve(total);
+  out.lv.reserve(total);
+  for (int64_t s = 0; s < ns; ++s) {
+    out.lri.insert(out.lri.end(), sn_ri[s].begin(), sn_ri[s].end());
+    out.lv.insert(out.lv.end(), sn_v[s].begin(), sn_v[s].end());
+    for (int64_t c : sn_cnt[s]) out.lcp.push_back(out.lcp.back() + c);
+    std::vector<int64_t>().swap(sn_ri[s]);
+    std::vector<T>().swap(sn_v[s]);
   }
   out.n_perturbed = nperturbed;
   return OK;
@@ -761,6 +919,35 @@ int solve_block(const Factors<T>& f, const T* b, int64_t nrhs, T* x) {
   return OK;
 }
 
+// solve_ldlt_many (src/dense/ldlt_generic.rs:564-614): with >= 8 columns and
+// n * nrhs >= 2^18 the columns are split into one contiguous chunk per
+// thread, each solved by solve_block on a compact copy; every column sees the
+// same operations as in one block solve, so the result is bit-identical.
+template <typename T>
+int solve_many(const Factors<T>& f, const T* b, int64_t nrhs, T* x) {
+  const int64_t n = f.n;
+  const int nth = omp_get_max_threads();
+  if (nrhs < 8 || n * nrhs < (1 << 18) || nth < 2) return solve_block(f, b, nrhs, x);
+  const int64_t nch = std::min<int64_t>(nth, nrhs), w0 = (nrhs + nch - 1) / nch;
+  int bad = OK;
+#pragma omp parallel for schedule(static, 1)
+  for (int64_t t = 0; t < nch; ++t) {
+    const int64_t c0 = t * w0, c1 = std::min(nrhs, c0 + w0), w = c1 - c0;
+    if (w <= 0) continue;
+    std::vector<T> sub(n * w), xs(n * w);
+    for (int64_t i = 0; i < n; ++i)
+      for (int64_t c = 0; c < w; ++c) sub[i * w + c] = b[i * nrhs + c0 + c];
+    const int st = solve_block(f, sub.data(), w, xs.data());
+    if (st != OK) {
+#pragma omp critical
+      bad = st;
+    }
+    for (int64_t i = 0; i < n; ++i)
+      for (int64_t c = 0; c < w; ++c) x[i * nrhs + c0 + c] = xs[i * w + c];
+  }
+  return bad;
+}
+
 // LdltSolver::solve_many: scale, solve, scale back.
 template <typename T>
 int solver_solve(const OracleFactor<T>& F, const T* b, int64_t nrhs, T* x) {
@@ -768,7 +955,7 @@ int solver_solve(const OracleFactor<T>& F, const T* b, int64_t nrhs, T* x) {
   std::vector<T> bh(b, b + n * nrhs);
   for (int64_t i = 0; i < n; ++i)
     for (int64_t c = 0; c < nrhs; ++c) bh[i * nrhs + c] = bh[i * nrhs + c] * S<T>::from_real(F.scale[i]);
-  int st = solve_block(F.f, bh.data(), nrhs, x);
+  int st = solve_many(F.f, bh.data(), nrhs, x);
   if (st != OK) return st;
   for (int64_t i = 0; i < n; ++i)
     for (int64_t c = 0; c < nrhs; ++c) x[i * nrhs + c] = x[i * nrhs + c] * S<T>::from_real(F.scale[i]);
@@ -1011,6 +1198,31 @@ using namespace orc;
 
 extern "C" {
 
+// Timing mode on (fast = 1: BLAS products from the ILP64 OpenBLAS at
+// blas_path, `threads` OpenMP threads and BLAS threads) or off (fast = 0:
+// the exact plain-loop checker).  Returns 0, or -1 if the BLAS did not load.
+int oracle_set_parallel(int fast, const char* blas_path, int threads) {
+  if (threads > 0) omp_set_num_threads(threads);
+  if (!fast) {
+    g_fast = false;
+    return 0;
+  }
+  if (!g_blas.ok()) {
+    void* h = dlopen(blas_path, RTLD_NOW | RTLD_LOCAL);
+    if (!h) return -1;
+    g_blas.dgemm = (Blas::real_gemm_d)dlsym(h, "scipy_cblas_dgemm64_");
+    g_blas.sgemm = (Blas::real_gemm_s)dlsym(h, "scipy_cblas_sgemm64_");
+    g_blas.zgemm = (Blas::cplx_gemm)dlsym(h, "scipy_cblas_zgemm64_");
+    g_blas.cgemm = (Blas::cplx_gemm)dlsym(h, "scipy_cblas_cgemm64_");
+    g_blas.set_threads = (void (*)(int))dlsym(h, "scipy_openblas_set_num_threads64_");
+    if (!g_blas.ok()) return -1;
+  }
+  g_blas.threads = threads > 0 ? threads : omp_get_max_threads();
+  g_blas.set_threads(g_blas.threads);
+  g_fast = true;
+  return 0;
+}
+
 // Factor `A` (lower CSC, values of dtype) with the given symbolic structure.
 void* oracle_factor(int dtype, int64_t n, const int64_t* cp, const int64_t* ri, const void* vals, const int64_t* perm,
                     int64_t ns, const int64_t* sn_first, const int64_t* sn_ncol, const int64_t* ch_ptr,
@@ -1036,6 +1248,7 @@ void* oracle_factor(int dtype, int64_t n, const int64_t* cp, const int64_t* ri, 
     o.drop_tol = drop_tol;
   }
   o.panel_nb = std::max<int64_t>(panel_nb, 8);
+  o.fast = g_fast;
   auto* h = new Handle{dtype, nullptr};
   int st = OK;
   switch (dtype) {

@@ -48,6 +48,8 @@ def _load():
     lib.oracle_symv.argtypes = [C.c_int, C.c_int64, i64p, i64p, vp, vp, vp]
     lib.oracle_free.restype = None
     lib.oracle_free.argtypes = [vp]
+    lib.oracle_set_parallel.restype = C.c_int
+    lib.oracle_set_parallel.argtypes = [C.c_int, C.c_char_p, C.c_int]
     lib.oracle_symbolic.restype = C.c_int64
     lib.oracle_symbolic.argtypes = [C.c_int64, i64p, i64p, i64p, C.c_int64, C.c_int64, C.c_int64] + [i64p] * 9 + \
         [C.POINTER(C.c_int32)]
@@ -66,6 +68,26 @@ def lib():
 
 def _p(a):
     return a.ctypes.data_as(i64p)
+
+
+def openblas_path() -> str:
+    """The ILP64 OpenBLAS that numpy ships (numpy.libs/libscipy_openblas64_*.so)."""
+    import glob
+    import os
+
+    d = os.path.join(os.path.dirname(os.path.dirname(np.__file__)), "numpy.libs")
+    hits = sorted(glob.glob(os.path.join(d, "libscipy_openblas64_*.so")))
+    if not hits:
+        raise RuntimeError(f"no libscipy_openblas64_*.so under {d}")
+    return hits[0]
+
+
+def set_parallel(fast: bool, threads: int = 0) -> None:
+    """Timing mode (BLAS products, level-parallel schedule) on or off; off is
+    the exact checker.  threads 0 = all cores."""
+    path = openblas_path().encode() if fast else b""
+    if lib().oracle_set_parallel(int(fast), path, int(threads)) != 0:
+        raise RuntimeError("oracle: OpenBLAS did not load")
 
 
 def oracle_structure(a, ordering: np.ndarray, nemin: int = 16, relax=(256, 64)) -> dict:
