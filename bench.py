@@ -51,10 +51,12 @@ def parse():
     p.add_argument("--target", type=float, default=1e-14)
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--workload", default="helmholtz", choices=["helmholtz", "sweep", "tiers"],
+    p.add_argument("--workload", default="helmholtz", choices=["helmholtz", "sweep", "tiers", "batch"],
                    help="helmholtz: the 64^3 Helmholtz factor+solve step (default); sweep: the "
                         "same-pattern frequency sweep, 48^3 27-point K - w^2 M + i w C, 64 frequencies; "
-                        "tiers: the learned precision tier on the held-out 80^3 27-point complex Helmholtz")
+                        "tiers: the learned precision tier on the held-out 80^3 27-point complex Helmholtz; "
+                        "batch: 512 uneven shifted 3D Laplacians (sides 12-40) factored and solved together")
+    p.add_argument("--batch-count", type=int, default=512)
     p.add_argument("--ordering", default="tuned", choices=["tuned", "amd", "metis"],
                    help="fill-reducing ordering of the helmholtz workload: tuned = the default pick of "
                         "LdltSolver::factor (nested-dissection bakeoff; MetisND on this matrix), amd, metis")
@@ -594,6 +596,145 @@ def run_tiers(args, ws, rank, local):
         dist.destroy_process_group()
 
 
+def run_batch(args, ws, rank, local):
+    """Batched uneven systems: 512 real symmetric indefinite 3D 7-point
+    shifted Laplacians, cube sides U{12..40} (seed 2), shift 0.1 lambda_max,
+    4 right-hand sides each (U[-1, 1), seed 2), every (system, column)
+    certified at normwise backward error <= 1e-14.  One analysis handle holds
+    every system (one launch per assembly-tree level and block index covers
+    that level of every system); a step is the f32 refactor with tensor-core
+    descendant updates + the FP64 refinement ladder.  The plain FP64 factor +
+    solve of the same batch is timed for the ratio.  Multi-GPU: the systems are
+    split over ranks by weight (n^2), no data exchange."""
+    import ctypes as C
+
+    import torch
+
+    from rslab_b200 import CscMatrix, MixedLdltSolver, SolverSettings, matgen
+    from rslab_b200 import _native as N
+    from rslab_b200.batch import BatchSystems, analyze_batch, mixed_batch_result, shard_by_weight
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    sides = matgen.c3_sides(args.batch_count, 2)
+    mine = shard_by_weight([float(s) ** 6 for s in sides], ws)[rank]
+    mats = [matgen.c3_matrix(sides[i]) for i in mine]
+    batch = BatchSystems(mats)
+    nrhs = 4
+    t0 = time.perf_counter()
+    sym = analyze_batch(batch)
+    t_an = time.perf_counter() - t0
+    info = sym.info()
+    flops = info.flops_model
+    a = batch.as_matrix()
+    b = matgen.uniform_rhs(batch.total_n, nrhs, 2)
+    st = SolverSettings()
+    vals_d = torch.from_numpy(np.ascontiguousarray(a.values)).to(dev)
+    b_d = torch.from_numpy(np.ascontiguousarray(b)).to(dev)
+    x_d = torch.empty_like(b_d)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def timed(fn, strm, steps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        barrier(ws)
+        tot, last = 0.0, None
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(strm)
+            last = fn()
+            e1.record(strm)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        barrier(ws)
+        return tot / steps, last
+
+    mixed = MixedLdltSolver.factor_with(a, st, sym=sym)
+
+    def mixed_step():
+        rc = N.lib.rslab_refactor(mixed._h, C.c_void_p(vals_d.data_ptr()), 1)
+        assert rc == 0, N.last_error()
+        inf = N.MixedInfoC()
+        rc = N.lib.rslab_mixed_solve(mixed._h, C.c_void_p(b_d.data_ptr()), nrhs, args.target,
+                                     C.c_void_p(x_d.data_ptr()), 1, C.byref(inf))
+        assert rc == 0, N.last_error()
+        return inf
+
+    clk = ClockSampler(local)
+    clk.start()
+    ms, minfo = timed(mixed_step, torch.cuda.ExternalStream(mixed.stream()), args.steps, args.warmup)
+    clocks = clk.stop()
+    ms = allmax(ms, ws)
+    from rslab_b200.solver import MixedInfo
+    res = mixed_batch_result(mixed, batch.count, nrhs, args.target,
+                             MixedInfo(int(minfo.ir_iters), int(minfo.gmres_iters), float(minfo.backward_error),
+                                       bool(minfo.certified)))
+    # end to end through the public API with page-locked host buffers
+    def pinned(arr):
+        t = torch.empty(arr.shape, dtype=torch.float64, pin_memory=True)
+        v = t.numpy()
+        v[...] = arr
+        return t, v
+    _pa, vals_h = pinned(np.ascontiguousarray(a.values))
+    _pb, b_h = pinned(np.ascontiguousarray(b))
+    _px, x_h = pinned(np.zeros_like(np.ascontiguousarray(b)))
+    a_h = CscMatrix(a.n, a.col_ptr, a.row_idx, vals_h)
+    te = []
+    for it in range(2):
+        t1 = time.perf_counter()
+        mixed.refactor(a_h)
+        x_h, inf_h = mixed.solve_to(a_h, b_h, args.target, out=x_h)
+        if it:
+            te.append(time.perf_counter() - t1)
+    e2e_s = allmax(float(np.mean(te)), ws)
+    del mixed
+    torch.cuda.synchronize()
+    out64 = None
+    if not args.no_fp64:
+        f64 = sym.factor(a, st)
+
+        def fp64_step():
+            rc = N.lib.rslab_refactor(f64._h, C.c_void_p(vals_d.data_ptr()), 1)
+            assert rc == 0, N.last_error()
+            rc = N.lib.rslab_solve(f64._h, C.c_void_p(b_d.data_ptr()), nrhs, C.c_void_p(x_d.data_ptr()), 1)
+            assert rc == 0, N.last_error()
+
+        ms64, _ = timed(fp64_step, torch.cuda.ExternalStream(f64.stream()), max(1, args.steps // 2), 1)
+        ms64 = allmax(ms64, ws)
+        out64 = {"ms_per_step": ms64, "gflops": flops / (ms64 * 1e-3) / 1e9 * ws,
+                 "backward_error_no_ir": host_backward_error(a, x_d.cpu().numpy(), b)}
+        del f64
+    if rank == 0:
+        line = {
+            "metric": "LDLT factor+solve GFLOP/s at bwd err <= 1e-14 (mixed/batched vs FP64 GPU)",
+            "value": flops / (ms * 1e-3) / 1e9 * ws, "unit": "GFLOP/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32 factor / f64 refinement", "data": "synthetic",
+            "config": {"workload": f"batch{args.batch_count}_laplacian3d_sides12-40_f64_nrhs{nrhs}",
+                       "systems": batch.count, "total_n": batch.total_n, "nnz_lower": a.nnz, "nrhs": nrhs,
+                       "ordering": "AMD", "target_backward_error": args.target, "model_flops": flops,
+                       "supernodes": int(info.nsuper), "levels": int(info.nlevels),
+                       "factor_launches": int(info.n_factor_launches), "analysis_s": t_an,
+                       "parallelism": f"systems split over {ws} rank(s) by weight",
+                       "l2": "flushed between steps (256 MB write)"},
+            "mixed": {"certified_units": int(res.certified.sum()), "units": int(res.certified.size),
+                      "max_backward_error": float(res.backward_error.max()), "ir_iters": int(minfo.ir_iters),
+                      "gmres_iters": int(minfo.gmres_iters)},
+            "fp64_gpu": out64,
+            "e2e": {"value": flops / e2e_s / 1e9 * ws, "unit": "GFLOP/s", "seconds_per_step": e2e_s,
+                    "h2d_bytes_per_step": int(a.values.nbytes + b.nbytes), "d2h_bytes_per_step": int(b.nbytes),
+                    "certified": bool(inf_h.certified), "host_buffers": "page-locked (torch pin_memory) numpy views"},
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init(args)
@@ -605,6 +746,9 @@ def main():
         return
     if args.workload == "tiers":
         run_tiers(args, ws, rank, local)
+        return
+    if args.workload == "batch":
+        run_batch(args, ws, rank, local)
         return
     import torch
 

@@ -27,6 +27,7 @@
  *                        (src/numeric/sparse_solver.rs:81,72,57)
  *   rslab_export_factors LdltFactors (src/dense/ldlt_generic.rs:31-66), the
  *                        factor_numeric return value
+ *   rslab_compress_factors / rslab_cfac_*  CompressedLdltFactors (src/dense/ldlt_generic.rs:434-536)
  *   rslab_amd_order      rslab_amd::amd_order (crates/rslab-amd/src/lib.rs:66)
  *   rslab_metis_order    rslab_metis::metis_order_full (crates/rslab-metis/src/lib.rs:204)
  */
@@ -253,6 +254,22 @@ int rslab_export_factors(const rslab_fac_handle* fac, int64_t* l_col_ptr, int64_
                          void* d_diag, void* d_subdiag, uint8_t* two_by_two, int64_t* perm, double* scale,
                          int64_t* nnz_out);
 void rslab_free_factor(rslab_fac_handle* fac);
+
+/* CompressedLdltFactors (src/dense/ldlt_generic.rs:434-536): the factor in
+ * the LdltFactors layout with uint32 index arrays and pivot permutation, on
+ * the host, and its single-right-hand-side solve with the reference's
+ * solve_ldlt expressions (bit-identical to it on the same factors; like the
+ * reference container it solves with the factors of the equilibrated matrix,
+ * A_hat = S A S, S the rslab_export_factors scale).  rslab_compress_factors
+ * returns RSLAB_INVALID_INPUT when n or nnz(L) does not fit 32 bits (the
+ * reference's from_factors returns None).  index_bytes = 4 (n + 1 + nnz + n). */
+typedef struct rslab_cfac_handle rslab_cfac_handle;
+int rslab_compress_factors(const rslab_fac_handle* fac, rslab_cfac_handle** out);
+int rslab_cfac_info(const rslab_cfac_handle* c, int64_t* n, int64_t* nnz, int64_t* index_bytes, int32_t* dtype);
+int rslab_cfac_export(const rslab_cfac_handle* c, uint32_t* l_col_ptr, uint32_t* l_row_idx, void* l_values,
+                      void* d_diag, void* d_subdiag, uint8_t* two_by_two, uint32_t* perm);
+int rslab_cfac_solve(const rslab_cfac_handle* c, const void* rhs, void* x);
+void rslab_free_cfac(rslab_cfac_handle* c);
 
 /* Mixed precision: factor cast(A) in f32/c32, refine against the f64/c64 A. */
 int rslab_mixed_factor(rslab_sym_handle* sym, int dtype_hi, const void* values_hi, int values_on_device,

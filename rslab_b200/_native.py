@@ -130,6 +130,12 @@ SIGNATURES = {
     "rslab_rng_units": (C.c_uint64, [C.c_uint64, C.c_int64, C.POINTER(C.c_double)]),
     "rslab_amd_order": (C.c_int, [C.c_int64, i64p, i64p, i64p, C.POINTER(C.c_double)]),
     "rslab_metis_order": (C.c_int, [C.c_int64, i64p, i64p, C.c_uint64, C.c_int, C.c_int64, i64p]),
+    "rslab_compress_factors": (C.c_int, [vp, C.POINTER(vp)]),
+    "rslab_cfac_info": (C.c_int, [vp, i64p, i64p, i64p, i32p]),
+    "rslab_cfac_export": (C.c_int, [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), vp, vp, vp,
+                                    C.POINTER(C.c_uint8), C.POINTER(C.c_uint32)]),
+    "rslab_cfac_solve": (C.c_int, [vp, vp, vp]),
+    "rslab_free_cfac": (None, [vp]),
     "rslab_panel_factor_noalloc": (C.c_int, [C.c_int, vp, C.c_int64, C.c_int64, C.c_int64, vp, vp, vp, vp, vp,
                                              vp]),
 }

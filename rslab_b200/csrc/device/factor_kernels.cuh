@@ -251,20 +251,46 @@ __device__ __forceinline__ int lower_bound_i(const int* __restrict__ a, int lo, 
 // [r0, r0+64) x cols [c0, c0+64) of s's panel.  The pairs, precomputed at
 // analysis, list in update-list order every descendant k whose update lands
 // in the tile: (k, a, q0, nr << 16 | nc) = k's off-diagonal rows [a, a+nr)
-// times its rows [q0, q0+nc) (the tile's columns).  No searches at run time.
+// times its rows [q0, q0+nc) (the tile's columns).  No searches at run time
+// beyond the tile-local row positions.
+//
+// Per pair the product U = L_k[a.., :] G_k[q0.., :]^T (G_k = L21_k D_k,
+// formed once per updater by k_make_g with ld_G's arithmetic) runs in the
+// updater's row space: operands are contiguous column runs of k's panel and
+// of G_k, staged by cp.async into two shared-memory stages (the next chunk,
+// possibly of the next pair, loads while the current one is multiplied).
+// 128 threads, warp w owns rows 16w..16w+15 of the pair, each thread an 8 x 4
+// register micro-tile (8 consecutive rows, columns cx + 16 j: conflict-free
+// shared-memory reads); warps whose rows lie past nr skip the arithmetic.
+// Every product is one explicit FMA per column t in ascending t, then
+// subtracted from the tile held in shared memory through the pair's row /
+// column maps (rows r >= column c in k's ordering only): the same operations
+// in the same order as the oracle, so the result is bit-identical to it.
 // ---------------------------------------------------------------------------
+constexpr int CM_NT = 128;
+template <typename T> struct CmChunk { static constexpr int v = 16; };
+template <> struct CmChunk<c64> { static constexpr int v = 8; };
+
+// Shared memory of k_cmod: the tile, two operand stages, two row / column
+// maps and the tile's row structure.
 template <typename T>
-__global__ void __launch_bounds__(TPB) k_cmod(FactorArgs fa, const int4* __restrict__ tasks,
-                                              const int4* __restrict__ pairs) {
+__host__ __device__ constexpr size_t smem_cmod_bytes() {
+  return (size_t)TILE * TILE * sizeof(T) + 2 * 2 * (size_t)CmChunk<T>::v * TILE * sizeof(T) + 5 * TILE * 4 + 16;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(CM_NT, 2) k_cmod(FactorArgs fa, const int4* __restrict__ tasks,
+                                                   const int4* __restrict__ pairs) {
   using F = Field<T>;
+  constexpr int KC = CmChunk<T>::v;
+  constexpr int STAGE = 2 * KC * TILE;  // A chunk [t][64 rows] then B chunk [t][64 cols]
   if (fa.status[0] != 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* acc_s = reinterpret_cast<T*>(smem_raw);          // [64 cols][64 rows]
-  T* As = acc_s + TILE * TILE;
-  T* Bs = As + KChunk<T>::v * TILE;
-  int* rs_tile = reinterpret_cast<int*>(Bs + KChunk<T>::v * TILE);  // 64
-  int* rowmap = rs_tile + TILE;                                       // 64
-  int* colmap = rowmap + TILE;                                        // 64
+  T* acc_s = reinterpret_cast<T*>(smem_raw);  // [64 cols][64 rows]
+  T* stg = acc_s + TILE * TILE;               // 2 stages
+  int* rs_tile = reinterpret_cast<int*>(stg + 2 * STAGE);  // 64
+  int* rowmap = rs_tile + TILE;                            // 2 x 64 (pair parity)
+  int* colmap = rowmap + 2 * TILE;                         // 2 x 64
 
   const int4 tk = tasks[blockIdx.x];
   const int s = tk.x, r0 = (tk.y >> 16) * TILE, c0 = (tk.y & 0xffff) * TILE;
@@ -272,51 +298,132 @@ __global__ void __launch_bounds__(TPB) k_cmod(FactorArgs fa, const int4* __restr
   const int rows_here = min(TILE, nrow - r0), cols_here = min(TILE, ncol - c0);
   T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
   const int* rss = fa.rs + fa.sn_rsoff[s];
-  const int tid = threadIdx.x;
-  for (int e = tid; e < TILE * TILE; e += TPB) {
-    int c = e / TILE, r = e % TILE;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int e = tid; e < TILE * TILE; e += CM_NT) {
+    const int c = e / TILE, r = e % TILE;
     T v = F::zero();
     if (r < rows_here && c < cols_here) v = panel[(r0 + r) + (long long)(c0 + c) * nrow];
     acc_s[e] = v;
   }
   if (tid < TILE) rs_tile[tid] = tid < rows_here ? rss[r0 + tid] : INT_MAX;
-  __syncthreads();
-  const T* dall = reinterpret_cast<const T*>(fa.d);
-  const T* dsall = reinterpret_cast<const T*>(fa.dsub);
   const T* pall = reinterpret_cast<const T*>(fa.panel);
-  for (int u = tk.z; u < tk.w; ++u) {
-    const int4 pr = pairs[u];
+  const T* gall = reinterpret_cast<const T*>(fa.gpool);
+
+  // chunk stream over (pair u, columns [t0, t0 + KC) of its updater)
+  struct Cur {
+    int u, t0;
+  };
+  auto issue = [&](Cur x, int st) {
+    const int4 pr = pairs[x.u];
     const int k = pr.x, a = pr.y, q0 = pr.z, nr = pr.w >> 16, nc = pr.w & 0xffff;
-    const int nck = fa.sn_ncol[k], nrk = fa.sn_nrow[k], fk = fa.sn_first[k];
-    const int* ok = fa.rs + fa.sn_rsoff[k] + nck;
-    // Row map: position of ok[a + i] inside this tile's row slice (smem search).
-    if (tid < TILE) {
-      if (tid < nr) rowmap[tid] = lower_bound_i(rs_tile, 0, rows_here, ok[a + tid]);
-      if (tid < nc) colmap[tid] = ok[q0 + tid] - first - c0;
+    const int nck = fa.sn_ncol[k], nrk = fa.sn_nrow[k];
+    const T* A = pall + fa.sn_poff[k] + nck + a;
+    const T* B = gall + fa.goff[k] + q0;
+    const long long ldb = nrk - nck;
+    T* As = stg + st * STAGE;
+    T* Bs = As + KC * TILE;
+    for (int e = tid; e < KC * TILE; e += CM_NT) {
+      const int t = e / TILE, r = e % TILE, tt = x.t0 + t;
+      const bool in_t = tt < nck;
+      cp_async_zfill<(int)sizeof(T)>(As + e, in_t && r < nr ? A + r + (long long)tt * nrk : A, in_t && r < nr);
+      cp_async_zfill<(int)sizeof(T)>(Bs + e, in_t && r < nc ? B + r + (long long)tt * ldb : B, in_t && r < nc);
     }
-    const T* Lk = pall + fa.sn_poff[k];
-    T acc[4][4];
-    tile_product<T>(acc, Lk + nck + a, nrk, nr, Lk + nck + q0, nrk, nc, nck, dall + fk, dsall + fk, fa.kind + fk,
-                    As, Bs);
-    // Scatter-subtract (rows r >= column c in k's ordering only).
-    const int tx = tid & 15, ty = tid >> 4;
+    cp_async_commit();
+  };
+  auto advance = [&](Cur x) -> Cur {
+    const int nck = fa.sn_ncol[pairs[x.u].x];
+    x.t0 += KC;
+    if (x.t0 >= nck) {
+      x.u += 1;
+      x.t0 = 0;
+    }
+    return x;
+  };
+
+  const int ry = lane >> 4, cx = lane & 15;
+  const int rb = 16 * warp + 8 * ry;  // this thread's rows rb..rb+7, columns cx + 16 j
+  T acc[8][4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      int ri = ty + 16 * i;
-      if (ri >= nr) continue;
+  for (int i = 0; i < 8; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        int cj = tx + 16 * j;
-        if (cj >= nc) continue;
-        if (a + ri < q0 + cj) continue;
-        int e = colmap[cj] * TILE + rowmap[ri];
-        acc_s[e] = F::sub(acc_s[e], acc[i][j]);
-      }
+    for (int j = 0; j < 4; ++j) acc[i][j] = F::zero();
+
+  Cur cur{tk.z, 0};
+  if (tk.z < tk.w) issue(cur, 0);
+  int st = 0, parity = 0;
+  while (cur.u < tk.w) {
+    const int4 pr = pairs[cur.u];
+    const int k = pr.x, a = pr.y, q0 = pr.z, nr = pr.w >> 16, nc = pr.w & 0xffff;
+    const int nck = fa.sn_ncol[k];
+    if (cur.t0 == 0) {
+      // the tile positions of this pair's rows and columns (read only at the
+      // pair's scatter, after at least one block barrier)
+      __syncthreads();  // rs_tile written / the map slot's previous reader done
+      const int* ok = fa.rs + fa.sn_rsoff[k] + nck;
+      if (tid < nr) rowmap[parity * TILE + tid] = lower_bound_i(rs_tile, 0, rows_here, ok[a + tid]);
+      if (tid >= TILE && tid - TILE < nc) colmap[parity * TILE + tid - TILE] = ok[q0 + tid - TILE] - first - c0;
+    }
+    const Cur nx = advance(cur);
+    if (nx.u < tk.w) {
+      issue(nx, st ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
+    const T* As = stg + st * STAGE;
+    const T* Bs = As + KC * TILE;
+    const int kt = min(KC, nck - cur.t0);
+    if (rb - 8 * ry < nr) {  // the warp has rows of this pair
+      if (kt == KC) {
+#pragma unroll 2
+        for (int t = 0; t < KC; ++t) {
+          T av[8], bv[4];
+          lds_row<T, 8>(As + t * TILE + rb, av);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) bv[j] = Bs[t * TILE + cx + 16 * j];
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = F::fma_(av[i], bv[j], acc[i][j]);
+        }
+      } else {
+        for (int t = 0; t < kt; ++t) {
+          T av[8], bv[4];
+          lds_row<T, 8>(As + t * TILE + rb, av);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) bv[j] = Bs[t * TILE + cx + 16 * j];
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = F::fma_(av[i], bv[j], acc[i][j]);
+        }
+      }
+    }
+    if (nx.u != cur.u) {
+      // the pair is complete: subtract it from the tile, reset the registers
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int ri = rb + i;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int cj = cx + 16 * j;
+          if (ri < nr && cj < nc && a + ri >= q0 + cj) {
+            const int e = colmap[parity * TILE + cj] * TILE + rowmap[parity * TILE + ri];
+            acc_s[e] = F::sub(acc_s[e], acc[i][j]);
+          }
+          acc[i][j] = F::zero();
+        }
+      }
+      parity ^= 1;
+    }
+    __syncthreads();  // the stage is free for the load after next
+    st ^= 1;
+    cur = nx;
   }
-  for (int e = tid; e < TILE * TILE; e += TPB) {
-    int c = e / TILE, r = e % TILE;
+  __syncthreads();
+  for (int e = tid; e < TILE * TILE; e += CM_NT) {
+    const int c = e / TILE, r = e % TILE;
     if (r < rows_here && c < cols_here && r0 + r >= c0 + c) panel[(r0 + r) + (long long)(c0 + c) * nrow] = acc_s[e];
   }
 }

@@ -12,8 +12,10 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <atomic>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/rslab_b200.h"
@@ -699,7 +701,6 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
 
 // Chunk depth of the tile engine for an element size (KChunk<T>::v).
 size_t kchunk(size_t es) { return es == 16 ? 16 : 32; }
-size_t smem_cmod(size_t es) { return (size_t)TILE * TILE * es + 2 * kchunk(es) * TILE * es + 3 * TILE * 4 + 64; }
 size_t smem_schur(size_t es) { return 2 * kchunk(es) * TILE * es; }
 // Deep-row staging (DEEP_R + 1) x nb plus the replay program, 16-byte aligned.
 size_t smem_replay(size_t es, int nb) {
@@ -769,7 +770,7 @@ struct KernelSetup {
       CK(cudaFuncSetAttribute(k_cmod_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_tc_bytes()));
       CK(cudaFuncSetAttribute(k_schur_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_tc_bytes()));
     }
-    CK(cudaFuncSetAttribute(k_cmod<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod(es)));
+    CK(cudaFuncSetAttribute(k_cmod<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_bytes<T>()));
     CK(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
     CK(cudaFuncSetAttribute(k_getf2<T, GETF2_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)smem_getf2(es, 128)));
@@ -818,7 +819,7 @@ struct rslab_fac_handle {
   unsigned long long* amax_dev = nullptr;
   void* scratch = nullptr;
   long long scratch_stride = 0;
-  void* gpool = nullptr;  // G_k = L21_k D_k (tensor-core cmod only)
+  void* gpool = nullptr;  // G_k = L21_k D_k of every updater (read by both cmod engines)
   void* linv = nullptr;   // inverse diagonal blocks of the wide supernodes
   // graph of the numeric factor (values read from `aval`)
   cudaGraphExec_t fgraph = nullptr;
@@ -974,7 +975,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
     switch (L.kind) {
       case L_CMOD: return !use_tc;
       case L_CMOD_TC: return use_tc;
-      case L_MAKE_G: return use_tc;
+      case L_MAKE_G: return true;  // both descendant-update engines read G_k
       case L_DEEP: return !fa.deep_mm;
       case L_MAKE_M: case L_DEEP_MM: return fa.deep_mm != 0;
       case L_SCHUR: return !use_tc;
@@ -1008,7 +1009,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
     switch (L.kind) {
       case L_CMOD:
         if (use_tc) continue;
-        k_cmod<T><<<L.ntasks, TPB, smem_cmod(es), ls>>>(fa, H.d_t4 + L.task_off, H.d_cpairs);
+        k_cmod<T><<<L.ntasks, CM_NT, smem_cmod_bytes<T>(), ls>>>(fa, H.d_t4 + L.task_off, H.d_cpairs);
         break;
       case L_CMOD_TC:
         if constexpr (TensorCmod<T>::ok) {
@@ -1020,7 +1021,6 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         }
         break;
       case L_MAKE_G:
-        if (!use_tc) continue;
         k_make_g<T><<<L.ntasks, 256, 0, ls>>>(fa, H.d_t4 + L.task_off);
         break;
       case L_DIAG_INV:
@@ -1545,6 +1545,8 @@ namespace rslab {
 // Sets the calling thread's last-error message (for entry points defined in
 // other translation units of the library).
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+// Matrix dimension of a factor handle (-1 for a null handle).
+int64_t factor_dimension(const rslab_fac_handle* F) { return F && F->sym ? F->sym->n : -1; }
 }  // namespace rslab
 
 extern "C" {
@@ -1732,9 +1734,30 @@ int rslab_analyze_batch(int64_t count, const int64_t* n, const int64_t* const* c
       if (n[i] < 0 || !col_ptr[i] || (n[i] > 0 && !row_idx[i] && col_ptr[i][n[i]] > 0))
         throw RslabError(Status::InvalidInput, "bad CSC of system " + std::to_string(i));
       rslab::validate_lower_csc(n[i], col_ptr[i], row_idx[i], col_ptr[i][n[i]]);
-      parts[i] = rslab::analyze(n[i], col_ptr[i], row_idx[i], o);
       seg.push_back(seg.back() + n[i]);
       nz.push_back(nz.back() + col_ptr[i][n[i]]);
+    }
+    // the systems' analyses are independent: host threads take systems in
+    // turn; each result lands in its own slot, so the merge is unchanged
+    {
+      std::atomic<int64_t> next{0};
+      std::vector<std::string> errs((size_t)count);
+      const int nth = (int)std::max<int64_t>(1, std::min<int64_t>(count, std::thread::hardware_concurrency()));
+      auto work = [&]() {
+        for (int64_t i; (i = next.fetch_add(1)) < count;) {
+          try {
+            parts[i] = rslab::analyze(n[i], col_ptr[i], row_idx[i], o);
+          } catch (const std::exception& e) {
+            errs[i] = e.what();
+          }
+        }
+      };
+      std::vector<std::thread> pool;
+      for (int t = 1; t < nth; ++t) pool.emplace_back(work);
+      work();
+      for (auto& t : pool) t.join();
+      for (int64_t i = 0; i < count; ++i)
+        if (!errs[i].empty()) throw RslabError(Status::InvalidInput, "system " + std::to_string(i) + ": " + errs[i]);
     }
     if (seg.back() >= (1LL << 31)) throw RslabError(Status::InvalidInput, "batch too large");
     // block-diagonal lower CSC of the whole batch (user order)
@@ -1903,8 +1926,7 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
       F->floor_dev = F->al<double>(1);
       F->amax_dev = F->al<unsigned long long>(1);
     }
-    if ((dtype == RSLAB_F32 || dtype == RSLAB_C32) && F->set.schur_engine == RSLAB_SCHUR_TENSOR)
-      F->gpool = F->al<unsigned char>((size_t)std::max(sym->g_elems, 1LL) * es);
+    F->gpool = F->al<unsigned char>((size_t)std::max(sym->g_elems, 1LL) * es);
     if (F->set.scaling != RSLAB_SCALING_ONEPASS) {
       std::vector<double> ones(n, 1.0);
       CK(cudaMemcpyAsync(F->scale, ones.data(), n * 8, cudaMemcpyHostToDevice, F->st));

@@ -16,6 +16,7 @@
 #include "host.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <numeric>
@@ -165,7 +166,7 @@ namespace {
 // unstable sort, which is an insertion sort (hence stable) for slices of at
 // most 20 elements; longer child lists with tied keys are counted so a caller
 // can see where the tie order might differ.
-static int64_t g_long_tie_lists = 0;
+static std::atomic<int64_t> g_long_tie_lists{0};
 void sort_by_size(std::vector<int64_t>& v, const std::vector<int64_t>& sizes) {
   std::stable_sort(v.begin(), v.end(), [&](int64_t a, int64_t b) { return sizes[a] < sizes[b]; });
   if (v.size() > 20)

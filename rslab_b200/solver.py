@@ -582,6 +582,71 @@ class LdltSolver:
                            self.inertia(), scale)
 
 
+class CompressedLdltFactors:
+    """CompressedLdltFactors (src/dense/ldlt_generic.rs:434-536): the factor
+    in the LdltFactors layout with uint32 index arrays and pivot permutation
+    (half the index bytes), held on the host; `solve` is the reference's
+    solve_ldlt on these factors, bit for bit.  Like the reference container it
+    holds the factors of the equilibrated matrix S A S (S = the factor's
+    `scale`), so `solve` solves with S A S."""
+
+    def __init__(self, handle, dtype):
+        self._h = handle
+        self.dtype = np.dtype(dtype)
+        n, nnz, ib, dt = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int32()
+        _check(N.lib.rslab_cfac_info(handle, C.byref(n), C.byref(nnz), C.byref(ib), C.byref(dt)))
+        self.n, self._nnz, self._index_bytes = int(n.value), int(nnz.value), int(ib.value)
+
+    @classmethod
+    def from_factors(cls, solver: "LdltSolver") -> Optional["CompressedLdltFactors"]:
+        """The compressed copy of `solver`'s factor, or None when n or nnz(L)
+        does not fit 32 bits (the reference's from_factors returns None)."""
+        h = C.c_void_p()
+        rc = N.lib.rslab_compress_factors(solver._h, C.byref(h))
+        if rc == 2 and "32 bits" in N.last_error():
+            return None
+        _check(rc)
+        return cls(h, solver.dtype)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        lib = getattr(N, "lib", None)
+        if h and lib is not None:
+            lib.rslab_free_cfac(h)
+            self._h = None
+
+    def factor_nnz(self) -> int:
+        return self._nnz
+
+    def index_bytes(self) -> int:
+        return self._index_bytes
+
+    def arrays(self) -> dict:
+        n, nnz = self.n, self._nnz
+        u32 = C.POINTER(C.c_uint32)
+        out = {"l_col_ptr": np.zeros(n + 1, np.uint32), "l_row_idx": np.zeros(max(nnz, 1), np.uint32),
+               "l_values": np.zeros(max(nnz, 1), self.dtype), "d_diag": np.zeros(n, self.dtype),
+               "d_subdiag": np.zeros(n, self.dtype), "two_by_two": np.zeros(n, np.uint8),
+               "perm": np.zeros(n, np.uint32)}
+        _check(N.lib.rslab_cfac_export(
+            self._h, out["l_col_ptr"].ctypes.data_as(u32), out["l_row_idx"].ctypes.data_as(u32),
+            out["l_values"].ctypes.data_as(C.c_void_p), out["d_diag"].ctypes.data_as(C.c_void_p),
+            out["d_subdiag"].ctypes.data_as(C.c_void_p), out["two_by_two"].ctypes.data_as(C.POINTER(C.c_uint8)),
+            out["perm"].ctypes.data_as(u32)))
+        out["l_row_idx"] = out["l_row_idx"][:nnz]
+        out["l_values"] = out["l_values"][:nnz]
+        out["two_by_two"] = out["two_by_two"].astype(bool)
+        return out
+
+    def solve(self, rhs) -> np.ndarray:
+        b = np.ascontiguousarray(rhs, dtype=self.dtype).reshape(-1)
+        if b.shape[0] != self.n:
+            raise DimensionMismatch(self.n, b.shape[0])
+        x = np.empty_like(b)
+        _check(N.lib.rslab_cfac_solve(self._h, b.ctypes.data_as(C.c_void_p), x.ctypes.data_as(C.c_void_p)))
+        return x
+
+
 CERT_FACTOR = 64.0
 EPS_F64 = 2.220446049250313e-16
 
