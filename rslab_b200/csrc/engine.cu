@@ -4,6 +4,8 @@
 // capture of the frozen-pattern refactor and of the solve, the device-side
 // mixed-precision refinement ladder, and the extern "C" entry points declared
 // in include/rslab_b200.h.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -21,6 +23,7 @@
 #include "../../include/rslab_b200.h"
 #include "device/factor_kernels.cuh"
 #include "device/cmod_tc.cuh"
+#include "device/cmod_mm.cuh"
 #include "device/solve_kernels.cuh"
 #include "device/wave_solve.cuh"
 #include "host/host.hpp"
@@ -104,7 +107,7 @@ size_t elem_size(int dtype) {
 enum LaunchKind {
   L_CMOD, L_GETF2, L_DEEP, L_SCHUR,
   L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD,
-  L_UNUSED8, L_UNUSED9, L_UNUSED10, L_UNUSED11, L_FWD_GATHER, L_CMOD_TC, L_MAKE_G, L_DIAG_INV,
+  L_MM_GEMM, L_MM_ASM, L_SPLIT_R, L_SPLIT_C, L_FWD_GATHER, L_CMOD_TC, L_MAKE_G, L_DIAG_INV,
   L_BWD_OFF_RED, L_SCHUR_TC, L_FWD_CHAIN, L_BWD_CHAIN, L_BWD_GATHER, L_DEEP_MM, L_MAKE_M,
   L_FWD_PUSH_RED,
   L_JOIN_CM  // no kernel: the level's early cmod updates must be complete from here on
@@ -156,6 +159,21 @@ struct rslab_sym_handle {
   std::vector<int4> cpairs;   // cmod (k, a, q0, nr << 16 | nc) per tile, in update order
   std::vector<int4> t4tc, cpairs_tc;  // the same for the 128 x 64 tensor-core tiles
   std::vector<int8_t> tcmaps;         // per tensor-core pair: 128 + 64 inverse scatter maps
+  // tensor-core cmod in the updater's row space (device/cmod_mm.cuh): the
+  // W offset of every update-list entry in its target level's buffer, the
+  // GEMM tiles (k, r0, c0, nrows | nn << 16) with their W element offsets /
+  // row strides, the assembly pairs' W offsets / strides (parallel to
+  // cpairs_tc), and the split pools of every updater for the real (32-column
+  // chunks) and complex (16-column chunks) fields
+  std::vector<long long> upd_woff;
+  long long w_elems = 0;              // one level buffer (field elements)
+  std::vector<int4> mm_t4;
+  std::vector<long long> mm_wb, asm_wb;
+  std::vector<int> mm_wl, asm_wl;
+  std::vector<int> kpad_r, kpad_c;
+  std::vector<long long> soff_a_r, soff_b_r, soff_a_c, soff_b_c;
+  long long split_a_r = 0, split_b_r = 0, split_a_c = 0, split_b_c = 0;
+  std::vector<int4> sp_r, sp_c;       // split tasks (k, r0, chunk, 0)
   std::vector<long long> goff;        // G_k = L21_k D_k pool offsets ((nrow - ncol) x ncol each)
   long long g_elems = 0;
   int bwd_slots = 0;                  // partial-sum slots of the split push / backward dots (max per level)
@@ -193,6 +211,12 @@ struct rslab_sym_handle {
   int4* d_cpairs = nullptr;
   int4 *d_t4tc = nullptr, *d_cpairs_tc = nullptr;
   int8_t* d_tcmaps = nullptr;
+  int4* d_mm_t4 = nullptr;
+  long long *d_mm_wb = nullptr, *d_asm_wb = nullptr;
+  int *d_mm_wl = nullptr, *d_asm_wl = nullptr;
+  int *d_kpad_r = nullptr, *d_kpad_c = nullptr;
+  long long *d_soff_a_r = nullptr, *d_soff_b_r = nullptr, *d_soff_a_c = nullptr, *d_soff_b_c = nullptr;
+  int4 *d_sp_r = nullptr, *d_sp_c = nullptr;
   long long* d_goff = nullptr;
   long long* d_linv_off = nullptr;
   int* d_t1 = nullptr;
@@ -252,6 +276,19 @@ struct rslab_sym_handle {
     d_t4tc = up(t4tc, st);
     d_cpairs_tc = up(cpairs_tc, st);
     d_tcmaps = up(tcmaps, st);
+    d_mm_t4 = up(mm_t4, st);
+    d_mm_wb = up(mm_wb, st);
+    d_mm_wl = up(mm_wl, st);
+    d_asm_wb = up(asm_wb, st);
+    d_asm_wl = up(asm_wl, st);
+    d_kpad_r = up(kpad_r, st);
+    d_kpad_c = up(kpad_c, st);
+    d_soff_a_r = up(soff_a_r, st);
+    d_soff_b_r = up(soff_b_r, st);
+    d_soff_a_c = up(soff_a_c, st);
+    d_soff_b_c = up(soff_b_c, st);
+    d_sp_r = up(sp_r, st);
+    d_sp_c = up(sp_c, st);
     d_goff = up(goff, st);
     d_linv_off = up(linv_off, st);
     d_t1 = up(t1, st);
@@ -285,7 +322,8 @@ namespace {
 // updates into those final one level earlier and the rest).
 void add_cmod_tiles(rslab_sym_handle& H, const std::vector<int64_t>& lvl, int tr, int tcw, std::vector<int4>& tasks,
                     std::vector<int4>& pairs, bool count_flops, std::vector<int8_t>* maps = nullptr,
-                    const std::vector<int>* lv_of = nullptr, int lv_lo = 0, int lv_hi = 0) {
+                    const std::vector<int>* lv_of = nullptr, int lv_lo = 0, int lv_hi = 0,
+                    std::vector<long long>* wbase = nullptr, std::vector<int>* wld = nullptr) {
   const auto& S = H.S;
   for (int64_t s : lvl) {
     if (S.upd_ptr[s + 1] == S.upd_ptr[s]) continue;
@@ -295,6 +333,8 @@ void add_cmod_tiles(rslab_sym_handle& H, const std::vector<int64_t>& lvl, int tr
     const int ntc = (nc + tcw - 1) / tcw, ntr = (nr + tr - 1) / tr;
     std::vector<std::vector<int4>> tp((size_t)ntc * ntr);
     std::vector<std::vector<int8_t>> tm(maps ? (size_t)ntc * ntr : 0);
+    std::vector<std::vector<long long>> twb(wbase ? (size_t)ntc * ntr : 0);
+    std::vector<std::vector<int>> twl(wbase ? (size_t)ntc * ntr : 0);
     for (int64_t u = S.upd_ptr[s]; u < S.upd_ptr[s + 1]; ++u) {
       const int64_t k = S.upd[u], p0 = S.upd_p0[u], p1 = S.upd_p1[u];
       if (lv_of && ((*lv_of)[k] < lv_lo || (*lv_of)[k] > lv_hi)) continue;
@@ -321,6 +361,10 @@ void add_cmod_tiles(rslab_sym_handle& H, const std::vector<int64_t>& lvl, int tr
           while (rb < nok && rel[rb - p0] / tr == rt) ++rb;
           tp[(size_t)ct * ntr + rt].push_back(
               make_int4((int)k, (int)ra, (int)qa, (int)(((rb - ra) << 16) | (qb - qa))));
+          if (wbase) {  // W element (ra, qa) of the pair's row-major (nok - p0) x (p1 - p0) block
+            twb[(size_t)ct * ntr + rt].push_back(H.upd_woff[u] + (ra - p0) * (p1 - p0) + (qa - p0));
+            twl[(size_t)ct * ntr + rt].push_back((int)(p1 - p0));
+          }
           if (maps) {
             auto& m = tm[(size_t)ct * ntr + rt];
             const size_t base = m.size();
@@ -354,9 +398,40 @@ void add_cmod_tiles(rslab_sym_handle& H, const std::vector<int64_t>& lvl, int tr
           const auto& m = tm[(size_t)ct * ntr + rt];
           maps->insert(maps->end(), m.begin(), m.end());
         }
+        if (wbase) {
+          const auto& b = twb[(size_t)ct * ntr + rt];
+          const auto& l = twl[(size_t)ct * ntr + rt];
+          wbase->insert(wbase->end(), b.begin(), b.end());
+          wld->insert(wld->end(), l.begin(), l.end());
+        }
         tasks.push_back(make_int4((int)s, (rt << 16) | ct, pb, (int)pairs.size()));
       }
   }
+}
+
+// GEMM tiles of the updater-space tensor-core cmod for the targets of a
+// level: for every update-list entry (k -> s) whose updater level lies in
+// [lv_lo, lv_hi], column tiles of 64 of k's rows [p0, p1) and, for each, row
+// tiles of 128 of k's rows from the column tile's first row to the end (the
+// lower trapezoid), with the W offset of the tile's first element.
+void add_mm_tiles(rslab_sym_handle& H, const std::vector<int64_t>& lvl, const std::vector<int>& lv_of, int lv_lo,
+                  int lv_hi) {
+  const auto& S = H.S;
+  for (int64_t s : lvl)
+    for (int64_t u = S.upd_ptr[s]; u < S.upd_ptr[s + 1]; ++u) {
+      const int64_t k = S.upd[u], p0 = S.upd_p0[u], p1 = S.upd_p1[u];
+      if (lv_of[k] < lv_lo || lv_of[k] > lv_hi) continue;
+      const int64_t m = H.nrow[k] - S.sn[k].ncol, npk = p1 - p0;
+      for (int64_t c0 = p0; c0 < p1; c0 += MM_NC) {
+        const int64_t nn = std::min<int64_t>(MM_NC, p1 - c0);
+        for (int64_t r0 = c0; r0 < m; r0 += MM_M) {
+          const int64_t nr = std::min<int64_t>(MM_M, m - r0);
+          H.mm_t4.push_back(make_int4((int)k, (int)r0, (int)c0, (int)(nr | (nn << 16))));
+          H.mm_wb.push_back(H.upd_woff[u] + (r0 - p0) * npk + (c0 - p0));
+          H.mm_wl.push_back((int)npk);
+        }
+      }
+    }
 }
 
 // Build panel offsets, assembly targets, SpMV structure and the launch plan.
@@ -390,6 +465,44 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
   for (int s = 0; s < ns; ++s) {
     H.goff[s] = H.g_elems;
     H.g_elems += (long long)(H.nrow[s] - S.sn[s].ncol) * S.sn[s].ncol;
+  }
+  // updater-space tensor-core cmod: the W block of update-list entry u
+  // (k -> s) is k's rows [p0, nok) x its rows [p0, p1), row-major, in the
+  // buffer of s's level; split pools per updater, K' padded to 32-wide chunks
+  {
+    std::vector<int> lev(ns, 0);
+    for (size_t li = 0; li < S.by_level.size(); ++li)
+      for (int64_t s : S.by_level[li]) lev[s] = (int)li;
+    std::vector<long long> acc(S.by_level.size(), 0);
+    H.upd_woff.assign(S.upd.size(), 0);
+    for (int s = 0; s < ns; ++s)
+      for (int64_t u = S.upd_ptr[s]; u < S.upd_ptr[s + 1]; ++u) {
+        const int64_t k = S.upd[u];
+        const long long nok = H.nrow[k] - S.sn[k].ncol;
+        H.upd_woff[u] = acc[lev[s]];
+        acc[lev[s]] += (nok - S.upd_p0[u]) * (S.upd_p1[u] - S.upd_p0[u]);
+      }
+    H.w_elems = 1;
+    for (long long v : acc) H.w_elems = std::max(H.w_elems, v);
+    H.kpad_r.assign(ns, 0);
+    H.kpad_c.assign(ns, 0);
+    H.soff_a_r.assign(ns, 0);
+    H.soff_b_r.assign(ns, 0);
+    H.soff_a_c.assign(ns, 0);
+    H.soff_b_c.assign(ns, 0);
+    for (int s = 0; s < ns; ++s) {
+      const long long nc = S.sn[s].ncol, m = H.nrow[s] - nc;
+      H.kpad_r[s] = (int)(32 * ((nc + 31) / 32));
+      H.kpad_c[s] = (int)(32 * ((nc + 15) / 16));
+      H.soff_a_r[s] = H.split_a_r;
+      H.soff_b_r[s] = H.split_b_r;
+      H.soff_a_c[s] = H.split_a_c;
+      H.soff_b_c[s] = H.split_b_c;
+      H.split_a_r += m * H.kpad_r[s];
+      H.split_b_r += m * H.kpad_r[s];
+      H.split_a_c += m * H.kpad_c[s];
+      H.split_b_c += 2 * m * H.kpad_c[s];
+    }
   }
   H.linv_off.assign(ns, 0);
   H.linv_elems = 0;
@@ -490,10 +603,13 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
     // tag = their level); this level's own launch then adds the updates
     // from the level just below.
     {
+      // tensor-core engine: the W tiles of the next level from updaters two
+      // or more levels below it (side 2, overlapping this level; tag = the
+      // target level, whose parity picks the W buffer) ...
       if (li + 1 < nlev) {
-        Launch Le{L_CMOD_TC, (long long)H.t4tc.size(), 0, li + 1, 2};
-        add_cmod_tiles(H, S.by_level[li + 1], TC_M, TC_N, H.t4tc, H.cpairs_tc, false, &H.tcmaps, &lv_of, 0, li - 1);
-        Le.ntasks = (int)(H.t4tc.size() - Le.task_off);
+        Launch Le{L_MM_GEMM, (long long)H.mm_t4.size(), 0, li + 1, 2};
+        add_mm_tiles(H, S.by_level[li + 1], lv_of, 0, li - 1);
+        Le.ntasks = (int)(H.mm_t4.size() - Le.task_off);
         if (Le.ntasks) H.fplan.push_back(Le);
       }
       H.fplan.push_back(Launch{L_JOIN_CM, 0, 0, li});
@@ -501,10 +617,16 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       add_cmod_tiles(H, lvl, TILE, TILE, H.t4, H.cpairs, true);
       L.ntasks = (int)(H.t4.size() - L.task_off);
       if (L.ntasks) H.fplan.push_back(L);
-      Launch Lt{L_CMOD_TC, (long long)H.t4tc.size(), 0, li};
-      add_cmod_tiles(H, lvl, TC_M, TC_N, H.t4tc, H.cpairs_tc, false, &H.tcmaps, &lv_of, li - 1, li - 1);
-      Lt.ntasks = (int)(H.t4tc.size() - Lt.task_off);
+      // ... this level's own tiles from the level just below, then the
+      // assembly of every pair of the level into its 128 x 64 target tiles
+      Launch Lt{L_MM_GEMM, (long long)H.mm_t4.size(), 0, li};
+      add_mm_tiles(H, lvl, lv_of, li - 1, li - 1);
+      Lt.ntasks = (int)(H.mm_t4.size() - Lt.task_off);
       if (Lt.ntasks) H.fplan.push_back(Lt);
+      Launch La{L_MM_ASM, (long long)H.t4tc.size(), 0, li};
+      add_cmod_tiles(H, lvl, TC_M, TC_N, H.t4tc, H.cpairs_tc, false, &H.tcmaps, nullptr, 0, 0, &H.asm_wb, &H.asm_wl);
+      La.ntasks = (int)(H.t4tc.size() - La.task_off);
+      if (La.ntasks) H.fplan.push_back(La);
     }
     int maxblocks = 0;
     for (int64_t s : lvl) maxblocks = std::max(maxblocks, (int)((S.sn[s].ncol + nb_of(s) - 1) / nb_of(s)));
@@ -575,8 +697,9 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         H.fplan.push_back(Ct);
       }
     }
-    // G_k = L21_k D_k of this level's updaters, for the tensor-core cmod of
-    // their ancestors (32-column tasks).
+    // G_k = L21_k D_k of this level's updaters, for the CUDA-core cmod of
+    // their ancestors (32-column tasks), and the tensor-core engine's split
+    // operands (rows of 256 x one 32-wide K' chunk per task).
     {
       Launch Mg{L_MAKE_G, (long long)H.t4.size(), 0, 0};
       for (int64_t s : lvl) {
@@ -586,6 +709,18 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       }
       Mg.ntasks = (int)(H.t4.size() - Mg.task_off);
       if (Mg.ntasks) H.fplan.push_back(Mg);
+      Launch Sr{L_SPLIT_R, (long long)H.sp_r.size(), 0, 0}, Sc{L_SPLIT_C, (long long)H.sp_c.size(), 0, 0};
+      for (int64_t s : lvl) {
+        const int off = H.nrow[s] - (int)S.sn[s].ncol;
+        for (int r0 = 0; r0 < off; r0 += MM_SPLIT_ROWS) {
+          for (int c = 0; c < H.kpad_r[s] / 32; ++c) H.sp_r.push_back(make_int4((int)s, r0, c, 0));
+          for (int c = 0; c < H.kpad_c[s] / 32; ++c) H.sp_c.push_back(make_int4((int)s, r0, c, 0));
+        }
+      }
+      Sr.ntasks = (int)(H.sp_r.size() - Sr.task_off);
+      Sc.ntasks = (int)(H.sp_c.size() - Sc.task_off);
+      if (Sr.ntasks) H.fplan.push_back(Sr);
+      if (Sc.ntasks) H.fplan.push_back(Sc);
       // inverses of the diagonal TB-blocks of this level's supernodes (used
       // by the block-chain triangular solves)
       Launch Dv{L_DIAG_INV, (long long)H.t2.size(), 0, 0};
@@ -767,6 +902,7 @@ struct KernelSetup {
     if (done) return;
     const size_t es = sizeof(T);
     if constexpr (TensorCmod<T>::ok) {
+      CK(cudaFuncSetAttribute(k_cmod_mm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_mm_bytes()));
       CK(cudaFuncSetAttribute(k_cmod_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_tc_bytes()));
       CK(cudaFuncSetAttribute(k_schur_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_tc_bytes()));
     }
@@ -821,6 +957,12 @@ struct rslab_fac_handle {
   long long scratch_stride = 0;
   void* gpool = nullptr;  // G_k = L21_k D_k of every updater (read by both cmod engines)
   void* linv = nullptr;   // inverse diagonal blocks of the wide supernodes
+  // updater-space tensor-core cmod (f32 / c32, tensor engine): split operand
+  // pools (tf32 hi / lo of L21 and of G), two level buffers of W, and the
+  // TMA tensor maps of every updater's pools (MM_MAPS per supernode)
+  float *sp_ahi = nullptr, *sp_alo = nullptr, *sp_bhi = nullptr, *sp_blo = nullptr;
+  float* wbuf = nullptr;
+  CUtensorMap* tmaps = nullptr;
   // graph of the numeric factor (values read from `aval`)
   cudaGraphExec_t fgraph = nullptr;
   // solve workspace
@@ -974,8 +1116,11 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
   auto runs = [&](const Launch& L) {
     switch (L.kind) {
       case L_CMOD: return !use_tc;
-      case L_CMOD_TC: return use_tc;
-      case L_MAKE_G: return true;  // both descendant-update engines read G_k
+      case L_CMOD_TC: return false;  // superseded by the updater-space GEMM + assembly
+      case L_MM_GEMM: case L_MM_ASM: return use_tc;
+      case L_SPLIT_R: return use_tc && !Field<T>::complex;
+      case L_SPLIT_C: return use_tc && Field<T>::complex;
+      case L_MAKE_G: return !use_tc;  // G_k of the CUDA-core cmod
       case L_DEEP: return !fa.deep_mm;
       case L_MAKE_M: case L_DEEP_MM: return fa.deep_mm != 0;
       case L_SCHUR: return !use_tc;
@@ -1022,6 +1167,29 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         break;
       case L_MAKE_G:
         k_make_g<T><<<L.ntasks, 256, 0, ls>>>(fa, H.d_t4 + L.task_off);
+        break;
+      case L_MM_GEMM:
+      case L_MM_ASM:
+      case L_SPLIT_R:
+      case L_SPLIT_C:
+        if constexpr (TensorCmod<T>::ok) {
+          constexpr bool cx = Field<T>::complex;
+          const size_t wsz = (size_t)H.w_elems * (cx ? 2 : 1);
+          if (L.kind == L_MM_GEMM)
+            k_cmod_mm<T><<<L.ntasks, MM_NT, smem_cmod_mm_bytes(), ls>>>(
+                fa, H.d_mm_t4 + L.task_off, H.d_mm_wb + L.task_off, H.d_mm_wl + L.task_off, F.tmaps,
+                cx ? H.d_kpad_c : H.d_kpad_r, F.wbuf + (L.nb_slot & 1) * wsz);
+          else if (L.kind == L_MM_ASM)
+            k_cmod_asm<T><<<L.ntasks, 256, 0, ls>>>(fa, H.d_t4tc + L.task_off, H.d_cpairs_tc, H.d_tcmaps, H.d_asm_wb,
+                                                    H.d_asm_wl, F.wbuf + (L.nb_slot & 1) * wsz);
+          else
+            k_split<T><<<L.ntasks, MM_SPLIT_ROWS, 0, ls>>>(
+                fa, (cx ? H.d_sp_c : H.d_sp_r) + L.task_off, cx ? H.d_soff_a_c : H.d_soff_a_r,
+                cx ? H.d_soff_b_c : H.d_soff_b_r, cx ? H.d_kpad_c : H.d_kpad_r, F.sp_ahi, F.sp_alo, F.sp_bhi,
+                F.sp_blo);
+        } else {
+          continue;
+        }
         break;
       case L_DIAG_INV:
         k_diag_inv<T><<<L.ntasks, DI_NT, smem_diag_inv(es), ls>>>(H.d_t2 + L.task_off, H.d_sn_ncol, H.d_sn_nrow,
@@ -1074,7 +1242,8 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
     }
     if (prof)
       prof->mark(st,
-                 (L.kind == L_CMOD || L.kind == L_CMOD_TC || L.kind == L_MAKE_G) ? 1
+                 (L.kind == L_CMOD || L.kind == L_CMOD_TC || L.kind == L_MAKE_G || L.kind == L_MM_GEMM ||
+                  L.kind == L_MM_ASM || L.kind == L_SPLIT_R || L.kind == L_SPLIT_C) ? 1
                  : (L.kind == L_DIAG_INV || L.kind == L_SCHUR_TC)             ? 4
                  : L.kind == L_GETF2                                           ? 2
                  : (L.kind == L_DEEP || L.kind == L_DEEP_MM || L.kind == L_MAKE_M) ? 3
@@ -1857,6 +2026,59 @@ int rslab_symbolic_export(const rslab_sym_handle* h, int64_t* perm, int64_t* sn_
   return 0;
 }
 
+// Tensor maps of the split pools (cuTensorMapEncodeTiled through the runtime's
+// driver entry point): for updater k, A hi / lo over m_k rows and B hi / lo
+// over m_k (real) or 2 m_k (complex: B'_re rows, then B'_im rows) rows, each
+// row kpad_k fp32 (a multiple of 32: 128-byte aligned rows); boxes of 32
+// fp32 x 128 rows (A) and 32 x 16 (B), 128-byte swizzle, out-of-range rows
+// read as zero.  The pools are this GPU's own memory.
+static void setup_mm_pools(rslab_fac_handle& F) {
+  auto& H = *F.sym;
+  const bool cx = F.dtype == RSLAB_C32;
+  const long long na = std::max(cx ? H.split_a_c : H.split_a_r, 32LL);
+  const long long nb = std::max(cx ? H.split_b_c : H.split_b_r, 32LL);
+  F.sp_ahi = F.al<float>(na);
+  F.sp_alo = F.al<float>(na);
+  F.sp_bhi = F.al<float>(nb);
+  F.sp_blo = F.al<float>(nb);
+  F.wbuf = F.al<float>((size_t)2 * H.w_elems * (cx ? 2 : 1));
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (!fn || q != cudaDriverEntryPointSuccess)
+      throw RslabError(Status::CudaError, "cuTensorMapEncodeTiled is not available");
+    encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  }
+  const int ns = H.ns;
+  std::vector<CUtensorMap> maps((size_t)std::max(ns, 1) * MM_MAPS);
+  std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
+  for (int k = 0; k < ns; ++k) {
+    const long long m = H.nrow[k] - H.S.sn[k].ncol;
+    if (m <= 0) continue;
+    const long long kp = cx ? H.kpad_c[k] : H.kpad_r[k];
+    const long long oa = cx ? H.soff_a_c[k] : H.soff_a_r[k];
+    const long long ob = cx ? H.soff_b_c[k] : H.soff_b_r[k];
+    const long long brows = cx ? 2 * m : m;
+    float* bases[MM_MAPS] = {F.sp_ahi + oa, F.sp_alo + oa, F.sp_bhi + ob, F.sp_blo + ob};
+    for (int j = 0; j < MM_MAPS; ++j) {
+      const cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)(j < 2 ? m : brows)};
+      const cuuint64_t strides[1] = {(cuuint64_t)kp * 4};
+      const cuuint32_t box[2] = {32, (cuuint32_t)(j < 2 ? MM_M : MM_BOX_B)};
+      const cuuint32_t estr[2] = {1, 1};
+      const CUresult r = encode(&maps[(size_t)k * MM_MAPS + j], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, bases[j], dims,
+                                strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS)
+        throw RslabError(Status::CudaError, "cuTensorMapEncodeTiled failed for supernode " + std::to_string(k));
+    }
+  }
+  F.tmaps = reinterpret_cast<CUtensorMap*>(F.al<unsigned char>(maps.size() * sizeof(CUtensorMap)));
+  CK(cudaMemcpyAsync(F.tmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, F.st));
+  CK(cudaStreamSynchronize(F.st));
+}
+
 // The matrix values into the handle: straight into the factor's input, or,
 // for a refined handle, into the original (FP64) copy and from there demoted
 // (or, for the FP64 tier, copied) into the factor's input.
@@ -1926,7 +2148,11 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
       F->floor_dev = F->al<double>(1);
       F->amax_dev = F->al<unsigned long long>(1);
     }
-    F->gpool = F->al<unsigned char>((size_t)std::max(sym->g_elems, 1LL) * es);
+    const bool tensor = (dtype == RSLAB_F32 || dtype == RSLAB_C32) && F->set.schur_engine == RSLAB_SCHUR_TENSOR;
+    if (tensor)
+      setup_mm_pools(*F);
+    else
+      F->gpool = F->al<unsigned char>((size_t)std::max(sym->g_elems, 1LL) * es);
     if (F->set.scaling != RSLAB_SCALING_ONEPASS) {
       std::vector<double> ones(n, 1.0);
       CK(cudaMemcpyAsync(F->scale, ones.data(), n * 8, cudaMemcpyHostToDevice, F->st));

@@ -54,11 +54,15 @@ def as_hi(x):
     return x.astype(np.complex128 if np.iscomplexobj(x) else np.float64)
 
 
-@pytest.mark.parametrize("complex_", [False, True])
-def test_tensor_cmod_entrywise_on_fixed_pivot_sequence(complex_):
-    a = spd3d(20, complex_)
+@pytest.mark.parametrize("complex_,side,metis", [(False, 20, False), (True, 20, False), (False, 28, True),
+                                                 (True, 28, True)])
+def test_tensor_cmod_entrywise_on_fixed_pivot_sequence(complex_, side, metis):
+    """MetisND structures add wide separator updaters: updates of more than
+    64 columns (several W column tiles), taller than 128 rows, many K chunks."""
+    a = spd3d(side, complex_)
     dt = np.complex64 if complex_ else np.float32
-    sym = LdltSymbolic.analyze(a)
+    from rslab_b200 import Ordering
+    sym = LdltSymbolic.analyze_with(a, SolverSettings(ordering=Ordering.METIS_ND if metis else Ordering.AMD))
     f64 = sym.factor(a).export_factors()
     tc = sym.factor(a.astype(dt), SolverSettings(schur_engine="tensor")).export_factors()
     fma = sym.factor(a.astype(dt), SolverSettings(schur_engine="fma")).export_factors()
