@@ -652,6 +652,11 @@ def run_batch(args, ws, rank, local):
         barrier(ws)
         return tot / steps, last
 
+    # the engine and launch schedule of this batch, measured on it before the
+    # timed region (the analysis-time block width stays at its default)
+    from rslab_b200.autotune import candidates, tune_mixed
+    tuned = tune_mixed(a, b, args.target, sym=sym, cands=candidates(), reps=2, warmup=1)
+    st = tuned.settings(SolverSettings())
     mixed = MixedLdltSolver.factor_with(a, st, sym=sym)
 
     def mixed_step():
@@ -694,7 +699,7 @@ def run_batch(args, ws, rank, local):
     torch.cuda.synchronize()
     out64 = None
     if not args.no_fp64:
-        f64 = sym.factor(a, st)
+        f64 = sym.factor(a, SolverSettings())
 
         def fp64_step():
             rc = N.lib.rslab_refactor(f64._h, C.c_void_p(vals_d.data_ptr()), 1)
@@ -720,6 +725,10 @@ def run_batch(args, ws, rank, local):
                        "factor_launches": int(info.n_factor_launches), "analysis_s": t_an,
                        "parallelism": f"systems split over {ws} rank(s) by weight",
                        "l2": "flushed between steps (256 MB write)"},
+            "autotune": {"chosen": {"schur_engine": tuned.chosen[0], "overlap": tuned.chosen[1],
+                                    "panel_nb": tuned.chosen[2]},
+                         "ms_per_candidate": tuned.table(), "tuning_s": tuned.tuning_seconds,
+                         "note": "measured before the timed region: refactor + solve with host buffers"},
             "mixed": {"certified_units": int(res.certified.sum()), "units": int(res.certified.size),
                       "max_backward_error": float(res.backward_error.max()), "ir_iters": int(minfo.ir_iters),
                       "gmres_iters": int(minfo.gmres_iters)},
@@ -878,27 +887,31 @@ def main():
     except Exception:
         pass
     peak_tf = float(peaks.get("bf16_tflops", 1590.0))
-    # Dominant kernel: the tensor-core descendant update k_cmod_tc (3xTF32).
-    # Time from the per-launch trace of the eager refactor above; algorithmic
-    # flops = the cmod model flops; DRAM traffic per flop from the committed
-    # ncu summary (captured on the 48^3 case, scaled by flops).
+    # Dominant kernel: the tensor-core descendant update, k_cmod_mm (3xTF32
+    # GEMM tiles in the updater's row space).  Time from the per-launch trace
+    # of the eager refactor above; algorithmic flops = the cmod model flops
+    # (multiply + add of every (r >= c) update entry).  The assembly and the
+    # operand split are reported beside it.
     from rslab_b200.solver import profile_trace
     factor_profile(mixed._h)
     tr = profile_trace(mixed._h)
-    tc_ms = sum(ms for k, _, ms in tr if k == "cmod_tc")
-    tc_n = sum(1 for k, _, _ in tr if k == "cmod_tc")
+    mm_ms = sum(ms for k, _, ms in tr if k == "cmod_mm")
+    mm_n = sum(1 for k, _, _ in tr if k == "cmod_mm")
+    asm_ms = sum(ms for k, _, ms in tr if k == "cmod_asm")
+    split_ms = sum(ms for k, _, ms in tr if k in ("split_r", "split_c"))
     cm = prof_mixed["cmod"]
-    ach = cm["flops"] / (tc_ms * 1e-3) / 1e12 if tc_ms > 0 else 0.0
-    roofline = {"bound": "tensor", "kernel": "k_cmod_tc (c32, tcgen05 kind::tf32, 3xTF32 split)",
+    ach = cm["flops"] / (mm_ms * 1e-3) / 1e12 if mm_ms > 0 else 0.0
+    roofline = {"bound": "tensor", "kernel": "k_cmod_mm (c32, tcgen05 kind::tf32, 3xTF32 split, TMA-staged)",
                 "achieved": ach, "peak": peak_tf, "unit": "TFLOP/s", "frac": ach / peak_tf,
                 "traffic": None,
                 "traffic_note": "not measured by this run: dram bytes per launch come from an ncu capture "
                                 "of the kernel (profiles/)",
                 "peak_source": ("MEASURED_PEAKS.json bf16_tflops (burst), of measured" if "bf16_tflops" in peaks
                                 else "fallback 1590 TFLOP/s"),
-                "launches": tc_n, "avg_launch_ms": tc_ms / max(tc_n, 1),
+                "launches": mm_n, "avg_launch_ms": mm_ms / max(mm_n, 1),
+                "assembly_ms": asm_ms, "split_ms": split_ms,
                 "tf32_pipe_frac": 3.0 * ach / (peak_tf / 2.0),
-                "note": "achieved = algorithmic flops / time; the 3xTF32 split issues 3 tf32 products per "
+                "note": "achieved = algorithmic flops / k_cmod_mm time; the 3xTF32 split issues 3 tf32 products per "
                         "flop on a pipe with half the bf16 rate, tf32_pipe_frac = 3 x achieved / (peak / 2)"}
 
     # End-to-end through the public API with host buffers: the step's inputs

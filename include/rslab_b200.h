@@ -100,6 +100,9 @@ typedef struct {
   int32_t schur_engine;        /* RSLAB_SCHUR_*: how f32/c32 descendant updates run */
   double drop_tol;             /* > 0: incomplete factor, drop |L_ip| < drop_tol * max_i |L_ip| per
                                 * column (SolverSettings::drop_tol, multifrontal_ldlt.rs:2359-2367) */
+  int32_t overlap;             /* schedule: run the Schur update beyond the next block and the next
+                                * level's early descendant updates on side streams (1, default) or
+                                * everything in order on one stream (0); the factor is the same */
 } rslab_factor_settings;
 
 /* Descendant (cmod) updates of the single-precision fields: 3xTF32 split
@@ -218,6 +221,16 @@ int rslab_mixed_batch_result(const rslab_fac_handle* fac, int64_t cap, double* b
 int rslab_factor(rslab_sym_handle* sym, int dtype, const void* values, int values_on_device,
                  const rslab_factor_settings* settings, rslab_fac_handle** out);
 int rslab_refactor(rslab_fac_handle* fac, const void* values, int values_on_device);
+/* Static pivot reuse across a value sweep of one pattern (the LDL^T
+ * counterpart of the reference's static-pivot sweep,
+ * src/numeric/multifrontal_lu.rs:3551: factor once with the pivot search,
+ * then refactor new values without it).  Every factor that searches records
+ * its Bunch-Kaufman steps (1x1 / 2x2 and the interchange of each step); with
+ * on = 1 the following refactors replay that record instead of searching, a
+ * zero or (with static pivoting) tiny pivot being perturbed as usual; on = 0
+ * restores the search.  Pair it with refinement (rslab_mixed_solve) and fall
+ * back to a searching refactor when a solve does not certify. */
+int rslab_set_pivot_reuse(rslab_fac_handle* fac, int on);
 /* x = A^-1 b, b and x row-major n x nrhs. */
 int rslab_solve(rslab_fac_handle* fac, const void* b, int64_t nrhs, void* x, int on_device);
 /* LdltSolver::solve_refined (src/numeric/sparse_solver.rs:335-375): solve, then
@@ -239,14 +252,16 @@ int rslab_factor_profile(rslab_fac_handle* fac, double* kind_ms, int64_t* kind_l
 int rslab_solve_profile(rslab_fac_handle* fac, int64_t nrhs, double* kind_ms, int64_t* kind_launches);
 /* Per-launch rows of the handle's last factor/solve profile: launch kind
  * (0 cmod, 1 getf2, 2 deep replay, 3 panel Schur, 4 forward diagonal,
- * 5 forward push, 6 backward dots, 7 backward diagonal, 8-11 unused, 12
+ * 5 forward push, 6 backward dots, 7 backward diagonal, 8-11 see below, 12
  * forward gather, 13 tensor-core cmod, 14 G = L21 D, 15 diagonal-block
  * inverses, 16 backward partial-sum reduction, 17 tensor-core panel Schur,
  * 18/19 forward/backward block-chain solve, 20 backward gather, 21 deep rows
  * as a product with the block transform, 22 block transform, 23 forward push
  * partial-sum reduction, -1 other), grid
  * size and device ms.  *count = rows available; at most cap are written.
- * A measurement aid with no reference counterpart. */
+ * A measurement aid with no reference counterpart.  Kinds 8-11 are the
+ * tensor-core cmod's GEMM tiles, its assembly and the real / complex operand
+ * split. */
 int rslab_profile_trace(const rslab_fac_handle* fac, int64_t cap, int32_t* kind, int32_t* grid, float* ms,
                         int64_t* count);
 /* Reference LdltFactors layout; pass NULL arrays to query *nnz_out first. */

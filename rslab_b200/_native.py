@@ -46,6 +46,7 @@ class FactorSettings(C.Structure):
         ("stream", vp),
         ("schur_engine", C.c_int32),
         ("drop_tol", C.c_double),
+        ("overlap", C.c_int32),
     ]
 
 
@@ -105,6 +106,7 @@ SIGNATURES = {
     "rslab_factor": (C.c_int, [vp, C.c_int, vp, C.c_int, C.POINTER(FactorSettings), C.POINTER(vp)]),
     "rslab_refactor": (C.c_int, [vp, vp, C.c_int]),
     "rslab_solve": (C.c_int, [vp, vp, C.c_int64, vp, C.c_int]),
+    "rslab_set_pivot_reuse": (C.c_int, [vp, C.c_int]),
     "rslab_factor_info": (C.c_int, [vp, C.POINTER(FactorInfo)]),
     "rslab_factor_stream": (vp, [vp]),
     "rslab_export_factors": (C.c_int, [vp, i64p, i64p, vp, vp, vp, C.POINTER(C.c_uint8), i64p,

@@ -54,6 +54,12 @@ struct FactorArgs {
   const long long* goff;
   const double* floor_dev;  // non-null: static-pivot floor computed on the device (force-accept)
   int deep_mm;              // tall panels: getf2 forms the block transform M, k_deep_mm applies it
+  // Pivot record (e-indexed, block-local): kp for a 1x1 step at e, -(kp + 1)
+  // for a 2x2 step starting at e.  Written by every factor that searches; when
+  // *pivot_reuse is set, getf2 replays the recorded steps instead of searching
+  // (static pivot reuse across a value sweep of one pattern).
+  int* pivrec;
+  const int* pivot_reuse;
 };
 
 // Byte offset of the block transform M in a getf2 scratch slot, and the slot
@@ -881,9 +887,19 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
   // Warp 0: decide step k into multiplier set / control slot `par`.  With
   // `full` false, returns false (writing nothing) when the row-maximum test
   // is needed.
+  const bool reuse = fa.pivot_reuse && fa.pivrec && *fa.pivot_reuse != 0;
+  int* prec = fa.pivrec ? fa.pivrec + first + kb : nullptr;  // no record without a handle
   auto decide = [&](int k, int par, bool full) -> bool {
     T *L1, *L2, *U1, *U2;
     bufs(par, L1, L2, U1, U2);
+    int kstep = 1, kp = k;
+    bool err = false;
+    if (reuse) {
+      // the recorded step: no search (a zero pivot is still caught below)
+      const int code = prec[k];
+      kstep = code < 0 ? 2 : 1;
+      kp = code < 0 ? -code - 1 : code;
+    } else {
     // |a_kk| first: independent of the column scan, its latency overlaps it
     const double absakk = F::mag(A[pk(k, k, pw)]);
     double v = -1.0;
@@ -897,8 +913,6 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
     warp_argmax(v, idx);
     const double colmax = sqrt(v > 0.0 ? v : 0.0);
     const int imax = v > 0.0 ? idx : k;
-    int kstep = 1, kp = k;
-    bool err = false;
     if (fmax(absakk, colmax) == 0.0) {
       err = pfloor < 0.0;
     } else if (absakk >= alpha * colmax) {
@@ -917,6 +931,8 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
         kstep = 2;
         kp = imax;
       }
+    }
+    if (lane == 0 && !err && prec) prec[k] = kstep == 2 ? -kp - 1 : kp;
     }
     if (!err) {
       const int p = kstep == 1 ? k : k + 1;

@@ -963,6 +963,11 @@ struct rslab_fac_handle {
   float *sp_ahi = nullptr, *sp_alo = nullptr, *sp_bhi = nullptr, *sp_blo = nullptr;
   float* wbuf = nullptr;
   CUtensorMap* tmaps = nullptr;
+  // static pivot reuse: the pivot record of the last searching factor and the
+  // device flag that makes getf2 replay it (read inside the captured graph)
+  int* pivrec = nullptr;
+  int* pivot_reuse = nullptr;
+  bool reuse_on = false;
   // graph of the numeric factor (values read from `aval`)
   cudaGraphExec_t fgraph = nullptr;
   // solve workspace
@@ -1041,6 +1046,8 @@ FactorArgs make_fargs(rslab_fac_handle& F) {
   a.gpool = F.gpool;
   a.goff = H.d_goff;
   a.floor_dev = F.floor_dev;
+  a.pivrec = F.pivrec;
+  a.pivot_reuse = F.pivot_reuse;
   if (F.set.on_zero_pivot == RSLAB_PIVOT_FORCE_ACCEPT) a.perturb_floor = 0.0;
   return a;
 }
@@ -1111,7 +1118,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
   // Launches marked `side` (the Schur update beyond the next block) run on
   // the side stream when not profiling; every later launch except the next
   // block's getf2 / deep-row launches waits for them first.
-  const bool overlap = prof == nullptr && F.st2 != nullptr;
+  const bool overlap = prof == nullptr && F.st2 != nullptr && F.set.overlap != 0;
   bool side_pending = false;
   auto runs = [&](const Launch& L) {
     switch (L.kind) {
@@ -1743,6 +1750,7 @@ void rslab_default_factor_settings(rslab_factor_settings* s) {
   s->stream = nullptr;
   s->schur_engine = RSLAB_SCHUR_TENSOR;
   s->drop_tol = 0.0;
+  s->overlap = 1;
 }
 
 int rslab_validate_lower_csc(int64_t n, const int64_t* col_ptr, const int64_t* row_idx, int64_t nnz) {
@@ -2134,6 +2142,9 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
     F->dsub = F->al<unsigned char>(n * es);
     F->kind = F->al<unsigned char>(n);
     F->lperm = F->al<int>(n);
+    F->pivrec = F->al<int>(std::max(n, 1));
+    F->pivot_reuse = F->al<int>(1);
+    CK(cudaMemsetAsync(F->pivot_reuse, 0, sizeof(int), F->st));
     F->scale = F->al<double>(n);
     F->rowmax = F->al<unsigned long long>(n);
     F->status = F->al<int>(4);
@@ -2227,6 +2238,19 @@ int rslab_refactor(rslab_fac_handle* F, const void* values, int values_on_device
     return fail(e);
   } catch (const std::exception& e) {
     return fail(RslabError(Status::InvalidInput, e.what()));
+  }
+}
+
+int rslab_set_pivot_reuse(rslab_fac_handle* F, int on) {
+  try {
+    if (!F) throw RslabError(Status::InvalidInput, "null handle");
+    const int v = on ? 1 : 0;
+    CK(cudaMemcpyAsync(F->pivot_reuse, &v, sizeof(int), cudaMemcpyHostToDevice, F->st));
+    CK(cudaStreamSynchronize(F->st));
+    F->reuse_on = v != 0;
+    return 0;
+  } catch (const RslabError& e) {
+    return fail(e);
   }
 }
 

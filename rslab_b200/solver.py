@@ -204,6 +204,9 @@ class SolverSettings:
     schur_engine: str = "tensor"
     # incomplete factor: drop |L_ip| < drop_tol * max_i |L_ip| per column
     drop_tol: Optional[float] = None
+    # schedule of the factor's launches: side streams overlap independent
+    # work (True) or everything runs in order on one stream (False)
+    overlap: bool = True
 
     @staticmethod
     def exact() -> "SolverSettings":
@@ -268,6 +271,7 @@ class SolverSettings:
         s.use_graph = int(self.use_graph)
         s.stream = stream
         s.schur_engine = N.SCHUR_FMA if self.schur_engine == "fma" else N.SCHUR_TENSOR
+        s.overlap = int(bool(self.overlap))
         return s
 
 
@@ -499,6 +503,11 @@ class LdltSolver:
         vals = np.ascontiguousarray(a.values, dtype=self.dtype)
         _check(N.lib.rslab_refactor(self._h, vals.ctypes.data_as(C.c_void_p), 0))
 
+    def reuse_pivots(self, on: bool = True) -> None:
+        """Static pivot reuse: the following refactors replay the pivot steps
+        of the last factor that searched (rslab_set_pivot_reuse)."""
+        _check(N.lib.rslab_set_pivot_reuse(self._h, int(bool(on))))
+
     def _info(self) -> N.FactorInfo:
         inf = N.FactorInfo()
         _check(N.lib.rslab_factor_info(self._h, C.byref(inf)))
@@ -717,6 +726,11 @@ class MixedLdltSolver:
         vals = np.ascontiguousarray(a.values, dtype=self.dtype)
         _check(N.lib.rslab_refactor(self._h, vals.ctypes.data_as(C.c_void_p), 0))
 
+    def reuse_pivots(self, on: bool = True) -> None:
+        """Static pivot reuse: the following refactors replay the pivot steps
+        of the last factor that searched (rslab_set_pivot_reuse)."""
+        _check(N.lib.rslab_set_pivot_reuse(self._h, int(bool(on))))
+
     def solve(self, a: CscMatrix, b) -> tuple:
         return self.solve_to(a, b, CERT_FACTOR * EPS_F64)
 
@@ -781,7 +795,7 @@ def solve_profile(handle, nrhs: int) -> dict:
 
 
 LAUNCH_KINDS = ("cmod", "getf2", "deep_replay", "panel_schur", "fwd_diag", "fwd_push", "bwd_off", "bwd_diag",
-                "unused8", "unused9", "unused10", "unused11", "fwd_gather", "cmod_tc", "make_g", "diag_inv",
+                "cmod_mm", "cmod_asm", "split_r", "split_c", "fwd_gather", "cmod_tc", "make_g", "diag_inv",
                 "bwd_off_reduce", "schur_tc", "fwd_chain", "bwd_chain", "bwd_gather", "deep_mm", "make_m", "push_reduce",
                 "join")
 
