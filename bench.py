@@ -64,6 +64,8 @@ def parse():
     p.add_argument("--tier-model", default=None, help="tier network .npz (default: the package's trained one)")
     p.add_argument("--sweep-side", type=int, default=48)
     p.add_argument("--sweep-count", type=int, default=64)
+    p.add_argument("--no-pivot-reuse", action="store_true",
+                   help="sweep: search pivots at every frequency instead of replaying the first factor's")
     p.add_argument("--sweep-fp64-count", type=int, default=4,
                    help="frequencies (evenly spread) timed on the plain FP64 path for the ratio")
     p.add_argument("--profile-step", action="store_true",
@@ -285,31 +287,41 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
-def sweep_cpu_sample(side: int = 24, count: int = 4):
-    """The oracle on a bounded sample of the sweep: the same 27-point
-    K - w^2 M + i w C family on a side^3 grid, FP64 factor + 8-RHS solve at
-    `count` frequencies spread over the band."""
-    from oracle.oracle import OracleSolver, backward_error
-    from rslab_b200 import LdltSymbolic, matgen
-    from rslab_b200.sweep import sweep_settings
+def sweep_cpu_sample(side: int = 48, count: int = 4):
+    """The oracle (timing mode, all host threads) on a bounded sample of the
+    sweep: the full 48^3 27-point K - w^2 M + i w C matrix at `count`
+    frequencies spread over the band, FP64 factor + 8-RHS solve each, on the
+    oracle's own structure for the tuned ordering (MetisND here)."""
+    from oracle.oracle import OracleSolver, backward_error, oracle_structure, set_parallel
+    from rslab_b200 import LdltSymbolic, Ordering, matgen
+    from rslab_b200.solver import amd_order, metis_order
+    set_parallel(True)
     c4 = matgen.C4System(side, 3)
     om = c4.omegas(64)[np.linspace(0, 63, count).round().astype(int)]
     b = matgen.uniform_rhs(c4.n, 8, 4, complex_=True)
-    sym = LdltSymbolic.analyze_with(c4.matrix(om[0]), sweep_settings())
-    flops = 4.0 * sym.info().flops_model
-    ex = sym.export()
+    a0 = c4.matrix(om[0])
+    _, st = LdltSymbolic.tuned(a0)
+    full = a0.to_scipy_full().tocsc()
+    full.sort_indices()
+    cp, ri = np.asarray(full.indptr, np.int64), np.asarray(full.indices, np.int64)
+    nd = st.ordering == Ordering.METIS_ND
+    ex = oracle_structure(a0, metis_order(a0.n, cp, ri) if nd else amd_order(a0.n, cp, ri)[0])
+    c, r = ex["sn_ncol"].astype(np.float64), ex["sn_nrow"].astype(np.float64)
+    m = r - c + 1.0
+    flops = 4.0 * float(np.sum((r * (r + 1) * (2 * r + 1) - (m - 1) * m * (2 * m - 1)) / 6.0 - c))
     t = 0.0
     be = 0.0
     for w in om:
         a = c4.matrix(w)
         t0 = time.perf_counter()
-        x = OracleSolver(a, ex).solve_many(b, 8)
+        x = OracleSolver(a, ex, perturb_floor=1e-10).solve_many(b, 8)
         t += time.perf_counter() - t0
         be = max(be, backward_error(a, x, b))
     return {"value": flops * len(om) / t / 1e9, "unit": "GFLOP/s", "cores": os.cpu_count(), "kind": "port",
             "seconds": t,
             "sample": f"FP64 factor + 8-RHS solve of the {side}^3 27-point sweep matrix at {len(om)} frequencies "
-                      f"(n={c4.n}, model flops {flops:.3g} each); max backward error {be:.2e}"}
+                      f"({'MetisND' if nd else 'AMD'}, n={c4.n}, model flops {flops:.3g} each, static pivoting at "
+                      f"1e-10); max backward error {be:.2e}; oracle timing mode, {os.cpu_count()} threads"}
 
 
 def run_sweep(args, ws, rank, local):
@@ -338,6 +350,11 @@ def run_sweep(args, ws, rank, local):
     b = matgen.uniform_rhs(c4.n, nrhs, 4, complex_=True)
     st = sweep_settings()
     mats = [c4.matrix(om_all[i]) for i in mine]
+    # the ordering of the default settings pick (LdltSolver::tuned): the
+    # nested-dissection bakeoff adopts MetisND on this 27-point grid
+    from rslab_b200 import Ordering
+    _, st_t = LdltSymbolic.tuned(mats[0])
+    st.ordering = st_t.ordering
     sym = LdltSymbolic.analyze_with(mats[0], st)
     info = sym.info()
     flops = 4.0 * info.flops_model
@@ -347,16 +364,32 @@ def run_sweep(args, ws, rank, local):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     mixed = MixedLdltSolver.factor_with(mats[0], st, sym=sym)
     stream = torch.cuda.ExternalStream(mixed.stream())
+    reuse = not args.no_pivot_reuse
+    # static pivot reuse: the factor above searched and recorded its pivot
+    # steps; every refactor of the sweep replays them, falling back to a
+    # searching refactor for a frequency that does not certify
+    if reuse:
+        mixed.reuse_pivots(True)
+    fallbacks = [0]
+
+    def solve_one(v):
+        rc = N.lib.rslab_refactor(mixed._h, C.c_void_p(v.data_ptr()), 1)
+        assert rc == 0, N.last_error()
+        inf = N.MixedInfoC()
+        rc = N.lib.rslab_mixed_solve(mixed._h, C.c_void_p(b_d.data_ptr()), nrhs, args.target,
+                                     C.c_void_p(x_d.data_ptr()), 1, C.byref(inf))
+        assert rc == 0, N.last_error()
+        return inf
 
     def sweep_step():
         infos = []
         for v in vals_d:
-            rc = N.lib.rslab_refactor(mixed._h, C.c_void_p(v.data_ptr()), 1)
-            assert rc == 0, N.last_error()
-            inf = N.MixedInfoC()
-            rc = N.lib.rslab_mixed_solve(mixed._h, C.c_void_p(b_d.data_ptr()), nrhs, args.target,
-                                         C.c_void_p(x_d.data_ptr()), 1, C.byref(inf))
-            assert rc == 0, N.last_error()
+            inf = solve_one(v)
+            if reuse and not inf.certified:
+                fallbacks[0] += 1
+                N.lib.rslab_set_pivot_reuse(mixed._h, 0)
+                inf = solve_one(v)
+                N.lib.rslab_set_pivot_reuse(mixed._h, 1)
             infos.append((inf.certified, inf.backward_error, inf.ir_iters, inf.gmres_iters))
         return infos
 
@@ -442,13 +475,16 @@ def run_sweep(args, ws, rank, local):
             "scaling": "strong", "vs_baseline": None, "dtype": "c32 factor / f64 refinement", "data": "synthetic",
             "config": {"workload": f"freq_sweep_{args.sweep_side}^3_27pt_c32_nrhs{nrhs}_{len(om_all)}w",
                        "n": c4.n, "nnz_lower": mats[0].nnz, "frequencies": len(om_all), "nrhs": nrhs,
-                       "ordering": "AMD", "static_pivot": 1e-10, "target_backward_error": args.target,
-                       "model_flops_per_frequency": flops, "parallelism": f"frequencies round-robin over {ws}",
+                       "ordering": "MetisND" if st.ordering == Ordering.METIS_ND else "AMD",
+                       "static_pivot": 1e-10, "target_backward_error": args.target,
+                       "pivot_reuse": reuse, "model_flops_per_frequency": flops,
+                       "parallelism": f"frequencies round-robin over {ws}",
                        "l2": "flushed between steps (256 MB write)"},
             "sweep": {"ms_per_frequency": ms_sweep / len(mine),
                       "certified": int(sum(1 for c, *_ in infos if c)), "of": len(infos),
                       "max_backward_error": max(be for _, be, _, _ in infos),
                       "ir_iters_max": max(i for _, _, i, _ in infos),
+                      "searching_refactors_after_failure": fallbacks[0],
                       "gmres_iters_max": max(g for *_, g in infos)},
             "fp64_gpu": out_fp64,
             "e2e": {"value": flops * len(mine) / e2e_s / 1e9 * ws, "unit": "GFLOP/s", "seconds_per_step": e2e_s,

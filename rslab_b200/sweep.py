@@ -24,19 +24,45 @@ def sweep_settings() -> SolverSettings:
     return SolverSettings.preconditioner(1e-10)
 
 
-def frequency_sweep(matrices, b: np.ndarray, target: float = 1e-14,
-                    settings: Optional[SolverSettings] = None) -> Iterator[Tuple[int, np.ndarray, MixedInfo]]:
+def frequency_sweep(matrices, b: np.ndarray, target: float = 1e-14, settings: Optional[SolverSettings] = None,
+                    reuse_pivots: bool = False,
+                    stats: Optional[dict] = None) -> Iterator[Tuple[int, np.ndarray, MixedInfo]]:
     """Yield (index, x, info) for every matrix of `matrices` (an iterable of
-    CscMatrix on one pattern), solving A_i x = b to `target`."""
+    CscMatrix on one pattern), solving A_i x = b to `target`.
+
+    reuse_pivots: static pivot reuse (the counterpart of the reference's
+    static-pivot sweep, src/numeric/multifrontal_lu.rs:3551): the first
+    matrix is factored with the Bunch-Kaufman search, which records its
+    pivot steps, and the following refactors replay them without searching;
+    a frequency whose refined solve does not certify is refactored with the
+    search (which records its steps afresh) and solved again.  `stats`
+    (optional) receives the counts of reused and re-searched factors."""
     st = settings or sweep_settings()
     solver = None
+    if stats is not None:
+        stats.update(reused=0, searched=0, refactored_after_failure=0)
     for i, a in enumerate(matrices):
         if solver is None:
             sym = LdltSymbolic.analyze_with(a, st)
             solver = MixedLdltSolver.factor_with(a, st, sym=sym)
-        else:
-            solver.refactor(a)
+            if stats is not None:
+                stats["searched"] += 1
+            if reuse_pivots:
+                solver.reuse_pivots(True)
+            x, info = solver.solve_to(a, b, target)
+            yield i, x, info
+            continue
+        solver.refactor(a)
+        if stats is not None:
+            stats["reused" if reuse_pivots else "searched"] += 1
         x, info = solver.solve_to(a, b, target)
+        if reuse_pivots and not info.certified:
+            solver.reuse_pivots(False)
+            solver.refactor(a)
+            solver.reuse_pivots(True)
+            x, info = solver.solve_to(a, b, target)
+            if stats is not None:
+                stats["refactored_after_failure"] += 1
         yield i, x, info
 
 
