@@ -253,7 +253,7 @@ int rslab_solve_profile(rslab_fac_handle* fac, int64_t nrhs, double* kind_ms, in
 /* Per-launch rows of the handle's last factor/solve profile: launch kind
  * (0 cmod, 1 getf2, 2 deep replay, 3 panel Schur, 4 forward diagonal,
  * 5 forward push, 6 backward dots, 7 backward diagonal, 8-11 see below, 12
- * forward gather, 13 tensor-core cmod, 14 G = L21 D, 15 diagonal-block
+ * forward gather, 13 unused, 14 G = L21 D, 15 diagonal-block
  * inverses, 16 backward partial-sum reduction, 17 tensor-core panel Schur,
  * 18/19 forward/backward block-chain solve, 20 backward gather, 21 deep rows
  * as a product with the block transform, 22 block transform, 23 forward push

@@ -1,27 +1,22 @@
-// Tensor-core cmod for the single-precision factor fields (f32, c32):
-// the descendant updates of one 128 x 64 target tile accumulate in TMEM with
-// tcgen05.mma kind::tf32 in the 3xTF32 split (hi*hi + hi*lo + lo*hi), and the
-// tile is read-modify-written once at the end.
+// The 3xTF32 tensor-core tile pipeline of the single-precision fields, used by
+// the deferred in-panel Schur update (k_schur_tc): the update of one 128 x 64
+// target tile accumulates in TMEM with tcgen05.mma kind::tf32 in the 3xTF32
+// split (hi*hi + hi*lo + lo*hi), and the tile is read-modify-written once at
+// the end.  Also here: k_make_g (G_k = L21_k D_k of every updater, read by the
+// CUDA-core cmod) and the shared tcgen05 staging helpers.
 //
-// Task (s, rt << 16 | ct, pair_begin, pair_end): tile rows [128 rt, +128) x
-// columns [64 ct, +64) of s's panel.  Pair (k, a, q0, nr << 16 | nc): k's
-// off-diagonal rows [a, a+nr) land on tile rows, its rows [q0, q0+nc) on
-// tile columns; U = L_k[a.., :] D_k L_k[q0.., :]^T.  The scatter is applied
-// while staging: operand row t of A holds the k row that maps to tile row t
-// (zero when none), operand row u of B holds the row of G = L_k D_k that
-// maps to tile column u, so every pair of every updater adds into the same
-// accumulator and the K dimension is the concatenation of the updaters'
-// columns.  Complex operands use the real embedding
+// The pipeline is generic over its operand source (Src): operand row t of A
+// holds the source row that maps to tile row t (zero when none), operand row
+// u of B the row of G = L D that maps to tile column u, and the K dimension is
+// the concatenation of the source's K-ranges.  Complex operands use the real
+// embedding
 //   A' = [Ar | Ai],  B' = [[Gr, -Gi], [Gi, Gr]]  ->  A' B'^T = [Re | Im],
-// i.e. M = 128, N = 128, and 16 complex columns of k per 32-wide K stage.
-//
-// G_k = L21_k D_k is formed once per updater (k_make_g, after k's level is
-// factored), so staging is plain loads plus the hi/lo split.
-// Warp-specialised pipeline (one CTA per SM): 16 producer warps load, split
-// and store K chunks into three shared-memory stages and arrive on the
+// i.e. M = 128, N = 128, and 16 complex columns per 32-wide K stage.
+// Warp-specialised (one CTA per SM): 16 producer warps load, split and store
+// K chunks (A into TMEM, B into three shared-memory stages) and arrive on the
 // stage's `full` mbarrier; one MMA warp waits on `full`, issues the 12
-// tcgen05.mma of the chunk and commits to the stage's `empty` mbarrier,
-// which gates the stage's reuse.  No block-wide barrier in the main loop.
+// tcgen05.mma of the chunk and commits to the stage's `empty` mbarrier.  No
+// block-wide barrier in the main loop.
 // Accuracy: the tensor pipe does not round its accumulation to nearest, so
 // the sum runs in windows of TC_WIN chunks over two TMEM accumulators; the
 // producers add each finished window into per-thread fp32 registers (round
@@ -29,7 +24,7 @@
 // signal the MMA warp (`promoted` mbarrier) before the accumulator is reused.
 // Every wait is bounded; on a timeout the kernel flags status 2, drains what
 // it issued (bounded) and frees its TMEM.
-// Reference: ll_factor_node cmod, src/numeric/multifrontal_ldlt.rs:2452-2728.
+// Reference: ll_cdiv_emit deferred Schur, src/numeric/multifrontal_ldlt.rs:3085-3167.
 #pragma once
 
 #include "factor_kernels.cuh"
@@ -393,47 +388,6 @@ __device__ __forceinline__ void tc_tile_pipeline(const FactorArgs& fa, const Src
   if (warp == 0) tmem_dealloc(tmem, TC_TMEM_COLS);
 }
 
-
-// cmod source: the (updater, tile) pairs of the task; A' = updater rows from
-// its panel, B' = rows of its precomputed G_k, through the int8 inverse maps.
-template <typename T>
-struct CmodSrc {
-  static constexpr bool kBonfly = false;
-  const FactorArgs* fa;
-  const int4* pairs;
-  const int8_t* maps;
-  int pb, pe;
-  __device__ int npairs() const { return pe - pb; }
-  __device__ int ncols(int u) const { return fa->sn_ncol[pairs[pb + u].x]; }
-  __device__ void open(TcCur<T>& x, int u, int row, int col) const {
-    const int4 pr = pairs[pb + u];
-    const int k = pr.x, a = pr.y, q0 = pr.z;
-    const int nck = fa->sn_ncol[k], nrk = fa->sn_nrow[k];
-    const int8_t* m = maps + (long long)(pb + u) * TC_MAP;
-    x.i = m[row];
-    x.j = m[TC_M + col];
-    x.lda = nrk;
-    x.ldb = nrk - nck;
-    x.Ar = reinterpret_cast<const T*>(fa->panel) + fa->sn_poff[k] + nck + a + x.i;
-    x.Br = reinterpret_cast<const T*>(fa->gpool) + fa->goff[k] + q0 + x.j;
-    x.dk = nullptr;
-    x.dsk = nullptr;
-    x.kk = nullptr;
-  }
-};
-
-template <typename T>
-__global__ void __launch_bounds__(TC_NT, 1) k_cmod_tc(FactorArgs fa, const int4* __restrict__ tasks,
-                                                      const int4* __restrict__ pairs,
-                                                      const int8_t* __restrict__ maps) {
-  if (fa.status[0] != 0) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];  // re-aligned to 1024 inside
-  const int4 tk = tasks[blockIdx.x];
-  const int s = tk.x, r0 = (tk.y >> 16) * TC_M, c0 = (tk.y & 0xffff) * TC_N;
-  const int ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
-  CmodSrc<T> src{&fa, pairs, maps, tk.z, tk.w};
-  tc_tile_pipeline<T>(fa, src, s, 0, 0, r0, c0, min(TC_M, nrow - r0), min(TC_N, ncol - c0), smem_raw);
-}
 
 // In-panel (deferred) Schur source of block [kb, ke) of supernode s: one
 // K-range of pw columns; A' = L21 rows [ke + r0, ...) of the panel (every

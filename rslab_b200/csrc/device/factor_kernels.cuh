@@ -895,10 +895,13 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
     int kstep = 1, kp = k;
     bool err = false;
     if (reuse) {
-      // the recorded step: no search (a zero pivot is still caught below)
+      // the recorded step: no search (a zero pivot is still caught below).
+      // An early decision (other warps still updating) may only take a 1x1
+      // step without interchange, as in the search below: defer the rest.
       const int code = prec[k];
       kstep = code < 0 ? 2 : 1;
       kp = code < 0 ? -code - 1 : code;
+      if (!full && (kstep != 1 || kp != k)) return false;
     } else {
     // |a_kk| first: independent of the column scan, its latency overlaps it
     const double absakk = F::mag(A[pk(k, k, pw)]);

@@ -107,7 +107,7 @@ size_t elem_size(int dtype) {
 enum LaunchKind {
   L_CMOD, L_GETF2, L_DEEP, L_SCHUR,
   L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD,
-  L_MM_GEMM, L_MM_ASM, L_SPLIT_R, L_SPLIT_C, L_FWD_GATHER, L_CMOD_TC, L_MAKE_G, L_DIAG_INV,
+  L_MM_GEMM, L_MM_ASM, L_SPLIT_R, L_SPLIT_C, L_FWD_GATHER, L_UNUSED13, L_MAKE_G, L_DIAG_INV,
   L_BWD_OFF_RED, L_SCHUR_TC, L_FWD_CHAIN, L_BWD_CHAIN, L_BWD_GATHER, L_DEEP_MM, L_MAKE_M,
   L_FWD_PUSH_RED,
   L_JOIN_CM  // no kernel: the level's early cmod updates must be complete from here on
@@ -903,7 +903,6 @@ struct KernelSetup {
     const size_t es = sizeof(T);
     if constexpr (TensorCmod<T>::ok) {
       CK(cudaFuncSetAttribute(k_cmod_mm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_mm_bytes()));
-      CK(cudaFuncSetAttribute(k_cmod_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_tc_bytes()));
       CK(cudaFuncSetAttribute(k_schur_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_tc_bytes()));
     }
     CK(cudaFuncSetAttribute(k_cmod<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_bytes<T>()));
@@ -1123,7 +1122,6 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
   auto runs = [&](const Launch& L) {
     switch (L.kind) {
       case L_CMOD: return !use_tc;
-      case L_CMOD_TC: return false;  // superseded by the updater-space GEMM + assembly
       case L_MM_GEMM: case L_MM_ASM: return use_tc;
       case L_SPLIT_R: return use_tc && !Field<T>::complex;
       case L_SPLIT_C: return use_tc && Field<T>::complex;
@@ -1162,15 +1160,6 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
       case L_CMOD:
         if (use_tc) continue;
         k_cmod<T><<<L.ntasks, CM_NT, smem_cmod_bytes<T>(), ls>>>(fa, H.d_t4 + L.task_off, H.d_cpairs);
-        break;
-      case L_CMOD_TC:
-        if constexpr (TensorCmod<T>::ok) {
-          if (!use_tc) continue;
-          k_cmod_tc<T><<<L.ntasks, TC_NT, smem_cmod_tc_bytes(), ls>>>(fa, H.d_t4tc + L.task_off, H.d_cpairs_tc,
-                                                                      H.d_tcmaps);
-        } else {
-          continue;
-        }
         break;
       case L_MAKE_G:
         k_make_g<T><<<L.ntasks, 256, 0, ls>>>(fa, H.d_t4 + L.task_off);
@@ -1249,7 +1238,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
     }
     if (prof)
       prof->mark(st,
-                 (L.kind == L_CMOD || L.kind == L_CMOD_TC || L.kind == L_MAKE_G || L.kind == L_MM_GEMM ||
+                 (L.kind == L_CMOD || L.kind == L_MAKE_G || L.kind == L_MM_GEMM ||
                   L.kind == L_MM_ASM || L.kind == L_SPLIT_R || L.kind == L_SPLIT_C) ? 1
                  : (L.kind == L_DIAG_INV || L.kind == L_SCHUR_TC)             ? 4
                  : L.kind == L_GETF2                                           ? 2

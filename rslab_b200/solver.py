@@ -795,7 +795,7 @@ def solve_profile(handle, nrhs: int) -> dict:
 
 
 LAUNCH_KINDS = ("cmod", "getf2", "deep_replay", "panel_schur", "fwd_diag", "fwd_push", "bwd_off", "bwd_diag",
-                "cmod_mm", "cmod_asm", "split_r", "split_c", "fwd_gather", "cmod_tc", "make_g", "diag_inv",
+                "cmod_mm", "cmod_asm", "split_r", "split_c", "fwd_gather", "unused13", "make_g", "diag_inv",
                 "bwd_off_reduce", "schur_tc", "fwd_chain", "bwd_chain", "bwd_gather", "deep_mm", "make_m", "push_reduce",
                 "join")
 
