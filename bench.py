@@ -691,9 +691,13 @@ def run_batch(args, ws, rank, local):
     # the engine and launch schedule of this batch, measured on it before the
     # timed region (the analysis-time block width stays at its default)
     from rslab_b200.autotune import candidates, tune_mixed
-    tuned = tune_mixed(a, b, args.target, sym=sym, cands=candidates(), reps=2, warmup=1)
+    tuned = tune_mixed(a, b, args.target, sym=sym, cands=candidates(engines=("tensor", "fma", "fp64")), reps=2,
+                       warmup=1)
     st = tuned.settings(SolverSettings())
-    mixed = MixedLdltSolver.factor_with(a, st, sym=sym)
+    if tuned.fp64:
+        mixed = MixedLdltSolver.factor_tier(a, N.TIER_FP64, st, sym=sym)
+    else:
+        mixed = MixedLdltSolver.factor_with(a, st, sym=sym)
 
     def mixed_step():
         rc = N.lib.rslab_refactor(mixed._h, C.c_void_p(vals_d.data_ptr()), 1)
@@ -753,7 +757,9 @@ def run_batch(args, ws, rank, local):
             "metric": "LDLT factor+solve GFLOP/s at bwd err <= 1e-14 (mixed/batched vs FP64 GPU)",
             "value": flops / (ms * 1e-3) / 1e9 * ws, "unit": "GFLOP/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
-            "vs_baseline": None, "dtype": "f32 factor / f64 refinement", "data": "synthetic",
+            "vs_baseline": None,
+            "dtype": ("f64 factor / f64 refinement" if tuned.fp64 else "f32 factor / f64 refinement"),
+            "data": "synthetic",
             "config": {"workload": f"batch{args.batch_count}_laplacian3d_sides12-40_f64_nrhs{nrhs}",
                        "systems": batch.count, "total_n": batch.total_n, "nnz_lower": a.nnz, "nrhs": nrhs,
                        "ordering": "AMD", "target_backward_error": args.target, "model_flops": flops,

@@ -7,8 +7,11 @@ module measures them on the actual pattern and keeps the fastest.  The knobs
 are value independent, so a pattern is tuned once and the choice reused for
 every refactor of it (frequency sweeps, batches, time steps):
 
-  schur_engine  descendant updates of the single-precision fields: tcgen05
-                tensor-core GEMM tiles ("tensor") or CUDA-core tiles ("fma")
+  schur_engine  the refined factor's precision tier and update engine: an
+                f32 / c32 factor with tcgen05 tensor-core GEMM tiles
+                ("tensor") or CUDA-core tiles ("fma"), or the FP64 factor
+                under the same refinement ladder ("fp64": the cheapest when
+                the single-precision factor needs many corrections)
   overlap       launch schedule: side streams overlapping independent work
                 (the Schur update beyond the next block, the next level's
                 early updates) or one in-order stream
@@ -47,9 +50,16 @@ class TuneResult:
     history: List[Tuple[Candidate, float]] = field(default_factory=list)
 
     def settings(self, base: Optional[SolverSettings] = None) -> SolverSettings:
+        """The chosen knobs as settings; for the "fp64" tier the engine field
+        keeps its default (use `fp64` to pick the factor call)."""
         s = base or SolverSettings()
-        s.schur_engine, s.overlap, s.panel_nb = self.chosen
+        eng, s.overlap, s.panel_nb = self.chosen
+        s.schur_engine = "tensor" if eng == "fp64" else eng
         return s
+
+    @property
+    def fp64(self) -> bool:
+        return self.chosen[0] == "fp64"
 
     def table(self) -> dict:
         return {f"{e}/{'overlap' if o else 'in-order'}/nb{nb}": round(t * 1e3, 3)
@@ -94,8 +104,13 @@ def tune_mixed(a, b, target: float = 1e-14, sym: Optional[LdltSymbolic] = None,
         if nb not in syms:
             s_an = SolverSettings(ordering=sym.settings.ordering, panel_nb=nb)
             syms[nb] = LdltSymbolic.analyze_with(a, s_an)
-        st = SolverSettings(ordering=syms[nb].settings.ordering, schur_engine=eng, overlap=ovl, panel_nb=nb)
-        m = MixedLdltSolver.factor_with(a, st, sym=syms[nb])
+        st = SolverSettings(ordering=syms[nb].settings.ordering, schur_engine="tensor" if eng == "fp64" else eng,
+                            overlap=ovl, panel_nb=nb)
+        if eng == "fp64":
+            from . import _native as N
+            m = MixedLdltSolver.factor_tier(a, N.TIER_FP64, st, sym=syms[nb])
+        else:
+            m = MixedLdltSolver.factor_with(a, st, sym=syms[nb])
         ok = True
         times = []
         for it in range(warmup + reps):
