@@ -105,10 +105,13 @@ typedef struct {
                                 * everything in order on one stream (0); the factor is the same */
 } rslab_factor_settings;
 
-/* Descendant (cmod) updates of the single-precision fields: 3xTF32 split
- * products on the tcgen05 tensor cores with fp32 accumulation (default), or
- * fp32 FMA on the CUDA cores in the oracle's operation order (bit-exact).
- * FP64 fields always use FP64 FMA. */
+/* Descendant (cmod) updates.  RSLAB_SCHUR_TENSOR (default): per (updater,
+ * target) pair a dense product over the updater's contiguous rows, in GEMM
+ * tiles on the tensor cores (f32 / c32: tcgen05 3xTF32 split products with
+ * fp32 accumulation, operands staged by TMA; f64 / c64: FP64 DMMA), written to
+ * a level workspace and assembled into the targets in update order
+ * (deterministic; parity with the oracle by tolerance).  RSLAB_SCHUR_FMA: FMA
+ * on the CUDA cores in the oracle's operation order (bit-exact). */
 #define RSLAB_SCHUR_TENSOR 0
 #define RSLAB_SCHUR_FMA 1
 

@@ -43,7 +43,9 @@ constexpr int MM_NC = 64;        // W tile columns (complex or real)
 constexpr int MM_NS = 3;         // operand stages
 constexpr int MM_BOX_B = 16;     // rows of one B box
 constexpr int MM_NT = 6 * 32;    // producer warp, MMA warp, 4 epilogue warps
-constexpr int MM_SPLIT_ROWS = 256;
+constexpr int MM_SPLIT_ROWS = 32;   // rows of one split task
+constexpr int MM_SPLIT_NT = 256;    // threads of a split task (8 column groups)
+constexpr int MM_SPLIT_LD = 36;     // padded shared-memory row (floats): 4-way bank spread, 16-byte rows
 constexpr uint32_t MM_TMEM_COLS = 256;  // two 128-column accumulators
 
 // Operand maps of updater k: [0] A hi, [1] A lo, [2] B hi, [3] B lo.
@@ -80,88 +82,90 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 }
 
 // ---------------------------------------------------------------------------
-// k_split: task (k, r0, chunk, 0): rows [r0, r0 + 256) of k's off-diagonal
-// block, K' chunk `chunk`.  One thread per row; reads of L21 are coalesced
-// across the warp (consecutive rows of one column), each thread writes its
-// row's 32 hi and 32 lo values (128-byte runs).
+// k_split: task (k, r0, chunk, 0): rows [r0, r0 + 32) of k's off-diagonal
+// block, K' chunk `chunk`.  Phase 1: thread (row, column group) reads L21 and
+// forms G = L21 D (ld_G's arithmetic) for its columns, coalesced across the
+// rows of a column, splitting into hi / lo rows in shared memory.  Phase 2:
+// eight consecutive threads store one row's 128 bytes of each operand, so a
+// warp writes four whole rows per store.  The rows of the shared tile are
+// padded to 36 floats, which spreads phase 1's column-wise writes over banks.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(MM_SPLIT_ROWS) k_split(FactorArgs fa, const int4* __restrict__ tasks,
-                                                         const long long* __restrict__ soff_a,
-                                                         const long long* __restrict__ soff_b,
-                                                         const int* __restrict__ kpad, float* __restrict__ a_hi,
-                                                         float* __restrict__ a_lo, float* __restrict__ b_hi,
-                                                         float* __restrict__ b_lo) {
+__global__ void __launch_bounds__(MM_SPLIT_NT) k_split(FactorArgs fa, const int4* __restrict__ tasks,
+                                                       const long long* __restrict__ soff_a,
+                                                       const long long* __restrict__ soff_b,
+                                                       const int* __restrict__ kpad, float* __restrict__ a_hi,
+                                                       float* __restrict__ a_lo, float* __restrict__ b_hi,
+                                                       float* __restrict__ b_lo) {
   using F = Field<T>;
   using Sh = MmShape<T>;
+  constexpr bool CX = Field<T>::complex;
+  constexpr int NOP = CX ? 6 : 4;  // A hi/lo, B(_re) hi/lo[, B_im hi/lo]
+  __shared__ __align__(16) float tile[NOP][MM_SPLIT_ROWS][MM_SPLIT_LD];
   if (fa.status[0] != 0) return;
   const int4 tk = tasks[blockIdx.x];
-  const int k = tk.x, r = tk.y + (int)threadIdx.x, ch = tk.z;
+  const int k = tk.x, r0 = tk.y, ch = tk.z;
   const int first = fa.sn_first[k], ncol = fa.sn_ncol[k], nrow = fa.sn_nrow[k];
   const int m = nrow - ncol;
-  if (r >= m) return;
   const int kp = kpad[k];
   const T* L = reinterpret_cast<const T*>(fa.panel) + fa.sn_poff[k] + ncol;  // L21, column stride nrow
   const T* d = reinterpret_cast<const T*>(fa.d) + first;
   const T* ds = reinterpret_cast<const T*>(fa.dsub) + first;
   const unsigned char* kd = fa.kind + first;
-  const long long ra = soff_a[k] + (long long)r * kp + 32 * ch;
   const int t0 = ch * Sh::cols_per_chunk;
-  if constexpr (!Field<T>::complex) {
-    const long long rb = soff_b[k] + (long long)r * kp + 32 * ch;
-#pragma unroll 4
-    for (int q = 0; q < 32; q += 4) {
-      float av[4], gv[4];
+  const int tid = threadIdx.x, rl = tid % MM_SPLIT_ROWS, grp = tid / MM_SPLIT_ROWS;
+  constexpr int GROUPS = MM_SPLIT_NT / MM_SPLIT_ROWS;
+  constexpr int PER = Sh::cols_per_chunk / GROUPS;  // columns per thread
+  const int r = r0 + rl;
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int t = t0 + q + e;
-        av[e] = t < ncol ? L[r + (long long)t * nrow] : 0.0f;
-        gv[e] = t < ncol ? ld_G(L, nrow, r, t, d, ds, kd) : 0.0f;
-      }
-      float ah[4], al[4], gh[4], gl[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        split_tf32(av[e], ah[e], al[e]);
-        split_tf32(gv[e], gh[e], gl[e]);
-      }
-      *reinterpret_cast<float4*>(a_hi + ra + q) = make_float4(ah[0], ah[1], ah[2], ah[3]);
-      *reinterpret_cast<float4*>(a_lo + ra + q) = make_float4(al[0], al[1], al[2], al[3]);
-      *reinterpret_cast<float4*>(b_hi + rb + q) = make_float4(gh[0], gh[1], gh[2], gh[3]);
-      *reinterpret_cast<float4*>(b_lo + rb + q) = make_float4(gl[0], gl[1], gl[2], gl[3]);
+  for (int e = 0; e < PER; ++e) {
+    const int q = grp * PER + e, t = t0 + q;
+    T a = F::zero(), g = F::zero();
+    if (r < m && t < ncol) {
+      a = L[r + (long long)t * nrow];
+      g = ld_G(L, nrow, r, t, d, ds, kd);
     }
-  } else {
-    // B'_re row r and B'_im row r (the im block starts m rows later)
-    const long long rre = soff_b[k] + (long long)r * kp + 32 * ch;
-    const long long rim = rre + (long long)m * kp;
-#pragma unroll 2
-    for (int q = 0; q < 16; q += 4) {
-      float ar[4], ai[4], gr[4], gi[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int t = t0 + q + e;
-        T a = F::zero(), g = F::zero();
-        if (t < ncol) {
-          a = L[r + (long long)t * nrow];
-          g = ld_G(L, nrow, r, t, d, ds, kd);
-        }
-        ar[e] = a.re;
-        ai[e] = a.im;
-        gr[e] = g.re;
-        gi[e] = g.im;
-      }
-      float h[4], l[4];
-      auto put = [&](float* hi, float* lo, long long off, const float (&v)[4], float sgn) {
-#pragma unroll
-        for (int e = 0; e < 4; ++e) split_tf32(sgn * v[e], h[e], l[e]);
-        *reinterpret_cast<float4*>(hi + off) = make_float4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<float4*>(lo + off) = make_float4(l[0], l[1], l[2], l[3]);
-      };
-      put(a_hi, a_lo, ra + q, ar, 1.0f);        // A': Re in 0..15
-      put(a_hi, a_lo, ra + 16 + q, ai, 1.0f);   //     Im in 16..31
-      put(b_hi, b_lo, rre + q, gr, 1.0f);       // B'_re: Gr
-      put(b_hi, b_lo, rre + 16 + q, gi, -1.0f); //        -Gi
-      put(b_hi, b_lo, rim + q, gi, 1.0f);       // B'_im: Gi
-      put(b_hi, b_lo, rim + 16 + q, gr, 1.0f);  //        Gr
+    float h, l;
+    if constexpr (!CX) {
+      split_tf32(a, h, l);
+      tile[0][rl][q] = h;
+      tile[1][rl][q] = l;
+      split_tf32(g, h, l);
+      tile[2][rl][q] = h;
+      tile[3][rl][q] = l;
+    } else {
+      split_tf32(a.re, h, l);   // A': Re in 0..15, Im in 16..31
+      tile[0][rl][q] = h;
+      tile[1][rl][q] = l;
+      split_tf32(a.im, h, l);
+      tile[0][rl][16 + q] = h;
+      tile[1][rl][16 + q] = l;
+      split_tf32(g.re, h, l);   // B'_re = [Gr | -Gi], B'_im = [Gi | Gr]
+      tile[2][rl][q] = h;
+      tile[3][rl][q] = l;
+      tile[4][rl][16 + q] = h;
+      tile[5][rl][16 + q] = l;
+      split_tf32(g.im, h, l);
+      tile[2][rl][16 + q] = -h;
+      tile[3][rl][16 + q] = -l;
+      tile[4][rl][q] = h;
+      tile[5][rl][q] = l;
+    }
+  }
+  __syncthreads();
+  const long long rowa = soff_a[k] + 32LL * ch, rowb = soff_b[k] + 32LL * ch;
+  for (int e = tid; e < MM_SPLIT_ROWS * 8; e += MM_SPLIT_NT) {
+    const int rr = e >> 3, q4 = (e & 7) * 4, gr = r0 + rr;
+    if (gr >= m) continue;
+    const long long oa = rowa + (long long)gr * kp + q4, ob = rowb + (long long)gr * kp + q4;
+    *reinterpret_cast<float4*>(a_hi + oa) = *reinterpret_cast<const float4*>(&tile[0][rr][q4]);
+    *reinterpret_cast<float4*>(a_lo + oa) = *reinterpret_cast<const float4*>(&tile[1][rr][q4]);
+    *reinterpret_cast<float4*>(b_hi + ob) = *reinterpret_cast<const float4*>(&tile[2][rr][q4]);
+    *reinterpret_cast<float4*>(b_lo + ob) = *reinterpret_cast<const float4*>(&tile[3][rr][q4]);
+    if constexpr (CX) {  // the B'_im block starts m rows later
+      const long long oi = ob + (long long)m * kp;
+      *reinterpret_cast<float4*>(b_hi + oi) = *reinterpret_cast<const float4*>(&tile[4][rr][q4]);
+      *reinterpret_cast<float4*>(b_lo + oi) = *reinterpret_cast<const float4*>(&tile[5][rr][q4]);
     }
   }
 }
@@ -357,7 +361,6 @@ __global__ void __launch_bounds__(256) k_cmod_asm(FactorArgs fa, const int4* __r
                                                   const float* __restrict__ W) {
   using F = Field<T>;
   if (fa.status[0] != 0) return;
-  __shared__ int8_t cmap[2][TC_N];
   const int4 tk = tasks[blockIdx.x];
   const int s = tk.x, r0 = (tk.y >> 16) * TC_M, c0 = (tk.y & 0xffff) * TC_N;
   const int ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
@@ -366,21 +369,22 @@ __global__ void __launch_bounds__(256) k_cmod_asm(FactorArgs fa, const int4* __r
   T acc[32];
 #pragma unroll
   for (int j = 0; j < 32; ++j) acc[j] = F::zero();
-  int par = 0;
-  for (int u = tk.z; u < tk.w; ++u, par ^= 1) {
-    const int4 pr = pairs[u];
+  // no block barrier: every thread reads its own row map entry and its 32
+  // column map entries (two 16-byte loads) straight from the pair's maps
+  for (int u = tk.z; u < tk.w; ++u) {
     const int8_t* mp = maps + (long long)u * TC_MAP;
-    if (threadIdx.x < TC_N) cmap[par][threadIdx.x] = mp[TC_M + threadIdx.x];
-    __syncthreads();
     const int i = mp[t];
-    if (i >= 0) {
-      const int a = pr.y, q0 = pr.z;
-      const T* wrow = reinterpret_cast<const T*>(W) + wb[u] + (long long)i * wl[u];
+    if (i < 0) continue;
+    const int4 pr = pairs[u];
+    const int a = pr.y, q0 = pr.z;
+    int8_t cm[32];
+    *reinterpret_cast<int4*>(cm) = *reinterpret_cast<const int4*>(mp + TC_M + 32 * h);
+    *reinterpret_cast<int4*>(cm + 16) = *reinterpret_cast<const int4*>(mp + TC_M + 32 * h + 16);
+    const T* wrow = reinterpret_cast<const T*>(W) + wb[u] + (long long)i * wl[u];
 #pragma unroll
-      for (int jj = 0; jj < 32; ++jj) {
-        const int j = cmap[par][32 * h + jj];
-        if (j >= 0 && a + i >= q0 + j) acc[jj] = F::add(acc[jj], wrow[j]);
-      }
+    for (int jj = 0; jj < 32; ++jj) {
+      const int j = cm[jj];
+      if (j >= 0 && a + i >= q0 + j) acc[jj] = F::add(acc[jj], wrow[j]);
     }
   }
   T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
@@ -393,6 +397,160 @@ __global__ void __launch_bounds__(256) k_cmod_asm(FactorArgs fa, const int4* __r
         *p = F::sub(*p, acc[jj]);
       }
     }
+}
+
+}  // namespace rsd
+
+namespace rsd {
+
+// ---------------------------------------------------------------------------
+// FP64 fields: the same updater-space GEMM tiles on the FP64 tensor cores
+// (mma.sync m8n8k4 .f64, DMMA).  Task and W layout as k_cmod_mm; the A
+// operand is L21_k (the panel, column stride nrow_k), the B operand G_k (the
+// G pool, column stride m_k), staged by cp.async in K chunks (two stages).
+// 256 threads: warp (wr, wc) of a 4 x 2 grid owns rows 32 wr .. +31 and
+// columns 32 wc .. +31 of the tile, i.e. 4 x 4 m8n8 blocks.  Complex
+// products use four real DMMA per block: Re += Ar Br - Ai Bi, Im += Ar Bi +
+// Ai Br.  Results agree with the FMA engine to rounding (the DMMA sums its
+// four products in its own order); the FMA engine (schur_engine = fma)
+// remains the bit-exact reference engine.
+// ---------------------------------------------------------------------------
+constexpr int DM_NT = 256;
+// K chunk and padded shared-memory columns (elements) of the A / B chunks:
+// with these strides the fragment loads of a warp (rows g, K columns q) hit
+// distinct banks (8-byte elements: stride = 4 mod 16 words; 16-byte
+// elements: 2 mod 8 elements).
+template <typename T> struct DmShape {
+  static constexpr int kc = 16, lda = 132, ldb = 68;
+};
+template <> struct DmShape<c64> {
+  static constexpr int kc = 8, lda = 130, ldb = 66;
+};
+template <typename T>
+__host__ __device__ constexpr size_t smem_cmod_dmm_bytes() {
+  return 2 * (size_t)DmShape<T>::kc * (DmShape<T>::lda + DmShape<T>::ldb) * sizeof(T);
+}
+
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(DM_NT) k_cmod_dmm(FactorArgs fa, const int4* __restrict__ tasks,
+                                                   const long long* __restrict__ wbase,
+                                                   const int* __restrict__ wld, T* __restrict__ W) {
+  using F = Field<T>;
+  constexpr bool CX = Field<T>::complex;
+  constexpr int KC = DmShape<T>::kc, DM_LDA = DmShape<T>::lda, DM_LDB = DmShape<T>::ldb;
+  constexpr int STAGE = KC * (DM_LDA + DM_LDB);
+  if (fa.status[0] != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* stg = reinterpret_cast<T*>(smem_raw);
+  const int4 tk = tasks[blockIdx.x];
+  const int k = tk.x, r0 = tk.y, c0 = tk.z, nrows = tk.w & 0xffff, nn = tk.w >> 16;
+  const int nck = fa.sn_ncol[k], nrk = fa.sn_nrow[k], m = nrk - nck;
+  const T* A = reinterpret_cast<const T*>(fa.panel) + fa.sn_poff[k] + nck + r0;  // + t * nrk
+  const T* B = reinterpret_cast<const T*>(fa.gpool) + fa.goff[k] + c0;           // + t * m
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int wr = warp >> 1, wc = warp & 1;
+  const int g = lane >> 2, q = lane & 3;  // fragment group / thread in group
+
+  auto issue = [&](int t0, int st) {
+    T* As = stg + st * STAGE;
+    T* Bs = As + KC * DM_LDA;
+    for (int e = tid; e < KC * MM_M; e += DM_NT) {
+      const int t = e / MM_M, r = e % MM_M, tt = t0 + t;
+      const bool ok = tt < nck && r < nrows;
+      cp_async_zfill<(int)sizeof(T)>(As + t * DM_LDA + r, ok ? A + r + (long long)tt * nrk : A, ok);
+    }
+    for (int e = tid; e < KC * MM_NC; e += DM_NT) {
+      const int t = e / MM_NC, c = e % MM_NC, tt = t0 + t;
+      const bool ok = tt < nck && c < nn;
+      cp_async_zfill<(int)sizeof(T)>(Bs + t * DM_LDB + c, ok ? B + c + (long long)tt * m : B, ok);
+    }
+    cp_async_commit();
+  };
+
+  // accumulators: [row block i][col block j][2] (complex: re, im pairs)
+  double acc[4][4][CX ? 4 : 2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int v = 0; v < (CX ? 4 : 2); ++v) acc[i][j][v] = 0.0;
+
+  const int nchunk = (nck + KC - 1) / KC;
+  if (nchunk > 0) issue(0, 0);
+  for (int c = 0; c < nchunk; ++c) {
+    const int st = c & 1;
+    if (c + 1 < nchunk) {
+      issue((c + 1) * KC, st ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const T* As = stg + st * STAGE;
+    const T* Bs = As + KC * DM_LDA;
+    const bool active = 32 * wr < nrows && 32 * wc < nn;
+    if (active) {
+#pragma unroll
+      for (int k4 = 0; k4 < KC; k4 += 4) {
+        const int t = k4 + q;
+        if constexpr (!CX) {
+          double a[4], b[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) a[i] = As[t * DM_LDA + 32 * wr + 8 * i + g];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) b[j] = Bs[t * DM_LDB + 32 * wc + 8 * j + g];
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) dmma884(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        } else {
+          T a[4], b[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) a[i] = As[t * DM_LDA + 32 * wr + 8 * i + g];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) b[j] = Bs[t * DM_LDB + 32 * wc + 8 * j + g];
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              dmma884(acc[i][j][0], acc[i][j][1], a[i].re, b[j].re);   // Re += Ar Br
+              dmma884(acc[i][j][0], acc[i][j][1], -a[i].im, b[j].im);  //       - Ai Bi
+              dmma884(acc[i][j][2], acc[i][j][3], a[i].re, b[j].im);   // Im += Ar Bi
+              dmma884(acc[i][j][2], acc[i][j][3], a[i].im, b[j].re);   //       + Ai Br
+            }
+        }
+      }
+    }
+    __syncthreads();  // the stage is free for the load after next
+  }
+  // W[row, col] for row < nrows, col < nn (fragment: row g, columns 2q, 2q+1)
+  const long long wb = wbase[blockIdx.x];
+  const int ld = wld[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int row = 32 * wr + 8 * i + g;
+    if (row >= nrows) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        const int col = 32 * wc + 8 * j + 2 * q + v;
+        if (col >= nn) continue;
+        T out;
+        if constexpr (CX)
+          out = T{acc[i][j][v], acc[i][j][2 + v]};
+        else
+          out = acc[i][j][v];
+        W[wb + (long long)row * ld + col] = out;
+      }
+  }
 }
 
 }  // namespace rsd

@@ -906,6 +906,9 @@ struct KernelSetup {
       CK(cudaFuncSetAttribute(k_schur_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_tc_bytes()));
     }
     CK(cudaFuncSetAttribute(k_cmod<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_bytes<T>()));
+    if constexpr (!TensorCmod<T>::ok)
+      CK(cudaFuncSetAttribute(k_cmod_dmm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_cmod_dmm_bytes<T>()));
     CK(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
     CK(cudaFuncSetAttribute(k_getf2<T, GETF2_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)smem_getf2(es, 128)));
@@ -1105,7 +1108,11 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
                                                 (T*)F.panel);
   FactorArgs fa = make_fargs<T>(F);
   const int nb_small = H.panel_nb, nb_big = std::max(H.panel_nb, 128);
-  const bool use_tc = TensorCmod<T>::ok && F.set.schur_engine == RSLAB_SCHUR_TENSOR;
+  // tensor engine: descendant updates as updater-space GEMM tiles + assembly
+  // (tcgen05 3xTF32 for f32 / c32, DMMA for f64 / c64); the single-precision
+  // fields also run their panel Schur / deep rows on the tensor-core kernels
+  const bool mm = F.set.schur_engine == RSLAB_SCHUR_TENSOR;
+  const bool use_tc = TensorCmod<T>::ok && mm;
   fa.deep_mm = use_tc ? 1 : 0;
   if (F.floor_dev) {
     CK(cudaMemsetAsync(F.amax_dev, 0, sizeof(unsigned long long), st));
@@ -1121,11 +1128,11 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
   bool side_pending = false;
   auto runs = [&](const Launch& L) {
     switch (L.kind) {
-      case L_CMOD: return !use_tc;
-      case L_MM_GEMM: case L_MM_ASM: return use_tc;
+      case L_CMOD: return !mm;
+      case L_MM_GEMM: case L_MM_ASM: return mm;
       case L_SPLIT_R: return use_tc && !Field<T>::complex;
       case L_SPLIT_C: return use_tc && Field<T>::complex;
-      case L_MAKE_G: return !use_tc;  // G_k of the CUDA-core cmod
+      case L_MAKE_G: return !use_tc;  // G_k of the CUDA-core cmod and of the DMMA tiles
       case L_DEEP: return !fa.deep_mm;
       case L_MAKE_M: case L_DEEP_MM: return fa.deep_mm != 0;
       case L_SCHUR: return !use_tc;
@@ -1158,7 +1165,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
     }
     switch (L.kind) {
       case L_CMOD:
-        if (use_tc) continue;
+        if (mm) continue;
         k_cmod<T><<<L.ntasks, CM_NT, smem_cmod_bytes<T>(), ls>>>(fa, H.d_t4 + L.task_off, H.d_cpairs);
         break;
       case L_MAKE_G:
@@ -1168,7 +1175,18 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
       case L_MM_ASM:
       case L_SPLIT_R:
       case L_SPLIT_C:
-        if constexpr (TensorCmod<T>::ok) {
+        if constexpr (!TensorCmod<T>::ok) {
+          // FP64 fields: DMMA tiles from L21 and the G pool, then the same assembly
+          T* wb = reinterpret_cast<T*>(F.wbuf) + (size_t)(L.nb_slot & 1) * H.w_elems;
+          if (L.kind == L_MM_GEMM)
+            k_cmod_dmm<T><<<L.ntasks, DM_NT, smem_cmod_dmm_bytes<T>(), ls>>>(
+                fa, H.d_mm_t4 + L.task_off, H.d_mm_wb + L.task_off, H.d_mm_wl + L.task_off, wb);
+          else if (L.kind == L_MM_ASM)
+            k_cmod_asm<T><<<L.ntasks, 256, 0, ls>>>(fa, H.d_t4tc + L.task_off, H.d_cpairs_tc, H.d_tcmaps, H.d_asm_wb,
+                                                    H.d_asm_wl, F.wbuf + (size_t)(L.nb_slot & 1) * H.w_elems * es / 4);
+          else
+            continue;
+        } else {
           constexpr bool cx = Field<T>::complex;
           const size_t wsz = (size_t)H.w_elems * (cx ? 2 : 1);
           if (L.kind == L_MM_GEMM)
@@ -1179,12 +1197,10 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
             k_cmod_asm<T><<<L.ntasks, 256, 0, ls>>>(fa, H.d_t4tc + L.task_off, H.d_cpairs_tc, H.d_tcmaps, H.d_asm_wb,
                                                     H.d_asm_wl, F.wbuf + (L.nb_slot & 1) * wsz);
           else
-            k_split<T><<<L.ntasks, MM_SPLIT_ROWS, 0, ls>>>(
+            k_split<T><<<L.ntasks, MM_SPLIT_NT, 0, ls>>>(
                 fa, (cx ? H.d_sp_c : H.d_sp_r) + L.task_off, cx ? H.d_soff_a_c : H.d_soff_a_r,
                 cx ? H.d_soff_b_c : H.d_soff_b_r, cx ? H.d_kpad_c : H.d_kpad_r, F.sp_ahi, F.sp_alo, F.sp_bhi,
                 F.sp_blo);
-        } else {
-          continue;
         }
         break;
       case L_DIAG_INV:
@@ -2148,10 +2164,14 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
       F->floor_dev = F->al<double>(1);
       F->amax_dev = F->al<unsigned long long>(1);
     }
-    const bool tensor = (dtype == RSLAB_F32 || dtype == RSLAB_C32) && F->set.schur_engine == RSLAB_SCHUR_TENSOR;
-    if (tensor)
-      setup_mm_pools(*F);
-    else
+    const bool single = dtype == RSLAB_F32 || dtype == RSLAB_C32;
+    if (F->set.schur_engine == RSLAB_SCHUR_TENSOR) {
+      if (single)
+        setup_mm_pools(*F);
+      else  // FP64 DMMA tiles: the level W buffers (the A / B operands are L21 and G)
+        F->wbuf = F->al<float>((size_t)2 * sym->w_elems * es / 4);
+    }
+    if (!(single && F->set.schur_engine == RSLAB_SCHUR_TENSOR))
       F->gpool = F->al<unsigned char>((size_t)std::max(sym->g_elems, 1LL) * es);
     if (F->set.scaling != RSLAB_SCALING_ONEPASS) {
       std::vector<double> ones(n, 1.0);

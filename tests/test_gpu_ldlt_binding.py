@@ -126,8 +126,9 @@ def test_drop_tol_matches_oracle_rule():
     a = matgen.c3_matrix(12)
     tau = 0.05
     sym = LdltSymbolic.analyze(a)
-    full = sym.factor(a, SolverSettings(drop_tol=None)).export_factors()
-    inc = sym.factor(a, SolverSettings(drop_tol=tau)).export_factors()
+    # the bit-exact engine: the kept entries are compared with the oracle's exactly
+    full = sym.factor(a, SolverSettings(drop_tol=None, schur_engine="fma")).export_factors()
+    inc = sym.factor(a, SolverSettings(drop_tol=tau, schur_engine="fma")).export_factors()
     ref = OracleSolver(a, sym.export()).factors()
     r_idx, r_val, r_ptr = drop_rule(ref, tau)
     assert len(inc.l_values) < len(full.l_values)

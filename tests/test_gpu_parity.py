@@ -21,7 +21,10 @@ EPS = 2.220446049250313e-16
 
 
 def both(a, settings=None, dtype=None):
-    settings = settings or SolverSettings()
+    # the bit-exact CUDA-core engine: the oracle's operation order, so pivot
+    # sequences and factors compare exactly (the default FP64 engine, DMMA
+    # tiles, is checked by tolerance in test_gpu_fp64_dmma.py)
+    settings = settings or SolverSettings(schur_engine="fma")
     sym = LdltSymbolic.analyze_with(a, settings)
     aa = a if dtype is None else a.astype(dtype)
     gpu = sym.factor(aa, settings)
@@ -164,6 +167,7 @@ def test_kkt_fixtures_match_oracle(case):
 def test_static_pivoting_matches_oracle():
     e, a, rhs = next(c for c in KKT if c[0]["name"] == "HYDCAR20_0000")
     st = SolverSettings.preconditioner(1e-10)
+    st.schur_engine = "fma"
     sym = LdltSymbolic.analyze(a)
     gpu = sym.factor(a, st)
     o = OracleSolver(a, sym.export(), perturb_floor=1e-10).factors()
