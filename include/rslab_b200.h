@@ -97,7 +97,7 @@ typedef struct {
   int32_t scaling;             /* RSLAB_SCALING_* */
   int32_t use_graph;           /* capture factor / solve as CUDA graphs (1) */
   void* stream;                /* cudaStream_t to run on, or NULL for a private one */
-  int32_t schur_engine;        /* RSLAB_SCHUR_*: how f32/c32 descendant updates run */
+  int32_t schur_engine;        /* RSLAB_SCHUR_*: how descendant updates run (AUTO) */
   double drop_tol;             /* > 0: incomplete factor, drop |L_ip| < drop_tol * max_i |L_ip| per
                                 * column (SolverSettings::drop_tol, multifrontal_ldlt.rs:2359-2367) */
   int32_t overlap;             /* schedule: run the Schur update beyond the next block and the next
@@ -105,15 +105,23 @@ typedef struct {
                                 * everything in order on one stream (0); the factor is the same */
 } rslab_factor_settings;
 
-/* Descendant (cmod) updates.  RSLAB_SCHUR_TENSOR (default): per (updater,
- * target) pair a dense product over the updater's contiguous rows, in GEMM
- * tiles on the tensor cores (f32 / c32: tcgen05 3xTF32 split products with
- * fp32 accumulation, operands staged by TMA; f64 / c64: FP64 DMMA), written to
- * a level workspace and assembled into the targets in update order
+/* Descendant (cmod) updates.  RSLAB_SCHUR_TENSOR: per (updater, target) pair
+ * a dense product over the updater's contiguous rows, in GEMM tiles on the
+ * tensor cores (f32 / c32: tcgen05 3xTF32 split products with fp32
+ * accumulation, operands staged by TMA, complex products in the 3M form of
+ * three real products; f64 / c64: FP64 DMMA), written to a
+ * level workspace and assembled into the targets in update order
  * (deterministic; parity with the oracle by tolerance).  RSLAB_SCHUR_FMA: FMA
- * on the CUDA cores in the oracle's operation order (bit-exact). */
+ * on the CUDA cores in the oracle's operation order (bit-exact).
+ * RSLAB_SCHUR_AUTO (default): TENSOR when the analysis' model flops reach
+ * RSLAB_SCHUR_AUTO_MIN_FLOPS, else FMA — below that size the workspace and
+ * assembly launches cost more than the tiles save, and the factor keeps the
+ * oracle's bits (and so its pivot decisions on near-singular KKT systems).
+ * rslab_factor_info reports the engine a factor ran with. */
 #define RSLAB_SCHUR_TENSOR 0
 #define RSLAB_SCHUR_FMA 1
+#define RSLAB_SCHUR_AUTO 2
+#define RSLAB_SCHUR_AUTO_MIN_FLOPS 2.0e8
 
 typedef struct {
   int64_t n, nnz, nsuper, nlevels;
@@ -139,6 +147,7 @@ typedef struct {
   int32_t dtype, dtype_hi;
   int32_t multiprocessors;     /* SMs of the handle's device (the reference's Diagnostics::threads
                                 * counts CPU workers) */
+  int32_t schur_engine;        /* RSLAB_SCHUR_TENSOR or RSLAB_SCHUR_FMA: the engine AUTO resolved to */
 } rslab_factor_info_t;
 
 typedef struct {

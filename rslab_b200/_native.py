@@ -14,7 +14,7 @@ F64, C64, F32, C32 = 0, 1, 2, 3
 ORDER_AMD, ORDER_METIS_ND, ORDER_NATURAL, ORDER_GIVEN = 0, 1, 2, 3
 PIVOT_FAIL, PIVOT_PERTURB, PIVOT_FORCE_ACCEPT = 0, 1, 2
 SCALING_ONEPASS, SCALING_IDENTITY = 0, 1
-SCHUR_TENSOR, SCHUR_FMA = 0, 1
+SCHUR_TENSOR, SCHUR_FMA, SCHUR_AUTO = 0, 1, 2
 TIER_FP64, TIER_FP32, TIER_TF32X3 = 0, 1, 2
 TIER_MLP_PARAMS = 4931
 
@@ -70,6 +70,7 @@ class FactorInfo(C.Structure):
         ("inertia_pos", C.c_int64), ("inertia_neg", C.c_int64), ("inertia_zero", C.c_int64),
         ("n_perturbed", C.c_int64), ("factor_ms", C.c_double), ("solve_ms", C.c_double),
         ("dtype", C.c_int32), ("dtype_hi", C.c_int32), ("multiprocessors", C.c_int32),
+        ("schur_engine", C.c_int32),
     ]
 
 

@@ -22,7 +22,7 @@ BUILD = HERE.parent / "_build" / "rslab_b200"
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-Xcompiler", "-ffp-contract=off",
     "--expt-relaxed-constexpr",
 ]
 

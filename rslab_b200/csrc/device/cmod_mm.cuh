@@ -8,18 +8,23 @@
 // row c0 of k takes k's rows from c0 on.  The three kernels:
 //   k_split   once per updater, after its level is factored: writes A = L21_k
 //             and B = G_k as row-major, K-contiguous tf32 hi / lo pairs (the
-//             3xTF32 split), zero-padded to whole 32-wide K chunks; complex
-//             fields use the real embedding A' = [Ar | Ai] per 16-column
-//             chunk, B'_re = [Gr | -Gi], B'_im = [Gi | Gr] (so A' B'_re^T =
-//             Re U, A' B'_im^T = Im U);
+//             3xTF32 split), zero-padded to whole 32-wide K chunks.  Complex
+//             fields take the 3M form of the product: per 16-column chunk
+//             A' = [Ar | Ai], B' = [Gr | Gi] (hi and lo arrays) and the sums
+//             As = Ar + Ai, Bs = Gr + Gi as one [hi | lo] array each, so
+//               P1 = Ar Gr^T, P2 = Ai Gi^T, P3 = As Bs^T,
+//               Re U = P1 - P2,  Im U = P3 - P1 - P2
+//             takes three real products of K = 16 (the real embedding took
+//             four);
 //   k_cmod_mm one 128-row x (<= 64)-column tile of W per CTA: a TMA producer
-//             thread loads A hi / lo (128 x 32 boxes) and B hi / lo (16-row
-//             boxes) into 128-byte-swizzled K-major stages, one thread issues
-//             tcgen05.mma kind::tf32 (hi*hi + hi*lo + lo*hi) into a TMEM
-//             accumulator, four epilogue warps promote every window of
-//             TC_WIN chunks into fp32 registers (the tensor pipe does not
-//             round its accumulation to nearest) and write the tile to the
-//             level's W workspace;
+//             thread loads the A boxes (128 x 32) and B boxes (16-row) into
+//             128-byte-swizzled K-major stages, one thread issues
+//             tcgen05.mma kind::tf32 (hi*hi + hi*lo + lo*hi) into TMEM
+//             accumulators (complex: P1, P2, P3), four epilogue warps promote
+//             every window of TC_WIN chunks into fp32 registers (the tensor
+//             pipe does not round its accumulation to nearest; complex
+//             windows are combined into Re / Im there) and write the tile to
+//             the level's W workspace;
 //   k_cmod_asm one 128 x 64 target tile per CTA: subtracts, in update order,
 //             every pair's W entries that land in the tile (rows r >= column
 //             c in k's ordering), through the pairs' inverse row / column
@@ -40,32 +45,40 @@ namespace rsd {
 
 constexpr int MM_M = 128;        // W tile rows (UMMA M)
 constexpr int MM_NC = 64;        // W tile columns (complex or real)
-constexpr int MM_NS = 3;         // operand stages
 constexpr int MM_BOX_B = 16;     // rows of one B box
 constexpr int MM_NT = 6 * 32;    // producer warp, MMA warp, 4 epilogue warps
 constexpr int MM_SPLIT_ROWS = 32;   // rows of one split task
 constexpr int MM_SPLIT_NT = 256;    // threads of a split task (8 column groups)
 constexpr int MM_SPLIT_LD = 36;     // padded shared-memory row (floats): 4-way bank spread, 16-byte rows
-constexpr uint32_t MM_TMEM_COLS = 256;  // two 128-column accumulators
+constexpr uint32_t MM_TMEM_COLS = 512;  // two windows of up to 3 x 64 accumulator columns (at 0, 64, 128)
+constexpr uint32_t MM_WIN_COLS = 256;   // TMEM columns per window buffer
 
-// Operand maps of updater k: [0] A hi, [1] A lo, [2] B hi, [3] B lo.
-constexpr int MM_MAPS = 4;
+// Operand maps of updater k: [0] A hi, [1] A lo, [2] B hi, [3] B lo, and for
+// complex fields [4] As = [hi | lo] of Ar + Ai, [5] Bs = [hi | lo] of Gr + Gi.
+constexpr int MM_MAPS = 6;
 
-// one stage: A hi, A lo (128 rows x 128 B), B hi, B lo (up to 128 rows x 128 B)
-constexpr int MM_OPER = MM_M * 128;
-constexpr int MM_STAGE = 4 * MM_OPER;
-__host__ __device__ constexpr size_t smem_cmod_mm_bytes() { return 1024 + MM_NS * (size_t)MM_STAGE + 128; }
+// one stage: A boxes of 128 rows x 128 B, B boxes of up to 64 rows x 128 B
+constexpr int MM_AOP = MM_M * 128;
+constexpr int MM_BOP = MM_NC * 128;
 
 // Split-pool geometry of an updater: K' chunks of 32 fp32 per row.
 template <typename T> struct MmShape;
 template <> struct MmShape<float> {
   static constexpr int cols_per_chunk = 32;  // k columns per 32-wide K' chunk
-  static constexpr int brows = 1;            // B rows per G row (re only)
+  static constexpr int nops = 2;             // A / B arrays: hi, lo
+  static constexpr int stages = 4;
 };
 template <> struct MmShape<c32> {
   static constexpr int cols_per_chunk = 16;
-  static constexpr int brows = 2;            // B'_re rows, then B'_im rows
+  static constexpr int nops = 3;             // A / B arrays: hi, lo, [sum hi | sum lo]
+  static constexpr int stages = 3;
 };
+template <typename T>
+__host__ __device__ constexpr int mm_stage_bytes() { return MmShape<T>::nops * (MM_AOP + MM_BOP); }
+template <typename T>
+__host__ __device__ constexpr size_t smem_cmod_mm_bytes() {
+  return 1024 + MmShape<T>::stages * (size_t)mm_stage_bytes<T>() + 128;
+}
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
@@ -96,11 +109,12 @@ __global__ void __launch_bounds__(MM_SPLIT_NT) k_split(FactorArgs fa, const int4
                                                        const long long* __restrict__ soff_b,
                                                        const int* __restrict__ kpad, float* __restrict__ a_hi,
                                                        float* __restrict__ a_lo, float* __restrict__ b_hi,
-                                                       float* __restrict__ b_lo) {
+                                                       float* __restrict__ b_lo, float* __restrict__ a_s,
+                                                       float* __restrict__ b_s) {
   using F = Field<T>;
   using Sh = MmShape<T>;
   constexpr bool CX = Field<T>::complex;
-  constexpr int NOP = CX ? 6 : 4;  // A hi/lo, B(_re) hi/lo[, B_im hi/lo]
+  constexpr int NOP = CX ? 6 : 4;  // A hi/lo, B hi/lo[, As, Bs]
   __shared__ __align__(16) float tile[NOP][MM_SPLIT_ROWS][MM_SPLIT_LD];
   if (fa.status[0] != 0) return;
   const int4 tk = tasks[blockIdx.x];
@@ -134,22 +148,24 @@ __global__ void __launch_bounds__(MM_SPLIT_NT) k_split(FactorArgs fa, const int4
       tile[2][rl][q] = h;
       tile[3][rl][q] = l;
     } else {
-      split_tf32(a.re, h, l);   // A': Re in 0..15, Im in 16..31
+      split_tf32(a.re, h, l);   // A' = [Ar | Ai], B' = [Gr | Gi]
       tile[0][rl][q] = h;
       tile[1][rl][q] = l;
       split_tf32(a.im, h, l);
       tile[0][rl][16 + q] = h;
       tile[1][rl][16 + q] = l;
-      split_tf32(g.re, h, l);   // B'_re = [Gr | -Gi], B'_im = [Gi | Gr]
+      split_tf32(g.re, h, l);
       tile[2][rl][q] = h;
       tile[3][rl][q] = l;
-      tile[4][rl][16 + q] = h;
-      tile[5][rl][16 + q] = l;
       split_tf32(g.im, h, l);
-      tile[2][rl][16 + q] = -h;
-      tile[3][rl][16 + q] = -l;
+      tile[2][rl][16 + q] = h;
+      tile[3][rl][16 + q] = l;
+      split_tf32(a.re + a.im, h, l);  // As = [hi | lo] of Ar + Ai, Bs of Gr + Gi
       tile[4][rl][q] = h;
-      tile[5][rl][q] = l;
+      tile[4][rl][16 + q] = l;
+      split_tf32(g.re + g.im, h, l);
+      tile[5][rl][q] = h;
+      tile[5][rl][16 + q] = l;
     }
   }
   __syncthreads();
@@ -162,10 +178,9 @@ __global__ void __launch_bounds__(MM_SPLIT_NT) k_split(FactorArgs fa, const int4
     *reinterpret_cast<float4*>(a_lo + oa) = *reinterpret_cast<const float4*>(&tile[1][rr][q4]);
     *reinterpret_cast<float4*>(b_hi + ob) = *reinterpret_cast<const float4*>(&tile[2][rr][q4]);
     *reinterpret_cast<float4*>(b_lo + ob) = *reinterpret_cast<const float4*>(&tile[3][rr][q4]);
-    if constexpr (CX) {  // the B'_im block starts m rows later
-      const long long oi = ob + (long long)m * kp;
-      *reinterpret_cast<float4*>(b_hi + oi) = *reinterpret_cast<const float4*>(&tile[4][rr][q4]);
-      *reinterpret_cast<float4*>(b_lo + oi) = *reinterpret_cast<const float4*>(&tile[5][rr][q4]);
+    if constexpr (CX) {
+      *reinterpret_cast<float4*>(a_s + oa) = *reinterpret_cast<const float4*>(&tile[4][rr][q4]);
+      *reinterpret_cast<float4*>(b_s + ob) = *reinterpret_cast<const float4*>(&tile[5][rr][q4]);
     }
   }
 }
@@ -173,8 +188,8 @@ __global__ void __launch_bounds__(MM_SPLIT_NT) k_split(FactorArgs fa, const int4
 // ---------------------------------------------------------------------------
 // k_cmod_mm: task (k, r0, c0, nrows | nn << 16) with rows [r0, r0 + nrows)
 // and columns [c0, c0 + nn) of k's off-diagonal block (indices relative to
-// its first off-diagonal row), written to W at wbase (row stride ldw
-// elements of the field).
+// its first off-diagonal row), written to W at wbase (column-major, column
+// stride wld elements of the field).
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(MM_NT, 1) k_cmod_mm(FactorArgs fa, const int4* __restrict__ tasks,
@@ -184,26 +199,25 @@ __global__ void __launch_bounds__(MM_NT, 1) k_cmod_mm(FactorArgs fa, const int4*
                                                       const int* __restrict__ kpad, float* __restrict__ W) {
   using Sh = MmShape<T>;
   constexpr bool CX = Field<T>::complex;
+  constexpr int NS = Sh::stages, NOP = Sh::nops, STAGE = mm_stage_bytes<T>();
   if (fa.status[0] != 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t sraw = smem_u32(smem_raw);
   unsigned char* sm = smem_raw + (((sraw + 1023u) & ~1023u) - sraw);
-  uint64_t* full = reinterpret_cast<uint64_t*>(sm + MM_NS * MM_STAGE);
-  uint64_t* empty = full + MM_NS;
-  uint64_t* wbar = empty + MM_NS;  // 2
-  uint64_t* pbar = wbar + 2;       // 2
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + NS * STAGE);
+  uint64_t* empty = full + NS;
+  uint64_t* wbar = empty + NS;  // 2
+  uint64_t* pbar = wbar + 2;    // 2
   uint32_t* tslot = reinterpret_cast<uint32_t*>(pbar + 2);
 
   const int4 tk = tasks[blockIdx.x];
   const int k = tk.x, r0 = tk.y, c0 = tk.z, nrows = tk.w & 0xffff, nn = tk.w >> 16;
-  const int m = fa.sn_nrow[k] - fa.sn_ncol[k];
   const int nchunks = kpad[k] / 32;
-  const int nr16 = (nn + 15) & ~15;              // B rows per half
-  const uint32_t nprime = CX ? 2u * nr16 : nr16; // UMMA N
+  const uint32_t nr16 = (uint32_t)((nn + 15) & ~15);  // UMMA N = B rows of a box set
   const CUtensorMap* mk = maps + (long long)k * MM_MAPS;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
-    for (int i = 0; i < MM_NS; ++i) {
+    for (int i = 0; i < NS; ++i) {
       mbar_init(&full[i], 1);
       mbar_init(&empty[i], 1);
     }
@@ -220,62 +234,95 @@ __global__ void __launch_bounds__(MM_NT, 1) k_cmod_mm(FactorArgs fa, const int4*
   const uint32_t tmem = *tslot;
   bool ok = true;
   int issued = 0;  // MMA warp: chunks committed
+  // promoted tile: real -> acc[j]; complex -> Re in acc[j], Im in acc[64 + j]
   float acc[128];
 #pragma unroll
   for (int j = 0; j < 128; ++j) acc[j] = 0.0f;
 
+  // stage layout: A arrays (A hi, A lo[, As]) then B arrays (B hi, B lo[, Bs])
   int loaded = 0;  // TMA producer: chunks whose loads were issued
   if (warp == 0) {
     // ---------------- TMA producer ----------------
     if (lane == 0) {
-      const uint32_t bbytes = nprime * 128u;
+      const uint32_t bbytes = nr16 * 128u;
       for (int c = 0; c < nchunks; ++c) {
-        const int st = c % MM_NS;
-        if (c >= MM_NS && !mbar_wait_bounded(&empty[st], (uint32_t)(((c / MM_NS) - 1) & 1))) {
+        const int st = c % NS;
+        if (c >= NS && !mbar_wait_bounded(&empty[st], (uint32_t)(((c / NS) - 1) & 1))) {
           ok = false;
           break;
         }
-        unsigned char* stg = sm + st * MM_STAGE;
-        mbar_expect_tx(&full[st], 2u * MM_OPER + 2u * bbytes);
-        tma_load_2d(stg, mk + 0, 32 * c, r0, &full[st]);
-        tma_load_2d(stg + MM_OPER, mk + 1, 32 * c, r0, &full[st]);
-        for (int h = 0; h < (CX ? 2 : 1); ++h)
-          for (int b = 0; b < nr16; b += MM_BOX_B) {
-            const int row = c0 + b + h * m;  // complex: the B'_im block starts m rows later
-            const uint32_t off = (uint32_t)(h * nr16 + b) * 128u;
-            tma_load_2d(stg + 2 * MM_OPER + off, mk + 2, 32 * c, row, &full[st]);
-            tma_load_2d(stg + 3 * MM_OPER + off, mk + 3, 32 * c, row, &full[st]);
-          }
+        unsigned char* stg = sm + st * STAGE;
+        mbar_expect_tx(&full[st], (uint32_t)NOP * ((uint32_t)MM_AOP + bbytes));
+#pragma unroll
+        for (int o = 0; o < NOP; ++o) {
+          const int amap = o < 2 ? o : 4, bmap = o < 2 ? 2 + o : 5;
+          tma_load_2d(stg + o * MM_AOP, mk + amap, 32 * c, r0, &full[st]);
+          for (uint32_t b = 0; b < nr16; b += MM_BOX_B)
+            tma_load_2d(stg + NOP * MM_AOP + o * MM_BOP + b * 128u, mk + bmap, 32 * c, c0 + (int)b, &full[st]);
+        }
         loaded = c + 1;
       }
     }
   } else if (warp == 1) {
     // ---------------- MMA issue ----------------
     if (lane == 0) {
-      const uint32_t idesc = idesc_tf32(MM_M, nprime);
+      const uint32_t idesc = idesc_tf32(MM_M, nr16);
       const uint32_t sbase = smem_u32(sm);
       for (int c = 0; c < nchunks && ok; ++c) {
-        const int st = c % MM_NS, w = c / TC_WIN;
+        const int st = c % NS, w = c / TC_WIN;
         if (c % TC_WIN == 0 && w >= 2 && !mbar_wait_bounded(&pbar[w & 1], (uint32_t)(((w - 2) >> 1) & 1))) {
           ok = false;
           break;
         }
-        if (!mbar_wait_bounded(&full[st], (uint32_t)((c / MM_NS) & 1))) {
+        if (!mbar_wait_bounded(&full[st], (uint32_t)((c / NS) & 1))) {
           ok = false;
           break;
         }
         tc_fence_after();
-        const uint32_t sa = sbase + (uint32_t)(st * MM_STAGE);
-        const uint32_t dacc = tmem + (uint32_t)(w & 1) * 128u;
-        uint32_t accf = (c % TC_WIN) != 0 ? 1u : 0u;
+        const uint32_t sa = sbase + (uint32_t)(st * STAGE), sb = sa + NOP * MM_AOP;
+        const uint32_t dacc = tmem + (uint32_t)(w & 1) * MM_WIN_COLS;
+        const uint32_t first = (c % TC_WIN) != 0 ? 1u : 0u;
+        if constexpr (!CX) {
+          uint32_t accf = first;
 #pragma unroll
-        for (int p = 0; p < 3; ++p) {
-          const uint32_t at = sa + (p == 2 ? MM_OPER : 0);              // A hi, A hi, A lo
-          const uint32_t bt = sa + 2 * MM_OPER + (p == 1 ? MM_OPER : 0);  // B hi, B lo, B hi
+          for (int p = 0; p < 3; ++p) {
+            const uint32_t at = sa + (p == 2 ? MM_AOP : 0);   // A hi, A hi, A lo
+            const uint32_t bt = sb + (p == 1 ? MM_BOP : 0);   // B hi, B lo, B hi
 #pragma unroll
-          for (int ks = 0; ks < 4; ++ks) {
-            mma_tf32(dacc, desc_sw128(at + 32u * ks), desc_sw128(bt + 32u * ks), idesc, accf);
-            accf = 1u;
+            for (int ks = 0; ks < 4; ++ks) {
+              mma_tf32(dacc, desc_sw128(at + 32u * ks), desc_sw128(bt + 32u * ks), idesc, accf);
+              accf = 1u;
+            }
+          }
+        } else {
+          // P1 (accumulator columns 0 ..), P2 (64 ..): the Re / Im halves of
+          // the A hi / lo and B hi / lo boxes (K steps 0-1 and 2-3)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const uint32_t d = dacc + 64u * (uint32_t)h;
+            uint32_t accf = first;
+#pragma unroll
+            for (int p = 0; p < 3; ++p) {
+              const uint32_t at = sa + (p == 2 ? MM_AOP : 0);
+              const uint32_t bt = sb + (p == 1 ? MM_BOP : 0);
+#pragma unroll
+              for (int ks = 2 * h; ks < 2 * h + 2; ++ks) {
+                mma_tf32(d, desc_sw128(at + 32u * ks), desc_sw128(bt + 32u * ks), idesc, accf);
+                accf = 1u;
+              }
+            }
+          }
+          // P3 (128 ..): As and Bs hold [hi | lo] in K steps 0-1 / 2-3
+          const uint32_t d = dacc + 128u, at = sa + 2 * MM_AOP, bt = sb + 2 * MM_BOP;
+          uint32_t accf = first;
+#pragma unroll
+          for (int p = 0; p < 3; ++p) {
+            const uint32_t ak = p == 2 ? 2u : 0u, bk = p == 1 ? 2u : 0u;  // hi*hi, hi*lo, lo*hi
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+              mma_tf32(d, desc_sw128(at + 32u * (ak + ks)), desc_sw128(bt + 32u * (bk + ks)), idesc, accf);
+              accf = 1u;
+            }
           }
         }
         mma_commit(&empty[st]);
@@ -293,14 +340,28 @@ __global__ void __launch_bounds__(MM_NT, 1) k_cmod_mm(FactorArgs fa, const int4*
         break;
       }
       tc_fence_after();
-      const uint32_t base = tmem + (uint32_t)(w & 1) * 128u + ((uint32_t)(32 * q) << 16);
+      const uint32_t base = tmem + (uint32_t)(w & 1) * MM_WIN_COLS + ((uint32_t)(32 * q) << 16);
 #pragma unroll
-      for (int g = 0; g < 8; ++g) {
-        if ((uint32_t)(16 * g) < nprime) {
-          float v[16];
-          tmem_ld16(base + 16u * g, v);
+      for (int g = 0; g < 4; ++g) {
+        if ((uint32_t)(16 * g) < nr16) {
+          if constexpr (!CX) {
+            float v[16];
+            tmem_ld16(base + 16u * g, v);
 #pragma unroll
-          for (int j = 0; j < 16; ++j) acc[16 * g + j] += v[j];
+            for (int j = 0; j < 16; ++j) acc[16 * g + j] += v[j];
+          } else {
+            float v1[16], v2[16];
+            tmem_ld16(base + 16u * g, v1);
+            tmem_ld16(base + 64u + 16u * g, v2);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              acc[16 * g + j] += v1[j] - v2[j];  // Re = P1 - P2
+              v1[j] += v2[j];
+            }
+            tmem_ld16(base + 128u + 16u * g, v2);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[64 + 16 * g + j] += v2[j] - v1[j];  // Im = P3 - P1 - P2
+          }
         }
       }
       tc_fence_before();
@@ -311,35 +372,26 @@ __global__ void __launch_bounds__(MM_NT, 1) k_cmod_mm(FactorArgs fa, const int4*
   if (warp >= 2 && all_ok) {
     const int row = 32 * (warp & 3) + lane;
     if (row < nrows) {
-      float* wr = W + (long long)(CX ? 2 : 1) * (wbase[blockIdx.x] + (long long)row * wld[blockIdx.x]);
+      // W is column-major: the lanes of a warp store 32 consecutive rows
+      const long long ld = wld[blockIdx.x];
+      float* wr = W + (long long)(CX ? 2 : 1) * (wbase[blockIdx.x] + row);
       if constexpr (CX) {
-        // the imaginary parts start at accumulator column nr16 (16, 32, 48
-        // or 64): a compile-time offset per case keeps acc in registers
-        auto put = [&](auto off) {
-          constexpr int o = decltype(off)::value;
 #pragma unroll
-          for (int j = 0; j < MM_NC; ++j)
-            if (j < nn) *reinterpret_cast<float2*>(wr + 2 * j) = make_float2(acc[j], acc[(o + j) & 127]);
-        };
-        switch (nr16) {
-          case 16: put(std::integral_constant<int, 16>{}); break;
-          case 32: put(std::integral_constant<int, 32>{}); break;
-          case 48: put(std::integral_constant<int, 48>{}); break;
-          default: put(std::integral_constant<int, 64>{}); break;
-        }
+        for (int j = 0; j < MM_NC; ++j)
+          if (j < nn) *reinterpret_cast<float2*>(wr + 2 * j * ld) = make_float2(acc[j], acc[64 + j]);
       } else {
 #pragma unroll
         for (int j = 0; j < MM_NC; ++j)
-          if (j < nn) wr[j] = acc[j];
+          if (j < nn) wr[j * ld] = acc[j];
       }
     }
   } else if (!all_ok && warp == 1 && lane == 0 && issued > 0) {
     // drain (bounded): the last commit covers every MMA issued before it
-    (void)mbar_wait_bounded(&empty[(issued - 1) % MM_NS], (uint32_t)(((issued - 1) / MM_NS) & 1));
+    (void)mbar_wait_bounded(&empty[(issued - 1) % NS], (uint32_t)(((issued - 1) / NS) & 1));
   } else if (!all_ok && warp == 0 && lane == 0) {
     // drain (bounded): the TMA loads still in flight land before the CTA exits
-    for (int c = std::max(0, loaded - MM_NS); c < loaded; ++c)
-      (void)mbar_wait_bounded(&full[c % MM_NS], (uint32_t)((c / MM_NS) & 1));
+    for (int c = std::max(0, loaded - NS); c < loaded; ++c)
+      (void)mbar_wait_bounded(&full[c % NS], (uint32_t)((c / NS) & 1));
   }
   if (!all_ok && tid == 0 && atomicCAS(&fa.status[0], 0, 2) == 0) fa.status[1] = k;
   tc_fence_before();
@@ -351,14 +403,15 @@ __global__ void __launch_bounds__(MM_NT, 1) k_cmod_mm(FactorArgs fa, const int4*
 // k_cmod_asm: task (s, rt << 16 | ct, pair_begin, pair_end) over the 128 x 64
 // tiles of the tensor-core plan; pair u (k, a, q0, nr << 16 | nc) with its
 // inverse maps (tile row -> offset from a, tile column -> offset from q0) and
-// its W element (a, q0) at wb[u], row stride wl[u].  256 threads: thread
+// its W element (a, q0) at wb[u], column stride wl[u].  256 threads: thread
 // (row t = tid & 127, half h = tid >> 7) owns tile columns 32 h .. 32 h + 31.
 // ---------------------------------------------------------------------------
+// Two CTAs per SM except for c64, whose 32 accumulators take 128 registers.
 template <typename T>
-__global__ void __launch_bounds__(256) k_cmod_asm(FactorArgs fa, const int4* __restrict__ tasks,
-                                                  const int4* __restrict__ pairs, const int8_t* __restrict__ maps,
-                                                  const long long* __restrict__ wb, const int* __restrict__ wl,
-                                                  const float* __restrict__ W) {
+__global__ void __launch_bounds__(256, sizeof(T) >= 16 ? 1 : 2)
+    k_cmod_asm(FactorArgs fa, const int4* __restrict__ tasks, const int4* __restrict__ pairs,
+               const int8_t* __restrict__ maps, const long long* __restrict__ wb, const int* __restrict__ wl,
+               const float* __restrict__ W) {
   using F = Field<T>;
   if (fa.status[0] != 0) return;
   const int4 tk = tasks[blockIdx.x];
@@ -380,11 +433,13 @@ __global__ void __launch_bounds__(256) k_cmod_asm(FactorArgs fa, const int4* __r
     int8_t cm[32];
     *reinterpret_cast<int4*>(cm) = *reinterpret_cast<const int4*>(mp + TC_M + 32 * h);
     *reinterpret_cast<int4*>(cm + 16) = *reinterpret_cast<const int4*>(mp + TC_M + 32 * h + 16);
-    const T* wrow = reinterpret_cast<const T*>(W) + wb[u] + (long long)i * wl[u];
+    // W is column-major: consecutive tile rows read (mostly) consecutive W rows
+    const T* wrow = reinterpret_cast<const T*>(W) + wb[u] + i;
+    const long long ld = wl[u];
 #pragma unroll
     for (int jj = 0; jj < 32; ++jj) {
       const int j = cm[jj];
-      if (j >= 0 && a + i >= q0 + j) acc[jj] = F::add(acc[jj], wrow[j]);
+      if (j >= 0 && a + i >= q0 + j) acc[jj] = F::add(acc[jj], wrow[j * ld]);
     }
   }
   T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
@@ -548,7 +603,7 @@ __global__ void __launch_bounds__(DM_NT) k_cmod_dmm(FactorArgs fa, const int4* _
           out = T{acc[i][j][v], acc[i][j][2 + v]};
         else
           out = acc[i][j][v];
-        W[wb + (long long)row * ld + col] = out;
+        W[wb + row + (long long)col * ld] = out;
       }
   }
 }

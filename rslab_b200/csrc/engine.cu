@@ -162,7 +162,7 @@ struct rslab_sym_handle {
   // tensor-core cmod in the updater's row space (device/cmod_mm.cuh): the
   // W offset of every update-list entry in its target level's buffer, the
   // GEMM tiles (k, r0, c0, nrows | nn << 16) with their W element offsets /
-  // row strides, the assembly pairs' W offsets / strides (parallel to
+  // column strides, the assembly pairs' W offsets / strides (parallel to
   // cpairs_tc), and the split pools of every updater for the real (32-column
   // chunks) and complex (16-column chunks) fields
   std::vector<long long> upd_woff;
@@ -361,9 +361,9 @@ void add_cmod_tiles(rslab_sym_handle& H, const std::vector<int64_t>& lvl, int tr
           while (rb < nok && rel[rb - p0] / tr == rt) ++rb;
           tp[(size_t)ct * ntr + rt].push_back(
               make_int4((int)k, (int)ra, (int)qa, (int)(((rb - ra) << 16) | (qb - qa))));
-          if (wbase) {  // W element (ra, qa) of the pair's row-major (nok - p0) x (p1 - p0) block
-            twb[(size_t)ct * ntr + rt].push_back(H.upd_woff[u] + (ra - p0) * (p1 - p0) + (qa - p0));
-            twl[(size_t)ct * ntr + rt].push_back((int)(p1 - p0));
+          if (wbase) {  // W element (ra, qa) of the pair's column-major (nok - p0) x (p1 - p0) block
+            twb[(size_t)ct * ntr + rt].push_back(H.upd_woff[u] + (qa - p0) * (nok - p0) + (ra - p0));
+            twl[(size_t)ct * ntr + rt].push_back((int)(nok - p0));
           }
           if (maps) {
             auto& m = tm[(size_t)ct * ntr + rt];
@@ -421,14 +421,14 @@ void add_mm_tiles(rslab_sym_handle& H, const std::vector<int64_t>& lvl, const st
     for (int64_t u = S.upd_ptr[s]; u < S.upd_ptr[s + 1]; ++u) {
       const int64_t k = S.upd[u], p0 = S.upd_p0[u], p1 = S.upd_p1[u];
       if (lv_of[k] < lv_lo || lv_of[k] > lv_hi) continue;
-      const int64_t m = H.nrow[k] - S.sn[k].ncol, npk = p1 - p0;
+      const int64_t m = H.nrow[k] - S.sn[k].ncol;
       for (int64_t c0 = p0; c0 < p1; c0 += MM_NC) {
         const int64_t nn = std::min<int64_t>(MM_NC, p1 - c0);
         for (int64_t r0 = c0; r0 < m; r0 += MM_M) {
           const int64_t nr = std::min<int64_t>(MM_M, m - r0);
           H.mm_t4.push_back(make_int4((int)k, (int)r0, (int)c0, (int)(nr | (nn << 16))));
-          H.mm_wb.push_back(H.upd_woff[u] + (r0 - p0) * npk + (c0 - p0));
-          H.mm_wl.push_back((int)npk);
+          H.mm_wb.push_back(H.upd_woff[u] + (c0 - p0) * (m - p0) + (r0 - p0));
+          H.mm_wl.push_back((int)(m - p0));
         }
       }
     }
@@ -467,7 +467,7 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
     H.g_elems += (long long)(H.nrow[s] - S.sn[s].ncol) * S.sn[s].ncol;
   }
   // updater-space tensor-core cmod: the W block of update-list entry u
-  // (k -> s) is k's rows [p0, nok) x its rows [p0, p1), row-major, in the
+  // (k -> s) is k's rows [p0, nok) x its rows [p0, p1), column-major, in the
   // buffer of s's level; split pools per updater, K' padded to 32-wide chunks
   {
     std::vector<int> lev(ns, 0);
@@ -501,7 +501,7 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       H.split_a_r += m * H.kpad_r[s];
       H.split_b_r += m * H.kpad_r[s];
       H.split_a_c += m * H.kpad_c[s];
-      H.split_b_c += 2 * m * H.kpad_c[s];
+      H.split_b_c += m * H.kpad_c[s];
     }
   }
   H.linv_off.assign(ns, 0);
@@ -902,7 +902,8 @@ struct KernelSetup {
     if (done) return;
     const size_t es = sizeof(T);
     if constexpr (TensorCmod<T>::ok) {
-      CK(cudaFuncSetAttribute(k_cmod_mm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_mm_bytes()));
+      CK(cudaFuncSetAttribute(k_cmod_mm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_cmod_mm_bytes<T>()));
       CK(cudaFuncSetAttribute(k_schur_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_tc_bytes()));
     }
     CK(cudaFuncSetAttribute(k_cmod<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_bytes<T>()));
@@ -960,9 +961,11 @@ struct rslab_fac_handle {
   void* gpool = nullptr;  // G_k = L21_k D_k of every updater (read by both cmod engines)
   void* linv = nullptr;   // inverse diagonal blocks of the wide supernodes
   // updater-space tensor-core cmod (f32 / c32, tensor engine): split operand
-  // pools (tf32 hi / lo of L21 and of G), two level buffers of W, and the
-  // TMA tensor maps of every updater's pools (MM_MAPS per supernode)
+  // pools (tf32 hi / lo of L21 and of G; complex fields also the [hi | lo]
+  // sums Ar + Ai and Gr + Gi of the 3M product), two level buffers of W, and
+  // the TMA tensor maps of every updater's pools (MM_MAPS per supernode)
   float *sp_ahi = nullptr, *sp_alo = nullptr, *sp_bhi = nullptr, *sp_blo = nullptr;
+  float *sp_as = nullptr, *sp_bs = nullptr;
   float* wbuf = nullptr;
   CUtensorMap* tmaps = nullptr;
   // static pivot reuse: the pivot record of the last searching factor and the
@@ -1190,7 +1193,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
           constexpr bool cx = Field<T>::complex;
           const size_t wsz = (size_t)H.w_elems * (cx ? 2 : 1);
           if (L.kind == L_MM_GEMM)
-            k_cmod_mm<T><<<L.ntasks, MM_NT, smem_cmod_mm_bytes(), ls>>>(
+            k_cmod_mm<T><<<L.ntasks, MM_NT, smem_cmod_mm_bytes<T>(), ls>>>(
                 fa, H.d_mm_t4 + L.task_off, H.d_mm_wb + L.task_off, H.d_mm_wl + L.task_off, F.tmaps,
                 cx ? H.d_kpad_c : H.d_kpad_r, F.wbuf + (L.nb_slot & 1) * wsz);
           else if (L.kind == L_MM_ASM)
@@ -1200,7 +1203,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
             k_split<T><<<L.ntasks, MM_SPLIT_NT, 0, ls>>>(
                 fa, (cx ? H.d_sp_c : H.d_sp_r) + L.task_off, cx ? H.d_soff_a_c : H.d_soff_a_r,
                 cx ? H.d_soff_b_c : H.d_soff_b_r, cx ? H.d_kpad_c : H.d_kpad_r, F.sp_ahi, F.sp_alo, F.sp_bhi,
-                F.sp_blo);
+                F.sp_blo, F.sp_as, F.sp_bs);
         }
         break;
       case L_DIAG_INV:
@@ -1753,7 +1756,7 @@ void rslab_default_factor_settings(rslab_factor_settings* s) {
   s->scaling = RSLAB_SCALING_ONEPASS;
   s->use_graph = 1;
   s->stream = nullptr;
-  s->schur_engine = RSLAB_SCHUR_TENSOR;
+  s->schur_engine = RSLAB_SCHUR_AUTO;
   s->drop_tol = 0.0;
   s->overlap = 1;
 }
@@ -2054,6 +2057,10 @@ static void setup_mm_pools(rslab_fac_handle& F) {
   F.sp_alo = F.al<float>(na);
   F.sp_bhi = F.al<float>(nb);
   F.sp_blo = F.al<float>(nb);
+  if (cx) {
+    F.sp_as = F.al<float>(na);
+    F.sp_bs = F.al<float>(nb);
+  }
   F.wbuf = F.al<float>((size_t)2 * H.w_elems * (cx ? 2 : 1));
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
@@ -2073,12 +2080,13 @@ static void setup_mm_pools(rslab_fac_handle& F) {
     const long long kp = cx ? H.kpad_c[k] : H.kpad_r[k];
     const long long oa = cx ? H.soff_a_c[k] : H.soff_a_r[k];
     const long long ob = cx ? H.soff_b_c[k] : H.soff_b_r[k];
-    const long long brows = cx ? 2 * m : m;
-    float* bases[MM_MAPS] = {F.sp_ahi + oa, F.sp_alo + oa, F.sp_bhi + ob, F.sp_blo + ob};
-    for (int j = 0; j < MM_MAPS; ++j) {
-      const cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)(j < 2 ? m : brows)};
+    float* bases[MM_MAPS] = {F.sp_ahi + oa, F.sp_alo + oa, F.sp_bhi + ob, F.sp_blo + ob,
+                             cx ? F.sp_as + oa : nullptr, cx ? F.sp_bs + ob : nullptr};
+    for (int j = 0; j < (cx ? MM_MAPS : 4); ++j) {
+      const bool a_side = j < 2 || j == 4;
+      const cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)m};
       const cuuint64_t strides[1] = {(cuuint64_t)kp * 4};
-      const cuuint32_t box[2] = {32, (cuuint32_t)(j < 2 ? MM_M : MM_BOX_B)};
+      const cuuint32_t box[2] = {32, (cuuint32_t)(a_side ? MM_M : MM_BOX_B)};
       const cuuint32_t estr[2] = {1, 1};
       const CUresult r = encode(&maps[(size_t)k * MM_MAPS + j], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, bases[j], dims,
                                 strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -2123,6 +2131,10 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
       F->set = *settings;
     else
       rslab_default_factor_settings(&F->set);
+    if (F->set.schur_engine == RSLAB_SCHUR_AUTO)
+      F->set.schur_engine = sym->flops_model >= RSLAB_SCHUR_AUTO_MIN_FLOPS ? RSLAB_SCHUR_TENSOR : RSLAB_SCHUR_FMA;
+    if (F->set.schur_engine != RSLAB_SCHUR_TENSOR && F->set.schur_engine != RSLAB_SCHUR_FMA)
+      throw RslabError(Status::InvalidInput, "schur_engine must be RSLAB_SCHUR_TENSOR, _FMA or _AUTO");
     int prio_lo = 0, prio_hi = 0;
     CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     if (F->set.stream) {
@@ -2351,6 +2363,7 @@ int rslab_factor_info(const rslab_fac_handle* F, rslab_factor_info_t* info) {
   info->dtype = F->dtype;
   info->dtype_hi = F->dtype_hi;
   info->multiprocessors = 0;
+  info->schur_engine = F->set.schur_engine;
   if (F->sym && F->sym->device >= 0)
     cudaDeviceGetAttribute(&info->multiprocessors, cudaDevAttrMultiProcessorCount, F->sym->device);
   return 0;

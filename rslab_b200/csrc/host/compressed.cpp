@@ -44,9 +44,7 @@ struct Cx {
 // The reference's Scalar operations (src/scalar.rs): fmadd is the fused
 // mul_add (complex: re = fma(a.re, b.re, fma(-a.im, b.im, c.re)), im =
 // fma(a.re, b.im, fma(a.im, b.re, c.im))); every other product and sum is
-// rounded on its own.
-#pragma GCC push_options
-#pragma GCC optimize("fp-contract=off")
+// rounded on its own (the host sources are built with -ffp-contract=off).
 template <typename R>
 struct Ops {
   static R zero() { return R(0); }
@@ -115,7 +113,6 @@ int solve_compressed(const rslab_cfac_handle& C, const T* rhs, T* x) {
   for (int64_t i = 0; i < n; ++i) x[C.perm[i]] = y[i];
   return 0;
 }
-#pragma GCC pop_options
 
 size_t field_bytes(int dtype) { return dtype == RSLAB_C64 ? 16 : (dtype == RSLAB_F64 || dtype == RSLAB_C32) ? 8 : 4; }
 

@@ -199,9 +199,10 @@ class SolverSettings:
     scaling: str = "onepass"  # or "identity"
     use_graph: bool = True
     given_perm: Optional[np.ndarray] = None
-    # f32/c32 descendant updates: "tensor" (3xTF32 tcgen05) or "fma" (CUDA-core
-    # fp32 in the oracle's operation order, bit-exact)
-    schur_engine: str = "tensor"
+    # descendant updates: "tensor" (GEMM tiles: 3xTF32 tcgen05 for f32 / c32,
+    # FP64 DMMA for f64 / c64), "fma" (CUDA cores in the oracle's operation
+    # order, bit-exact) or "auto" (tensor from 2e8 model flops, else fma)
+    schur_engine: str = "auto"
     # incomplete factor: drop |L_ip| < drop_tol * max_i |L_ip| per column
     drop_tol: Optional[float] = None
     # schedule of the factor's launches: side streams overlap independent
@@ -270,7 +271,10 @@ class SolverSettings:
         s.scaling = N.SCALING_ONEPASS if self.scaling == "onepass" else N.SCALING_IDENTITY
         s.use_graph = int(self.use_graph)
         s.stream = stream
-        s.schur_engine = N.SCHUR_FMA if self.schur_engine == "fma" else N.SCHUR_TENSOR
+        engines = {"tensor": N.SCHUR_TENSOR, "fma": N.SCHUR_FMA, "auto": N.SCHUR_AUTO}
+        if self.schur_engine not in engines:
+            raise ValueError(f"schur_engine must be one of {sorted(engines)}")
+        s.schur_engine = engines[self.schur_engine]
         s.overlap = int(bool(self.overlap))
         return s
 
@@ -331,6 +335,7 @@ class Diagnostics:
     threads: int = 0
     estimate: Optional[MemoryEstimate] = None
     stages: list = field(default_factory=list)
+    schur_engine: str = ""   # the descendant-update engine the factor ran with
 
     def total_ms(self) -> float:
         return sum(s.wall_ms for s in self.stages)
@@ -535,7 +540,8 @@ class LdltSolver:
         return Diagnostics(i.factor_ms, i.solve_ms, nnz, si.flops_model, si.flops_proxy, int(si.nsuper),
                            int(si.nlevels), threads=int(i.multiprocessors),
                            estimate=self._sym.estimate_memory(self.dtype),
-                           stages=[StageReport("factor", float(i.factor_ms), int(si.flops_model), nnz * entry_bytes)])
+                           stages=[StageReport("factor", float(i.factor_ms), int(si.flops_model), nnz * entry_bytes)],
+                           schur_engine="fma" if i.schur_engine == N.SCHUR_FMA else "tensor")
 
     def stream(self) -> int:
         return int(N.lib.rslab_factor_stream(self._h) or 0)

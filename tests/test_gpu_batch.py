@@ -18,14 +18,18 @@ def systems():
     return [matgen.c3_matrix(s) for s in (6, 11, 9, 14)] + [matgen.c1_matrix(20), matgen.c1_matrix(13)]
 
 
-def test_batch_factor_bit_identical_to_single_factors():
+# The engine is pinned: "auto" picks by the analysis' size, and the merged
+# batch is larger than any of its systems.
+@pytest.mark.parametrize("engine", ["fma", "tensor"])
+def test_batch_factor_bit_identical_to_single_factors(engine):
+    st = SolverSettings(schur_engine=engine)
     sy = systems()
     b = BatchSystems(sy)
     sym = analyze_batch(b)
-    fb = factor_batch(b, sym).export_factors()
+    fb = factor_batch(b, sym, st).export_factors()
     off = 0
     for a in sy:
-        f = LdltSymbolic.analyze(a).factor(a).export_factors()
+        f = LdltSymbolic.analyze(a).factor(a, st).export_factors()
         sl = slice(off, off + a.n)
         assert np.array_equal(fb.d_diag[sl], f.d_diag)
         assert np.array_equal(fb.d_subdiag[sl], f.d_subdiag)
@@ -34,20 +38,21 @@ def test_batch_factor_bit_identical_to_single_factors():
         off += a.n
     total = [0, 0, 0]
     for a in sy:
-        i = LdltSymbolic.analyze(a).factor(a).inertia()
+        i = LdltSymbolic.analyze(a).factor(a, st).inertia()
         total = [total[0] + i.positive, total[1] + i.negative, total[2] + i.zero]
     assert tuple(fb.inertia) == tuple(total)
 
 
 def test_batch_solve_matches_single_solves():
+    st = SolverSettings(schur_engine="fma")
     sy = systems()
     b = BatchSystems(sy)
     sym = analyze_batch(b)
-    s = factor_batch(b, sym)
+    s = factor_batch(b, sym, st)
     rhs = [matgen.uniform_rhs(a.n, 4, 10 + i) for i, a in enumerate(sy)]
     xs = b.split(s.solve_many(b.stack_rhs(rhs), 4))
     for a, r, x in zip(sy, rhs, xs):
-        x1 = LdltSymbolic.analyze(a).factor(a).solve_many(r, 4)
+        x1 = LdltSymbolic.analyze(a).factor(a, st).solve_many(r, 4)
         assert np.array_equal(x, x1)
 
 

@@ -5,13 +5,16 @@ tolerance against the bit-exact CUDA-core engine (itself bit-identical to the
 oracle): on fixed pivot sequences (diagonally dominant stencils, every pivot
 a diagonal 1x1) L and D agree entry by entry within 1e-12 relative; on
 indefinite matrices the inertia is exact and backward errors stay at the
-FP64 level; the engine is deterministic."""
+FP64 level; the engine is deterministic.  The default engine setting ("auto")
+picks these tiles from 2e8 model flops and the bit-exact engine below."""
 import numpy as np
 import pytest
 
 from oracle.oracle import OracleSolver, backward_error
 from rslab_b200 import LdltSymbolic, Ordering, SolverSettings, matgen
-from tests.helpers import rel_err
+from tests.helpers import kkt_cases, rel_err
+
+TENSOR = dict(schur_engine="tensor")
 
 pytestmark = pytest.mark.gpu
 
@@ -28,7 +31,7 @@ def dominant3d(side, complex_):
                                                  (True, 28, True)])
 def test_dmma_entrywise_on_fixed_pivot_sequence(complex_, side, metis):
     a = dominant3d(side, complex_)
-    st = SolverSettings(ordering=Ordering.METIS_ND if metis else Ordering.AMD)
+    st = SolverSettings(ordering=Ordering.METIS_ND if metis else Ordering.AMD, **TENSOR)
     sym = LdltSymbolic.analyze_with(a, st)
     dm = sym.factor(a, st).export_factors()
     fm = sym.factor(a, SolverSettings(ordering=st.ordering, schur_engine="fma")).export_factors()
@@ -41,11 +44,11 @@ def test_dmma_entrywise_on_fixed_pivot_sequence(complex_, side, metis):
 @pytest.mark.parametrize("case", ["c1_128", "c3_20", "c2_24_metis"])
 def test_dmma_indefinite_inertia_and_backward_error(case):
     if case == "c1_128":
-        a, st, cx = matgen.c1_matrix(128), SolverSettings(), False
+        a, st, cx = matgen.c1_matrix(128), SolverSettings(**TENSOR), False
     elif case == "c3_20":
-        a, st, cx = matgen.c3_matrix(20), SolverSettings(), False
+        a, st, cx = matgen.c3_matrix(20), SolverSettings(**TENSOR), False
     else:
-        a, st, cx = matgen.c2_matrix(24), SolverSettings(ordering=Ordering.METIS_ND), True
+        a, st, cx = matgen.c2_matrix(24), SolverSettings(ordering=Ordering.METIS_ND, **TENSOR), True
     sym = LdltSymbolic.analyze_with(a, st)
     dm = sym.factor(a, st)
     orc = OracleSolver(a, sym.export())
@@ -59,7 +62,46 @@ def test_dmma_indefinite_inertia_and_backward_error(case):
 
 def test_dmma_deterministic():
     a = matgen.c2_matrix(20)
-    sym = LdltSymbolic.analyze_with(a, SolverSettings(ordering=Ordering.METIS_ND))
-    f1 = sym.factor(a).export_factors()
-    f2 = sym.factor(a).export_factors()
+    st = SolverSettings(ordering=Ordering.METIS_ND, **TENSOR)
+    sym = LdltSymbolic.analyze_with(a, st)
+    f1 = sym.factor(a, st).export_factors()
+    f2 = sym.factor(a, st).export_factors()
     assert np.array_equal(f1.l_values, f2.l_values) and np.array_equal(f1.d_diag, f2.d_diag)
+
+
+KKT = kkt_cases()
+
+
+@pytest.mark.parametrize("case", KKT, ids=[c[0]["name"] for c in KKT])
+def test_dmma_kkt_fixtures(case):
+    """The reference's KKT fixtures through the DMMA tiles: the oracle's
+    inertia wherever the fixture's own second solver agrees with it (where
+    it does not, the matrix is singular to working precision and the sign of
+    its smallest pivot is rounding), backward error at the oracle's level."""
+    e, a, rhs = case
+    st = SolverSettings(**TENSOR)
+    sym = LdltSymbolic.analyze_with(a, st)
+    orc = OracleSolver(a, sym.export())
+    o = orc.factors()
+    if o.status != 0:
+        return
+    g = sym.factor(a, st)
+    ref, second = e["inertia"], e["mumps_inertia"]
+    if (second["positive"], second["negative"], second["zero"]) == (ref["positive"], ref["negative"], ref["zero"]):
+        assert tuple(g.inertia()) == o.inertia
+    x = g.solve(rhs)
+    xo = orc.solve_many(rhs, 1)
+    assert backward_error(a, x, rhs) <= max(1e-12, 100 * backward_error(a, xo, rhs))
+
+
+def test_auto_engine_by_size():
+    small = matgen.c1_matrix(48)
+    sym = LdltSymbolic.analyze(small)
+    assert sym.info().flops_model < 2e8
+    assert sym.factor(small).diagnostics().schur_engine == "fma"
+    big = dominant3d(28, True)
+    st = SolverSettings(ordering=Ordering.METIS_ND)
+    sym = LdltSymbolic.analyze_with(big, st)
+    assert sym.info().flops_model >= 2e8
+    assert sym.factor(big, st).diagnostics().schur_engine == "tensor"
+    assert sym.factor(big, SolverSettings(ordering=Ordering.METIS_ND, schur_engine="fma")).diagnostics().schur_engine == "fma"
