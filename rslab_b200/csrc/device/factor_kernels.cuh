@@ -800,6 +800,99 @@ __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int n
 
 constexpr int DEEP_R = 32;  // deep rows per replay chunk
 
+// The end of a BK panel block, shared by both getf2 kernels: the block's
+// local pivot order into lperm, the status word (first failing supernode,
+// perturbation count), the packed block back into the panel (the 2x2
+// coupling entry lives in dsub only: its panel slot is stored as an exact
+// zero), the block's interchanges applied to the rows' left segments
+// (columns [0, kb)), and for a short panel the replay of the block's pivot
+// steps on its deep rows.  Every thread of the CTA calls it; `src_row` has
+// room for pw ints.
+template <typename T, int NT>
+__device__ void getf2_finish(const FactorArgs& fa, int s, int kb, int pw, int nb, int nrow, int ke, int fuse,
+                             T* panel, T* A, int* lp_s, int* lpermG, int* ctl, int* swp_p, int* swp_q, int* supp,
+                             int* src_row, unsigned char* kindG, T* dG, T* dsG, T* snap, int* swaps, int nperturbed,
+                             unsigned char* smem_raw) {
+  using F = Field<T>;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  constexpr int NW = NT / 32;
+  for (int i = tid; i < pw; i += NT) lpermG[kb + i] = lp_s[i];
+  if (ctl[3]) {
+    if (tid == 0) {
+      if (atomicCAS(&fa.status[0], 0, 1) == 0) fa.status[1] = s;
+    }
+    return;
+  }
+  if (tid == 0 && nperturbed) atomicAdd(&fa.status[2], nperturbed);
+  // Write the block back; the 2x2 coupling entry (i = j + 1 of a 2x2) lives
+  // in dsub only, so its panel slot is stored as an exact zero (it is never
+  // an L multiplier).
+  __syncthreads();
+  for (int j = warp; j < pw; j += NW) {
+    const bool two = kindG[j] == 1;
+    for (int i = j + lane; i < pw; i += 32)
+      panel[(kb + i) + (long long)(kb + j) * nrow] = (two && i == j + 1) ? F::zero() : A[pk(i, j, pw)];
+  }
+  // Left row segments of the interchanges (columns [0, kb), rows of this
+  // block): the swap sequence composes to one row permutation of the block;
+  // only the rows it moves are copied, in column chunks whose loads are all
+  // in flight before the barrier that precedes the stores (same final values).
+  const int nsw = ctl[2];
+  if (nsw > 0 && kb > 0) {
+    __syncthreads();
+    if (tid == 0) {
+      for (int r = 0; r < pw; ++r) src_row[r] = r;
+      for (int t = 0; t < nsw; ++t) {
+        const int p = swp_p[t] - kb, q = swp_q[t] - kb;
+        const int x = src_row[p];
+        src_row[p] = src_row[q];
+        src_row[q] = x;
+      }
+      int m = 0;
+      for (int r = 0; r < pw; ++r)
+        if (src_row[r] != r) supp[m++] = r;
+      ctl[1] = m;
+    }
+    __syncthreads();
+    const int ns = ctl[1];
+    if (ns > 0) {
+      constexpr int PER = 8;  // elements per thread per chunk
+      const int cols = max(1, (NT * PER) / ns);
+      for (int j0 = 0; j0 < kb; j0 += cols) {
+        const int jn = min(cols, kb - j0);
+        T v[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+          const int idx = tid + u * NT;
+          if (idx < ns * jn) {
+            const int r = supp[idx % ns], j = j0 + idx / ns;
+            v[u] = panel[(kb + src_row[r]) + (long long)j * nrow];
+          }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+          const int idx = tid + u * NT;
+          if (idx < ns * jn) {
+            const int r = supp[idx % ns], j = j0 + idx / ns;
+            panel[(kb + r) + (long long)j * nrow] = v[u];
+          }
+        }
+        __syncthreads();
+      }
+    }
+  }
+  // kind/d written by tid 0 are read by the replay below.
+  __syncthreads();
+  if (fuse && nrow > ke) {
+    // Replay this block's pivot steps on the deep rows [ke, nrow).
+    unsigned char* pmem = smem_raw + (((size_t)(DEEP_R + 1) * nb * sizeof(T) + 15) & ~size_t(15));
+    const ReplayProg<T> P = load_replay_prog<T, NT>(pmem, pw, nb, swaps, dG, dsG, kindG);
+    __syncthreads();
+    replay_deep_rows<T, NT>(panel, nrow, kb, pw, nb, ke, nrow, snap, P, A);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // getf2: task = (s, kb, slot, fuse) — unblocked BK over panel columns [kb, ke)
 // with every pivot candidate, update and interchange bounded to rows < ke.
@@ -1115,82 +1208,397 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
     }
     __syncthreads();
   }
-  for (int i = tid; i < pw; i += NT) lpermG[kb + i] = lp_s[i];
-  if (ctl[3]) {
-    if (tid == 0) {
-      if (atomicCAS(&fa.status[0], 0, 1) == 0) fa.status[1] = s;
-    }
-    return;
+  getf2_finish<T, NT>(fa, s, kb, pw, nb, nrow, ke, fuse, panel, A, lp_s, lpermG, ctl, swp_p, swp_q, supp,
+                      reinterpret_cast<int*>(l1), kindG, dG, dsG, snap, swaps, nperturbed, smem_raw);
+}
+
+// ---------------------------------------------------------------------------
+// getf2, left-looking form (the single-precision fields' tensor engine): the
+// same panel-bounded Bunch-Kaufman steps, decisions and outputs as k_getf2,
+// but no trailing update of the block.  The block keeps its ORIGINAL values
+// in the columns not yet pivoted; step k first forms the column it needs,
+//   v[i] = A0(i, c) - sum_{p < k} G(i, p) L(c, p),   i in [k, pw),
+// G = L D the unscaled columns of the finished steps, as one GEMV over all
+// 16 warps (4 to 16 partial sums per row), for c = k and, when the BK test
+// needs the row maximum (or a recorded step names another column), for the
+// candidate column too.  The rest of a step runs on the row team, warps 0-3
+// (one per SM sub-partition, one row per thread): the partial sums, the
+// arg-max, the decision (every team thread takes it from the same values),
+// and the multipliers; the interchange, when there is one, on warp 0.  The
+// BK tests compare squared moduli, so the decision path has no square roots
+// or divisions.  A step costs two block barriers (four with the candidate
+// column) and a named barrier of the team.  The sums run in another order
+// than the oracle's, so this form is used only where parity is by
+// tolerance; k_getf2 stays the bit-exact form.
+// ---------------------------------------------------------------------------
+template <typename T>
+__host__ __device__ constexpr size_t smem_getf2_ll_bytes(int nb) {
+  const size_t steps = (size_t)nb * (nb + 1) * sizeof(T)  // A and G, packed lower
+                       + (size_t)2 * nb * sizeof(T)       // the formed columns
+                       + (size_t)4 * 128 * sizeof(T)      // GEMV partial sums
+                       + 16 + 32 * 8 + 32 * 4 + 16 * 4 + 4 * (size_t)nb * 4;
+  // the fused deep-row replay reuses the same memory after the write-back
+  const size_t replay =
+      (((size_t)(DEEP_R + 1) * nb * sizeof(T) + 15) & ~size_t(15)) + (size_t)nb * (3 * sizeof(T) + 5) + 16;
+  return (steps > replay ? steps : replay) + 64;
+}
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* __restrict__ tasks, int nb_small,
+                                                 int nb_big) {
+  static_assert(NT == 512, "four partial sums of 128 rows");
+  using F = Field<T>;
+  if (fa.status[0] != 0) return;
+  const double pfloor = fa.floor_dev ? *fa.floor_dev : fa.perturb_floor;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, kb = tk.y, slot = tk.z, fuse = tk.w;
+  const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
+  const int nb = ncol >= 512 ? nb_big : nb_small;
+  const int ke = min(kb + nb, ncol), pw = ke - kb;
+  T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
+  T* dG = reinterpret_cast<T*>(fa.d) + first + kb;
+  T* dsG = reinterpret_cast<T*>(fa.dsub) + first + kb;
+  unsigned char* kindG = fa.kind + first + kb;
+  int* lpermG = fa.lperm + first;
+  unsigned char* sc = reinterpret_cast<unsigned char*>(fa.scratch) + (long long)slot * fa.scratch_stride;
+  T* snap = reinterpret_cast<T*>(sc);                              // nb x nb
+  int* swaps = reinterpret_cast<int*>(snap + (long long)nb * nb);  // nb
+
+  const int npk = pw * (pw + 1) / 2;
+  T* A = reinterpret_cast<T*>(smem_raw);  // packed lower: L (pivoted columns), A0 (the rest)
+  T* Gs = A + npk;                        // packed lower: G of the pivoted columns
+  T* v1 = Gs + npk;                       // formed column k
+  T* v2 = v1 + pw;                        // formed candidate column
+  T* red = v2 + pw;                       // 4 x 128 partial sums
+  double* red_v = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(red + 4 * 128) + 15) & ~uintptr_t(15));
+  int* red_i = reinterpret_cast<int*>(red_v + 32);
+  int* ctl = red_i + 32;  // [1] scratch [2] nswaps [3] error [4] step k [5] kstep [6] kp [7] extra column
+  int* lp_s = ctl + 16;
+  int* swp_p = lp_s + nb;
+  int* swp_q = swp_p + nb;
+  int* supp = swp_q + nb;
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+#pragma unroll 8
+  for (int e = tid; e < 128 * 128; e += NT) {
+    const int i = e & 127, j = e >> 7;
+    if (i < pw && j <= i) A[pk(i, j, pw)] = panel[(kb + i) + (long long)(kb + j) * nrow];
   }
-  if (tid == 0 && nperturbed) atomicAdd(&fa.status[2], nperturbed);
-  // Write the block back; the 2x2 coupling entry (i = j + 1 of a 2x2) lives
-  // in dsub only, so its panel slot is stored as an exact zero (it is never
-  // an L multiplier).
+  if (kb == 0)
+    for (int p = tid; p < ncol; p += NT) lpermG[p] = p;
+  for (int e = tid; e < pw; e += NT) {
+    dG[e] = F::zero();
+    dsG[e] = F::zero();
+    kindG[e] = 0;
+    swaps[e] = -1;
+  }
+  for (int e = tid; e < pw * nb; e += NT) snap[(e / nb) * nb + (e % nb)] = F::zero();
+  if (tid == 0) {
+    ctl[2] = 0;
+    ctl[3] = 0;
+    ctl[4] = 0;
+    ctl[7] = -1;
+  }
   __syncthreads();
-  for (int j = warp; j < pw; j += NW) {
-    const bool two = kindG[j] == 1;
-    for (int i = j + lane; i < pw; i += 32)
-      panel[(kb + i) + (long long)(kb + j) * nrow] = (two && i == j + 1) ? F::zero() : A[pk(i, j, pw)];
-  }
-  // Left row segments of the interchanges (columns [0, kb), rows of this
-  // block): the swap sequence composes to one row permutation of the block;
-  // only the rows it moves are copied, in column chunks whose loads are all
-  // in flight before the barrier that precedes the stores (same final values).
-  const int nsw = ctl[2];
-  if (nsw > 0 && kb > 0) {
-    int* src_row = reinterpret_cast<int*>(l1);  // pw ints (l1/l2 are free now)
-    __syncthreads();
-    if (tid == 0) {
-      for (int r = 0; r < pw; ++r) src_row[r] = r;
-      for (int t = 0; t < nsw; ++t) {
-        const int p = swp_p[t] - kb, q = swp_q[t] - kb;
-        const int x = src_row[p];
-        src_row[p] = src_row[q];
-        src_row[q] = x;
-      }
-      int m = 0;
-      for (int r = 0; r < pw; ++r)
-        if (src_row[r] != r) supp[m++] = r;
-      ctl[1] = m;
-    }
-    __syncthreads();
-    const int ns = ctl[1];
-    if (ns > 0) {
-      constexpr int PER = 8;  // elements per thread per chunk
-      const int cols = max(1, (NT * PER) / ns);
-      for (int j0 = 0; j0 < kb; j0 += cols) {
-        const int jn = min(cols, kb - j0);
-        T v[PER];
-#pragma unroll
-        for (int u = 0; u < PER; ++u) {
-          const int idx = tid + u * NT;
-          if (idx < ns * jn) {
-            const int r = supp[idx % ns], j = j0 + idx / ns;
-            v[u] = panel[(kb + src_row[r]) + (long long)j * nrow];
-          }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int u = 0; u < PER; ++u) {
-          const int idx = tid + u * NT;
-          if (idx < ns * jn) {
-            const int r = supp[idx % ns], j = j0 + idx / ns;
-            panel[(kb + r) + (long long)j * nrow] = v[u];
-          }
-        }
-        __syncthreads();
-      }
-    }
-  }
-  // kind/d written by tid 0 are read by the replay below.
+  for (int i = tid; i < pw; i += NT) lp_s[i] = lpermG[kb + i];
   __syncthreads();
-  if (fuse && nrow > ke) {
-    // Replay this block's pivot steps on the deep rows [ke, nrow).
-    unsigned char* pmem = smem_raw + (((size_t)(DEEP_R + 1) * nb * sizeof(T) + 15) & ~size_t(15));
-    const ReplayProg<T> P = load_replay_prog<T, NT>(pmem, pw, nb, swaps, dG, dsG, kindG);
+  const double alpha = (1.0 + sqrt(17.0)) / 8.0;
+  int nperturbed = 0;
+  const bool reuse = fa.pivot_reuse && fa.pivrec && *fa.pivot_reuse != 0;
+  int* prec = fa.pivrec ? fa.pivrec + first + kb : nullptr;
+
+  // Partial sums of column c over the pivoted columns p < k.  The rows
+  // [k, pw) take R = 32, 64 or 128 threads each group (the smallest that
+  // covers them) and the 512 / R groups split the columns: thread (row k +
+  // tid % R, group g = tid / R) sums p = g, g + 512 / R, ... in two
+  // interleaved accumulators (independent loads in flight).
+  auto groups_of = [&](int k) { return pw - k <= 32 ? 16 : pw - k <= 64 ? 8 : 4; };
+  auto gemv = [&](int k, int c) {
+    const int ng = groups_of(k), lr = ng == 4 ? 7 : ng == 8 ? 6 : 5;  // R = 512 / ng = 1 << lr
+    const int rr = tid & ((1 << lr) - 1), g = tid >> lr, i = k + rr, R = 1 << lr;
+    if (i < pw) {
+      T acc0 = F::zero(), acc1 = F::zero();
+      int p = g;
+      for (; p + ng < k; p += 2 * ng) {
+        const int cp0 = p * pw - (p * (p + 1)) / 2, cp1 = (p + ng) * pw - ((p + ng) * (p + ng + 1)) / 2;
+        acc0 = F::fma_(Gs[cp0 + i], A[cp0 + c], acc0);
+        acc1 = F::fma_(Gs[cp1 + i], A[cp1 + c], acc1);
+      }
+      if (p < k) {
+        const int cp = p * pw - (p * (p + 1)) / 2;
+        acc0 = F::fma_(Gs[cp + i], A[cp + c], acc0);
+      }
+      red[g * R + rr] = F::add(acc0, acc1);
+    }
+  };
+  // The row team: warps 0-3 (one per SM sub-partition), thread r owns row
+  // k + r of the formed columns.  Its phases synchronise on a named barrier
+  // of 128 threads; the other 12 warps only take part in the GEMVs.
+  auto team_sync = []() { asm volatile("bar.sync 1, 128;" ::: "memory"); };
+  // Team thread r: v[k + r] = A0(k + r, c) - the partial sums (all of the
+  // row's partial loads issued before its tree sum).
+  auto form_row = [&](int k, int c, T* v, int r) {
+    const int ng = groups_of(k), R = ng == 4 ? 128 : ng == 8 ? 64 : 32, i = k + r;
+    if (r < R && i < pw) {
+      const T a = i >= c ? A[pk(i, c, pw)] : A[pk(c, i, pw)];
+      T part[16];
+#pragma unroll
+      for (int g = 0; g < 16; ++g) part[g] = g < ng ? red[g * R + r] : F::zero();
+#pragma unroll
+      for (int h = 8; h > 0; h >>= 1)
+#pragma unroll
+        for (int g = 0; g < h; ++g) part[g] = F::add(part[g], part[g + h]);
+      v[i] = F::sub(a, part[0]);
+    }
+  };
+  // 1 / z with one division (the multipliers only need fp32 accuracy here)
+  auto inv = [&](T z) -> T {
+    if constexpr (F::complex) {
+      const float rz = 1.0f / (z.re * z.re + z.im * z.im);
+      return T{z.re * rz, -z.im * rz};
+    } else {
+      return 1.0f / z;
+    }
+  };
+  // Warp 0 of the team: the interchange of p = k (1x1) or k + 1 (2x2) with q
+  // in the unpivoted part (A0), in rows p, q of the pivoted columns (L, G)
+  // and of the formed columns, in lperm and the swap log.
+  auto interchange = [&](int k, int p, int q) {
+    for (int i = q + 1 + lane; i < pw; i += 32) {
+      T t = A[pk(i, p, pw)];
+      A[pk(i, p, pw)] = A[pk(i, q, pw)];
+      A[pk(i, q, pw)] = t;
+    }
+    for (int i = p + 1 + lane; i < q; i += 32) {
+      T t = A[pk(i, p, pw)];
+      A[pk(i, p, pw)] = A[pk(q, i, pw)];
+      A[pk(q, i, pw)] = t;
+    }
+    for (int jj = lane; jj < p; jj += 32) {
+      T t = A[pk(p, jj, pw)];
+      A[pk(p, jj, pw)] = A[pk(q, jj, pw)];
+      A[pk(q, jj, pw)] = t;
+      if (jj < k) {
+        t = Gs[pk(p, jj, pw)];
+        Gs[pk(p, jj, pw)] = Gs[pk(q, jj, pw)];
+        Gs[pk(q, jj, pw)] = t;
+      }
+    }
+    if (lane == 0) {
+      T t = A[pk(p, p, pw)];
+      A[pk(p, p, pw)] = A[pk(q, q, pw)];
+      A[pk(q, q, pw)] = t;
+      t = v1[p];
+      v1[p] = v1[q];
+      v1[q] = t;
+      t = v2[p];
+      v2[p] = v2[q];
+      v2[q] = t;
+      const int lpv = lp_s[p];
+      lp_s[p] = lp_s[q];
+      lp_s[q] = lpv;
+      swaps[k] = kb + q;
+      const int ns = ctl[2];
+      swp_p[ns] = kb + p;
+      swp_q[ns] = kb + q;
+      ctl[2] = ns + 1;
+    }
+  };
+  // Team thread r after the interchange: the multipliers of row k + r (1x1)
+  // or k + 2 + r (2x2), their G and snapshot entries, and (thread 0) D and
+  // the pivot block's entries of A.  Every team thread evaluates the pivot
+  // block itself (same values, same result); returns the error flag.
+  auto finish_rows = [&](int k, int kstep, int kp, int r) -> bool {
+    bool err = false;
+    if (kstep == 1) {
+      const T* v = kp == k ? v1 : v2;  // a 1x1 step with interchange pivots on the candidate column
+      T dk = v[k];
+      if (pfloor >= 0.0) {
+        const double m = F::mag(dk);
+        if (m < pfloor) {
+          dk = m == 0.0 ? F::from_real(pfloor) : F::scale(dk, pfloor / m);
+          if (r == 0) ++nperturbed;
+        }
+      } else if (F::is_zero(dk)) {
+        err = true;
+      }
+      if (!err) {
+        const T dinv = inv(dk);
+        const int i = k + 1 + r;
+        if (i < pw) {
+          const T a = v[i], w = F::mul(a, dinv);
+          Gs[pk(i, k, pw)] = a;
+          snap[k * nb + i] = w;
+          A[pk(i, k, pw)] = w;
+        }
+        if (r == 0) {
+          A[pk(k, k, pw)] = dk;
+          dG[k] = dk;
+        }
+      }
+    } else {
+      T d11 = v1[k], d21 = v1[k + 1], d22 = v2[k + 1];
+      T det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
+      // the growth test |det| <= 1e-14 scale^2 on squares (scale = the
+      // largest modulus of the block)
+      const double scale2 = fmax(fmax(F::mag2(d11), F::mag2(d22)), F::mag2(d21));
+      const double growth_floor = 1e-14 * scale2;
+      if (pfloor >= 0.0) {
+        const double fl = fmax(pfloor * pfloor, growth_floor);
+        if (F::mag2(det) < fl * fl) {
+          const double lift = fmax(pfloor, sqrt(scale2) * sqrt(1e-14));
+          d11 = F::add(d11, F::from_real(lift));
+          d22 = F::add(d22, F::from_real(lift));
+          det = F::sub(F::mul(d11, d22), F::mul(d21, d21));
+          if (F::mag2(det) < fl * fl) det = F::add(det, F::from_real(fl));
+          if (r == 0) ++nperturbed;
+        }
+      } else if (F::mag2(det) <= growth_floor * growth_floor) {
+        err = true;
+      }
+      if (!err) {
+        const T detinv = inv(det);
+        if (r == 0) {
+          dG[k] = d11;
+          dsG[k] = d21;
+          dG[k + 1] = d22;
+          kindG[k] = 1;
+          kindG[k + 1] = 2;
+          A[pk(k, k, pw)] = d11;
+          A[pk(k + 1, k, pw)] = d21;
+          A[pk(k + 1, k + 1, pw)] = d22;
+        }
+        const int i = k + 2 + r;
+        if (i < pw) {
+          const T wik = v1[i], wik1 = v2[i];
+          const T a1 = F::mul(F::sub(F::mul(d22, wik), F::mul(d21, wik1)), detinv);
+          const T a2 = F::mul(F::sub(F::mul(d11, wik1), F::mul(d21, wik)), detinv);
+          Gs[pk(i, k, pw)] = wik;
+          Gs[pk(i, k + 1, pw)] = wik1;
+          snap[k * nb + i] = a1;
+          snap[(k + 1) * nb + i] = a2;
+          A[pk(i, k, pw)] = a1;
+          A[pk(i, k + 1, pw)] = a2;
+        }
+      }
+    }
+    return err;
+  };
+
+  const bool team = tid < 128;
+  const double a2 = alpha * alpha;
+  for (int k = 0; k < pw;) {
+    gemv(k, k);
     __syncthreads();
-    replay_deep_rows<T, NT>(panel, nrow, kb, pw, nb, ke, nrow, snap, P, A);
+    if (team) {
+      // column k, and per team warp the arg-max of the squared moduli below
+      // the diagonal (the BK tests run on squares: no square roots or
+      // divisions on the decision path)
+      const int r = tid;
+      form_row(k, k, v1, r);
+      double m2 = -1.0;
+      int idx = INT_MAX;
+      if (r >= 1 && k + r < pw) {
+        m2 = F::mag2(v1[k + r]);
+        idx = k + r;
+      }
+      warp_argmax(m2, idx);
+      if (lane == 0) {
+        red_v[warp] = m2;
+        red_i[warp] = idx;
+      }
+      if (r == 0) red_v[4] = F::mag2(v1[k]);
+      team_sync();
+      // every team thread takes the same decision from the same values
+      double col2 = -1.0;
+      int imax = INT_MAX;
+#pragma unroll
+      for (int w = 0; w < 4; ++w) argmax_combine(col2, imax, red_v[w], red_i[w]);
+      const double akk2 = red_v[4];
+      if (col2 < 0.0) {
+        col2 = 0.0;
+        imax = k;
+      }
+      int kstep = 1, kp = k, extra = -1;
+      bool err = false;
+      if (reuse) {
+        const int code = prec[k];
+        kstep = code < 0 ? 2 : 1;
+        kp = code < 0 ? -code - 1 : code;
+        if (kstep == 2 || kp != k) extra = kp;
+      } else if (fmax(akk2, col2) == 0.0) {
+        err = pfloor < 0.0;
+      } else if (akk2 < a2 * col2) {
+        extra = imax;
+      }
+      if (extra < 0 && !err) {
+        if (r == 0 && prec && !reuse) prec[k] = k;
+        err = finish_rows(k, 1, k, r);
+      }
+      if (r == 0) {
+        if (err) ctl[3] = 1;
+        ctl[4] = k + 1;
+        ctl[5] = kstep;
+        ctl[6] = kp;
+        ctl[7] = err ? -1 : extra;
+        red_v[5] = akk2;
+        red_v[6] = col2;
+      }
+    }
+    __syncthreads();
+    if (ctl[3]) break;
+    const int extra = ctl[7];
+    if (extra >= 0) {
+      gemv(k, extra);
+      __syncthreads();
+      if (team) {
+        const int r = tid;
+        form_row(k, extra, v2, r);
+        int kstep = ctl[5], kp = ctl[6];
+        if (!reuse) {
+          // the row maximum of the candidate row: its column over every row
+          // of the unpivoted part but itself
+          double m2 = 0.0;
+          if (k + r < pw && k + r != extra) m2 = F::mag2(v2[k + r]);
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+          if (lane == 0) red_v[8 + warp] = m2;
+          team_sync();
+          const double rmx = fmax(fmax(red_v[8], red_v[9]), fmax(red_v[10], red_v[11]));
+          // |a_kk| rowmax >= alpha colmax^2, |a_rr| >= alpha rowmax, squared
+          const double akk2 = red_v[5], col2 = red_v[6];
+          kstep = 1;
+          kp = k;
+          if (akk2 * rmx >= a2 * col2 * col2) {
+          } else if (F::mag2(v2[extra]) >= a2 * rmx) {
+            kp = extra;
+          } else {
+            kstep = 2;
+            kp = extra;
+          }
+          if (r == 0 && prec) prec[k] = kstep == 2 ? -kp - 1 : kp;
+        }
+        const int p = kstep == 1 ? k : k + 1;
+        if (kp != p) {
+          team_sync();  // every team thread has read v2 / red_v for its decision
+          if (warp == 0) interchange(k, p, kp);
+        }
+        team_sync();
+        const bool err = finish_rows(k, kstep, kp, r);
+        if (r == 0) {
+          if (err) ctl[3] = 1;
+          ctl[4] = k + kstep;
+        }
+      }
+      __syncthreads();
+      if (ctl[3]) break;
+    }
+    k = ctl[4];
   }
+  getf2_finish<T, NT>(fa, s, kb, pw, nb, nrow, ke, fuse, panel, A, lp_s, lpermG, ctl, swp_p, swp_q, supp,
+                      reinterpret_cast<int*>(v1), kindG, dG, dsG, snap, swaps, nperturbed, smem_raw);
 }
 
 // ---------------------------------------------------------------------------

@@ -913,6 +913,9 @@ struct KernelSetup {
     CK(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
     CK(cudaFuncSetAttribute(k_getf2<T, GETF2_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)smem_getf2(es, 128)));
+    if constexpr (TensorCmod<T>::ok)
+      CK(cudaFuncSetAttribute(k_getf2_ll<T, GETF2_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_getf2_ll_bytes<T>(128)));
     CK(cudaFuncSetAttribute(k_deep<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep(es, 128)));
     CK(cudaFuncSetAttribute(k_diag_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_diag_inv(es)));
     if constexpr (TensorCmod<T>::ok) {
@@ -1214,6 +1217,13 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
       case L_GETF2: {
         FactorArgs f2 = fa;
         f2.scratch_stride = getf2_scratch_stride(L.nb_slot, (long long)es);
+        if constexpr (TensorCmod<T>::ok) {
+          if (use_tc) {  // left-looking form: parity by tolerance, like the rest of the engine
+            k_getf2_ll<T, GETF2_NT><<<L.ntasks, GETF2_NT, smem_getf2_ll_bytes<T>(L.nb_slot), ls>>>(
+                f2, H.d_t4 + L.task_off, nb_small, nb_big);
+            break;
+          }
+        }
         k_getf2<T, GETF2_NT><<<L.ntasks, GETF2_NT, smem_getf2(es, L.nb_slot), ls>>>(f2, H.d_t4 + L.task_off,
                                                                                   nb_small, nb_big);
         break;

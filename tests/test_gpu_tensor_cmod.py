@@ -100,9 +100,29 @@ def test_tensor_cmod_deterministic():
     mk, dt = CASES["c32_3d"]
     a = mk().astype(dt)
     sym = LdltSymbolic.analyze(a)
-    f1 = sym.factor(a).export_factors()
-    f2 = sym.factor(a).export_factors()
+    st = SolverSettings(schur_engine="tensor")
+    f1 = sym.factor(a, st).export_factors()
+    f2 = sym.factor(a, st).export_factors()
     assert np.array_equal(f1.l_values, f2.l_values) and np.array_equal(f1.d_diag, f2.d_diag)
+
+
+@pytest.mark.parametrize("nb", [32, 64])
+def test_tensor_engine_with_panel_widths(nb):
+    """The tensor engine's panel kernels (left-looking getf2, block transform
+    of the deep rows, tensor-core in-panel Schur) with 32- and 64-wide blocks
+    (128 for the wide separators): on a fixed pivot sequence the factor
+    agrees with the FP64 one at fp32 level."""
+    from rslab_b200 import Ordering
+    a = spd3d(24, True)
+    st = SolverSettings(ordering=Ordering.METIS_ND, panel_nb=nb)
+    sym = LdltSymbolic.analyze_with(a, st)
+    f64 = sym.factor(a, SolverSettings(ordering=Ordering.METIS_ND, panel_nb=nb, schur_engine="fma")).export_factors()
+    tc = sym.factor(a.astype(np.complex64),
+                    SolverSettings(ordering=Ordering.METIS_ND, panel_nb=nb, schur_engine="tensor")).export_factors()
+    assert np.array_equal(tc.perm, f64.perm)
+    ld = float(np.max(np.abs(as_hi(tc.d_diag) - f64.d_diag) / np.abs(f64.d_diag)))
+    ll = float(np.max(np.abs(as_hi(tc.l_values) - f64.l_values)) / np.max(np.abs(f64.l_values)))
+    assert ld <= 2e-6 and ll <= 2e-6, (ld, ll)
 
 
 @pytest.mark.parametrize("kind", ["real", "complex"])
