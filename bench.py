@@ -211,6 +211,7 @@ def cpu_sample(args):
     cpu_run(a, ex, b, args.nrhs)
     t, x = cpu_run(a, ex, b, args.nrhs)
     be = backward_error(a, x, b)
+    cpu_sample.solution = x  # the oracle's FP64 solution, for the GPU arms' forward errors
     return {"value": flops / t / 1e9, "unit": "GFLOP/s", "cores": os.cpu_count(), "kind": "port",
             "seconds": t,
             "sample": f"FP64 factor + {args.nrhs}-RHS solve of the full {args.side}^3 Helmholtz workload ({ordering}, "
@@ -995,6 +996,14 @@ def main():
     solve_gbs["note"] = ("algorithmic bytes 2 sum_s(c(c+1)/2 + (r-c)c) + 4 n nrhs + 2 n scalars per solve, "
                          "eager solve with per-launch events (no graph), of measured hbm_gbs")
     cpu_base = cpu_sample(args) if (rank == 0 and ws == 1 and not args.no_cpu) else None
+    if cpu_base is not None:
+        # forward errors of the GPU solutions against the oracle's FP64 solution
+        # of the same system (same matrix, ordering output and right-hand sides)
+        xo = np.asarray(cpu_sample.solution).reshape(x_mixed.shape)
+        fe = lambda x: float(np.abs(x - xo).max() / np.abs(xo).max())
+        cpu_base["mixed_forward_error_vs_oracle"] = fe(x_mixed)
+        if out_fp64 is not None:
+            cpu_base["fp64_forward_error_vs_oracle"] = fe(x64)
     if rank == 0:
         line = {
             "metric": "LDLT factor+solve GFLOP/s at bwd err <= 1e-14 (mixed/batched vs FP64 GPU)",
