@@ -59,7 +59,12 @@ template <> struct TcShape<c32> {
 
 constexpr int TC_MAP = TC_M + TC_N;      // bytes of the inverse maps of one pair
 
-__host__ __device__ constexpr size_t smem_cmod_tc_bytes() { return 1024 + TC_NS * (size_t)TC_STAGE + 128; }
+// After the stages: the barriers (128 bytes), then the block's D, dsub and
+// kind (at most 128 columns of an f32 / c32 block) staged by k_schur_tc.
+constexpr int TC_DSTAGE = 128 * (8 + 8 + 1) + 16;
+__host__ __device__ constexpr size_t smem_cmod_tc_bytes() {
+  return 1024 + TC_NS * (size_t)TC_STAGE + 128 + TC_DSTAGE;
+}
 
 // hi/lo split of 4 (or 2) consecutive K elements of an operand row, stored
 // at byte offset `off` of the hi and lo tiles.
@@ -267,13 +272,39 @@ __device__ __forceinline__ void tc_tile_pipeline(const FactorArgs& fa, const Src
         const int t = x.t0 + ta + jj;
         va[jj] = (x.i >= 0 && t < x.nck) ? x.Ar[(long long)t * x.lda] : F::zero();
       }
+      if constexpr (Src::kBonfly) {
+        // G = L D on the fly: the thread's columns and one neighbour on each
+        // side (a 2x2 pivot couples a column to one of them) in one batch of
+        // independent loads; D, dsub and kind come from shared memory.  The
+        // arithmetic is ld_G's.
+        T nv[NB + 2];
 #pragma unroll
-      for (int jj = 0; jj < NB; ++jj) {
-        const int t = x.t0 + tb + jj;
-        if constexpr (Src::kBonfly)
-          vb[jj] = (x.j >= 0 && t < x.nck) ? ld_G(x.Br, x.ldb, 0, t, x.dk, x.dsk, x.kk) : F::zero();
-        else
+        for (int jj = 0; jj < NB + 2; ++jj) {
+          const int t = x.t0 + tb + jj - 1;
+          nv[jj] = (x.j >= 0 && t >= 0 && t < x.nck) ? x.Br[(long long)t * x.ldb] : F::zero();
+        }
+#pragma unroll
+        for (int jj = 0; jj < NB; ++jj) {
+          const int t = x.t0 + tb + jj;
+          T g = F::zero();
+          if (x.j >= 0 && t < x.nck) {
+            const unsigned char kd = x.kk[t];
+            const T a = nv[jj + 1];
+            if (kd == 0)
+              g = F::mul(a, x.dk[t]);
+            else if (kd == 1)
+              g = F::add(F::mul(x.dk[t], a), F::mul(x.dsk[t], nv[jj + 2]));
+            else
+              g = F::add(F::mul(x.dsk[t - 1], nv[jj]), F::mul(x.dk[t], a));
+          }
+          vb[jj] = g;
+        }
+      } else {
+#pragma unroll
+        for (int jj = 0; jj < NB; ++jj) {
+          const int t = x.t0 + tb + jj;
           vb[jj] = (x.j >= 0 && t < x.nck) ? x.Br[(long long)t * x.ldb] : F::zero();
+        }
       }
     };
     int c = 0, pw = 0;
@@ -432,10 +463,21 @@ __global__ void __launch_bounds__(TC_NT, 1) k_schur_tc(FactorArgs fa, const int4
   const int ke = min(kb + nb, ncol);
   const int mt = nrow - ke, cw = ncol - ke;
   const T* panel = reinterpret_cast<const T*>(fa.panel) + fa.sn_poff[s];
-  SchurSrc<T> src{panel + ke + (long long)kb * nrow, (long long)nrow, ke - kb, r0, c0,
-                  min(TC_M, mt - r0), min(TC_N, cw - c0),
-                  reinterpret_cast<const T*>(fa.d) + first + kb, reinterpret_cast<const T*>(fa.dsub) + first + kb,
-                  fa.kind + first + kb};
+  // the block's D, dsub and kind into shared memory (after the stages and
+  // barriers; the pipeline's first block barrier publishes them)
+  const int pw = ke - kb;
+  const uint32_t sraw = smem_u32(smem_raw);
+  unsigned char* dst = smem_raw + (((sraw + 1023u) & ~1023u) - sraw) + TC_NS * TC_STAGE + 128;
+  T* d_s = reinterpret_cast<T*>(dst);
+  T* ds_s = d_s + 128;
+  unsigned char* kd_s = reinterpret_cast<unsigned char*>(ds_s + 128);
+  for (int t = threadIdx.x; t < pw; t += blockDim.x) {
+    d_s[t] = reinterpret_cast<const T*>(fa.d)[first + kb + t];
+    ds_s[t] = reinterpret_cast<const T*>(fa.dsub)[first + kb + t];
+    kd_s[t] = fa.kind[first + kb + t];
+  }
+  SchurSrc<T> src{panel + ke + (long long)kb * nrow, (long long)nrow, pw, r0, c0,
+                  min(TC_M, mt - r0), min(TC_N, cw - c0), d_s, ds_s, kd_s};
   tc_tile_pipeline<T>(fa, src, s, ke, ke, r0, c0, min(TC_M, mt - r0), min(TC_N, cw - c0), smem_raw);
 }
 
