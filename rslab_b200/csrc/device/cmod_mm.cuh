@@ -403,50 +403,73 @@ __global__ void __launch_bounds__(MM_NT, 1) k_cmod_mm(FactorArgs fa, const int4*
 // k_cmod_asm: task (s, rt << 16 | ct, pair_begin, pair_end) over the 128 x 64
 // tiles of the tensor-core plan; pair u (k, a, q0, nr << 16 | nc) with its
 // inverse maps (tile row -> offset from a, tile column -> offset from q0) and
-// its W element (a, q0) at wb[u], column stride wl[u].  256 threads: thread
-// (row t = tid & 127, half h = tid >> 7) owns tile columns 32 h .. 32 h + 31.
+// its W element (a, q0) at wb[u], column stride wl[u].  512 threads: thread
+// (row t = tid & 127, quarter h = tid >> 7) owns tile columns 16 h .. +15.
+// The pairs' maps and descriptors are copied to shared memory in batches of
+// ASM_PB (one coalesced copy), so per pair a thread issues only its 16
+// independent W loads; every tile element sums its pairs in update order.
 // ---------------------------------------------------------------------------
-// Two CTAs per SM except for c64, whose 32 accumulators take 128 registers.
+constexpr int ASM_NT = 512;
+constexpr int ASM_PB = 48;  // pairs per shared-memory batch
+// Two CTAs per SM except for c64, whose 16 accumulators take 64 registers.
 template <typename T>
-__global__ void __launch_bounds__(256, sizeof(T) >= 16 ? 1 : 2)
+__global__ void __launch_bounds__(ASM_NT, sizeof(T) >= 16 ? 1 : 2)
     k_cmod_asm(FactorArgs fa, const int4* __restrict__ tasks, const int4* __restrict__ pairs,
                const int8_t* __restrict__ maps, const long long* __restrict__ wb, const int* __restrict__ wl,
                const float* __restrict__ W) {
   using F = Field<T>;
+  __shared__ __align__(16) int8_t smap[ASM_PB][TC_MAP];
+  __shared__ int2 spr[ASM_PB];      // (a, q0)
+  __shared__ long long swb[ASM_PB];
+  __shared__ int swl[ASM_PB];
   if (fa.status[0] != 0) return;
   const int4 tk = tasks[blockIdx.x];
   const int s = tk.x, r0 = (tk.y >> 16) * TC_M, c0 = (tk.y & 0xffff) * TC_N;
   const int ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
   const int rows_here = min(TC_M, nrow - r0), cols_here = min(TC_N, ncol - c0);
-  const int t = threadIdx.x & 127, h = threadIdx.x >> 7;
-  T acc[32];
+  const int tid = threadIdx.x, t = tid & 127, h = tid >> 7;
+  T acc[16];
 #pragma unroll
-  for (int j = 0; j < 32; ++j) acc[j] = F::zero();
-  // no block barrier: every thread reads its own row map entry and its 32
-  // column map entries (two 16-byte loads) straight from the pair's maps
-  for (int u = tk.z; u < tk.w; ++u) {
-    const int8_t* mp = maps + (long long)u * TC_MAP;
-    const int i = mp[t];
-    if (i < 0) continue;
-    const int4 pr = pairs[u];
-    const int a = pr.y, q0 = pr.z;
-    int8_t cm[32];
-    *reinterpret_cast<int4*>(cm) = *reinterpret_cast<const int4*>(mp + TC_M + 32 * h);
-    *reinterpret_cast<int4*>(cm + 16) = *reinterpret_cast<const int4*>(mp + TC_M + 32 * h + 16);
-    // W is column-major: consecutive tile rows read (mostly) consecutive W rows
-    const T* wrow = reinterpret_cast<const T*>(W) + wb[u] + i;
-    const long long ld = wl[u];
+  for (int j = 0; j < 16; ++j) acc[j] = F::zero();
+  static_assert(TC_MAP % 16 == 0, "maps copied as int4");
+  for (int u0 = tk.z; u0 < tk.w; u0 += ASM_PB) {
+    const int nb = min(ASM_PB, tk.w - u0);
+    __syncthreads();  // the previous batch is consumed
+    const int4* src = reinterpret_cast<const int4*>(maps + (long long)u0 * TC_MAP);
+    int4* dstm = reinterpret_cast<int4*>(&smap[0][0]);
+    for (int e = tid; e < nb * (TC_MAP / 16); e += ASM_NT) dstm[e] = src[e];
+    for (int e = tid; e < nb; e += ASM_NT) {
+      const int4 pr = pairs[u0 + e];
+      spr[e] = make_int2(pr.y, pr.z);
+      swb[e] = wb[u0 + e];
+      swl[e] = wl[u0 + e];
+    }
+    __syncthreads();
+    for (int v = 0; v < nb; ++v) {
+      const int i = smap[v][t];
+      if (i < 0) continue;
+      const int2 pr = spr[v];
+      int8_t cm[16];
+      *reinterpret_cast<int4*>(cm) = *reinterpret_cast<const int4*>(&smap[v][TC_M + 16 * h]);
+      // W is column-major: consecutive tile rows read (mostly) consecutive W rows
+      const T* wrow = reinterpret_cast<const T*>(W) + swb[v] + i;
+      const long long ld = swl[v];
+      T w[16];
 #pragma unroll
-    for (int jj = 0; jj < 32; ++jj) {
-      const int j = cm[jj];
-      if (j >= 0 && a + i >= q0 + j) acc[jj] = F::add(acc[jj], wrow[j * ld]);
+      for (int jj = 0; jj < 16; ++jj) {
+        const int j = cm[jj];
+        w[jj] = (j >= 0 && pr.x + i >= pr.y + j) ? wrow[j * ld] : F::zero();
+      }
+#pragma unroll
+      for (int jj = 0; jj < 16; ++jj)
+        if (cm[jj] >= 0 && pr.x + i >= pr.y + cm[jj]) acc[jj] = F::add(acc[jj], w[jj]);
     }
   }
   T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
   if (t < rows_here)
 #pragma unroll
-    for (int jj = 0; jj < 32; ++jj) {
-      const int col = 32 * h + jj;
+    for (int jj = 0; jj < 16; ++jj) {
+      const int col = 16 * h + jj;
       if (col < cols_here && r0 + t >= c0 + col) {
         T* p = panel + (r0 + t) + (long long)(c0 + col) * nrow;
         *p = F::sub(*p, acc[jj]);

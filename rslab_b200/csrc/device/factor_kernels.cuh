@@ -1632,7 +1632,7 @@ __global__ void __launch_bounds__(NT) k_deep(FactorArgs fa, const int4* __restri
 // the same rows of the pw x pw identity (one row per warp, so each step's
 // dependency chain is short).  Task (s, kb, slot, i0).
 // ---------------------------------------------------------------------------
-constexpr int MM_RB = 16;  // identity rows per block-transform CTA (one per warp)
+constexpr int MM_RB = 8;  // identity rows per block-transform CTA (one per warp)
 
 __host__ __device__ constexpr size_t smem_make_m_off_prog(size_t es, int nb) {
   return (((size_t)(MM_RB + 1) * nb * es + 15) & ~size_t(15));

@@ -1188,7 +1188,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
             k_cmod_dmm<T><<<L.ntasks, DM_NT, smem_cmod_dmm_bytes<T>(), ls>>>(
                 fa, H.d_mm_t4 + L.task_off, H.d_mm_wb + L.task_off, H.d_mm_wl + L.task_off, wb);
           else if (L.kind == L_MM_ASM)
-            k_cmod_asm<T><<<L.ntasks, 256, 0, ls>>>(fa, H.d_t4tc + L.task_off, H.d_cpairs_tc, H.d_tcmaps, H.d_asm_wb,
+            k_cmod_asm<T><<<L.ntasks, ASM_NT, 0, ls>>>(fa, H.d_t4tc + L.task_off, H.d_cpairs_tc, H.d_tcmaps, H.d_asm_wb,
                                                     H.d_asm_wl, F.wbuf + (size_t)(L.nb_slot & 1) * H.w_elems * es / 4);
           else
             continue;
@@ -1200,7 +1200,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
                 fa, H.d_mm_t4 + L.task_off, H.d_mm_wb + L.task_off, H.d_mm_wl + L.task_off, F.tmaps,
                 cx ? H.d_kpad_c : H.d_kpad_r, F.wbuf + (L.nb_slot & 1) * wsz);
           else if (L.kind == L_MM_ASM)
-            k_cmod_asm<T><<<L.ntasks, 256, 0, ls>>>(fa, H.d_t4tc + L.task_off, H.d_cpairs_tc, H.d_tcmaps, H.d_asm_wb,
+            k_cmod_asm<T><<<L.ntasks, ASM_NT, 0, ls>>>(fa, H.d_t4tc + L.task_off, H.d_cpairs_tc, H.d_tcmaps, H.d_asm_wb,
                                                     H.d_asm_wl, F.wbuf + (L.nb_slot & 1) * wsz);
           else
             k_split<T><<<L.ntasks, MM_SPLIT_NT, 0, ls>>>(
