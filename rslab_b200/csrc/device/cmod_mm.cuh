@@ -465,16 +465,26 @@ __global__ void __launch_bounds__(ASM_NT, sizeof(T) >= 16 ? 1 : 2)
         if (cm[jj] >= 0 && pr.x + i >= pr.y + cm[jj]) acc[jj] = F::add(acc[jj], w[jj]);
     }
   }
-  T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
-  if (t < rows_here)
+  T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s] + (r0 + t);
+  if (t < rows_here) {
+    // groups of 8: every load of a group before its first store (distinct
+    // targets; one round trip per element would serialise the tile)
 #pragma unroll
-    for (int jj = 0; jj < 16; ++jj) {
-      const int col = 16 * h + jj;
-      if (col < cols_here && r0 + t >= c0 + col) {
-        T* p = panel + (r0 + t) + (long long)(c0 + col) * nrow;
-        *p = F::sub(*p, acc[jj]);
+    for (int j0 = 0; j0 < 16; j0 += 8) {
+      T old[8];
+#pragma unroll
+      for (int jj = 0; jj < 8; ++jj) {
+        const int col = 16 * h + j0 + jj;
+        old[jj] = (col < cols_here && r0 + t >= c0 + col) ? panel[(long long)(c0 + col) * nrow] : F::zero();
+      }
+#pragma unroll
+      for (int jj = 0; jj < 8; ++jj) {
+        const int col = 16 * h + j0 + jj;
+        if (col < cols_here && r0 + t >= c0 + col)
+          panel[(long long)(c0 + col) * nrow] = F::sub(old[jj], acc[j0 + jj]);
       }
     }
+  }
 }
 
 }  // namespace rsd

@@ -395,16 +395,31 @@ __device__ __forceinline__ void tc_tile_pipeline(const FactorArgs& fa, const Src
       if (trow < rows_here) {
         const int gr = rbase + r0 + trow;
         float* pf = reinterpret_cast<float*>(reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s]);
+        // groups of 8: every load of a group before its first store (the
+        // targets are distinct; one load-store round trip per element would
+        // serialise the tile)
 #pragma unroll
-        for (int jj = 0; jj < NC; ++jj) {
-          const int colj = cg * NC + jj;
-          const int col = Field<T>::complex ? (colj & (TC_N - 1)) : colj;
-          const int comp = Field<T>::complex ? (colj >> 6) : 0;
-          const int gc = cbase + c0 + col;
-          if (col < cols_here && gr >= gc) {
+        for (int j0 = 0; j0 < NC; j0 += 8) {
+          float old[8];
+#pragma unroll
+          for (int jj = 0; jj < 8; ++jj) {
+            const int colj = cg * NC + j0 + jj;
+            const int col = Field<T>::complex ? (colj & (TC_N - 1)) : colj;
+            const int comp = Field<T>::complex ? (colj >> 6) : 0;
+            const int gc = cbase + c0 + col;
             const long long e = gr + (long long)gc * nrow;
-            float* p = Field<T>::complex ? pf + 2 * e + comp : pf + e;
-            *p -= acc[jj];
+            old[jj] = (col < cols_here && gr >= gc) ? (Field<T>::complex ? pf[2 * e + comp] : pf[e]) : 0.0f;
+          }
+#pragma unroll
+          for (int jj = 0; jj < 8; ++jj) {
+            const int colj = cg * NC + j0 + jj;
+            const int col = Field<T>::complex ? (colj & (TC_N - 1)) : colj;
+            const int comp = Field<T>::complex ? (colj >> 6) : 0;
+            const int gc = cbase + c0 + col;
+            if (col < cols_here && gr >= gc) {
+              const long long e = gr + (long long)gc * nrow;
+              (Field<T>::complex ? pf[2 * e + comp] : pf[e]) = old[jj] - acc[j0 + jj];
+            }
           }
         }
       }
