@@ -460,18 +460,24 @@ __global__ void __launch_bounds__(TPB) k_schur(FactorArgs fa, const int4* __rest
                   reinterpret_cast<const T*>(fa.d) + first + kb, reinterpret_cast<const T*>(fa.dsub) + first + kb,
                   fa.kind + first + kb, As, Bs);
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  // every load before the first store (distinct targets)
+  T old[4][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    int rr = r0 + ty + 16 * i;
-    if (ty + 16 * i >= rows_here) continue;
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      int cc = c0 + tx + 16 * j;
-      if (tx + 16 * j >= cols_here || rr < cc) continue;
-      T* p = panel + (ke + rr) + (long long)(ke + cc) * nrow;
-      *p = F::sub(*p, acc[i][j]);
+      const int rr = r0 + ty + 16 * i, cc = c0 + tx + 16 * j;
+      const bool in = ty + 16 * i < rows_here && tx + 16 * j < cols_here && rr >= cc;
+      old[i][j] = in ? panel[(ke + rr) + (long long)(ke + cc) * nrow] : F::zero();
     }
-  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int rr = r0 + ty + 16 * i, cc = c0 + tx + 16 * j;
+      if (ty + 16 * i < rows_here && tx + 16 * j < cols_here && rr >= cc)
+        panel[(ke + rr) + (long long)(ke + cc) * nrow] = F::sub(old[i][j], acc[i][j]);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1235,7 +1241,7 @@ template <typename T>
 __host__ __device__ constexpr size_t smem_getf2_ll_bytes(int nb) {
   const size_t steps = (size_t)nb * (nb + 1) * sizeof(T)  // A and G, packed lower
                        + (size_t)2 * nb * sizeof(T)       // the formed columns
-                       + (size_t)4 * 128 * sizeof(T)      // GEMV partial sums
+                       + (size_t)(4 + 6) * 128 * sizeof(T)  // GEMV and look-ahead partial sums
                        + 16 + 32 * 8 + 32 * 4 + 16 * 4 + 4 * (size_t)nb * 4;
   // the fused deep-row replay reuses the same memory after the write-back
   const size_t replay =
@@ -1271,9 +1277,9 @@ __global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* _
   T* v1 = Gs + npk;                       // formed column k
   T* v2 = v1 + pw;                        // formed candidate column
   T* red = v2 + pw;                       // 4 x 128 partial sums
-  double* red_v = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(red + 4 * 128) + 15) & ~uintptr_t(15));
+  double* red_v = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(red + 10 * 128) + 15) & ~uintptr_t(15));
   int* red_i = reinterpret_cast<int*>(red_v + 32);
-  int* ctl = red_i + 32;  // [1] scratch [2] nswaps [3] error [4] step k [5] kstep [6] kp [7] extra column
+  int* ctl = red_i + 32;  // [1] scratch [2] nswaps [3] error [4..15] the steps' control words
   int* lp_s = ctl + 16;
   int* swp_p = lp_s + nb;
   int* swp_q = swp_p + nb;
@@ -1295,12 +1301,7 @@ __global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* _
     swaps[e] = -1;
   }
   for (int e = tid; e < pw * nb; e += NT) snap[(e / nb) * nb + (e % nb)] = F::zero();
-  if (tid == 0) {
-    ctl[2] = 0;
-    ctl[3] = 0;
-    ctl[4] = 0;
-    ctl[7] = -1;
-  }
+  if (tid < 16) ctl[tid] = 0;  // [2] nswaps, [3] error, [4..15] the steps' control words
   __syncthreads();
   for (int i = tid; i < pw; i += NT) lp_s[i] = lpermG[kb + i];
   __syncthreads();
@@ -1489,15 +1490,59 @@ __global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* _
 
   const bool team = tid < 128;
   const double a2 = alpha * alpha;
-  for (int k = 0; k < pw;) {
-    gemv(k, k);
-    __syncthreads();
+  // Look-ahead: while the team finishes step k, warps 4-15 form the partial
+  // sums of column k + 1 over the pivoted columns p < k (three groups of 128
+  // rows).  When step k is a 1x1 pivot without interchange, step k + 1 uses
+  // them (adding its one missing term, p = k) and skips its GEMV and block
+  // barrier.  Control words are double-buffered by iteration parity: with
+  // the GEMV barrier skipped, a thread may still read iteration i's words
+  // while the team writes iteration i + 1's.
+  T* const rs0 = red + 4 * 128;  // two look-ahead buffers of 3 x 128 partial sums, by iteration parity
+  auto spec_gemv = [&](int k, T* out) {
+    const int u = tid - 128, rr = u & 127, g = u >> 7, c = k + 1, i = c + rr;
+    if (i < pw) {
+      T acc0 = F::zero(), acc1 = F::zero();
+      int p = g;
+      for (; p + 3 < k; p += 6) {
+        const int cp0 = p * pw - (p * (p + 1)) / 2, cp1 = (p + 3) * pw - ((p + 3) * (p + 4)) / 2;
+        acc0 = F::fma_(Gs[cp0 + i], A[cp0 + c], acc0);
+        acc1 = F::fma_(Gs[cp1 + i], A[cp1 + c], acc1);
+      }
+      if (p < k) {
+        const int cp = p * pw - (p * (p + 1)) / 2;
+        acc0 = F::fma_(Gs[cp + i], A[cp + c], acc0);
+      }
+      out[g * 128 + rr] = F::add(acc0, acc1);
+    }
+  };
+  // team thread r, look-ahead case: v[k + r] = A0(k + r, k) - the three
+  // partials - G(k + r, k - 1) L(k, k - 1)
+  auto form_row_la = [&](int k, const T* part, int r) {
+    const int i = k + r;
+    if (i < pw) {
+      const T a = A[pk(i, k, pw)];
+      const T u = F::add(F::add(part[r], part[128 + r]), part[256 + r]);
+      const int cl = (k - 1) * pw - ((k - 1) * k) / 2;  // packed start of column k - 1
+      v1[i] = F::sub(F::sub(a, u), F::mul(Gs[cl + i], A[cl + k]));
+    }
+  };
+  for (int k = 0, it = 0; k < pw; ++it) {
+    int* cc = ctl + 4 + 6 * (it & 1);         // this iteration: next k, kstep, kp, extra, error
+    int* cn = ctl + 4 + 6 * ((it + 1) & 1);   // cn[5]: the next iteration may use the look-ahead
+    const bool la = cc[5] != 0;
+    if (!la) {
+      gemv(k, k);
+      __syncthreads();
+    }
     if (team) {
       // column k, and per team warp the arg-max of the squared moduli below
       // the diagonal (the BK tests run on squares: no square roots or
       // divisions on the decision path)
       const int r = tid;
-      form_row(k, k, v1, r);
+      if (la)
+        form_row_la(k, rs0 + 384 * ((it + 1) & 1), r);
+      else
+        form_row(k, k, v1, r);
       double m2 = -1.0;
       int idx = INT_MAX;
       if (r >= 1 && k + r < pw) {
@@ -1539,24 +1584,28 @@ __global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* _
       }
       if (r == 0) {
         if (err) ctl[3] = 1;
-        ctl[4] = k + 1;
-        ctl[5] = kstep;
-        ctl[6] = kp;
-        ctl[7] = err ? -1 : extra;
+        cc[0] = k + 1;
+        cc[1] = kstep;
+        cc[2] = kp;
+        cc[3] = err ? -1 : extra;
+        cc[4] = err ? 1 : 0;
+        cn[5] = (!err && extra < 0 && k + 1 < pw) ? 1 : 0;
         red_v[5] = akk2;
         red_v[6] = col2;
       }
+    } else if (k + 1 < pw) {
+      spec_gemv(k, rs0 + 384 * (it & 1));
     }
     __syncthreads();
-    if (ctl[3]) break;
-    const int extra = ctl[7];
+    if (cc[4]) break;
+    const int extra = cc[3];
     if (extra >= 0) {
       gemv(k, extra);
       __syncthreads();
       if (team) {
         const int r = tid;
         form_row(k, extra, v2, r);
-        int kstep = ctl[5], kp = ctl[6];
+        int kstep = cc[1], kp = cc[2];
         if (!reuse) {
           // the row maximum of the candidate row: its column over every row
           // of the unpivoted part but itself
@@ -1589,13 +1638,14 @@ __global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* _
         const bool err = finish_rows(k, kstep, kp, r);
         if (r == 0) {
           if (err) ctl[3] = 1;
-          ctl[4] = k + kstep;
+          cc[0] = k + kstep;
+          cc[4] = err ? 1 : 0;
         }
       }
       __syncthreads();
-      if (ctl[3]) break;
+      if (cc[4]) break;
     }
-    k = ctl[4];
+    k = cc[0];
   }
   getf2_finish<T, NT>(fa, s, kb, pw, nb, nrow, ke, fuse, panel, A, lp_s, lpermG, ctl, swp_p, swp_q, supp,
                       reinterpret_cast<int*>(v1), kindG, dG, dsG, snap, swaps, nperturbed, smem_raw);
