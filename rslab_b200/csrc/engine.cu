@@ -1868,19 +1868,35 @@ int rslab_analyze_tuned(int64_t n, const int64_t* col_ptr, const int64_t* row_id
     check_lower_input(n, col_ptr, row_idx);
     rslab_analyze_settings st;
     rslab_default_analyze_settings(&st);
-    rslab::Symbolic S = rslab::analyze(n, col_ptr, row_idx, analyze_options(st));
-    if (n >= RSLAB_ND_BAKEOFF_MIN_N) {
-      const rslab::MemoryEstimate est = rslab::estimate_memory(S, value_bytes);
-      if (est.factor_flops >= (uint64_t)RSLAB_ND_BAKEOFF_MIN_FLOPS) {
-        rslab_analyze_settings st_nd = st;
-        st_nd.ordering = RSLAB_ORDER_METIS_ND;
-        bool nd_ok = true;
-        rslab::Symbolic S_nd;
+    rslab_analyze_settings st_nd = st;
+    st_nd.ordering = RSLAB_ORDER_METIS_ND;
+    // The ND candidate's analysis runs on a second host thread while the
+    // default analysis runs here (the bake-off reads both); it is discarded
+    // when the default pattern is below the flop threshold.
+    const bool try_nd = n >= RSLAB_ND_BAKEOFF_MIN_N;
+    rslab::Symbolic S_nd;
+    bool nd_ok = false;  // the ND analysis failed: keep the first pick
+    std::thread nd_thread;
+    if (try_nd)
+      nd_thread = std::thread([&] {
         try {
           S_nd = rslab::analyze(n, col_ptr, row_idx, analyze_options(st_nd));
-        } catch (const std::exception&) {
-          nd_ok = false;  // the ND analysis failed: keep the first pick
+          nd_ok = true;
+        } catch (...) {
+          nd_ok = false;
         }
+      });
+    struct Joiner {
+      std::thread& t;
+      ~Joiner() {
+        if (t.joinable()) t.join();
+      }
+    } joiner{nd_thread};
+    rslab::Symbolic S = rslab::analyze(n, col_ptr, row_idx, analyze_options(st));
+    if (nd_thread.joinable()) nd_thread.join();
+    if (try_nd) {
+      const rslab::MemoryEstimate est = rslab::estimate_memory(S, value_bytes);
+      if (est.factor_flops >= (uint64_t)RSLAB_ND_BAKEOFF_MIN_FLOPS) {
         if (nd_ok) {
           const rslab::MemoryEstimate est_nd = rslab::estimate_memory(S_nd, value_bytes);
           const bool flops_win = (double)est_nd.factor_flops < (double)est.factor_flops * RSLAB_ND_BAKEOFF_ADOPT_RATIO;
