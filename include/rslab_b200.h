@@ -103,7 +103,23 @@ typedef struct {
   int32_t overlap;             /* schedule: run the Schur update beyond the next block and the next
                                 * level's early descendant updates on side streams (1, default) or
                                 * everything in order on one stream (0); the factor is the same */
+  int32_t method;              /* RSLAB_METHOD_*: SolverSettings::method (FactorMethod,
+                                * multifrontal_ldlt.rs:283) */
 } rslab_factor_settings;
+
+/* Numeric schedule.  RSLAB_METHOD_LEFT_LOOKING (default): every supernode
+ * gathers its descendants' updates (cmod, per the schur_engine).
+ * RSLAB_METHOD_MULTIFRONTAL: every supernode's front is its panel plus a
+ * contribution block; the children's contribution blocks are extend-added
+ * into it (in child order, deterministic), the panel is factored with the same
+ * Bunch-Kaufman kernels, and the contribution block becomes CB - L21 D L21^T
+ * for the parent (factor_front + extend-add, multifrontal_ldlt.rs:901,
+ * 1494-1510).  Same pivoting; the sums run in another order, so the factors
+ * agree with the left-looking ones to rounding.  It runs on the CUDA cores
+ * (schur_engine is ignored) and holds every contribution block (sum of
+ * (nrow - ncol)^2 scalars) for the factor's lifetime. */
+#define RSLAB_METHOD_LEFT_LOOKING 0
+#define RSLAB_METHOD_MULTIFRONTAL 1
 
 /* Descendant (cmod) updates.  RSLAB_SCHUR_TENSOR: per (updater, target) pair
  * a dense product over the updater's contiguous rows, in GEMM tiles on the
@@ -148,6 +164,7 @@ typedef struct {
   int32_t multiprocessors;     /* SMs of the handle's device (the reference's Diagnostics::threads
                                 * counts CPU workers) */
   int32_t schur_engine;        /* RSLAB_SCHUR_TENSOR or RSLAB_SCHUR_FMA: the engine AUTO resolved to */
+  int32_t method;              /* RSLAB_METHOD_* */
 } rslab_factor_info_t;
 
 typedef struct {
@@ -265,11 +282,12 @@ int rslab_solve_profile(rslab_fac_handle* fac, int64_t nrhs, double* kind_ms, in
 /* Per-launch rows of the handle's last factor/solve profile: launch kind
  * (0 cmod, 1 getf2, 2 deep replay, 3 panel Schur, 4 forward diagonal,
  * 5 forward push, 6 backward dots, 7 backward diagonal, 8-11 see below, 12
- * forward gather, 13 unused, 14 G = L21 D, 15 diagonal-block
- * inverses, 16 backward partial-sum reduction, 17 tensor-core panel Schur,
- * 18/19 forward/backward block-chain solve, 20 backward gather, 21 deep rows
- * as a product with the block transform, 22 block transform, 23 forward push
- * partial-sum reduction, -1 other), grid
+ * forward gather, 13 multifrontal extend-add, 14 G = L21 D, 15
+ * diagonal-block inverses, 16 backward partial-sum reduction, 17 tensor-core
+ * panel Schur, 18/19 forward/backward block-chain solve, 20 backward gather,
+ * 21 deep rows as a product with the block transform, 22 block transform, 23
+ * forward push partial-sum reduction, 24 multifrontal contribution block,
+ * -1 other), grid
  * size and device ms.  *count = rows available; at most cap are written.
  * A measurement aid with no reference counterpart.  Kinds 8-11 are the
  * tensor-core cmod's GEMM tiles, its assembly and the real / complex operand

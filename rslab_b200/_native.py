@@ -15,6 +15,7 @@ ORDER_AMD, ORDER_METIS_ND, ORDER_NATURAL, ORDER_GIVEN = 0, 1, 2, 3
 PIVOT_FAIL, PIVOT_PERTURB, PIVOT_FORCE_ACCEPT = 0, 1, 2
 SCALING_ONEPASS, SCALING_IDENTITY = 0, 1
 SCHUR_TENSOR, SCHUR_FMA, SCHUR_AUTO = 0, 1, 2
+METHOD_LEFT_LOOKING, METHOD_MULTIFRONTAL = 0, 1
 TIER_FP64, TIER_FP32, TIER_TF32X3 = 0, 1, 2
 TIER_MLP_PARAMS = 4931
 
@@ -47,6 +48,7 @@ class FactorSettings(C.Structure):
         ("schur_engine", C.c_int32),
         ("drop_tol", C.c_double),
         ("overlap", C.c_int32),
+        ("method", C.c_int32),
     ]
 
 
@@ -70,7 +72,7 @@ class FactorInfo(C.Structure):
         ("inertia_pos", C.c_int64), ("inertia_neg", C.c_int64), ("inertia_zero", C.c_int64),
         ("n_perturbed", C.c_int64), ("factor_ms", C.c_double), ("solve_ms", C.c_double),
         ("dtype", C.c_int32), ("dtype_hi", C.c_int32), ("multiprocessors", C.c_int32),
-        ("schur_engine", C.c_int32),
+        ("schur_engine", C.c_int32), ("method", C.c_int32),
     ]
 
 

@@ -54,6 +54,10 @@ struct FactorArgs {
   const long long* goff;
   const double* floor_dev;  // non-null: static-pivot floor computed on the device (force-accept)
   int deep_mm;              // tall panels: getf2 forms the block transform M, k_deep_mm applies it
+  // Multifrontal variant: the contribution blocks of the fronts, supernode
+  // s's (nrow - ncol)^2 column-major block at cb_off[s].
+  void* cbpool;
+  const long long* cb_off;
   // Pivot record (e-indexed, block-local): kp for a 1x1 step at e, -(kp + 1)
   // for a 2x2 step starting at e.  Written by every factor that searches; when
   // *pivot_reuse is set, getf2 replays the recorded steps instead of searching
@@ -477,6 +481,89 @@ __global__ void __launch_bounds__(TPB) k_schur(FactorArgs fa, const int4* __rest
       const int rr = r0 + ty + 16 * i, cc = c0 + tx + 16 * j;
       if (ty + 16 * i < rows_here && tx + 16 * j < cols_here && rr >= cc)
         panel[(ke + rr) + (long long)(ke + cc) * nrow] = F::sub(old[i][j], acc[i][j]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Multifrontal variant (factor_front + extend-add, multifrontal_ldlt.rs:901,
+// 1494-1510).  A front of supernode s is its panel (nrow x ncol, the
+// fully-summed columns) plus its contribution block CB_s (m x m, m = nrow -
+// ncol, the trailing rows and columns, lower part).
+//
+// k_extend_add: task (s, ct, pair_begin, pair_end): front columns [64 ct,
+// 64 ct + 64) of s; pair (c, ja, jb): child c's contribution-block columns
+// [ja, jb) land there.  Children are added in order (a block barrier between
+// them), each entry (i, j), i >= j, of a child's block into the front entry
+// (map[i], map[j]) (the child's rows' positions in the front): the panel
+// when map[j] < ncol, CB_s otherwise.  Deterministic; no atomics.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_extend_add(FactorArgs fa, const int4* __restrict__ tasks,
+                                                    const int4* __restrict__ pairs, const int* __restrict__ emap,
+                                                    const long long* __restrict__ emoff) {
+  using F = Field<T>;
+  if (fa.status[0] != 0) return;
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s], ms = nrow - ncol;
+  T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
+  T* cbs = reinterpret_cast<T*>(fa.cbpool) + fa.cb_off[s];
+  for (int u = tk.z; u < tk.w; ++u) {
+    const int4 pr = pairs[u];
+    const int c = pr.x, mc = fa.sn_nrow[c] - fa.sn_ncol[c];
+    const T* cbc = reinterpret_cast<const T*>(fa.cbpool) + fa.cb_off[c];
+    const int* map = emap + emoff[c];
+    for (int j = pr.y; j < pr.z; ++j) {
+      const int lj = map[j];
+      for (int i = j + (int)threadIdx.x; i < mc; i += 256) {
+        const int li = map[i];
+        const T v = cbc[i + (long long)j * mc];
+        T* t = lj < ncol ? panel + li + (long long)lj * nrow : cbs + (li - ncol) + (long long)(lj - ncol) * ms;
+        *t = F::add(*t, v);
+      }
+    }
+    __syncthreads();  // the next child's additions follow this one's
+  }
+}
+
+// k_front_cb: task (s, r0, c0, 0): CB_s rows [r0, r0 + 64) x columns [c0,
+// c0 + 64), r0 >= c0, minus (L21 D L21^T) over all of s's columns (the
+// tile engine with D on the row operand, as the in-panel Schur update), on
+// its lower part.
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_front_cb(FactorArgs fa, const int4* __restrict__ tasks) {
+  using F = Field<T>;
+  if (fa.status[0] != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* As = reinterpret_cast<T*>(smem_raw);
+  T* Bs = As + KChunk<T>::v * TILE;
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, r0 = tk.y, c0 = tk.z;
+  const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s], m = nrow - ncol;
+  const T* L21 = reinterpret_cast<const T*>(fa.panel) + fa.sn_poff[s] + ncol;
+  T* cb = reinterpret_cast<T*>(fa.cbpool) + fa.cb_off[s];
+  const int rows_here = min(TILE, m - r0), cols_here = min(TILE, m - c0);
+  T acc[4][4];
+  tile_product<T, true>(acc, L21 + r0, nrow, rows_here, L21 + c0, nrow, cols_here, ncol,
+                        reinterpret_cast<const T*>(fa.d) + first, reinterpret_cast<const T*>(fa.dsub) + first,
+                        fa.kind + first, As, Bs);
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  // every load before the first store (distinct targets)
+  T old[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int rr = r0 + ty + 16 * i, cc = c0 + tx + 16 * j;
+      const bool in = ty + 16 * i < rows_here && tx + 16 * j < cols_here && rr >= cc;
+      old[i][j] = in ? cb[rr + (long long)cc * m] : F::zero();
+    }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int rr = r0 + ty + 16 * i, cc = c0 + tx + 16 * j;
+      if (ty + 16 * i < rows_here && tx + 16 * j < cols_here && rr >= cc)
+        cb[rr + (long long)cc * m] = F::sub(old[i][j], acc[i][j]);
     }
 }
 

@@ -107,9 +107,9 @@ size_t elem_size(int dtype) {
 enum LaunchKind {
   L_CMOD, L_GETF2, L_DEEP, L_SCHUR,
   L_FWD_DIAG, L_FWD_PUSH, L_BWD_OFF, L_BWD,
-  L_MM_GEMM, L_MM_ASM, L_SPLIT_R, L_SPLIT_C, L_FWD_GATHER, L_UNUSED13, L_MAKE_G, L_DIAG_INV,
+  L_MM_GEMM, L_MM_ASM, L_SPLIT_R, L_SPLIT_C, L_FWD_GATHER, L_EXT_ADD, L_MAKE_G, L_DIAG_INV,
   L_BWD_OFF_RED, L_SCHUR_TC, L_FWD_CHAIN, L_BWD_CHAIN, L_BWD_GATHER, L_DEEP_MM, L_MAKE_M,
-  L_FWD_PUSH_RED,
+  L_FWD_PUSH_RED, L_FRONT_CB,
   L_JOIN_CM  // no kernel: the level's early cmod updates must be complete from here on
 };
 // Inverse diagonal blocks of a supernode with ncol columns: TB x TB per
@@ -154,6 +154,14 @@ struct rslab_sym_handle {
   // full symmetric CSR of A for SpMV
   std::vector<long long> sp_rp, sp_vmap;
   std::vector<int> sp_ci;
+  // multifrontal variant: each supernode's contribution block (m x m
+  // column-major, m = nrow - ncol) at cb_off[s]; per child its off-diagonal
+  // rows' positions in the parent's front (ea_map from ea_moff[c]); extend-add
+  // pairs (child, column range [ja, jb)) per (parent, 64-column front tile)
+  std::vector<long long> cb_off, ea_moff;
+  long long cb_elems = 0;
+  std::vector<int> ea_map;
+  std::vector<int4> ea_pairs;
   // plan
   std::vector<int4> t4;
   std::vector<int4> cpairs;   // cmod (k, a, q0, nr << 16 | nc) per tile, in update order
@@ -218,6 +226,9 @@ struct rslab_sym_handle {
   long long *d_soff_a_r = nullptr, *d_soff_b_r = nullptr, *d_soff_a_c = nullptr, *d_soff_b_c = nullptr;
   int4 *d_sp_r = nullptr, *d_sp_c = nullptr;
   long long* d_goff = nullptr;
+  long long *d_cb_off = nullptr, *d_ea_moff = nullptr;
+  int* d_ea_map = nullptr;
+  int4* d_ea_pairs = nullptr;
   long long* d_linv_off = nullptr;
   int* d_t1 = nullptr;
   int2* d_t2 = nullptr;
@@ -290,6 +301,10 @@ struct rslab_sym_handle {
     d_sp_r = up(sp_r, st);
     d_sp_c = up(sp_c, st);
     d_goff = up(goff, st);
+    d_cb_off = up(cb_off, st);
+    d_ea_moff = up(ea_moff, st);
+    d_ea_map = up(ea_map, st);
+    d_ea_pairs = up(ea_pairs, st);
     d_linv_off = up(linv_off, st);
     d_t1 = up(t1, st);
     d_t2 = up(t2, st);
@@ -466,6 +481,40 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
     H.goff[s] = H.g_elems;
     H.g_elems += (long long)(H.nrow[s] - S.sn[s].ncol) * S.sn[s].ncol;
   }
+  // multifrontal variant (factor_front + extend-add, multifrontal_ldlt.rs:
+  // 901, 1426-1530): contribution blocks, and for every child the position
+  // of each of its off-diagonal rows in its parent's front (the parent's row
+  // structure: own columns, then its off-diagonal rows)
+  H.cb_off.assign(ns, 0);
+  H.cb_elems = 0;
+  for (int s = 0; s < ns; ++s) {
+    const long long m = H.nrow[s] - S.sn[s].ncol;
+    H.cb_off[s] = H.cb_elems;
+    H.cb_elems += m * m;
+  }
+  H.ea_moff.assign(ns, 0);
+  H.ea_map.clear();
+  {
+    std::vector<int> par(ns, -1);
+    for (int s = 0; s < ns; ++s)
+      for (int64_t c : S.sn[s].children) par[c] = s;
+    for (int c = 0; c < ns; ++c) {
+      H.ea_moff[c] = (long long)H.ea_map.size();
+      const int p = par[c];
+      const int64_t m = H.nrow[c] - S.sn[c].ncol;
+      if (p < 0 || m <= 0) continue;
+      const int64_t* rc = S.rs.data() + S.rs_ptr[c] + S.sn[c].ncol;
+      const int64_t* rp = S.rs.data() + S.rs_ptr[p];
+      const int np = H.nrow[p];
+      int64_t pos = 0;
+      for (int64_t i = 0; i < m; ++i) {
+        while (pos < np && rp[pos] < rc[i]) ++pos;
+        if (pos >= np || rp[pos] != rc[i])
+          throw RslabError(Status::InvalidInput, "contribution row outside the parent front");
+        H.ea_map.push_back((int)pos);
+      }
+    }
+  }
   // updater-space tensor-core cmod: the W block of update-list entry u
   // (k -> s) is k's rows [p0, nok) x its rows [p0, p1), column-major, in the
   // buffer of s's level; split pools per updater, K' padded to 32-wide chunks
@@ -628,6 +677,31 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       La.ntasks = (int)(H.t4tc.size() - La.task_off);
       if (La.ntasks) H.fplan.push_back(La);
     }
+    // multifrontal variant: the children's contribution blocks into this
+    // level's fronts, per (parent, 64-column front tile), children in order
+    {
+      Launch Le{L_EXT_ADD, (long long)H.t4.size(), 0, 0};
+      for (int64_t s : lvl) {
+        const auto& ch = S.sn[s].children;
+        if (ch.empty()) continue;
+        const int nt = (H.nrow[s] + 63) / 64;
+        for (int ct = 0; ct < nt; ++ct) {
+          const int pb = (int)H.ea_pairs.size();
+          for (int64_t c : ch) {
+            const int64_t m = H.nrow[c] - S.sn[c].ncol;
+            if (m <= 0) continue;
+            const int* mp = H.ea_map.data() + H.ea_moff[c];
+            // the child columns j whose front column mp[j] lies in this tile
+            const int ja = (int)(std::lower_bound(mp, mp + m, 64 * ct) - mp);
+            const int jb = (int)(std::lower_bound(mp, mp + m, 64 * ct + 64) - mp);
+            if (jb > ja) H.ea_pairs.push_back(make_int4((int)c, ja, jb, 0));
+          }
+          if ((int)H.ea_pairs.size() > pb) H.t4.push_back(make_int4((int)s, ct, pb, (int)H.ea_pairs.size()));
+        }
+      }
+      Le.ntasks = (int)(H.t4.size() - Le.task_off);
+      if (Le.ntasks) H.fplan.push_back(Le);
+    }
     int maxblocks = 0;
     for (int64_t s : lvl) maxblocks = std::max(maxblocks, (int)((S.sn[s].ncol + nb_of(s) - 1) / nb_of(s)));
     for (int b = 0; b < maxblocks; ++b) {
@@ -696,6 +770,18 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         H.t4.insert(H.t4.end(), schur_tc_r.begin(), schur_tc_r.end());
         H.fplan.push_back(Ct);
       }
+    }
+    // multifrontal variant: each front's contribution block, CB -= L21 D L21^T
+    // over all its columns, in 64 x 64 tiles of its lower triangle
+    {
+      Launch Lf{L_FRONT_CB, (long long)H.t4.size(), 0, 0};
+      for (int64_t s : lvl) {
+        const int m = H.nrow[s] - (int)S.sn[s].ncol;
+        for (int c0 = 0; c0 < m; c0 += TILE)
+          for (int r0 = c0; r0 < m; r0 += TILE) H.t4.push_back(make_int4((int)s, r0, c0, 0));
+      }
+      Lf.ntasks = (int)(H.t4.size() - Lf.task_off);
+      if (Lf.ntasks) H.fplan.push_back(Lf);
     }
     // G_k = L21_k D_k of this level's updaters, for the CUDA-core cmod of
     // their ancestors (32-column tasks), and the tensor-core engine's split
@@ -911,6 +997,7 @@ struct KernelSetup {
       CK(cudaFuncSetAttribute(k_cmod_dmm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)smem_cmod_dmm_bytes<T>()));
     CK(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
+    CK(cudaFuncSetAttribute(k_front_cb<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
     CK(cudaFuncSetAttribute(k_getf2<T, GETF2_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)smem_getf2(es, 128)));
     if constexpr (TensorCmod<T>::ok)
@@ -962,6 +1049,7 @@ struct rslab_fac_handle {
   void* scratch = nullptr;
   long long scratch_stride = 0;
   void* gpool = nullptr;  // G_k = L21_k D_k of every updater (read by both cmod engines)
+  void* cbpool = nullptr; // multifrontal variant: every supernode's contribution block
   void* linv = nullptr;   // inverse diagonal blocks of the wide supernodes
   // updater-space tensor-core cmod (f32 / c32, tensor engine): split operand
   // pools (tf32 hi / lo of L21 and of G; complex fields also the [hi | lo]
@@ -1056,6 +1144,8 @@ FactorArgs make_fargs(rslab_fac_handle& F) {
   a.floor_dev = F.floor_dev;
   a.pivrec = F.pivrec;
   a.pivot_reuse = F.pivot_reuse;
+  a.cbpool = F.cbpool;
+  a.cb_off = H.d_cb_off;
   if (F.set.on_zero_pivot == RSLAB_PIVOT_FORCE_ACCEPT) a.perturb_floor = 0.0;
   return a;
 }
@@ -1120,6 +1210,9 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
   const bool mm = F.set.schur_engine == RSLAB_SCHUR_TENSOR;
   const bool use_tc = TensorCmod<T>::ok && mm;
   fa.deep_mm = use_tc ? 1 : 0;
+  // multifrontal variant: contribution blocks and extend-add instead of cmod
+  const bool mf = F.set.method == RSLAB_METHOD_MULTIFRONTAL;
+  if (mf) CK(cudaMemsetAsync(F.cbpool, 0, (size_t)std::max(H.cb_elems, 1LL) * es, st));
   if (F.floor_dev) {
     CK(cudaMemsetAsync(F.amax_dev, 0, sizeof(unsigned long long), st));
     k_panel_absmax<T><<<(unsigned)std::min<long long>(grid1(H.panel_elems), 148LL * 8), 256, 0, st>>>(
@@ -1134,11 +1227,12 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
   bool side_pending = false;
   auto runs = [&](const Launch& L) {
     switch (L.kind) {
-      case L_CMOD: return !mm;
-      case L_MM_GEMM: case L_MM_ASM: return mm;
-      case L_SPLIT_R: return use_tc && !Field<T>::complex;
-      case L_SPLIT_C: return use_tc && Field<T>::complex;
-      case L_MAKE_G: return !use_tc;  // G_k of the CUDA-core cmod and of the DMMA tiles
+      case L_CMOD: return !mm && !mf;
+      case L_MM_GEMM: case L_MM_ASM: return mm && !mf;
+      case L_SPLIT_R: return use_tc && !mf && !Field<T>::complex;
+      case L_SPLIT_C: return use_tc && !mf && Field<T>::complex;
+      case L_MAKE_G: return !use_tc && !mf;  // G_k of the CUDA-core cmod and of the DMMA tiles
+      case L_EXT_ADD: case L_FRONT_CB: return mf;
       case L_DEEP: return !fa.deep_mm;
       case L_MAKE_M: case L_DEEP_MM: return fa.deep_mm != 0;
       case L_SCHUR: return !use_tc;
@@ -1256,6 +1350,12 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         if (use_tc) continue;
         k_schur<T><<<L.ntasks, TPB, smem_schur(es), ls>>>(fa, H.d_t4 + L.task_off, nb_small, nb_big);
         break;
+      case L_EXT_ADD:
+        k_extend_add<T><<<L.ntasks, 256, 0, ls>>>(fa, H.d_t4 + L.task_off, H.d_ea_pairs, H.d_ea_map, H.d_ea_moff);
+        break;
+      case L_FRONT_CB:
+        k_front_cb<T><<<L.ntasks, TPB, smem_schur(es), ls>>>(fa, H.d_t4 + L.task_off);
+        break;
       case L_SCHUR_TC:
         if constexpr (TensorCmod<T>::ok) {
           if (!use_tc) continue;
@@ -1267,8 +1367,8 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
     }
     if (prof)
       prof->mark(st,
-                 (L.kind == L_CMOD || L.kind == L_MAKE_G || L.kind == L_MM_GEMM ||
-                  L.kind == L_MM_ASM || L.kind == L_SPLIT_R || L.kind == L_SPLIT_C) ? 1
+                 (L.kind == L_CMOD || L.kind == L_MAKE_G || L.kind == L_MM_GEMM || L.kind == L_MM_ASM ||
+                  L.kind == L_SPLIT_R || L.kind == L_SPLIT_C || L.kind == L_EXT_ADD || L.kind == L_FRONT_CB) ? 1
                  : (L.kind == L_DIAG_INV || L.kind == L_SCHUR_TC)             ? 4
                  : L.kind == L_GETF2                                           ? 2
                  : (L.kind == L_DEEP || L.kind == L_DEEP_MM || L.kind == L_MAKE_M) ? 3
@@ -1767,6 +1867,7 @@ void rslab_default_factor_settings(rslab_factor_settings* s) {
   s->use_graph = 1;
   s->stream = nullptr;
   s->schur_engine = RSLAB_SCHUR_AUTO;
+  s->method = RSLAB_METHOD_LEFT_LOOKING;
   s->drop_tol = 0.0;
   s->overlap = 1;
 }
@@ -2157,6 +2258,10 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
       F->set = *settings;
     else
       rslab_default_factor_settings(&F->set);
+    if (F->set.method != RSLAB_METHOD_LEFT_LOOKING && F->set.method != RSLAB_METHOD_MULTIFRONTAL)
+      throw RslabError(Status::InvalidInput, "method must be RSLAB_METHOD_LEFT_LOOKING or _MULTIFRONTAL");
+    // the multifrontal variant runs on the CUDA-core kernels
+    if (F->set.method == RSLAB_METHOD_MULTIFRONTAL) F->set.schur_engine = RSLAB_SCHUR_FMA;
     if (F->set.schur_engine == RSLAB_SCHUR_AUTO)
       F->set.schur_engine = sym->flops_model >= RSLAB_SCHUR_AUTO_MIN_FLOPS ? RSLAB_SCHUR_TENSOR : RSLAB_SCHUR_FMA;
     if (F->set.schur_engine != RSLAB_SCHUR_TENSOR && F->set.schur_engine != RSLAB_SCHUR_FMA)
@@ -2211,6 +2316,8 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
     }
     if (!(single && F->set.schur_engine == RSLAB_SCHUR_TENSOR))
       F->gpool = F->al<unsigned char>((size_t)std::max(sym->g_elems, 1LL) * es);
+    if (F->set.method == RSLAB_METHOD_MULTIFRONTAL)
+      F->cbpool = F->al<unsigned char>((size_t)std::max(sym->cb_elems, 1LL) * es);
     if (F->set.scaling != RSLAB_SCALING_ONEPASS) {
       std::vector<double> ones(n, 1.0);
       CK(cudaMemcpyAsync(F->scale, ones.data(), n * 8, cudaMemcpyHostToDevice, F->st));
@@ -2390,6 +2497,7 @@ int rslab_factor_info(const rslab_fac_handle* F, rslab_factor_info_t* info) {
   info->dtype_hi = F->dtype_hi;
   info->multiprocessors = 0;
   info->schur_engine = F->set.schur_engine;
+  info->method = F->set.method;
   if (F->sym && F->sym->device >= 0)
     cudaDeviceGetAttribute(&info->multiprocessors, cudaDevAttrMultiProcessorCount, F->sym->device);
   return 0;

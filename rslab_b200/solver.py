@@ -208,6 +208,9 @@ class SolverSettings:
     # schedule of the factor's launches: side streams overlap independent
     # work (True) or everything runs in order on one stream (False)
     overlap: bool = True
+    # FactorMethod (multifrontal_ldlt.rs:283): "left_looking" (default) or
+    # "multifrontal" (fronts with contribution blocks and extend-add)
+    method: str = "left_looking"
 
     @staticmethod
     def exact() -> "SolverSettings":
@@ -276,6 +279,10 @@ class SolverSettings:
             raise ValueError(f"schur_engine must be one of {sorted(engines)}")
         s.schur_engine = engines[self.schur_engine]
         s.overlap = int(bool(self.overlap))
+        methods = {"left_looking": N.METHOD_LEFT_LOOKING, "multifrontal": N.METHOD_MULTIFRONTAL}
+        if self.method not in methods:
+            raise ValueError(f"method must be one of {sorted(methods)}")
+        s.method = methods[self.method]
         return s
 
 
@@ -336,6 +343,7 @@ class Diagnostics:
     estimate: Optional[MemoryEstimate] = None
     stages: list = field(default_factory=list)
     schur_engine: str = ""   # the descendant-update engine the factor ran with
+    method: str = ""         # left_looking or multifrontal
 
     def total_ms(self) -> float:
         return sum(s.wall_ms for s in self.stages)
@@ -541,7 +549,8 @@ class LdltSolver:
                            int(si.nlevels), threads=int(i.multiprocessors),
                            estimate=self._sym.estimate_memory(self.dtype),
                            stages=[StageReport("factor", float(i.factor_ms), int(si.flops_model), nnz * entry_bytes)],
-                           schur_engine="fma" if i.schur_engine == N.SCHUR_FMA else "tensor")
+                           schur_engine="fma" if i.schur_engine == N.SCHUR_FMA else "tensor",
+                           method="multifrontal" if i.method == N.METHOD_MULTIFRONTAL else "left_looking")
 
     def stream(self) -> int:
         return int(N.lib.rslab_factor_stream(self._h) or 0)
@@ -801,9 +810,9 @@ def solve_profile(handle, nrhs: int) -> dict:
 
 
 LAUNCH_KINDS = ("cmod", "getf2", "deep_replay", "panel_schur", "fwd_diag", "fwd_push", "bwd_off", "bwd_diag",
-                "cmod_mm", "cmod_asm", "split_r", "split_c", "fwd_gather", "unused13", "make_g", "diag_inv",
+                "cmod_mm", "cmod_asm", "split_r", "split_c", "fwd_gather", "extend_add", "make_g", "diag_inv",
                 "bwd_off_reduce", "schur_tc", "fwd_chain", "bwd_chain", "bwd_gather", "deep_mm", "make_m", "push_reduce",
-                "join")
+                "front_cb", "join")
 
 
 def profile_trace(handle) -> list:
