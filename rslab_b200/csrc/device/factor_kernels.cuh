@@ -1777,8 +1777,12 @@ __host__ __device__ constexpr size_t smem_make_m_off_prog(size_t es, int nb) {
 __host__ __device__ constexpr size_t smem_make_m_off_slice(size_t es, int nb) {
   return ((smem_make_m_off_prog(es, nb) + (size_t)nb * (3 * es + 4 + 1) + 16) + 15) & ~size_t(15);
 }
+// snapshot steps staged per slice: the whole block for 4- and 8-byte
+// fields, 64 steps for 16-byte ones (a 128-step c64 snapshot is 256 KB)
+__host__ __device__ constexpr int make_m_sl(size_t es) { return es >= 16 ? 64 : 128; }
 __host__ __device__ constexpr size_t smem_make_m_bytes(size_t es, int nb) {
-  return smem_make_m_off_slice(es, nb) + (size_t)nb * nb * es + 64;
+  return smem_make_m_off_slice(es, nb) +
+         (size_t)(make_m_sl(es) >= nb ? nb : make_m_sl(es) + 1) * nb * es + 64;
 }
 
 template <typename T, int NT>
@@ -1804,8 +1808,10 @@ __global__ void __launch_bounds__(NT) k_make_m(FactorArgs fa, const int4* __rest
                               reinterpret_cast<const T*>(fa.dsub) + first + kb, fa.kind + first + kb);
   T* S = reinterpret_cast<T*>(smem_raw + smem_make_m_off_slice(sizeof(T), nb));
   __syncthreads();
-  // the whole snapshot in one slice: no staging round trips inside the steps
-  replay_deep_rows<T, NT, true, MM_RB, 128>(panel, nrow, kb, pw, nb, i0, min(i0 + MM_RB, pw), snap, P, X, M, S);
+  // the snapshot in one slice (two for 16-byte fields): few staging round
+  // trips inside the steps
+  replay_deep_rows<T, NT, true, MM_RB, make_m_sl(sizeof(T))>(panel, nrow, kb, pw, nb, i0, min(i0 + MM_RB, pw), snap,
+                                                             P, X, M, S);
 }
 
 // ---------------------------------------------------------------------------
@@ -1815,9 +1821,9 @@ __global__ void __launch_bounds__(NT) k_make_m(FactorArgs fa, const int4* __rest
 // block is staged in shared memory first (the product overwrites it in
 // place), M streams through in mm_cw-column chunks; thread (r = tid %
 // MM_ROWS, g = tid / MM_ROWS) owns row r and a contiguous group of columns of
-// each chunk, summing over k in ascending order.  Task (s, kb, slot, r0).  Used with the tensor-core
-// engine of the single-precision fields (the FMA engine replays row by row,
-// in the oracle's operation order).
+// each chunk, summing over k in ascending order.  Task (s, kb, slot, r0).  Used with the tensor
+// engine of every field (the FMA engine replays row by row, in the oracle's
+// operation order).
 // ---------------------------------------------------------------------------
 template <typename T>
 __host__ __device__ constexpr int mm_cw() {

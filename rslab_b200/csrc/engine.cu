@@ -1005,11 +1005,9 @@ struct KernelSetup {
                               (int)smem_getf2_ll_bytes<T>(128)));
     CK(cudaFuncSetAttribute(k_deep<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep(es, 128)));
     CK(cudaFuncSetAttribute(k_diag_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_diag_inv(es)));
-    if constexpr (TensorCmod<T>::ok) {
-      CK(cudaFuncSetAttribute(k_deep_mm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep_mm_bytes<T>()));
-      CK(cudaFuncSetAttribute(k_make_m<T, 32 * MM_RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)smem_make_m_bytes(es, 128)));
-    }
+    CK(cudaFuncSetAttribute(k_deep_mm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep_mm_bytes<T>()));
+    CK(cudaFuncSetAttribute(k_make_m<T, 32 * MM_RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)smem_make_m_bytes(es, 128)));
     solve_nr_attrs<T, 1>();
     solve_nr_attrs<T, 4>();
     solve_nr_attrs<T, RHS_MAX>();
@@ -1209,7 +1207,9 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
   // fields also run their panel Schur / deep rows on the tensor-core kernels
   const bool mm = F.set.schur_engine == RSLAB_SCHUR_TENSOR;
   const bool use_tc = TensorCmod<T>::ok && mm;
-  fa.deep_mm = use_tc ? 1 : 0;
+  // deep rows of tall panels as a product with the block transform on the
+  // tensor engine of every field; the FMA engine replays them row by row
+  fa.deep_mm = mm ? 1 : 0;
   // multifrontal variant: contribution blocks and extend-add instead of cmod
   const bool mf = F.set.method == RSLAB_METHOD_MULTIFRONTAL;
   if (mf) CK(cudaMemsetAsync(F.cbpool, 0, (size_t)std::max(H.cb_elems, 1LL) * es, st));
@@ -1339,7 +1339,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
       }
       case L_DEEP_MM: {
         if (!fa.deep_mm) continue;
-        if constexpr (TensorCmod<T>::ok) {
+        {
           FactorArgs f2 = fa;
           f2.scratch_stride = getf2_scratch_stride(L.nb_slot, (long long)es);
           k_deep_mm<T><<<L.ntasks, 256, smem_deep_mm_bytes<T>(), ls>>>(f2, H.d_t4 + L.task_off, nb_small, nb_big);
