@@ -27,6 +27,13 @@ namespace rsd {
 constexpr int TILE = 64;      // output tile edge of the GEMM-class kernels
 constexpr int TPB = 256;      // threads per CTA of the GEMM-class kernels
 constexpr int FUSE_DEEP_ROWS = 192;  // getf2 replays this many deep rows itself
+// Blocks of at most this many columns with at most this many deep rows run
+// on the 128-thread getf2 (registers capped so several CTAs share an SM).
+constexpr int GETF2_NARROW_PW = 32, GETF2_NARROW_DEEP = 96;
+__host__ __device__ constexpr int getf2_narrow_minb(size_t es) { return es >= 16 ? 4 : 8; }
+// CTAs per SM the 512-thread getf2 is compiled for (64 registers a thread
+// for 4- and 8-byte fields)
+__host__ __device__ constexpr int getf2_wide_minb(size_t es) { return es >= 16 ? 1 : 2; }
 
 struct FactorArgs {
   // structure (device)
@@ -893,6 +900,28 @@ __device__ void replay_deep_rows(T* panel, long long nrow, int kb, int pw, int n
 
 constexpr int DEEP_R = 32;  // deep rows per replay chunk
 
+// The lower pw x pw block of panel columns [kb, kb + pw) into packed
+// storage: a fixed-count loop over the smallest W x W square (W = 32, 64 or
+// 128) that holds the block, so every load of a thread is in flight at once
+// and a narrow block does not walk the 128 x 128 index space.
+template <typename T, int NT, int W>
+__device__ __forceinline__ void load_packed_block_w(T* A, const T* panel, long long nrow, int kb, int pw) {
+#pragma unroll 8
+  for (int e = threadIdx.x; e < W * W; e += NT) {
+    const int i = e % W, j = e / W;
+    if (i < pw && j <= i) A[pk(i, j, pw)] = panel[(kb + i) + (long long)(kb + j) * nrow];
+  }
+}
+template <typename T, int NT>
+__device__ __forceinline__ void load_packed_block(T* A, const T* panel, long long nrow, int kb, int pw) {
+  if (pw > 64)
+    load_packed_block_w<T, NT, 128>(A, panel, nrow, kb, pw);
+  else if (pw > 32)
+    load_packed_block_w<T, NT, 64>(A, panel, nrow, kb, pw);
+  else
+    load_packed_block_w<T, NT, 32>(A, panel, nrow, kb, pw);
+}
+
 // The end of a BK panel block, shared by both getf2 kernels: the block's
 // local pivot order into lperm, the status word (first failing supernode,
 // perturbation count), the packed block back into the panel (the 2x2
@@ -982,7 +1011,8 @@ __device__ void getf2_finish(const FactorArgs& fa, int s, int kb, int pw, int nb
     unsigned char* pmem = smem_raw + (((size_t)(DEEP_R + 1) * nb * sizeof(T) + 15) & ~size_t(15));
     const ReplayProg<T> P = load_replay_prog<T, NT>(pmem, pw, nb, swaps, dG, dsG, kindG);
     __syncthreads();
-    replay_deep_rows<T, NT>(panel, nrow, kb, pw, nb, ke, nrow, snap, P, A);
+    // rows per pass: 32 with 8 or more warps, 8 with 4 (two rows a warp)
+    replay_deep_rows<T, NT, false, (NT >= 256 ? 32 : 8)>(panel, nrow, kb, pw, nb, ke, nrow, snap, P, A);
   }
 }
 
@@ -990,8 +1020,8 @@ __device__ void getf2_finish(const FactorArgs& fa, int s, int kb, int pw, int nb
 // getf2: task = (s, kb, slot, fuse) — unblocked BK over panel columns [kb, ke)
 // with every pivot candidate, update and interchange bounded to rows < ke.
 // ---------------------------------------------------------------------------
-template <typename T, int NT>
-__global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restrict__ tasks, int nb_small,
+template <typename T, int NT, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) k_getf2(FactorArgs fa, const int4* __restrict__ tasks, int nb_small,
                                               int nb_big) {
   using F = Field<T>;
   if (fa.status[0] != 0) return;
@@ -1029,11 +1059,7 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
   const int warp = tid >> 5, lane = tid & 31;
   constexpr int NW = NT / 32;
   // flat fixed-count load of the lower block (at most 128 x 128): loads in flight
-#pragma unroll 8
-  for (int e = tid; e < 128 * 128; e += NT) {
-    const int i = e & 127, j = e >> 7;
-    if (i < pw && j <= i) A[pk(i, j, pw)] = panel[(kb + i) + (long long)(kb + j) * nrow];
-  }
+  load_packed_block<T, NT>(A, panel, nrow, kb, pw);
   if (kb == 0)
     for (int p = tid; p < ncol; p += NT) lpermG[p] = p;
   for (int e = tid; e < pw; e += NT) {
@@ -1042,7 +1068,7 @@ __global__ void __launch_bounds__(NT) k_getf2(FactorArgs fa, const int4* __restr
     kindG[e] = 0;
     swaps[e] = -1;
   }
-  for (int e = tid; e < pw * nb; e += NT) snap[(e / nb) * nb + (e % nb)] = F::zero();
+  for (int e = tid; e < pw * nb; e += NT) snap[e] = F::zero();
   if (tid == 0) {
     ctl[2] = 0;
     ctl[3] = 0;
@@ -1374,11 +1400,7 @@ __global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* _
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
-#pragma unroll 8
-  for (int e = tid; e < 128 * 128; e += NT) {
-    const int i = e & 127, j = e >> 7;
-    if (i < pw && j <= i) A[pk(i, j, pw)] = panel[(kb + i) + (long long)(kb + j) * nrow];
-  }
+  load_packed_block<T, NT>(A, panel, nrow, kb, pw);
   if (kb == 0)
     for (int p = tid; p < ncol; p += NT) lpermG[p] = p;
   for (int e = tid; e < pw; e += NT) {
@@ -1387,7 +1409,7 @@ __global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* _
     kindG[e] = 0;
     swaps[e] = -1;
   }
-  for (int e = tid; e < pw * nb; e += NT) snap[(e / nb) * nb + (e % nb)] = F::zero();
+  for (int e = tid; e < pw * nb; e += NT) snap[e] = F::zero();
   if (tid < 16) ctl[tid] = 0;  // [2] nswaps, [3] error, [4..15] the steps' control words
   __syncthreads();
   for (int i = tid; i < pw; i += NT) lp_s[i] = lpermG[kb + i];

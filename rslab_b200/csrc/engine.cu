@@ -128,6 +128,8 @@ struct Launch {
                        // getf2 / deep-row launches (Schur update beyond the next block);
                        // 2 = on the cmod stream, overlapping the whole level (early
                        // tensor-core cmod of the next level, tagged by nb_slot)
+  int narrow = 0;      // getf2: 0, or the block width that sizes the shared memory of a
+                       // launch of narrow tasks (the 128-thread kernel)
 };
 
 }  // namespace
@@ -706,15 +708,20 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
     for (int64_t s : lvl) maxblocks = std::max(maxblocks, (int)((S.sn[s].ncol + nb_of(s) - 1) / nb_of(s)));
     for (int b = 0; b < maxblocks; ++b) {
       Launch G{L_GETF2, (long long)H.t4.size(), 0, 0};
-      std::vector<int4> deep, make_m, deep_mm, schur, schur_tc, schur_r, schur_tc_r;
-      int slot = 0, launch_nb = 0;
+      std::vector<int4> deep, make_m, deep_mm, schur, schur_tc, schur_r, schur_tc_r, narrow;
+      int slot = 0, launch_nb = 0, narrow_nb = 0;
       for (int64_t s : lvl) {
         int nb = nb_of(s), nc = (int)S.sn[s].ncol, nr = H.nrow[s];
         int kb = b * nb;
         if (kb >= nc) continue;
         int ke = std::min(kb + nb, nc);
         bool fuse = (nr - ke) <= FUSE_DEEP_ROWS;
-        H.t4.push_back(make_int4((int)s, kb, slot, fuse ? 1 : 0));
+        // narrow blocks with few deep rows (most leaves of a 3D problem are
+        // one to a few columns) go to a 128-thread launch: several CTAs per
+        // SM instead of one or two 512-thread ones
+        const bool nar = ke - kb <= GETF2_NARROW_PW && nr - ke <= GETF2_NARROW_DEEP;
+        (nar ? narrow : H.t4).push_back(make_int4((int)s, kb, slot, fuse ? 1 : 0));
+        if (nar) narrow_nb = std::max(narrow_nb, nb);
         launch_nb = std::max(launch_nb, nb);
         if (!fuse) {
           for (int r0 = ke; r0 < nr; r0 += DEEP_R) deep.push_back(make_int4((int)s, kb, slot, r0));
@@ -736,10 +743,17 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
             (c0 < nxt ? schur_tc : schur_tc_r).push_back(make_int4((int)s, kb, r0, c0));
         ++slot;
       }
-      G.ntasks = slot;
+      G.ntasks = (int)(H.t4.size() - G.task_off);
       G.nb_slot = launch_nb;
       if (!slot) continue;
-      H.fplan.push_back(G);
+      if (G.ntasks) H.fplan.push_back(G);
+      if (!narrow.empty()) {
+        // the same scratch slots and stride as the wide launch of this block
+        Launch Gn{L_GETF2, (long long)H.t4.size(), (int)narrow.size(), launch_nb};
+        Gn.narrow = narrow_nb;
+        H.t4.insert(H.t4.end(), narrow.begin(), narrow.end());
+        H.fplan.push_back(Gn);
+      }
       H.max_getf2_tasks = std::max(H.max_getf2_tasks, slot);
       if (!deep.empty()) {
         Launch D{L_DEEP, (long long)H.t4.size(), (int)deep.size(), launch_nb};
@@ -998,8 +1012,10 @@ struct KernelSetup {
                               (int)smem_cmod_dmm_bytes<T>()));
     CK(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
     CK(cudaFuncSetAttribute(k_front_cb<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
-    CK(cudaFuncSetAttribute(k_getf2<T, GETF2_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CK(cudaFuncSetAttribute(k_getf2<T, GETF2_NT, getf2_wide_minb(sizeof(T))>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)smem_getf2(es, 128)));
+    CK(cudaFuncSetAttribute(k_getf2<T, 128, getf2_narrow_minb(sizeof(T))>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_getf2(es, 128)));
     if constexpr (TensorCmod<T>::ok)
       CK(cudaFuncSetAttribute(k_getf2_ll<T, GETF2_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)smem_getf2_ll_bytes<T>(128)));
@@ -1311,6 +1327,11 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
       case L_GETF2: {
         FactorArgs f2 = fa;
         f2.scratch_stride = getf2_scratch_stride(L.nb_slot, (long long)es);
+        if (L.narrow) {  // narrow blocks: the bit-exact form on 4 warps, every field
+          k_getf2<T, 128, getf2_narrow_minb(sizeof(T))>
+              <<<L.ntasks, 128, smem_getf2(es, L.narrow), ls>>>(f2, H.d_t4 + L.task_off, nb_small, nb_big);
+          break;
+        }
         if constexpr (TensorCmod<T>::ok) {
           if (use_tc) {  // left-looking form: parity by tolerance, like the rest of the engine
             k_getf2_ll<T, GETF2_NT><<<L.ntasks, GETF2_NT, smem_getf2_ll_bytes<T>(L.nb_slot), ls>>>(
@@ -1318,7 +1339,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
             break;
           }
         }
-        k_getf2<T, GETF2_NT><<<L.ntasks, GETF2_NT, smem_getf2(es, L.nb_slot), ls>>>(f2, H.d_t4 + L.task_off,
+        k_getf2<T, GETF2_NT, getf2_wide_minb(sizeof(T))><<<L.ntasks, GETF2_NT, smem_getf2(es, L.nb_slot), ls>>>(f2, H.d_t4 + L.task_off,
                                                                                   nb_small, nb_big);
         break;
       }
