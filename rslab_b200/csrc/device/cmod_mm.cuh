@@ -642,3 +642,177 @@ __global__ void __launch_bounds__(DM_NT) k_cmod_dmm(FactorArgs fa, const int4* _
 }
 
 }  // namespace rsd
+
+namespace rsd {
+
+// ---------------------------------------------------------------------------
+// FP64 fields, tensor engine: the deferred in-panel Schur update on DMMA.
+// Task (s, kb, r0, c0) as k_schur_tc: trailing-part tile rows [ke + r0,
+// +128) x columns [ke + c0, +64) of block [kb, ke) of supernode s, minus
+// L21 G^T over the block's columns, G = L21 D formed while it is staged
+// (the block's D, dsub and kind in shared memory), on the lower part.  The
+// A chunks (L21 rows) arrive by cp.async; the B chunk of step c + 1 is read
+// into registers before the products of step c and stored after them, so
+// its loads overlap the DMMA.  Warp tiles and fragments as k_cmod_dmm.
+// ---------------------------------------------------------------------------
+template <typename T>
+__host__ __device__ constexpr size_t smem_schur_dmm_bytes() {
+  return smem_cmod_dmm_bytes<T>() + (size_t)128 * (2 * sizeof(T) + 1) + 16;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(DM_NT) k_schur_dmm(FactorArgs fa, const int4* __restrict__ tasks, int nb_small,
+                                                    int nb_big) {
+  using F = Field<T>;
+  constexpr bool CX = Field<T>::complex;
+  constexpr int KC = DmShape<T>::kc, DM_LDA = DmShape<T>::lda, DM_LDB = DmShape<T>::ldb;
+  constexpr int STAGE = KC * (DM_LDA + DM_LDB);
+  constexpr int PB = KC * MM_NC / DM_NT;  // B elements staged per thread per chunk
+  static_assert(PB * DM_NT == KC * MM_NC, "B chunk divides over the CTA");
+  if (fa.status[0] != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* stg = reinterpret_cast<T*>(smem_raw);
+  T* d_s = stg + 2 * STAGE;
+  T* ds_s = d_s + 128;
+  unsigned char* kd_s = reinterpret_cast<unsigned char*>(ds_s + 128);
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, kb = tk.y, r0 = tk.z, c0 = tk.w;
+  const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
+  const int nb = ncol >= 512 ? nb_big : nb_small;
+  const int ke = min(kb + nb, ncol), pw = ke - kb;
+  const int rows_here = min(MM_M, nrow - ke - r0), cols_here = min(MM_NC, ncol - ke - c0);
+  T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
+  const T* Lb = panel + ke + (long long)kb * nrow;  // the block's L21: row i, column t at Lb[i + t nrow]
+  const T* A = Lb + r0;
+  const T* Bl = Lb + c0;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int wr = warp >> 1, wc = warp & 1;
+  const int g = lane >> 2, q = lane & 3;
+  for (int t = tid; t < pw; t += DM_NT) {
+    d_s[t] = reinterpret_cast<const T*>(fa.d)[first + kb + t];
+    ds_s[t] = reinterpret_cast<const T*>(fa.dsub)[first + kb + t];
+    kd_s[t] = fa.kind[first + kb + t];
+  }
+  __syncthreads();
+
+  auto issue_a = [&](int t0, int st) {
+    T* As = stg + st * STAGE;
+    for (int e = tid; e < KC * MM_M; e += DM_NT) {
+      const int t = e / MM_M, r = e % MM_M, tt = t0 + t;
+      const bool ok = tt < pw && r < rows_here;
+      cp_async_zfill<(int)sizeof(T)>(As + t * DM_LDA + r, ok ? A + r + (long long)tt * nrow : A, ok);
+    }
+    cp_async_commit();
+  };
+  T bv[PB];
+  auto load_b = [&](int t0) {
+#pragma unroll
+    for (int u = 0; u < PB; ++u) {
+      const int e = tid + u * DM_NT, t = e / MM_NC, c = e % MM_NC, tt = t0 + t;
+      bv[u] = (tt < pw && c < cols_here) ? ld_G(Bl, (long long)nrow, c, tt, d_s, ds_s, kd_s) : F::zero();
+    }
+  };
+  auto store_b = [&](int st) {
+    T* Bs = stg + st * STAGE + KC * DM_LDA;
+#pragma unroll
+    for (int u = 0; u < PB; ++u) {
+      const int e = tid + u * DM_NT, t = e / MM_NC, c = e % MM_NC;
+      Bs[t * DM_LDB + c] = bv[u];
+    }
+  };
+
+  double acc[4][4][CX ? 4 : 2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int v = 0; v < (CX ? 4 : 2); ++v) acc[i][j][v] = 0.0;
+
+  // warps whose 32 x 32 block lies wholly above the diagonal skip the products
+  const bool active = 32 * wr < rows_here && 32 * wc < cols_here && r0 + 32 * wr + 31 >= c0 + 32 * wc;
+  const int nchunk = (pw + KC - 1) / KC;
+  if (nchunk > 0) {
+    issue_a(0, 0);
+    load_b(0);
+    store_b(0);
+  }
+  for (int c = 0; c < nchunk; ++c) {
+    const int st = c & 1;
+    if (c + 1 < nchunk) {
+      issue_a((c + 1) * KC, st ^ 1);
+      load_b((c + 1) * KC);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const T* As = stg + st * STAGE;
+    const T* Bs = As + KC * DM_LDA;
+    if (active) {
+#pragma unroll
+      for (int k4 = 0; k4 < KC; k4 += 4) {
+        const int t = k4 + q;
+        if constexpr (!CX) {
+          double a[4], b[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) a[i] = As[t * DM_LDA + 32 * wr + 8 * i + g];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) b[j] = Bs[t * DM_LDB + 32 * wc + 8 * j + g];
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) dmma884(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        } else {
+          T a[4], b[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) a[i] = As[t * DM_LDA + 32 * wr + 8 * i + g];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) b[j] = Bs[t * DM_LDB + 32 * wc + 8 * j + g];
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              dmma884(acc[i][j][0], acc[i][j][1], a[i].re, b[j].re);   // Re += Ar Br
+              dmma884(acc[i][j][0], acc[i][j][1], -a[i].im, b[j].im);  //       - Ai Bi
+              dmma884(acc[i][j][2], acc[i][j][3], a[i].re, b[j].im);   // Im += Ar Bi
+              dmma884(acc[i][j][2], acc[i][j][3], a[i].im, b[j].re);   //       + Ai Br
+            }
+        }
+      }
+    }
+    if (c + 1 < nchunk) store_b(st ^ 1);  // that stage was released by the last iteration's barrier
+    __syncthreads();
+  }
+  // panel -= acc on the lower part; per row block every load before its stores
+  T* tile = panel + (ke + r0) + (long long)(ke + c0) * nrow;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int row = 32 * wr + 8 * i + g;
+    T old[4][2];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        const int col = 32 * wc + 8 * j + 2 * q + v;
+        const bool in = row < rows_here && col < cols_here && r0 + row >= c0 + col;
+        old[j][v] = in ? tile[row + (long long)col * nrow] : F::zero();
+      }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        const int col = 32 * wc + 8 * j + 2 * q + v;
+        if (row < rows_here && col < cols_here && r0 + row >= c0 + col) {
+          T u;
+          if constexpr (CX)
+            u = T{acc[i][j][v], acc[i][j][2 + v]};
+          else
+            u = acc[i][j][v];
+          tile[row + (long long)col * nrow] = F::sub(old[j][v], u);
+        }
+      }
+  }
+}
+
+}  // namespace rsd

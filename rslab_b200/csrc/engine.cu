@@ -1007,9 +1007,12 @@ struct KernelSetup {
       CK(cudaFuncSetAttribute(k_schur_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_tc_bytes()));
     }
     CK(cudaFuncSetAttribute(k_cmod<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cmod_bytes<T>()));
-    if constexpr (!TensorCmod<T>::ok)
+    if constexpr (!TensorCmod<T>::ok) {
       CK(cudaFuncSetAttribute(k_cmod_dmm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)smem_cmod_dmm_bytes<T>()));
+      CK(cudaFuncSetAttribute(k_schur_dmm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_schur_dmm_bytes<T>()));
+    }
     CK(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
     CK(cudaFuncSetAttribute(k_front_cb<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
     CK(cudaFuncSetAttribute(k_getf2<T, GETF2_NT, getf2_wide_minb(sizeof(T))>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1251,8 +1254,8 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
       case L_EXT_ADD: case L_FRONT_CB: return mf;
       case L_DEEP: return !fa.deep_mm;
       case L_MAKE_M: case L_DEEP_MM: return fa.deep_mm != 0;
-      case L_SCHUR: return !use_tc;
-      case L_SCHUR_TC: return use_tc;
+      case L_SCHUR: return !mm;
+      case L_SCHUR_TC: return mm;  // tcgen05 tiles (f32 / c32) or DMMA tiles (f64 / c64)
       default: return true;
     }
   };
@@ -1368,7 +1371,7 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         break;
       }
       case L_SCHUR:
-        if (use_tc) continue;
+        if (mm) continue;
         k_schur<T><<<L.ntasks, TPB, smem_schur(es), ls>>>(fa, H.d_t4 + L.task_off, nb_small, nb_big);
         break;
       case L_EXT_ADD:
@@ -1378,12 +1381,12 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         k_front_cb<T><<<L.ntasks, TPB, smem_schur(es), ls>>>(fa, H.d_t4 + L.task_off);
         break;
       case L_SCHUR_TC:
-        if constexpr (TensorCmod<T>::ok) {
-          if (!use_tc) continue;
+        if (!mm) continue;
+        if constexpr (TensorCmod<T>::ok)
           k_schur_tc<T><<<L.ntasks, TC_NT, smem_cmod_tc_bytes(), ls>>>(fa, H.d_t4 + L.task_off, nb_small, nb_big);
-        } else {
-          continue;
-        }
+        else
+          k_schur_dmm<T><<<L.ntasks, DM_NT, smem_schur_dmm_bytes<T>(), ls>>>(fa, H.d_t4 + L.task_off, nb_small,
+                                                                            nb_big);
         break;
     }
     if (prof)
