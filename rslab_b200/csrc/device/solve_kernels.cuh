@@ -6,14 +6,15 @@
 // src/dense/ldlt_generic.rs:556-714).  Two index spaces are used:
 //   g : the analysed (fill-reducing) order — panel row structures live here;
 //   e : pivot order, e = first_col(s) + pivot position inside s.
-// Forward:  per level, k_fwd_gather pulls every descendant's push
-//           U_k = L21_k z_k into the columns of s (update-list order, no
-//           atomics), k_chain (wave_solve.cuh) solves the unit-lower
+// Forward:  per level, k_chain (wave_solve.cuh) pulls every descendant's
+//           push U_k = L21_k z_k into the columns of s (update-list order,
+//           no atomics) and solves the unit-lower
 //           diagonal blocks in pivot order with their precomputed
 //           inverses, and k_stream forms U_s; D^-1 follows the whole sweep
 //           (k_dsolve).
-// Backward: per level (root first), k_bwd_gather / k_stream form the
-//           off-diagonal dots against the ancestors' x, then k_chain
+// Backward: per level (root first), k_stream forms the off-diagonal dots
+//           against the ancestors' x (read through the row structure),
+//           then k_chain
 //           back-substitutes the diagonal blocks.
 // Reference: solve_ldlt_block (src/dense/ldlt_generic.rs:618-714).
 #pragma once
@@ -91,26 +92,6 @@ __device__ __forceinline__ T shfl_T(T v, int src) {
   } else {
     return __shfl_sync(0xffffffffu, v, src);
   }
-}
-
-// Forward gather of supernode s, pivot positions [p0, p0 + 16) (thread =
-// position x right-hand side): Z[p] = Y[g] minus every push U_k[r] that lands
-// on g = first + lperm[p], in update-list order (the pull list of g, built
-// at analysis).  No atomics and no block-wide barrier per updater.
-template <typename T>
-__global__ void __launch_bounds__(SOLVE_NT) k_fwd_gather(SolveArgs a, const int2* __restrict__ tasks) {
-  using F = Field<T>;
-  const int2 tk = tasks[blockIdx.x];
-  const int s = tk.x, p = tk.y + (int)(threadIdx.x / RHS_MAX), c = (int)(threadIdx.x % RHS_MAX);
-  const int first = a.sn_first[s], ncol = a.sn_ncol[s];
-  if (p >= ncol || c >= a.nrhs) return;
-  const int g = first + a.lperm[first + p];
-  const T* U = reinterpret_cast<const T*>(a.U) + a.c0 + c;
-  T y = reinterpret_cast<const T*>(a.Yg)[a.c0 + (long long)g * a.ld + c];
-  const int t0 = a.pull_ptr[g], t1 = a.pull_ptr[g + 1];
-#pragma unroll 4
-  for (int t = t0; t < t1; ++t) y = F::sub(y, U[(long long)a.pull_src[t] * a.ld]);
-  reinterpret_cast<T*>(a.Ze)[a.c0 + (long long)(first + p) * a.ld + c] = y;
 }
 
 // Inverse of the unit lower TB x TB diagonal block [j0, j0+nb) of a

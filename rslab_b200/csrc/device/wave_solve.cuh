@@ -15,8 +15,8 @@
 // [8g, 8g + 8) of every unit; the four slice partials are added in order
 // g = 0..3 at the end, so results are deterministic.  The right-hand sides
 // read here are final before the launch (forward: z of this level, solved
-// by an earlier launch; backward: the ancestors' x gathered into a
-// contiguous buffer by k_bwd_gather).
+// by an earlier launch; backward: the ancestors' x, each unit's 32 rows
+// read through the supernode's row structure).
 //
 // Chain (k_chain): every supernode is cut into TB = 64 column blocks whose
 // solves form a chain (forward: block i needs z of blocks j < i; backward:
@@ -54,6 +54,8 @@ constexpr int PUSH_KS = 16;               // column units (of 32) per forward-pu
 // of at most CH_NR columns (more CTAs, shorter per-block products).
 constexpr int CH_NR = 4;
 constexpr int CH_GROUPS = RHS_MAX / CH_NR;
+// blocks in a level from which its chains take every column of a pass
+constexpr int CH_WIDE_ITEMS = 600;
 
 // Stages in flight: 4, or 3 where the wide elements of 16 right-hand sides
 // would otherwise keep a second CTA off the SM.
@@ -144,7 +146,8 @@ struct StItem {
   long long ld;       // panel leading dimension (nrow)
   int r0, rlim;       // tile rows
   int c0, clim;       // tile columns
-  const T* V;         // right-hand-side row 0 of the item (row stride a.ld)
+  const T* V;         // right-hand-side row 0 of the item (row stride a.ld); backward: x in g order
+  const int* vrows;   // backward: g of each of the item's rows (x is read through it)
   int vlim;           // right-hand-side rows valid < vlim (relative)
   int cu;             // forward: column units per 64-row block (of this item's column chunk)
   int cb0;            // forward: first column unit of the item
@@ -173,7 +176,10 @@ __device__ __forceinline__ StItem<T, FWD> st_item(const SolveArgs& a, int4 tk) {
   } else {
     it.r0 = ncol + tk.z; it.rlim = min(nrow, it.r0 + BWD_CH);
     it.c0 = tk.y * TB; it.clim = ncol;
-    it.V = reinterpret_cast<const T*>(a.U) + a.c0 + (a.uoff[s] + tk.z) * a.ld;
+    // the ancestors' x straight from the solution vector: row r of the item
+    // is g = rs[ncol + r0 + r] (no gathered copy)
+    it.V = reinterpret_cast<const T*>(a.Xg) + a.c0;
+    it.vrows = a.rs + a.sn_rsoff[s] + ncol + tk.z;
     it.vlim = it.rlim - it.r0;
     it.cu = 1;
     it.cb0 = 0;
@@ -207,7 +213,8 @@ __device__ __forceinline__ void st_issue(T* S, T* Vs, const StItem<T, FWD>& it, 
   for (int e = threadIdx.x; e < 32 * nr; e += WV_NT) {
     const int k = e / nr, c = e - k * nr, row = vr0 + k;
     const bool ok = row < it.vlim;
-    const T* g = ok ? it.V + (long long)row * ld + c : it.V;
+    const long long vr = FWD ? row : (ok ? it.vrows[row] : 0);
+    const T* g = ok ? it.V + vr * ld + c : it.V;
     cp_async_zfill<sizeof(T)>(Vs + k * NR + c, g, ok);
   }
 }
@@ -332,25 +339,6 @@ __global__ void __launch_bounds__(WV_NT) k_push_reduce(SolveArgs a, const int4* 
   }
 }
 
-// Backward: the ancestors' x of every off-diagonal row of the level's
-// supernodes, gathered (g order -> row order) into the push buffer U, which
-// the backward dots stream contiguously.  Task (s, r0): rows [r0, r0 + 256).
-template <typename T>
-__global__ void __launch_bounds__(WV_NT) k_bwd_gather(SolveArgs a, const int2* __restrict__ tasks) {
-  const int2 tk = tasks[blockIdx.x];
-  const int s = tk.x;
-  const int ncol = a.sn_ncol[s], nrow = a.sn_nrow[s];
-  const int nr = a.nrhs;
-  const int* rss = a.rs + a.sn_rsoff[s];
-  const T* Xg = reinterpret_cast<const T*>(a.Xg) + a.c0;
-  T* U = reinterpret_cast<T*>(a.U) + a.c0 + a.uoff[s] * a.ld;
-  for (int e = threadIdx.x; e < 256 * nr; e += WV_NT) {
-    const int k = e / nr, c = e - k * nr, r = tk.y + k;
-    if (ncol + r >= nrow) continue;
-    U[(long long)r * a.ld + c] = Xg[(long long)rss[ncol + r] * a.ld + c];
-  }
-}
-
 // ---------------------------------------------------------------------------
 // Chain items (s, 0 / 1 = forward / backward, block i, first flag of s).
 // ---------------------------------------------------------------------------
@@ -397,8 +385,12 @@ __device__ __forceinline__ void ch_tile_mv(T (&acc)[NR], const T* S, const T* V,
   }
 }
 
+// gw: right-hand-side columns per chain group (CH_NR, or every column of the
+// pass for the levels whose items already fill the GPU: one CTA per block
+// then reads the block's inverse and dependency tiles once).
 template <typename T, bool FWD, int NR>
-__global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __restrict__ tasks, int ctr, int flag_base) {
+__global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __restrict__ tasks, int ctr, int flag_base,
+                                                 int gw) {
   using F = Field<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int sh_t, sh_abort;
@@ -420,8 +412,8 @@ __global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __rest
   // column group: columns [cg0, cg0 + nr) of the pass; a group with no
   // columns in this pass has nothing to do (its dependents are in the same
   // group)
-  const int cg0 = CH_NR * (tk.y >> 1);
-  const int nr = min(CH_NR, a.nrhs - cg0);
+  const int cg0 = gw * (tk.y >> 1);
+  const int nr = min(gw, a.nrhs - cg0);
   if (nr <= 0) return;
   // flags of group g: flag index (fb + block) * CH_GROUPS + g
   int* flags = a.wstate + flag_base + (long long)fb * CH_GROUPS + (tk.y >> 1);
@@ -441,14 +433,27 @@ __global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __rest
   ch_issue<T>(Lv, Li, ncol <= TB ? ncol : TB, 0, nb, 0, nb);
   if (nd > 0) issue(0);
   cp_async_commit();
-  // block vector: y_i (forward) or w_i - W_i (backward; W_i = off-diagonal dots)
+  // block vector.  Forward: y_i, gathered here — the right-hand side at
+  // g = first + lperm[p] minus every push that lands on g, in update-list
+  // order (the pull list of g, built at analysis; the pushes are final
+  // before this launch), so no separate gather pass.  Backward: w_i - W_i
+  // (W_i = off-diagonal dots).
   const T* Wb = (!FWD && nrow > ncol) ? reinterpret_cast<const T*>(a.Wb) + a.c0 + cg0 + (long long)first * ld : nullptr;
   for (int e = tid; e < 64 * NR; e += WV_NT) {
     const int r = e / NR, c = e % NR;
     T v = F::zero();
     if (r < nb && c < nr) {
-      v = ld_cg(Ze + (long long)(i * TB + r) * ld + c);
-      if (Wb) v = F::sub(v, Wb[(long long)(i * TB + r) * ld + c]);
+      if constexpr (FWD) {
+        const int gg = first + a.lperm[first + i * TB + r];
+        const T* Uc = reinterpret_cast<const T*>(a.U) + a.c0 + cg0 + c;
+        v = reinterpret_cast<const T*>(a.Yg)[a.c0 + cg0 + (long long)gg * ld + c];
+        const int t0 = a.pull_ptr[gg], t1 = a.pull_ptr[gg + 1];
+#pragma unroll 4
+        for (int t = t0; t < t1; ++t) v = F::sub(v, Uc[(long long)a.pull_src[t] * ld]);
+      } else {
+        v = ld_cg(Ze + (long long)(i * TB + r) * ld + c);
+        if (Wb) v = F::sub(v, Wb[(long long)(i * TB + r) * ld + c]);
+      }
     }
     wv[e] = v;
   }

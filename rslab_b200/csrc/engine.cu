@@ -129,7 +129,8 @@ struct Launch {
                        // 2 = on the cmod stream, overlapping the whole level (early
                        // tensor-core cmod of the next level, tagged by nb_slot)
   int narrow = 0;      // getf2: 0, or the block width that sizes the shared memory of a
-                       // launch of narrow tasks (the 128-thread kernel)
+                       // launch of narrow tasks (the 128-thread kernel); chain solves: 1 =
+                       // one chain per block over every column of the pass
 };
 
 }  // namespace
@@ -837,21 +838,24 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
     // stream the off-diagonal dots W_s = L21_s^T x_anc (row-chunk partials
     // reduced in chunk order), then the diagonal blocks (block chain).
     {
-      Launch Fg{L_FWD_GATHER, (long long)H.t2.size(), 0, 0};
-      for (int64_t s : lvl)
-        for (int p0 = 0; p0 < S.sn[s].ncol; p0 += SOLVE_NT / RHS_MAX) H.t2.push_back(make_int2((int)s, p0));
-      Fg.ntasks = (int)(H.t2.size() - Fg.task_off);
-      if (Fg.ntasks) H.fwdplan.push_back(Fg);
       int maxb = 0;
       for (int64_t s : lvl) maxb = std::max(maxb, (int)((S.sn[s].ncol + TB - 1) / TB));
       // diagonal blocks: chain items in block order across the level's
       // supernodes (ticket order = dependency order)
+      // a level with at least CH_WIDE_ITEMS blocks solves every column of a
+      // pass in one chain per block (enough CTAs already); narrower levels
+      // split the columns into CH_GROUPS chains of CH_NR
+      int items = 0;
+      for (int64_t s : lvl) items += (int)((S.sn[s].ncol + TB - 1) / TB);
+      const bool wide = items >= CH_WIDE_ITEMS;
+      const int ngroups = wide ? 1 : CH_GROUPS;
       if (maxb > 0) {
         Launch W{L_FWD_CHAIN, (long long)H.st4.size(), 0, H.nwave++};
+        W.narrow = wide ? 1 : 0;
         for (int b = 0; b < maxb; ++b)
           for (int64_t s : lvl)
             if (b * TB < S.sn[s].ncol)
-              for (int g = 0; g < CH_GROUPS; ++g) H.st4.push_back(make_int4((int)s, 2 * g, b, H.flag_off[s]));
+              for (int g = 0; g < ngroups; ++g) H.st4.push_back(make_int4((int)s, 2 * g, b, H.flag_off[s]));
         W.ntasks = (int)(H.st4.size() - W.task_off);
         H.fwdplan.push_back(W);
       }
@@ -884,11 +888,6 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       if (Pr.ntasks) H.fwdplan.push_back(Pr);
 
       std::vector<Launch> bw;
-      Launch Bg{L_BWD_GATHER, (long long)H.t2.size(), 0, 0};
-      for (int64_t s : lvl)
-        for (int r0 = 0; r0 < H.nrow[s] - S.sn[s].ncol; r0 += 256) H.t2.push_back(make_int2((int)s, r0));
-      Bg.ntasks = (int)(H.t2.size() - Bg.task_off);
-      if (Bg.ntasks) bw.push_back(Bg);
       // dots items (s, block, row chunk, slot); a block with several row
       // chunks writes partial sums to slots, reduced in chunk order next
       Launch Bo{L_BWD_OFF, (long long)H.st4.size(), 0, 0};
@@ -916,11 +915,12 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       if (Br.ntasks) bw.push_back(Br);
       if (maxb > 0) {
         Launch W{L_BWD_CHAIN, (long long)H.st4.size(), 0, H.nwave++};
+        W.narrow = wide ? 1 : 0;
         for (int dd = 0; dd < maxb; ++dd)
           for (int64_t s : lvl) {
             const int nblk = (int)((S.sn[s].ncol + TB - 1) / TB);
             if (dd < nblk)
-              for (int g = 0; g < CH_GROUPS; ++g)
+              for (int g = 0; g < ngroups; ++g)
                 H.st4.push_back(make_int4((int)s, 1 + 2 * g, nblk - 1 - dd, H.flag_off[s]));
           }
         W.ntasks = (int)(H.st4.size() - W.task_off);
@@ -971,20 +971,22 @@ void solve_nr_attrs() {
 // the smallest NR in {1, 4, RHS_MAX} that holds nr columns.
 template <typename T, bool FWD, int NR>
 void launch_solve_nr(int kind, int grid, int nr, const SolveArgs& sa, const int4* tasks, int ctr, int flags,
-                     cudaStream_t st) {
+                     cudaStream_t st, int gw = CH_NR) {
   if (kind == 0)
     k_stream<T, FWD, NR><<<grid, WV_NT, st_smem_bytes<T>(NR), st>>>(sa, tasks);
   else
-    k_chain<T, FWD, NR><<<grid, WV_NT, ch_smem_bytes<T>(NR), st>>>(sa, tasks, ctr, flags);
+    k_chain<T, FWD, NR><<<grid, WV_NT, ch_smem_bytes<T>(NR), st>>>(sa, tasks, ctr, flags, gw);
 }
 template <typename T, bool FWD>
 void launch_solve(int kind, int grid, int nr, const SolveArgs& sa, const int4* tasks, int ctr = 0, int flags = 0,
-                  cudaStream_t st = nullptr) {
-  if (kind == 1) {  // chain items carry at most CH_NR columns each
+                  cudaStream_t st = nullptr, bool wide = false) {
+  if (kind == 1) {  // chain items carry at most CH_NR columns each, or all of them (wide levels)
     if (nr <= 1)
       launch_solve_nr<T, FWD, 1>(kind, grid, nr, sa, tasks, ctr, flags, st);
-    else
+    else if (nr <= CH_NR || !wide)
       launch_solve_nr<T, FWD, CH_NR>(kind, grid, nr, sa, tasks, ctr, flags, st);
+    else
+      launch_solve_nr<T, FWD, RHS_MAX>(kind, grid, nr, sa, tasks, ctr, flags, st, RHS_MAX);
     return;
   }
   if (nr <= 1)
@@ -1568,11 +1570,8 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
     const int fwd_flags = WV_STATE_CTR + H.nwave, bwd_flags = fwd_flags + CH_GROUPS * H.nflags;
     for (const Launch& L : H.fwdplan) {
       switch (L.kind) {
-        case L_FWD_GATHER:
-          k_fwd_gather<T><<<L.ntasks, SOLVE_NT, 0, st>>>(sa, H.d_t2 + L.task_off);
-          break;
         case L_FWD_CHAIN:
-          launch_solve<T, true>(1, L.ntasks, nr, sa, H.d_st4 + L.task_off, L.nb_slot, fwd_flags, st);
+          launch_solve<T, true>(1, L.ntasks, nr, sa, H.d_st4 + L.task_off, L.nb_slot, fwd_flags, st, L.narrow != 0);
           break;
         case L_FWD_PUSH_RED:
           k_push_reduce<T><<<L.ntasks, WV_NT, 0, st>>>(sa, H.d_st4 + L.task_off);
@@ -1586,9 +1585,6 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
     if (prof) prof->mark(st, 3);
     for (const Launch& L : H.bwdplan) {
       switch (L.kind) {
-        case L_BWD_GATHER:
-          k_bwd_gather<T><<<L.ntasks, WV_NT, 0, st>>>(sa, H.d_t2 + L.task_off);
-          break;
         case L_BWD_OFF:
           launch_solve<T, false>(0, L.ntasks, nr, sa, H.d_st4 + L.task_off, 0, 0, st);
           break;
@@ -1596,7 +1592,7 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
           k_dots_reduce<T><<<L.ntasks, WV_NT, 0, st>>>(sa, H.d_st4 + L.task_off);
           break;
         default:  // L_BWD_CHAIN
-          launch_solve<T, false>(1, L.ntasks, nr, sa, H.d_st4 + L.task_off, L.nb_slot, bwd_flags, st);
+          launch_solve<T, false>(1, L.ntasks, nr, sa, H.d_st4 + L.task_off, L.nb_slot, bwd_flags, st, L.narrow != 0);
       }
       if (prof)
         prof->mark(st, (L.kind == L_BWD_OFF || L.kind == L_BWD_OFF_RED || L.kind == L_BWD_GATHER) ? 4 : 5, L.ntasks,
