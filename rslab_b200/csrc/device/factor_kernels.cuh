@@ -1600,20 +1600,25 @@ __global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* _
   const bool team = tid < 128;
   const double a2 = alpha * alpha;
   // Look-ahead: while the team finishes step k, warps 4-15 form the partial
-  // sums of column k + 1 over the pivoted columns p < k (three groups of 128
-  // rows).  When step k is a 1x1 pivot without interchange, step k + 1 uses
+  // sums of column k + 1 over the pivoted columns p < k (the rows [k + 1,
+  // pw) take R = 32, 64 or 128 of the 384 threads and the 384 / R groups
+  // split the columns).  When step k is a 1x1 pivot without interchange, step k + 1 uses
   // them (adding its one missing term, p = k) and skips its GEMV and block
   // barrier.  Control words are double-buffered by iteration parity: with
   // the GEMV barrier skipped, a thread may still read iteration i's words
   // while the team writes iteration i + 1's.
-  T* const rs0 = red + 4 * 128;  // two look-ahead buffers of 3 x 128 partial sums, by iteration parity
+  T* const rs0 = red + 4 * 128;  // two look-ahead buffers of 384 partial sums, by iteration parity
+  // log2 of the rows per look-ahead group for column c: the smallest of
+  // 32, 64, 128 that covers the rows [c, pw)
+  auto la_lr = [&](int c) { return pw - c <= 32 ? 5 : pw - c <= 64 ? 6 : 7; };
   auto spec_gemv = [&](int k, T* out) {
-    const int u = tid - 128, rr = u & 127, g = u >> 7, c = k + 1, i = c + rr;
+    const int c = k + 1, lr = la_lr(c), ng = 384 >> lr;
+    const int u = tid - 128, rr = u & ((1 << lr) - 1), g = u >> lr, i = c + rr;
     if (i < pw) {
       T acc0 = F::zero(), acc1 = F::zero();
       int p = g;
-      for (; p + 3 < k; p += 6) {
-        const int cp0 = p * pw - (p * (p + 1)) / 2, cp1 = (p + 3) * pw - ((p + 3) * (p + 4)) / 2;
+      for (; p + ng < k; p += 2 * ng) {
+        const int cp0 = p * pw - (p * (p + 1)) / 2, cp1 = (p + ng) * pw - ((p + ng) * (p + ng + 1)) / 2;
         acc0 = F::fma_(Gs[cp0 + i], A[cp0 + c], acc0);
         acc1 = F::fma_(Gs[cp1 + i], A[cp1 + c], acc1);
       }
@@ -1621,16 +1626,18 @@ __global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* _
         const int cp = p * pw - (p * (p + 1)) / 2;
         acc0 = F::fma_(Gs[cp + i], A[cp + c], acc0);
       }
-      out[g * 128 + rr] = F::add(acc0, acc1);
+      out[(g << lr) + rr] = F::add(acc0, acc1);
     }
   };
-  // team thread r, look-ahead case: v[k + r] = A0(k + r, k) - the three
-  // partials - G(k + r, k - 1) L(k, k - 1)
+  // team thread r, look-ahead case: v[k + r] = A0(k + r, k) - the group
+  // partials (in group order) - G(k + r, k - 1) L(k, k - 1)
   auto form_row_la = [&](int k, const T* part, int r) {
     const int i = k + r;
     if (i < pw) {
       const T a = A[pk(i, k, pw)];
-      const T u = F::add(F::add(part[r], part[128 + r]), part[256 + r]);
+      const int lr = la_lr(k), ng = 384 >> lr;
+      T u = part[r];
+      for (int g = 1; g < ng; ++g) u = F::add(u, part[(g << lr) + r]);
       const int cl = (k - 1) * pw - ((k - 1) * k) / 2;  // packed start of column k - 1
       v1[i] = F::sub(F::sub(a, u), F::mul(Gs[cl + i], A[cl + k]));
     }
