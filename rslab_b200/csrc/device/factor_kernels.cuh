@@ -1449,8 +1449,11 @@ __global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* _
   auto team_sync = []() { asm volatile("bar.sync 1, 128;" ::: "memory"); };
   // Team thread r: v[k + r] = A0(k + r, c) - the partial sums (all of the
   // row's partial loads issued before its tree sum).
-  auto form_row = [&](int k, int c, T* v, int r) {
+  // (returns the row's value, zero for a thread past the rows, so the
+  // caller's arg-max needs no shared-memory round trip)
+  auto form_row = [&](int k, int c, T* v, int r) -> T {
     const int ng = groups_of(k), R = ng == 4 ? 128 : ng == 8 ? 64 : 32, i = k + r;
+    T out = F::zero();
     if (r < R && i < pw) {
       const T a = i >= c ? A[pk(i, c, pw)] : A[pk(c, i, pw)];
       T part[16];
@@ -1460,8 +1463,10 @@ __global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* _
       for (int h = 8; h > 0; h >>= 1)
 #pragma unroll
         for (int g = 0; g < h; ++g) part[g] = F::add(part[g], part[g + h]);
-      v[i] = F::sub(a, part[0]);
+      out = F::sub(a, part[0]);
+      v[i] = out;
     }
+    return out;
   };
   // 1 / z with one division (the multipliers only need fp32 accuracy here)
   auto inv = [&](T z) -> T {
@@ -1630,17 +1635,27 @@ __global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* _
     }
   };
   // team thread r, look-ahead case: v[k + r] = A0(k + r, k) - the group
-  // partials (in group order) - G(k + r, k - 1) L(k, k - 1)
-  auto form_row_la = [&](int k, const T* part, int r) {
+  // partials (all loaded, then a tree sum) - G(k + r, k - 1) L(k, k - 1);
+  // returns the value (zero past the rows)
+  auto form_row_la = [&](int k, const T* part, int r) -> T {
     const int i = k + r;
+    T out = F::zero();
     if (i < pw) {
       const T a = A[pk(i, k, pw)];
       const int lr = la_lr(k), ng = 384 >> lr;
-      T u = part[r];
-      for (int g = 1; g < ng; ++g) u = F::add(u, part[(g << lr) + r]);
       const int cl = (k - 1) * pw - ((k - 1) * k) / 2;  // packed start of column k - 1
-      v1[i] = F::sub(F::sub(a, u), F::mul(Gs[cl + i], A[cl + k]));
+      const T gl = F::mul(Gs[cl + i], A[cl + k]);
+      T pp[16];
+#pragma unroll
+      for (int g = 0; g < 16; ++g) pp[g] = g < ng ? part[(g << lr) + r] : F::zero();
+#pragma unroll
+      for (int h = 8; h > 0; h >>= 1)
+#pragma unroll
+        for (int g = 0; g < h; ++g) pp[g] = F::add(pp[g], pp[g + h]);
+      out = F::sub(F::sub(a, pp[0]), gl);
+      v1[i] = out;
     }
+    return out;
   };
   for (int k = 0, it = 0; k < pw; ++it) {
     int* cc = ctl + 4 + 6 * (it & 1);         // this iteration: next k, kstep, kp, extra, error
@@ -1655,14 +1670,11 @@ __global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* _
       // the diagonal (the BK tests run on squares: no square roots or
       // divisions on the decision path)
       const int r = tid;
-      if (la)
-        form_row_la(k, rs0 + 384 * ((it + 1) & 1), r);
-      else
-        form_row(k, k, v1, r);
+      const T vk = la ? form_row_la(k, rs0 + 384 * ((it + 1) & 1), r) : form_row(k, k, v1, r);
       double m2 = -1.0;
       int idx = INT_MAX;
       if (r >= 1 && k + r < pw) {
-        m2 = F::mag2(v1[k + r]);
+        m2 = F::mag2(vk);
         idx = k + r;
       }
       warp_argmax(m2, idx);
@@ -1670,7 +1682,7 @@ __global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* _
         red_v[warp] = m2;
         red_i[warp] = idx;
       }
-      if (r == 0) red_v[4] = F::mag2(v1[k]);
+      if (r == 0) red_v[4] = F::mag2(vk);
       team_sync();
       // every team thread takes the same decision from the same values
       double col2 = -1.0;
@@ -1720,13 +1732,13 @@ __global__ void __launch_bounds__(NT, 1) k_getf2_ll(FactorArgs fa, const int4* _
       __syncthreads();
       if (team) {
         const int r = tid;
-        form_row(k, extra, v2, r);
+        const T ve = form_row(k, extra, v2, r);
         int kstep = cc[1], kp = cc[2];
         if (!reuse) {
           // the row maximum of the candidate row: its column over every row
           // of the unpivoted part but itself
           double m2 = 0.0;
-          if (k + r < pw && k + r != extra) m2 = F::mag2(v2[k + r]);
+          if (k + r < pw && k + r != extra) m2 = F::mag2(ve);
 #pragma unroll
           for (int o = 16; o > 0; o >>= 1) m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
           if (lane == 0) red_v[8 + warp] = m2;
