@@ -115,9 +115,12 @@ typedef struct {
  * Bunch-Kaufman kernels, and the contribution block becomes CB - L21 D L21^T
  * for the parent (factor_front + extend-add, multifrontal_ldlt.rs:901,
  * 1494-1510).  Same pivoting; the sums run in another order, so the factors
- * agree with the left-looking ones to rounding.  It runs on the CUDA cores
- * (schur_engine is ignored) and holds every contribution block (sum of
- * (nrow - ncol)^2 scalars) for the factor's lifetime. */
+ * agree with the left-looking ones to rounding.  schur_engine picks the panel
+ * kernels as for the left-looking method and, for f64 / c64, the engine of the
+ * contribution-block products (FP64 tensor-core tiles or the CUDA-core FMA
+ * tiles; the f32 / c32 ones run on the CUDA cores).  It holds every
+ * contribution block (sum of (nrow - ncol)^2 scalars) for the factor's
+ * lifetime and allocates none of the left-looking update buffers. */
 #define RSLAB_METHOD_LEFT_LOOKING 0
 #define RSLAB_METHOD_MULTIFRONTAL 1
 

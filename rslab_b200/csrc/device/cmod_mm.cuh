@@ -660,47 +660,30 @@ __host__ __device__ constexpr size_t smem_schur_dmm_bytes() {
   return smem_cmod_dmm_bytes<T>() + (size_t)128 * (2 * sizeof(T) + 1) + 16;
 }
 
+// One 128 x 64 tile: tile[row + col ldt] -= sum_t A[row + t lda] G(col, t)
+// over t in [0, kdim), G(col, t) = ld_G(B, lda, col, t, d, dsub, kind), for
+// row < rows_here, col < cols_here and r0 + row >= c0 + col (the lower part
+// of the trailing matrix).  256 threads; every thread calls it.
 template <typename T>
-__global__ void __launch_bounds__(DM_NT) k_schur_dmm(FactorArgs fa, const int4* __restrict__ tasks, int nb_small,
-                                                    int nb_big) {
+__device__ __forceinline__ void dmm_lower_update(const T* A, const T* B, long long lda, int kdim, const T* d,
+                                                 const T* dsub, const unsigned char* kind, T* tile, long long ldt,
+                                                 int rows_here, int cols_here, int r0, int c0, T* stg) {
   using F = Field<T>;
   constexpr bool CX = Field<T>::complex;
   constexpr int KC = DmShape<T>::kc, DM_LDA = DmShape<T>::lda, DM_LDB = DmShape<T>::ldb;
   constexpr int STAGE = KC * (DM_LDA + DM_LDB);
   constexpr int PB = KC * MM_NC / DM_NT;  // B elements staged per thread per chunk
   static_assert(PB * DM_NT == KC * MM_NC, "B chunk divides over the CTA");
-  if (fa.status[0] != 0) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* stg = reinterpret_cast<T*>(smem_raw);
-  T* d_s = stg + 2 * STAGE;
-  T* ds_s = d_s + 128;
-  unsigned char* kd_s = reinterpret_cast<unsigned char*>(ds_s + 128);
-  const int4 tk = tasks[blockIdx.x];
-  const int s = tk.x, kb = tk.y, r0 = tk.z, c0 = tk.w;
-  const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
-  const int nb = ncol >= 512 ? nb_big : nb_small;
-  const int ke = min(kb + nb, ncol), pw = ke - kb;
-  const int rows_here = min(MM_M, nrow - ke - r0), cols_here = min(MM_NC, ncol - ke - c0);
-  T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
-  const T* Lb = panel + ke + (long long)kb * nrow;  // the block's L21: row i, column t at Lb[i + t nrow]
-  const T* A = Lb + r0;
-  const T* Bl = Lb + c0;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int wr = warp >> 1, wc = warp & 1;
   const int g = lane >> 2, q = lane & 3;
-  for (int t = tid; t < pw; t += DM_NT) {
-    d_s[t] = reinterpret_cast<const T*>(fa.d)[first + kb + t];
-    ds_s[t] = reinterpret_cast<const T*>(fa.dsub)[first + kb + t];
-    kd_s[t] = fa.kind[first + kb + t];
-  }
-  __syncthreads();
 
   auto issue_a = [&](int t0, int st) {
     T* As = stg + st * STAGE;
     for (int e = tid; e < KC * MM_M; e += DM_NT) {
       const int t = e / MM_M, r = e % MM_M, tt = t0 + t;
-      const bool ok = tt < pw && r < rows_here;
-      cp_async_zfill<(int)sizeof(T)>(As + t * DM_LDA + r, ok ? A + r + (long long)tt * nrow : A, ok);
+      const bool ok = tt < kdim && r < rows_here;
+      cp_async_zfill<(int)sizeof(T)>(As + t * DM_LDA + r, ok ? A + r + (long long)tt * lda : A, ok);
     }
     cp_async_commit();
   };
@@ -709,7 +692,7 @@ __global__ void __launch_bounds__(DM_NT) k_schur_dmm(FactorArgs fa, const int4* 
 #pragma unroll
     for (int u = 0; u < PB; ++u) {
       const int e = tid + u * DM_NT, t = e / MM_NC, c = e % MM_NC, tt = t0 + t;
-      bv[u] = (tt < pw && c < cols_here) ? ld_G(Bl, (long long)nrow, c, tt, d_s, ds_s, kd_s) : F::zero();
+      bv[u] = (tt < kdim && c < cols_here) ? ld_G(B, lda, c, tt, d, dsub, kind) : F::zero();
     }
   };
   auto store_b = [&](int st) {
@@ -731,7 +714,7 @@ __global__ void __launch_bounds__(DM_NT) k_schur_dmm(FactorArgs fa, const int4* 
 
   // warps whose 32 x 32 block lies wholly above the diagonal skip the products
   const bool active = 32 * wr < rows_here && 32 * wc < cols_here && r0 + 32 * wr + 31 >= c0 + 32 * wc;
-  const int nchunk = (pw + KC - 1) / KC;
+  const int nchunk = (kdim + KC - 1) / KC;
   if (nchunk > 0) {
     issue_a(0, 0);
     load_b(0);
@@ -784,8 +767,7 @@ __global__ void __launch_bounds__(DM_NT) k_schur_dmm(FactorArgs fa, const int4* 
     if (c + 1 < nchunk) store_b(st ^ 1);  // that stage was released by the last iteration's barrier
     __syncthreads();
   }
-  // panel -= acc on the lower part; per row block every load before its stores
-  T* tile = panel + (ke + r0) + (long long)(ke + c0) * nrow;
+  // tile -= acc on the lower part; per row block every load before its stores
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int row = 32 * wr + 8 * i + g;
@@ -796,7 +778,7 @@ __global__ void __launch_bounds__(DM_NT) k_schur_dmm(FactorArgs fa, const int4* 
       for (int v = 0; v < 2; ++v) {
         const int col = 32 * wc + 8 * j + 2 * q + v;
         const bool in = row < rows_here && col < cols_here && r0 + row >= c0 + col;
-        old[j][v] = in ? tile[row + (long long)col * nrow] : F::zero();
+        old[j][v] = in ? tile[row + (long long)col * ldt] : F::zero();
       }
 #pragma unroll
     for (int j = 0; j < 4; ++j)
@@ -809,10 +791,57 @@ __global__ void __launch_bounds__(DM_NT) k_schur_dmm(FactorArgs fa, const int4* 
             u = T{acc[i][j][v], acc[i][j][2 + v]};
           else
             u = acc[i][j][v];
-          tile[row + (long long)col * nrow] = F::sub(old[j][v], u);
+          tile[row + (long long)col * ldt] = F::sub(old[j][v], u);
         }
       }
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(DM_NT) k_schur_dmm(FactorArgs fa, const int4* __restrict__ tasks, int nb_small,
+                                                    int nb_big) {
+  if (fa.status[0] != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* stg = reinterpret_cast<T*>(smem_raw);
+  T* d_s = stg + 2 * DmShape<T>::kc * (DmShape<T>::lda + DmShape<T>::ldb);
+  T* ds_s = d_s + 128;
+  unsigned char* kd_s = reinterpret_cast<unsigned char*>(ds_s + 128);
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, kb = tk.y, r0 = tk.z, c0 = tk.w;
+  const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s];
+  const int nb = ncol >= 512 ? nb_big : nb_small;
+  const int ke = min(kb + nb, ncol), pw = ke - kb;
+  T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
+  const T* Lb = panel + ke + (long long)kb * nrow;  // the block's L21: row i, column t at Lb[i + t nrow]
+  for (int t = threadIdx.x; t < pw; t += DM_NT) {
+    d_s[t] = reinterpret_cast<const T*>(fa.d)[first + kb + t];
+    ds_s[t] = reinterpret_cast<const T*>(fa.dsub)[first + kb + t];
+    kd_s[t] = fa.kind[first + kb + t];
+  }
+  __syncthreads();
+  dmm_lower_update<T>(Lb + r0, Lb + c0, (long long)nrow, pw, d_s, ds_s, kd_s,
+                      panel + (ke + r0) + (long long)(ke + c0) * nrow, (long long)nrow,
+                      min(MM_M, nrow - ke - r0), min(MM_NC, ncol - ke - c0), r0, c0, stg);
+}
+
+// Multifrontal method, FP64 fields on the tensor engine: the contribution
+// block of front s, CB -= L21 D L21^T over all ncol columns, in 128 x 64
+// tiles (task (s, r0, c0, 0), r0 a multiple of 128 at or below c0) of its
+// lower part; D, dsub and kind read through ld_G from the factor's arrays.
+template <typename T>
+__global__ void __launch_bounds__(DM_NT) k_front_cb_dmm(FactorArgs fa, const int4* __restrict__ tasks) {
+  if (fa.status[0] != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* stg = reinterpret_cast<T*>(smem_raw);
+  const int4 tk = tasks[blockIdx.x];
+  const int s = tk.x, r0 = tk.y, c0 = tk.z;
+  const int first = fa.sn_first[s], ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s], m = nrow - ncol;
+  const T* L21 = reinterpret_cast<const T*>(fa.panel) + fa.sn_poff[s] + ncol;
+  T* cb = reinterpret_cast<T*>(fa.cbpool) + fa.cb_off[s];
+  dmm_lower_update<T>(L21 + r0, L21 + c0, (long long)nrow, ncol, reinterpret_cast<const T*>(fa.d) + first,
+                      reinterpret_cast<const T*>(fa.dsub) + first, fa.kind + first,
+                      cb + r0 + (long long)c0 * m, (long long)m, min(MM_M, m - r0), min(MM_NC, m - c0), r0, c0,
+                      stg);
 }
 
 }  // namespace rsd

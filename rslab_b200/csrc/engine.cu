@@ -797,6 +797,16 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       }
       Lf.ntasks = (int)(H.t4.size() - Lf.task_off);
       if (Lf.ntasks) H.fplan.push_back(Lf);
+      // the same blocks as 128 x 64 DMMA tiles (FP64 fields, tensor engine)
+      Launch Ld{L_FRONT_CB, (long long)H.t4.size(), 0, 0};
+      Ld.narrow = 1;
+      for (int64_t s : lvl) {
+        const int m = H.nrow[s] - (int)S.sn[s].ncol;
+        for (int c0 = 0; c0 < m; c0 += TC_N)
+          for (int r0 = (c0 / TC_M) * TC_M; r0 < m; r0 += TC_M) H.t4.push_back(make_int4((int)s, r0, c0, 0));
+      }
+      Ld.ntasks = (int)(H.t4.size() - Ld.task_off);
+      if (Ld.ntasks) H.fplan.push_back(Ld);
     }
     // G_k = L21_k D_k of this level's updaters, for the CUDA-core cmod of
     // their ancestors (32-column tasks), and the tensor-core engine's split
@@ -1014,6 +1024,8 @@ struct KernelSetup {
                               (int)smem_cmod_dmm_bytes<T>()));
       CK(cudaFuncSetAttribute(k_schur_dmm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)smem_schur_dmm_bytes<T>()));
+      CK(cudaFuncSetAttribute(k_front_cb_dmm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_cmod_dmm_bytes<T>()));
     }
     CK(cudaFuncSetAttribute(k_schur<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
     CK(cudaFuncSetAttribute(k_front_cb<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
@@ -1253,7 +1265,8 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
       case L_SPLIT_R: return use_tc && !mf && !Field<T>::complex;
       case L_SPLIT_C: return use_tc && !mf && Field<T>::complex;
       case L_MAKE_G: return !use_tc && !mf;  // G_k of the CUDA-core cmod and of the DMMA tiles
-      case L_EXT_ADD: case L_FRONT_CB: return mf;
+      case L_EXT_ADD: return mf;
+      case L_FRONT_CB: return mf && (L.narrow != 0) == (mm && !TensorCmod<T>::ok);  // DMMA tiles or FMA tiles
       case L_DEEP: return !fa.deep_mm;
       case L_MAKE_M: case L_DEEP_MM: return fa.deep_mm != 0;
       case L_SCHUR: return !mm;
@@ -1380,6 +1393,12 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         k_extend_add<T><<<L.ntasks, 256, 0, ls>>>(fa, H.d_t4 + L.task_off, H.d_ea_pairs, H.d_ea_map, H.d_ea_moff);
         break;
       case L_FRONT_CB:
+        if constexpr (!TensorCmod<T>::ok) {
+          if (L.narrow) {
+            k_front_cb_dmm<T><<<L.ntasks, DM_NT, smem_cmod_dmm_bytes<T>(), ls>>>(fa, H.d_t4 + L.task_off);
+            break;
+          }
+        }
         k_front_cb<T><<<L.ntasks, TPB, smem_schur(es), ls>>>(fa, H.d_t4 + L.task_off);
         break;
       case L_SCHUR_TC:
@@ -2280,8 +2299,6 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
       rslab_default_factor_settings(&F->set);
     if (F->set.method != RSLAB_METHOD_LEFT_LOOKING && F->set.method != RSLAB_METHOD_MULTIFRONTAL)
       throw RslabError(Status::InvalidInput, "method must be RSLAB_METHOD_LEFT_LOOKING or _MULTIFRONTAL");
-    // the multifrontal variant runs on the CUDA-core kernels
-    if (F->set.method == RSLAB_METHOD_MULTIFRONTAL) F->set.schur_engine = RSLAB_SCHUR_FMA;
     if (F->set.schur_engine == RSLAB_SCHUR_AUTO)
       F->set.schur_engine = sym->flops_model >= RSLAB_SCHUR_AUTO_MIN_FLOPS ? RSLAB_SCHUR_TENSOR : RSLAB_SCHUR_FMA;
     if (F->set.schur_engine != RSLAB_SCHUR_TENSOR && F->set.schur_engine != RSLAB_SCHUR_FMA)
@@ -2328,13 +2345,16 @@ static int factor_impl(rslab_sym_handle* sym, int dtype, int dtype_hi, const voi
       F->amax_dev = F->al<unsigned long long>(1);
     }
     const bool single = dtype == RSLAB_F32 || dtype == RSLAB_C32;
-    if (F->set.schur_engine == RSLAB_SCHUR_TENSOR) {
+    // descendant-update buffers: the left-looking method only (the
+    // multifrontal one updates through its contribution blocks)
+    const bool ll = F->set.method == RSLAB_METHOD_LEFT_LOOKING;
+    if (ll && F->set.schur_engine == RSLAB_SCHUR_TENSOR) {
       if (single)
         setup_mm_pools(*F);
       else  // FP64 DMMA tiles: the level W buffers (the A / B operands are L21 and G)
         F->wbuf = F->al<float>((size_t)2 * sym->w_elems * es / 4);
     }
-    if (!(single && F->set.schur_engine == RSLAB_SCHUR_TENSOR))
+    if (ll && !(single && F->set.schur_engine == RSLAB_SCHUR_TENSOR))
       F->gpool = F->al<unsigned char>((size_t)std::max(sym->g_elems, 1LL) * es);
     if (F->set.method == RSLAB_METHOD_MULTIFRONTAL)
       F->cbpool = F->al<unsigned char>((size_t)std::max(sym->cb_elems, 1LL) * es);

@@ -29,13 +29,17 @@ def dominant3d(side, complex_):
     return matgen.shifted_laplacian(dims, -0.5 * lm)
 
 
+@pytest.mark.parametrize("engine", ["fma", "tensor"])
 @pytest.mark.parametrize("complex_,side,metis", [(False, 12, False), (True, 12, False), (False, 24, True),
                                                  (True, 24, True)])
-def test_multifrontal_matches_left_looking_entrywise(complex_, side, metis):
+def test_multifrontal_matches_left_looking_entrywise(complex_, side, metis, engine):
+    """engine "tensor": the panel kernels and the contribution-block products
+    on the FP64 tensor cores (DMMA tiles)."""
     a = dominant3d(side, complex_)
     o = Ordering.METIS_ND if metis else Ordering.AMD
     sym = LdltSymbolic.analyze_with(a, SolverSettings(ordering=o))
-    mf = sym.factor(a, SolverSettings(ordering=o, **MF))
+    mf = sym.factor(a, SolverSettings(ordering=o, schur_engine=engine, **MF))
+    assert mf.diagnostics().schur_engine == engine
     assert mf.diagnostics().method == "multifrontal"
     fm = mf.export_factors()
     lm = sym.factor(a, SolverSettings(ordering=o, **LL)).export_factors()
