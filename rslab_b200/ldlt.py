@@ -7,9 +7,10 @@ Same call shape and keyword meaning: the lower triangle of `A` is extracted
 complex128, complex64 — complex matrices are complex-symmetric, not
 Hermitian), the analysis uses the default settings, and the keywords layer on
 top.  `threads` sizes the reference's CPU pool and has no effect here;
-`method` ('left_looking' / 'multifrontal') and `memory` ('low' / 'eager')
-only change the reference's schedule and memory profile, never the factor,
-so they are validated and otherwise ignored.
+`method` ('left_looking' / 'multifrontal') picks the numeric schedule (the
+same pivoting; the factors agree to rounding); `memory` ('low' / 'eager')
+only changes the reference's CPU memory profile, never the factor, so it is
+validated and otherwise ignored (every panel here is resident on the device).
 """
 from __future__ import annotations
 
@@ -105,7 +106,7 @@ def ldlt(A, *, threads: Optional[int] = None, preconditioner: Optional[float] = 
     if threads is not None and threads < 0:
         raise ValueError("threads must be non-negative")
     a = _lower_csc(A)
-    st = SolverSettings()
+    st = SolverSettings(method="multifrontal" if method in ("multifrontal", "mf") else "left_looking")
     if preconditioner is not None:
         st.on_zero_pivot = ZeroPivotAction.perturb_to_eps(float(preconditioner))
     elif force_accept:

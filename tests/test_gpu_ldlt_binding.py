@@ -141,3 +141,18 @@ def test_drop_tol_matches_oracle_rule():
     assert f.factor_nnz < ldlt(A).factor_nnz
     b = np.ones(400)
     assert rel_res(A, f.solve(b, refine=40), b) < 1e-10
+
+
+@pytest.mark.parametrize("complex_", [False, True])
+def test_method_multifrontal_solves_alike(complex_):
+    """`method="multifrontal"` factors with contribution blocks and
+    extend-add; it solves like the left-looking default (the reference's LL
+    vs MF check is a 1e-9 solution tolerance, multifrontal_ldlt.rs:3865-3883)
+    with the same inertia."""
+    A = sym_dominant(400, 6, complex_=complex_)
+    b = np.linspace(-1, 1, 400) + (0.5j if complex_ else 0.0)
+    ll, mf = ldlt(A), ldlt(A, method="multifrontal")
+    assert mf.inertia == ll.inertia
+    xl, xm = ll.solve(b), mf.solve(b)
+    assert np.max(np.abs(xm - xl)) <= 1e-9 * np.max(np.abs(xl))
+    assert rel_res(A, xm, b) < 1e-12
