@@ -60,6 +60,9 @@ def parse():
     p.add_argument("--ordering", default="tuned", choices=["tuned", "amd", "metis"],
                    help="fill-reducing ordering of the helmholtz workload: tuned = the default pick of "
                         "LdltSolver::factor (nested-dissection bakeoff; MetisND on this matrix), amd, metis")
+    p.add_argument("--method", default="left_looking", choices=["left_looking", "multifrontal"],
+                   help="helmholtz workload: the numeric schedule of both legs (the multifrontal "
+                        "method factors through contribution blocks and extend-add)")
     p.add_argument("--tiers-side", type=int, default=80)
     p.add_argument("--tier-model", default=None, help="tier network .npz (default: the package's trained one)")
     p.add_argument("--sweep-side", type=int, default=48)
@@ -836,7 +839,7 @@ def main():
     x_d = torch.empty_like(b_d)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
-    st = SolverSettings()
+    st = SolverSettings(method=args.method)
     # The tier network picks the factor's precision tier from the matrix's
     # features, outside the timed region like the analysis.
     from rslab_b200.tiers import TIERS, TierModel, tier_features
@@ -956,6 +959,12 @@ def main():
                 "tf32_pipe_frac": 3.0 * ach / (peak_tf / 2.0),
                 "note": "achieved = algorithmic flops / k_cmod_mm time; the 3xTF32 split issues 3 tf32 products per "
                         "flop on a pipe with half the bf16 rate, tf32_pipe_frac = 3 x achieved / (peak / 2)"}
+    if args.method != "left_looking":
+        # no descendant-update tiles in this schedule: its c32 contribution-block
+        # products run on the CUDA cores (k_front_cb), timed in the profile
+        roofline = {"bound": None, "kernel": None,
+                    "note": "multifrontal schedule: no k_cmod_mm launches; the tensor-core roofline is reported "
+                            "for the default left-looking schedule"}
 
     # End-to-end through the public API with host buffers: the step's inputs
     # (matrix values, right-hand sides) and its result in page-locked host
@@ -1013,6 +1022,7 @@ def main():
             "config": {"workload": f"helmholtz3d_{args.side}^3_c64_nrhs{nrhs}", "n": n, "nnz_lower": a.nnz,
                        "nrhs": nrhs, "ordering": "MetisND" if ordering == Ordering.METIS_ND else "AMD",
                        "ordering_pick": args.ordering, "analysis_s": t_an,
+                       **({"method": args.method} if args.method != "left_looking" else {}),
                        "target_backward_error": args.target,
                        "model_flops": flops, "factor_nnz_panels": info.panel_elems,
                        "parallelism": f"replicas{ws}", "l2": "flushed between steps (256 MB write)"},

@@ -27,6 +27,7 @@ namespace rsd {
 constexpr int TILE = 64;      // output tile edge of the GEMM-class kernels
 constexpr int TPB = 256;      // threads per CTA of the GEMM-class kernels
 constexpr int FUSE_DEEP_ROWS = 192;  // getf2 replays this many deep rows itself
+constexpr int EA_ROWS = 1024;        // front rows per extend-add task
 // Blocks of at most this many columns with at most this many deep rows run
 // on the 128-thread getf2 (registers capped so several CTAs share an SM).
 constexpr int GETF2_NARROW_PW = 32, GETF2_NARROW_DEEP = 96;
@@ -498,15 +499,17 @@ __global__ void __launch_bounds__(TPB) k_schur(FactorArgs fa, const int4* __rest
 // ncol, the trailing rows and columns, lower part).
 //
 // k_extend_add: task (s, ct, pair_begin, pair_end): front columns [64 ct,
-// 64 ct + 64) of s; pair (c, ja, jb): child c's contribution-block columns
-// [ja, jb) land there.  Children are added in order (a block barrier between
+// 64 ct + 64) of s, front rows of one chunk of EA_ROWS; pair (c, ja, jb):
+// child c's contribution-block columns [ja, jb) land there, its rows
+// [i0, i1) (the pair's row range) in the chunk.  Children are added in order (a block barrier between
 // them), each entry (i, j), i >= j, of a child's block into the front entry
 // (map[i], map[j]) (the child's rows' positions in the front): the panel
 // when map[j] < ncol, CB_s otherwise.  Deterministic; no atomics.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(256) k_extend_add(FactorArgs fa, const int4* __restrict__ tasks,
-                                                    const int4* __restrict__ pairs, const int* __restrict__ emap,
+                                                    const int4* __restrict__ pairs, const int2* __restrict__ prow,
+                                                    const int* __restrict__ emap,
                                                     const long long* __restrict__ emoff) {
   using F = Field<T>;
   if (fa.status[0] != 0) return;
@@ -514,19 +517,40 @@ __global__ void __launch_bounds__(256) k_extend_add(FactorArgs fa, const int4* _
   const int s = tk.x, ncol = fa.sn_ncol[s], nrow = fa.sn_nrow[s], ms = nrow - ncol;
   T* panel = reinterpret_cast<T*>(fa.panel) + fa.sn_poff[s];
   T* cbs = reinterpret_cast<T*>(fa.cbpool) + fa.cb_off[s];
+  constexpr int EB = 8;  // entries per thread per batch: every load of a batch before its stores
   for (int u = tk.z; u < tk.w; ++u) {
     const int4 pr = pairs[u];
     const int c = pr.x, mc = fa.sn_nrow[c] - fa.sn_ncol[c];
     const T* cbc = reinterpret_cast<const T*>(fa.cbpool) + fa.cb_off[c];
     const int* map = emap + emoff[c];
-    for (int j = pr.y; j < pr.z; ++j) {
-      const int lj = map[j];
-      for (int i = j + (int)threadIdx.x; i < mc; i += 256) {
-        const int li = map[i];
-        const T v = cbc[i + (long long)j * mc];
-        T* t = lj < ncol ? panel + li + (long long)lj * nrow : cbs + (li - ncol) + (long long)(lj - ncol) * ms;
-        *t = F::add(*t, v);
+    // the child's columns [ja, jb) x rows [i0, i1) (the rows landing in this
+    // task's row chunk) as one index space (rows fastest: coalesced reads of
+    // the child's block), entries above the diagonal skipped; the targets of
+    // one child are distinct
+    const int2 rr = prow[u];
+    const int len = rr.y - rr.x;
+    const int tot = (pr.z - pr.y) * len;  // at most 64 columns x EA_ROWS rows
+    for (int e0 = 0; e0 < tot; e0 += EB * 256) {
+      T* tp[EB];
+      T v[EB], old[EB];
+#pragma unroll
+      for (int q = 0; q < EB; ++q) {
+        const int e = e0 + (int)threadIdx.x + q * 256;
+        tp[q] = nullptr;
+        if (e < tot) {
+          const int j = pr.y + e / len, i = rr.x + e % len;
+          if (i >= j) {
+            const int li = map[i], lj = map[j];
+            tp[q] = lj < ncol ? panel + li + (long long)lj * nrow : cbs + (li - ncol) + (long long)(lj - ncol) * ms;
+            v[q] = cbc[i + (long long)j * mc];
+          }
+        }
       }
+#pragma unroll
+      for (int q = 0; q < EB; ++q) old[q] = tp[q] ? *tp[q] : F::zero();
+#pragma unroll
+      for (int q = 0; q < EB; ++q)
+        if (tp[q]) *tp[q] = F::add(old[q], v[q]);
     }
     __syncthreads();  // the next child's additions follow this one's
   }

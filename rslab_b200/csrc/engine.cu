@@ -165,6 +165,7 @@ struct rslab_sym_handle {
   long long cb_elems = 0;
   std::vector<int> ea_map;
   std::vector<int4> ea_pairs;
+  std::vector<int2> ea_rows;  // per pair: the child rows [i0, i1) whose front rows lie in its task's row chunk
   // plan
   std::vector<int4> t4;
   std::vector<int4> cpairs;   // cmod (k, a, q0, nr << 16 | nc) per tile, in update order
@@ -232,6 +233,7 @@ struct rslab_sym_handle {
   long long *d_cb_off = nullptr, *d_ea_moff = nullptr;
   int* d_ea_map = nullptr;
   int4* d_ea_pairs = nullptr;
+  int2* d_ea_rows = nullptr;
   long long* d_linv_off = nullptr;
   int* d_t1 = nullptr;
   int2* d_t2 = nullptr;
@@ -308,6 +310,7 @@ struct rslab_sym_handle {
     d_ea_moff = up(ea_moff, st);
     d_ea_map = up(ea_map, st);
     d_ea_pairs = up(ea_pairs, st);
+    d_ea_rows = up(ea_rows, st);
     d_linv_off = up(linv_off, st);
     d_t1 = up(t1, st);
     d_t2 = up(t2, st);
@@ -688,19 +691,28 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
         const auto& ch = S.sn[s].children;
         if (ch.empty()) continue;
         const int nt = (H.nrow[s] + 63) / 64;
-        for (int ct = 0; ct < nt; ++ct) {
-          const int pb = (int)H.ea_pairs.size();
-          for (int64_t c : ch) {
-            const int64_t m = H.nrow[c] - S.sn[c].ncol;
-            if (m <= 0) continue;
-            const int* mp = H.ea_map.data() + H.ea_moff[c];
-            // the child columns j whose front column mp[j] lies in this tile
-            const int ja = (int)(std::lower_bound(mp, mp + m, 64 * ct) - mp);
-            const int jb = (int)(std::lower_bound(mp, mp + m, 64 * ct + 64) - mp);
-            if (jb > ja) H.ea_pairs.push_back(make_int4((int)c, ja, jb, 0));
+        // tasks: (64-column tile, chunk of EA_ROWS front rows at or below it),
+        // so a tall front spreads over many CTAs; targets stay disjoint
+        for (int ct = 0; ct < nt; ++ct)
+          for (int R0 = (64 * ct / EA_ROWS) * EA_ROWS; R0 < H.nrow[s]; R0 += EA_ROWS) {
+            const int pb = (int)H.ea_pairs.size();
+            for (int64_t c : ch) {
+              const int64_t m = H.nrow[c] - S.sn[c].ncol;
+              if (m <= 0) continue;
+              const int* mp = H.ea_map.data() + H.ea_moff[c];
+              // the child columns j whose front column mp[j] lies in this
+              // tile, and the child rows whose front row lies in this chunk
+              const int ja = (int)(std::lower_bound(mp, mp + m, 64 * ct) - mp);
+              const int jb = (int)(std::lower_bound(mp, mp + m, 64 * ct + 64) - mp);
+              const int i0 = std::max(ja, (int)(std::lower_bound(mp, mp + m, R0) - mp));
+              const int i1 = (int)(std::lower_bound(mp, mp + m, R0 + EA_ROWS) - mp);
+              if (jb > ja && i1 > i0) {
+                H.ea_pairs.push_back(make_int4((int)c, ja, jb, 0));
+                H.ea_rows.push_back(make_int2(i0, i1));
+              }
+            }
+            if ((int)H.ea_pairs.size() > pb) H.t4.push_back(make_int4((int)s, ct, pb, (int)H.ea_pairs.size()));
           }
-          if ((int)H.ea_pairs.size() > pb) H.t4.push_back(make_int4((int)s, ct, pb, (int)H.ea_pairs.size()));
-        }
       }
       Le.ntasks = (int)(H.t4.size() - Le.task_off);
       if (Le.ntasks) H.fplan.push_back(Le);
@@ -1390,7 +1402,8 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         k_schur<T><<<L.ntasks, TPB, smem_schur(es), ls>>>(fa, H.d_t4 + L.task_off, nb_small, nb_big);
         break;
       case L_EXT_ADD:
-        k_extend_add<T><<<L.ntasks, 256, 0, ls>>>(fa, H.d_t4 + L.task_off, H.d_ea_pairs, H.d_ea_map, H.d_ea_moff);
+        k_extend_add<T><<<L.ntasks, 256, 0, ls>>>(fa, H.d_t4 + L.task_off, H.d_ea_pairs, H.d_ea_rows, H.d_ea_map,
+                                                   H.d_ea_moff);
         break;
       case L_FRONT_CB:
         if constexpr (!TensorCmod<T>::ok) {
