@@ -51,6 +51,7 @@ struct SolveArgs {
   const long long* uoff;  // row offset of U_s
   const int* pull_ptr;    // n + 1: pull list of column g (g order)
   const int* pull_src;    // U row of each push, update-list order per g
+  const int2* dots_red;   // per supernode: (first partial-sum slot, row chunks) of its split backward dots
   const void* linv;       // inverses of the TB x TB diagonal blocks of wide supernodes
   const long long* linv_off;
   void* Wp;               // slots x 32 x ld partial sums of the split backward dots

@@ -299,26 +299,6 @@ __global__ void __launch_bounds__(WV_NT) k_stream(SolveArgs a, const int4* __res
   if (it.nunits > 0) flush(FWD ? (it.nunits - 1) / it.cu : 0);
 }
 
-// Backward: sum the row-chunk partials of (s, block i) in chunk order into
-// Wb.  Task (s, i, slot0, nchunks).
-template <typename T>
-__global__ void __launch_bounds__(WV_NT) k_dots_reduce(SolveArgs a, const int4* __restrict__ tasks) {
-  using F = Field<T>;
-  const int4 tk = tasks[blockIdx.x];
-  const int s = tk.x, i = tk.y, slot0 = tk.z, nch = tk.w;
-  const int ncol = a.sn_ncol[s];
-  const int ld = a.ld, nr = a.nrhs;
-  const T* part = reinterpret_cast<const T*>(a.Wp) + (long long)slot0 * 64 * ld;
-  T* Wb = reinterpret_cast<T*>(a.Wb) + a.c0 + (long long)a.sn_first[s] * ld;
-  for (int e = threadIdx.x; e < 64 * nr; e += WV_NT) {
-    const int p = e / nr, c = e - p * nr;
-    if (i * TB + p >= ncol) continue;
-    T v = part[(long long)p * ld + c];
-    for (int k = 1; k < nch; ++k) v = F::add(v, part[((long long)k * 64 + p) * ld + c]);
-    Wb[(long long)(i * TB + p) * ld + c] = v;
-  }
-}
-
 // Forward: sum the column-chunk partials of (s, 64-row block r0) in chunk
 // order into U.  Task (s, r0, slot0, nchunks).
 template <typename T>
@@ -437,8 +417,11 @@ __global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __rest
   // g = first + lperm[p] minus every push that lands on g, in update-list
   // order (the pull list of g, built at analysis; the pushes are final
   // before this launch), so no separate gather pass.  Backward: w_i - W_i
-  // (W_i = off-diagonal dots).
+  // (W_i = off-diagonal dots; for a supernode whose dots were split into
+  // row chunks, the chunk partials summed here in chunk order).
   const T* Wb = (!FWD && nrow > ncol) ? reinterpret_cast<const T*>(a.Wb) + a.c0 + cg0 + (long long)first * ld : nullptr;
+  const int2 dred = FWD ? make_int2(0, 0) : a.dots_red[s];
+  const T* Wpart = reinterpret_cast<const T*>(a.Wp) + (long long)(dred.x + i * dred.y) * 64 * ld + cg0;
   for (int e = tid; e < 64 * NR; e += WV_NT) {
     const int r = e / NR, c = e % NR;
     T v = F::zero();
@@ -452,7 +435,13 @@ __global__ void __launch_bounds__(WV_NT) k_chain(SolveArgs a, const int4* __rest
         for (int t = t0; t < t1; ++t) v = F::sub(v, Uc[(long long)a.pull_src[t] * ld]);
       } else {
         v = ld_cg(Ze + (long long)(i * TB + r) * ld + c);
-        if (Wb) v = F::sub(v, Wb[(long long)(i * TB + r) * ld + c]);
+        if (dred.y > 1) {
+          T w = Wpart[(long long)r * ld + c];
+          for (int q = 1; q < dred.y; ++q) w = F::add(w, Wpart[((long long)q * 64 + r) * ld + c]);
+          v = F::sub(v, w);
+        } else if (Wb) {
+          v = F::sub(v, Wb[(long long)(i * TB + r) * ld + c]);
+        }
       }
     }
     wv[e] = v;

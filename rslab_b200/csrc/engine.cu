@@ -202,6 +202,7 @@ struct rslab_sym_handle {
   long long urows = 0;
   // forward pull lists: for column g, the U rows pushed into it (update order)
   std::vector<int> pull_ptr, pull_src;
+  std::vector<int2> dots_red;  // per supernode: (first slot, chunks) of its split backward dots
   std::vector<Launch> fplan, fwdplan, bwdplan;
   int max_getf2_tasks = 0;
   int max_nb = 64;
@@ -240,6 +241,7 @@ struct rslab_sym_handle {
   int4* d_st4 = nullptr;
   long long* d_uoff = nullptr;
   int *d_pull_ptr = nullptr, *d_pull_src = nullptr;
+  int2* d_dots_red = nullptr;
   int* d_seg_of_row = nullptr;  // system of every user row (batch handles)
   long long* d_seg_begin = nullptr;
   std::mutex mu;
@@ -318,6 +320,7 @@ struct rslab_sym_handle {
     d_uoff = up(uoff, st);
     d_pull_ptr = up(pull_ptr, st);
     d_pull_src = up(pull_src, st);
+    d_dots_red = up(dots_red, st);
     if (seg_begin.size() > 2) {
       std::vector<int> sr(n);
       for (size_t i = 0; i + 1 < seg_begin.size(); ++i)
@@ -575,6 +578,7 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
   // Pull lists: every off-diagonal row r of updater k (U row uoff[k] + r)
   // lands on one column g of an ancestor; list the pushes per g in the
   // ancestor's update-list order so the gather subtracts them in that order.
+  H.dots_red.assign(ns, make_int2(0, 0));
   H.pull_ptr.assign(n + 1, 0);
   for (int s = 0; s < ns; ++s)
     for (int64_t u = S.upd_ptr[s]; u < S.upd_ptr[s + 1]; ++u) {
@@ -912,18 +916,19 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       std::vector<Launch> bw;
       // dots items (s, block, row chunk, slot); a block with several row
       // chunks writes partial sums to slots, reduced in chunk order next
+      // (the backward chain item of block i sums a split block's chunk
+      // partials itself, in chunk order: slots dots_red[s].x + i * chunks)
       Launch Bo{L_BWD_OFF, (long long)H.st4.size(), 0, 0};
-      std::vector<int4> red;
       int slot = 0;
       for (int64_t s : lvl) {
         const int off = H.nrow[s] - (int)S.sn[s].ncol;
         if (off <= 0) continue;
         const int nch = (off + BWD_CH - 1) / BWD_CH;
+        if (nch > 1) H.dots_red[s] = make_int2(slot, nch);
         for (int i = 0; i * TB < S.sn[s].ncol; ++i) {
           if (nch == 1) {
             H.st4.push_back(make_int4((int)s, i, 0, -1));
           } else {
-            red.push_back(make_int4((int)s, i, slot, nch));
             for (int q = 0; q < nch; ++q) H.st4.push_back(make_int4((int)s, i, q * BWD_CH, slot + q));
             slot += nch;
           }
@@ -932,9 +937,6 @@ void build_plan(rslab_sym_handle& H, const int64_t* col_ptr, const int64_t* row_
       Bo.ntasks = (int)(H.st4.size() - Bo.task_off);
       if (Bo.ntasks) bw.push_back(Bo);
       H.bwd_slots = std::max(H.bwd_slots, slot);
-      Launch Br{L_BWD_OFF_RED, (long long)H.st4.size(), (int)red.size(), 0};
-      H.st4.insert(H.st4.end(), red.begin(), red.end());
-      if (Br.ntasks) bw.push_back(Br);
       if (maxb > 0) {
         Launch W{L_BWD_CHAIN, (long long)H.st4.size(), 0, H.nwave++};
         W.narrow = wide ? 1 : 0;
@@ -1576,6 +1578,7 @@ SolveArgs make_sargs(rslab_fac_handle& F, int ld, int c0, int nr) {
   a.uoff = H.d_uoff;
   a.pull_ptr = H.d_pull_ptr;
   a.pull_src = H.d_pull_src;
+  a.dots_red = H.d_dots_red;
   a.linv = F.linv;
   a.linv_off = H.d_linv_off;
   a.Wp = F.Wp;
@@ -1619,9 +1622,6 @@ void enqueue_solve(rslab_fac_handle& F, const T* b, T* x, int nrhs, Prof* prof =
       switch (L.kind) {
         case L_BWD_OFF:
           launch_solve<T, false>(0, L.ntasks, nr, sa, H.d_st4 + L.task_off, 0, 0, st);
-          break;
-        case L_BWD_OFF_RED:
-          k_dots_reduce<T><<<L.ntasks, WV_NT, 0, st>>>(sa, H.d_st4 + L.task_off);
           break;
         default:  // L_BWD_CHAIN
           launch_solve<T, false>(1, L.ntasks, nr, sa, H.d_st4 + L.task_off, L.nb_slot, bwd_flags, st, L.narrow != 0);
