@@ -1365,7 +1365,11 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
           break;
         }
         if constexpr (TensorCmod<T>::ok) {
-          if (use_tc) {  // left-looking form: parity by tolerance, like the rest of the engine
+          // left-looking form (parity by tolerance, like the rest of the
+          // engine) for launches of a few blocks, where a block's step
+          // latency is the critical path; launches of many blocks take the
+          // right-looking form, which fits two CTAs per SM instead of one
+          if (use_tc && L.ntasks < GETF2_LL_MAX_TASKS) {
             k_getf2_ll<T, GETF2_NT><<<L.ntasks, GETF2_NT, smem_getf2_ll_bytes<T>(L.nb_slot), ls>>>(
                 f2, H.d_t4 + L.task_off, nb_small, nb_big);
             break;
