@@ -1848,13 +1848,15 @@ __host__ __device__ constexpr size_t smem_make_m_off_slice(size_t es, int nb) {
 }
 // snapshot steps staged per slice: the whole block for 4- and 8-byte
 // fields, 64 steps for 16-byte ones (a 128-step c64 snapshot is 256 KB)
+// (launches of many blocks take 32-step slices: a quarter of the shared
+// memory, so several CTAs share an SM)
 __host__ __device__ constexpr int make_m_sl(size_t es) { return es >= 16 ? 64 : 128; }
-__host__ __device__ constexpr size_t smem_make_m_bytes(size_t es, int nb) {
-  return smem_make_m_off_slice(es, nb) +
-         (size_t)(make_m_sl(es) >= nb ? nb : make_m_sl(es) + 1) * nb * es + 64;
+constexpr int MAKE_M_SL_WIDE = 32;
+__host__ __device__ constexpr size_t smem_make_m_bytes(size_t es, int nb, int sl) {
+  return smem_make_m_off_slice(es, nb) + (size_t)(sl >= nb ? nb : sl + 1) * nb * es + 64;
 }
 
-template <typename T, int NT>
+template <typename T, int NT, int SL>
 __global__ void __launch_bounds__(NT) k_make_m(FactorArgs fa, const int4* __restrict__ tasks, int nb_small,
                                                int nb_big) {
   static_assert(MM_RB == NT / 32, "one identity row per warp");
@@ -1877,10 +1879,9 @@ __global__ void __launch_bounds__(NT) k_make_m(FactorArgs fa, const int4* __rest
                               reinterpret_cast<const T*>(fa.dsub) + first + kb, fa.kind + first + kb);
   T* S = reinterpret_cast<T*>(smem_raw + smem_make_m_off_slice(sizeof(T), nb));
   __syncthreads();
-  // the snapshot in one slice (two for 16-byte fields): few staging round
-  // trips inside the steps
-  replay_deep_rows<T, NT, true, MM_RB, make_m_sl(sizeof(T))>(panel, nrow, kb, pw, nb, i0, min(i0 + MM_RB, pw), snap,
-                                                             P, X, M, S);
+  // the snapshot in slices of SL steps (the whole block, or two for 16-byte
+  // fields, in launches of a few blocks): few staging round trips
+  replay_deep_rows<T, NT, true, MM_RB, SL>(panel, nrow, kb, pw, nb, i0, min(i0 + MM_RB, pw), snap, P, X, M, S);
 }
 
 // ---------------------------------------------------------------------------

@@ -1053,8 +1053,11 @@ struct KernelSetup {
     CK(cudaFuncSetAttribute(k_deep<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep(es, 128)));
     CK(cudaFuncSetAttribute(k_diag_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_diag_inv(es)));
     CK(cudaFuncSetAttribute(k_deep_mm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_deep_mm_bytes<T>()));
-    CK(cudaFuncSetAttribute(k_make_m<T, 32 * MM_RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)smem_make_m_bytes(es, 128)));
+    CK(cudaFuncSetAttribute(k_make_m<T, 32 * MM_RB, make_m_sl(sizeof(T))>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)smem_make_m_bytes(es, 128, make_m_sl(sizeof(T)))));
+    CK(cudaFuncSetAttribute(k_make_m<T, 32 * MM_RB, MAKE_M_SL_WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)smem_make_m_bytes(es, 128, MAKE_M_SL_WIDE)));
     solve_nr_attrs<T, 1>();
     solve_nr_attrs<T, 4>();
     solve_nr_attrs<T, RHS_MAX>();
@@ -1390,8 +1393,14 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
         if (!fa.deep_mm) continue;
         FactorArgs f2 = fa;
         f2.scratch_stride = getf2_scratch_stride(L.nb_slot, (long long)es);
-        k_make_m<T, 32 * MM_RB><<<L.ntasks, 32 * MM_RB, smem_make_m_bytes(es, L.nb_slot), ls>>>(
-            f2, H.d_t4 + L.task_off, nb_small, nb_big);
+        if (L.ntasks >= GETF2_LL_MAX_TASKS)  // many blocks: smaller slices, more CTAs per SM
+          k_make_m<T, 32 * MM_RB, MAKE_M_SL_WIDE>
+              <<<L.ntasks, 32 * MM_RB, smem_make_m_bytes(es, L.nb_slot, MAKE_M_SL_WIDE), ls>>>(
+                  f2, H.d_t4 + L.task_off, nb_small, nb_big);
+        else
+          k_make_m<T, 32 * MM_RB, make_m_sl(sizeof(T))>
+              <<<L.ntasks, 32 * MM_RB, smem_make_m_bytes(es, L.nb_slot, make_m_sl(sizeof(T))), ls>>>(
+                  f2, H.d_t4 + L.task_off, nb_small, nb_big);
         break;
       }
       case L_DEEP_MM: {
