@@ -35,6 +35,8 @@ __host__ __device__ constexpr int getf2_narrow_minb(size_t es) { return es >= 16
 // CTAs per SM the 512-thread getf2 is compiled for (64 registers a thread
 // for 4- and 8-byte fields)
 __host__ __device__ constexpr int getf2_wide_minb(size_t es) { return es >= 16 ? 1 : 2; }
+// ... and the 256-thread one, used for launches of many blocks
+__host__ __device__ constexpr int getf2_mid_minb(size_t es) { return es >= 16 ? 2 : 4; }
 // Tensor engine of the single-precision fields: getf2 launches of at least
 // this many blocks use the right-looking kernel (two CTAs per SM) rather
 // than the left-looking one (one CTA per SM, shorter steps).

@@ -1045,6 +1045,8 @@ struct KernelSetup {
     CK(cudaFuncSetAttribute(k_front_cb<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_schur(es)));
     CK(cudaFuncSetAttribute(k_getf2<T, GETF2_NT, getf2_wide_minb(sizeof(T))>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)smem_getf2(es, 128)));
+    CK(cudaFuncSetAttribute(k_getf2<T, 256, getf2_mid_minb(sizeof(T))>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)smem_getf2(es, 128)));
     CK(cudaFuncSetAttribute(k_getf2<T, 128, getf2_narrow_minb(sizeof(T))>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_getf2(es, 128)));
     if constexpr (TensorCmod<T>::ok)
@@ -1378,8 +1380,12 @@ void enqueue_factor(rslab_fac_handle& F, Prof* prof = nullptr) {
             break;
           }
         }
-        k_getf2<T, GETF2_NT, getf2_wide_minb(sizeof(T))><<<L.ntasks, GETF2_NT, smem_getf2(es, L.nb_slot), ls>>>(f2, H.d_t4 + L.task_off,
-                                                                                  nb_small, nb_big);
+        if (L.ntasks >= GETF2_LL_MAX_TASKS)  // many blocks: 8 warps, more CTAs per SM
+          k_getf2<T, 256, getf2_mid_minb(sizeof(T))>
+              <<<L.ntasks, 256, smem_getf2(es, L.nb_slot), ls>>>(f2, H.d_t4 + L.task_off, nb_small, nb_big);
+        else
+          k_getf2<T, GETF2_NT, getf2_wide_minb(sizeof(T))>
+              <<<L.ntasks, GETF2_NT, smem_getf2(es, L.nb_slot), ls>>>(f2, H.d_t4 + L.task_off, nb_small, nb_big);
         break;
       }
       case L_DEEP: {
