@@ -284,13 +284,13 @@ int rslab_factor_profile(rslab_fac_handle* fac, double* kind_ms, int64_t* kind_l
 int rslab_solve_profile(rslab_fac_handle* fac, int64_t nrhs, double* kind_ms, int64_t* kind_launches);
 /* Per-launch rows of the handle's last factor/solve profile: launch kind
  * (0 cmod, 1 getf2, 2 deep replay, 3 panel Schur, 4 forward diagonal,
- * 5 forward push, 6 backward dots, 7 backward diagonal, 8-11 see below, 12
- * forward gather, 13 multifrontal extend-add, 14 G = L21 D, 15
- * diagonal-block inverses, 16 backward partial-sum reduction, 17 tensor-core
- * panel Schur, 18/19 forward/backward block-chain solve, 20 backward gather,
- * 21 deep rows as a product with the block transform, 22 block transform, 23
- * forward push partial-sum reduction, 24 multifrontal contribution block,
- * -1 other), grid
+ * 5 forward push, 6 backward dots, 7 backward diagonal, 8-11 see below, 13
+ * multifrontal extend-add, 14 G = L21 D, 15 diagonal-block inverses, 17
+ * tensor-core panel Schur (tcgen05 or DMMA tiles), 18/19 forward/backward
+ * block-chain solve, 21 deep rows as a product with the block transform, 22
+ * block transform, 23 forward push partial-sum reduction, 24 multifrontal
+ * contribution block, -1 other; 12, 16 and 20 are not launched any more: the
+ * chain items gather their own right-hand sides and sum split dots), grid
  * size and device ms.  *count = rows available; at most cap are written.
  * A measurement aid with no reference counterpart.  Kinds 8-11 are the
  * tensor-core cmod's GEMM tiles, its assembly and the real / complex operand
