@@ -759,9 +759,18 @@ __device__ void replay_rows_warp(T (&x)[NR][NS], int pw, const T* S, int lds, in
   using F = Field<T>;
   const int lane = threadIdx.x & 31;
   int k = k_begin;
+  // the next step's program words are read one step ahead, so a step's
+  // branches do not wait on shared memory
+  int kp_n = k < k_end ? P.sw[k] : -1;
+  bool two_n = k < k_end && P.kd[k] == 1;
   while (k < k_end) {
-    const int kp = P.sw[k];
-    const bool two = P.kd[k] == 1;
+    const int kp = kp_n;
+    const bool two = two_n;
+    const int kn = k + (two ? 2 : 1);
+    if (kn < k_end) {
+      kp_n = P.sw[kn];
+      two_n = P.kd[kn] == 1;
+    }
     if (kp >= 0) {
       const int src = two ? k + 1 : k, dst = kp - kb;
 #pragma unroll
@@ -791,24 +800,24 @@ __device__ void replay_rows_warp(T (&x)[NR][NS], int pw, const T* S, int lds, in
         if (lane == ((k + 1) & 31))
           put(x[r], (k + 1) >> 5, F::mul(F::sub(F::mul(d11, xk1), F::mul(d21, xk)), detinv));
       }
-      k += 2;
     } else {
       const T dinv = P.inv[k];
+      T w[NS];  // the step's multipliers, loaded before the broadcast they do not depend on
+#pragma unroll
+      for (int j = 0; j < NS; ++j) {
+        const int col = lane + 32 * j;
+        w[j] = (col > k && col < pw) ? S[(k - k_begin) * lds + col] : F::zero();
+      }
 #pragma unroll
       for (int r = 0; r < NR; ++r) {
         const T xk = shfl_t(pick(x[r], k >> 5), k & 31);
 #pragma unroll
-        for (int j = 0; j < NS; ++j) {
-          const int col = lane + 32 * j;
-          if (col > k && col < pw) {
-            const T w = S[(k - k_begin) * lds + col];
-            if (!F::is_zero(w)) x[r][j] = F::sub(x[r][j], F::mul(xk, w));
-          }
-        }
+        for (int j = 0; j < NS; ++j)
+          if (!F::is_zero(w[j])) x[r][j] = F::sub(x[r][j], F::mul(xk, w[j]));
         if (lane == (k & 31)) put(x[r], k >> 5, F::mul(xk, dinv));
       }
-      k += 1;
     }
+    k = kn;
   }
 }
 
