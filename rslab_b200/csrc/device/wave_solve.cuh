@@ -138,7 +138,8 @@ __device__ __forceinline__ void store_partials(T* red, const T (&acc)[NR], int x
 // Backward dots (s, i, r0, slot): for the columns of block i, sum over
 // off-diagonal rows [ncol + r0, ncol + r0 + BWD_CH) of L[r, p] x_anc[r];
 // slot < 0 (the only chunk) writes Wb, else partial sums go to slot `slot`
-// (64 x ld each).
+// (64 x ld each), which the backward chain item of block i adds up in chunk
+// order.
 // ---------------------------------------------------------------------------
 template <typename T, bool FWD>
 struct StItem {
