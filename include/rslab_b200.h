@@ -206,6 +206,10 @@ typedef struct {
   uint64_t factor_flops, critical_path_flops;
   int64_t max_tree_width;
   int64_t symbolic_factor_nnz; /* exact column-count fill x 1.2 (src/symbolic/mod.rs:1189,1202) */
+  /* MemoryEstimate::mf_transient_peak_bytes (src/diagnostics.rs:30-40): the
+   * figure for RSLAB_METHOD_MULTIFRONTAL, which here keeps every contribution
+   * block resident: transient_peak_bytes + sum (nrow - ncol)^2 value_bytes */
+  int64_t mf_transient_peak_bytes;
 } rslab_memory_estimate_t;
 int rslab_symbolic_estimate(const rslab_sym_handle* sym, int64_t value_bytes, rslab_memory_estimate_t* est);
 

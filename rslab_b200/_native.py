@@ -81,7 +81,7 @@ class MemoryEstimateC(C.Structure):
         ("value_bytes", C.c_int64), ("factor_nnz", C.c_int64), ("factor_bytes", C.c_int64),
         ("panels_all_bytes", C.c_int64), ("panel_live_peak_bytes", C.c_int64), ("transient_peak_bytes", C.c_int64),
         ("factor_flops", C.c_uint64), ("critical_path_flops", C.c_uint64), ("max_tree_width", C.c_int64),
-        ("symbolic_factor_nnz", C.c_int64),
+        ("symbolic_factor_nnz", C.c_int64), ("mf_transient_peak_bytes", C.c_int64),
     ]
 
 

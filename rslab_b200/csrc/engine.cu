@@ -1999,6 +1999,7 @@ void fill_estimate(const rslab::MemoryEstimate& e, const rslab::Symbolic& S, rsl
   out->critical_path_flops = e.critical_path_flops;
   out->max_tree_width = e.max_tree_width;
   out->symbolic_factor_nnz = rslab::symbolic_factor_nnz(S);
+  out->mf_transient_peak_bytes = e.mf_transient_peak_bytes;
 }
 
 }  // namespace

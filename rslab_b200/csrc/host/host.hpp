@@ -135,6 +135,9 @@ struct MemoryEstimate {
   int64_t panel_live_peak_bytes = 0, transient_peak_bytes = 0;
   uint64_t factor_flops = 0, critical_path_flops = 0;
   int64_t max_tree_width = 0;
+  // the multifrontal method's figure: the left-looking one plus every
+  // contribution block, all of which it keeps resident on the device
+  int64_t mf_transient_peak_bytes = 0;
 };
 MemoryEstimate estimate_memory(const Symbolic& S, int64_t value_bytes);
 // symbolic_factor_nnz (src/numeric/sparse_solver.rs:550-555): the exact

@@ -736,6 +736,12 @@ MemoryEstimate estimate_memory(const Symbolic& S, int64_t value_bytes) {
   e.factor_nnz = factor_bytes / std::max<int64_t>(value_bytes + 8, 1);
   e.panel_live_peak_bytes = std::max<int64_t>(peak, 0);
   e.transient_peak_bytes = panels_all + factor_bytes + input_bytes + scratch;
+  int64_t cb_all = 0;  // sum over supernodes of (nrow - ncol)^2 scalars
+  for (int64_t s = 0; s < ns; ++s) {
+    const int64_t m = nrow(s) - S.sn[s].ncol;
+    cb_all += m * m * value_bytes;
+  }
+  e.mf_transient_peak_bytes = e.transient_peak_bytes + cb_all;
   std::vector<uint64_t> crit(ns, 0);
   uint64_t cp = 0, flops = 0;
   for (int64_t s = 0; s < ns; ++s) {

@@ -314,6 +314,7 @@ class MemoryEstimate:
     factor_flops: int
     critical_path_flops: int
     max_tree_width: int
+    mf_transient_peak_bytes: int = 0  # the multifrontal method's figure (every contribution block resident)
 
 
 @dataclass
@@ -413,7 +414,7 @@ class LdltSymbolic:
         _check(N.lib.rslab_symbolic_estimate(self._h, np.dtype(dtype).itemsize, C.byref(e)))
         return MemoryEstimate(int(e.value_bytes), int(e.factor_nnz), int(e.factor_bytes), int(e.panels_all_bytes),
                               int(e.panel_live_peak_bytes), int(e.transient_peak_bytes), int(e.factor_flops),
-                              int(e.critical_path_flops), int(e.max_tree_width))
+                              int(e.critical_path_flops), int(e.max_tree_width), int(e.mf_transient_peak_bytes))
 
     def symbolic_factor_nnz(self) -> int:
         """Exact symbolic fill x 1.2 slack (sparse_solver.rs:550-555)."""

@@ -61,3 +61,5 @@ def test_estimate_matches_structure():
     assert sym.symbolic_factor_nnz() == int(1.2 * int(np.sum(ex["col_counts"])))
     # the critical path is at least the root chain's own work and at most the total
     assert int(np.max(r * r * c)) <= e.critical_path_flops <= e.factor_flops
+    # the multifrontal figure adds every contribution block, (nrow - ncol)^2 scalars each
+    assert e.mf_transient_peak_bytes == e.transient_peak_bytes + int(np.sum((r - c) ** 2)) * 16
